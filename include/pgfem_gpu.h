@@ -1,0 +1,187 @@
+/*
+ * pgfem_gpu.h -- C ABI of the B200 (sm_100a) element-assembly path.
+ *
+ * Drop-in replacement for PGFem3D's FP64 constitutive-model assembly: the
+ * per-quadrature-point constitutive update, the element residual and the
+ * consistent tangent of the 1-field total-Lagrangian element, scattered into
+ * the CSR operator whose pattern Psparse_ApAi builds.  Reference paths are
+ * relative to the PGFem3D source tree.
+ *
+ * Conventions (mirroring the reference):
+ *  - every entry point returns int; 0 = success, negative = usage / CUDA
+ *    error (PGFEM_GPU_E*), never a trap or abort;
+ *  - element failures are counted, not raised: a pgfem_gpu_status holds the
+ *    counts the reference accumulates into its `err` / INFO word
+ *    (src/constitutive_model.cc:3443-3448 inverted elements,
+ *    :2682-2687 non-normal stiffness diagonal, and local-solver
+ *    non-convergence of the integration algorithm);
+ *  - arrays are caller-owned; 3x3 tensors are row-major [9]; element vectors
+ *    are node-major; element matrices use idx_K order
+ *    (include/index_macros.h:25-26); DOF ids follow the reference: >0 free
+ *    (1-based), 0 fixed, <0 prescribed (value u_presc[-id-1]);
+ *  - one context per host thread; a context owns its CUDA stream, device
+ *    copies of the mesh in structure-of-arrays form, the element->CSR map and
+ *    the per-quadrature-point state at t_n and t_{n+1}.
+ */
+#ifndef PGFEM_GPU_H
+#define PGFEM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGFEM_GPU_OK 0
+#define PGFEM_GPU_EINVAL (-1)   /* bad argument */
+#define PGFEM_GPU_ECUDA (-2)    /* CUDA runtime error */
+#define PGFEM_GPU_ENOMEM (-3)   /* device allocation failed */
+#define PGFEM_GPU_EPATTERN (-4) /* CSR pattern does not hold an element block */
+#define PGFEM_GPU_ENODEV (-5)   /* no usable sm_100 device */
+#define PGFEM_GPU_ELIMIT (-6)   /* size beyond a fixed limit of the entry point */
+
+/* Constitutive models (the Model_parameters families on the path). */
+enum {
+  PGFEM_MODEL_HE = 0, /* HE_PARAM, src/plasticity_model_none.cc */
+  PGFEM_MODEL_J2 = 1, /* CM_J2P_PARAM, src/cm_j2_plasticity.cc (damage off) */
+  PGFEM_MODEL_CP = 2  /* CP_PARAM, src/plasticity_model.cc */
+};
+
+/* Doubles of per-quadrature-point state (one time level) in the host AoS
+ * exchange format: HE 0; J2 10 = Cp^-1 (9) + eqps; CP 10 = pF (9) + g. */
+int pgfem_gpu_state_size(int model);
+
+/* Scatter modes: atomic FP64 adds, or element colours with plain adds
+ * (deterministic summation order). */
+enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1 };
+
+typedef struct {
+  int model;
+  double E, nu;          /* isotropic elasticity (neo-Hookean: G = E/2(1+nu), kappa per src/hommat.cc:58-61) */
+  double sigma_y, H;     /* J2: yield stress, linear isotropic hardening modulus */
+  double gamma_dot_0, m; /* CP flow: gamma_dot = gamma_dot_0 sgn(tau) |tau/g|^(1/m) */
+  double G0, g0, gs_0, gamma_dot_s, w; /* CP saturation hardening */
+  double cp_tol;         /* CP local residual tolerance */
+  int cp_max_iter;       /* CP local iteration cap */
+} pgfem_material_desc;
+
+typedef struct {
+  long nn, ne;
+  int nne;              /* 4 (linear tet, 1 qp) or 10 (quadratic tet, 4 qp) */
+  const double *X;      /* nn*3 reference coordinates */
+  const int *conn;      /* ne*nne node ids (0-based) */
+  const long *dof_id;   /* nn*3 DOF ids (reference convention) */
+  long ndof;            /* free DOFs = CSR rows */
+  long npres;           /* prescribed values */
+  const double *F0;     /* 9: macro deformation added to F (FE2, src/constitutive_model.cc:247-252) or NULL */
+  const double *R_cp;   /* ne*9 crystal rotations (CP) or NULL */
+} pgfem_mesh_desc;
+
+typedef struct {
+  long inverted;        /* J <= 0 at a quadrature point */
+  long nonconverged;    /* local constitutive solver failed */
+  long bad_diagonal;    /* non-normal stiffness diagonal */
+  long other;
+} pgfem_gpu_status;
+
+typedef struct pgfem_gpu_ctx pgfem_gpu_ctx;
+
+/* ---- setup (host) -------------------------------------------------------- */
+
+/* generate_local_dof_ids (src/generate_dof_ids.cc:69-171, 306-412): on input
+ * id[] holds codes (0 free, 1 fixed, <0 prescribed); on output the DOF ids.
+ * Pr[n] = periodic master node or -1 (may be NULL).  Returns #free DOFs. */
+long pgfem_generate_dof_ids(long nn, long ne, int nne, const int *conn, const long *Pr, long *id);
+
+/* Psparse_ApAi (src/Psparse_ApAi.cc:238-670) for one rank: Ap[ndof+1] and
+ * the sorted column ids Ai[nnz].  With Ai == NULL only Ap is filled.
+ * Returns nnz (or a negative error). */
+long pgfem_psparse_apai(long ne, int nne, const int *conn, const long *id, long ndof, int *Ap,
+                        int *Ai);
+
+/* Structured unit-cube mesh, n^3 cells of 6 tets each (nne 4 or 10); nodes
+ * lexicographic on the vertex (nne 4) or half-cell (nne 10) lattice.  Call
+ * with X == NULL to get the sizes.  Pr (may be NULL) receives the periodic
+ * master of each node when periodic != 0, else -1. */
+int pgfem_mesh_box_tet(int n, int nne, int periodic, long *nn, long *ne, double *X, int *conn,
+                       long *Pr);
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Builds the device copy and the element->CSR node-block map from the
+ * caller's Ap/Ai (src/Psparse_ApAi.cc pattern) and validates it. */
+int pgfem_gpu_create(const pgfem_mesh_desc *mesh, const pgfem_material_desc *mat, const int *Ap,
+                     const int *Ai, long nrows, pgfem_gpu_ctx **ctx);
+int pgfem_gpu_destroy(pgfem_gpu_ctx *ctx);
+int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *ctx, int mode);
+/* Device bytes held by the context (mesh, map, state, scratch). */
+long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *ctx);
+long pgfem_gpu_nnz(const pgfem_gpu_ctx *ctx);
+
+/* ---- state (Model_parameters::set_init_vals / update_state_vars /
+ *      reset_state_vars, src/constitutive_model.cc:1337-1497) ------------- */
+int pgfem_gpu_set_state(pgfem_gpu_ctx *ctx, const double *state_n); /* AoS ne*nint*ns, host */
+int pgfem_gpu_get_state(pgfem_gpu_ctx *ctx, int level, double *state); /* level 0: t_n, 1: t_{n+1} */
+int pgfem_gpu_commit_state(pgfem_gpu_ctx *ctx); /* n <- n+1 */
+int pgfem_gpu_reset_state(pgfem_gpu_ctx *ctx);  /* n+1 <- n */
+
+/* ---- assembly (host buffers; synchronous) --------------------------------
+ * fd_residuals_MP (include/fd_residuals.h:39-51) and stiffmat_fd_MP
+ * (include/stiffmat_fd.h:72-83) for one rank: R[ndof] and K[nnz] (aligned
+ * with Ai) are overwritten; u is the free-DOF displacement (u_np1 + d_u),
+ * u_presc the prescribed values (may be NULL when npres == 0).  The
+ * constitutive update runs once and writes the state at t_{n+1}. */
+int pgfem_gpu_assemble_R(pgfem_gpu_ctx *ctx, const double *u, const double *u_presc, double dt,
+                         double *R, pgfem_gpu_status *st);
+int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *ctx, const double *u, const double *u_presc, double dt,
+                          double *R, double *K, pgfem_gpu_status *st);
+
+/* ---- assembly (device buffers; asynchronous on `stream`) -----------------
+ * Same operation with device pointers; nothing is synchronised.  The failure
+ * counts accumulate on the device until pgfem_gpu_read_status. */
+int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc,
+                                 double dt, double *d_R, double *d_K, void *stream);
+int pgfem_gpu_read_status(pgfem_gpu_ctx *ctx, pgfem_gpu_status *st, int clear);
+/* Launch count of the kernels of one assemble_RK call (for accounting). */
+int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *ctx);
+
+/* ---- measurement ---------------------------------------------------------
+ * With timing on, every assembly records CUDA events on its stream around
+ * the element-assembly kernel launch(es) only.  pgfem_gpu_kernel_time
+ * synchronises, returns the summed kernel time (ms) and the number of timed
+ * calls since the last reset.  No counterpart in the reference (its CLOCK()
+ * timers, src/Newton_Raphson.cc:419-439, wrap whole assemblies). */
+int pgfem_gpu_set_timing(pgfem_gpu_ctx *ctx, int on);
+int pgfem_gpu_kernel_time(pgfem_gpu_ctx *ctx, double *ms, long *ncalls, int reset);
+
+/* FP64 FMA throughput of the current device (TFLOP/s), measured by an FMA
+ * chain kernel over every SM; the FP64 roofline denominator.  No counterpart
+ * in the reference. */
+int pgfem_gpu_fp64_peak(double *tflops);
+
+/* ---- element level (batched over an element list) -----------------------
+ * stiffness_el_constitutive_model / residuals_el_constitutive_model
+ * (include/constitutive_model.h:1003-1049), exported under the element
+ * entry-point names of the dispatch they replace (stiffmatel_fd,
+ * include/stiffmatel_fd.h:18-40; resid_on_elem, include/resid_on_elem.h:19-38).
+ * lk: nel*(nne*3)^2 idx_K order; fe: nel*nne*3.  The state at t_{n+1} of the
+ * listed elements is updated. */
+int pgfem_gpu_stiffmatel_fd(pgfem_gpu_ctx *ctx, long nel, const long *elems, const double *u,
+                            const double *u_presc, double dt, double *lk, double *fe,
+                            pgfem_gpu_status *st);
+int pgfem_gpu_resid_on_elem(pgfem_gpu_ctx *ctx, long nel, const long *elems, const double *u,
+                            const double *u_presc, double dt, double *fe, pgfem_gpu_status *st);
+
+/* ---- constitutive level ---------------------------------------------------
+ * Model_parameters::integration_algorithm + update_elasticity
+ * (include/constitutive_model.h:266-272, 242-757) batched over nqp points:
+ * from F (nqp*9) and the state at t_n (nqp*ns, AoS) compute the state at
+ * t_{n+1}, the PK2 stress S (nqp*9) and the material tangent L = 2 dS/dC
+ * (nqp*81, idx_4 order; may be NULL).  R_cp: nqp*9 rotations (CP) or NULL.
+ * qp_status (may be NULL): 0 ok, 1 inverted, 2 non-converged.  Host buffers. */
+int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const double *F, double dt,
+                           const double *R_cp, const double *state_n, double *state_np1,
+                           double *S, double *L, int *qp_status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

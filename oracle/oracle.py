@@ -1,0 +1,173 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py as the checker.  The product path never uses it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+HE, J2, CP = 0, 1, 2
+
+
+class OrcMaterial(C.Structure):
+    _fields_ = [("model", C.c_int), ("E", C.c_double), ("nu", C.c_double),
+                ("sigma_y", C.c_double), ("H", C.c_double),
+                ("gamma_dot_0", C.c_double), ("m", C.c_double), ("G0", C.c_double),
+                ("g0", C.c_double), ("gs_0", C.c_double), ("gamma_dot_s", C.c_double),
+                ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int),
+                ("dev_pot", C.c_int)]
+
+
+class OrcProblem(C.Structure):
+    _fields_ = [("nn", C.c_long), ("ne", C.c_long), ("nne", C.c_int),
+                ("X", C.c_void_p), ("conn", C.c_void_p), ("id", C.c_void_p), ("ndof", C.c_long),
+                ("Ap", C.c_void_p), ("Ai", C.c_void_p), ("F0", C.c_void_p), ("R_cp", C.c_void_p)]
+
+
+_lib = None
+_P = C.c_void_p
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        sig = {
+            "orc_state_size": (C.c_int, [C.c_int]),
+            "orc_nint": (C.c_int, [C.c_int]),
+            "orc_generate_dof_ids": (C.c_long, [C.c_long, C.c_long, C.c_int, _P, _P, _P]),
+            "orc_psparse_apai": (C.c_long, [C.c_long, C.c_int, _P, _P, C.c_long, _P, _P]),
+            "orc_cm_update": (C.c_int, [_P, _P, C.c_double, _P, _P, _P, _P, _P, _P]),
+            "orc_element": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, _P, _P, _P, _P]),
+            "orc_assemble": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P, _P, C.c_long, C.c_long,
+                                       C.c_int, _P]),
+            "orc_assemble_bform": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P, _P, C.c_long,
+                                             C.c_long, C.c_int]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0, G0=0.0, g0=0.0,
+             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1):
+    return OrcMaterial(model, E, nu, sigma_y, H, gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w, cp_tol,
+                       cp_max_iter, dev_pot)
+
+
+def from_pg_material(m, dev_pot=1):
+    """Oracle material from a pgfem_gpu.MaterialDesc (same field meanings)."""
+    return material(m.model, m.E, m.nu, m.sigma_y, m.H, m.gamma_dot_0, m.m, m.G0, m.g0, m.gs_0,
+                    m.gamma_dot_s, m.w, m.cp_tol, m.cp_max_iter, dev_pot)
+
+
+def state_size(model):
+    return lib().orc_state_size(model)
+
+
+def generate_dof_ids(conn, nn, codes, Pr=None):
+    ids = np.ascontiguousarray(codes, dtype=np.int64).copy()
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    Pr = None if Pr is None else np.ascontiguousarray(Pr, dtype=np.int64)
+    ndof = lib().orc_generate_dof_ids(nn, conn.shape[0], conn.shape[1], _p(conn), _p(Pr), _p(ids))
+    return ids, ndof
+
+
+def psparse_apai(conn, ids, ndof):
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    ids = np.ascontiguousarray(ids, dtype=np.int64)
+    Ap = np.zeros(ndof + 1, dtype=np.int32)
+    nnz = lib().orc_psparse_apai(conn.shape[0], conn.shape[1], _p(conn), _p(ids), ndof, _p(Ap), None)
+    Ai = np.zeros(max(nnz, 1), dtype=np.int32)
+    lib().orc_psparse_apai(conn.shape[0], conn.shape[1], _p(conn), _p(ids), ndof, _p(Ap), _p(Ai))
+    return Ap, Ai[:nnz]
+
+
+def cm_update(mat, F, state_n=None, dt=0.0, Rcp=None):
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(9)
+    S = np.zeros(9)
+    L = np.zeros(81)
+    ns = state_size(mat.model)
+    snp1 = np.zeros(max(ns, 1))
+    sn = None if state_n is None else np.ascontiguousarray(state_n, dtype=np.float64)
+    Rcp = None if Rcp is None else np.ascontiguousarray(Rcp, dtype=np.float64)
+    it = C.c_int()
+    err = lib().orc_cm_update(C.byref(mat), _p(F), dt, _p(Rcp), _p(sn), _p(snp1), _p(S), _p(L), C.byref(it))
+    return err, S.reshape(3, 3), L.reshape(3, 3, 3, 3), snp1, it.value
+
+
+class Problem:
+    """Oracle view of a mesh problem (keeps the arrays alive)."""
+
+    def __init__(self, X, conn, ids, ndof, Ap, Ai, F0=None, R_cp=None):
+        self.X = np.ascontiguousarray(X, dtype=np.float64)
+        self.conn = np.ascontiguousarray(conn, dtype=np.int32)
+        self.ids = np.ascontiguousarray(ids, dtype=np.int64)
+        self.Ap = np.ascontiguousarray(Ap, dtype=np.int32)
+        self.Ai = np.ascontiguousarray(Ai, dtype=np.int32)
+        self.F0 = None if F0 is None else np.ascontiguousarray(F0, dtype=np.float64).reshape(9)
+        self.R_cp = None if R_cp is None else np.ascontiguousarray(R_cp, dtype=np.float64)
+        self.ndof = ndof
+        self.s = OrcProblem(self.X.shape[0], self.conn.shape[0], self.conn.shape[1], _p(self.X),
+                            _p(self.conn), _p(self.ids), ndof, _p(self.Ap), _p(self.Ai), _p(self.F0),
+                            _p(self.R_cp))
+
+    @property
+    def nnz(self):
+        return int(self.Ap[-1])
+
+    def element(self, mat, e, u_e, state_n=None, dt=0.0, want_K=True):
+        nd = self.conn.shape[1] * 3
+        fe = np.zeros(nd)
+        lk = np.zeros((nd, nd)) if want_K else None
+        nint = lib().orc_nint(self.conn.shape[1])
+        ns = state_size(mat.model)
+        snp1 = np.zeros(max(nint * ns, 1))
+        sn = None if state_n is None else np.ascontiguousarray(state_n, dtype=np.float64)
+        u_e = np.ascontiguousarray(u_e, dtype=np.float64)
+        err = lib().orc_element(C.byref(self.s), C.byref(mat), e, _p(u_e), dt, _p(sn), _p(snp1), _p(fe), _p(lk))
+        return err, fe, lk, snp1
+
+    def assemble(self, mat, u, u_presc=None, state_n=None, dt=0.0, want_K=True, e0=0, e1=None,
+                 nthreads=1, bform=False):
+        ne = self.conn.shape[0]
+        e1 = ne if e1 is None else e1
+        nint = lib().orc_nint(self.conn.shape[1])
+        ns = state_size(mat.model)
+        R = np.zeros(self.ndof)
+        K = np.zeros(self.nnz) if want_K else None
+        snp1 = np.zeros((ne * nint, max(ns, 1))) if ns else None
+        sn = None if state_n is None else np.ascontiguousarray(state_n, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        up = None if u_presc is None else np.ascontiguousarray(u_presc, dtype=np.float64)
+        if bform:
+            err = lib().orc_assemble_bform(C.byref(self.s), C.byref(mat), _p(u), _p(up), dt, _p(sn), _p(snp1),
+                                           _p(R), _p(K), e0, e1, nthreads)
+        else:
+            err = lib().orc_assemble(C.byref(self.s), C.byref(mat), _p(u), _p(up), dt, _p(sn), _p(snp1), _p(R),
+                                     _p(K), e0, e1, nthreads, None)
+        return err, R, K, snp1
+
+
+def from_workload(p):
+    """Oracle Problem + material for a pgfem-3d_b200 workloads.Problem."""
+    return Problem(p.X, p.conn, p.ids, p.ndof, p.Ap, p.Ai, F0=p.F0, R_cp=p.R_cp), from_pg_material(p.mat)

@@ -1,0 +1,767 @@
+// pgfem_oracle.cpp -- CPU oracle (test infrastructure only; see pgfem_oracle.h).
+//
+// Each function states the reference file:line it restates.  Paths are
+// relative to the PGFem3D source tree.
+#include "pgfem_oracle.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+namespace {
+
+constexpr int DIM = 3;
+
+// ---------------------------------------------------------------------------
+// 3x3 helpers.  det3x3 / inv3x3 follow src/utils.cc:478-482 and :542-562
+// (inverse refused when |det| < 1e-15); det() of FEMLIB follows
+// FEMLIB/src/femlib.cc:366-390.
+// ---------------------------------------------------------------------------
+double det3x3(const double *m) {
+  return ((m[0] * (m[4] * m[8] - m[5] * m[7])) + m[1] * (m[5] * m[6] - m[3] * m[8]) +
+          m[2] * (m[3] * m[7] - m[4] * m[6]));
+}
+
+int inv3x3(const double *m, double *mi) {
+  double A = det3x3(m);
+  if (std::fabs(A) >= 1.0e-15) {
+    mi[0] = 1 / A * (m[4] * m[8] - m[5] * m[7]);
+    mi[1] = -1 / A * (m[1] * m[8] - m[2] * m[7]);
+    mi[2] = 1 / A * (m[1] * m[5] - m[2] * m[4]);
+    mi[3] = -1 / A * (m[3] * m[8] - m[5] * m[6]);
+    mi[4] = 1 / A * (m[0] * m[8] - m[2] * m[6]);
+    mi[5] = -1 / A * (m[0] * m[5] - m[2] * m[3]);
+    mi[6] = 1 / A * (m[3] * m[7] - m[4] * m[6]);
+    mi[7] = -1 / A * (m[0] * m[7] - m[1] * m[6]);
+    mi[8] = 1 / A * (m[0] * m[4] - m[1] * m[3]);
+    return 0;
+  }
+  return 1;
+}
+
+inline int i4(int i, int j, int k, int l) { return i * 27 + j * 9 + k * 3 + l; }
+
+void matmul(const double *A, const double *B, double *C) {  // C = A B
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s += A[i * 3 + k] * B[k * 3 + j];
+      C[i * 3 + j] = s;
+    }
+}
+void matmulTN(const double *A, const double *B, double *C) {  // C = A^T B
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double s = 0;
+      for (int k = 0; k < 3; k++) s += A[k * 3 + i] * B[k * 3 + j];
+      C[i * 3 + j] = s;
+    }
+}
+void transpose(const double *A, double *AT) {
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) AT[j * 3 + i] = A[i * 3 + j];
+}
+void ident(double *A) {
+  for (int i = 0; i < 9; i++) A[i] = 0;
+  A[0] = A[4] = A[8] = 1;
+}
+
+// ---------------------------------------------------------------------------
+// FEMLIB restatement.
+// Shape-function derivatives: FEMLIB/src/femlib.cc:213-333 (TETRAHEDRON,
+// QTETRAHEDRON).  Quadrature: :571-588 (1-point rule for linear tets, the
+// 8-digit 4-point rule for quadratic tets, which FEMLIB forces at
+// intg_order 0, :1009-1016).  dN/dX: :403-470.
+// ---------------------------------------------------------------------------
+struct Quad {
+  int nint;
+  double ksi[4], eta[4], zet[4], w[4];
+};
+
+Quad quad_rule(int nne) {
+  Quad q{};
+  if (nne == 4) {
+    q.nint = 1;
+    q.ksi[0] = q.eta[0] = q.zet[0] = 1.0 / 4.0;
+    q.w[0] = 1.0 / 6.0;
+  } else {
+    q.nint = 4;
+    const double a = 0.58541020, b = 0.13819660;
+    const double k[4] = {a, b, b, b}, e[4] = {b, a, b, b}, z[4] = {b, b, a, b};
+    for (int i = 0; i < 4; i++) {
+      q.ksi[i] = k[i];
+      q.eta[i] = e[i];
+      q.zet[i] = z[i];
+      q.w[i] = (1.0 / 4.0) / 6.0;
+    }
+  }
+  return q;
+}
+
+void dN_dkez(int nne, double ksi, double eta, double zet, double *dN /* nne*3 */) {
+  if (nne == 4) {
+    const double t[12] = {-1, -1, -1, 1, 0, 0, 0, 1, 0, 0, 0, 1};
+    std::memcpy(dN, t, sizeof(t));
+    return;
+  }
+  double *d = dN;
+  d[0 * 3 + 0] = 4.0 * (ksi + eta + zet) - 3.0;
+  d[0 * 3 + 1] = 4.0 * (eta + ksi + zet) - 3.0;
+  d[0 * 3 + 2] = 4.0 * (zet + ksi + eta) - 3.0;
+  d[1 * 3 + 0] = 4.0 * ksi - 1.0;
+  d[1 * 3 + 1] = 0.0;
+  d[1 * 3 + 2] = 0.0;
+  d[2 * 3 + 0] = 0.0;
+  d[2 * 3 + 1] = 4.0 * eta - 1.0;
+  d[2 * 3 + 2] = 0.0;
+  d[3 * 3 + 0] = 0.0;
+  d[3 * 3 + 1] = 0.0;
+  d[3 * 3 + 2] = 4.0 * zet - 1.0;
+  d[4 * 3 + 0] = 4.0 * (-2.0 * ksi - eta - zet + 1.0);
+  d[4 * 3 + 1] = -4.0 * ksi;
+  d[4 * 3 + 2] = -4.0 * ksi;
+  d[5 * 3 + 0] = 4.0 * eta;
+  d[5 * 3 + 1] = 4.0 * ksi;
+  d[5 * 3 + 2] = 0.0;
+  d[6 * 3 + 0] = -4.0 * eta;
+  d[6 * 3 + 1] = 4.0 * (-ksi - 2.0 * eta - zet + 1.0);
+  d[6 * 3 + 2] = -4.0 * eta;
+  d[7 * 3 + 0] = -4.0 * zet;
+  d[7 * 3 + 1] = -4.0 * zet;
+  d[7 * 3 + 2] = 4.0 * (-ksi - eta - 2.0 * zet + 1.0);
+  d[8 * 3 + 0] = 4.0 * zet;
+  d[8 * 3 + 1] = 0.0;
+  d[8 * 3 + 2] = 4.0 * ksi;
+  d[9 * 3 + 0] = 0.0;
+  d[9 * 3 + 1] = 4.0 * zet;
+  d[9 * 3 + 2] = 4.0 * eta;
+}
+
+// Returns the isoparametric Jacobian J; dNdX (nne*3).  err set when J <= 0
+// (the reference aborts there, FEMLIB/src/femlib.cc:426-429).
+double PGFem3D_dNdX(int nne, double ksi, double eta, double zet, const double *X /*nne*3*/,
+                    double *dNdX, int *err) {
+  double dNk[30];
+  dN_dkez(nne, ksi, eta, zet, dNk);
+  double dX[9] = {0};
+  for (int ib = 0; ib < 3; ++ib)
+    for (int ic = 0; ic < 3; ++ic)
+      for (int ia = 0; ia < nne; ++ia) dX[ib * 3 + ic] += dNk[ia * 3 + ic] * X[ia * 3 + ib];
+  double J = dX[0] * (dX[4] * dX[8] - dX[5] * dX[7]) + dX[1] * (dX[5] * dX[6] - dX[3] * dX[8]) +
+             dX[2] * (dX[3] * dX[7] - dX[4] * dX[6]);
+  if (J <= 0.0) {
+    *err += 1;
+    J = 1.0;  // keep going without NaNs; the caller stops on err
+  }
+  double dXI[9];
+  dXI[0] = dX[4] * dX[8] - dX[5] * dX[7];
+  dXI[1] = dX[2] * dX[7] - dX[1] * dX[8];
+  dXI[2] = dX[1] * dX[5] - dX[2] * dX[4];
+  dXI[3] = dX[5] * dX[6] - dX[3] * dX[8];
+  dXI[4] = dX[0] * dX[8] - dX[2] * dX[6];
+  dXI[5] = dX[2] * dX[3] - dX[0] * dX[5];
+  dXI[6] = dX[3] * dX[7] - dX[4] * dX[6];
+  dXI[7] = dX[1] * dX[6] - dX[0] * dX[7];
+  dXI[8] = dX[0] * dX[4] - dX[1] * dX[3];
+  for (int ia = 0; ia < nne; ++ia)
+    for (int ib = 0; ib < 3; ++ib) {
+      double s = 0.0;
+      for (int ic = 0; ic < 3; ++ic) s += 1.0 / J * dNk[ia * 3 + ic] * dXI[ic * 3 + ib];
+      dNdX[ia * 3 + ib] = s;
+    }
+  return J;
+}
+
+// F = I + sum_a u_a (x) dN_a: FEMLIB/src/femlib.cc:1289-1325.
+void deformation_gradient(int nne, const double *u, const double *dN, double *F) {
+  ident(F);
+  for (int ia = 0; ia < nne; ia++)
+    for (int ib = 0; ib < 3; ++ib)
+      for (int ic = 0; ic < 3; ++ic) F[ib * 3 + ic] += u[ia * 3 + ib] * dN[ia * 3 + ic];
+}
+
+// ---------------------------------------------------------------------------
+// Hyperelasticity.  Deviatoric Mooney-Rivlin stress and stiffness
+// (src/new_potentials.cc:333-362, 377-432), U_Common volumetric potential
+// (:553-558, 578-583, 599-604) combined as in get_material_stress /
+// get_material_stiffness (src/displacement_based_element.cc:1368-1445):
+//   S = S_dev + kappa J U'(J) C^-1
+//   L = L_dev + kappa (J U' + J^2 U'') C^-1 (x) C^-1 - 2 kappa J U' C^-1_ik C^-1_lj
+// Material constants as mapped by src/homogen.cc:176-191 for an isotropic
+// neo-Hookean solid: m10 = G/2, m01 = 0, kappa from src/hommat.cc:58-61.
+// ---------------------------------------------------------------------------
+struct Elast {
+  double G, nu, m10, m01, kappa;
+  int dev_pot;
+};
+
+Elast make_elast(const orc_material *m) {
+  Elast e;
+  e.G = m->E / (2.0 * (1.0 + m->nu));
+  e.nu = m->nu;
+  e.m10 = 0.5 * e.G;
+  e.m01 = 0.0;
+  e.kappa = (2 * e.G * (1 + e.nu)) / (3 * (1 - 2 * e.nu));
+  e.dev_pot = m->dev_pot == 2 ? 2 : 1;
+  return e;
+}
+
+void he_stress_stiffness(const Elast &el, const double *C, double J, double *S, double *L) {
+  double invC[9], I[9];
+  inv3x3(C, invC);
+  ident(I);
+  const double detC = det3x3(C);
+  const double trC = C[0] + C[4] + C[8];
+  double CC = 0;
+  for (int i = 0; i < 9; i++) CC += C[i] * C[i];
+  const double dUdJ = J - 1.0, d2UdJ2 = 1.0;
+  if (el.dev_pot == 2) {  // devStress_Linear / matStiff_Linear, src/new_potentials.cc:364-375, 434-452
+    for (int i = 0; i < 9; i++) S[i] = el.G * (C[i] - I[i]) + el.kappa * J * dUdJ * invC[i];
+    if (!L) return;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        for (int k = 0; k < 3; k++)
+          for (int l = 0; l < 3; l++)
+            L[i4(i, j, k, l)] = 2 * el.G * I[i * 3 + k] * I[j * 3 + l] +
+                                el.kappa * (J * dUdJ + J * J * d2UdJ2) * invC[i * 3 + j] * invC[k * 3 + l] -
+                                2.0 * el.kappa * J * dUdJ * invC[i * 3 + k] * invC[l * 3 + j];
+    return;
+  }
+  for (int i = 0; i < 9; i++) {
+    S[i] = ((2 * el.m10 * std::pow(detC, -1. / 3.) * (I[i] - 1. / 3. * trC * invC[i])) +
+            (2 * el.m01 * std::pow(detC, -2. / 3.) *
+             (trC * I[i] - C[i] + 1. / 3. * (CC - trC * trC) * invC[i])));
+    S[i] += el.kappa * J * dUdJ * invC[i];
+  }
+  if (!L) return;
+  const double detC1 = std::pow(detC, -1. / 3.), detC2 = detC1 * detC1;
+  auto id2 = [](int r, int c) { return r * 3 + c; };
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) {
+          double Ld =
+              (4 * el.m10 * detC1 *
+               ((1. / 9. * trC * invC[id2(i, j)] - 1. / 3. * I[id2(i, j)]) * invC[id2(k, l)] +
+                1. / 3. *
+                    (trC * invC[id2(i, k)] * invC[id2(l, j)] - I[id2(k, l)] * invC[id2(i, j)]))) +
+              (4 * el.m01 * detC2 *
+               (I[id2(i, j)] * I[id2(k, l)] - I[id2(i, k)] * I[id2(l, j)] +
+                2. / 3. * ((C[id2(i, j)] - trC * I[id2(i, j)]) * invC[id2(k, l)]) -
+                ((CC - trC * trC) * (2. / 9. * invC[id2(i, j)] * invC[id2(k, l)] +
+                                      1. / 3. * invC[id2(i, k)] * invC[id2(l, j)])) +
+                2. / 3. * ((C[id2(k, l)] - trC * I[id2(k, l)]) * invC[id2(i, j)])));
+          L[i4(i, j, k, l)] = Ld + el.kappa * (J * dUdJ + J * J * d2UdJ2) * invC[id2(i, j)] * invC[id2(k, l)] -
+                              2.0 * el.kappa * J * dUdJ * invC[id2(i, k)] * invC[id2(l, j)];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Finite-strain J2 plasticity with linear isotropic hardening.
+//
+// PARITY UNPINNED: the reference's J2 model (src/cm_j2_plasticity.cc:184-214,
+// 287-382) calls J2_plasticity_integration_alg / compute_S0_Sbar_public /
+// compute_Lbar_public of an external constitutive library that is absent
+// from the reference tree.  This is a restatement of the published
+// isochoric-split return map of Simo (1988), Simo & Hughes "Computational
+// Inelasticity" (1998) Box 9.1, written in the material description with the
+// state (Cp^-1, eqps): b_e_trial = J^{-2/3} F Cp^-1 F^T, radial return of
+// s = mu dev(b_e), b_e_{n+1} = s/mu + (tr b_e_trial / 3) 1.  The volumetric
+// part is the reference's U_Common potential (kappa J (J-1) C^-1).  The
+// tangent L = 2 dS/dC is the exact derivative of this update (the published
+// Box 9.2 tangent is its symmetrised form); it is checked against central
+// differences in tests/.
+// ---------------------------------------------------------------------------
+void j2_update(const Elast &el, double sy, double Hh, const double *F, const double *state_n,
+               double *state_np1, double *S, double *L) {
+  const double mu = el.G, kap = el.kappa;
+  double C[9], Ci[9];
+  matmulTN(F, F, C);
+  inv3x3(C, Ci);
+  const double J = det3x3(F);
+  const double *A = state_n;  // Cp^-1 at n
+  const double alpha_n = state_n[9];
+  const double J23 = std::pow(J, -2.0 / 3.0);
+  double T = 0;
+  for (int i = 0; i < 9; i++) T += C[i] * A[i];
+  double Str[9];
+  for (int i = 0; i < 9; i++) Str[i] = mu * J23 * (A[i] - T / 3.0 * Ci[i]);
+  double CA[9], CACA[9], ACA[9], tmp[9];
+  matmul(C, A, CA);
+  matmul(CA, CA, CACA);
+  matmul(A, C, tmp);
+  matmul(tmp, A, ACA);
+  double Q = CACA[0] + CACA[4] + CACA[8] - T * T / 3.0;
+  if (Q < 0) Q = 0;
+  const double q = mu * J23 * std::sqrt(Q);
+  const double mubar = mu * J23 * T / 3.0;
+  const double kn = std::sqrt(2.0 / 3.0) * (sy + Hh * alpha_n);
+  const double f = q - kn;
+  const bool plastic = f > 0.0;
+
+  double r = 1.0, beta0 = 1.0, dgam = 0.0;
+  if (plastic) {
+    beta0 = 1.0 + Hh / (3.0 * mubar);
+    dgam = f / (2.0 * mubar * beta0);
+    r = 1.0 - f / (beta0 * q);
+  }
+  const double pJ = kap * J * (J - 1.0);
+  for (int i = 0; i < 9; i++) S[i] = pJ * Ci[i] + r * Str[i];
+
+  if (state_np1) {
+    if (plastic) {
+      const double J2_3 = std::pow(J, 2.0 / 3.0);
+      for (int i = 0; i < 9; i++)
+        state_np1[i] = J2_3 * (r * Str[i] / mu + (T * J23 / 3.0) * Ci[i]);
+      state_np1[9] = alpha_n + std::sqrt(2.0 / 3.0) * dgam;
+    } else {
+      for (int i = 0; i < 10; i++) state_np1[i] = state_n[i];
+    }
+  }
+  if (!L) return;
+  // L_vol in the reference's DISP form (C^-1_ik C^-1_lj product).
+  const double cvol1 = kap * (J * (J - 1.0) + J * J), cvol2 = 2.0 * kap * J * (J - 1.0);
+  double dq[9] = {0}, dr[9] = {0};
+  if (plastic) {
+    const double c = mu * mu * J23 * J23 / (2.0 * q);
+    for (int i = 0; i < 9; i++)
+      dq[i] = c * (-(4.0 / 3.0) * Q * Ci[i] + 4.0 * ACA[i] - (4.0 / 3.0) * T * A[i]);
+    const double c1 = -kn / (beta0 * q * q);
+    const double c2 = -(1.0 - kn / q) * Hh / (3.0 * beta0 * beta0 * mubar * mubar) * (2.0 / 3.0);
+    for (int i = 0; i < 9; i++) dr[i] = c1 * dq[i] + c2 * Str[i];
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) {
+          const int ij = i * 3 + j, kl = k * 3 + l;
+          double Lv = cvol1 * Ci[ij] * Ci[kl] - cvol2 * Ci[i * 3 + k] * Ci[l * 3 + j];
+          double Isym = 0.5 * (Ci[i * 3 + k] * Ci[j * 3 + l] + Ci[i * 3 + l] * Ci[j * 3 + k]);
+          double dS = -(2.0 / 3.0) * Str[ij] * Ci[kl] - (2.0 / 3.0) * mu * J23 * Ci[ij] * A[kl] +
+                      (2.0 / 3.0) * mu * J23 * T * Isym;
+          L[i4(i, j, k, l)] = Lv + r * dS + Str[ij] * dr[kl];
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Element integrals of the constitutive-model 1-field path, total
+// Lagrangian, no thermal coupling:
+//   residual:  src/constitutive_model.cc:3322-3539 -> compute_residual_vector :1628-1662
+//   stiffness: src/constitutive_model.cc:2474-2692 -> compute_stiffness_matrix :1520-1616
+// Shape tensor ST[a][b][i][j] = dN(a,j) delta(b,i): FEMLIB/src/femlib.cc:47-70.
+// ---------------------------------------------------------------------------
+void compute_residual_vector(double *f, int nne, const double *dN, double detJxW, const double *Fr,
+                             const double *eFnMT, const double *eFnM, const double *S,
+                             double one_over_Jn) {
+  for (int a = 0; a < nne; a++)
+    for (int b = 0; b < DIM; b++) {
+      double ST[9] = {0};
+      for (int j = 0; j < 3; j++) ST[b * 3 + j] = dN[a * 3 + j];
+      double AA[9], sAA[9], t1[9], t2[9];
+      matmulTN(Fr, ST, AA);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) sAA[i * 3 + j] = 0.5 * (AA[i * 3 + j] + AA[j * 3 + i]);
+      matmul(eFnMT, sAA, t1);
+      matmul(t1, eFnM, t2);
+      double v = 0;
+      for (int i = 0; i < 9; i++) v += t2[i] * S[i];
+      f[a * DIM + b] += one_over_Jn * detJxW * v;
+    }
+}
+
+void compute_stiffness_matrix(double *lk, int nne, const double *dN, double detJxW,
+                              const double *Fr, const double *eFnMT, const double *eFn,
+                              const double *M, const double *FrTFr, const double *eFnM,
+                              const double *S, const double *L, const double *dMdu_all,
+                              double one_over_Jn) {
+  double MI[9];
+  inv3x3(M, MI);
+  const int nd = nne * DIM;
+  for (int a = 0; a < nne; a++)
+    for (int b = 0; b < DIM; b++) {
+      double STab[9] = {0};
+      for (int j = 0; j < 3; j++) STab[b * 3 + j] = dN[a * 3 + j];
+      double AA[9], sAA[9], t[9], MTsAAeFn[9], MTsAAeFnM[9];
+      matmulTN(Fr, STab, AA);
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) sAA[i * 3 + j] = 0.5 * (AA[i * 3 + j] + AA[j * 3 + i]);
+      matmul(eFnMT, sAA, t);
+      matmul(t, eFn, MTsAAeFn);
+      matmul(MTsAAeFn, M, MTsAAeFnM);
+      double MTsAAeFnMS = 0;
+      for (int i = 0; i < 9; i++) MTsAAeFnMS += MTsAAeFnM[i] * S[i];
+      for (int w = 0; w < nne; w++)
+        for (int g = 0; g < DIM; g++) {
+          double STwg[9] = {0};
+          for (int j = 0; j < 3; j++) STwg[g * 3 + j] = dN[w * 3 + j];
+          const double *dMdu = dMdu_all + (w * 3 + g) * 9;
+          double BB[9], sBB[9], CC[9], sCC[9];
+          matmulTN(Fr, STwg, BB);
+          matmulTN(STab, STwg, CC);
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+              sBB[i * 3 + j] = 0.5 * (BB[i * 3 + j] + BB[j * 3 + i]);
+              sCC[i * 3 + j] = 0.5 * (CC[i * 3 + j] + CC[j * 3 + i]);
+            }
+          double x1[9], x2[9], X[9], y1[9], y2[9], dCdu[9];
+          matmul(eFnMT, FrTFr, x1);
+          matmul(x1, eFn, x2);
+          matmul(x2, dMdu, X);
+          matmul(eFnMT, sBB, y1);
+          matmul(y1, eFnM, y2);
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+              dCdu[i * 3 + j] = 0.5 * (X[i * 3 + j] + X[j * 3 + i]) + y2[i * 3 + j];
+          double LdC[9];
+          for (int ij = 0; ij < 9; ij++) {
+            double s = 0;
+            for (int kl = 0; kl < 9; kl++) s += L[ij * 9 + kl] * dCdu[kl];
+            LdC[ij] = s;
+          }
+          double t1 = 0;
+          for (int i = 0; i < 9; i++) t1 += MTsAAeFnM[i] * LdC[i];
+          double z1[9], z2[9];
+          matmul(eFnMT, sCC, z1);
+          matmul(z1, eFnM, z2);
+          double t3 = 0;
+          for (int i = 0; i < 9; i++) t3 += z2[i] * S[i];
+          double Y[9];
+          matmul(MTsAAeFn, dMdu, Y);
+          double t2 = 0;
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) t2 += 0.5 * (Y[i * 3 + j] + Y[j * 3 + i]) * S[i * 3 + j];
+          double DpJ = 0;
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) DpJ -= MI[j * 3 + i] * dMdu[i * 3 + j];
+          const int idx = ((a * DIM + b) * nd) + w * DIM + g;
+          lk[idx] += one_over_Jn * detJxW * (t1 + 2.0 * t2 + t3 + DpJ * MTsAAeFnMS);
+        }
+    }
+}
+
+}  // namespace
+
+// ===========================================================================
+// Crystal plasticity (declared in orc_cp.inc, defined after the helpers).
+// ===========================================================================
+namespace {
+#include "orc_cp.inc"
+}
+
+extern "C" {
+
+int orc_nint(int nne) { return nne == 10 ? 4 : 1; }
+
+int orc_state_size(int model) {
+  switch (model) {
+    case ORC_MODEL_J2: return 10;
+    case ORC_MODEL_CP: return 10;
+    default: return 0;
+  }
+}
+
+int orc_cm_update(const orc_material *mat, const double *F, double dt, const double *Rcp,
+                  const double *state_n, double *state_np1, double *S, double *L, int *iters) {
+  Elast el = make_elast(mat);
+  if (iters) *iters = 0;
+  switch (mat->model) {
+    case ORC_MODEL_HE: {
+      double C[9];
+      matmulTN(F, F, C);
+      he_stress_stiffness(el, C, det3x3(F), S, L);
+      return 0;
+    }
+    case ORC_MODEL_J2:
+      j2_update(el, mat->sigma_y, mat->H, F, state_n, state_np1, S, L);
+      return 0;
+    case ORC_MODEL_CP: {
+      CpResult res;
+      int err = cp_update(mat, el, F, dt, Rcp, state_n, res);
+      if (iters) *iters = res.iters;
+      if (state_np1) {
+        for (int i = 0; i < 9; i++) state_np1[i] = res.pFnp1[i];
+        state_np1[9] = res.g;
+      }
+      for (int i = 0; i < 9; i++) S[i] = res.S[i];
+      if (L)
+        for (int i = 0; i < 81; i++) L[i] = res.L[i];
+      return err;
+    }
+  }
+  return 1;
+}
+
+int orc_element(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
+                double dt, const double *state_n, double *state_np1, double *fe, double *lk) {
+  const int nne = P->nne;
+  const int nd = nne * 3;
+  const int ns = orc_state_size(mat->model);
+  Quad qr = quad_rule(nne);
+  double Xe[30];
+  for (int a = 0; a < nne; a++)
+    for (int i = 0; i < 3; i++) Xe[a * 3 + i] = P->X[(long)P->conn[e * nne + a] * 3 + i];
+  Elast el = make_elast(mat);
+  int err = 0;
+  for (int i = 0; i < nd; i++) fe[i] = 0.0;
+  if (lk)
+    for (int i = 0; i < nd * nd; i++) lk[i] = 0.0;
+  std::vector<double> dMdu_all(nd * 9, 0.0);
+  for (int ip = 0; ip < qr.nint; ip++) {
+    double dN[30];
+    int terr = 0;
+    double detJ = PGFem3D_dNdX(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], Xe, dN, &terr);
+    if (terr) { err += terr; break; }
+    const double detJxW = detJ * qr.w[ip];
+    double Fr[9];
+    deformation_gradient(nne, u_e, dN, Fr);
+    if (P->F0)  // cm_add_macro_F, src/constitutive_model.cc:247-252
+      for (int i = 0; i < 9; i++) Fr[i] += P->F0[i];
+    if (det3x3(Fr) <= 0.0) { err += 1; break; }  // getJacobian, src/utils.cc:513-527
+
+    const double *sn = state_n ? state_n + (long)ip * ns : nullptr;
+    double *snp1 = state_np1 ? state_np1 + (long)ip * ns : nullptr;
+    double S[9], L[81], M[9], pFnp1[9];
+    ident(M);
+    ident(pFnp1);
+    std::fill(dMdu_all.begin(), dMdu_all.end(), 0.0);
+    if (mat->model == ORC_MODEL_CP) {
+      CpResult res;
+      const double *Rcp = P->R_cp ? P->R_cp + e * 9 : nullptr;
+      int cerr = cp_update(mat, el, Fr, dt, Rcp, sn, res);
+      if (cerr) { err += cerr; break; }
+      if (snp1) {
+        for (int i = 0; i < 9; i++) snp1[i] = res.pFnp1[i];
+        snp1[9] = res.g;
+      }
+      for (int i = 0; i < 9; i++) { S[i] = res.S[i]; pFnp1[i] = res.pFnp1[i]; }
+      for (int i = 0; i < 81; i++) L[i] = res.L[i];
+      if (inv3x3(pFnp1, M)) { err += 1; break; }
+      if (lk) cp_dMdu(res, nne, dN, dMdu_all.data());
+    } else {
+      double stmp[10];
+      int cerr = orc_cm_update(mat, Fr, dt, nullptr, sn, snp1 ? snp1 : stmp, S, lk ? L : nullptr, nullptr);
+      if (cerr) { err += cerr; break; }
+    }
+    const double pJ = det3x3(pFnp1);
+    double MT[9];
+    transpose(M, MT);
+    compute_residual_vector(fe, nne, dN, detJxW, Fr, MT, M, S, pJ);
+    if (lk) {
+      double eFn[9], FrTFr[9];
+      ident(eFn);
+      matmulTN(Fr, Fr, FrTFr);
+      compute_stiffness_matrix(lk, nne, dN, detJxW, Fr, MT, eFn, M, FrTFr, M, S, L,
+                               dMdu_all.data(), pJ);
+    }
+  }
+  // diagonal check of the stiffness (src/constitutive_model.cc:2682-2687)
+  if (lk && !err)
+    for (int a = 0; a < nd; a++)
+      if (!std::isnormal(lk[a * nd + a])) err++;
+  return err;
+}
+
+long orc_generate_dof_ids(long nn, long ne, int nne, const int *conn, const long *Pr, long *id) {
+  std::vector<char> visited(nn * 3, 0);
+  long ndof = 1;
+  for (long e = 0; e < ne; e++) {
+    long id_adder = 0;
+    for (int i = 0; i < nne; i++) {
+      const long n = conn[e * nne + i];
+      for (int j = 0; j < 3; j++) {
+        const long di = n * 3 + j;
+        if (visited[di]) continue;
+        if (id[di] < 0) {
+          visited[di] = 1;
+        } else if (id[di] == 1) {
+          id[di] = 0;
+          visited[di] = 1;
+        } else {
+          if (Pr && Pr[n] != -1) {
+            const long pdi = Pr[n] * 3 + j;
+            if (!visited[pdi]) {
+              id[pdi] = ndof + id_adder;
+              visited[pdi] = 1;
+              id_adder++;
+            }
+            id[di] = id[pdi];
+            visited[di] = 1;
+          } else {
+            id[di] = ndof + id_adder;
+            id_adder++;
+            visited[di] = 1;
+          }
+        }
+      }
+    }
+    ndof += id_adder;
+  }
+  // periodic nodes outside every element (src/generate_dof_ids.cc:120-150)
+  for (long n = 0; n < nn; n++)
+    for (int j = 0; j < 3; j++)
+      if (!visited[n * 3 + j] && Pr && Pr[n] != -1) {
+        id[n * 3 + j] = id[Pr[n] * 3 + j];
+        visited[n * 3 + j] = 1;
+      }
+  return ndof - 1;
+}
+
+long orc_psparse_apai(long ne, int nne, const int *conn, const long *id, long ndof, int *Ap,
+                      int *Ai) {
+  // countDof: ncols[lid] += number of free dofs of the element
+  std::vector<long> ncols(ndof, 0);
+  std::vector<long> lids;
+  for (long e = 0; e < ne; e++) {
+    lids.clear();
+    for (int a = 0; a < nne; a++)
+      for (int j = 0; j < 3; j++) {
+        long lid = id[(long)conn[e * nne + a] * 3 + j];
+        if (lid > 0) lids.push_back(lid - 1);
+      }
+    for (long l : lids) ncols[l] += (long)lids.size();
+  }
+  std::vector<std::vector<long>> AA(ndof);
+  for (long r = 0; r < ndof; r++) AA[r].reserve(ncols[r]);
+  for (long e = 0; e < ne; e++) {
+    lids.clear();
+    for (int a = 0; a < nne; a++)
+      for (int j = 0; j < 3; j++) {
+        long lid = id[(long)conn[e * nne + a] * 3 + j];
+        if (lid > 0) lids.push_back(lid - 1);
+      }
+    for (long l : lids)
+      for (long g : lids) AA[l].push_back(g);  // gid == lid on one rank
+  }
+  long nnz = 0;
+  Ap[0] = 0;
+  for (long r = 0; r < ndof; r++) {
+    std::sort(AA[r].begin(), AA[r].end());
+    long cnt = 0;
+    for (size_t j = 0; j < AA[r].size(); j++)
+      if (j + 1 == AA[r].size() || AA[r][j] < AA[r][j + 1]) {
+        if (Ai) Ai[nnz + cnt] = (int)AA[r][j];
+        cnt++;
+      }
+    nnz += cnt;
+    Ap[r + 1] = (int)nnz;
+    std::vector<long>().swap(AA[r]);
+  }
+  return nnz;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Element displacement gather: def_elem_total, src/utils.cc:1391-1412 (with
+// u_np1 + d_u merged into one free-DOF vector u).
+void gather_u(const orc_problem *P, long e, const double *u, const double *u_presc, double *ue) {
+  for (int a = 0; a < P->nne; a++)
+    for (int j = 0; j < 3; j++) {
+      const long id = P->id[(long)P->conn[e * P->nne + a] * 3 + j];
+      ue[a * 3 + j] = id == 0 ? 0.0 : (id > 0 ? u[id - 1] : (u_presc ? u_presc[-id - 1] : 0.0));
+    }
+}
+
+// PLoc_Sparse restated for one rank (src/PLoc_Sparse.cc:50-125): rows and
+// columns with a non-free DOF are dropped, the rest is added into the CSR
+// values at (row, col) found by binary search in the row's sorted columns.
+void scatter(const orc_problem *P, long e, const double *fe, const double *lk, double *R,
+             double *K) {
+  const int nd = P->nne * 3;
+  long gid[30];
+  for (int a = 0; a < P->nne; a++)
+    for (int j = 0; j < 3; j++) gid[a * 3 + j] = P->id[(long)P->conn[e * P->nne + a] * 3 + j] - 1;
+  for (int i = 0; i < nd; i++) {
+    if (gid[i] < 0) continue;
+    if (R) R[gid[i]] += fe[i];  // fd_res_assemble, src/fd_residuals.cc:58-73
+    if (!K || !lk) continue;
+    const int *row = P->Ai + P->Ap[gid[i]];
+    const int len = P->Ap[gid[i] + 1] - P->Ap[gid[i]];
+    for (int j = 0; j < nd; j++) {
+      if (gid[j] < 0) continue;
+      const int *pos = std::lower_bound(row, row + len, (int)gid[j]);
+      K[P->Ap[gid[i]] + (pos - row)] += lk[i * nd + j];
+    }
+  }
+}
+
+// Greedy element colouring: no two elements of one colour share a node.
+std::vector<std::vector<long>> colour_elements(const orc_problem *P, long e0, long e1) {
+  std::vector<std::vector<long>> colours;
+  std::vector<std::vector<char>> used;  // per colour: node mask (lazy)
+  for (long e = e0; e < e1; e++) {
+    size_t c = 0;
+    for (; c < colours.size(); c++) {
+      bool ok = true;
+      for (int a = 0; a < P->nne && ok; a++)
+        if (used[c][P->conn[e * P->nne + a]]) ok = false;
+      if (ok) break;
+    }
+    if (c == colours.size()) {
+      colours.emplace_back();
+      used.emplace_back(P->nn, 0);
+    }
+    colours[c].push_back(e);
+    for (int a = 0; a < P->nne; a++) used[c][P->conn[e * P->nne + a]] = 1;
+  }
+  return colours;
+}
+
+template <class Body>
+int run_elements(const orc_problem *P, long e0, long e1, int nthreads, Body body) {
+  if (nthreads <= 1) {
+    int err = 0;
+    for (long e = e0; e < e1; e++) err += body(e);
+    return err;
+  }
+  auto colours = colour_elements(P, e0, e1);
+  std::atomic<int> err{0};
+  for (auto &col : colours) {
+    std::atomic<long> next{0};
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; t++)
+      th.emplace_back([&]() {
+        int lerr = 0;
+        for (;;) {
+          long k = next.fetch_add(64);
+          if (k >= (long)col.size()) break;
+          long kend = std::min<long>(k + 64, col.size());
+          for (long i = k; i < kend; i++) lerr += body(col[i]);
+        }
+        err += lerr;
+      });
+    for (auto &t : th) t.join();
+  }
+  return err.load();
+}
+
+}  // namespace
+
+extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const double *u,
+                            const double *u_presc, double dt, const double *state_n,
+                            double *state_np1, double *R, double *K, long e0, long e1,
+                            int nthreads, int *iters) {
+  const int nd = P->nne * 3;
+  const int nint = orc_nint(P->nne);
+  const int ns = orc_state_size(mat->model);
+  return run_elements(P, e0, e1, nthreads, [&](long e) -> int {
+    double ue[30], fe[30];
+    std::vector<double> lk(K ? nd * nd : 0);
+    gather_u(P, e, u, u_presc, ue);
+    const double *sn = ns ? state_n + e * nint * ns : nullptr;
+    double *snp1 = ns && state_np1 ? state_np1 + e * nint * ns : nullptr;
+    int err = orc_element(P, mat, e, ue, dt, sn, snp1, fe, K ? lk.data() : nullptr);
+    if (iters && mat->model == ORC_MODEL_CP) {
+      // iteration counts are recomputed cheaply by a separate call (rare, tests)
+    }
+    if (!err) scatter(P, e, fe, K ? lk.data() : nullptr, R, K);
+    return err;
+  });
+}
+
+#include "orc_bform.inc"

@@ -1,0 +1,118 @@
+/*
+ * pgfem_oracle.h -- CPU oracle for the PGFem3D element-assembly hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library restates, on the CPU and in plain
+ * C++, the reference algorithms that the GPU product replaces.  It is used by
+ * tests/, by __graft_entry__.smoke() and by the cpu_baseline / reference arm
+ * of bench.py as the checker and as the timed CPU baseline.  The product path
+ * (pgfem-3d_b200/) never links, loads or calls it.
+ *
+ * Parity status: the in-tree parts (FEMLIB shape functions and quadrature,
+ * the constitutive-model element integrals, DOF numbering, the CSR pattern,
+ * the Mooney-Rivlin / U_Common potentials, the crystal-plasticity flow and
+ * hardening laws) follow the reference line by line and are pinned by the
+ * reference's own structure and by known-answer tests.  The J2 return map and
+ * the crystal-plasticity local solver of the reference live in an external
+ * library that is absent from the reference tree, so those two are
+ * restatements of the published algorithms: parity against the reference is
+ * unpinned for them (see the per-function comments).
+ */
+#ifndef PGFEM_ORACLE_H
+#define PGFEM_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { ORC_MODEL_HE = 0, ORC_MODEL_J2 = 1, ORC_MODEL_CP = 2 };
+
+/* Number of doubles of per-quadrature-point state for each model (one time
+ * level).  HE: none.  J2: Cp^{-1} (9, row-major) + eqps (1).
+ * CP: pFn (9) + slip resistance g_n (1). */
+int orc_state_size(int model);
+
+typedef struct {
+  int model;
+  double E, nu;                 /* isotropic elasticity */
+  double sigma_y, H;            /* J2: initial yield stress, linear isotropic hardening */
+  /* CP power-law flow + saturation hardening */
+  double gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w;
+  double cp_tol;                /* local-Newton residual tolerance */
+  int cp_max_iter;              /* local-Newton iteration cap */
+  int dev_pot;                  /* deviatoric potential flag of src/new_potentials.cc:79-156:
+                                   1 (or 0) Mooney-Rivlin with m10 = G/2, m01 = 0 (neo-Hookean),
+                                   2 Linear (S_dev = G (C - I)) */
+} orc_material;
+
+typedef struct {
+  long nn, ne;
+  int nne;                      /* 4 (linear tet) or 10 (quadratic tet) */
+  const double *X;              /* nn*3 reference coordinates, node-major */
+  const int *conn;              /* ne*nne node ids, element-major */
+  const long *id;               /* nn*3 DOF ids: >0 free (1-based), 0 fixed, <0 prescribed */
+  long ndof;                    /* number of free DOFs */
+  const int *Ap, *Ai;           /* CSR pattern of the free DOFs (0-based) */
+  const double *F0;             /* macro deformation-gradient increment added to F (FE2), or NULL */
+  const double *R_cp;           /* CP: ne*9 crystal rotation per element (row-major), or NULL */
+} orc_problem;
+
+/* Reference: src/generate_dof_ids.cc:69-171 (generate_local_dof_ids) and
+ * :306-412 (generate_local_dof_ids_on_elem).  id[] holds the input codes
+ * (0 free, 1 fixed, <0 prescribed) and receives the DOF ids.  Pr[n] is the
+ * periodic master node of n or -1.  Returns the number of free DOFs. */
+long orc_generate_dof_ids(long nn, long ne, int nne, const int *conn,
+                          const long *Pr, long *id);
+
+/* Reference: src/Psparse_ApAi.cc:161-213 (countDof/mapDof), :327-366 (row
+ * sort + dedupe), :639-658 (Ap prefix, Ai).  Single rank.  With Ai == NULL
+ * only Ap is filled and nnz is returned. */
+long orc_psparse_apai(long ne, int nne, const int *conn, const long *id,
+                      long ndof, int *Ap, int *Ai);
+
+/* One constitutive update at one quadrature point, the equivalent of
+ * run_integration_algorithm followed by update_elasticity
+ * (src/constitutive_model.cc:1100-1129, 1139-1164).  Outputs the PK2 stress
+ * S (9) and the material tangent L = 2 dS/dC (81, idx_4 order) at the
+ * elastic deformation, and the state at n+1.  For CP it also returns pF_{n+1}
+ * (9) in pFnp1 and dM/du support data is handled inside orc_element.
+ * Returns a non-zero error count on failure. */
+int orc_cm_update(const orc_material *mat, const double *F, double dt,
+                  const double *Rcp, const double *state_n,
+                  double *state_np1, double *S, double *L, int *iters);
+
+/* Element residual fe (nne*3) and stiffness lk ((nne*3)^2, idx_K order) of
+ * element e through the constitutive-model 1-field path
+ * (src/constitutive_model.cc:3322-3539, 2474-2692, 1520-1662).  u_e is the
+ * element displacement (nne*3, node-major), state_n/state_np1 point at the
+ * element's nint state records.  lk may be NULL. */
+int orc_element(const orc_problem *P, const orc_material *mat, long e,
+                const double *u_e, double dt, const double *state_n,
+                double *state_np1, double *fe, double *lk);
+
+/* Global assembly: R (ndof) and K values (nnz, aligned with Ai), the
+ * equivalent of fd_residuals_MP + stiffmat_fd_MP on one rank
+ * (src/fd_residuals.cc:468-636, 58-73; src/stiffmat_fd.cc:831-993;
+ * src/PLoc_Sparse.cc:15-175).  u is the free-DOF displacement vector,
+ * u_presc the prescribed values (indexed by -id-1, may be NULL).  Elements
+ * [e0, e1) only; R and K are accumulated (caller zeroes them).  K may be NULL.
+ * nthreads > 1 runs element colours in parallel (deterministic per colour).
+ * iter_hist (may be NULL) receives per-qp local-iteration counts (CP). */
+int orc_assemble(const orc_problem *P, const orc_material *mat,
+                 const double *u, const double *u_presc, double dt,
+                 const double *state_n, double *state_np1, double *R,
+                 double *K, long e0, long e1, int nthreads, int *iters);
+
+/* Same element integrals in the algebraically identical B-matrix form (the
+ * "best CPU algorithm" baseline).  Same arguments as orc_assemble. */
+int orc_assemble_bform(const orc_problem *P, const orc_material *mat,
+                       const double *u, const double *u_presc, double dt,
+                       const double *state_n, double *state_np1, double *R,
+                       double *K, long e0, long e1, int nthreads);
+
+/* Number of quadrature points per element for nne (1 for 4, 4 for 10). */
+int orc_nint(int nne);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

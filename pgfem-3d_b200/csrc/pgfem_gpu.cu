@@ -1,0 +1,750 @@
+// pgfem_gpu.cu -- C ABI of the sm_100a assembly path (include/pgfem_gpu.h).
+//
+// The context keeps every array of the path resident in HBM in
+// structure-of-arrays form: node coordinates X[3][nn], connectivity
+// conn[nne][ne] (int32), DOF ids dof[3][nn], the element->CSR node-block map
+// (pos[ne][nne][nne], uint16 column offsets inside the rows of the block's
+// first node), the per-node row offsets/lengths and free-component masks, and
+// the per-quadrature-point state at t_n and t_{n+1} as [comp][nqp].  No call
+// falls back to a CPU path: without an sm_100 device every entry point
+// returns PGFEM_GPU_ENODEV.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "assemble.cuh"
+#include "cm_integrate.cuh"
+#include "peak_probe.cuh"
+#include "pgfem_gpu.h"
+
+using namespace pgb;
+
+struct pgfem_gpu_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int nne = 0, nqp_e = 0;
+  long nn = 0, ne = 0, ndof = 0, npres = 0, nnz = 0, nqp = 0;
+  int model = 0, nstate = 0;  // device state components per qp
+  Mat mat{};
+  ShapeTable shp{};
+  // device arrays
+  double *X = nullptr;
+  int *conn = nullptr;
+  int *dof = nullptr;
+  int *rowptr0 = nullptr;
+  int *rowlen = nullptr;
+  uint8_t *mask = nullptr;
+  uint16_t *pos = nullptr;
+  double *unode = nullptr;
+  double *F0 = nullptr;
+  double *state_n = nullptr, *state_np1 = nullptr;
+  unsigned long long *status = nullptr;
+  // scratch for host-buffer calls
+  double *d_u = nullptr, *d_presc = nullptr, *d_R = nullptr, *d_K = nullptr;
+  // colour mode
+  int scatter_mode = PGFEM_SCATTER_ATOMIC;
+  std::vector<long> colour_off;  // offsets into colour element list
+  int *colour_elems = nullptr;
+  long bytes = 0;
+  // kernel timing
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
+};
+
+namespace {
+
+#define CK(x)                                                                            \
+  do {                                                                                   \
+    cudaError_t _e = (x);                                                                \
+    if (_e != cudaSuccess) {                                                             \
+      std::fprintf(stderr, "pgfem_gpu: %s failed: %s (%s:%d)\n", #x, cudaGetErrorString(_e), \
+                   __FILE__, __LINE__);                                                  \
+      return PGFEM_GPU_ECUDA;                                                            \
+    }                                                                                    \
+  } while (0)
+
+template <class T>
+int dalloc(pgfem_gpu_ctx *c, T **p, size_t n) {
+  if (n == 0) n = 1;
+  if (cudaMalloc((void **)p, n * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return PGFEM_GPU_ENOMEM;
+  }
+  c->bytes += (long)(n * sizeof(T));
+  return PGFEM_GPU_OK;
+}
+
+int check_device() {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return PGFEM_GPU_ENODEV;
+  }
+  cudaDeviceProp p;
+  if (cudaGetDeviceProperties(&p, dev) != cudaSuccess) return PGFEM_GPU_ENODEV;
+  if (p.major != 10) return PGFEM_GPU_ENODEV;
+  return PGFEM_GPU_OK;
+}
+
+// Quadrature tables with the reference constants (FEMLIB/src/femlib.cc:571-588,
+// shape-function derivatives :213-333); evaluated on the host in FP64.
+ShapeTable make_shape(int nne) {
+  ShapeTable t{};
+  if (nne == 4) {
+    const double d[4][3] = {{-1, -1, -1}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    for (int a = 0; a < 4; a++)
+      for (int c = 0; c < 3; c++) t.dNxi[0][a][c] = d[a][c];
+    t.w[0] = 1.0 / 6.0;
+    return t;
+  }
+  const double A = 0.58541020, B = 0.13819660;
+  const double k[4] = {A, B, B, B}, e[4] = {B, A, B, B}, z[4] = {B, B, A, B};
+  for (int q = 0; q < 4; q++) {
+    const double ksi = k[q], eta = e[q], zet = z[q];
+    double d[10][3] = {
+        {4.0 * (ksi + eta + zet) - 3.0, 4.0 * (eta + ksi + zet) - 3.0, 4.0 * (zet + ksi + eta) - 3.0},
+        {4.0 * ksi - 1.0, 0.0, 0.0},
+        {0.0, 4.0 * eta - 1.0, 0.0},
+        {0.0, 0.0, 4.0 * zet - 1.0},
+        {4.0 * (-2.0 * ksi - eta - zet + 1.0), -4.0 * ksi, -4.0 * ksi},
+        {4.0 * eta, 4.0 * ksi, 0.0},
+        {-4.0 * eta, 4.0 * (-ksi - 2.0 * eta - zet + 1.0), -4.0 * eta},
+        {-4.0 * zet, -4.0 * zet, 4.0 * (-ksi - eta - 2.0 * zet + 1.0)},
+        {4.0 * zet, 0.0, 4.0 * ksi},
+        {0.0, 4.0 * zet, 4.0 * eta}};
+    for (int a = 0; a < 10; a++)
+      for (int c = 0; c < 3; c++) t.dNxi[q][a][c] = d[a][c];
+    t.w[q] = (1.0 / 4.0) / 6.0;
+  }
+  return t;
+}
+
+Mat make_mat(const pgfem_material_desc *m) {
+  Mat r{};
+  r.model = m->model;
+  r.mu = m->E / (2.0 * (1.0 + m->nu));
+  r.kappa = (2 * r.mu * (1 + m->nu)) / (3 * (1 - 2 * m->nu));
+  r.sy = m->sigma_y;
+  r.H = m->H;
+  r.gdot0 = m->gamma_dot_0;
+  r.m = m->m;
+  r.G0 = m->G0;
+  r.g0 = m->g0;
+  r.gs0 = m->gs_0;
+  r.gdots = m->gamma_dot_s;
+  r.w = m->w;
+  r.tol = m->cp_tol > 0 ? m->cp_tol : 1e-10;
+  r.max_iter = m->cp_max_iter > 0 ? m->cp_max_iter : 25;
+  return r;
+}
+
+int device_state_size(int model) {
+  switch (model) {
+    case PGFEM_MODEL_J2: return 7;   // Cp^-1 (Voigt 6) + eqps
+    case PGFEM_MODEL_CP: return 10;  // pF (9) + g
+    default: return 0;
+  }
+}
+
+__global__ void k_expand_u(const int *dof, long nn, const double *u, const double *presc,
+                           double *unode) {
+  const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (n >= 3 * nn) return;
+  const int id = dof[n];
+  unode[n] = id > 0 ? u[id - 1] : (id < 0 && presc ? presc[-id - 1] : 0.0);
+}
+
+// Element->CSR node-block map: for each element and node pair (a, b), the
+// column position of node b's first free DOF inside the rows of node a,
+// checked against the caller's pattern (all free columns of b present and
+// consecutive).  0xFFFF marks pairs without a free row or column.
+__global__ void k_build_map(const int *conn, long ne, int nne, const int *dof, long nn,
+                            const int *rowptr0, const int *rowlen, const uint8_t *mask,
+                            const int *Ai, uint16_t *pos, int *err) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const long npair = (long)nne * nne;
+  if (t >= ne * npair) return;
+  const long e = t / npair;
+  const int a = (int)(t % npair) / nne, b = (int)(t % npair) % nne;
+  const int A = conn[(long)a * ne + e], B = conn[(long)b * ne + e];
+  const unsigned mA = mask[A], mB = mask[B];
+  uint16_t out = 0xFFFF;
+  if (mA && mB) {
+    int first = -1;
+    for (int c = 0; c < 3 && first < 0; c++)
+      if (dof[c * nn + B] > 0) first = dof[c * nn + B] - 1;
+    const int *row = Ai + rowptr0[A];
+    int lo = 0, hi = rowlen[A];
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (row[mid] < first) lo = mid + 1;
+      else hi = mid;
+    }
+    const int nb = __popc(mB);
+    bool ok = lo + nb <= rowlen[A] && lo < 0xFFFF;
+    for (int k = 0; ok && k < nb; k++) ok = row[lo + k] == first + k;
+    if (ok) out = (uint16_t)lo;
+    else atomicAdd(err, 1);
+  }
+  pos[t] = out;
+}
+
+template <class T>
+int upload(pgfem_gpu_ctx *c, T **d, const T *h, size_t n) {
+  int r = dalloc(c, d, n);
+  if (r) return r;
+  CK(cudaMemcpyAsync(*d, h, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return PGFEM_GPU_OK;
+}
+
+void drop_events(pgfem_gpu_ctx *c) {
+  for (auto &p : c->events) {
+    cudaEventDestroy(p.first);
+    cudaEventDestroy(p.second);
+  }
+  c->events.clear();
+}
+
+void release(pgfem_gpu_ctx *c) {
+  drop_events(c);
+  void *ptrs[] = {c->X, c->conn, c->dof, c->rowptr0, c->rowlen, c->mask, c->pos, c->unode, c->F0,
+                  c->state_n, c->state_np1, c->status, c->d_u, c->d_presc, c->d_R, c->d_K,
+                  c->colour_elems};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (c->stream) cudaStreamDestroy(c->stream);
+}
+
+AsmArgs base_args(const pgfem_gpu_ctx *c) {
+  AsmArgs a{};
+  a.X = c->X;
+  a.conn = c->conn;
+  a.dof = c->dof;
+  a.rowptr0 = c->rowptr0;
+  a.rowlen = c->rowlen;
+  a.mask = c->mask;
+  a.pos = c->pos;
+  a.nn = c->nn;
+  a.ne = c->ne;
+  a.unode = c->unode;
+  a.F0 = c->F0;
+  a.state_n = c->state_n;
+  a.state_np1 = c->state_np1;
+  a.nqp = c->nqp;
+  a.status = c->status;
+  a.mat = c->mat;
+  a.shp = c->shp;
+  return a;
+}
+
+int g_num_sms = 0;
+
+int grid_for(long nitems, int te, int per_sm) {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  const long tiles = (nitems + te - 1) / te;
+  return (int)std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm * 8));
+}
+
+template <int NNE, int NQP, int MODEL, bool ATOMIC, bool WANT_K, bool DENSE>
+int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
+  constexpr size_t smem = asm_smem_bytes<NNE, NQP>();
+  auto kern = k_assemble<NNE, NQP, MODEL, ATOMIC, WANT_K, DENSE>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Tile<NNE>::TE * NNE, smem));
+  if (per_sm < 1) per_sm = 1;
+  const int grid = grid_for(nitems, Tile<NNE>::TE, per_sm);
+  kern<<<grid, Tile<NNE>::TE * NNE, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+template <bool ATOMIC, bool WANT_K, bool DENSE>
+int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
+  if (c->nne == 4) {
+    switch (c->model) {
+      case PGFEM_MODEL_HE: return launch_asm<4, 1, 0, ATOMIC, WANT_K, DENSE>(a, nitems, s);
+      case PGFEM_MODEL_J2: return launch_asm<4, 1, 1, ATOMIC, WANT_K, DENSE>(a, nitems, s);
+    }
+  } else {
+    switch (c->model) {
+      case PGFEM_MODEL_HE: return launch_asm<10, 4, 0, ATOMIC, WANT_K, DENSE>(a, nitems, s);
+      case PGFEM_MODEL_J2: return launch_asm<10, 4, 1, ATOMIC, WANT_K, DENSE>(a, nitems, s);
+    }
+  }
+  return PGFEM_GPU_EINVAL;
+}
+
+// One assembly on device buffers (zeroing R and K first).
+int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
+                    double *d_K, cudaStream_t s) {
+  if (c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
+  if (d_K) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
+  {
+    const long n3 = 3 * c->nn;
+    k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
+    CK(cudaGetLastError());
+  }
+  AsmArgs a = base_args(c);
+  a.R = d_R;
+  a.K = d_K;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->timing && c->events.size() < 4096) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+  }
+  int r = PGFEM_GPU_OK;
+  if (c->scatter_mode == PGFEM_SCATTER_COLOUR && c->colour_elems) {
+    for (size_t k = 0; k + 1 < c->colour_off.size() && !r; k++) {
+      a.elist = c->colour_elems + c->colour_off[k];
+      a.nlist = c->colour_off[k + 1] - c->colour_off[k];
+      r = d_K ? dispatch<false, true, false>(c, a, a.nlist, s)
+              : dispatch<false, false, false>(c, a, a.nlist, s);
+    }
+  } else {
+    r = d_K ? dispatch<true, true, false>(c, a, c->ne, s) : dispatch<true, false, false>(c, a, c->ne, s);
+  }
+  if (e0) {
+    CK(cudaEventRecord(e1, s));
+    c->events.emplace_back(e0, e1);
+  }
+  return r;
+}
+
+int read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, bool clear) {
+  unsigned long long h[4];
+  CK(cudaMemcpyAsync(h, c->status, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st) {
+    st->inverted = (long)h[0];
+    st->nonconverged = (long)h[1];
+    st->bad_diagonal = (long)h[2];
+    st->other = (long)h[3];
+  }
+  if (clear) CK(cudaMemsetAsync(c->status, 0, sizeof(h), c->stream));
+  return PGFEM_GPU_OK;
+}
+
+// Greedy colouring: elements of one colour share no node, so their R and K
+// updates touch disjoint rows and need no atomics.
+void build_colours(const pgfem_mesh_desc *m, std::vector<int> &elems, std::vector<long> &off) {
+  std::vector<int> colour(m->ne, -1);
+  std::vector<std::vector<uint8_t>> used;
+  int ncol = 0;
+  for (long e = 0; e < m->ne; e++) {
+    int c = 0;
+    for (; c < ncol; c++) {
+      bool ok = true;
+      for (int a = 0; a < m->nne && ok; a++) ok = !used[c][m->conn[e * m->nne + a]];
+      if (ok) break;
+    }
+    if (c == ncol) {
+      used.emplace_back(m->nn, 0);
+      ncol++;
+    }
+    colour[e] = c;
+    for (int a = 0; a < m->nne; a++) used[c][m->conn[e * m->nne + a]] = 1;
+  }
+  off.assign(ncol + 1, 0);
+  for (long e = 0; e < m->ne; e++) off[colour[e] + 1]++;
+  for (int c = 0; c < ncol; c++) off[c + 1] += off[c];
+  elems.resize(m->ne);
+  std::vector<long> fill(off.begin(), off.end() - 1);
+  for (long e = 0; e < m->ne; e++) elems[fill[colour[e]]++] = (int)e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgfem_gpu_state_size(int model) {
+  switch (model) {
+    case PGFEM_MODEL_J2: return 10;
+    case PGFEM_MODEL_CP: return 10;
+    default: return 0;
+  }
+}
+
+int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, const int *Ap,
+                     const int *Ai, long nrows, pgfem_gpu_ctx **out) {
+  if (!m || !mat || !out || !m->X || !m->conn || !m->dof_id || (m->nne != 4 && m->nne != 10) ||
+      m->nn <= 0 || m->ne <= 0 || nrows != m->ndof || !Ap || !Ai)
+    return PGFEM_GPU_EINVAL;
+  if (mat->model < 0 || mat->model > 2) return PGFEM_GPU_EINVAL;
+  if (m->nn > 0x7fffffffL || m->ne > 0x7fffffffL) return PGFEM_GPU_ELIMIT;
+  int r = check_device();
+  if (r) return r;
+  auto *c = new pgfem_gpu_ctx();
+  c->nne = m->nne;
+  c->nqp_e = m->nne == 10 ? 4 : 1;
+  c->nn = m->nn;
+  c->ne = m->ne;
+  c->ndof = m->ndof;
+  c->npres = m->npres;
+  c->nnz = Ap[m->ndof];
+  c->nqp = c->ne * c->nqp_e;
+  c->model = mat->model;
+  c->nstate = device_state_size(mat->model);
+  c->mat = make_mat(mat);
+  c->shp = make_shape(m->nne);
+  cudaGetDevice(&c->device);
+  auto fail = [&](int code) {
+    cudaStreamSynchronize(c->stream);
+    release(c);
+    delete c;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(PGFEM_GPU_ECUDA);
+
+  // ---- host-side SoA + per-node row information ----
+  const long nn = m->nn, ne = m->ne;
+  std::vector<double> X(3 * nn);
+  std::vector<int> dof(3 * nn), rowptr0(nn, -1), rowlen(nn, 0);
+  std::vector<uint8_t> mask(nn, 0);
+  for (long n = 0; n < nn; n++) {
+    int first = -1, prev = -1;
+    for (int j = 0; j < 3; j++) {
+      X[j * nn + n] = m->X[n * 3 + j];
+      const long id = m->dof_id[n * 3 + j];
+      if (id > m->ndof || (id < 0 && -id > m->npres)) return fail(PGFEM_GPU_EINVAL);
+      dof[j * nn + n] = (int)id;
+      if (id > 0) {
+        mask[n] |= (uint8_t)(1u << j);
+        if (first < 0) first = (int)id - 1;
+        else if (id - 1 != prev + 1) return fail(PGFEM_GPU_EPATTERN);
+        prev = (int)id - 1;
+      }
+    }
+    if (first >= 0) {
+      rowptr0[n] = Ap[first];
+      rowlen[n] = Ap[first + 1] - Ap[first];
+      for (int k = 1; k < __builtin_popcount(mask[n]); k++)
+        if (Ap[first + k + 1] - Ap[first + k] != rowlen[n] ||
+            Ap[first + k] != rowptr0[n] + k * rowlen[n])
+          return fail(PGFEM_GPU_EPATTERN);
+    }
+  }
+  std::vector<int> conn((size_t)m->nne * ne);
+  for (long e = 0; e < ne; e++)
+    for (int a = 0; a < m->nne; a++) {
+      const int v = m->conn[e * m->nne + a];
+      if (v < 0 || v >= nn) return fail(PGFEM_GPU_EINVAL);
+      conn[(size_t)a * ne + e] = v;
+    }
+  if ((r = upload(c, &c->X, X.data(), X.size())) || (r = upload(c, &c->dof, dof.data(), dof.size())) ||
+      (r = upload(c, &c->rowptr0, rowptr0.data(), nn)) ||
+      (r = upload(c, &c->rowlen, rowlen.data(), nn)) || (r = upload(c, &c->mask, mask.data(), nn)) ||
+      (r = upload(c, &c->conn, conn.data(), conn.size())))
+    return fail(r);
+  if (m->F0 && (r = upload(c, &c->F0, m->F0, 9))) return fail(r);
+  if ((r = dalloc(c, &c->unode, 3 * nn)) || (r = dalloc(c, &c->status, 4)) ||
+      (r = dalloc(c, &c->pos, (size_t)ne * m->nne * m->nne)))
+    return fail(r);
+  if (c->nstate) {
+    if ((r = dalloc(c, &c->state_n, (size_t)c->nstate * c->nqp)) ||
+        (r = dalloc(c, &c->state_np1, (size_t)c->nstate * c->nqp)))
+      return fail(r);
+  }
+  if (cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream) != cudaSuccess)
+    return fail(PGFEM_GPU_ECUDA);
+
+  // ---- element->CSR map, built and validated on the device ----
+  {
+    int *dAi = nullptr, *derr = nullptr;
+    if (cudaMalloc(&dAi, sizeof(int) * std::max<long>(1, c->nnz)) != cudaSuccess ||
+        cudaMalloc(&derr, sizeof(int)) != cudaSuccess) {
+      cudaGetLastError();
+      if (dAi) cudaFree(dAi);
+      return fail(PGFEM_GPU_ENOMEM);
+    }
+    cudaMemcpyAsync(dAi, Ai, sizeof(int) * c->nnz, cudaMemcpyHostToDevice, c->stream);
+    cudaMemsetAsync(derr, 0, sizeof(int), c->stream);
+    const long nt = ne * m->nne * m->nne;
+    k_build_map<<<(unsigned)((nt + 255) / 256), 256, 0, c->stream>>>(
+        c->conn, ne, m->nne, c->dof, nn, c->rowptr0, c->rowlen, c->mask, dAi, c->pos, derr);
+    int herr = 0;
+    cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    cudaFree(dAi);
+    cudaFree(derr);
+    if (ce != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
+    if (herr) return fail(PGFEM_GPU_EPATTERN);
+  }
+  // default state: identity Cp^-1 / pF, zero eqps, g = g0
+  if (c->nstate) {
+    std::vector<double> s0((size_t)c->nstate * c->nqp, 0.0);
+    if (c->model == PGFEM_MODEL_J2)
+      for (int k = 0; k < 3; k++) std::fill(s0.begin() + k * c->nqp, s0.begin() + (k + 1) * c->nqp, 1.0);
+    if (c->model == PGFEM_MODEL_CP) {
+      for (int k : {0, 4, 8}) std::fill(s0.begin() + k * c->nqp, s0.begin() + (k + 1) * c->nqp, 1.0);
+      std::fill(s0.begin() + 9 * c->nqp, s0.end(), mat->g0);
+    }
+    cudaMemcpyAsync(c->state_n, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    cudaMemcpyAsync(c->state_np1, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
+  }
+  // colours for the deterministic scatter mode
+  {
+    std::vector<int> el;
+    build_colours(m, el, c->colour_off);
+    if ((r = upload(c, &c->colour_elems, el.data(), el.size()))) return fail(r);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
+  }
+  *out = c;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_destroy(pgfem_gpu_ctx *c) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  cudaStreamSynchronize(c->stream);
+  release(c);
+  delete c;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
+  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR)) return PGFEM_GPU_EINVAL;
+  c->scatter_mode = mode;
+  return PGFEM_GPU_OK;
+}
+
+long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *c) { return c ? c->bytes : -1; }
+long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
+
+int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
+  if (!c) return -1;
+  const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
+  return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
+}
+
+int pgfem_gpu_set_timing(pgfem_gpu_ctx *c, int on) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  c->timing = on != 0;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_kernel_time(pgfem_gpu_ctx *c, double *ms, long *ncalls, int reset) {
+  if (!c || !ms) return PGFEM_GPU_EINVAL;
+  double tot = 0.0;
+  for (auto &p : c->events) {
+    CK(cudaEventSynchronize(p.second));
+    float t = 0.f;
+    CK(cudaEventElapsedTime(&t, p.first, p.second));
+    tot += t;
+  }
+  *ms = tot;
+  if (ncalls) *ncalls = (long)c->events.size();
+  if (reset) drop_events(c);
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_fp64_peak(double *tflops) {
+  if (!tflops) return PGFEM_GPU_EINVAL;
+  int r = check_device();
+  if (r) return r;
+  return fp64_peak_probe(tflops);
+}
+
+int pgfem_gpu_set_state(pgfem_gpu_ctx *c, const double *st) {
+  if (!c || !st) return PGFEM_GPU_EINVAL;
+  if (!c->nstate) return PGFEM_GPU_OK;
+  const long nq = c->nqp;
+  std::vector<double> soa((size_t)c->nstate * nq);
+  for (long q = 0; q < nq; q++) {
+    const double *s = st + q * 10;
+    if (c->model == PGFEM_MODEL_J2) {
+      const double v[7] = {s[0], s[4], s[8], s[5], s[2], s[1], s[9]};
+      for (int k = 0; k < 7; k++) soa[k * nq + q] = v[k];
+    } else {
+      for (int k = 0; k < 10; k++) soa[k * nq + q] = s[k];
+    }
+  }
+  CK(cudaMemcpyAsync(c->state_n, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->state_np1, c->state_n, soa.size() * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_get_state(pgfem_gpu_ctx *c, int level, double *st) {
+  if (!c || !st || (level != 0 && level != 1)) return PGFEM_GPU_EINVAL;
+  if (!c->nstate) return PGFEM_GPU_OK;
+  const long nq = c->nqp;
+  std::vector<double> soa((size_t)c->nstate * nq);
+  CK(cudaMemcpyAsync(soa.data(), level ? c->state_np1 : c->state_n, soa.size() * sizeof(double),
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (long q = 0; q < nq; q++) {
+    double *s = st + q * 10;
+    if (c->model == PGFEM_MODEL_J2) {
+      const double xx = soa[0 * nq + q], yy = soa[1 * nq + q], zz = soa[2 * nq + q],
+                   yz = soa[3 * nq + q], xz = soa[4 * nq + q], xy = soa[5 * nq + q];
+      const double v[10] = {xx, xy, xz, xy, yy, yz, xz, yz, zz, soa[6 * nq + q]};
+      for (int k = 0; k < 10; k++) s[k] = v[k];
+    } else {
+      for (int k = 0; k < 10; k++) s[k] = soa[k * nq + q];
+    }
+  }
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_commit_state(pgfem_gpu_ctx *c) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  if (c->nstate)
+    CK(cudaMemcpyAsync(c->state_n, c->state_np1, sizeof(double) * c->nstate * c->nqp,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_reset_state(pgfem_gpu_ctx *c) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  if (c->nstate)
+    CK(cudaMemcpyAsync(c->state_np1, c->state_n, sizeof(double) * c->nstate * c->nqp,
+                       cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+static int ensure_scratch(pgfem_gpu_ctx *c, bool wantK) {
+  int r;
+  if (!c->d_u && (r = dalloc(c, &c->d_u, c->ndof))) return r;
+  if (!c->d_presc && (r = dalloc(c, &c->d_presc, std::max<long>(1, c->npres)))) return r;
+  if (!c->d_R && (r = dalloc(c, &c->d_R, c->ndof))) return r;
+  if (wantK && !c->d_K && (r = dalloc(c, &c->d_K, c->nnz))) return r;
+  return PGFEM_GPU_OK;
+}
+
+static int assemble_host(pgfem_gpu_ctx *c, const double *u, const double *presc, double *R,
+                         double *K, pgfem_gpu_status *st) {
+  if (!c || !u || !R || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
+  int r = ensure_scratch(c, K != nullptr);
+  if (r) return r;
+  CK(cudaMemcpyAsync(c->d_u, u, sizeof(double) * c->ndof, cudaMemcpyHostToDevice, c->stream));
+  if (c->npres)
+    CK(cudaMemcpyAsync(c->d_presc, presc, sizeof(double) * c->npres, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream));
+  r = assemble_device(c, c->d_u, c->npres ? c->d_presc : nullptr, c->d_R, K ? c->d_K : nullptr, c->stream);
+  if (r) return r;
+  CK(cudaMemcpyAsync(R, c->d_R, sizeof(double) * c->ndof, cudaMemcpyDeviceToHost, c->stream));
+  if (K) CK(cudaMemcpyAsync(K, c->d_K, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost, c->stream));
+  return read_status(c, st, false);
+}
+
+int pgfem_gpu_assemble_R(pgfem_gpu_ctx *c, const double *u, const double *presc, double dt,
+                         double *R, pgfem_gpu_status *st) {
+  (void)dt;
+  return assemble_host(c, u, presc, R, nullptr, st);
+}
+
+int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *c, const double *u, const double *presc, double dt,
+                          double *R, double *K, pgfem_gpu_status *st) {
+  (void)dt;
+  if (!K) return PGFEM_GPU_EINVAL;
+  return assemble_host(c, u, presc, R, K, st);
+}
+
+int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc,
+                                 double dt, double *d_R, double *d_K, void *stream) {
+  (void)dt;
+  if (!c || !d_u || !d_R || !d_K) return PGFEM_GPU_EINVAL;
+  return assemble_device(c, d_u, d_presc, d_R, d_K, (cudaStream_t)stream);
+}
+
+int pgfem_gpu_read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, int clear) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  return read_status(c, st, clear != 0);
+}
+
+static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
+                         const double *presc, double *lk, double *fe, pgfem_gpu_status *st) {
+  if (!c || nel < 0 || (nel && (!elems || !fe)) || !u || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
+  if (c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  if (nel == 0) return PGFEM_GPU_OK;
+  for (long i = 0; i < nel; i++)
+    if (elems[i] < 0 || elems[i] >= c->ne) return PGFEM_GPU_EINVAL;
+  int r = ensure_scratch(c, false);
+  if (r) return r;
+  const int nd = c->nne * 3;
+  std::vector<int> el(elems, elems + nel);
+  int *d_el = nullptr;
+  double *d_lk = nullptr, *d_fe = nullptr;
+  auto cleanup = [&]() {
+    if (d_el) cudaFree(d_el);
+    if (d_lk) cudaFree(d_lk);
+    if (d_fe) cudaFree(d_fe);
+  };
+  if (cudaMalloc(&d_el, sizeof(int) * nel) != cudaSuccess ||
+      cudaMalloc(&d_fe, sizeof(double) * nel * nd) != cudaSuccess ||
+      (lk && cudaMalloc(&d_lk, sizeof(double) * nel * nd * nd) != cudaSuccess)) {
+    cudaGetLastError();
+    cleanup();
+    return PGFEM_GPU_ENOMEM;
+  }
+  cudaMemcpyAsync(d_el, el.data(), sizeof(int) * nel, cudaMemcpyHostToDevice, c->stream);
+  cudaMemcpyAsync(c->d_u, u, sizeof(double) * c->ndof, cudaMemcpyHostToDevice, c->stream);
+  if (c->npres) cudaMemcpyAsync(c->d_presc, presc, sizeof(double) * c->npres, cudaMemcpyHostToDevice, c->stream);
+  cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream);
+  const long n3 = 3 * c->nn;
+  k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, c->stream>>>(c->dof, c->nn, c->d_u,
+                                                                   c->npres ? c->d_presc : nullptr, c->unode);
+  AsmArgs a = base_args(c);
+  a.elist = d_el;
+  a.nlist = nel;
+  a.lk_out = d_lk;
+  a.fe_out = d_fe;
+  r = lk ? dispatch<false, true, true>(c, a, nel, c->stream) : dispatch<false, false, true>(c, a, nel, c->stream);
+  if (!r) {
+    cudaMemcpyAsync(fe, d_fe, sizeof(double) * nel * nd, cudaMemcpyDeviceToHost, c->stream);
+    if (lk) cudaMemcpyAsync(lk, d_lk, sizeof(double) * nel * nd * nd, cudaMemcpyDeviceToHost, c->stream);
+    r = read_status(c, st, false);
+  }
+  cudaStreamSynchronize(c->stream);
+  cleanup();
+  return r;
+}
+
+int pgfem_gpu_stiffmatel_fd(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
+                            const double *presc, double dt, double *lk, double *fe,
+                            pgfem_gpu_status *st) {
+  (void)dt;
+  if (!lk) return PGFEM_GPU_EINVAL;
+  return element_level(c, nel, elems, u, presc, lk, fe, st);
+}
+
+int pgfem_gpu_resid_on_elem(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
+                            const double *presc, double dt, double *fe, pgfem_gpu_status *st) {
+  (void)dt;
+  return element_level(c, nel, elems, u, presc, nullptr, fe, st);
+}
+
+int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const double *F, double dt,
+                           const double *R_cp, const double *state_n, double *state_np1, double *S,
+                           double *L, int *qp_status) {
+  if (!mat || nqp < 0 || (nqp && (!F || !S))) return PGFEM_GPU_EINVAL;
+  if (mat->model != PGFEM_MODEL_HE && mat->model != PGFEM_MODEL_J2) return PGFEM_GPU_EINVAL;
+  if (mat->model == PGFEM_MODEL_J2 && nqp && (!state_n || !state_np1)) return PGFEM_GPU_EINVAL;
+  int r = check_device();
+  if (r) return r;
+  if (nqp == 0) return PGFEM_GPU_OK;
+  return cm_integrate_host(make_mat(mat), nqp, F, dt, state_n, state_np1, S, L, qp_status);
+}
+
+}  // extern "C"

@@ -1,0 +1,307 @@
+"""ctypes binding of the C ABI in include/pgfem_gpu.h.
+
+This is harness plumbing for tests and benchmarks: every numerical operation
+runs inside libpgfem_gpu.so (setup on the host in C++, assembly on the GPU).
+Loading fails loudly when the library is missing; there is no fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpgfem_gpu.so")
+
+MODEL_HE, MODEL_J2, MODEL_CP = 0, 1, 2
+SCATTER_ATOMIC, SCATTER_COLOUR = 0, 1
+
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT"}
+
+
+class PgfemError(RuntimeError):
+    def __init__(self, fn, code):
+        super().__init__("%s failed: %s (%d)" % (fn, ERRORS.get(code, "?"), code))
+        self.code = code
+
+
+class MaterialDesc(C.Structure):
+    _fields_ = [("model", C.c_int), ("E", C.c_double), ("nu", C.c_double),
+                ("sigma_y", C.c_double), ("H", C.c_double),
+                ("gamma_dot_0", C.c_double), ("m", C.c_double), ("G0", C.c_double),
+                ("g0", C.c_double), ("gs_0", C.c_double), ("gamma_dot_s", C.c_double),
+                ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("nn", C.c_long), ("ne", C.c_long), ("nne", C.c_int),
+                ("X", C.POINTER(C.c_double)), ("conn", C.POINTER(C.c_int)),
+                ("dof_id", C.POINTER(C.c_long)), ("ndof", C.c_long), ("npres", C.c_long),
+                ("F0", C.POINTER(C.c_double)), ("R_cp", C.POINTER(C.c_double))]
+
+
+class Status(C.Structure):
+    _fields_ = [("inverted", C.c_long), ("nonconverged", C.c_long),
+                ("bad_diagonal", C.c_long), ("other", C.c_long)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+    def ok(self):
+        return self.inverted == 0 and self.nonconverged == 0 and self.bad_diagonal == 0 and self.other == 0
+
+
+_lib = None
+
+_P = C.c_void_p
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError("libpgfem_gpu.so not built: run pgfem-3d_b200/build.py")
+        L = C.CDLL(LIB_PATH)
+        sig = {
+            "pgfem_gpu_state_size": (C.c_int, [C.c_int]),
+            "pgfem_generate_dof_ids": (C.c_long, [C.c_long, C.c_long, C.c_int, _P, _P, _P]),
+            "pgfem_psparse_apai": (C.c_long, [C.c_long, C.c_int, _P, _P, C.c_long, _P, _P]),
+            "pgfem_mesh_box_tet": (C.c_int, [C.c_int, C.c_int, C.c_int, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_create": (C.c_int, [_P, _P, _P, _P, C.c_long, _P]),
+            "pgfem_gpu_destroy": (C.c_int, [_P]),
+            "pgfem_gpu_set_scatter_mode": (C.c_int, [_P, C.c_int]),
+            "pgfem_gpu_device_bytes": (C.c_long, [_P]),
+            "pgfem_gpu_nnz": (C.c_long, [_P]),
+            "pgfem_gpu_set_state": (C.c_int, [_P, _P]),
+            "pgfem_gpu_get_state": (C.c_int, [_P, C.c_int, _P]),
+            "pgfem_gpu_commit_state": (C.c_int, [_P]),
+            "pgfem_gpu_reset_state": (C.c_int, [_P]),
+            "pgfem_gpu_assemble_R": (C.c_int, [_P, _P, _P, C.c_double, _P, _P]),
+            "pgfem_gpu_assemble_RK": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, _P]),
+            "pgfem_gpu_assemble_RK_device": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, _P]),
+            "pgfem_gpu_read_status": (C.c_int, [_P, _P, C.c_int]),
+            "pgfem_gpu_launches_per_assembly": (C.c_int, [_P]),
+            "pgfem_gpu_stiffmatel_fd": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_double, _P, _P, _P]),
+            "pgfem_gpu_resid_on_elem": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_double, _P, _P]),
+            "pgfem_gpu_cm_integrate": (C.c_int, [_P, C.c_long, _P, C.c_double, _P, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_set_timing": (C.c_int, [_P, C.c_int]),
+            "pgfem_gpu_kernel_time": (C.c_int, [_P, _P, _P, C.c_int]),
+            "pgfem_gpu_fp64_peak": (C.c_int, [_P]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a  # integer device pointer
+
+
+def _check(fn, r):
+    if r < 0:
+        raise PgfemError(fn, r)
+    return r
+
+
+def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0, G0=0.0, g0=0.0,
+             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25):
+    return MaterialDesc(model, E, nu, sigma_y, H, gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w,
+                        cp_tol, cp_max_iter)
+
+
+# ---------------------------------------------------------------- setup ----
+def mesh_box_tet(n, nne, periodic=False):
+    """Structured unit-cube mesh (6 tets per cell).  Returns X (nn,3), conn (ne,nne), Pr (nn,)."""
+    nn = C.c_long()
+    ne = C.c_long()
+    _check("pgfem_mesh_box_tet", lib().pgfem_mesh_box_tet(n, nne, int(periodic), C.byref(nn), C.byref(ne),
+                                                          None, None, None))
+    X = np.zeros((nn.value, 3))
+    conn = np.zeros((ne.value, nne), dtype=np.int32)
+    Pr = np.zeros(nn.value, dtype=np.int64)
+    _check("pgfem_mesh_box_tet", lib().pgfem_mesh_box_tet(n, nne, int(periodic), C.byref(nn), C.byref(ne),
+                                                          _ptr(X), _ptr(conn), _ptr(Pr)))
+    return X, conn, Pr
+
+
+def generate_dof_ids(conn, nn, codes, Pr=None):
+    """codes (nn,3) int64: 0 free, 1 fixed, <0 prescribed.  Returns (ids, ndof)."""
+    ids = np.ascontiguousarray(codes, dtype=np.int64).copy()
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    Pr = None if Pr is None else np.ascontiguousarray(Pr, dtype=np.int64)
+    ndof = _check("pgfem_generate_dof_ids", lib().pgfem_generate_dof_ids(
+        nn, conn.shape[0], conn.shape[1], _ptr(conn), _ptr(Pr), _ptr(ids)))
+    return ids, ndof
+
+
+def psparse_apai(conn, ids, ndof):
+    conn = np.ascontiguousarray(conn, dtype=np.int32)
+    ids = np.ascontiguousarray(ids, dtype=np.int64)
+    Ap = np.zeros(ndof + 1, dtype=np.int32)
+    nnz = _check("pgfem_psparse_apai", lib().pgfem_psparse_apai(
+        conn.shape[0], conn.shape[1], _ptr(conn), _ptr(ids), ndof, _ptr(Ap), None))
+    Ai = np.zeros(max(nnz, 1), dtype=np.int32)
+    _check("pgfem_psparse_apai", lib().pgfem_psparse_apai(
+        conn.shape[0], conn.shape[1], _ptr(conn), _ptr(ids), ndof, _ptr(Ap), _ptr(Ai)))
+    return Ap, Ai[:nnz]
+
+
+def state_size(model):
+    return lib().pgfem_gpu_state_size(model)
+
+
+# -------------------------------------------------------------- context ----
+class Context:
+    """Device-resident assembly context (pgfem_gpu_create / _destroy)."""
+
+    def __init__(self, X, conn, ids, ndof, Ap, Ai, mat, npres=0, F0=None, R_cp=None):
+        self._keep = dict(X=np.ascontiguousarray(X, dtype=np.float64),
+                          conn=np.ascontiguousarray(conn, dtype=np.int32),
+                          ids=np.ascontiguousarray(ids, dtype=np.int64),
+                          Ap=np.ascontiguousarray(Ap, dtype=np.int32),
+                          Ai=np.ascontiguousarray(Ai, dtype=np.int32),
+                          F0=None if F0 is None else np.ascontiguousarray(F0, dtype=np.float64).reshape(9),
+                          R_cp=None if R_cp is None else np.ascontiguousarray(R_cp, dtype=np.float64))
+        k = self._keep
+        dp = C.POINTER(C.c_double)
+        self.mesh = MeshDesc(k["X"].shape[0], k["conn"].shape[0], k["conn"].shape[1],
+                             k["X"].ctypes.data_as(dp), k["conn"].ctypes.data_as(C.POINTER(C.c_int)),
+                             k["ids"].ctypes.data_as(C.POINTER(C.c_long)), ndof, npres,
+                             None if k["F0"] is None else k["F0"].ctypes.data_as(dp),
+                             None if k["R_cp"] is None else k["R_cp"].ctypes.data_as(dp))
+        self.mat = mat
+        self.ndof = ndof
+        self.npres = npres
+        self.nne = k["conn"].shape[1]
+        self.ne = k["conn"].shape[0]
+        self.nint = 4 if self.nne == 10 else 1
+        self.ns = state_size(mat.model)
+        h = C.c_void_p()
+        _check("pgfem_gpu_create", lib().pgfem_gpu_create(C.byref(self.mesh), C.byref(self.mat), _ptr(k["Ap"]),
+                                                          _ptr(k["Ai"]), ndof, C.byref(h)))
+        self.h = h
+        self.nnz = lib().pgfem_gpu_nnz(h)
+
+    def close(self):
+        if self.h:
+            lib().pgfem_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_scatter_mode(self, mode):
+        _check("pgfem_gpu_set_scatter_mode", lib().pgfem_gpu_set_scatter_mode(self.h, mode))
+
+    def device_bytes(self):
+        return lib().pgfem_gpu_device_bytes(self.h)
+
+    def launches_per_assembly(self):
+        return lib().pgfem_gpu_launches_per_assembly(self.h)
+
+    def set_state(self, state):
+        state = np.ascontiguousarray(state, dtype=np.float64)
+        _check("pgfem_gpu_set_state", lib().pgfem_gpu_set_state(self.h, _ptr(state)))
+
+    def get_state(self, level=1):
+        out = np.zeros((self.ne * self.nint, max(self.ns, 1)))
+        _check("pgfem_gpu_get_state", lib().pgfem_gpu_get_state(self.h, level, _ptr(out)))
+        return out
+
+    def commit_state(self):
+        _check("pgfem_gpu_commit_state", lib().pgfem_gpu_commit_state(self.h))
+
+    def reset_state(self):
+        _check("pgfem_gpu_reset_state", lib().pgfem_gpu_reset_state(self.h))
+
+    def _presc(self, u_presc):
+        if self.npres == 0:
+            return None
+        return np.ascontiguousarray(u_presc, dtype=np.float64)
+
+    def assemble_R(self, u, u_presc=None, dt=0.0):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        R = np.zeros(self.ndof)
+        st = Status()
+        _check("pgfem_gpu_assemble_R", lib().pgfem_gpu_assemble_R(
+            self.h, _ptr(u), _ptr(self._presc(u_presc)), dt, _ptr(R), C.byref(st)))
+        return R, st
+
+    def assemble_RK(self, u, u_presc=None, dt=0.0, R=None, K=None):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        R = np.zeros(self.ndof) if R is None else R
+        K = np.zeros(self.nnz) if K is None else K
+        st = Status()
+        _check("pgfem_gpu_assemble_RK", lib().pgfem_gpu_assemble_RK(
+            self.h, _ptr(u), _ptr(self._presc(u_presc)), dt, _ptr(R), _ptr(K), C.byref(st)))
+        return R, K, st
+
+    def assemble_RK_device(self, d_u, d_presc, d_R, d_K, stream, dt=0.0):
+        """Device pointers (ints) and a cudaStream_t handle (int)."""
+        _check("pgfem_gpu_assemble_RK_device", lib().pgfem_gpu_assemble_RK_device(
+            self.h, d_u, d_presc, dt, d_R, d_K, stream))
+
+    def set_timing(self, on=True):
+        _check("pgfem_gpu_set_timing", lib().pgfem_gpu_set_timing(self.h, int(on)))
+
+    def kernel_time(self, reset=True):
+        ms = C.c_double()
+        n = C.c_long()
+        _check("pgfem_gpu_kernel_time", lib().pgfem_gpu_kernel_time(self.h, C.byref(ms), C.byref(n), int(reset)))
+        return ms.value, n.value
+
+    def read_status(self, clear=False):
+        st = Status()
+        _check("pgfem_gpu_read_status", lib().pgfem_gpu_read_status(self.h, C.byref(st), int(clear)))
+        return st
+
+    def stiffmatel_fd(self, elems, u, u_presc=None, dt=0.0):
+        elems = np.ascontiguousarray(elems, dtype=np.int64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        nd = self.nne * 3
+        lk = np.zeros((len(elems), nd, nd))
+        fe = np.zeros((len(elems), nd))
+        st = Status()
+        _check("pgfem_gpu_stiffmatel_fd", lib().pgfem_gpu_stiffmatel_fd(
+            self.h, len(elems), _ptr(elems), _ptr(u), _ptr(self._presc(u_presc)), dt, _ptr(lk), _ptr(fe),
+            C.byref(st)))
+        return lk, fe, st
+
+    def resid_on_elem(self, elems, u, u_presc=None, dt=0.0):
+        elems = np.ascontiguousarray(elems, dtype=np.int64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        fe = np.zeros((len(elems), self.nne * 3))
+        st = Status()
+        _check("pgfem_gpu_resid_on_elem", lib().pgfem_gpu_resid_on_elem(
+            self.h, len(elems), _ptr(elems), _ptr(u), _ptr(self._presc(u_presc)), dt, _ptr(fe), C.byref(st)))
+        return fe, st
+
+
+def fp64_peak_tflops():
+    t = C.c_double()
+    _check("pgfem_gpu_fp64_peak", lib().pgfem_gpu_fp64_peak(C.byref(t)))
+    return t.value
+
+
+def cm_integrate(mat, F, state_n=None, dt=0.0, want_L=True):
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(-1, 9)
+    nqp = F.shape[0]
+    ns = state_size(mat.model)
+    S = np.zeros((nqp, 9))
+    L = np.zeros((nqp, 81)) if want_L else None
+    snp1 = np.zeros((nqp, max(ns, 1)))
+    sn = None if state_n is None else np.ascontiguousarray(state_n, dtype=np.float64)
+    qst = np.zeros(nqp, dtype=np.int32)
+    _check("pgfem_gpu_cm_integrate", lib().pgfem_gpu_cm_integrate(
+        C.byref(mat), nqp, _ptr(F), dt, None, _ptr(sn), _ptr(snp1), _ptr(S), _ptr(L), _ptr(qst)))
+    return S, L, snp1, qst

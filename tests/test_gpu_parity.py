@@ -1,0 +1,189 @@
+"""GPU parity of the assembly path against the CPU oracle, through the C ABI.
+
+Tolerance (FP64 path): R and K agree with the oracle to 1e-10 relative in
+norm, R per entry to 1e-10 max|R|, K per entry to 1e-10 of the row's max
+|K_ij| (row-scaled), state per entry to 1e-10 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import pgfem_gpu as pg
+import workloads as wl
+
+TOL = 1e-10
+pytestmark = pytest.mark.gpu
+
+
+def check_R(Rg, Ro, tol=TOL):
+    assert np.linalg.norm(Rg - Ro) <= tol * np.linalg.norm(Ro), np.linalg.norm(Rg - Ro) / np.linalg.norm(Ro)
+    assert np.abs(Rg - Ro).max() <= tol * np.abs(Ro).max()
+
+
+def check_K(Kg, Ko, Ap, tol=TOL):
+    assert np.linalg.norm(Kg - Ko) <= tol * np.linalg.norm(Ko), np.linalg.norm(Kg - Ko) / np.linalg.norm(Ko)
+    rows = np.repeat(np.arange(len(Ap) - 1), np.diff(Ap))
+    rmax = np.zeros(len(Ap) - 1)
+    np.maximum.at(rmax, rows, np.abs(Ko))
+    assert np.all(np.abs(Kg - Ko) <= tol * rmax[rows])
+
+
+def oracle_assemble(p, nthreads=8):
+    P, mat = oracle.from_workload(p)
+    err, R, K, s = P.assemble(mat, p.u, p.u_presc, state_n=p.state, dt=p.dt, nthreads=nthreads)
+    assert err == 0
+    return R, K, s
+
+
+def test_config1_he_p1_full_size(gpu):
+    p = wl.he_p1(10)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    Ro, Ko, _ = oracle_assemble(p)
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+
+
+@pytest.mark.parametrize("n,stretch", [(3, None), (4, None), (3, 4e-3)])
+def test_j2_p2_parity(gpu, n, stretch):
+    p = wl.j2_p2(n=n, seed=11, stretch=stretch, perturb=5e-3)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    Ro, Ko, so = oracle_assemble(p)
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    sg = ctx.get_state(1)
+    assert np.abs(sg - so).max() <= TOL * np.abs(so).max()
+    frac = (so[:, 9] > 0).mean()
+    if stretch is None:
+        assert 0.05 < frac < 0.95, frac
+
+
+def test_j2_p1_parity(gpu):
+    p = wl.he_p1(5)
+    p.mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
+    p.u = p.u * 0.3
+    p.state = np.zeros((p.nqp, 10))
+    p.state[:, [0, 4, 8]] = 1.0
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok()
+    Ro, Ko, so = oracle_assemble(p)
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    assert (so[:, 9] > 0).any()
+
+
+def test_colour_scatter_deterministic_and_equal(gpu):
+    p = wl.j2_p2(n=3, seed=5, perturb=5e-3)
+    ctx = p.context()
+    Ra, Ka, _ = ctx.assemble_RK(p.u)
+    ctx.set_scatter_mode(pg.SCATTER_COLOUR)
+    R1, K1, _ = ctx.assemble_RK(p.u)
+    R2, K2, _ = ctx.assemble_RK(p.u)
+    assert np.array_equal(R1, R2) and np.array_equal(K1, K2)
+    check_R(R1, Ra, 1e-12)
+    check_K(K1, Ka, p.Ap, 1e-12)
+
+
+def test_assemble_R_only_equals_RK(gpu):
+    p = wl.j2_p2(n=3, seed=5, perturb=5e-3)
+    ctx = p.context()
+    R, K, _ = ctx.assemble_RK(p.u)
+    R2, st = ctx.assemble_R(p.u)
+    assert st.ok()
+    check_R(R2, R, 1e-13)
+
+
+def test_element_level_entry_points(gpu):
+    p = wl.j2_p2(n=3, seed=9, perturb=5e-3, stretch=3e-3)
+    ctx = p.context()
+    P, mat = oracle.from_workload(p)
+    elems = np.array([0, 7, 31, 100, 161])
+    lk, fe, st = ctx.stiffmatel_fd(elems, p.u)
+    fe2, st2 = ctx.resid_on_elem(elems, p.u)
+    assert st.ok() and st2.ok()
+    for k, e in enumerate(elems):
+        ue = np.zeros(30)
+        for a in range(10):
+            for j in range(3):
+                i = p.ids[p.conn[e, a], j]
+                ue[a * 3 + j] = p.u[i - 1] if i > 0 else 0.0
+        err, feo, lko, _ = P.element(mat, e, ue, p.state[e * 4:(e + 1) * 4].ravel())
+        assert err == 0
+        assert np.linalg.norm(fe[k] - feo) <= TOL * np.linalg.norm(feo)
+        assert np.linalg.norm(fe2[k] - feo) <= TOL * np.linalg.norm(feo)
+        assert np.linalg.norm(lk[k] - lko) <= TOL * np.linalg.norm(lko)
+
+
+def sym_L(L):
+    L = L.reshape(-1, 3, 3, 3, 3)
+    L = 0.5 * (L + L.transpose(0, 2, 1, 3, 4))
+    return 0.5 * (L + L.transpose(0, 1, 2, 4, 3))
+
+
+@pytest.mark.parametrize("model", [pg.MODEL_HE, pg.MODEL_J2])
+def test_cm_integrate_matches_oracle(gpu, model):
+    rng = np.random.default_rng(2)
+    nq = 64
+    F = np.eye(3)[None] + rng.uniform(-4e-3, 4e-3, (nq, 3, 3))
+    mat = pg.material(model, sigma_y=250.0, H=2000.0)
+    st = np.zeros((nq, 10))
+    st[:, [0, 4, 8]] = 1.0
+    S, L, snp1, q = pg.cm_integrate(mat, F.reshape(nq, 9), st)
+    assert (q == 0).all()
+    om = oracle.from_pg_material(mat)
+    for i in range(nq):
+        err, So, Lo, so, _ = oracle.cm_update(om, F[i], st[i])
+        assert err == 0
+        assert np.abs(S[i] - So.ravel()).max() <= TOL * np.abs(So).max()
+        Ls, Los = sym_L(L[i]), sym_L(Lo)
+        assert np.abs(Ls - Los).max() <= TOL * np.abs(Los).max()
+        if model == pg.MODEL_J2:
+            assert np.abs(snp1[i] - so).max() <= TOL * np.abs(so).max()
+
+
+def test_state_commit_and_reset(gpu):
+    p = wl.j2_p2(n=2, seed=4, perturb=5e-3, stretch=3e-3)
+    ctx = p.context()
+    ctx.assemble_RK(p.u)
+    s1 = ctx.get_state(1)
+    assert (s1[:, 9] > 0).any()
+    ctx.reset_state()
+    assert np.array_equal(ctx.get_state(1), ctx.get_state(0))
+    ctx.assemble_RK(p.u)
+    ctx.commit_state()
+    assert np.array_equal(ctx.get_state(0), s1)
+    # a second load step from the committed state matches the oracle
+    u2 = p.u * 1.5
+    R, K, _ = ctx.assemble_RK(u2)
+    P, mat = oracle.from_workload(p)
+    _, Ro, Ko, so = P.assemble(mat, u2, state_n=s1)
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+
+
+def test_inverted_element_is_counted_not_trapped(gpu):
+    p = wl.he_p1(3)
+    u = p.u.copy()
+    node = p.conn[40, 3]
+    for j in range(3):
+        if p.ids[node, j] > 0:
+            u[p.ids[node, j] - 1] -= 2.0  # push a vertex through its element
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(u)
+    assert st.inverted > 0
+    # the context stays usable
+    R2, K2, st2 = ctx.assemble_RK(p.u)
+    assert st2.ok()
+
+
+def test_pattern_mismatch_is_rejected(gpu):
+    p = wl.he_p1(2)
+    Ai = p.Ai.copy()
+    Ai[5] = Ai[6]  # corrupt one column id
+    with pytest.raises(pg.PgfemError) as ei:
+        pg.Context(p.X, p.conn, p.ids, p.ndof, p.Ap, Ai, p.mat)
+    assert ei.value.code == -4

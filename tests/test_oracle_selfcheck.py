@@ -1,0 +1,132 @@
+"""Known-answer and consistency checks of the CPU oracle itself.
+
+- central differences of the element residual reproduce the consistent
+  tangent (HE; J2 elastic and plastic points)
+- the spatial B-form ("best CPU") assembly equals the reference-form
+  4-nested compute_stiffness_matrix assembly
+- patch test: an affine displacement gives zero residual on interior DOFs
+- rigid rotation leaves S unchanged; HE and J2 elastic K are symmetric
+"""
+import numpy as np
+import pytest
+
+import oracle
+import workloads as wl
+
+
+def rot(a, b, c):
+    def Rx(t):
+        return np.array([[1, 0, 0], [0, np.cos(t), -np.sin(t)], [0, np.sin(t), np.cos(t)]])
+
+    def Rz(t):
+        return np.array([[np.cos(t), -np.sin(t), 0], [np.sin(t), np.cos(t), 0], [0, 0, 1]])
+    return Rz(a) @ Rx(b) @ Rz(c)
+
+
+def small_problem(kind, n=2, stretch=None):
+    if kind == "he":
+        p = wl.he_p1(n=n, seed=7)
+    else:
+        p = wl.j2_p2(n=n, seed=3, stretch=stretch, perturb=2e-2)
+    P, mat = oracle.from_workload(p)
+    return p, P, mat
+
+
+def elem_u(p, e, u):
+    ue = np.zeros(p.nne * 3)
+    for a in range(p.nne):
+        for j in range(3):
+            i = p.ids[p.conn[e, a], j]
+            ue[a * 3 + j] = u[i - 1] if i > 0 else 0.0
+    return ue
+
+
+@pytest.mark.parametrize("kind,stretch", [("he", None), ("j2", 1e-4), ("j2", 6e-3)])
+def test_tangent_matches_central_differences(kind, stretch):
+    p, P, mat = small_problem(kind, stretch=stretch)
+    rng = np.random.default_rng(0)
+    for e in rng.choice(p.ne, 4, replace=False):
+        ue = elem_u(p, e, p.u)
+        sn = None if p.state is None else p.state[e * p.nint:(e + 1) * p.nint].ravel()
+        err, fe, lk, _ = P.element(mat, e, ue, sn)
+        assert err == 0
+        h = 1e-7 * max(1.0, np.abs(ue).max())
+        fd = np.zeros_like(lk)
+        for k in range(len(ue)):
+            up, um = ue.copy(), ue.copy()
+            up[k] += h
+            um[k] -= h
+            _, fp, _, _ = P.element(mat, e, up, sn, want_K=False)
+            _, fm, _, _ = P.element(mat, e, um, sn, want_K=False)
+            fd[:, k] = (fp - fm) / (2 * h)
+        assert np.linalg.norm(fd - lk) <= 1e-6 * np.linalg.norm(lk), (e, np.linalg.norm(fd - lk) / np.linalg.norm(lk))
+
+
+def test_j2_plastic_points_exist_in_plastic_case():
+    p, P, mat = small_problem("j2", stretch=6e-3)
+    err, R, K, snp1 = P.assemble(mat, p.u, state_n=p.state)
+    assert err == 0
+    assert (snp1[:, 9] > 0).mean() > 0.5
+
+
+@pytest.mark.parametrize("kind,stretch", [("he", None), ("j2", None), ("j2", 6e-3)])
+def test_bform_equals_reference_form(kind, stretch):
+    p, P, mat = small_problem(kind, n=3, stretch=stretch)
+    err, R, K, s1 = P.assemble(mat, p.u, state_n=p.state)
+    err2, R2, K2, s2 = P.assemble(mat, p.u, state_n=p.state, bform=True)
+    assert err == 0 and err2 == 0
+    assert np.linalg.norm(R2 - R) <= 1e-12 * np.linalg.norm(R)
+    assert np.linalg.norm(K2 - K) <= 1e-12 * np.linalg.norm(K)
+    if s1 is not None:
+        assert np.abs(s2 - s1).max() <= 1e-12 * max(1.0, np.abs(s1).max())
+
+
+def test_multithreaded_assembly_equals_serial():
+    p, P, mat = small_problem("j2", n=3)
+    _, R1, K1, _ = P.assemble(mat, p.u, state_n=p.state, nthreads=1)
+    _, R4, K4, _ = P.assemble(mat, p.u, state_n=p.state, nthreads=4)
+    assert np.linalg.norm(R4 - R1) <= 1e-13 * np.linalg.norm(R1)
+    assert np.linalg.norm(K4 - K1) <= 1e-13 * np.linalg.norm(K1)
+
+
+@pytest.mark.parametrize("nne", [4, 10])
+def test_patch_affine_displacement_interior_residual_zero(nne):
+    import pgfem_gpu as pg
+    X, conn, Pr = pg.mesh_box_tet(3, nne)
+    nn = X.shape[0]
+    codes = np.zeros((nn, 3), dtype=np.int64)
+    ids, ndof = oracle.generate_dof_ids(conn, nn, codes)
+    Ap, Ai = oracle.psparse_apai(conn, ids, ndof)
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai)
+    G = np.array([[2e-3, 1e-3, -5e-4], [4e-4, -1e-3, 2e-4], [1e-4, 3e-4, 1.5e-3]])
+    disp = X @ G.T
+    u = wl.nodal_to_free(ids, disp)
+    mat = oracle.material(oracle.HE)
+    err, R, K, _ = P.assemble(mat, u)
+    assert err == 0
+    interior = np.all((X > 1e-12) & (X < 1 - 1e-12), axis=1)
+    rows = ids[interior].ravel() - 1
+    assert np.abs(R[rows]).max() <= 1e-10 * np.abs(R).max()
+    # all-free: internal forces sum to zero per component
+    for c in range(3):
+        assert abs(R[ids[:, c] - 1].sum()) <= 1e-11 * np.abs(R).max()
+
+
+@pytest.mark.parametrize("model", [oracle.HE, oracle.J2])
+def test_rigid_rotation_invariance(model):
+    mat = oracle.material(model, sigma_y=250.0, H=2000.0)
+    F = np.eye(3) + np.array([[3e-3, 1e-3, 0], [0, -1e-3, 2e-3], [5e-4, 0, 2e-3]])
+    st = np.zeros(10)
+    st[[0, 4, 8]] = 1.0
+    e1, S1, _, _, _ = oracle.cm_update(mat, F, st)
+    Q = rot(0.3, -1.1, 2.0)
+    e2, S2, _, _, _ = oracle.cm_update(mat, Q @ F, st)
+    assert e1 == 0 and e2 == 0
+    assert np.abs(S1 - S2).max() <= 1e-10 * np.abs(S1).max()
+
+
+def test_he_stiffness_symmetric():
+    p, P, mat = small_problem("he", n=2)
+    err, fe, lk, _ = P.element(mat, 5, elem_u(p, 5, p.u))
+    assert err == 0
+    assert np.abs(lk - lk.T).max() <= 1e-10 * np.abs(lk).max()
