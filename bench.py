@@ -181,6 +181,8 @@ def run_ours(args, ws, rank, local):
     ctx = p.context()
     log("[rank %d] context (device copy + element->CSR map) %.1f s, %.2f GB on device"
         % (rank, time.perf_counter() - t0, ctx.device_bytes() / 1e9))
+    ctx.set_scatter_mode({"atomic": pg.SCATTER_ATOMIC, "colour": pg.SCATTER_COLOUR,
+                          "tiles": pg.SCATTER_TILES}[args.scatter])
     fp64_peak = pg.fp64_peak_tflops()
     hbm_peak, hbm_src = measured_hbm_gbs()
 
@@ -273,7 +275,7 @@ def run_ours(args, ws, rank, local):
                       "elements": p.ne, "quad_points": p.nqp, "dofs": p.ndof, "nnz": p.nnz,
                       "yielded_fraction": yielded, "parallelism": "replicas%d" % ws if ws > 1 else "1 GPU",
                       "l2": "inputs larger than L2 (K values %.2f GB)" % (8e-9 * p.nnz),
-                      "scatter": "atomic"},
+                      "scatter": args.scatter},
            "roofline": roof, "clocks": clocks,
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
                    "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "steps": n_e2e},
@@ -341,6 +343,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles"])
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":

@@ -49,9 +49,14 @@ enum {
  * exchange format: HE 0; J2 10 = Cp^-1 (9) + eqps; CP 10 = pF (9) + g. */
 int pgfem_gpu_state_size(int model);
 
-/* Scatter modes: atomic FP64 adds, or element colours with plain adds
- * (deterministic summation order). */
-enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1 };
+/* Scatter modes:
+ *  ATOMIC  one fused kernel, FP64 atomic adds per element entry (default);
+ *  COLOUR  element colours with plain adds (deterministic summation order);
+ *  TILES   point-update kernel + persistent tile kernel that combines the
+ *          blocks of a cell of elements in shared memory, issues address-
+ *          ordered reductions and zero-fills the CSR rows a tile touches first
+ *          instead of a full memset (2.3x less DRAM traffic per iterate). */
+enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1, PGFEM_SCATTER_TILES = 2 };
 
 typedef struct {
   int model;

@@ -14,10 +14,13 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
 #include "assemble.cuh"
+#include "tile_plan.hpp"
+#include "assemble_tiles.cuh"
 #include "cm_integrate.cuh"
 #include "peak_probe.cuh"
 #include "pgfem_gpu.h"
@@ -51,6 +54,20 @@ struct pgfem_gpu_ctx {
   std::vector<long> colour_off;  // offsets into colour element list
   int *colour_elems = nullptr;
   long bytes = 0;
+  // tiled assembly plan (device copies)
+  bool tiles = false;
+  int tile_zero_mode = 0, nslots_max = 0;
+  long ntiles = 0;
+  int *t_nodes = nullptr;
+  uint8_t *t_nl = nullptr, *t_lnode = nullptr;
+  uint16_t *t_slot = nullptr, *t_aoff = nullptr;
+  long long *t_soff = nullptr, *t_zlo = nullptr, *t_zhi = nullptr;
+  uint32_t *t_sinfo = nullptr;
+  int *t_deps = nullptr;
+  uint8_t *t_allfree = nullptr;
+  unsigned *t_flags = nullptr, *t_ticket = nullptr;
+  unsigned epoch = 0;
+  double *qrec = nullptr;  // point records (kQRec x nqp)
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -215,7 +232,8 @@ void release(pgfem_gpu_ctx *c) {
   drop_events(c);
   void *ptrs[] = {c->X, c->conn, c->dof, c->rowptr0, c->rowlen, c->mask, c->pos, c->unode, c->F0,
                   c->state_n, c->state_np1, c->status, c->d_u, c->d_presc, c->d_R, c->d_K,
-                  c->colour_elems};
+                  c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
+                  c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -274,6 +292,78 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+template <int NNE, int NQP, int MODEL>
+int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  {
+    QpArgs q{};
+    q.X = c->X;
+    q.unode = c->unode;
+    q.conn = c->conn;
+    q.nn = c->nn;
+    q.ne = c->ne;
+    q.nqp = c->nqp;
+    q.F0 = c->F0;
+    q.state_n = c->state_n;
+    q.state_np1 = c->state_np1;
+    q.qrec = c->qrec;
+    q.status = c->status;
+    q.mat = c->mat;
+    q.shp = c->shp;
+    k_qp_update<NNE, NQP, MODEL><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
+    CK(cudaGetLastError());
+  }
+  const size_t smem = tiles_smem_bytes<NNE, NQP>(c->nslots_max);
+  auto kern = k_assemble_tiles<NNE, NQP, MODEL>;
+  constexpr int T = tile_threads<NNE>();
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long grid = std::max<long>(1, std::min<long>(c->ntiles, (long)g_num_sms * per_sm));
+  TileArgs a{};
+  a.dof = c->dof;
+  a.rowptr0 = c->rowptr0;
+  a.rowlen = c->rowlen;
+  a.mask = c->mask;
+  a.nn = c->nn;
+  a.ne = c->ne;
+  a.nqp = c->nqp;
+  a.qrec = c->qrec;
+  a.tile_nodes = c->t_nodes;
+  a.tile_nl = c->t_nl;
+  a.elem_lnode = c->t_lnode;
+  a.elem_slot = c->t_slot;
+  a.slot_off = c->t_soff;
+  a.slot_info = c->t_sinfo;
+  a.aoff = c->t_aoff;
+  a.zlo = c->t_zlo;
+  a.zhi = c->t_zhi;
+  a.deps = c->t_deps;
+  a.allfree = c->t_allfree;
+  a.flags = c->t_flags;
+  a.ticket = c->t_ticket;
+  a.epoch = ++c->epoch;
+  a.zero_mode = c->tile_zero_mode;
+  a.zahead = (int)std::min<long>(c->ntiles, std::max<long>(64, (3 * grid) / 2));
+  a.ntiles = c->ntiles;
+  a.nslots_max = c->nslots_max;
+  a.R = d_R;
+  a.K = d_K;
+  a.status = c->status;
+  a.shp = c->shp;
+  CK(cudaMemsetAsync(c->t_ticket, 0, sizeof(unsigned), s));
+  kern<<<(unsigned)grid, T, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+int dispatch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  if (c->nne == 4)
+    return c->model == PGFEM_MODEL_J2 ? launch_tiles<4, 1, 1>(c, d_R, d_K, s) : launch_tiles<4, 1, 0>(c, d_R, d_K, s);
+  return c->model == PGFEM_MODEL_J2 ? launch_tiles<10, 4, 1>(c, d_R, d_K, s) : launch_tiles<10, 4, 0>(c, d_R, d_K, s);
+}
+
 template <bool ATOMIC, bool WANT_K, bool DENSE>
 int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
   if (c->nne == 4) {
@@ -294,8 +384,9 @@ int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t
 int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
                     double *d_K, cudaStream_t s) {
   if (c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  const bool use_tiles = c->tiles && d_K && c->scatter_mode == PGFEM_SCATTER_TILES;
   if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
-  if (d_K) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
+  if (d_K && !(use_tiles && c->tile_zero_mode)) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
   {
     const long n3 = 3 * c->nn;
     k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
@@ -311,7 +402,9 @@ int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, 
     CK(cudaEventRecord(e0, s));
   }
   int r = PGFEM_GPU_OK;
-  if (c->scatter_mode == PGFEM_SCATTER_COLOUR && c->colour_elems) {
+  if (use_tiles) {
+    r = dispatch_tiles(c, d_R, d_K, s);
+  } else if (c->scatter_mode == PGFEM_SCATTER_COLOUR && c->colour_elems) {
     for (size_t k = 0; k + 1 < c->colour_off.size() && !r; k++) {
       a.elist = c->colour_elems + c->colour_off[k];
       a.nlist = c->colour_off[k + 1] - c->colour_off[k];
@@ -488,6 +581,40 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if (ce != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
     if (herr) return fail(PGFEM_GPU_EPATTERN);
   }
+  // tiled assembly plan (HE / J2)
+  if (c->model != PGFEM_MODEL_CP && !getenv("PGFEM_GPU_NO_TILES")) {
+    std::vector<int> first_dof(nn, -1);
+    for (long n = 0; n < nn; n++)
+      for (int j = 0; j < 3 && first_dof[n] < 0; j++)
+        if (m->dof_id[n * 3 + j] > 0) first_dof[n] = (int)m->dof_id[n * 3 + j] - 1;
+    std::vector<int> conn_em(m->conn, m->conn + (size_t)ne * m->nne);
+    TilePlan P;
+    const int TE = m->nne == 10 ? TileCfg<10>::TE : TileCfg<4>::TE;
+    if (!build_tile_plan(P, TE, m->nne, ne, conn_em, first_dof, mask, Ap, Ai, m->ndof))
+      return fail(PGFEM_GPU_EPATTERN);
+    c->ntiles = P.ntiles;
+    c->nslots_max = P.nslots_max;
+    c->tile_zero_mode = P.first_touch ? 1 : 0;
+    if (getenv("PGFEM_GPU_TILE_MEMSET")) c->tile_zero_mode = 0;
+    if ((r = upload(c, &c->t_nodes, P.tile_nodes.data(), P.tile_nodes.size())) ||
+        (r = upload(c, &c->t_nl, P.tile_nl.data(), P.tile_nl.size())) ||
+        (r = upload(c, &c->t_lnode, P.elem_lnode.data(), P.elem_lnode.size())) ||
+        (r = upload(c, &c->t_slot, P.elem_slot.data(), P.elem_slot.size())) ||
+        (r = upload(c, &c->t_soff, P.slot_off.data(), P.slot_off.size())) ||
+        (r = upload(c, &c->t_sinfo, P.slot_info.data(), std::max<size_t>(1, P.slot_info.size()))) ||
+        (r = upload(c, &c->t_aoff, P.aoff.data(), P.aoff.size())) ||
+        (r = upload(c, &c->t_zlo, P.zlo.data(), P.zlo.size())) ||
+        (r = upload(c, &c->t_zhi, P.zhi.data(), P.zhi.size())) ||
+        (r = upload(c, &c->t_deps, P.deps.data(), P.deps.size())) ||
+        (r = upload(c, &c->t_allfree, P.allfree.data(), P.allfree.size())) ||
+        (r = dalloc(c, &c->t_flags, P.ntiles)) || (r = dalloc(c, &c->t_ticket, 1)) ||
+        (r = dalloc(c, &c->qrec, (size_t)kQRec * c->nqp)))
+      return fail(r);
+    if (cudaMemsetAsync(c->t_flags, 0, sizeof(unsigned) * P.ntiles, c->stream) != cudaSuccess ||
+        cudaStreamSynchronize(c->stream) != cudaSuccess)
+      return fail(PGFEM_GPU_ECUDA);
+    c->tiles = true;
+  }
   // default state: identity Cp^-1 / pF, zero eqps, g = g0
   if (c->nstate) {
     std::vector<double> s0((size_t)c->nstate * c->nqp, 0.0);
@@ -521,7 +648,9 @@ int pgfem_gpu_destroy(pgfem_gpu_ctx *c) {
 }
 
 int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
-  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR)) return PGFEM_GPU_EINVAL;
+  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR && mode != PGFEM_SCATTER_TILES))
+    return PGFEM_GPU_EINVAL;
+  if (mode == PGFEM_SCATTER_TILES && !c->tiles) return PGFEM_GPU_EINVAL;
   c->scatter_mode = mode;
   return PGFEM_GPU_OK;
 }
@@ -531,6 +660,7 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
+  if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
 }

@@ -187,3 +187,66 @@ def test_pattern_mismatch_is_rejected(gpu):
     with pytest.raises(pg.PgfemError) as ei:
         pg.Context(p.X, p.conn, p.ids, p.ndof, p.Ap, Ai, p.mat)
     assert ei.value.code == -4
+
+
+def _ctx_with_env(p, **env):
+    import os
+    old = {k: os.environ.get(k) for k in env}
+    try:
+        for k, v in env.items():
+            os.environ[k] = v
+        return p.context()
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+
+
+@pytest.mark.parametrize("kind", ["j2_p2", "he_p1"])
+def test_tiled_first_touch_memset_and_untiled_agree(gpu, kind):
+    p = wl.j2_p2(n=4, seed=2, perturb=1e-4) if kind == "j2_p2" else wl.he_p1(6, seed=3)
+    ref = _ctx_with_env(p, PGFEM_GPU_NO_TILES="1")
+    Ru, Ku, _ = ref.assemble_RK(p.u)
+    with pytest.raises(pg.PgfemError):
+        ref.set_scatter_mode(pg.SCATTER_TILES)  # no tile plan in this context
+    for env in ({}, {"PGFEM_GPU_TILE_MEMSET": "1"}):
+        ctx = _ctx_with_env(p, **env)
+        ctx.set_scatter_mode(pg.SCATTER_TILES)
+        R, K, st = ctx.assemble_RK(p.u)
+        assert st.ok(), st.as_dict()
+        check_R(R, Ru, 1e-12)
+        check_K(K, Ku, p.Ap, 1e-12)
+        # repeated calls (flags carry an epoch; no reset between calls)
+        R2, K2, st2 = ctx.assemble_RK(p.u)
+        assert st2.ok()
+        check_R(R2, R, 1e-13)
+        check_K(K2, K, p.Ap, 1e-13)
+
+
+def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
+    # number the nodes in reverse order (ids stay consecutive per node, but the
+    # rows are no longer first touched in element order)
+    import pgfem_gpu as pgm
+    X, conn, _ = pgm.mesh_box_tet(3, 10)
+    nn = X.shape[0]
+    ids = np.zeros((nn, 3), dtype=np.int64)
+    order = np.arange(nn)[::-1]
+    ids[order] = (np.arange(nn)[:, None] * 3 + np.arange(3)[None, :] + 1)
+    ndof = 3 * nn
+    Ap, Ai = pgm.psparse_apai(conn, ids, ndof)
+    r = wl.splitmix64(5, nn * 3).reshape(nn, 3)
+    disp = (2 * r - 1) * 1e-4 / 3 + np.outer(X[:, 0], [wl.j2_yield_strain(), 0, 0])
+    u = wl.nodal_to_free(ids, disp)
+    mat = pg.material(pg.MODEL_J2, sigma_y=250.0, H=2000.0)
+    state = np.zeros((conn.shape[0] * 4, 10))
+    state[:, [0, 4, 8]] = 1.0
+    prob = wl.Problem("rev", X, conn, ids, ndof, Ap, Ai, mat, u, state=state)
+    ctx = prob.context()
+    ctx.set_scatter_mode(pg.SCATTER_TILES)
+    R, K, st = ctx.assemble_RK(u)
+    assert st.ok()
+    Ro, Ko, _ = oracle_assemble(prob)
+    check_R(R, Ro)
+    check_K(K, Ko, Ap)
