@@ -295,6 +295,82 @@ def run_ours(args, ws, rank, local):
     return out
 
 
+def run_cp(args, ws, rank, local):
+    """Config 3: FCC crystal plasticity, 48^3 cells x 6 linear tets, one R+K
+    iterate at load step `--cp-step` of the 1 % tension ramp (the state of the
+    previous step is produced on the GPU first)."""
+    import torch
+
+    import pgfem_gpu as pg
+    import workloads as wl
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    p = wl.cp_p1(n=args.cp_n, seed=2)
+    ctx = p.context()
+    log("[rank %d] CP setup %.1f s, %d elements" % (rank, time.perf_counter() - t0, p.ne))
+    for s in range(1, args.cp_step):
+        _, _, st = ctx.assemble_RK(p.displacement(s), dt=p.dt)
+        assert st.ok(), st.as_dict()
+        ctx.commit_state()
+    u = p.displacement(args.cp_step)
+    stream = torch.cuda.current_stream()
+    d_u = torch.from_numpy(u).to(dev)
+    d_R = torch.empty(p.ndof, dtype=torch.float64, device=dev)
+    d_K = torch.empty(p.nnz, dtype=torch.float64, device=dev)
+    sh = stream.cuda_stream
+
+    def step():
+        ctx.assemble_RK_device(d_u.data_ptr(), None, d_R.data_ptr(), d_K.data_ptr(), sh, dt=p.dt)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    st = ctx.read_status(clear=True)
+    assert st.ok(), st.as_dict()
+    ctx.set_timing(True)
+    ctx.kernel_time(reset=True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = allreduce_max(e0.elapsed_time(e1), ws)
+    kms, kc = ctx.kernel_time(reset=True)
+    it = ctx.cp_iterations()
+    out = {"metric": METRIC, "value": ws * p.nqp * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64)",
+           "config": {"workload": "FCC crystal plasticity, %d^3 cells x 6 linear tets (%d elements, 1 point each), "
+                                  "512 Voronoi grains, R+K at load step %d of %d (1 %% tension ramp, dt 0.1 s), "
+                                  "cold-start local Newton to 1e-10" % (args.cp_n, p.ne, args.cp_step, wl.CP_STEPS),
+                      "local_newton_ms": kms / max(kc, 1),
+                      "iterations_hist": np.bincount(it).tolist(), "iterations_mean": float(it.mean())},
+           "gpu_launches": args.steps * ctx.launches_per_assembly()}
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        P, mat = oracle.from_workload(p)
+        sn = ctx.get_state(0)
+        e1_ = 256
+        t0 = time.perf_counter()
+        P.assemble(mat, u, state_n=sn, dt=p.dt, e1=e1_)
+        dt_ = time.perf_counter() - t0
+        S = int(min(p.ne, max(e1_, e1_ * args.cpu_seconds / max(dt_, 1e-6))))
+        t0 = time.perf_counter()
+        P.assemble(mat, u, state_n=sn, dt=p.dt, e1=S)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": S / t, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": "first %d elements of the same step, reference element algorithm + "
+                                         "restated CP local Newton, 1 thread, %.1f s" % (S, t)}
+    ctx.close()
+    return out
+
+
 def run_reference(args, ws, rank):
     import workloads as wl
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -344,6 +420,9 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles"])
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "cp_p1"])
+    ap.add_argument("--cp-n", type=int, default=48)
+    ap.add_argument("--cp-step", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
@@ -354,7 +433,7 @@ def main():
             print(json.dumps(out), flush=True)
         return
     ws, rank, local = dist_setup(args.gpus)
-    out = run_ours(args, ws, rank, local)
+    out = run_cp(args, ws, rank, local) if args.workload == "cp_p1" else run_ours(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if ws > 1:

@@ -162,6 +162,17 @@ int pgfem_gpu_kernel_time(pgfem_gpu_ctx *ctx, double *ms, long *ncalls, int rese
  * in the reference. */
 int pgfem_gpu_fp64_peak(double *tflops);
 
+/* ---- crystal plasticity local solver -------------------------------------
+ * Initial guess of the local Newton per quadrature point (host AoS nqp*10:
+ * M0 = pF_n pF_{n+1}^-1 guess (9), g guess); NULL restores the elastic
+ * predictor (M = I, g = g_n).  The plain solve always remains the fallback:
+ * a point whose Newton from the guess fails is counted as non-converged.
+ * No counterpart in the reference. */
+int pgfem_gpu_set_cp_guess(pgfem_gpu_ctx *ctx, const double *guess);
+/* Per-point local Newton iteration counts (nqp) and slip increments
+ * dt*gamma_dot_a (nqp*12, may be NULL) of the last assembly. */
+int pgfem_gpu_get_cp_iterations(pgfem_gpu_ctx *ctx, int *iters, double *dgam);
+
 /* ---- element level (batched over an element list) -----------------------
  * stiffness_el_constitutive_model / residuals_el_constitutive_model
  * (include/constitutive_model.h:1003-1049), exported under the element

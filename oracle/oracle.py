@@ -55,6 +55,8 @@ def lib():
                                        C.c_int, _P]),
             "orc_assemble_bform": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P, _P, C.c_long,
                                              C.c_long, C.c_int]),
+            "orc_cp_update_batch": (C.c_long, [_P, C.c_long, _P, C.c_double, _P, _P, _P, _P, _P, _P, _P,
+                                               _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -113,6 +115,22 @@ def cm_update(mat, F, state_n=None, dt=0.0, Rcp=None):
     it = C.c_int()
     err = lib().orc_cm_update(C.byref(mat), _p(F), dt, _p(Rcp), _p(sn), _p(snp1), _p(S), _p(L), C.byref(it))
     return err, S.reshape(3, 3), L.reshape(3, 3, 3, 3), snp1, it.value
+
+
+def cp_update_batch(mat, F, state_n, dt, Rcp, M0=None, g_guess=None):
+    F = np.ascontiguousarray(F, dtype=np.float64).reshape(-1, 9)
+    nq = F.shape[0]
+    state_n = np.ascontiguousarray(state_n, dtype=np.float64).reshape(nq, 10)
+    Rcp = np.ascontiguousarray(Rcp, dtype=np.float64).reshape(nq, 9)
+    M0 = None if M0 is None else np.ascontiguousarray(M0, dtype=np.float64).reshape(nq, 9)
+    gg = None if g_guess is None else np.ascontiguousarray(g_guess, dtype=np.float64).reshape(nq)
+    snp1 = np.zeros((nq, 10))
+    it = np.zeros(nq, dtype=np.int32)
+    dg = np.zeros((nq, 12))
+    cv = np.zeros(nq, dtype=np.int32)
+    bad = lib().orc_cp_update_batch(C.byref(mat), nq, _p(F), dt, _p(Rcp), _p(state_n), _p(M0), _p(gg), _p(snp1),
+                                    _p(it), _p(dg), _p(cv))
+    return bad, snp1, it, dg, cv
 
 
 class Problem:

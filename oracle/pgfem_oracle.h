@@ -109,6 +109,16 @@ int orc_assemble_bform(const orc_problem *P, const orc_material *mat,
                        const double *state_n, double *state_np1, double *R,
                        double *K, long e0, long e1, int nthreads);
 
+/* Crystal-plasticity point updates over nqp points: F (nqp*9), rotations
+ * Rcp (nqp*9), state at t_n (nqp*10: pF_n 9, g_n).  M0/g_guess (may be NULL)
+ * give the Newton's initial guess per point (NULL: elastic predictor).
+ * Outputs the state at t_{n+1} (nqp*10), the iteration counts, the slip
+ * increments dt*gamma_dot_a (nqp*12, may be NULL) and a convergence flag.
+ * Returns the number of points that failed. */
+long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, double dt, const double *Rcp,
+                         const double *state_n, const double *M0, const double *g_guess,
+                         double *state_np1, int *iters, double *dgam, int *converged);
+
 /* Number of quadrature points per element for nne (1 for 4, 4 for 10). */
 int orc_nint(int nne);
 

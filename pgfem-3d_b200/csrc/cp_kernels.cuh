@@ -1,0 +1,636 @@
+// cp_kernels.cuh -- crystal plasticity (CP_PARAM) on the device.
+//
+// Constitutive law (the reference's CM crystal plasticity, src/plasticity_model.cc,
+// with the flow and hardening laws of src/TA_GA.cc:8-41 and
+// src/integration.cc:378-423): FCC {111}<110> slip, resolved shear
+// tau_a = s_a . (Ce S) n_a, gamma_dot_a = gamma_dot_0 sgn(tau_a)|tau_a/g|^(1/m),
+// M = pF_n pF_{n+1}^-1 = I - dt sum gamma_dot_a P_a, saturation hardening
+// g - g_n - dt G0 gamma_dot (gs - g)/(gs - g0) = 0 (w = 0), neo-Hookean +
+// U_Common elasticity at Ce = M^T Ce' M.  The local problem in x = (M, g) is
+// solved by Newton with backtracking from the elastic predictor or from a
+// supplied initial guess; at convergence the consistent dM/dF is formed.
+//
+// k_cp_update is persistent: every lane owns one quadrature point at a time
+// and takes a new one from a global counter as soon as its Newton converges,
+// so lanes with 2 and 15 iterations do not idle each other.  The 10x10
+// Jacobian of each lane lives in shared memory (lane-strided, bank-conflict
+// free).  Slip systems are evaluated in the crystal frame: the Mandel product
+// is rotated once per evaluation, the slip directions/normals are constants.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "cm_models.cuh"
+
+namespace pgb {
+
+constexpr int kSlip = 12;
+constexpr int kCpOut = 9 + 81 + 1 + 12;  // M (UL), dM/dF, g, dt*gamma_dot_a  (per point, SoA)
+
+// FCC slip directions (unnormalised <110>) and normals (unnormalised {111})
+__constant__ double c_slip_s[kSlip][3] = {{0, 1, -1}, {1, 0, -1}, {1, -1, 0}, {0, 1, -1}, {1, 0, 1}, {1, 1, 0},
+                                          {0, 1, 1},  {1, 0, -1}, {1, 1, 0},  {0, 1, 1},  {1, 0, 1}, {1, -1, 0}};
+__constant__ double c_slip_n[kSlip][3] = {{1, 1, 1},  {1, 1, 1},  {1, 1, 1},  {-1, 1, 1}, {-1, 1, 1}, {-1, 1, 1},
+                                          {1, -1, 1}, {1, -1, 1}, {1, -1, 1}, {1, 1, -1}, {1, 1, -1}, {1, 1, -1}};
+
+__device__ __forceinline__ void mm3(const double *A, const double *B, double *C) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C[i * 3 + j] = A[i * 3] * B[j] + A[i * 3 + 1] * B[3 + j] + A[i * 3 + 2] * B[6 + j];
+}
+__device__ __forceinline__ void mm3tn(const double *A, const double *B, double *C) {  // A^T B
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) C[i * 3 + j] = A[i] * B[j] + A[3 + i] * B[3 + j] + A[6 + i] * B[6 + j];
+}
+__device__ __forceinline__ void mm3nt(const double *A, const double *B, double *C) {  // A B^T
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      C[i * 3 + j] = A[i * 3] * B[j * 3] + A[i * 3 + 1] * B[j * 3 + 1] + A[i * 3 + 2] * B[j * 3 + 2];
+}
+
+// Neo-Hookean (Mooney-Rivlin m01 = 0) + U_Common PK2 stress at C and its
+// directional derivative dS[X] for symmetric X (= 1/2 L : X).
+struct NeoHooke {
+  double Ci[9], S[9], J, J23, trC;
+};
+
+__device__ __forceinline__ bool nh_stress(const Mat &mat, const double *C, NeoHooke &h) {
+  const double detC = det3(C);
+  if (!(detC > 0.0)) return false;
+  inv3(C, h.Ci);
+  h.J = sqrt(detC);
+  h.J23 = 1.0 / cbrt(detC);  // detC^{-1/3}
+  h.trC = C[0] + C[4] + C[8];
+  const double a = mat.mu * h.J23, pv = mat.kappa * h.J * (h.J - 1.0);
+#pragma unroll
+  for (int i = 0; i < 9; i++) h.S[i] = a * ((i % 4 == 0 ? 1.0 : 0.0) - h.trC / 3.0 * h.Ci[i]) + pv * h.Ci[i];
+  return true;
+}
+
+__device__ __forceinline__ void nh_dS(const Mat &mat, const NeoHooke &h, const double *X, double *dS) {
+  // S = mu detC^{-1/3} (I - trC/3 Ci) + kappa J(J-1) Ci
+  double CiX = 0, trX = X[0] + X[4] + X[8];
+#pragma unroll
+  for (int i = 0; i < 9; i++) CiX += h.Ci[i] * X[i];
+  double t[9], CXC[9];
+  mm3(h.Ci, X, t);
+  mm3(t, h.Ci, CXC);
+  const double a = mat.mu * h.J23;
+  const double dpv = mat.kappa * (2.0 * h.J - 1.0) * 0.5 * h.J * CiX;
+  const double pv = mat.kappa * h.J * (h.J - 1.0);
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const double d = (i % 4 == 0 ? 1.0 : 0.0);
+    dS[i] = a * (-CiX / 3.0 * (d - h.trC / 3.0 * h.Ci[i]) - trX / 3.0 * h.Ci[i] + h.trC / 3.0 * CXC[i]) +
+            dpv * h.Ci[i] - pv * CXC[i];
+  }
+}
+
+// Sample-frame Schmid tensor of system a from the crystal rotation R.
+__device__ __forceinline__ void schmid(const double *R, int a, double *P) {
+  const double is2 = 0.70710678118654752440, is3 = 0.57735026918962576451;
+  double s[3], n[3];
+#pragma unroll
+  for (int i = 0; i < 3; i++) {
+    s[i] = (R[i * 3] * c_slip_s[a][0] + R[i * 3 + 1] * c_slip_s[a][1] + R[i * 3 + 2] * c_slip_s[a][2]) * is2;
+    n[i] = (R[i * 3] * c_slip_n[a][0] + R[i * 3 + 1] * c_slip_n[a][1] + R[i * 3 + 2] * c_slip_n[a][2]) * is3;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) P[i * 3 + j] = s[i] * n[j];
+}
+
+__device__ __forceinline__ double flow_pow(double r, double e) { return pow(r, e); }
+
+// Residual of the local problem at (M, g).  Returns false on an invalid state.
+struct CpPoint {
+  double Cep[9], R[9];  // trial Ce' and crystal rotation
+  double g_n, dt;
+};
+
+__device__ __forceinline__ bool cp_residual(const Mat &mat, const CpPoint &pt, const double *M, double g,
+                                            double *Res, NeoHooke &h, double *gd, double *dgd, double &gdot) {
+  double t[9], Ce[9];
+  mm3(pt.Cep, M, t);
+  mm3tn(M, t, Ce);
+  if (!(g > 0.0) || !nh_stress(mat, Ce, h)) return false;
+  double CS[9];
+  mm3(Ce, h.S, CS);
+  const double im = 1.0 / mat.m;
+  gdot = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) Res[i] = M[i] - (i % 4 == 0 ? 1.0 : 0.0);
+  for (int a = 0; a < kSlip; a++) {
+    double P[9];
+    schmid(pt.R, a, P);
+    double tau = 0;
+#pragma unroll
+    for (int i = 0; i < 9; i++) tau += CS[i] * P[i];
+    const double pw = flow_pow(fabs(tau / g), im - 1.0);
+    gd[a] = mat.gdot0 * (tau / g) * pw;
+    dgd[a] = mat.gdot0 * im / g * pw;
+    gdot += fabs(gd[a]);
+#pragma unroll
+    for (int i = 0; i < 9; i++) Res[i] += pt.dt * gd[a] * P[i];
+  }
+  Res[9] = g - pt.g_n - pt.dt * mat.G0 * gdot * (mat.gs0 - g) / (mat.gs0 - mat.g0);
+  return true;
+}
+
+__device__ __forceinline__ double cp_norm(const double *R, double g0) {
+  double m = 0;
+#pragma unroll
+  for (int i = 0; i < 9; i++) m = fmax(m, fabs(R[i]));
+  return fmax(m, fabs(R[9]) / g0);
+}
+
+// Ysym_a = sym(P_a S + dS[sym(Ce P_a)]): d tau_a = dCe : Ysym_a.
+__device__ __forceinline__ void ysym(const Mat &mat, const NeoHooke &h, const double *Ce, const double *P,
+                                     double *Y) {
+  double PS[9], CP[9], X[9], dS[9];
+  mm3(P, h.S, PS);
+  mm3(Ce, P, CP);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) X[i * 3 + j] = 0.5 * (CP[i * 3 + j] + CP[j * 3 + i]);
+  nh_dS(mat, h, X, dS);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      const double y1 = PS[i * 3 + j] + dS[i * 3 + j], y2 = PS[j * 3 + i] + dS[j * 3 + i];
+      Y[i * 3 + j] = 0.5 * (y1 + y2);
+    }
+}
+
+// Lane-strided dense 10 x nc block in shared memory: element (r, c) at
+// base[(r * nc + c) * 32].
+__device__ __forceinline__ double &lm(double *base, int nc, int r, int c) { return base[(r * nc + c) * 32]; }
+
+// Gaussian elimination with partial pivoting, n x n matrix A with nrhs
+// right-hand sides B (both lane-strided).  false if singular.
+__device__ bool lane_solve(double *A, int n, double *B, int nrhs) {
+  for (int k = 0; k < n; k++) {
+    int p = k;
+    double best = fabs(lm(A, n, k, k));
+    for (int i = k + 1; i < n; i++) {
+      const double v = fabs(lm(A, n, i, k));
+      if (v > best) {
+        best = v;
+        p = i;
+      }
+    }
+    if (!(best > 0.0)) return false;
+    if (p != k) {
+      for (int j = 0; j < n; j++) {
+        const double t = lm(A, n, k, j);
+        lm(A, n, k, j) = lm(A, n, p, j);
+        lm(A, n, p, j) = t;
+      }
+      for (int j = 0; j < nrhs; j++) {
+        const double t = lm(B, nrhs, k, j);
+        lm(B, nrhs, k, j) = lm(B, nrhs, p, j);
+        lm(B, nrhs, p, j) = t;
+      }
+    }
+    const double inv = 1.0 / lm(A, n, k, k);
+    for (int i = k + 1; i < n; i++) {
+      const double f = lm(A, n, i, k) * inv;
+      if (f == 0.0) continue;
+      for (int j = k; j < n; j++) lm(A, n, i, j) -= f * lm(A, n, k, j);
+      for (int j = 0; j < nrhs; j++) lm(B, nrhs, i, j) -= f * lm(B, nrhs, k, j);
+    }
+  }
+  for (int k = n - 1; k >= 0; k--) {
+    const double inv = 1.0 / lm(A, n, k, k);
+    for (int j = 0; j < nrhs; j++) {
+      double v = lm(B, nrhs, k, j);
+      for (int i = k + 1; i < n; i++) v -= lm(A, n, k, i) * lm(B, nrhs, i, j);
+      lm(B, nrhs, k, j) = v * inv;
+    }
+  }
+  return true;
+}
+
+// Jacobian dR/dx (10 x 10, lane-strided) at an evaluated point.
+__device__ void cp_jacobian(const Mat &mat, const CpPoint &pt, const double *M, double g, const NeoHooke &h,
+                            const double *gd, const double *dgd, double gdot, double *Jm) {
+  double t[9], Ce[9], CepM[9];
+  mm3(pt.Cep, M, CepM);
+  mm3tn(M, CepM, Ce);
+  const double gs = mat.gs0, g0 = mat.g0, c = pt.dt * mat.G0 / (gs - g0);
+  for (int r = 0; r < 10; r++)
+    for (int q = 0; q < 10; q++) lm(Jm, 10, r, q) = (r == q && r < 9) ? 1.0 : 0.0;
+  double dgdM[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < kSlip; a++) {
+    double P[9], Y[9], dtau[9];
+    schmid(pt.R, a, P);
+    ysym(mat, h, Ce, P, Y);
+    mm3(CepM, Y, t);
+#pragma unroll
+    for (int i = 0; i < 9; i++) dtau[i] = 2.0 * t[i];
+    const double sg = gd[a] < 0 ? -1.0 : 1.0;
+    const double cf = pt.dt * dgd[a], cg = pt.dt * (-gd[a] / (mat.m * g));
+    for (int i = 0; i < 9; i++) {
+      const double Pi = P[i];
+      for (int j = 0; j < 9; j++) lm(Jm, 10, i, j) += cf * Pi * dtau[j];
+      lm(Jm, 10, i, 9) += cg * Pi;
+    }
+#pragma unroll
+    for (int j = 0; j < 9; j++) dgdM[j] += sg * dgd[a] * dtau[j];
+  }
+  for (int j = 0; j < 9; j++) lm(Jm, 10, 9, j) = -c * (gs - g) * dgdM[j];
+  lm(Jm, 10, 9, 9) = 1.0 + c * gdot + c * (gs - g) * gdot / (mat.m * g);
+}
+
+struct CpArgs {
+  long nqp;
+  const double *F;        // 9*nqp (SoA)
+  const double *Rcp;      // 9*nelem (SoA, per element; qp -> element = qp / nqp_e)
+  int nqp_e;
+  long ne;
+  const double *state_n;  // 10*nqp SoA
+  double *state_np1;      // 10*nqp SoA
+  const double *guess;    // 10*nqp SoA (M0 9, g0) or nullptr
+  double *out;            // kCpOut*nqp SoA: M (UL) 9, dM/dF 81, g
+  int *iters;             // nqp or nullptr
+  unsigned *counter;
+  unsigned long long *status;
+  Mat mat;
+  double dt;
+};
+
+constexpr int kCpWarps = 2;  // warps per CTA of k_cp_update
+
+__global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
+  extern __shared__ double smem_cp[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *Jm = smem_cp + warp * (100 + 90) * 32 + lane;  // 10x10 Jacobian
+  double *Bm = Jm + 100 * 32;                            // 10x9 right-hand sides
+  const unsigned FULL = 0xffffffffu;
+  const long S = A.nqp;
+  const double tol = A.mat.tol;
+  long qp = -1;
+  bool done = false;
+  CpPoint pt;
+  double M[9], g = 0, Res[10], nr = 0, gd[kSlip], dgd[kSlip], gdot = 0, Fq[9], pFni[9];
+  int it = 0;
+  NeoHooke h;
+  for (;;) {
+    // refill lanes without a point (warp-aggregated tickets)
+    const unsigned need = __ballot_sync(FULL, qp < 0 && !done);
+    if (need) {
+      unsigned base = 0;
+      const int leader = __ffs(need) - 1;
+      if (lane == leader) base = atomicAdd(A.counter, (unsigned)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (qp < 0 && !done) {
+        const long cand = (long)base + __popc(need & ((1u << lane) - 1u));
+        if (cand < S) {
+          qp = cand;
+          // point set-up: trial Ce', rotation, initial guess, first residual
+          const long e = qp / A.nqp_e;
+#pragma unroll
+          for (int i = 0; i < 9; i++) {
+            Fq[i] = A.F[i * S + qp];
+            pt.R[i] = A.Rcp[i * A.ne + e];
+          }
+          double pFn[9];
+#pragma unroll
+          for (int i = 0; i < 9; i++) pFn[i] = A.state_n[i * S + qp];
+          pt.g_n = A.state_n[9 * S + qp];
+          pt.dt = A.dt;
+          inv3(pFn, pFni);
+          double Fe[9];
+          mm3(Fq, pFni, Fe);
+          mm3tn(Fe, Fe, pt.Cep);
+          if (A.guess) {
+#pragma unroll
+            for (int i = 0; i < 9; i++) M[i] = A.guess[i * S + qp];
+            g = A.guess[9 * S + qp];
+          } else {
+#pragma unroll
+            for (int i = 0; i < 9; i++) M[i] = (i % 4 == 0) ? 1.0 : 0.0;
+            g = pt.g_n;
+          }
+          it = 0;
+          if (cp_residual(A.mat, pt, M, g, Res, h, gd, dgd, gdot)) nr = cp_norm(Res, A.mat.g0);
+          else nr = 1e300;
+        } else {
+          done = true;
+        }
+      }
+    }
+    if (__all_sync(FULL, done)) break;
+    if (qp < 0) continue;
+    // one Newton step (or finish)
+    bool finish = !(nr > tol) || it >= A.mat.max_iter || !(nr < 1e299);
+    if (!finish) {
+      cp_jacobian(A.mat, pt, M, g, h, gd, dgd, gdot, Jm);
+      for (int i = 0; i < 10; i++) lm(Bm, 1, i, 0) = -Res[i];
+      if (!lane_solve(Jm, 10, Bm, 1)) {
+        nr = 1e300;
+        finish = true;
+      } else {
+        double dx[10];
+        for (int i = 0; i < 10; i++) dx[i] = lm(Bm, 1, i, 0);
+        double lam = 1.0, Mt[9], gt = g, nt = 1e300;
+        double Rt[10], gdt[kSlip], dgdt[kSlip], gdott = 0;
+        NeoHooke ht;
+        for (int ls = 0; ls < 8; ls++) {
+#pragma unroll
+          for (int i = 0; i < 9; i++) Mt[i] = M[i] + lam * dx[i];
+          gt = g + lam * dx[9];
+          if (cp_residual(A.mat, pt, Mt, gt, Rt, ht, gdt, dgdt, gdott)) {
+            nt = cp_norm(Rt, A.mat.g0);
+            if (nt < nr || ls == 7) break;
+          }
+          lam *= 0.5;
+        }
+#pragma unroll
+        for (int i = 0; i < 9; i++) M[i] = Mt[i];
+        g = gt;
+        nr = nt;
+        h = ht;
+        gdot = gdott;
+#pragma unroll
+        for (int i = 0; i < 10; i++) Res[i] = Rt[i];
+#pragma unroll
+        for (int a = 0; a < kSlip; a++) {
+          gd[a] = gdt[a];
+          dgd[a] = dgdt[a];
+        }
+        it++;
+      }
+    }
+    if (finish) {
+      const bool conv = nr <= tol;
+      if (!conv) atomicAdd(&A.status[1], 1ull);
+      // state at n+1: pF_{n+1} = M^-1 pF_n
+      double Mi[9], pFn[9], pFnp1[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) pFn[i] = A.state_n[i * S + qp];
+      const bool okM = inv3(M, Mi);
+      mm3(Mi, pFn, pFnp1);
+#pragma unroll
+      for (int i = 0; i < 9; i++) A.state_np1[i * S + qp] = okM ? pFnp1[i] : pFn[i];
+      A.state_np1[9 * S + qp] = g;
+#pragma unroll
+      for (int i = 0; i < 9; i++) A.out[i * S + qp] = M[i];
+      A.out[90 * S + qp] = g;
+#pragma unroll
+      for (int a = 0; a < kSlip; a++) A.out[(91 + a) * S + qp] = A.dt * gd[a];
+      if (A.iters) A.iters[qp] = it;
+      // consistent dM/dF = -J^-1 dR/dF
+      if (conv && okM) {
+        cp_jacobian(A.mat, pt, M, g, h, gd, dgd, gdot, Jm);
+        for (int i = 0; i < 90; i++) Bm[i * 32] = 0.0;
+        double Ce[9], t[9], W[9];
+        mm3(pt.Cep, M, t);
+        mm3tn(M, t, Ce);
+        mm3(pFni, M, W);
+        const double gs = A.mat.gs0, c = A.dt * A.mat.G0 / (gs - A.mat.g0);
+        for (int a = 0; a < kSlip; a++) {
+          double P[9], Y[9], t1[9], Z[9], dtF[9];
+          schmid(pt.R, a, P);
+          ysym(A.mat, h, Ce, P, Y);
+          mm3(W, Y, t1);
+          mm3nt(t1, W, Z);  // Z = pFn^-1 M Ysym M^T pFn^-T
+          mm3(Fq, Z, dtF);
+          const double sg = gd[a] < 0 ? -1.0 : 1.0;
+          const double cf = A.dt * dgd[a];
+          for (int i = 0; i < 9; i++)
+            for (int kl = 0; kl < 9; kl++) lm(Bm, 9, i, kl) -= cf * P[i] * 2.0 * dtF[kl];
+          for (int kl = 0; kl < 9; kl++) lm(Bm, 9, 9, kl) -= -c * (gs - g) * sg * dgd[a] * 2.0 * dtF[kl];
+        }
+        if (lane_solve(Jm, 10, Bm, 9)) {
+          for (int r = 0; r < 9; r++)
+            for (int q = 0; q < 9; q++) A.out[(9 + r * 9 + q) * S + qp] = lm(Bm, 9, r, q);
+        } else {
+          atomicAdd(&A.status[3], 1ull);
+          for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
+        }
+      } else {
+        for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
+      }
+      qp = -1;
+    }
+  }
+}
+
+inline size_t cp_update_smem() { return sizeof(double) * kCpWarps * (100 + 90) * 32; }
+
+}  // namespace pgb
+
+namespace pgb {
+
+// Deformation gradient per point of linear tets (constant gradients).
+__global__ void k_cp_F(const double *X, const double *unode, const int *conn, long nn, long ne,
+                       const double *F0, double *F, double *detJw, unsigned long long *status) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  int nd[4];
+  double x[4][3], u[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    nd[a] = conn[(long)a * ne + e];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      x[a][i] = X[i * nn + nd[a]];
+      u[a][i] = unode[i * nn + nd[a]];
+    }
+  }
+  double dX[9], dU[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      dX[i * 3 + c] = x[c + 1][i] - x[0][i];
+      dU[i * 3 + c] = u[c + 1][i] - u[0][i];
+    }
+  double dXi[9], Fe[9];
+  const double dJ = det3(dX);
+  bool ok = dJ > 0.0 && inv3(dX, dXi);
+  if (ok) {
+    mm3(dU, dXi, Fe);
+#pragma unroll
+    for (int i = 0; i < 9; i++) Fe[i] += (i % 4 == 0 ? 1.0 : 0.0) + (F0 ? F0[i] : 0.0);
+    ok = det3(Fe) > 0.0;
+  }
+  if (!ok) {
+    atomicAdd(&status[0], 1ull);
+#pragma unroll
+    for (int i = 0; i < 9; i++) Fe[i] = (i % 4 == 0 ? 1.0 : 0.0);
+  }
+#pragma unroll
+  for (int i = 0; i < 9; i++) F[i * ne + e] = Fe[i];
+  detJw[e] = ok ? dJ / 6.0 : 0.0;
+}
+
+struct CpElemArgs {
+  const double *X;
+  const int *conn;
+  const int *dof, *rowptr0, *rowlen;
+  const uint8_t *mask;
+  const uint16_t *pos;  // element -> CSR node-block map
+  long nn, ne;
+  const double *F, *detJw;
+  const double *state_n;
+  const double *out;  // kCpOut * ne
+  double *R, *K;
+  Mat mat;
+};
+
+// Element residual and tangent of the CM 1-field element with plasticity
+// (compute_residual_vector / compute_stiffness_matrix,
+// src/constitutive_model.cc:1520-1662, with M = pF_{n+1}^-1 and dM/du),
+// written through the first Piola stress P = pJ F M S M^T of the element:
+// R_a = w P grad N_a and dR_a/du = w dP grad N_a.
+__global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= A.ne) return;
+  const long S = A.ne;
+  const double w = A.detJw[e];
+  if (!(w > 0.0)) return;
+  int nd[4];
+  double x[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    nd[a] = A.conn[(long)a * A.ne + e];
+#pragma unroll
+    for (int i = 0; i < 3; i++) x[a][i] = A.X[i * A.nn + nd[a]];
+  }
+  double dX[9], dXi[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) dX[i * 3 + c] = x[c + 1][i] - x[0][i];
+  inv3(dX, dXi);
+  double gN[4][3];  // grad_X N_a = dXi^T dN/dxi
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    gN[1][j] = dXi[0 * 3 + j];
+    gN[2][j] = dXi[1 * 3 + j];
+    gN[3][j] = dXi[2 * 3 + j];
+    gN[0][j] = -(gN[1][j] + gN[2][j] + gN[3][j]);
+  }
+  double F[9], Mu[9], pFn[9], pFni[9], M[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    F[i] = A.F[i * S + e];
+    Mu[i] = A.out[i * S + e];
+    pFn[i] = A.state_n[i * S + e];
+  }
+  inv3(pFn, pFni);
+  mm3(pFni, Mu, M);  // M_TL = pF_{n+1}^-1
+  double C[9], t[9], Ce[9];
+  mm3tn(F, F, C);
+  mm3(C, M, t);
+  mm3tn(M, t, Ce);
+  NeoHooke h;
+  if (!nh_stress(A.mat, Ce, h)) return;
+  const double pJ = det3(pFn) / det3(Mu);
+  double Mi[9];
+  inv3(M, Mi);
+  double FM[9], FMS[9], Pk[9];
+  mm3(F, M, FM);
+  mm3(FM, h.S, FMS);
+  mm3nt(FMS, M, Pk);  // F M S M^T
+  // residual
+  double Re[12];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      Re[a * 3 + i] = w * pJ * (Pk[i * 3] * gN[a][0] + Pk[i * 3 + 1] * gN[a][1] + Pk[i * 3 + 2] * gN[a][2]);
+  const unsigned mk[4] = {A.mask[nd[0]], A.mask[nd[1]], A.mask[nd[2]], A.mask[nd[3]]};
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int id = A.dof[i * A.nn + nd[a]];
+      if (id > 0) atomicAdd(A.R + (id - 1), Re[a * 3 + i]);
+    }
+  // tangent columns (node wn, component gc)
+  for (int wn = 0; wn < 4; wn++) {
+    if (!mk[wn]) continue;
+    for (int gc = 0; gc < 3; gc++) {
+      if (!((mk[wn] >> gc) & 1u)) continue;
+      double dMu[9], dM[9];
+#pragma unroll
+      for (int ij = 0; ij < 9; ij++)
+        dMu[ij] = A.out[(9 + ij * 9 + gc * 3 + 0) * S + e] * gN[wn][0] +
+                  A.out[(9 + ij * 9 + gc * 3 + 1) * S + e] * gN[wn][1] +
+                  A.out[(9 + ij * 9 + gc * 3 + 2) * S + e] * gN[wn][2];
+      mm3(pFni, dMu, dM);
+      double dF[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) dF[i] = 0.0;
+      dF[gc * 3 + 0] = gN[wn][0];
+      dF[gc * 3 + 1] = gN[wn][1];
+      dF[gc * 3 + 2] = gN[wn][2];
+      // dCe = dM^T C M + M^T (dF^T F + F^T dF) M + M^T C dM
+      double dC[9], a1[9], a2[9], dCe[9], CM[9], CdM[9];
+      mm3tn(dF, F, a1);
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) dC[i * 3 + j] = a1[i * 3 + j] + a1[j * 3 + i];
+      mm3(C, M, CM);
+      mm3(C, dM, CdM);
+      mm3(dC, M, a1);
+      mm3tn(M, a1, a2);  // M^T dC M
+      double b1[9];
+      mm3tn(M, CdM, b1);  // M^T C dM
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) dCe[i * 3 + j] = a2[i * 3 + j] + b1[i * 3 + j] + b1[j * 3 + i];
+      double dS[9];
+      nh_dS(A.mat, h, dCe, dS);
+      // dP/pJ = dF M S M^T + F dM S M^T + F M dS M^T + F M S dM^T - tr(M^-1 dM) F M S M^T
+      double q1[9], q2[9], q3[9], dP[9], tmp[9];
+      mm3(dF, M, tmp);
+      mm3(tmp, h.S, q1);
+      mm3nt(q1, M, dP);
+      mm3(F, dM, tmp);
+      mm3(tmp, h.S, q2);
+      mm3nt(q2, M, q3);
+#pragma unroll
+      for (int i = 0; i < 9; i++) dP[i] += q3[i];
+      mm3(FM, dS, q1);
+      mm3nt(q1, M, q3);
+#pragma unroll
+      for (int i = 0; i < 9; i++) dP[i] += q3[i];
+      mm3nt(FMS, dM, q3);
+      double trMdM = 0;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) trMdM += Mi[i * 3 + k] * dM[k * 3 + i];
+#pragma unroll
+      for (int i = 0; i < 9; i++) dP[i] = w * pJ * (dP[i] + q3[i] - trMdM * Pk[i]);
+      // scatter the column into the rows of the element's nodes
+      const long pcol = (e * 4 + 0) * 4 + wn;  // pos of (a, wn) at (e*4 + a)*4 + wn
+      for (int a = 0; a < 4; a++) {
+        if (!mk[a]) continue;
+        const long base = (long)A.rowptr0[nd[a]] + A.pos[pcol + a * 4] + rank_of(mk[wn], gc);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          if (!((mk[a] >> i) & 1u)) continue;
+          const double v = dP[i * 3] * gN[a][0] + dP[i * 3 + 1] * gN[a][1] + dP[i * 3 + 2] * gN[a][2];
+          atomicAdd(A.K + base + (long)rank_of(mk[a], i) * A.rowlen[nd[a]], v);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace pgb

@@ -22,6 +22,7 @@
 #include "tile_plan.hpp"
 #include "assemble_tiles.cuh"
 #include "cm_integrate.cuh"
+#include "cp_kernels.cuh"
 #include "peak_probe.cuh"
 #include "pgfem_gpu.h"
 
@@ -68,6 +69,11 @@ struct pgfem_gpu_ctx {
   unsigned *t_flags = nullptr, *t_ticket = nullptr;
   unsigned epoch = 0;
   double *qrec = nullptr;  // point records (kQRec x nqp)
+  // crystal plasticity
+  double *cp_R = nullptr, *cp_F = nullptr, *cp_detJw = nullptr, *cp_out = nullptr, *cp_guess = nullptr;
+  int *cp_iters = nullptr;
+  unsigned *cp_counter = nullptr;
+  bool cp_use_guess = false;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -233,7 +239,8 @@ void release(pgfem_gpu_ctx *c) {
   void *ptrs[] = {c->X, c->conn, c->dof, c->rowptr0, c->rowlen, c->mask, c->pos, c->unode, c->F0,
                   c->state_n, c->state_np1, c->status, c->d_u, c->d_presc, c->d_R, c->d_K,
                   c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
-                  c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree};
+                  c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree,
+                  c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -380,10 +387,83 @@ int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t
   return PGFEM_GPU_EINVAL;
 }
 
+int ensure_K_scratch(pgfem_gpu_ctx *c) {
+  if (c->d_K) return PGFEM_GPU_OK;
+  return dalloc(c, &c->d_K, std::max<long>(1, c->nnz));
+}
+
+int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStream_t s) {
+  k_cp_F<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(c->X, c->unode, c->conn, c->nn, c->ne, c->F0, c->cp_F,
+                                                          c->cp_detJw, c->status);
+  CK(cudaGetLastError());
+  CK(cudaMemsetAsync(c->cp_counter, 0, sizeof(unsigned), s));
+  CpArgs a{};
+  a.nqp = c->nqp;
+  a.F = c->cp_F;
+  a.Rcp = c->cp_R;
+  a.nqp_e = 1;
+  a.ne = c->ne;
+  a.state_n = c->state_n;
+  a.state_np1 = c->state_np1;
+  a.guess = c->cp_use_guess ? c->cp_guess : nullptr;
+  a.out = c->cp_out;
+  a.iters = c->cp_iters;
+  a.counter = c->cp_counter;
+  a.status = c->status;
+  a.mat = c->mat;
+  a.dt = dt;
+  const size_t smem = cp_update_smem();
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_cp_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cp_update, 32 * kCpWarps, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long need = (c->nqp + 32 * kCpWarps - 1) / (32 * kCpWarps);
+  const long grid = std::max<long>(1, std::min<long>(need, (long)g_num_sms * per_sm));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->timing && c->events.size() < 4096) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+  }
+  k_cp_update<<<(unsigned)grid, 32 * kCpWarps, smem, s>>>(a);
+  CK(cudaGetLastError());
+  if (e0) {
+    CK(cudaEventRecord(e1, s));
+    c->events.emplace_back(e0, e1);
+  }
+  if (d_K || d_R) {
+    CpElemArgs b{};
+    b.X = c->X;
+    b.conn = c->conn;
+    b.dof = c->dof;
+    b.rowptr0 = c->rowptr0;
+    b.rowlen = c->rowlen;
+    b.mask = c->mask;
+    b.pos = c->pos;
+    b.nn = c->nn;
+    b.ne = c->ne;
+    b.F = c->cp_F;
+    b.detJw = c->cp_detJw;
+    b.state_n = c->state_n;
+    b.out = c->cp_out;
+    b.R = d_R;
+    b.K = d_K;
+    b.mat = c->mat;
+    if (!d_K) return PGFEM_GPU_EINVAL;
+    k_cp_element<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(b);
+    CK(cudaGetLastError());
+  }
+  return PGFEM_GPU_OK;
+}
+
 // One assembly on device buffers (zeroing R and K first).
 int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
-                    double *d_K, cudaStream_t s) {
-  if (c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+                    double *d_K, cudaStream_t s, double dt = 0.0) {
   const bool use_tiles = c->tiles && d_K && c->scatter_mode == PGFEM_SCATTER_TILES;
   if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
   if (d_K && !(use_tiles && c->tile_zero_mode)) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
@@ -391,6 +471,15 @@ int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, 
     const long n3 = 3 * c->nn;
     k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
     CK(cudaGetLastError());
+  }
+  if (c->model == PGFEM_MODEL_CP) {
+    if (!d_K) {  // residual only: the tangent columns are skipped by a scratch K
+      int r = ensure_K_scratch(c);
+      if (r) return r;
+      CK(cudaMemsetAsync(c->d_K, 0, sizeof(double) * c->nnz, s));
+      return assemble_cp(c, d_R, c->d_K, dt, s);
+    }
+    return assemble_cp(c, d_R, d_K, dt, s);
   }
   AsmArgs a = base_args(c);
   a.R = d_R;
@@ -481,6 +570,9 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
       m->nn <= 0 || m->ne <= 0 || nrows != m->ndof || !Ap || !Ai)
     return PGFEM_GPU_EINVAL;
   if (mat->model < 0 || mat->model > 2) return PGFEM_GPU_EINVAL;
+  if (mat->model == PGFEM_MODEL_CP && (m->nne != 4 || !m->R_cp || !(mat->m > 0) || !(mat->g0 > 0) ||
+                                       !(mat->gs_0 > mat->g0)))
+    return PGFEM_GPU_EINVAL;
   if (m->nn > 0x7fffffffL || m->ne > 0x7fffffffL) return PGFEM_GPU_ELIMIT;
   int r = check_device();
   if (r) return r;
@@ -581,6 +673,17 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if (ce != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
     if (herr) return fail(PGFEM_GPU_EPATTERN);
   }
+  // crystal plasticity buffers (rotations SoA, F, point outputs)
+  if (c->model == PGFEM_MODEL_CP) {
+    std::vector<double> Rs((size_t)9 * ne);
+    for (long e = 0; e < ne; e++)
+      for (int i = 0; i < 9; i++) Rs[(size_t)i * ne + e] = m->R_cp[e * 9 + i];
+    if ((r = upload(c, &c->cp_R, Rs.data(), Rs.size())) || (r = dalloc(c, &c->cp_F, (size_t)9 * ne)) ||
+        (r = dalloc(c, &c->cp_detJw, ne)) || (r = dalloc(c, &c->cp_out, (size_t)kCpOut * c->nqp)) ||
+        (r = dalloc(c, &c->cp_iters, c->nqp)) || (r = dalloc(c, &c->cp_counter, 1)))
+      return fail(r);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
+  }
   // tiled assembly plan (HE / J2)
   if (c->model != PGFEM_MODEL_CP && !getenv("PGFEM_GPU_NO_TILES")) {
     std::vector<int> first_dof(nn, -1);
@@ -660,9 +763,42 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
+  if (c->model == PGFEM_MODEL_CP) return 4;  // u expansion, F, local Newton, element
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
+}
+
+int pgfem_gpu_set_cp_guess(pgfem_gpu_ctx *c, const double *guess) {
+  if (!c || c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  if (!guess) {
+    c->cp_use_guess = false;
+    return PGFEM_GPU_OK;
+  }
+  int r;
+  if (!c->cp_guess && (r = dalloc(c, &c->cp_guess, (size_t)10 * c->nqp))) return r;
+  std::vector<double> soa((size_t)10 * c->nqp);
+  for (long q = 0; q < c->nqp; q++)
+    for (int k = 0; k < 10; k++) soa[(size_t)k * c->nqp + q] = guess[q * 10 + k];
+  CK(cudaMemcpyAsync(c->cp_guess, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->cp_use_guess = true;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_get_cp_iterations(pgfem_gpu_ctx *c, int *iters, double *dgam) {
+  if (!c || c->model != PGFEM_MODEL_CP || !iters) return PGFEM_GPU_EINVAL;
+  CK(cudaMemcpyAsync(iters, c->cp_iters, sizeof(int) * c->nqp, cudaMemcpyDeviceToHost, c->stream));
+  if (dgam) {
+    std::vector<double> soa((size_t)12 * c->nqp);
+    CK(cudaMemcpyAsync(soa.data(), c->cp_out + (size_t)91 * c->nqp, soa.size() * sizeof(double),
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long q = 0; q < c->nqp; q++)
+      for (int a = 0; a < 12; a++) dgam[q * 12 + a] = soa[(size_t)a * c->nqp + q];
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
 }
 
 int pgfem_gpu_set_timing(pgfem_gpu_ctx *c, int on) {
@@ -763,7 +899,7 @@ static int ensure_scratch(pgfem_gpu_ctx *c, bool wantK) {
 }
 
 static int assemble_host(pgfem_gpu_ctx *c, const double *u, const double *presc, double *R,
-                         double *K, pgfem_gpu_status *st) {
+                         double *K, pgfem_gpu_status *st, double dt) {
   if (!c || !u || !R || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
   int r = ensure_scratch(c, K != nullptr);
   if (r) return r;
@@ -771,7 +907,7 @@ static int assemble_host(pgfem_gpu_ctx *c, const double *u, const double *presc,
   if (c->npres)
     CK(cudaMemcpyAsync(c->d_presc, presc, sizeof(double) * c->npres, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream));
-  r = assemble_device(c, c->d_u, c->npres ? c->d_presc : nullptr, c->d_R, K ? c->d_K : nullptr, c->stream);
+  r = assemble_device(c, c->d_u, c->npres ? c->d_presc : nullptr, c->d_R, K ? c->d_K : nullptr, c->stream, dt);
   if (r) return r;
   CK(cudaMemcpyAsync(R, c->d_R, sizeof(double) * c->ndof, cudaMemcpyDeviceToHost, c->stream));
   if (K) CK(cudaMemcpyAsync(K, c->d_K, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost, c->stream));
@@ -780,22 +916,19 @@ static int assemble_host(pgfem_gpu_ctx *c, const double *u, const double *presc,
 
 int pgfem_gpu_assemble_R(pgfem_gpu_ctx *c, const double *u, const double *presc, double dt,
                          double *R, pgfem_gpu_status *st) {
-  (void)dt;
-  return assemble_host(c, u, presc, R, nullptr, st);
+  return assemble_host(c, u, presc, R, nullptr, st, dt);
 }
 
 int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *c, const double *u, const double *presc, double dt,
                           double *R, double *K, pgfem_gpu_status *st) {
-  (void)dt;
   if (!K) return PGFEM_GPU_EINVAL;
-  return assemble_host(c, u, presc, R, K, st);
+  return assemble_host(c, u, presc, R, K, st, dt);
 }
 
 int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc,
                                  double dt, double *d_R, double *d_K, void *stream) {
-  (void)dt;
   if (!c || !d_u || !d_R || !d_K) return PGFEM_GPU_EINVAL;
-  return assemble_device(c, d_u, d_presc, d_R, d_K, (cudaStream_t)stream);
+  return assemble_device(c, d_u, d_presc, d_R, d_K, (cudaStream_t)stream, dt);
 }
 
 int pgfem_gpu_read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, int clear) {

@@ -86,6 +86,8 @@ def lib():
             "pgfem_gpu_set_timing": (C.c_int, [_P, C.c_int]),
             "pgfem_gpu_kernel_time": (C.c_int, [_P, _P, _P, C.c_int]),
             "pgfem_gpu_fp64_peak": (C.c_int, [_P]),
+            "pgfem_gpu_set_cp_guess": (C.c_int, [_P, _P]),
+            "pgfem_gpu_get_cp_iterations": (C.c_int, [_P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -259,6 +261,16 @@ class Context:
         n = C.c_long()
         _check("pgfem_gpu_kernel_time", lib().pgfem_gpu_kernel_time(self.h, C.byref(ms), C.byref(n), int(reset)))
         return ms.value, n.value
+
+    def set_cp_guess(self, guess):
+        g = None if guess is None else np.ascontiguousarray(guess, dtype=np.float64)
+        _check("pgfem_gpu_set_cp_guess", lib().pgfem_gpu_set_cp_guess(self.h, _ptr(g)))
+
+    def cp_iterations(self, want_slip=False):
+        it = np.zeros(self.ne * self.nint, dtype=np.int32)
+        dg = np.zeros((self.ne * self.nint, 12)) if want_slip else None
+        _check("pgfem_gpu_get_cp_iterations", lib().pgfem_gpu_get_cp_iterations(self.h, _ptr(it), _ptr(dg)))
+        return (it, dg) if want_slip else it
 
     def read_status(self, clear=False):
         st = Status()

@@ -136,3 +136,92 @@ def j2_p2(n=64, seed=1, stretch=None, perturb=1e-4, max_cells_z=None):
     state[:, [0, 4, 8]] = 1.0
     return Problem("j2_p2_n%d" % n, X, conn, ids, ndof, Ap, Ai, mat, u, state=state,
                    meta=dict(n=n, seed=seed, stretch=eps))
+
+
+# ----------------------------------------------------------------------------
+# crystal plasticity
+# ----------------------------------------------------------------------------
+CP_STEPS = 20  # load steps of the 1 % tension ramp
+CP_DT = 0.1
+
+
+def quat_to_rot(q):
+    """Rotation matrices (n,3,3) from unit quaternions (n,4) = (x, y, z, w)."""
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    R = np.empty((len(q), 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def shoemake_quaternions(seed, n):
+    """Uniform random rotations (Shoemake 1992) as unit quaternions."""
+    u = splitmix64(seed, 3 * n, stream=7).reshape(n, 3)
+    a, b = np.sqrt(1 - u[:, 0]), np.sqrt(u[:, 0])
+    t1, t2 = 2 * np.pi * u[:, 1], 2 * np.pi * u[:, 2]
+    return np.stack([a * np.sin(t1), a * np.cos(t1), b * np.sin(t2), b * np.cos(t2)], axis=1)
+
+
+def voronoi_grains(centroids, seed, ngrains):
+    """Grain id of each point: nearest of ngrains seeded uniform centres."""
+    c = splitmix64(seed, 3 * ngrains, stream=5).reshape(ngrains, 3)
+    gid = np.empty(len(centroids), dtype=np.int64)
+    for s in range(0, len(centroids), 65536):
+        d = ((centroids[s:s + 65536, None, :] - c[None, :, :]) ** 2).sum(-1)
+        gid[s:s + 65536] = d.argmin(1)
+    return gid
+
+
+def cp_material(max_iter=25, tol=1e-10):
+    return pg.material(pg.MODEL_CP, E=200e3, nu=0.3, gamma_dot_0=1e-3, m=0.05, G0=200.0, g0=60.0, gs_0=250.0,
+                       gamma_dot_s=1.0, w=0.0, cp_tol=tol, cp_max_iter=max_iter)
+
+
+class CpProblem(Problem):
+    """Config-3 style problem: the load ramp u(s) = s/CP_STEPS * u_final."""
+
+    def displacement(self, step):
+        return self.u_final * (step / CP_STEPS)
+
+
+def cp_p1(n=48, seed=2, ngrains=512, perturb=1e-4):
+    X, conn, Pr = pg.mesh_box_tet(n, 4)
+    nn = X.shape[0]
+    h = 1.0 / n
+    codes = np.zeros((nn, 3), dtype=np.int64)
+    ids, ndof = pg.generate_dof_ids(conn, nn, codes)
+    Ap, Ai = pg.psparse_apai(conn, ids, ndof)
+    cen = X[conn].mean(axis=1)
+    gid = voronoi_grains(cen, seed, ngrains)
+    Rg = quat_to_rot(shoemake_quaternions(seed, ngrains))
+    R_cp = np.ascontiguousarray(Rg[gid].reshape(-1, 9))
+    r = splitmix64(seed, nn * 3).reshape(nn, 3)
+    disp = (2.0 * r - 1.0) * perturb * h
+    disp[:, 0] += 0.01 * X[:, 0]
+    u_final = nodal_to_free(ids, disp)
+    state = np.zeros((conn.shape[0], 10))
+    state[:, [0, 4, 8]] = 1.0
+    state[:, 9] = 60.0
+    p = CpProblem("cp_p1_n%d" % n, X, conn, ids, ndof, Ap, Ai, cp_material(), u_final.copy(), state=state,
+                  R_cp=R_cp, dt=CP_DT, meta=dict(n=n, seed=seed, ngrains=ngrains))
+    p.u_final = u_final
+    p.grain = gid
+    p.quat = shoemake_quaternions(seed, ngrains)[gid]
+    return p
+
+
+def fcc_slip_systems():
+    """FCC {111}<110> slip directions s and normals n (unit, crystal frame), 12 x 3 each."""
+    N = np.array([[1, 1, 1], [-1, 1, 1], [1, -1, 1], [1, 1, -1]], dtype=float) / np.sqrt(3.0)
+    D = np.array([[[0, 1, -1], [1, 0, -1], [1, -1, 0]], [[0, 1, -1], [1, 0, 1], [1, 1, 0]],
+                  [[0, 1, 1], [1, 0, -1], [1, 1, 0]], [[0, 1, 1], [1, 0, 1], [1, -1, 0]]], dtype=float) / np.sqrt(2.0)
+    s = D.reshape(12, 3)
+    n = np.repeat(N, 3, axis=0)
+    return s, n

@@ -130,3 +130,80 @@ def test_he_stiffness_symmetric():
     err, fe, lk, _ = P.element(mat, 5, elem_u(p, 5, p.u))
     assert err == 0
     assert np.abs(lk - lk.T).max() <= 1e-10 * np.abs(lk).max()
+
+
+def test_cp_tangent_matches_central_differences():
+    p = wl.cp_p1(n=3, seed=2, ngrains=4)
+    P, mat = oracle.from_workload(p)
+    st = p.state.copy()
+    for s in range(1, 5):  # load to a plastic state
+        err, R, K, st = P.assemble(mat, p.displacement(s), state_n=st, dt=p.dt)
+        assert err == 0
+    u = p.displacement(5)
+    for e in (1, 40, 100):
+        ue = elem_u(p, e, u)
+        err, fe, lk, _ = P.element(mat, e, ue, st[e], dt=p.dt)
+        assert err == 0
+        h = 1e-8
+        fd = np.zeros_like(lk)
+        for k in range(12):
+            up, um = ue.copy(), ue.copy()
+            up[k] += h
+            um[k] -= h
+            _, fp, _, _ = P.element(mat, e, up, st[e], dt=p.dt, want_K=False)
+            _, fm, _, _ = P.element(mat, e, um, st[e], dt=p.dt, want_K=False)
+            fd[:, k] = (fp - fm) / (2 * h)
+        assert np.linalg.norm(fd - lk) <= 1e-6 * np.linalg.norm(lk)
+
+
+def test_cp_local_newton_converges_with_uneven_iterations():
+    p = wl.cp_p1(n=3, seed=2, ngrains=4)
+    mat = oracle.from_pg_material(p.mat)
+    st = p.state.copy()
+    seen = set()
+    for s in range(1, 6):
+        F = p1_deformation_gradients(p, p.displacement(s))
+        bad, st, it, dg, cv = oracle.cp_update_batch(mat, F, st, p.dt, p.R_cp)
+        assert bad == 0 and cv.all()
+        seen |= set(np.unique(it).tolist())
+    assert max(seen) - min(seen) >= 5
+
+
+def test_cp_warm_start_from_converged_increment_needs_no_iterations():
+    p = wl.cp_p1(n=3, seed=2, ngrains=4)
+    mat = oracle.from_pg_material(p.mat)
+    st = p.state.copy()
+    F = p1_deformation_gradients(p, p.displacement(1))
+    _, st, _, _, _ = oracle.cp_update_batch(mat, F, st, p.dt, p.R_cp)
+    F = p1_deformation_gradients(p, p.displacement(2))
+    _, s_cold, it_cold, dg, _ = oracle.cp_update_batch(mat, F, st, p.dt, p.R_cp)
+    M0 = cp_guess_from_slip(p, dg)
+    _, s_warm, it_warm, _, cv = oracle.cp_update_batch(mat, F, st, p.dt, p.R_cp, M0=M0[:, :9], g_guess=M0[:, 9] * 0 + s_cold[:, 9])
+    assert cv.all()
+    assert it_warm.max() <= 2 and it_cold.mean() > it_warm.mean()
+    assert np.abs(s_warm - s_cold).max() <= 1e-9 * np.abs(s_cold).max()
+
+
+def p1_deformation_gradients(p, u):
+    """F per linear tet from a free-DOF displacement vector (numpy)."""
+    X = p.X[p.conn]
+    ue = np.zeros((p.ne, 4, 3))
+    for a in range(4):
+        for j in range(3):
+            i = p.ids[p.conn[:, a], j]
+            ue[:, a, j] = np.where(i > 0, u[i - 1], 0.0)
+    D = np.stack([X[:, 1] - X[:, 0], X[:, 2] - X[:, 0], X[:, 3] - X[:, 0]], axis=2)
+    dU = np.stack([ue[:, 1] - ue[:, 0], ue[:, 2] - ue[:, 0], ue[:, 3] - ue[:, 0]], axis=2)
+    F = np.eye(3)[None] + dU @ np.linalg.inv(D)
+    return F.reshape(-1, 9)
+
+
+def cp_guess_from_slip(p, dgam):
+    """Initial guess M0 = I - sum dgam_a P_a (and a g column placeholder) from slip increments."""
+    s, n = wl.fcc_slip_systems()
+    R = p.R_cp.reshape(-1, 3, 3)
+    rs = np.einsum("eij,aj->eai", R, s)
+    rn = np.einsum("eij,aj->eai", R, n)
+    P = np.einsum("eai,eaj->eaij", rs, rn)
+    M0 = np.eye(3)[None] - np.einsum("ea,eaij->eij", dgam, P)
+    return np.concatenate([M0.reshape(-1, 9), np.zeros((len(M0), 1))], axis=1)
