@@ -197,6 +197,34 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
                            const double *R_cp, const double *state_n, double *state_np1,
                            double *S, double *L, int *qp_status);
 
+/* ---- crystal plasticity point update that allocates nothing --------------
+ * No counterpart in the reference.  For callers that must not call
+ * cudaMalloc: code running under another framework's memory pool (the pool
+ * owns the device memory, so a raw allocation bypasses it or fails), work on
+ * a latency-critical path where cudaMalloc's implicit device-wide
+ * synchronisation is unacceptable, and hosts that forbid allocation after
+ * start-up.  The local Newton of the CP model (the same kernel the CP
+ * assembly runs) for nqp <= 4096 points on caller-owned DEVICE buffers, all
+ * component-major (SoA): d_F [9][nqp], d_R_cp [9][nqp] crystal rotations,
+ * d_state_n / d_state_np1 [10][nqp] (pF 9, g), optional d_dgam [12][nqp]
+ * slip increments dt*gamma_dot_a and d_iters [nqp] Newton iteration counts.
+ * Asynchronous on `stream` unless st != NULL, in which case the call waits
+ * for the stream and returns the failure counts.
+ * Its working memory (about 3.4 MB: per-point Newton record, ticket counter,
+ * failure counters) is one fixed array in the library's device image, held
+ * by every GPU that loads the library until the process exits; each call
+ * zeroes the counters it needs.  Consequences:
+ *  - nqp > 4096 returns PGFEM_GPU_ELIMIT (split larger batches);
+ *  - calls that overlap on the GPU (different streams or host threads on the
+ *    same device) share the array and race: order them on one stream;
+ *  - the first call on each device performs a one-time set-up (looks up the
+ *    array's device address, sets the kernel's shared-memory limit); make
+ *    that first call before any stream capture. */
+int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, const double *d_F,
+                                   const double *d_R_cp, const double *d_state_n, double dt,
+                                   double *d_state_np1, double *d_dgam, int *d_iters,
+                                   pgfem_gpu_status *st, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

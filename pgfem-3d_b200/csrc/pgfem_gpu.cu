@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "assemble.cuh"
@@ -1008,6 +1009,126 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
   if (r) return r;
   if (nqp == 0) return PGFEM_GPU_OK;
   return cm_integrate_host(make_mat(mat), nqp, F, dt, state_n, state_np1, S, L, qp_status);
+}
+
+}  // extern "C"
+
+// ---- crystal plasticity point update without device allocation ------------
+//
+// For callers that may not call cudaMalloc: code that runs inside another
+// framework's memory pool (the pool owns the device memory and a raw
+// cudaMalloc would bypass its accounting or fail), callbacks on a time-
+// critical path where cudaMalloc's implicit device synchronisation is not
+// acceptable, and host runtimes whose policy forbids allocation after start-
+// up.  The caller owns every input and output; the work record of the local
+// Newton (M, dM/dF, g, slip increments per point), the work-stealing ticket
+// counter and the failure counters live in the file-scope array below, which
+// every GPU that loads this library holds until the process exits.
+//
+// Host code must not pass `pgfem_cp_scratch` itself to a kernel: on the host
+// that name is only a stand-in for the device array.  The device address is
+// taken with cudaGetSymbolAddress once per device, with that device current.
+
+#define PGFEM_CP_NOALLOC_MAX_POINTS 4096L
+namespace {
+constexpr long kNaHeader = 32;  // doubles: ticket counter (word 0), 4 failure counters (words 1-4), pad to 256 B
+constexpr long kNaWords = kNaHeader + (long)pgb::kCpOut * PGFEM_CP_NOALLOC_MAX_POINTS;
+}  // namespace
+static __device__ __align__(256) double pgfem_cp_scratch[kNaWords];
+
+namespace {
+struct NaDevice {
+  double *scratch = nullptr;  // device address of pgfem_cp_scratch on this device
+  int grid_cap = 0;           // SMs x resident CTAs of k_cp_update
+  bool ready = false;
+};
+constexpr int kNaMaxDevices = 64;
+NaDevice g_na[kNaMaxDevices];
+std::mutex g_na_mu;
+
+// One-time set-up on the current device: the scratch address, the dynamic
+// shared-memory opt-in of k_cp_update and its persistent grid size.
+int noalloc_setup(int dev, NaDevice **out) {
+  std::lock_guard<std::mutex> lk(g_na_mu);
+  NaDevice &d = g_na[dev];
+  if (!d.ready) {
+    void *p = nullptr;
+    CK(cudaGetSymbolAddress(&p, pgfem_cp_scratch));
+    if (!p || ((uintptr_t)p & 255u)) return PGFEM_GPU_ECUDA;
+    const size_t smem = pgb::cp_update_smem();
+    CK(cudaFuncSetAttribute(pgb::k_cp_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0, sms = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pgb::k_cp_update, 32 * pgb::kCpWarps, smem));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    d.scratch = (double *)p;
+    d.grid_cap = std::max(1, per_sm) * std::max(1, sms);
+    d.ready = true;
+  }
+  *out = &d;
+  return PGFEM_GPU_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, const double *d_F,
+                                   const double *d_R_cp, const double *d_state_n, double dt,
+                                   double *d_state_np1, double *d_dgam, int *d_iters,
+                                   pgfem_gpu_status *st, void *stream) {
+  if (!mat || nqp < 0 || (nqp && (!d_F || !d_R_cp || !d_state_n || !d_state_np1))) return PGFEM_GPU_EINVAL;
+  if (mat->model != PGFEM_MODEL_CP || !(mat->m > 0) || !(mat->g0 > 0) || !(mat->gs_0 > mat->g0))
+    return PGFEM_GPU_EINVAL;
+  if (nqp > PGFEM_CP_NOALLOC_MAX_POINTS) {
+    std::fprintf(stderr,
+                 "pgfem_gpu_cp_integrate_noalloc: %ld points exceed the fixed maximum of %ld per call; "
+                 "split the batch\n",
+                 nqp, PGFEM_CP_NOALLOC_MAX_POINTS);
+    return PGFEM_GPU_ELIMIT;
+  }
+  int r = check_device();
+  if (r) return r;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNaMaxDevices) return PGFEM_GPU_ENODEV;
+  NaDevice *d = nullptr;
+  if ((r = noalloc_setup(dev, &d))) return r;
+  if (st) *st = pgfem_gpu_status{};
+  if (nqp == 0) return PGFEM_GPU_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  // the ticket counter and the failure counters must start at zero; the work
+  // record is written in full for every point before it is read
+  CK(cudaMemsetAsync(d->scratch, 0, sizeof(double) * kNaHeader, s));
+  pgb::CpArgs a{};
+  a.nqp = nqp;
+  a.F = d_F;
+  a.Rcp = d_R_cp;
+  a.nqp_e = 1;
+  a.ne = nqp;
+  a.state_n = d_state_n;
+  a.state_np1 = d_state_np1;
+  a.guess = nullptr;
+  a.out = d->scratch + kNaHeader;
+  a.iters = d_iters;
+  a.counter = (unsigned *)d->scratch;
+  a.status = (unsigned long long *)(d->scratch + 1);
+  a.mat = make_mat(mat);
+  a.dt = dt;
+  const long need = (nqp + 32 * pgb::kCpWarps - 1) / (32 * pgb::kCpWarps);
+  const long grid = std::max<long>(1, std::min<long>(need, d->grid_cap));
+  pgb::k_cp_update<<<(unsigned)grid, 32 * pgb::kCpWarps, pgb::cp_update_smem(), s>>>(a);
+  CK(cudaGetLastError());
+  if (d_dgam)  // slip increments dt*gamma_dot_a: rows 91..102 of the work record, contiguous
+    CK(cudaMemcpyAsync(d_dgam, a.out + 91 * nqp, sizeof(double) * 12 * nqp, cudaMemcpyDeviceToDevice, s));
+  if (st) {
+    unsigned long long w[4];
+    CK(cudaMemcpyAsync(w, d->scratch + 1, sizeof(w), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    st->inverted = (long)w[0];
+    st->nonconverged = (long)w[1];
+    st->bad_diagonal = (long)w[2];
+    st->other = (long)w[3];
+  }
+  return PGFEM_GPU_OK;
 }
 
 }  // extern "C"

@@ -88,6 +88,8 @@ def lib():
             "pgfem_gpu_fp64_peak": (C.c_int, [_P]),
             "pgfem_gpu_set_cp_guess": (C.c_int, [_P, _P]),
             "pgfem_gpu_get_cp_iterations": (C.c_int, [_P, _P, _P]),
+            "pgfem_gpu_cp_integrate_noalloc": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_double, _P, _P, _P, _P,
+                                                         _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -317,3 +319,19 @@ def cm_integrate(mat, F, state_n=None, dt=0.0, want_L=True):
     _check("pgfem_gpu_cm_integrate", lib().pgfem_gpu_cm_integrate(
         C.byref(mat), nqp, _ptr(F), dt, None, _ptr(sn), _ptr(snp1), _ptr(S), _ptr(L), _ptr(qst)))
     return S, L, snp1, qst
+
+
+CP_NOALLOC_MAX_POINTS = 4096
+
+
+def cp_integrate_noalloc(mat, nqp, d_F, d_R_cp, d_state_n, dt, d_state_np1, d_dgam=None, d_iters=None,
+                         stream=None, want_status=True):
+    """CP point update on caller-owned device buffers (raw device addresses as ints,
+    component-major layouts) through pgfem_gpu_cp_integrate_noalloc, which allocates
+    no device memory.  Returns the failure counts (the call then waits for the
+    stream) or None when want_status is False (the call stays asynchronous)."""
+    st = Status() if want_status else None
+    _check("pgfem_gpu_cp_integrate_noalloc", lib().pgfem_gpu_cp_integrate_noalloc(
+        C.byref(mat), nqp, d_F, d_R_cp, d_state_n, dt, d_state_np1, d_dgam, d_iters,
+        C.byref(st) if st is not None else None, stream))
+    return st
