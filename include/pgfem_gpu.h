@@ -37,6 +37,7 @@ extern "C" {
 #define PGFEM_GPU_EPATTERN (-4) /* CSR pattern does not hold an element block */
 #define PGFEM_GPU_ENODEV (-5)   /* no usable sm_100 device */
 #define PGFEM_GPU_ELIMIT (-6)   /* size beyond a fixed limit of the entry point */
+#define PGFEM_GPU_ETIMEOUT (-7) /* a bounded device-side wait ran out (kernel returned early) */
 
 /* Constitutive models (the Model_parameters families on the path). */
 enum {
@@ -224,6 +225,42 @@ int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, con
                                    const double *d_R_cp, const double *d_state_n, double dt,
                                    double *d_state_np1, double *d_dgam, int *d_iters,
                                    pgfem_gpu_status *st, void *stream);
+
+/* ---- learned warm start of the CP local Newton ----------------------------
+ * No counterpart in the reference (its Newton starts from the elastic
+ * predictor, src/plasticity_model.cc:1148-1224).  A 34 -> 128 -> 128 -> 128
+ * (GELU) -> 12 network maps per-point features to the slip increments
+ * dt*gamma_dot_a; only the initial guess of the FP64 Newton is taken from it.
+ * Features (row of 34 FP32): F_{n+1} F_n^-1 - I (9), pF_n - I (9), the 12 slip
+ * resistances (g_n for every system of this model), lattice quaternion (4,
+ * w >= 0).  BF16 tensor-core (tcgen05) GEMMs, FP32 accumulation; trained on
+ * the GPU by the library's own fused forward/backward kernel and Adam.
+ * Parameter vector (FP32, 39,052): W1[128][34] b1 W2[128][128] b2 W3 b3
+ * W4[12][128] b4.  Device pointers are marked d_. */
+typedef struct pgfem_mlp pgfem_mlp;
+typedef struct {
+  int epochs, batch;        /* batch: samples per Adam step (>= 128) */
+  float lr, lr_min;         /* cosine decay from lr to lr_min over all steps */
+  float beta1, beta2, eps;  /* Adam */
+  unsigned long long seed;  /* shuffling */
+} pgfem_mlp_train_opts;
+long pgfem_mlp_num_params(void);
+int pgfem_mlp_create(unsigned long long seed, pgfem_mlp **m); /* Glorot-uniform weights, zero biases */
+int pgfem_mlp_destroy(pgfem_mlp *m);
+int pgfem_mlp_set_params(pgfem_mlp *m, const float *params);  /* host; resets the Adam moments */
+int pgfem_mlp_get_params(const pgfem_mlp *m, float *params);
+/* inputs are normalised as (x - x_mean) / x_std, outputs scaled by y_std */
+int pgfem_mlp_set_scaling(pgfem_mlp *m, const float *x_mean, const float *x_std, const float *y_std);
+int pgfem_mlp_get_scaling(const pgfem_mlp *m, float *x_mean, float *x_inv_std, float *y_std);
+/* scaling from data: feature mean / standard deviation, target RMS */
+int pgfem_mlp_fit_scaling(pgfem_mlp *m, long n, const float *d_x, const float *d_t);
+int pgfem_mlp_predict_device(pgfem_mlp *m, long n, const float *d_x, float *d_y, void *stream);
+int pgfem_mlp_predict(pgfem_mlp *m, long n, const float *x, float *y); /* host buffers */
+/* loss 1/(2n) sum |out - t/y_std|^2 over all n rows and its gradient (host buffers) */
+int pgfem_mlp_loss_grad(pgfem_mlp *m, long n, const float *x, const float *t, float *grad, double *loss);
+/* Adam over shuffled mini-batches of the n pairs; epoch_loss[epochs] (may be NULL) */
+int pgfem_mlp_train_device(pgfem_mlp *m, long n, const float *d_x, const float *d_t,
+                           const pgfem_mlp_train_opts *opts, double *epoch_loss);
 
 #ifdef __cplusplus
 }

@@ -15,7 +15,7 @@ LIB_PATH = os.path.join(HERE, "libpgfem_gpu.so")
 MODEL_HE, MODEL_J2, MODEL_CP = 0, 1, 2
 SCATTER_ATOMIC, SCATTER_COLOUR, SCATTER_TILES = 0, 1, 2
 
-ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT"}
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT", -7: "ETIMEOUT"}
 
 
 class PgfemError(RuntimeError):
@@ -90,6 +90,18 @@ def lib():
             "pgfem_gpu_get_cp_iterations": (C.c_int, [_P, _P, _P]),
             "pgfem_gpu_cp_integrate_noalloc": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_double, _P, _P, _P, _P,
                                                          _P]),
+            "pgfem_mlp_num_params": (C.c_long, []),
+            "pgfem_mlp_create": (C.c_int, [C.c_ulonglong, _P]),
+            "pgfem_mlp_destroy": (C.c_int, [_P]),
+            "pgfem_mlp_set_params": (C.c_int, [_P, _P]),
+            "pgfem_mlp_get_params": (C.c_int, [_P, _P]),
+            "pgfem_mlp_set_scaling": (C.c_int, [_P, _P, _P, _P]),
+            "pgfem_mlp_get_scaling": (C.c_int, [_P, _P, _P, _P]),
+            "pgfem_mlp_fit_scaling": (C.c_int, [_P, C.c_long, _P, _P]),
+            "pgfem_mlp_predict_device": (C.c_int, [_P, C.c_long, _P, _P, _P]),
+            "pgfem_mlp_predict": (C.c_int, [_P, C.c_long, _P, _P]),
+            "pgfem_mlp_loss_grad": (C.c_int, [_P, C.c_long, _P, _P, _P, _P]),
+            "pgfem_mlp_train_device": (C.c_int, [_P, C.c_long, _P, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -335,3 +347,78 @@ def cp_integrate_noalloc(mat, nqp, d_F, d_R_cp, d_state_n, dt, d_state_np1, d_dg
         C.byref(mat), nqp, d_F, d_R_cp, d_state_n, dt, d_state_np1, d_dgam, d_iters,
         C.byref(st) if st is not None else None, stream))
     return st
+
+
+# ------------------------------------------------------- warm-start network --
+MLP_IN, MLP_OUT = 34, 12
+
+
+class MlpTrainOpts(C.Structure):
+    _fields_ = [("epochs", C.c_int), ("batch", C.c_int), ("lr", C.c_float), ("lr_min", C.c_float),
+                ("beta1", C.c_float), ("beta2", C.c_float), ("eps", C.c_float), ("seed", C.c_ulonglong)]
+
+
+class Mlp:
+    """The warm-start network of the CP local Newton (pgfem_mlp_* entry points)."""
+
+    def __init__(self, seed=0):
+        h = C.c_void_p()
+        _check("pgfem_mlp_create", lib().pgfem_mlp_create(seed, C.byref(h)))
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pgfem_mlp_destroy(self.h)
+            self.h = None
+
+    @staticmethod
+    def num_params():
+        return lib().pgfem_mlp_num_params()
+
+    def params(self):
+        p = np.zeros(self.num_params(), dtype=np.float32)
+        _check("pgfem_mlp_get_params", lib().pgfem_mlp_get_params(self.h, _ptr(p)))
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.num_params()
+        _check("pgfem_mlp_set_params", lib().pgfem_mlp_set_params(self.h, _ptr(p)))
+
+    def set_scaling(self, x_mean, x_std, y_std):
+        a = [np.ascontiguousarray(v, dtype=np.float32) for v in (x_mean, x_std, y_std)]
+        _check("pgfem_mlp_set_scaling", lib().pgfem_mlp_set_scaling(self.h, *[_ptr(v) for v in a]))
+
+    def scaling(self):
+        xm, xi, ys = np.zeros(MLP_IN, np.float32), np.zeros(MLP_IN, np.float32), np.zeros(MLP_OUT, np.float32)
+        _check("pgfem_mlp_get_scaling", lib().pgfem_mlp_get_scaling(self.h, _ptr(xm), _ptr(xi), _ptr(ys)))
+        return xm, xi, ys
+
+    def fit_scaling(self, n, d_x, d_t):
+        _check("pgfem_mlp_fit_scaling", lib().pgfem_mlp_fit_scaling(self.h, n, d_x, d_t))
+
+    def predict(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        y = np.zeros((x.shape[0], MLP_OUT), dtype=np.float32)
+        _check("pgfem_mlp_predict", lib().pgfem_mlp_predict(self.h, x.shape[0], _ptr(x), _ptr(y)))
+        return y
+
+    def predict_device(self, n, d_x, d_y, stream=None):
+        _check("pgfem_mlp_predict_device", lib().pgfem_mlp_predict_device(self.h, n, d_x, d_y, stream))
+
+    def loss_grad(self, x, t):
+        x = np.ascontiguousarray(x, dtype=np.float32).reshape(-1, MLP_IN)
+        t = np.ascontiguousarray(t, dtype=np.float32).reshape(-1, MLP_OUT)
+        g = np.zeros(self.num_params(), dtype=np.float32)
+        loss = C.c_double()
+        _check("pgfem_mlp_loss_grad", lib().pgfem_mlp_loss_grad(self.h, x.shape[0], _ptr(x), _ptr(t), _ptr(g),
+                                                                C.byref(loss)))
+        return loss.value, g
+
+    def train_device(self, n, d_x, d_t, epochs=10, batch=4096, lr=2e-3, lr_min=5e-5, beta1=0.9, beta2=0.999,
+                     eps=1e-8, seed=0):
+        o = MlpTrainOpts(epochs, batch, lr, lr_min, beta1, beta2, eps, seed)
+        hist = np.zeros(max(epochs, 1))
+        _check("pgfem_mlp_train_device", lib().pgfem_mlp_train_device(self.h, n, d_x, d_t, C.byref(o),
+                                                                      _ptr(hist)))
+        return hist[:epochs]
