@@ -371,6 +371,113 @@ def run_cp(args, ws, rank, local):
     return out
 
 
+def run_cp_warm(args, ws, rank, local):
+    """Config 4: the config-3 local update started from the learned guess.  The
+    network is trained here, on the GPU, from plain-Newton pairs of 20 other
+    seeded meshes (seeds 100..119, 32^3 cells, one load step each); then the
+    same R+K iterate as config 3 is timed with the plain cold start and with
+    the warm start, both to the 1e-10 local residual."""
+    import torch
+
+    import pgfem_gpu as pg
+    import surrogate as sg
+    import workloads as wl
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    x, t, info = sg.generate_pairs(n=args.train_n)
+    net, hist, train_s = sg.train(x, t, seed=1, epochs=args.train_epochs, batch=8192, lr=2e-3, lr_min=2e-5)
+    del x, t
+    torch.cuda.empty_cache()
+    log("[rank %d] %d training pairs in %.1f s, trained in %.2f s, loss %.4f -> %.4f"
+        % (rank, info["pairs"], info["seconds"], train_s, hist[0], hist[-1]))
+    p = wl.cp_p1(n=args.cp_n, seed=2)
+    ctx = p.context()
+    for s in range(1, args.cp_step):
+        _, _, st = ctx.assemble_RK(p.displacement(s), dt=p.dt)
+        assert st.ok(), st.as_dict()
+        ctx.commit_state()
+    u = p.displacement(args.cp_step)
+    stream = torch.cuda.current_stream()
+    d_u = torch.from_numpy(u).to(dev)
+    d_R = torch.empty(p.ndof, dtype=torch.float64, device=dev)
+    d_K = torch.empty(p.nnz, dtype=torch.float64, device=dev)
+    sh = stream.cuda_stream
+
+    def step():
+        ctx.assemble_RK_device(d_u.data_ptr(), None, d_R.data_ptr(), d_K.data_ptr(), sh, dt=p.dt)
+
+    def timed():
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        st = ctx.read_status(clear=True)
+        assert st.ok(), st.as_dict()
+        ctx.set_timing(True)
+        ctx.kernel_time(reset=True)
+        barrier(ws)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = allreduce_max(e0.elapsed_time(e1), ws)
+        kms, kc = ctx.kernel_time(reset=True)
+        ctx.set_timing(False)
+        st = ctx.read_status(clear=True)
+        assert st.ok(), st.as_dict()
+        return ms / args.steps, kms / max(kc, 1), ctx.cp_iterations()
+
+    ms_c, upd_c, it_c = timed()
+    R_c = d_R.cpu().numpy()
+    s_c = ctx.get_state(1)
+    ctx.set_cp_warm_limit(args.warm_k)
+    ctx.set_cp_surrogate(net)
+    ms_w, upd_w, it_w = timed()
+    launches = ctx.launches_per_assembly()  # with the network attached
+    fb = ctx.cp_fallbacks()
+    R_w = d_R.cpu().numpy()
+    s_w = ctx.get_state(1)
+    # the warm start converges to the same point solution (both meet 1e-10)
+    state_rel = float(np.abs(s_w - s_c).max() / np.abs(s_c).max())
+    R_rel = float(np.linalg.norm(R_w - R_c) / np.linalg.norm(R_c))
+    # surrogate error on this step, judged by the converged plain Newton
+    xx = torch.empty((p.ne, pg.MLP_IN), dtype=torch.float32, device=dev)
+    tt = torch.empty((p.ne, pg.MLP_OUT), dtype=torch.float32, device=dev)
+    ctx.set_cp_surrogate(None)
+    step()
+    ctx.cp_training_pairs(xx.data_ptr(), tt.data_ptr())
+    yy = torch.empty_like(tt)
+    net.predict_device(p.ne, xx.data_ptr(), yy.data_ptr(), sh)
+    torch.cuda.synchronize()
+    pred_err = float(torch.linalg.norm(yy - tt) / torch.linalg.norm(tt))
+    out = {"metric": METRIC, "value": ws * p.nqp / (ms_w * 1e-3), "unit": UNIT, "n_gpus": ws,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_w, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network bf16 x bf16 -> f32)",
+           "data": "synthetic (seeded splitmix64)",
+           "config": {"workload": "FCC crystal plasticity, %d^3 cells x 6 linear tets (%d points), 512 grains, R+K "
+                                  "at load step %d of %d, local Newton to 1e-10 started from the learned guess "
+                                  "(cold-start fallback after %d iterations)"
+                                  % (args.cp_n, p.ne, args.cp_step, wl.CP_STEPS, args.warm_k),
+                      "plain_value": ws * p.nqp / (ms_c * 1e-3), "plain_ms_per_step": ms_c,
+                      "speedup_rk_iterate": ms_c / ms_w,
+                      "local_update_ms": {"plain": upd_c, "warm": upd_w},
+                      "speedup_local_update": upd_c / upd_w,
+                      "iterations_mean": {"plain": float(it_c.mean()), "warm": float(it_w.mean())},
+                      "iterations_hist": {"plain": np.bincount(it_c).tolist(), "warm": np.bincount(it_w).tolist()},
+                      "fallbacks": fb, "warm_vs_plain_state_rel": state_rel, "warm_vs_plain_R_rel": R_rel,
+                      "network": {"params": pg.Mlp.num_params(), "train_pairs": info["pairs"],
+                                  "train_seeds": "100..119 (%d^3 cells, one load step each)" % args.train_n,
+                                  "pair_generation_s": info["seconds"], "train_s": train_s,
+                                  "epochs": args.train_epochs, "loss_first_last": [float(hist[0]), float(hist[-1])],
+                                  "prediction_rel_err": pred_err}},
+           "gpu_launches": args.steps * launches}
+    ctx.close()
+    return out
+
+
 def run_reference(args, ws, rank):
     import workloads as wl
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -420,7 +527,10 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles"])
-    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "cp_p1"])
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "cp_p1", "cp_warm"])
+    ap.add_argument("--train-n", type=int, default=32)
+    ap.add_argument("--train-epochs", type=int, default=30)
+    ap.add_argument("--warm-k", type=int, default=6)
     ap.add_argument("--cp-n", type=int, default=48)
     ap.add_argument("--cp-step", type=int, default=10)
     args = ap.parse_args()
@@ -433,7 +543,12 @@ def main():
             print(json.dumps(out), flush=True)
         return
     ws, rank, local = dist_setup(args.gpus)
-    out = run_cp(args, ws, rank, local) if args.workload == "cp_p1" else run_ours(args, ws, rank, local)
+    if args.workload == "cp_p1":
+        out = run_cp(args, ws, rank, local)
+    elif args.workload == "cp_warm":
+        out = run_cp_warm(args, ws, rank, local)
+    else:
+        out = run_ours(args, ws, rank, local)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if ws > 1:

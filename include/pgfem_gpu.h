@@ -231,9 +231,9 @@ int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, con
  * predictor, src/plasticity_model.cc:1148-1224).  A 34 -> 128 -> 128 -> 128
  * (GELU) -> 12 network maps per-point features to the slip increments
  * dt*gamma_dot_a; only the initial guess of the FP64 Newton is taken from it.
- * Features (row of 34 FP32): F_{n+1} F_n^-1 - I (9), pF_n - I (9), the 12 slip
- * resistances (g_n for every system of this model), lattice quaternion (4,
- * w >= 0).  BF16 tensor-core (tcgen05) GEMMs, FP32 accumulation; trained on
+ * Features (row of 34 FP32): F_{n+1} F_n^-1 - I (9) and pF_n - I (9), both in
+ * the lattice frame of the point's crystal (R^T A R), the 12 slip resistances
+ * (g_n for every system of this model), lattice quaternion (4, w >= 0).  BF16 tensor-core (tcgen05) GEMMs, FP32 accumulation; trained on
  * the GPU by the library's own fused forward/backward kernel and Adam.
  * Parameter vector (FP32, 39,052): W1[128][34] b1 W2[128][128] b2 W3 b3
  * W4[12][128] b4.  Device pointers are marked d_. */
@@ -261,6 +261,22 @@ int pgfem_mlp_loss_grad(pgfem_mlp *m, long n, const float *x, const float *t, fl
 /* Adam over shuffled mini-batches of the n pairs; epoch_loss[epochs] (may be NULL) */
 int pgfem_mlp_train_device(pgfem_mlp *m, long n, const float *d_x, const float *d_t,
                            const pgfem_mlp_train_opts *opts, double *epoch_loss);
+
+/* Newton iterations allowed from a guess (set_cp_guess or the network) before
+ * the point restarts from the elastic predictor with the full cp_max_iter
+ * budget; 0 (default) = cp_max_iter.  Iteration counts report both runs. */
+int pgfem_gpu_set_cp_warm_limit(pgfem_gpu_ctx *ctx, int k);
+/* Attach (m != NULL) or detach the network: each CP assembly then computes
+ * the features on the device, runs the tcgen05 forward pass and starts the
+ * FP64 Newton from the predicted slip (M0 = I - sum dgam_a P_a, g0 from the
+ * hardening update).  The tolerance is unchanged; the cold start remains the
+ * fallback.  The network must live on the context's device and outlive use. */
+int pgfem_gpu_set_cp_surrogate(pgfem_gpu_ctx *ctx, pgfem_mlp *m);
+/* Training pairs of the last assembly: features (d_x, nqp x 34) and the
+ * converged slip increments (d_t, nqp x 12), device FP32 buffers. */
+int pgfem_gpu_cp_training_pairs(pgfem_gpu_ctx *ctx, float *d_x, float *d_t);
+/* Points of the last assembly that fell back to the cold start. */
+int pgfem_gpu_get_cp_fallbacks(pgfem_gpu_ctx *ctx, long *n);
 
 #ifdef __cplusplus
 }

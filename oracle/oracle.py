@@ -56,7 +56,7 @@ def lib():
             "orc_assemble_bform": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P, _P, C.c_long,
                                              C.c_long, C.c_int]),
             "orc_cp_update_batch": (C.c_long, [_P, C.c_long, _P, C.c_double, _P, _P, _P, _P, _P, _P, _P,
-                                               _P]),
+                                               _P, C.c_int, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -117,7 +117,7 @@ def cm_update(mat, F, state_n=None, dt=0.0, Rcp=None):
     return err, S.reshape(3, 3), L.reshape(3, 3, 3, 3), snp1, it.value
 
 
-def cp_update_batch(mat, F, state_n, dt, Rcp, M0=None, g_guess=None):
+def cp_update_batch(mat, F, state_n, dt, Rcp, M0=None, g_guess=None, warm_k=0, want_fallback=False):
     F = np.ascontiguousarray(F, dtype=np.float64).reshape(-1, 9)
     nq = F.shape[0]
     state_n = np.ascontiguousarray(state_n, dtype=np.float64).reshape(nq, 10)
@@ -128,8 +128,11 @@ def cp_update_batch(mat, F, state_n, dt, Rcp, M0=None, g_guess=None):
     it = np.zeros(nq, dtype=np.int32)
     dg = np.zeros((nq, 12))
     cv = np.zeros(nq, dtype=np.int32)
+    fb = np.zeros(nq, dtype=np.int32)
     bad = lib().orc_cp_update_batch(C.byref(mat), nq, _p(F), dt, _p(Rcp), _p(state_n), _p(M0), _p(gg), _p(snp1),
-                                    _p(it), _p(dg), _p(cv))
+                                    _p(it), _p(dg), _p(cv), int(warm_k), _p(fb))
+    if want_fallback:
+        return bad, snp1, it, dg, cv, fb
     return bad, snp1, it, dg, cv
 
 

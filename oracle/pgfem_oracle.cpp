@@ -769,13 +769,14 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 extern "C" long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, double dt,
                                     const double *Rcp, const double *state_n, const double *M0,
                                     const double *g_guess, double *state_np1, int *iters, double *dgam,
-                                    int *converged) {
+                                    int *converged, int warm_k, int *fallback) {
   Elast el = make_elast(mat);
   long bad = 0;
   for (long q = 0; q < nqp; q++) {
     CpResult res;
     int err = cp_update_guess(mat, el, F + q * 9, dt, Rcp ? Rcp + q * 9 : nullptr, state_n + q * 10,
-                              M0 ? M0 + q * 9 : nullptr, g_guess ? g_guess[q] : -1.0, res);
+                              M0 ? M0 + q * 9 : nullptr, g_guess ? g_guess[q] : -1.0, res, warm_k);
+    if (fallback) fallback[q] = res.fallback;
     if (state_np1) {
       for (int i = 0; i < 9; i++) state_np1[q * 10 + i] = res.pFnp1[i];
       state_np1[q * 10 + 9] = res.g;

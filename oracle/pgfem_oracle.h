@@ -114,10 +114,14 @@ int orc_assemble_bform(const orc_problem *P, const orc_material *mat,
  * give the Newton's initial guess per point (NULL: elastic predictor).
  * Outputs the state at t_{n+1} (nqp*10), the iteration counts, the slip
  * increments dt*gamma_dot_a (nqp*12, may be NULL) and a convergence flag.
+ * With a guess, the Newton gets warm_k iterations from it (0: cp_max_iter)
+ * before restarting from the elastic predictor; fallback[q] (may be NULL)
+ * flags those restarts and iters counts both runs.
  * Returns the number of points that failed. */
 long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, double dt, const double *Rcp,
                          const double *state_n, const double *M0, const double *g_guess,
-                         double *state_np1, int *iters, double *dgam, int *converged);
+                         double *state_np1, int *iters, double *dgam, int *converged, int warm_k,
+                         int *fallback);
 
 /* Number of quadrature points per element for nne (1 for 4, 4 for 10). */
 int orc_nint(int nne);

@@ -265,6 +265,8 @@ struct CpArgs {
   unsigned long long *status;
   Mat mat;
   double dt;
+  int warm_k;                     // Newton iterations from the guess before the cold restart (0: max_iter)
+  unsigned long long *fallbacks;  // cold restarts (or nullptr)
 };
 
 constexpr int kCpWarps = 2;  // warps per CTA of k_cp_update
@@ -281,7 +283,8 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
   bool done = false;
   CpPoint pt;
   double M[9], g = 0, Res[10], nr = 0, gd[kSlip], dgd[kSlip], gdot = 0, Fq[9], pFni[9];
-  int it = 0;
+  int it = 0, it0 = 0;  // total iterations; iterations before the current start
+  bool warm = false;    // Newton running from the caller's guess
   NeoHooke h;
   for (;;) {
     // refill lanes without a point (warp-aggregated tickets)
@@ -320,7 +323,8 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
             for (int i = 0; i < 9; i++) M[i] = (i % 4 == 0) ? 1.0 : 0.0;
             g = pt.g_n;
           }
-          it = 0;
+          it = it0 = 0;
+          warm = A.guess != nullptr;
           if (cp_residual(A.mat, pt, M, g, Res, h, gd, dgd, gdot)) nr = cp_norm(Res, A.mat.g0);
           else nr = 1e300;
         } else {
@@ -331,7 +335,8 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
     if (__all_sync(FULL, done)) break;
     if (qp < 0) continue;
     // one Newton step (or finish)
-    bool finish = !(nr > tol) || it >= A.mat.max_iter || !(nr < 1e299);
+    const int cap = warm && A.warm_k > 0 ? A.warm_k : A.mat.max_iter;
+    bool finish = !(nr > tol) || it - it0 >= cap || !(nr < 1e299);
     if (!finish) {
       cp_jacobian(A.mat, pt, M, g, h, gd, dgd, gdot, Jm);
       for (int i = 0; i < 10; i++) lm(Bm, 1, i, 0) = -Res[i];
@@ -369,6 +374,19 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
         }
         it++;
       }
+    }
+    if (finish && warm && !(nr <= tol)) {
+      // the guess did not converge in cap iterations (or left the domain):
+      // restart from the elastic predictor with the full iteration budget
+      warm = false;
+      it0 = it;
+      if (A.fallbacks) atomicAdd(A.fallbacks, 1ull);
+#pragma unroll
+      for (int i = 0; i < 9; i++) M[i] = (i % 4 == 0) ? 1.0 : 0.0;
+      g = pt.g_n;
+      if (cp_residual(A.mat, pt, M, g, Res, h, gd, dgd, gdot)) nr = cp_norm(Res, A.mat.g0);
+      else nr = 1e300;
+      finish = false;
     }
     if (finish) {
       const bool conv = nr <= tol;
@@ -631,6 +649,112 @@ __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
       }
     }
   }
+}
+
+
+// ---- learned warm start: features, guess, training pairs -------------------
+
+// Unit quaternion (w, x, y, z), w >= 0, of a rotation matrix (Shepperd's
+// method: branch on the largest of the trace and the diagonal).
+__device__ __forceinline__ void rot_to_quat(const double *R, double *q) {
+  const double tr = R[0] + R[4] + R[8];
+  double w, x, y, z;
+  if (tr > 0.0) {
+    const double s = 2.0 * sqrt(tr + 1.0);
+    w = 0.25 * s, x = (R[7] - R[5]) / s, y = (R[2] - R[6]) / s, z = (R[3] - R[1]) / s;
+  } else if (R[0] > R[4] && R[0] > R[8]) {
+    const double s = 2.0 * sqrt(1.0 + R[0] - R[4] - R[8]);
+    w = (R[7] - R[5]) / s, x = 0.25 * s, y = (R[1] + R[3]) / s, z = (R[2] + R[6]) / s;
+  } else if (R[4] > R[8]) {
+    const double s = 2.0 * sqrt(1.0 + R[4] - R[0] - R[8]);
+    w = (R[2] - R[6]) / s, x = (R[1] + R[3]) / s, y = 0.25 * s, z = (R[5] + R[7]) / s;
+  } else {
+    const double s = 2.0 * sqrt(1.0 + R[8] - R[0] - R[4]);
+    w = (R[3] - R[1]) / s, x = (R[2] + R[6]) / s, y = (R[5] + R[7]) / s, z = 0.25 * s;
+  }
+  const double sg = w < 0.0 ? -1.0 : 1.0;
+  q[0] = sg * w, q[1] = sg * x, q[2] = sg * y, q[3] = sg * z;
+}
+
+constexpr int kCpFeat = 34;
+
+// Network features per point (row of 34 FP32), tensors in the lattice frame of
+// the point's crystal (R^T A R), where the slip systems are the same for every
+// grain: F F_n^-1 - I (9), pF_n - I (9), the 12 slip resistances (g_n for every
+// system), lattice quaternion (4).
+__global__ void k_cp_features(long nqp, const double *__restrict__ F, const double *__restrict__ Fn,
+                              const double *__restrict__ state_n, const double *__restrict__ Rcp, int nqp_e,
+                              long ne, float *__restrict__ x) {
+  const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= nqp) return;
+  double f[9], fn[9], fni[9], d[9], R[9], qt[4];
+  const long e = q / nqp_e;
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    f[i] = F[i * nqp + q];
+    fn[i] = Fn[i * nqp + q];
+    R[i] = Rcp[i * ne + e];
+  }
+  if (!inv3(fn, fni))
+#pragma unroll
+    for (int i = 0; i < 9; i++) fni[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  mm3(f, fni, d);
+  rot_to_quat(R, qt);
+  double pf[9], t[9], dc[9], pc[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) pf[i] = state_n[i * nqp + q];
+  mm3(d, R, t);  // lattice frame: R^T A R
+  mm3tn(R, t, dc);
+  mm3(pf, R, t);
+  mm3tn(R, t, pc);
+  float *o = x + q * kCpFeat;
+#pragma unroll
+  for (int i = 0; i < 9; i++) o[i] = (float)(dc[i] - (i % 4 == 0 ? 1.0 : 0.0));
+#pragma unroll
+  for (int i = 0; i < 9; i++) o[9 + i] = (float)(pc[i] - (i % 4 == 0 ? 1.0 : 0.0));
+  const float gn = (float)state_n[9 * nqp + q];
+#pragma unroll
+  for (int a = 0; a < kSlip; a++) o[18 + a] = gn;
+#pragma unroll
+  for (int i = 0; i < 4; i++) o[30 + i] = (float)qt[i];
+}
+
+// Newton guess from predicted slip increments y (AoS nqp x 12):
+// M0 = I - sum_a y_a P_a, and g0 from the hardening update with
+// dt*gamma_dot = sum_a |y_a|:  g0 = (g_n + c gs) / (1 + c),  c = G0 sum|y| / (gs - g0).
+__global__ void k_cp_guess(long nqp, const float *__restrict__ y, const double *__restrict__ Rcp, int nqp_e,
+                           long ne, const double *__restrict__ state_n, const Mat mat, double *__restrict__ guess) {
+  const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= nqp) return;
+  double R[9], M[9];
+  const long e = q / nqp_e;
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    R[i] = Rcp[i * ne + e];
+    M[i] = (i % 4 == 0) ? 1.0 : 0.0;
+  }
+  double sabs = 0.0;
+  for (int a = 0; a < kSlip; a++) {
+    double P[9];
+    schmid(R, a, P);
+    const double da = (double)y[q * kSlip + a];
+    sabs += fabs(da);
+#pragma unroll
+    for (int i = 0; i < 9; i++) M[i] -= da * P[i];
+  }
+  const double c = mat.G0 * sabs / (mat.gs0 - mat.g0);
+  const double gn = state_n[9 * nqp + q];
+#pragma unroll
+  for (int i = 0; i < 9; i++) guess[i * nqp + q] = M[i];
+  guess[9 * nqp + q] = (gn + c * mat.gs0) / (1.0 + c);
+}
+
+// Converged slip increments of the last local solve as FP32 training targets (AoS nqp x 12).
+__global__ void k_cp_targets(long nqp, const double *__restrict__ out, float *__restrict__ t) {
+  const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= nqp) return;
+#pragma unroll
+  for (int a = 0; a < kSlip; a++) t[q * kSlip + a] = (float)out[(91 + a) * nqp + q];
 }
 
 }  // namespace pgb

@@ -75,6 +75,12 @@ struct pgfem_gpu_ctx {
   int *cp_iters = nullptr;
   unsigned *cp_counter = nullptr;
   bool cp_use_guess = false;
+  // learned warm start: F at t_n, network features / predictions, cold restarts
+  double *cp_Fn = nullptr;
+  float *cp_feat = nullptr, *cp_pred = nullptr;
+  pgfem_mlp *cp_net = nullptr;
+  int cp_warm_k = 0;
+  unsigned long long *cp_fallbacks = nullptr;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -241,7 +247,8 @@ void release(pgfem_gpu_ctx *c) {
                   c->state_n, c->state_np1, c->status, c->d_u, c->d_presc, c->d_R, c->d_K,
                   c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
                   c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree,
-                  c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter};
+                  c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
+                  c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -398,6 +405,22 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
                                                           c->cp_detJw, c->status);
   CK(cudaGetLastError());
   CK(cudaMemsetAsync(c->cp_counter, 0, sizeof(unsigned), s));
+  CK(cudaMemsetAsync(c->cp_fallbacks, 0, sizeof(unsigned long long), s));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (c->timing && c->events.size() < 4096) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    CK(cudaEventRecord(e0, s));
+  }
+  const unsigned pblk = (unsigned)((c->nqp + 127) / 128);
+  if (c->cp_net) {  // network guess: features -> tcgen05 forward -> M0, g0
+    k_cp_features<<<pblk, 128, 0, s>>>(c->nqp, c->cp_F, c->cp_Fn, c->state_n, c->cp_R, 1, c->ne, c->cp_feat);
+    CK(cudaGetLastError());
+    int r = pgfem_mlp_predict_device(c->cp_net, c->nqp, c->cp_feat, c->cp_pred, s);
+    if (r) return r;
+    k_cp_guess<<<pblk, 128, 0, s>>>(c->nqp, c->cp_pred, c->cp_R, 1, c->ne, c->state_n, c->mat, c->cp_guess);
+    CK(cudaGetLastError());
+  }
   CpArgs a{};
   a.nqp = c->nqp;
   a.F = c->cp_F;
@@ -406,7 +429,9 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   a.ne = c->ne;
   a.state_n = c->state_n;
   a.state_np1 = c->state_np1;
-  a.guess = c->cp_use_guess ? c->cp_guess : nullptr;
+  a.guess = (c->cp_use_guess || c->cp_net) ? c->cp_guess : nullptr;
+  a.warm_k = c->cp_warm_k;
+  a.fallbacks = c->cp_fallbacks;
   a.out = c->cp_out;
   a.iters = c->cp_iters;
   a.counter = c->cp_counter;
@@ -425,12 +450,6 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   if (!g_num_sms) grid_for(1, 1, 1);
   const long need = (c->nqp + 32 * kCpWarps - 1) / (32 * kCpWarps);
   const long grid = std::max<long>(1, std::min<long>(need, (long)g_num_sms * per_sm));
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (c->timing && c->events.size() < 4096) {
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
-    CK(cudaEventRecord(e0, s));
-  }
   k_cp_update<<<(unsigned)grid, 32 * kCpWarps, smem, s>>>(a);
   CK(cudaGetLastError());
   if (e0) {
@@ -681,8 +700,12 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
       for (int i = 0; i < 9; i++) Rs[(size_t)i * ne + e] = m->R_cp[e * 9 + i];
     if ((r = upload(c, &c->cp_R, Rs.data(), Rs.size())) || (r = dalloc(c, &c->cp_F, (size_t)9 * ne)) ||
         (r = dalloc(c, &c->cp_detJw, ne)) || (r = dalloc(c, &c->cp_out, (size_t)kCpOut * c->nqp)) ||
-        (r = dalloc(c, &c->cp_iters, c->nqp)) || (r = dalloc(c, &c->cp_counter, 1)))
+        (r = dalloc(c, &c->cp_iters, c->nqp)) || (r = dalloc(c, &c->cp_counter, 1)) ||
+        (r = dalloc(c, &c->cp_fallbacks, 1)))
       return fail(r);
+    std::vector<double> Fn((size_t)9 * c->nqp, 0.0);  // F at t_n: identity until the first commit
+    for (long q = 0; q < c->nqp; q++) Fn[0 * c->nqp + q] = Fn[4 * c->nqp + q] = Fn[8 * c->nqp + q] = 1.0;
+    if ((r = upload(c, &c->cp_Fn, Fn.data(), Fn.size()))) return fail(r);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
   }
   // tiled assembly plan (HE / J2)
@@ -764,7 +787,8 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
-  if (c->model == PGFEM_MODEL_CP) return 4;  // u expansion, F, local Newton, element
+  if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, element (+ features, network, guess)
+    return c->cp_net ? 7 : 4;
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
@@ -799,6 +823,44 @@ int pgfem_gpu_get_cp_iterations(pgfem_gpu_ctx *c, int *iters, double *dgam) {
       for (int a = 0; a < 12; a++) dgam[q * 12 + a] = soa[(size_t)a * c->nqp + q];
   }
   CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_cp_warm_limit(pgfem_gpu_ctx *c, int k) {
+  if (!c || c->model != PGFEM_MODEL_CP || k < 0) return PGFEM_GPU_EINVAL;
+  c->cp_warm_k = k;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_cp_surrogate(pgfem_gpu_ctx *c, pgfem_mlp *m) {
+  if (!c || c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  if (m) {
+    int r;
+    if (!c->cp_guess && (r = dalloc(c, &c->cp_guess, (size_t)10 * c->nqp))) return r;
+    if (!c->cp_feat && (r = dalloc(c, &c->cp_feat, (size_t)kCpFeat * c->nqp))) return r;
+    if (!c->cp_pred && (r = dalloc(c, &c->cp_pred, (size_t)kSlip * c->nqp))) return r;
+  }
+  c->cp_net = m;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_cp_training_pairs(pgfem_gpu_ctx *c, float *d_x, float *d_t) {
+  if (!c || c->model != PGFEM_MODEL_CP || !d_x || !d_t) return PGFEM_GPU_EINVAL;
+  const unsigned blk = (unsigned)((c->nqp + 127) / 128);
+  k_cp_features<<<blk, 128, 0, c->stream>>>(c->nqp, c->cp_F, c->cp_Fn, c->state_n, c->cp_R, 1, c->ne, d_x);
+  CK(cudaGetLastError());
+  k_cp_targets<<<blk, 128, 0, c->stream>>>(c->nqp, c->cp_out, d_t);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_get_cp_fallbacks(pgfem_gpu_ctx *c, long *n) {
+  if (!c || c->model != PGFEM_MODEL_CP || !n) return PGFEM_GPU_EINVAL;
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, c->cp_fallbacks, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *n = (long)v;
   return PGFEM_GPU_OK;
 }
 
@@ -877,6 +939,8 @@ int pgfem_gpu_commit_state(pgfem_gpu_ctx *c) {
   if (c->nstate)
     CK(cudaMemcpyAsync(c->state_n, c->state_np1, sizeof(double) * c->nstate * c->nqp,
                        cudaMemcpyDeviceToDevice, c->stream));
+  if (c->cp_Fn)  // F of the converged iterate becomes F_n (warm-start features)
+    CK(cudaMemcpyAsync(c->cp_Fn, c->cp_F, sizeof(double) * 9 * c->nqp, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PGFEM_GPU_OK;
 }

@@ -102,6 +102,10 @@ def lib():
             "pgfem_mlp_predict": (C.c_int, [_P, C.c_long, _P, _P]),
             "pgfem_mlp_loss_grad": (C.c_int, [_P, C.c_long, _P, _P, _P, _P]),
             "pgfem_mlp_train_device": (C.c_int, [_P, C.c_long, _P, _P, _P, _P]),
+            "pgfem_gpu_set_cp_warm_limit": (C.c_int, [_P, C.c_int]),
+            "pgfem_gpu_set_cp_surrogate": (C.c_int, [_P, _P]),
+            "pgfem_gpu_cp_training_pairs": (C.c_int, [_P, _P, _P]),
+            "pgfem_gpu_get_cp_fallbacks": (C.c_int, [_P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -285,6 +289,21 @@ class Context:
         dg = np.zeros((self.ne * self.nint, 12)) if want_slip else None
         _check("pgfem_gpu_get_cp_iterations", lib().pgfem_gpu_get_cp_iterations(self.h, _ptr(it), _ptr(dg)))
         return (it, dg) if want_slip else it
+
+    def set_cp_warm_limit(self, k):
+        _check("pgfem_gpu_set_cp_warm_limit", lib().pgfem_gpu_set_cp_warm_limit(self.h, int(k)))
+
+    def set_cp_surrogate(self, mlp):
+        self._net = mlp  # keep the network alive while attached
+        _check("pgfem_gpu_set_cp_surrogate", lib().pgfem_gpu_set_cp_surrogate(self.h, None if mlp is None else mlp.h))
+
+    def cp_training_pairs(self, d_x, d_t):
+        _check("pgfem_gpu_cp_training_pairs", lib().pgfem_gpu_cp_training_pairs(self.h, d_x, d_t))
+
+    def cp_fallbacks(self):
+        n = C.c_long()
+        _check("pgfem_gpu_get_cp_fallbacks", lib().pgfem_gpu_get_cp_fallbacks(self.h, C.byref(n)))
+        return n.value
 
     def read_status(self, clear=False):
         st = Status()
