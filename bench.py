@@ -182,7 +182,7 @@ def run_ours(args, ws, rank, local):
     log("[rank %d] context (device copy + element->CSR map) %.1f s, %.2f GB on device"
         % (rank, time.perf_counter() - t0, ctx.device_bytes() / 1e9))
     ctx.set_scatter_mode({"atomic": pg.SCATTER_ATOMIC, "colour": pg.SCATTER_COLOUR,
-                          "tiles": pg.SCATTER_TILES}[args.scatter])
+                          "tiles": pg.SCATTER_TILES, "cells": pg.SCATTER_CELLS}[args.scatter])
     fp64_peak = pg.fp64_peak_tflops()
     hbm_peak, hbm_src = measured_hbm_gbs()
 
@@ -526,7 +526,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles"])
+    ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles", "cells"])
     ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "cp_p1", "cp_warm"])
     ap.add_argument("--train-n", type=int, default=32)
     ap.add_argument("--train-epochs", type=int, default=30)

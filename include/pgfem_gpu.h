@@ -56,8 +56,11 @@ int pgfem_gpu_state_size(int model);
  *  TILES   point-update kernel + persistent tile kernel that combines the
  *          blocks of a cell of elements in shared memory, issues address-
  *          ordered reductions and zero-fills the CSR rows a tile touches first
- *          instead of a full memset (2.3x less DRAM traffic per iterate). */
-enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1, PGFEM_SCATTER_TILES = 2 };
+ *          instead of a full memset (2.3x less DRAM traffic per iterate);
+ *  CELLS   quadratic tets: one fused kernel per Kuhn cell of 6 elements --
+ *          point updates in registers, node-pair blocks combined in shared
+ *          memory, address-ordered coalesced reductions. */
+enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1, PGFEM_SCATTER_TILES = 2, PGFEM_SCATTER_CELLS = 3 };
 
 typedef struct {
   int model;

@@ -100,6 +100,10 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
   double *sXU = smem;                             // [TE][NNE][6]
   double *sRec = sXU + TE * NNE * 6;              // [TE][NQP][kRec]
   double *sVec = sRec + TE * NQP * kRec;          // [TE][NQP][NNE][kVec]
+  // per (element, node) metadata staged once per tile, so that the block and
+  // scatter phases issue no dependent global loads
+  int *sMeta = reinterpret_cast<int *>(sVec + TE * NQP * NNE * kVec);  // [TE*NNE][6]: mask, rp, rl, dof x3
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + TE * NNE * 6);  // [TE*NNE][NNE]
 
   const long ntot = args.elist ? args.nlist : args.ne;
   const int tid = threadIdx.x;
@@ -119,6 +123,21 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
       d[3] = args.unode[node];
       d[4] = args.unode[args.nn + node];
       d[5] = args.unode[2 * args.nn + node];
+      int *m = sMeta + (el * NNE + a) * 6;
+      if (DENSE) {
+        m[0] = 7;
+      } else {
+        m[0] = args.mask[node];
+        m[1] = args.rowptr0[node];
+        m[2] = args.rowlen[node];
+        m[3] = args.dof[node];
+        m[4] = args.dof[args.nn + node];
+        m[5] = args.dof[2 * args.nn + node];
+        const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
+        uint16_t *sp = sPos + (el * NNE + a) * NNE;
+#pragma unroll
+        for (int b = 0; b < NNE; b++) sp[b] = pr[b];
+      }
     }
     __syncthreads();
 
@@ -255,24 +274,25 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
         for (int i = 0; i < 3; i++) args.fe_out[ei * (NNE * 3) + a * 3 + i] = Ra[i];
         maskA = 7u;
       } else {
+        const int *m = sMeta + (el * NNE + a) * 6;
 #pragma unroll
         for (int i = 0; i < 3; i++) {
-          const int id = args.dof[i * args.nn + node];
+          const int id = m[3 + i];
           if (id > 0) add_to<ATOMIC>(&args.R[id - 1], Ra[i]);
         }
-        maskA = args.mask[node];
+        maskA = (unsigned)m[0];
       }
     }
     __syncthreads();
 
     // ---------------- phase 3: stiffness blocks + CSR scatter ----------------
     if (WANT_K && valid && maskA) {
-      const long rp = DENSE ? 0 : args.rowptr0[node];
-      const long rl = DENSE ? 0 : args.rowlen[node];
-      const uint16_t *posrow = DENSE ? nullptr : args.pos + (e * NNE + a) * NNE;
+      const int *mA = sMeta + (el * NNE + a) * 6;
+      const long rp = DENSE ? 0 : mA[1];
+      const long rl = DENSE ? 0 : mA[2];
+      const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
       for (int b = 0; b < NNE; b++) {
-        const int nodeB = args.conn[(long)b * args.ne + e];
-        const unsigned maskB = DENSE ? 7u : args.mask[nodeB];
+        const unsigned maskB = DENSE ? 7u : (unsigned)sMeta[(el * NNE + b) * 6];
         if (!maskB) continue;
         double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
@@ -342,7 +362,8 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
 
 template <int NNE, int NQP>
 constexpr size_t asm_smem_bytes() {
-  return sizeof(double) * (size_t)Tile<NNE>::TE * (NNE * 6 + NQP * kRec + NQP * NNE * kVec);
+  return sizeof(double) * (size_t)Tile<NNE>::TE * (NNE * 6 + NQP * kRec + NQP * NNE * kVec) +
+         (size_t)Tile<NNE>::TE * NNE * (6 * sizeof(int) + NNE * sizeof(uint16_t));
 }
 
 }  // namespace pgb

@@ -1,0 +1,282 @@
+// assemble_p2.cuh -- fused FP64 R+K assembly of quadratic tets with
+// column-split block rows (default path for 10-node elements).
+//
+// Same operation as k_assemble (fd_residuals_MP + stiffmat_fd_MP for the
+// constitutive-model element, src/fd_residuals.cc:468-636,
+// src/stiffmat_fd.cc:831-993), organised for the FP64 pipe and the L2
+// reduction units:
+//
+//  0  thread (element, node): node data and CSR row metadata -> shared memory;
+//  1  thread (element, point): F, the constitutive update
+//     (run_integration_algorithm, src/constitutive_model.cc:1100-1129; state
+//     n -> n+1) and a point record (G = (dX/dxi)^-1 F^-1, w, tau, s, n,
+//     dev(n^2), tangent coefficients);
+//  2  item (element, point, node): the spatial vectors of the node,
+//        p = G^T dN/dxi,  U = w (a2 p - 2/3 s p),  W = w (a4 n p + a5 dev(n^2) p),
+//        T = w (a1/2 p + tau p),  S = -2/3 w s p,  n p
+//     (the tangent c = a1 I + a2 1(x)1 - 2/3 (s(x)1 + 1(x)s) + a4 n(x)n
+//      + a5 n(x)dev(n^2) applied to p_a and p_b in closed form);
+//  3  thread (element, row node a, column component k): for every column
+//     node b the three entries (i = 0..2, k) of
+//        K_ab = sum_q (p_b)(a1/2 w p_a)^T + p_a U_b^T + S_a p_b^T + (n p_a) W_b^T + (p_a . T_b) 1
+//     (compute_stiffness_matrix, src/constitutive_model.cc:1520-1616, in
+//     spatial form) with the left vectors of a held in registers, and the
+//     residual w tau p_a (compute_residual_vector, :1628-1662).  The three
+//     lanes k of one (element, a) are adjacent, so each FP64 reduction
+//     instruction writes three consecutive doubles of a CSR row segment
+//     (fd_res_assemble, src/fd_residuals.cc:58-73; PLoc_Sparse,
+//     src/PLoc_Sparse.cc:15-175).
+#pragma once
+#include <cstdint>
+
+#include "assemble.cuh"
+
+namespace pgb {
+
+constexpr int kP2TE = 8;                      // elements per CTA iteration
+constexpr int kP2Threads = kP2TE * 10 * 3;    // (element, node, component)
+constexpr int kP2VS = 18;                     // doubles per (point, node) vector record
+constexpr int kP2Rec = 38;                    // doubles per point record
+
+inline size_t p2_smem_bytes() {
+  return sizeof(double) * ((size_t)kP2TE * 10 * 6 + (size_t)kP2TE * 4 * kRec + (size_t)kP2TE * 4 * 10 * kP2VS +
+                           (size_t)kP2TE * 4) +
+         sizeof(int) * (size_t)kP2TE * 10 * 6 + sizeof(uint16_t) * (size_t)kP2TE * 100;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs args) {
+  constexpr int NNE = 10, NQP = 4, TE = kP2TE, VS = kP2VS;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ double smem[];
+  double *sXU = smem;                          // [TE][NNE][6]
+  double *sRec = sXU + TE * NNE * 6;           // [TE][NQP][kRec]
+  double *sVec = sRec + TE * NQP * kRec;       // [TE][NQP][NNE][VS]
+  double *sA1 = sVec + TE * NQP * NNE * VS;    // [TE][NQP]  w a1 / 2
+  int *sMeta = reinterpret_cast<int *>(sA1 + TE * NQP);            // [TE*NNE][6]: mask, rp, rl, dof x3
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + TE * NNE * 6);  // [TE*NNE][NNE]
+  const int tid = threadIdx.x;
+  const long ne = args.ne;
+
+  for (long tile0 = (long)blockIdx.x * TE; tile0 < ne; tile0 += (long)gridDim.x * TE) {
+    // ---------------- 0: node data and row metadata ----------------
+    if (tid < TE * NNE) {
+      const int el = tid / NNE, a = tid - el * NNE;
+      const long e = tile0 + el;
+      if (e < ne) {
+        const int node = args.conn[(long)a * ne + e];
+        double *d = sXU + tid * 6;
+        d[0] = args.X[node];
+        d[1] = args.X[args.nn + node];
+        d[2] = args.X[2 * args.nn + node];
+        d[3] = args.unode[node];
+        d[4] = args.unode[args.nn + node];
+        d[5] = args.unode[2 * args.nn + node];
+        int *m = sMeta + tid * 6;
+        m[0] = args.mask[node];
+        m[1] = args.rowptr0[node];
+        m[2] = args.rowlen[node];
+        m[3] = args.dof[node];
+        m[4] = args.dof[args.nn + node];
+        m[5] = args.dof[2 * args.nn + node];
+        const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
+        uint16_t *sp = sPos + tid * NNE;
+#pragma unroll
+        for (int b = 0; b < NNE; b++) sp[b] = pr[b];
+      }
+    }
+    __syncthreads();
+
+    // ---------------- 1: quadrature points ----------------
+    if (tid < TE * NQP) {
+      const int el = tid / NQP, q = tid - el * NQP;
+      const long e = tile0 + el;
+      if (e < ne) {
+        const double *xu = sXU + el * NNE * 6;
+        double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int b = 0; b < NNE; b++) {
+          const double g0 = args.shp.dNxi[q][b][0], g1 = args.shp.dNxi[q][b][1], g2 = args.shp.dNxi[q][b][2];
+#pragma unroll
+          for (int i = 0; i < 3; i++) {
+            const double x = xu[b * 6 + i], u = xu[b * 6 + 3 + i];
+            dX[i * 3 + 0] += g0 * x;
+            dX[i * 3 + 1] += g1 * x;
+            dX[i * 3 + 2] += g2 * x;
+            dU[i * 3 + 0] += g0 * u;
+            dU[i * 3 + 1] += g1 * u;
+            dU[i * 3 + 2] += g2 * u;
+          }
+        }
+        double *rec = sRec + tid * kRec;
+        const double detJ = det3(dX);
+        double dXi[9], F[9], Fi[9];
+        bool ok = detJ > 0.0 && inv3(dX, dXi);
+        if (ok) {
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+              F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] +
+                             dU[i * 3 + 1] * dXi[1 * 3 + j] + dU[i * 3 + 2] * dXi[2 * 3 + j];
+          if (args.F0)
+#pragma unroll
+            for (int i = 0; i < 9; i++) F[i] += args.F0[i];
+        }
+        const double J = ok ? det3(F) : -1.0;
+        if (ok) ok = J > 0.0 && inv3(F, Fi);
+        if (!ok) {
+          atomicAdd(&args.status[0], 1ull);
+#pragma unroll
+          for (int i = 0; i < kRec; i++) rec[i] = 0.0;
+        } else {
+          const long qp = e * NQP + q;
+          double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
+          if (PLASTIC) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) Ast[c] = args.state_n[c * args.nqp + qp];
+            alpha = args.state_n[6 * args.nqp + qp];
+          }
+          QpTangent t;
+          double Anp1[6], alpha_np1;
+          spatial_update<PLASTIC>(args.mat, F, J, Ast, alpha, t, Anp1, &alpha_np1);
+          if (PLASTIC && args.state_np1) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) args.state_np1[c * args.nqp + qp] = Anp1[c];
+            args.state_np1[6 * args.nqp + qp] = alpha_np1;
+          }
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+              rec[i * 3 + j] = dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] +
+                               dXi[i * 3 + 2] * Fi[2 * 3 + j];
+          rec[9] = detJ * args.shp.w[q];
+#pragma unroll
+          for (int i = 0; i < 6; i++) {
+            rec[10 + i] = t.tau[i];
+            rec[16 + i] = t.s[i];
+            rec[22 + i] = t.n[i];
+            rec[28 + i] = t.D[i];
+          }
+          rec[34] = t.a1;
+          rec[35] = t.a2;
+          rec[36] = t.a4;
+          rec[37] = t.a5;
+        }
+      }
+    }
+    __syncthreads();
+
+    // ---------------- 2: node vectors per point ----------------
+    for (int it = tid; it < TE * NQP * NNE; it += kP2Threads) {
+      const int eq = it / NNE, a = it - eq * NNE;  // eq = el * NQP + q
+      const int q = eq % NQP;
+      const double *rec = sRec + eq * kRec;
+      const double w = rec[9];
+      const double a1h = 0.5 * rec[34] * w, a2w = rec[35] * w, c23 = (2.0 / 3.0) * w;
+      const double g0 = args.shp.dNxi[q][a][0], g1 = args.shp.dNxi[q][a][1], g2 = args.shp.dNxi[q][a][2];
+      double p[3], sp[3], tp[3];
+#pragma unroll
+      for (int j = 0; j < 3; j++) p[j] = rec[0 * 3 + j] * g0 + rec[1 * 3 + j] * g1 + rec[2 * 3 + j] * g2;
+      smv(rec + 16, p, sp);
+      smv(rec + 10, p, tp);
+      double *v = sVec + it * VS;
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        v[j] = p[j];
+        v[3 + j] = a2w * p[j] - c23 * sp[j];
+        v[9 + j] = a1h * p[j] + w * tp[j];
+        v[12 + j] = -c23 * sp[j];
+      }
+      if (PLASTIC) {
+        const double a4w = rec[36] * w, a5w = rec[37] * w;
+        double np_[3], mp[3];
+        smv(rec + 22, p, np_);
+        smv(rec + 28, p, mp);
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+          v[6 + j] = a4w * np_[j] + a5w * mp[j];
+          v[15 + j] = np_[j];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < 3; j++) v[6 + j] = v[15 + j] = 0.0;
+      }
+      if (a == 0) sA1[eq] = a1h;
+    }
+    __syncthreads();
+
+    // ---------------- 3: column-split block rows + scatter ----------------
+    {
+      const int el = tid / 30, r = tid - el * 30;
+      const int a = r / 3, k = r - a * 3;
+      const long e = tile0 + el;
+      const int *mA = sMeta + (el * NNE + a) * 6;
+      const unsigned maskA = (e < ne) ? (unsigned)mA[0] : 0u;
+      if (maskA) {
+        // left vectors of node a at the four points (registers)
+        double pa[NQP][3], Sa[NQP][3], na[NQP][3], ha[NQP], Rk = 0.0;
+#pragma unroll
+        for (int q = 0; q < NQP; q++) {
+          const double *L = sVec + ((el * NQP + q) * NNE + a) * VS;
+          const double a1h = sA1[el * NQP + q];
+#pragma unroll
+          for (int j = 0; j < 3; j++) {
+            pa[q][j] = L[j];
+            Sa[q][j] = L[12 + j];
+            na[q][j] = PLASTIC ? L[15 + j] : 0.0;
+          }
+          const double pk = k == 0 ? pa[q][0] : (k == 1 ? pa[q][1] : pa[q][2]);
+          ha[q] = a1h * pk;
+          Rk += L[9 + k] - ha[q];  // w tau p_a = T_a - a1/2 w p_a
+        }
+        // residual component k of node a
+        {
+          const int id = mA[3 + k];
+          if (id > 0) atomicAdd(&args.R[id - 1], Rk);
+        }
+        const long rp = mA[1], rl = mA[2];
+        const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
+#pragma unroll 1
+        for (int b = 0; b < NNE; b++) {
+          const unsigned maskB = (unsigned)sMeta[(el * NNE + b) * 6];
+          double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+          for (int q = 0; q < NQP; q++) {
+            const double *Rv = sVec + ((el * NQP + q) * NNE + b) * VS;
+            const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
+            const double pb[3] = {r0.x, r0.y, Rv[2]};
+            const double Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
+            const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
+            const double T[3] = {Rv[9], t01.x, t01.y};
+            const double pbk = k == 0 ? pb[0] : (k == 1 ? pb[1] : pb[2]);
+            const double dg = pa[q][0] * T[0] + pa[q][1] * T[1] + pa[q][2] * T[2];
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+              double v = acc[i];
+              v = fma(pb[i], ha[q], v);
+              v = fma(pa[q][i], Uk, v);
+              v = fma(Sa[q][i], pbk, v);
+              if (PLASTIC) v = fma(na[q][i], Wk, v);
+              acc[i] = v;
+            }
+            if (k == 0) acc[0] += dg;
+            else if (k == 1) acc[1] += dg;
+            else acc[2] += dg;
+          }
+          if (!((maskB >> k) & 1u)) continue;
+          const long col = rp + posrow[b] + rank_of(maskB, k);
+#pragma unroll
+          for (int i = 0; i < 3; i++) {
+            if (!((maskA >> i) & 1u)) continue;
+            atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[i]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace pgb

@@ -22,6 +22,8 @@
 #include "assemble.cuh"
 #include "tile_plan.hpp"
 #include "assemble_tiles.cuh"
+#include "assemble_cells.cuh"
+#include "assemble_p2.cuh"
 #include "cm_integrate.cuh"
 #include "cp_kernels.cuh"
 #include "peak_probe.cuh"
@@ -309,6 +311,10 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
 
 template <int NNE, int NQP, int MODEL>
 int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  if (!c->qrec) {  // point records of the two-kernel mode, allocated on first use
+    int r = dalloc(c, &c->qrec, (size_t)kQRec * c->nqp);
+    if (r) return r;
+  }
   {
     QpArgs q{};
     q.X = c->X;
@@ -373,14 +379,84 @@ int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+template <int MODEL>
+int launch_cells(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  const size_t smem = cells_smem_bytes(c->nslots_max);
+  auto kern = k_assemble_cells<MODEL>;
+  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCellThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long grid = std::max<long>(1, std::min<long>(c->ntiles, (long)g_num_sms * per_sm));
+  CellArgs a{};
+  a.X = c->X;
+  a.unode = c->unode;
+  a.conn = c->conn;
+  a.nn = c->nn;
+  a.ne = c->ne;
+  a.nqp = c->nqp;
+  a.F0 = c->F0;
+  a.state_n = c->state_n;
+  a.state_np1 = c->state_np1;
+  a.dof = c->dof;
+  a.rowptr0 = c->rowptr0;
+  a.rowlen = c->rowlen;
+  a.mask = c->mask;
+  a.tile_nodes = c->t_nodes;
+  a.tile_nl = c->t_nl;
+  a.elem_lnode = c->t_lnode;
+  a.elem_slot = c->t_slot;
+  a.slot_off = c->t_soff;
+  a.slot_info = c->t_sinfo;
+  a.aoff = c->t_aoff;
+  a.allfree = c->t_allfree;
+  a.ntiles = c->ntiles;
+  a.nslots_max = c->nslots_max;
+  a.R = d_R;
+  a.K = d_K;
+  a.status = c->status;
+  a.mat = c->mat;
+  a.shp = c->shp;
+  kern<<<(unsigned)grid, kCellThreads, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 int dispatch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  if (c->scatter_mode == PGFEM_SCATTER_CELLS)
+    return c->model == PGFEM_MODEL_J2 ? launch_cells<1>(c, d_R, d_K, s) : launch_cells<0>(c, d_R, d_K, s);
   if (c->nne == 4)
     return c->model == PGFEM_MODEL_J2 ? launch_tiles<4, 1, 1>(c, d_R, d_K, s) : launch_tiles<4, 1, 0>(c, d_R, d_K, s);
   return c->model == PGFEM_MODEL_J2 ? launch_tiles<10, 4, 1>(c, d_R, d_K, s) : launch_tiles<10, 4, 0>(c, d_R, d_K, s);
 }
 
+template <int MODEL>
+int launch_p2(const AsmArgs &a, cudaStream_t s) {
+  const size_t smem = p2_smem_bytes();
+  auto kern = k_assemble_p2<MODEL>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kP2Threads, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long tiles = (a.ne + kP2TE - 1) / kP2TE;
+  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
+  kern<<<(unsigned)grid, kP2Threads, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 template <bool ATOMIC, bool WANT_K, bool DENSE>
 int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
+  // quadratic tets, R+K into the CSR with atomic scatter over all elements:
+  // the column-split kernel
+  if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS"))
+    return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
   if (c->nne == 4) {
     switch (c->model) {
       case PGFEM_MODEL_HE: return launch_asm<4, 1, 0, ATOMIC, WANT_K, DENSE>(a, nitems, s);
@@ -484,9 +560,11 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
 // One assembly on device buffers (zeroing R and K first).
 int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
                     double *d_K, cudaStream_t s, double dt = 0.0) {
-  const bool use_tiles = c->tiles && d_K && c->scatter_mode == PGFEM_SCATTER_TILES;
+  const bool use_cells = c->tiles && d_K && c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_CELLS;
+  const bool use_tiles = c->tiles && d_K && (c->scatter_mode == PGFEM_SCATTER_TILES || use_cells);
   if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
-  if (d_K && !(use_tiles && c->tile_zero_mode)) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
+  if (d_K && !(use_tiles && !use_cells && c->tile_zero_mode))
+    CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
   {
     const long n3 = 3 * c->nn;
     k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
@@ -734,8 +812,7 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
         (r = upload(c, &c->t_zhi, P.zhi.data(), P.zhi.size())) ||
         (r = upload(c, &c->t_deps, P.deps.data(), P.deps.size())) ||
         (r = upload(c, &c->t_allfree, P.allfree.data(), P.allfree.size())) ||
-        (r = dalloc(c, &c->t_flags, P.ntiles)) || (r = dalloc(c, &c->t_ticket, 1)) ||
-        (r = dalloc(c, &c->qrec, (size_t)kQRec * c->nqp)))
+        (r = dalloc(c, &c->t_flags, P.ntiles)) || (r = dalloc(c, &c->t_ticket, 1)))
       return fail(r);
     if (cudaMemsetAsync(c->t_flags, 0, sizeof(unsigned) * P.ntiles, c->stream) != cudaSuccess ||
         cudaStreamSynchronize(c->stream) != cudaSuccess)
@@ -775,9 +852,11 @@ int pgfem_gpu_destroy(pgfem_gpu_ctx *c) {
 }
 
 int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
-  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR && mode != PGFEM_SCATTER_TILES))
+  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR && mode != PGFEM_SCATTER_TILES &&
+             mode != PGFEM_SCATTER_CELLS))
     return PGFEM_GPU_EINVAL;
-  if (mode == PGFEM_SCATTER_TILES && !c->tiles) return PGFEM_GPU_EINVAL;
+  if ((mode == PGFEM_SCATTER_TILES || mode == PGFEM_SCATTER_CELLS) && !c->tiles) return PGFEM_GPU_EINVAL;
+  if (mode == PGFEM_SCATTER_CELLS && c->nne != 10) return PGFEM_GPU_EINVAL;
   c->scatter_mode = mode;
   return PGFEM_GPU_OK;
 }
@@ -789,6 +868,7 @@ int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
   if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, element (+ features, network, guess)
     return c->cp_net ? 7 : 4;
+  if (c->tiles && c->scatter_mode == PGFEM_SCATTER_CELLS && c->nne == 10) return 2;  // u expansion, cells
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)

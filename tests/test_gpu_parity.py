@@ -250,3 +250,34 @@ def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
     Ro, Ko, _ = oracle_assemble(prob)
     check_R(R, Ro)
     check_K(K, Ko, Ap)
+
+
+@pytest.mark.parametrize("n,stretch,perturb,model", [(3, None, 1e-4, "j2"), (4, 4e-3, 5e-3, "j2"),
+                                                      (3, None, 1e-4, "he")])
+def test_cells_mode_matches_oracle(gpu, n, stretch, perturb, model):
+    """Fused one-cell-per-CTA kernel (quadratic tets) against the oracle; a
+    second call on the same buffers gives the same result."""
+    p = wl.j2_p2(n=n, seed=11, stretch=stretch, perturb=perturb)
+    if model == "he":
+        p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.3)
+        p.state = None
+    ctx = p.context()
+    ctx.set_scatter_mode(pg.SCATTER_CELLS)
+    assert ctx.launches_per_assembly() == 2
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    Ro, Ko, so = oracle_assemble(p)
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    if so is not None:
+        sg = ctx.get_state(1)
+        assert np.abs(sg - so).max() <= TOL * np.abs(so).max()
+    R2, K2, _ = ctx.assemble_RK(p.u)
+    check_R(R2, R, 1e-13)
+    check_K(K2, K, p.Ap, 1e-13)
+
+
+def test_cells_mode_is_for_quadratic_tets_only(gpu):
+    ctx = wl.he_p1(4).context()
+    with pytest.raises(pg.PgfemError):
+        ctx.set_scatter_mode(pg.SCATTER_CELLS)
