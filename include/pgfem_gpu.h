@@ -229,6 +229,35 @@ int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, con
                                    double *d_state_np1, double *d_dgam, int *d_iters,
                                    pgfem_gpu_status *st, void *stream);
 
+/* ---- batches of independent meshes (FE2 micro-structures) ---------------
+ * The context's mesh may be the union of independent meshes (e.g. the
+ * periodic RVEs of all macro points, src/stiffmat_fd.cc:1010-1128 assembles
+ * them one at a time): elements of group g are [elem_off[g], elem_off[g+1])
+ * and see the macro deformation F0[9g..9g+8] (added to F like
+ * cm_add_macro_F, src/constitutive_model.cc:247-252) instead of mesh->F0.
+ * The CSR is block diagonal over the groups (one Psparse_ApAi pattern over
+ * the union).  HE and J2. */
+int pgfem_gpu_set_mesh_groups(pgfem_gpu_ctx *ctx, int ngroups, const long *elem_off, const double *F0);
+/* Launch schedule of the linear-tet element kernel: elements per block
+ * (16, 32, 64; 0 = default 32) and work stealing (grab > 0: a persistent
+ * grid claims `grab` blocks of elements at a time from a counter; 0 = static
+ * grid-stride order).  No counterpart in the reference. */
+int pgfem_gpu_set_schedule(pgfem_gpu_ctx *ctx, int elems_per_block, int grab);
+int pgfem_gpu_get_schedule(const pgfem_gpu_ctx *ctx, int *elems_per_block, int *grab);
+/* One R+K assembly on device buffers captured as a CUDA graph (the
+ * context's stream; the capture runs the assembly once uncaptured first).
+ * Replays recompute R and K from the current contents of d_u / d_u_presc
+ * and the context state.  No counterpart in the reference. */
+typedef struct pgfem_gpu_graph pgfem_gpu_graph;
+int pgfem_gpu_graph_create(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc, double dt,
+                           double *d_R, double *d_K, pgfem_gpu_graph **graph);
+int pgfem_gpu_graph_launch(pgfem_gpu_graph *graph, void *stream);
+int pgfem_gpu_graph_destroy(pgfem_gpu_graph *graph);
+/* Times every schedule (3 block sizes x 5 steal sizes) as captured graphs,
+ * `reps` replays each, keeps the fastest and reports it.  Linear tets. */
+int pgfem_gpu_autotune(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc, double dt, double *d_R,
+                       double *d_K, int reps, int *best_elems_per_block, int *best_grab, double *best_ms);
+
 /* ---- learned warm start of the CP local Newton ----------------------------
  * No counterpart in the reference (its Newton starts from the elastic
  * predictor, src/plasticity_model.cc:1148-1224).  A 34 -> 128 -> 128 -> 128

@@ -64,6 +64,14 @@ struct AsmArgs {
   // dense element outputs (element-level entry points): lk[nlist][nd][nd], fe[nlist][nd]
   double *lk_out;
   double *fe_out;
+  // batches of independent meshes (FE2 micro-structures): element -> group,
+  // group -> macro deformation F0 (9); nullptr = the single F0 above
+  const int *elem_group;
+  const double *F0_tab;
+  // work stealing: tiles are claimed `grab` at a time from *ticket (zeroed
+  // before the launch); nullptr = static grid-stride order
+  unsigned *ticket;
+  int grab;
   Mat mat;
   ShapeTable shp;
 };
@@ -91,10 +99,10 @@ __device__ __forceinline__ void add_to(double *p, double v) {
     *p += v;
 }
 
-template <int NNE, int NQP, int MODEL, bool ATOMIC, bool WANT_K, bool DENSE>
-__global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
+template <int NNE, int NQP, int MODEL, bool ATOMIC, bool WANT_K, bool DENSE, int TEP = Tile<NNE>::TE>
+__global__ void __launch_bounds__(TEP *NNE)
     k_assemble(const AsmArgs args) {
-  constexpr int TE = Tile<NNE>::TE;
+  constexpr int TE = TEP;
   constexpr bool PLASTIC = (MODEL == 1);
   extern __shared__ double smem[];
   double *sXU = smem;                             // [TE][NNE][6]
@@ -107,7 +115,17 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
 
   const long ntot = args.elist ? args.nlist : args.ne;
   const int tid = threadIdx.x;
-  for (long tile0 = (long)blockIdx.x * TE; tile0 < ntot; tile0 += (long)gridDim.x * TE) {
+  __shared__ long s_claim;
+  long claim_end = 0;  // work stealing: end of the current claim of tiles
+  long tile0 = (long)blockIdx.x * TE;
+  if (args.ticket) {
+    if (tid == 0) s_claim = (long)atomicAdd(args.ticket, (unsigned)args.grab) * TE;
+    __syncthreads();
+    tile0 = s_claim;
+    claim_end = tile0 + (long)args.grab * TE;
+    __syncthreads();
+  }
+  while (tile0 < ntot) {
     // ---------------- phase 0: stage node data ----------------
     const int el = tid / NNE, a = tid % NNE;
     const long ei = tile0 + el;
@@ -177,9 +195,10 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
             for (int j = 0; j < 3; j++)
               F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] +
                              dU[i * 3 + 1] * dXi[1 * 3 + j] + dU[i * 3 + 2] * dXi[2 * 3 + j];
-          if (args.F0)
+          const double *F0 = args.elem_group ? args.F0_tab + 9 * (long)args.elem_group[qel] : args.F0;
+          if (F0)
 #pragma unroll
-            for (int i = 0; i < 9; i++) F[i] += args.F0[i];
+            for (int i = 0; i < 9; i++) F[i] += F0[i];
         }
         const double J = ok ? det3(F) : -1.0;
         double Fi[9];
@@ -357,13 +376,26 @@ __global__ void __launch_bounds__(Tile<NNE>::TE *NNE)
       }
     }
     __syncthreads();
+    // next tile: the rest of this claim, then a new claim
+    if (args.ticket) {
+      tile0 += TE;
+      if (tile0 >= claim_end) {
+        if (tid == 0) s_claim = (long)atomicAdd(args.ticket, (unsigned)args.grab) * TE;
+        __syncthreads();
+        tile0 = s_claim;
+        claim_end = tile0 + (long)args.grab * TE;
+        __syncthreads();
+      }
+    } else {
+      tile0 += (long)gridDim.x * TE;
+    }
   }
 }
 
-template <int NNE, int NQP>
+template <int NNE, int NQP, int TEP = Tile<NNE>::TE>
 constexpr size_t asm_smem_bytes() {
-  return sizeof(double) * (size_t)Tile<NNE>::TE * (NNE * 6 + NQP * kRec + NQP * NNE * kVec) +
-         (size_t)Tile<NNE>::TE * NNE * (6 * sizeof(int) + NNE * sizeof(uint16_t));
+  return sizeof(double) * (size_t)TEP * (NNE * 6 + NQP * kRec + NQP * NNE * kVec) +
+         (size_t)TEP * NNE * (6 * sizeof(int) + NNE * sizeof(uint16_t));
 }
 
 }  // namespace pgb

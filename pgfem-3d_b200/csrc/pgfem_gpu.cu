@@ -83,6 +83,12 @@ struct pgfem_gpu_ctx {
   pgfem_mlp *cp_net = nullptr;
   int cp_warm_k = 0;
   unsigned long long *cp_fallbacks = nullptr;
+  // batches of independent meshes and the work-stealing schedule
+  int *elem_group = nullptr;
+  double *F0_tab = nullptr;
+  int ngroups = 0;
+  unsigned *sched_ticket = nullptr;
+  int sched_epb = 0, sched_grab = 0;  // elements per block (0: default), tiles per steal (0: static)
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -250,7 +256,8 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
                   c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
-                  c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks};
+                  c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab,
+                  c->sched_ticket};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -275,6 +282,8 @@ AsmArgs base_args(const pgfem_gpu_ctx *c) {
   a.status = c->status;
   a.mat = c->mat;
   a.shp = c->shp;
+  a.elem_group = c->elem_group;
+  a.F0_tab = c->F0_tab;
   return a;
 }
 
@@ -291,20 +300,24 @@ int grid_for(long nitems, int te, int per_sm) {
   return (int)std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm * 8));
 }
 
-template <int NNE, int NQP, int MODEL, bool ATOMIC, bool WANT_K, bool DENSE>
+template <int NNE, int NQP, int MODEL, bool ATOMIC, bool WANT_K, bool DENSE, int TEP = Tile<NNE>::TE>
 int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
-  constexpr size_t smem = asm_smem_bytes<NNE, NQP>();
-  auto kern = k_assemble<NNE, NQP, MODEL, ATOMIC, WANT_K, DENSE>;
+  constexpr size_t smem = asm_smem_bytes<NNE, NQP, TEP>();
+  auto kern = k_assemble<NNE, NQP, MODEL, ATOMIC, WANT_K, DENSE, TEP>;
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Tile<NNE>::TE * NNE, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TEP * NNE, smem));
   if (per_sm < 1) per_sm = 1;
-  const int grid = grid_for(nitems, Tile<NNE>::TE, per_sm);
-  kern<<<grid, Tile<NNE>::TE * NNE, smem, s>>>(a);
+  int grid = grid_for(nitems, TEP, per_sm);
+  if (a.ticket) {  // persistent: every CTA resident, tiles claimed from the ticket
+    CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), s));
+    grid = (int)std::max<long>(1, std::min<long>((nitems + TEP - 1) / TEP, (long)g_num_sms * per_sm));
+  }
+  kern<<<grid, TEP * NNE, smem, s>>>(a);
   CK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }
@@ -457,6 +470,23 @@ int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t
   // the column-split kernel
   if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS"))
     return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
+  // linear tets over all elements: the tuned schedule (elements per block,
+  // work stealing)
+  if (c->nne == 4 && ATOMIC && !DENSE && !a.elist && (c->sched_epb || c->sched_grab)) {
+    AsmArgs b = a;
+    if (c->sched_grab > 0) {
+      b.ticket = c->sched_ticket;
+      b.grab = c->sched_grab;
+    }
+    if (c->sched_epb == 16)
+      return c->model == PGFEM_MODEL_J2 ? launch_asm<4, 1, 1, true, WANT_K, false, 16>(b, nitems, s)
+                                        : launch_asm<4, 1, 0, true, WANT_K, false, 16>(b, nitems, s);
+    if (c->sched_epb == 64)
+      return c->model == PGFEM_MODEL_J2 ? launch_asm<4, 1, 1, true, WANT_K, false, 64>(b, nitems, s)
+                                        : launch_asm<4, 1, 0, true, WANT_K, false, 64>(b, nitems, s);
+    return c->model == PGFEM_MODEL_J2 ? launch_asm<4, 1, 1, true, WANT_K, false>(b, nitems, s)
+                                      : launch_asm<4, 1, 0, true, WANT_K, false>(b, nitems, s);
+  }
   if (c->nne == 4) {
     switch (c->model) {
       case PGFEM_MODEL_HE: return launch_asm<4, 1, 0, ATOMIC, WANT_K, DENSE>(a, nitems, s);
@@ -1153,6 +1183,144 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
   if (r) return r;
   if (nqp == 0) return PGFEM_GPU_OK;
   return cm_integrate_host(make_mat(mat), nqp, F, dt, state_n, state_np1, S, L, qp_status);
+}
+
+
+// ---- batches of independent meshes, schedule, graph capture, autotuner ----
+
+int pgfem_gpu_set_mesh_groups(pgfem_gpu_ctx *c, int ngroups, const long *elem_off, const double *F0) {
+  if (!c || ngroups < 1 || !elem_off || !F0 || c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  if (elem_off[0] != 0 || elem_off[ngroups] != c->ne) return PGFEM_GPU_EINVAL;
+  std::vector<int> grp(c->ne);
+  for (int g = 0; g < ngroups; g++) {
+    if (elem_off[g + 1] < elem_off[g]) return PGFEM_GPU_EINVAL;
+    for (long e = elem_off[g]; e < elem_off[g + 1]; e++) grp[e] = g;
+  }
+  if (c->elem_group) cudaFree(c->elem_group);
+  if (c->F0_tab) cudaFree(c->F0_tab);
+  c->elem_group = nullptr;
+  c->F0_tab = nullptr;
+  int r;
+  if ((r = upload(c, &c->elem_group, grp.data(), grp.size())) ||
+      (r = upload(c, &c->F0_tab, F0, (size_t)9 * ngroups)))
+    return r;
+  CK(cudaStreamSynchronize(c->stream));
+  c->ngroups = ngroups;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_schedule(pgfem_gpu_ctx *c, int elems_per_block, int grab) {
+  if (!c || grab < 0 || (elems_per_block != 0 && elems_per_block != 16 && elems_per_block != 32 &&
+                         elems_per_block != 64))
+    return PGFEM_GPU_EINVAL;
+  if ((elems_per_block || grab) && c->nne != 4) return PGFEM_GPU_EINVAL;
+  if (grab > 0 && !c->sched_ticket) {
+    int r = dalloc(c, &c->sched_ticket, 1);
+    if (r) return r;
+  }
+  c->sched_epb = elems_per_block;
+  c->sched_grab = grab;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_get_schedule(const pgfem_gpu_ctx *c, int *elems_per_block, int *grab) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  if (elems_per_block) *elems_per_block = c->sched_epb;
+  if (grab) *grab = c->sched_grab;
+  return PGFEM_GPU_OK;
+}
+
+struct pgfem_gpu_graph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+int pgfem_gpu_graph_create(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double dt, double *d_R,
+                           double *d_K, pgfem_gpu_graph **out) {
+  if (!c || !d_u || !d_R || !d_K || !out) return PGFEM_GPU_EINVAL;
+  *out = nullptr;
+  const bool timing = c->timing;
+  c->timing = false;  // no event bookkeeping inside the captured work
+  // one uncaptured call sets the kernels' attributes before capture
+  int r = assemble_device(c, d_u, d_presc, d_R, d_K, c->stream, dt);
+  if (!r && cudaStreamSynchronize(c->stream) != cudaSuccess) r = PGFEM_GPU_ECUDA;
+  pgfem_gpu_graph *g = nullptr;
+  if (!r) {
+    g = new pgfem_gpu_graph();
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) r = PGFEM_GPU_ECUDA;
+    if (!r) {
+      const int ra = assemble_device(c, d_u, d_presc, d_R, d_K, c->stream, dt);
+      const cudaError_t ce = cudaStreamEndCapture(c->stream, &g->graph);
+      r = ra ? ra : (ce != cudaSuccess ? PGFEM_GPU_ECUDA : PGFEM_GPU_OK);
+    }
+    if (!r && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) r = PGFEM_GPU_ECUDA;
+  }
+  c->timing = timing;
+  if (r) {
+    cudaGetLastError();
+    if (g) {
+      if (g->exec) cudaGraphExecDestroy(g->exec);
+      if (g->graph) cudaGraphDestroy(g->graph);
+      delete g;
+    }
+    return r;
+  }
+  *out = g;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_graph_launch(pgfem_gpu_graph *g, void *stream) {
+  if (!g || !g->exec) return PGFEM_GPU_EINVAL;
+  CK(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_graph_destroy(pgfem_gpu_graph *g) {
+  if (!g) return PGFEM_GPU_OK;
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_autotune(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double dt, double *d_R,
+                       double *d_K, int reps, int *best_epb, int *best_grab, double *best_ms) {
+  if (!c || c->nne != 4 || reps < 1) return PGFEM_GPU_EINVAL;
+  const int epbs[] = {16, 32, 64};
+  const int grabs[] = {1, 2, 4, 8, 16};
+  double bms = 1e300;
+  int be = 32, bg = 1;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int r = PGFEM_GPU_OK;
+  for (int ie = 0; ie < 3 && !r; ie++)
+    for (int ig = 0; ig < 5 && !r; ig++) {
+      if ((r = pgfem_gpu_set_schedule(c, epbs[ie], grabs[ig]))) break;
+      pgfem_gpu_graph *g = nullptr;
+      if ((r = pgfem_gpu_graph_create(c, d_u, d_presc, dt, d_R, d_K, &g))) break;
+      for (int w = 0; w < 2 && !r; w++) r = pgfem_gpu_graph_launch(g, c->stream);
+      if (!r && (cudaEventRecord(e0, c->stream) != cudaSuccess)) r = PGFEM_GPU_ECUDA;
+      for (int k = 0; k < reps && !r; k++) r = pgfem_gpu_graph_launch(g, c->stream);
+      float ms = 0.f;
+      if (!r && (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                 cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        r = PGFEM_GPU_ECUDA;
+      pgfem_gpu_graph_destroy(g);
+      if (!r && ms / reps < bms) {
+        bms = ms / reps;
+        be = epbs[ie];
+        bg = grabs[ig];
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (r) return r;
+  if ((r = pgfem_gpu_set_schedule(c, be, bg))) return r;
+  if (best_epb) *best_epb = be;
+  if (best_grab) *best_grab = bg;
+  if (best_ms) *best_ms = bms;
+  return PGFEM_GPU_OK;
 }
 
 }  // extern "C"

@@ -106,6 +106,13 @@ def lib():
             "pgfem_gpu_set_cp_surrogate": (C.c_int, [_P, _P]),
             "pgfem_gpu_cp_training_pairs": (C.c_int, [_P, _P, _P]),
             "pgfem_gpu_get_cp_fallbacks": (C.c_int, [_P, _P]),
+            "pgfem_gpu_set_mesh_groups": (C.c_int, [_P, C.c_int, _P, _P]),
+            "pgfem_gpu_set_schedule": (C.c_int, [_P, C.c_int, C.c_int]),
+            "pgfem_gpu_get_schedule": (C.c_int, [_P, _P, _P]),
+            "pgfem_gpu_graph_create": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, _P]),
+            "pgfem_gpu_graph_launch": (C.c_int, [_P, _P]),
+            "pgfem_gpu_graph_destroy": (C.c_int, [_P]),
+            "pgfem_gpu_autotune": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, C.c_int, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -305,6 +312,33 @@ class Context:
         _check("pgfem_gpu_get_cp_fallbacks", lib().pgfem_gpu_get_cp_fallbacks(self.h, C.byref(n)))
         return n.value
 
+    def set_mesh_groups(self, elem_off, F0):
+        eo = np.ascontiguousarray(elem_off, dtype=np.int64)
+        f0 = np.ascontiguousarray(F0, dtype=np.float64).reshape(-1, 9)
+        assert len(eo) == len(f0) + 1
+        _check("pgfem_gpu_set_mesh_groups", lib().pgfem_gpu_set_mesh_groups(self.h, len(f0), _ptr(eo), _ptr(f0)))
+
+    def set_schedule(self, elems_per_block=0, grab=0):
+        _check("pgfem_gpu_set_schedule", lib().pgfem_gpu_set_schedule(self.h, elems_per_block, grab))
+
+    def schedule(self):
+        e, g = C.c_int(), C.c_int()
+        _check("pgfem_gpu_get_schedule", lib().pgfem_gpu_get_schedule(self.h, C.byref(e), C.byref(g)))
+        return e.value, g.value
+
+    def graph_create(self, d_u, d_presc, d_R, d_K, dt=0.0):
+        """CUDA graph of one R+K assembly on device buffers (raw addresses)."""
+        g = C.c_void_p()
+        _check("pgfem_gpu_graph_create", lib().pgfem_gpu_graph_create(self.h, d_u, d_presc, dt, d_R, d_K,
+                                                                      C.byref(g)))
+        return Graph(g)
+
+    def autotune(self, d_u, d_presc, d_R, d_K, reps=3, dt=0.0):
+        e, g, ms = C.c_int(), C.c_int(), C.c_double()
+        _check("pgfem_gpu_autotune", lib().pgfem_gpu_autotune(self.h, d_u, d_presc, dt, d_R, d_K, reps, C.byref(e),
+                                                              C.byref(g), C.byref(ms)))
+        return e.value, g.value, ms.value
+
     def read_status(self, clear=False):
         st = Status()
         _check("pgfem_gpu_read_status", lib().pgfem_gpu_read_status(self.h, C.byref(st), int(clear)))
@@ -441,3 +475,23 @@ class Mlp:
         _check("pgfem_mlp_train_device", lib().pgfem_mlp_train_device(self.h, n, d_x, d_t, C.byref(o),
                                                                       _ptr(hist)))
         return hist[:epochs]
+
+
+class Graph:
+    """A captured assembly (pgfem_gpu_graph_*)."""
+
+    def __init__(self, h):
+        self.h = h
+
+    def launch(self, stream=None):
+        _check("pgfem_gpu_graph_launch", lib().pgfem_gpu_graph_launch(self.h, stream))
+
+    def destroy(self):
+        if self.h:
+            lib().pgfem_gpu_graph_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.pgfem_gpu_graph_destroy(self.h)
+            self.h = None

@@ -227,3 +227,76 @@ def fcc_slip_systems():
     s = D.reshape(12, 3)
     n = np.repeat(N, 3, axis=0)
     return s, n
+
+
+# ------------------------------------------------------------ FE2 RVE batch --
+RVE_SEED = 3
+
+
+class RveBatch(Problem):
+    """Independent periodic unit cells (FE2 micro-structures) held as one mesh:
+    nodes, elements and DOFs of RVE r occupy the ranges node_off[r]..,
+    elem_off[r].., dof_off[r]..; the CSR pattern is block diagonal; RVE r sees
+    the macro deformation F0s[r] (F = I + grad u + F0s[r])."""
+
+    def rve(self, r):
+        """RVE r on its own (local numbering), for per-RVE reference checks."""
+        n0, n1 = self.node_off[r], self.node_off[r + 1]
+        e0, e1 = self.elem_off[r], self.elem_off[r + 1]
+        d0, d1 = self.dof_off[r], self.dof_off[r + 1]
+        conn = (self.conn[e0:e1] - n0).astype(np.int32)
+        ids = self.ids[n0:n1].copy()
+        ids[ids > 0] -= d0
+        Ap = (self.Ap[d0:d1 + 1] - self.Ap[d0]).astype(np.int32)
+        Ai = (self.Ai[self.Ap[d0]:self.Ap[d1]] - d0).astype(np.int32)
+        state = None if self.state is None else self.state[e0:e1]
+        return Problem("%s_rve%d" % (self.name, r), self.X[n0:n1], conn, ids, d1 - d0, Ap, Ai, self.mat,
+                       self.u[d0:d1].copy(), state=state, F0=self.F0s[r].copy(), meta=dict(n=int(self.n_r[r])))
+
+    def context(self):
+        ctx = super().context()
+        ctx.set_mesh_groups(self.elem_off, self.F0s)
+        return ctx
+
+
+def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3):
+    """Config 5: nrve periodic unit cubes, n_r^3 cells x 6 linear tets with n_r
+    uniform in nmin..nmax, macro F0 = sym(U(-0.02, 0.02)^{3x3}) per RVE, a
+    seeded periodic fluctuation field of amplitude fluct * h_r, J2 material
+    (E 200 GPa, nu 0.3, yield 250 MPa, H 2 GPa), state at identity."""
+    ns = nmin + np.minimum((splitmix64(seed, nrve, stream=7) * (nmax - nmin + 1)).astype(np.int64),
+                           nmax - nmin)
+    Xs, conns, idss, node_off, elem_off, dof_off = [], [], [], [0], [0], [0]
+    for r, n in enumerate(ns):
+        X, conn, Pr = pg.mesh_box_tet(int(n), 4, periodic=True)
+        nn = X.shape[0]
+        ids, ndof = pg.generate_dof_ids(conn, nn, np.zeros((nn, 3), dtype=np.int64), Pr=Pr)
+        Xs.append(X)
+        conns.append(conn.astype(np.int64) + node_off[-1])
+        ids = ids.copy()
+        ids[ids > 0] += dof_off[-1]
+        idss.append(ids)
+        node_off.append(node_off[-1] + nn)
+        elem_off.append(elem_off[-1] + conn.shape[0])
+        dof_off.append(dof_off[-1] + ndof)
+    X = np.concatenate(Xs)
+    conn = np.concatenate(conns).astype(np.int32)
+    ids = np.concatenate(idss)
+    ndof = dof_off[-1]
+    Ap, Ai = pg.psparse_apai(conn, ids, ndof)
+    A = (2.0 * splitmix64(seed, 9 * nrve, stream=8) - 1.0).reshape(nrve, 3, 3) * 0.02
+    F0s = (0.5 * (A + np.transpose(A, (0, 2, 1)))).reshape(nrve, 9)
+    # periodic fluctuation: one value per free DOF, scaled by the RVE's cell size
+    hs = np.repeat(1.0 / ns, np.diff(dof_off))
+    u = (2.0 * splitmix64(seed, ndof, stream=9) - 1.0) * fluct * hs
+    mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
+    state = np.zeros((conn.shape[0], 10))
+    state[:, [0, 4, 8]] = 1.0
+    p = RveBatch("rve_batch_%d" % nrve, X, conn, ids, ndof, Ap, Ai, mat, u, state=state,
+                 meta=dict(nrve=nrve, seed=seed, nmin=nmin, nmax=nmax))
+    p.n_r = ns
+    p.node_off = np.array(node_off, dtype=np.int64)
+    p.elem_off = np.array(elem_off, dtype=np.int64)
+    p.dof_off = np.array(dof_off, dtype=np.int64)
+    p.F0s = F0s
+    return p
