@@ -96,7 +96,9 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
-def dist_setup(ngpus):
+def dist_setup(ngpus, backend=None):
+    """One process per GPU (torchrun environment).  The backend is NCCL on the
+    GPUs; `gloo` (or PGFEM_DIST_BACKEND=gloo) runs the same host logic on CPU."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -105,19 +107,44 @@ def dist_setup(ngpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
+        backend = backend or os.environ.get("PGFEM_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
 
 
 def allreduce_max(x, ws):
+    """Max over ranks (device timings are reported as the slowest rank's)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rve_shard(nrve, ws, rank):
+    """RVEs assembled by `rank`: a contiguous block of the batch, sizes within
+    one of each other (the RVEs are independent: no data-path collective)."""
+    base, extra = divmod(nrve, ws)
+    lo = rank * base + min(rank, extra)
+    return list(range(lo, lo + base + (1 if rank < extra else 0)))
+
+
+def allreduce_sum(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -494,9 +521,10 @@ def run_rve(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     t0 = time.perf_counter()
-    p = wl.rve_batch(nrve=args.nrve)
-    log("[rank %d] %d RVEs: %d elements, %d DOFs, %d nnz, built in %.1f s"
-        % (rank, args.nrve, p.ne, p.ndof, p.nnz, time.perf_counter() - t0))
+    shard = rve_shard(args.nrve, ws, rank)
+    p = wl.rve_batch(nrve=args.nrve, subset=shard)
+    log("[rank %d] RVEs %d..%d of %d: %d elements, %d DOFs, %d nnz, built in %.1f s"
+        % (rank, shard[0], shard[-1], args.nrve, p.ne, p.ndof, p.nnz, time.perf_counter() - t0))
     ctx = p.context()
     fp64_peak = pg.fp64_peak_tflops()
     hbm_peak, hbm_src = measured_hbm_gbs()
@@ -592,10 +620,13 @@ def run_rve(args, ws, rank, local):
                 "peak_source": hbm_src}
     roof.update({"frac": roof["achieved"] / roof["peak"], "traffic": None, "kernel_ms": k_ms,
                  "roofline_ms": 1e3 * max(t_fp64, t_hbm), "alg_flops": flops, "alg_bytes": nbytes})
-    out = {"metric": METRIC, "value": ws * p.nqp / (ms_step * 1e-3), "unit": UNIT, "n_gpus": ws,
+    nqp_all = allreduce_sum(p.nqp, ws)
+    out = {"metric": METRIC, "value": nqp_all / (ms_step * 1e-3), "unit": UNIT, "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64)",
-           "config": {"workload": "FE2 micro-RVE batch: %d periodic unit cells, n^3 cells x 6 linear tets with n "
+           "scaling": "strong" if ws > 1 else "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded splitmix64)",
+           "config": {"parallelism": "RVEs sharded over %d ranks, no collective" % ws if ws > 1 else "1 GPU",
+                      "workload": "FE2 micro-RVE batch: %d periodic unit cells, n^3 cells x 6 linear tets with n "
                                   "uniform in 8..24 (%d elements, %d DOFs, %d nnz), J2, per-RVE macro F = I + "
                                   "sym(U(-0.02, 0.02)), one R+K iterate per step as one persistent work-stealing "
                                   "launch replayed from a CUDA graph" % (args.nrve, p.ne, p.ndof, p.nnz),
@@ -604,7 +635,7 @@ def run_rve(args, ws, rank, local):
                       "rve_checks_vs_oracle": checks,
                       "l2": "inputs larger than L2 (K values %.2f GB)" % (8e-9 * p.nnz)},
            "roofline": roof, "clocks": clocks,
-           "e2e": {"value": ws * p.nqp * n_e2e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
+           "e2e": {"value": nqp_all * n_e2e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
                    "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "steps": n_e2e},
            "gpu_launches": args.steps * ctx.launches_per_assembly()}
     ctx.close()

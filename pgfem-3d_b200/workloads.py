@@ -259,15 +259,21 @@ class RveBatch(Problem):
         return ctx
 
 
-def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3):
+def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3, subset=None):
     """Config 5: nrve periodic unit cubes, n_r^3 cells x 6 linear tets with n_r
     uniform in nmin..nmax, macro F0 = sym(U(-0.02, 0.02)^{3x3}) per RVE, a
     seeded periodic fluctuation field of amplitude fluct * h_r, J2 material
-    (E 200 GPa, nu 0.3, yield 250 MPa, H 2 GPa), state at identity."""
-    ns = nmin + np.minimum((splitmix64(seed, nrve, stream=7) * (nmax - nmin + 1)).astype(np.int64),
-                           nmax - nmin)
+    (E 200 GPa, nu 0.3, yield 250 MPa, H 2 GPa), state at identity.
+    subset: indices of the RVEs to build (a rank's shard); sizes, macro
+    deformations and fluctuations are those of the full batch."""
+    ns_all = nmin + np.minimum((splitmix64(seed, nrve, stream=7) * (nmax - nmin + 1)).astype(np.int64),
+                               nmax - nmin)
+    A_all = (2.0 * splitmix64(seed, 9 * nrve, stream=8) - 1.0).reshape(nrve, 3, 3) * 0.02
+    sel = np.arange(nrve) if subset is None else np.asarray(subset, dtype=np.int64)
+    ns = ns_all[sel]
     Xs, conns, idss, node_off, elem_off, dof_off = [], [], [], [0], [0], [0]
-    for r, n in enumerate(ns):
+    us = []
+    for r, n in zip(sel, ns):
         X, conn, Pr = pg.mesh_box_tet(int(n), 4, periodic=True)
         nn = X.shape[0]
         ids, ndof = pg.generate_dof_ids(conn, nn, np.zeros((nn, 3), dtype=np.int64), Pr=Pr)
@@ -279,21 +285,22 @@ def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3):
         node_off.append(node_off[-1] + nn)
         elem_off.append(elem_off[-1] + conn.shape[0])
         dof_off.append(dof_off[-1] + ndof)
+        # periodic fluctuation: one value per free DOF, scaled by the cell size,
+        # from a stream keyed by the RVE's index in the full batch
+        us.append((2.0 * splitmix64(seed * 1000003 + int(r), ndof, stream=9) - 1.0) * fluct / float(n))
     X = np.concatenate(Xs)
     conn = np.concatenate(conns).astype(np.int32)
     ids = np.concatenate(idss)
     ndof = dof_off[-1]
     Ap, Ai = pg.psparse_apai(conn, ids, ndof)
-    A = (2.0 * splitmix64(seed, 9 * nrve, stream=8) - 1.0).reshape(nrve, 3, 3) * 0.02
-    F0s = (0.5 * (A + np.transpose(A, (0, 2, 1)))).reshape(nrve, 9)
-    # periodic fluctuation: one value per free DOF, scaled by the RVE's cell size
-    hs = np.repeat(1.0 / ns, np.diff(dof_off))
-    u = (2.0 * splitmix64(seed, ndof, stream=9) - 1.0) * fluct * hs
+    A = A_all[sel]
+    F0s = (0.5 * (A + np.transpose(A, (0, 2, 1)))).reshape(len(sel), 9)
+    u = np.concatenate(us)
     mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
     state = np.zeros((conn.shape[0], 10))
     state[:, [0, 4, 8]] = 1.0
     p = RveBatch("rve_batch_%d" % nrve, X, conn, ids, ndof, Ap, Ai, mat, u, state=state,
-                 meta=dict(nrve=nrve, seed=seed, nmin=nmin, nmax=nmax))
+                 meta=dict(nrve=nrve, seed=seed, nmin=nmin, nmax=nmax, subset=sel.tolist()))
     p.n_r = ns
     p.node_off = np.array(node_off, dtype=np.int64)
     p.elem_off = np.array(elem_off, dtype=np.int64)
