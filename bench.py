@@ -202,7 +202,8 @@ def run_ours(args, ws, rank, local):
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
     t0 = time.perf_counter()
-    p = wl.j2_p2(n=args.n, seed=1)
+    he = args.workload == "he_p1"
+    p = wl.he_p1(n=10, seed=0) if he else wl.j2_p2(n=args.n, seed=1)
     log("[rank %d] setup (mesh, DOFs, CSR pattern %d nnz) %.1f s" % (rank, p.nnz, time.perf_counter() - t0))
     t0 = time.perf_counter()
     ctx = p.context()
@@ -254,7 +255,7 @@ def run_ours(args, ws, rank, local):
     ms_total = allreduce_max(ms_total, ws)
     ms_step = ms_total / args.steps
     value = ws * p.nqp * args.steps / (ms_total * 1e-3)
-    yielded = float((ctx.get_state(1)[:, 9] > 0).mean())
+    yielded = None if he else float((ctx.get_state(1)[:, 9] > 0).mean())
 
     # end to end through the host-buffer entry point (pinned host memory)
     u_h = torch.from_numpy(p.u).pin_memory().numpy()
@@ -272,7 +273,7 @@ def run_ours(args, ws, rank, local):
 
     # roofline of the dominant kernel (the fused assembly kernel)
     k_ms = kms / max(kcalls, 1)
-    flops = FLOP_PER_QP * p.nqp
+    flops = (2.5e3 if he else FLOP_PER_QP) * p.nqp
     nbytes = alg_bytes(p.X.shape[0], p.ndof, p.ne, p.nqp, p.nnz)
     t_fp64 = flops / (fp64_peak * 1e12)
     t_hbm = nbytes / (hbm_peak * 1e9)
@@ -296,9 +297,11 @@ def run_ours(args, ws, rank, local):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64)",
-           "config": {"workload": "J2 finite-strain plasticity, quadratic tets, %d^3 cells x 6 (%d elements, "
-                                  "%d quadrature points, %d DOFs, %d CSR non-zeros), one R+K iterate" %
-                                  (args.n, p.ne, p.nqp, p.ndof, p.nnz),
+           "config": {"workload": ("compressible neo-Hookean, linear tets, 10^3 cells x 6 (%d elements, %d DOFs, "
+                                   "%d CSR non-zeros), one R+K iterate" % (p.ne, p.ndof, p.nnz)) if he else
+                                  ("J2 finite-strain plasticity, quadratic tets, %d^3 cells x 6 (%d elements, "
+                                   "%d quadrature points, %d DOFs, %d CSR non-zeros), one R+K iterate" %
+                                   (args.n, p.ne, p.nqp, p.ndof, p.nnz)),
                       "elements": p.ne, "quad_points": p.nqp, "dofs": p.ndof, "nnz": p.nnz,
                       "yielded_fraction": yielded, "parallelism": "replicas%d" % ws if ws > 1 else "1 GPU",
                       "l2": "inputs larger than L2 (K values %.2f GB)" % (8e-9 * p.nnz),
@@ -501,6 +504,18 @@ def run_cp_warm(args, ws, rank, local):
                                   "epochs": args.train_epochs, "loss_first_last": [float(hist[0]), float(hist[-1])],
                                   "prediction_rel_err": pred_err}},
            "gpu_launches": args.steps * launches}
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        P, mat = oracle.from_workload(p)
+        sn = ctx.get_state(0)
+        S = 20000
+        t0 = time.perf_counter()
+        P.assemble(mat, u, state_n=sn, dt=p.dt, e1=S)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": S / t, "unit": UNIT, "cores": 1, "kind": "port",
+                               "sample": "first %d elements of the same step, reference element algorithm + "
+                                         "restated CP local Newton (cold start), 1 thread, %.1f s" % (S, t)}
     ctx.close()
     return out
 
@@ -592,6 +607,17 @@ def run_rve(args, ws, rank, local):
         checks.append({"rve": r, "n": int(p.n_r[r]),
                        "R_rel": float(np.linalg.norm(R_all[d0:d1] - Ro) / np.linalg.norm(Ro)),
                        "K_rel": float(np.linalg.norm(K_all[p.Ap[d0]:p.Ap[d1]] - Ko) / np.linalg.norm(Ko))})
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        q = p.rve(int(np.argmin(p.n_r)))
+        P, mat = oracle.from_workload(q)
+        t0 = time.perf_counter()
+        P.assemble(mat, q.u, state_n=q.state, nthreads=1)
+        t1 = time.perf_counter() - t0
+        cpu_base = {"value": q.nqp / t1, "unit": UNIT, "cores": 1, "kind": "port",
+                    "sample": "the smallest RVE (%d^3 cells, %d elements), reference element algorithm, 1 thread, "
+                              "%.2f s" % (q.meta["n"], q.ne, t1)}
+    else:
+        cpu_base = None
     # end to end: pinned host u in, R and K out, through the captured graph
     u_h = torch.from_numpy(p.u).pin_memory()
     R_h = torch.empty(p.ndof, dtype=torch.float64).pin_memory()
@@ -638,6 +664,8 @@ def run_rve(args, ws, rank, local):
            "e2e": {"value": nqp_all * n_e2e / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
                    "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "steps": n_e2e},
            "gpu_launches": args.steps * ctx.launches_per_assembly()}
+    if cpu_base:
+        out["cpu_baseline"] = cpu_base
     ctx.close()
     return out
 
@@ -691,7 +719,7 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles", "cells"])
-    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "cp_p1", "cp_warm", "rve_batch"])
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch"])
     ap.add_argument("--nrve", type=int, default=256)
     ap.add_argument("--train-n", type=int, default=32)
     ap.add_argument("--train-epochs", type=int, default=30)
