@@ -166,7 +166,7 @@ def measured_hbm_gbs():
 
 def traffic_per_launch():
     """dram bytes per launch of the assembly kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_assemble_j2_p2_traffic.txt")
+    path = os.path.join(ROOT, "profiles", "k_assemble_p2_j2_p2_traffic.txt")
     if not os.path.exists(path):
         return None
     for ln in open(path):
@@ -325,6 +325,42 @@ def run_ours(args, ws, rank, local):
     return out
 
 
+# Declared FP64 work of the CP local update (survey figures for this model):
+# one Newton iteration (residual with 12 power laws at 40 flop each, 10x10
+# Jacobian, LU solve, one line-search residual) and the per-point fixed work
+# (set-up, consistent dM/dF with 9 right-hand sides).
+FLOP_CP_ITER = 10.0e3
+FLOP_CP_POINT = 8.0e3
+
+
+def cp_roofline(kernel_ms, iters, nqp, fp64_peak):
+    flops = FLOP_CP_ITER * float(np.sum(iters)) + FLOP_CP_POINT * nqp
+    ach = flops / (kernel_ms * 1e-3) / 1e12
+    return {"bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+            "peak_source": "measured this run (FP64 FMA-chain probe, every SM)", "frac": ach / fp64_peak,
+            "traffic": None, "kernel": "k_cp_update (local Newton)", "kernel_ms": kernel_ms, "alg_flops": flops,
+            "flop_model": "%.0f per Newton iteration + %.0f per point" % (FLOP_CP_ITER, FLOP_CP_POINT)}
+
+
+def cp_e2e(ctx, p, u, ws, nsteps):
+    """Host-buffer path (pinned u in, R and K out) of the same R+K iterate."""
+    import torch
+    u_h = torch.from_numpy(u).pin_memory().numpy()
+    R_h = torch.empty(p.ndof, dtype=torch.float64).pin_memory().numpy()
+    K_h = torch.empty(p.nnz, dtype=torch.float64).pin_memory().numpy()
+    ctx.reset_state()
+    ctx.assemble_RK(u_h, dt=p.dt, R=R_h, K=K_h)
+    barrier(ws)
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        ctx.reset_state()
+        _, _, st = ctx.assemble_RK(u_h, dt=p.dt, R=R_h, K=K_h)
+    e2e_s = allreduce_max(time.perf_counter() - t0, ws)
+    assert st.ok(), st.as_dict()
+    return {"value": ws * p.nqp * nsteps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
+            "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "steps": nsteps}
+
+
 def run_cp(args, ws, rank, local):
     """Config 3: FCC crystal plasticity, 48^3 cells x 6 linear tets, one R+K
     iterate at load step `--cp-step` of the 1 % tension ramp (the state of the
@@ -358,8 +394,12 @@ def run_cp(args, ws, rank, local):
     torch.cuda.synchronize()
     st = ctx.read_status(clear=True)
     assert st.ok(), st.as_dict()
+    fp64_peak = pg.fp64_peak_tflops()
     ctx.set_timing(True)
     ctx.kernel_time(reset=True)
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
     barrier(ws)
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -369,8 +409,10 @@ def run_cp(args, ws, rank, local):
         step()
     e1.record(stream)
     torch.cuda.synchronize()
+    clocks = clk.stop()
     ms = allreduce_max(e0.elapsed_time(e1), ws)
     kms, kc = ctx.kernel_time(reset=True)
+    ctx.set_timing(False)
     it = ctx.cp_iterations()
     out = {"metric": METRIC, "value": ws * p.nqp * args.steps / (ms * 1e-3), "unit": UNIT, "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -379,7 +421,10 @@ def run_cp(args, ws, rank, local):
                                   "512 Voronoi grains, R+K at load step %d of %d (1 %% tension ramp, dt 0.1 s), "
                                   "cold-start local Newton to 1e-10" % (args.cp_n, p.ne, args.cp_step, wl.CP_STEPS),
                       "local_newton_ms": kms / max(kc, 1),
-                      "iterations_hist": np.bincount(it).tolist(), "iterations_mean": float(it.mean())},
+                      "iterations_hist": np.bincount(it).tolist(), "iterations_mean": float(it.mean()),
+                      "l2": "one R+K iterate touches 0.4 GB (K 0.12 GB, point records 0.55 GB) > L2"},
+           "roofline": cp_roofline(kms / max(kc, 1), it, p.nqp, fp64_peak), "clocks": clocks,
+           "e2e": cp_e2e(ctx, p, u, ws, max(1, min(args.steps, 3))),
            "gpu_launches": args.steps * ctx.launches_per_assembly()}
     if rank == 0 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -460,12 +505,17 @@ def run_cp_warm(args, ws, rank, local):
         assert st.ok(), st.as_dict()
         return ms / args.steps, kms / max(kc, 1), ctx.cp_iterations()
 
+    fp64_peak = pg.fp64_peak_tflops()
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
     ms_c, upd_c, it_c = timed()
     R_c = d_R.cpu().numpy()
     s_c = ctx.get_state(1)
     ctx.set_cp_warm_limit(args.warm_k)
     ctx.set_cp_surrogate(net)
     ms_w, upd_w, it_w = timed()
+    clocks = clk.stop()
     launches = ctx.launches_per_assembly()  # with the network attached
     fb = ctx.cp_fallbacks()
     R_w = d_R.cpu().numpy()
@@ -483,6 +533,8 @@ def run_cp_warm(args, ws, rank, local):
     net.predict_device(p.ne, xx.data_ptr(), yy.data_ptr(), sh)
     torch.cuda.synchronize()
     pred_err = float(torch.linalg.norm(yy - tt) / torch.linalg.norm(tt))
+    ctx.set_cp_surrogate(net)
+    e2e_w = cp_e2e(ctx, p, u, ws, max(1, min(args.steps, 3)))
     out = {"metric": METRIC, "value": ws * p.nqp / (ms_w * 1e-3), "unit": UNIT, "n_gpus": ws,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_w, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (network bf16 x bf16 -> f32)",
@@ -503,6 +555,7 @@ def run_cp_warm(args, ws, rank, local):
                                   "pair_generation_s": info["seconds"], "train_s": train_s,
                                   "epochs": args.train_epochs, "loss_first_last": [float(hist[0]), float(hist[-1])],
                                   "prediction_rel_err": pred_err}},
+           "roofline": cp_roofline(upd_w, it_w, p.nqp, fp64_peak), "clocks": clocks, "e2e": e2e_w,
            "gpu_launches": args.steps * launches}
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
