@@ -37,9 +37,12 @@ constexpr int kP2TE = 8;                      // elements per CTA iteration
 constexpr int kP2Threads = kP2TE * 10 * 3;    // (element, node, component)
 constexpr int kP2VS = 18;                     // doubles per (point, node) vector record
 constexpr int kP2Rec = 38;                    // doubles per point record
+// doubles per element in the vector records: 4 points x 10 nodes x 18, padded by
+// 6 so that the records of consecutive elements start 12 banks apart
+constexpr int kP2ES = 4 * 10 * kP2VS + 6;
 
 inline size_t p2_smem_bytes() {
-  return sizeof(double) * ((size_t)kP2TE * 10 * 6 + (size_t)kP2TE * 4 * kRec + (size_t)kP2TE * 4 * 10 * kP2VS +
+  return sizeof(double) * ((size_t)kP2TE * 10 * 6 + (size_t)kP2TE * 4 * kRec + (size_t)kP2TE * kP2ES +
                            (size_t)kP2TE * 4) +
          sizeof(int) * (size_t)kP2TE * 10 * 6 + sizeof(uint16_t) * (size_t)kP2TE * 100;
 }
@@ -51,8 +54,8 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
   extern __shared__ double smem[];
   double *sXU = smem;                          // [TE][NNE][6]
   double *sRec = sXU + TE * NNE * 6;           // [TE][NQP][kRec]
-  double *sVec = sRec + TE * NQP * kRec;       // [TE][NQP][NNE][VS]
-  double *sA1 = sVec + TE * NQP * NNE * VS;    // [TE][NQP]  w a1 / 2
+  double *sVec = sRec + TE * NQP * kRec;       // [TE][kP2ES]: [NQP][NNE][VS] per element
+  double *sA1 = sVec + TE * kP2ES;             // [TE][NQP]  w a1 / 2
   int *sMeta = reinterpret_cast<int *>(sA1 + TE * NQP);            // [TE*NNE][6]: mask, rp, rl, dof x3
   uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + TE * NNE * 6);  // [TE*NNE][NNE]
   const int tid = threadIdx.x;
@@ -181,7 +184,7 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
       for (int j = 0; j < 3; j++) p[j] = rec[0 * 3 + j] * g0 + rec[1 * 3 + j] * g1 + rec[2 * 3 + j] * g2;
       smv(rec + 16, p, sp);
       smv(rec + 10, p, tp);
-      double *v = sVec + it * VS;
+      double *v = sVec + (eq / NQP) * kP2ES + ((eq % NQP) * NNE + a) * VS;
 #pragma unroll
       for (int j = 0; j < 3; j++) {
         v[j] = p[j];
@@ -215,21 +218,53 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
       const int *mA = sMeta + (el * NNE + a) * 6;
       const unsigned maskA = (e < ne) ? (unsigned)mA[0] : 0u;
       if (maskA) {
-        // left vectors of node a at the four points (registers)
-        double pa[NQP][3], Sa[NQP][3], na[NQP][3], ha[NQP], Rk = 0.0;
+        // the diagonal term (p_a . T_b) 1 enters entry (k, k): weights instead
+        // of lane-dependent branches (the three lanes k of a warp stay converged)
+        const double ek0 = k == 0 ? 1.0 : 0.0, ek1 = k == 1 ? 1.0 : 0.0, ek2 = k == 2 ? 1.0 : 0.0;
+        // points outer, the 10 column nodes inner: 30 independent accumulators
+        double acc[NNE][3];
 #pragma unroll
+        for (int b = 0; b < NNE; b++) acc[b][0] = acc[b][1] = acc[b][2] = 0.0;
+        double Rk = 0.0;
+#pragma unroll 1
         for (int q = 0; q < NQP; q++) {
-          const double *L = sVec + ((el * NQP + q) * NNE + a) * VS;
-          const double a1h = sA1[el * NQP + q];
+          const double *base = sVec + el * kP2ES + q * NNE * VS;
+          const double *L = base + a * VS;
+          const double2 l01 = *reinterpret_cast<const double2 *>(L);
+          const double pa0 = l01.x, pa1 = l01.y, pa2 = L[2];
+          const double2 s01 = *reinterpret_cast<const double2 *>(L + 12);
+          const double2 s2n0 = *reinterpret_cast<const double2 *>(L + 14);
+          const double2 n12 = *reinterpret_cast<const double2 *>(L + 16);
+          const double pak = L[k];
+          const double ha = sA1[el * NQP + q] * pak;
+          Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
 #pragma unroll
-          for (int j = 0; j < 3; j++) {
-            pa[q][j] = L[j];
-            Sa[q][j] = L[12 + j];
-            na[q][j] = PLASTIC ? L[15 + j] : 0.0;
+          for (int b = 0; b < NNE; b++) {
+            const double *Rv = base + b * VS;
+            const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
+            const double pb2 = Rv[2];
+            const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
+            const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
+            const double dg = pa0 * Rv[9] + pa1 * t01.x + pa2 * t01.y;
+            double x0 = acc[b][0], x1 = acc[b][1], x2 = acc[b][2];
+            x0 = fma(r0.x, ha, x0);
+            x1 = fma(r0.y, ha, x1);
+            x2 = fma(pb2, ha, x2);
+            x0 = fma(pa0, Uk, x0);
+            x1 = fma(pa1, Uk, x1);
+            x2 = fma(pa2, Uk, x2);
+            x0 = fma(s01.x, pbk, x0);
+            x1 = fma(s01.y, pbk, x1);
+            x2 = fma(s2n0.x, pbk, x2);
+            if (PLASTIC) {
+              x0 = fma(s2n0.y, Wk, x0);
+              x1 = fma(n12.x, Wk, x1);
+              x2 = fma(n12.y, Wk, x2);
+            }
+            acc[b][0] = fma(ek0, dg, x0);
+            acc[b][1] = fma(ek1, dg, x1);
+            acc[b][2] = fma(ek2, dg, x2);
           }
-          const double pk = k == 0 ? pa[q][0] : (k == 1 ? pa[q][1] : pa[q][2]);
-          ha[q] = a1h * pk;
-          Rk += L[9 + k] - ha[q];  // w tau p_a = T_a - a1/2 w p_a
         }
         // residual component k of node a
         {
@@ -238,39 +273,15 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
         }
         const long rp = mA[1], rl = mA[2];
         const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
-#pragma unroll 1
+#pragma unroll
         for (int b = 0; b < NNE; b++) {
           const unsigned maskB = (unsigned)sMeta[(el * NNE + b) * 6];
-          double acc[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-          for (int q = 0; q < NQP; q++) {
-            const double *Rv = sVec + ((el * NQP + q) * NNE + b) * VS;
-            const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
-            const double pb[3] = {r0.x, r0.y, Rv[2]};
-            const double Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
-            const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
-            const double T[3] = {Rv[9], t01.x, t01.y};
-            const double pbk = k == 0 ? pb[0] : (k == 1 ? pb[1] : pb[2]);
-            const double dg = pa[q][0] * T[0] + pa[q][1] * T[1] + pa[q][2] * T[2];
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-              double v = acc[i];
-              v = fma(pb[i], ha[q], v);
-              v = fma(pa[q][i], Uk, v);
-              v = fma(Sa[q][i], pbk, v);
-              if (PLASTIC) v = fma(na[q][i], Wk, v);
-              acc[i] = v;
-            }
-            if (k == 0) acc[0] += dg;
-            else if (k == 1) acc[1] += dg;
-            else acc[2] += dg;
-          }
           if (!((maskB >> k) & 1u)) continue;
           const long col = rp + posrow[b] + rank_of(maskB, k);
 #pragma unroll
           for (int i = 0; i < 3; i++) {
             if (!((maskA >> i) & 1u)) continue;
-            atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[i]);
+            atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[b][i]);
           }
         }
       }
