@@ -41,54 +41,105 @@ constexpr int kP2Rec = 38;                    // doubles per point record
 // 6 so that the records of consecutive elements start 12 banks apart
 constexpr int kP2ES = 4 * 10 * kP2VS + 6;
 
+// shared memory: node data, J2 state and row metadata of two tiles (the tile
+// being assembled and the prefetched next one), point records, vector records
+constexpr int kP2XU = kP2TE * 10 * 6;     // doubles per node-data buffer
+constexpr int kP2ST = kP2TE * 4 * 7;      // doubles per state buffer
+constexpr int kP2MT = kP2TE * 10 * 7;     // ints per metadata buffer: mask word, rp, rl, dof x3, mask shift
+constexpr int kP2PS = kP2TE * 10 * 10;    // uint16 per position buffer
+
 inline size_t p2_smem_bytes() {
-  return sizeof(double) * ((size_t)kP2TE * 10 * 6 + (size_t)kP2TE * 4 * kRec + (size_t)kP2TE * kP2ES +
-                           (size_t)kP2TE * 4) +
-         sizeof(int) * (size_t)kP2TE * 10 * 6 + sizeof(uint16_t) * (size_t)kP2TE * 100;
+  return sizeof(double) * (2 * (size_t)kP2XU + 2 * (size_t)kP2ST + (size_t)kP2TE * 4 * kRec +
+                           (size_t)kP2TE * kP2ES + (size_t)kP2TE * 4) +
+         sizeof(int) * 2 * (size_t)kP2MT + sizeof(uint16_t) * 2 * (size_t)kP2PS;
 }
+
+__device__ __forceinline__ void cpa4(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa8(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 template <int MODEL>
 __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs args) {
   constexpr int NNE = 10, NQP = 4, TE = kP2TE, VS = kP2VS;
   constexpr bool PLASTIC = (MODEL == 1);
   extern __shared__ double smem[];
-  double *sXU = smem;                          // [TE][NNE][6]
-  double *sRec = sXU + TE * NNE * 6;           // [TE][NQP][kRec]
+  double *sXUb = smem;                         // [2][TE][NNE][6]
+  double *sStb = sXUb + 2 * kP2XU;             // [2][TE][NQP][7] state at t_n
+  double *sRec = sStb + 2 * kP2ST;             // [TE][NQP][kRec]
   double *sVec = sRec + TE * NQP * kRec;       // [TE][kP2ES]: [NQP][NNE][VS] per element
   double *sA1 = sVec + TE * kP2ES;             // [TE][NQP]  w a1 / 2
-  int *sMeta = reinterpret_cast<int *>(sA1 + TE * NQP);            // [TE*NNE][6]: mask, rp, rl, dof x3
-  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + TE * NNE * 6);  // [TE*NNE][NNE]
+  int *sMetab = reinterpret_cast<int *>(sA1 + TE * NQP);                // [2][TE*NNE][7]
+  uint16_t *sPosb = reinterpret_cast<uint16_t *>(sMetab + 2 * kP2MT);  // [2][TE*NNE][NNE]
   const int tid = threadIdx.x;
   const long ne = args.ne;
+  const long stride = (long)gridDim.x * TE;
 
-  for (long tile0 = (long)blockIdx.x * TE; tile0 < ne; tile0 += (long)gridDim.x * TE) {
-    // ---------------- 0: node data and row metadata ----------------
+  // asynchronous copy of tile t1's node data, row metadata and state into
+  // buffer `buf` (node = this thread's element node of that tile)
+  auto prefetch = [&](long t1, int buf, int node) {
     if (tid < TE * NNE) {
       const int el = tid / NNE, a = tid - el * NNE;
-      const long e = tile0 + el;
-      if (e < ne) {
-        const int node = args.conn[(long)a * ne + e];
-        double *d = sXU + tid * 6;
-        d[0] = args.X[node];
-        d[1] = args.X[args.nn + node];
-        d[2] = args.X[2 * args.nn + node];
-        d[3] = args.unode[node];
-        d[4] = args.unode[args.nn + node];
-        d[5] = args.unode[2 * args.nn + node];
-        int *m = sMeta + tid * 6;
-        m[0] = args.mask[node];
-        m[1] = args.rowptr0[node];
-        m[2] = args.rowlen[node];
-        m[3] = args.dof[node];
-        m[4] = args.dof[args.nn + node];
-        m[5] = args.dof[2 * args.nn + node];
+      const long e = t1 + el;
+      if (e < ne && node >= 0) {
+        double *d = sXUb + buf * kP2XU + tid * 6;
+        cpa8(d + 0, args.X + node);
+        cpa8(d + 1, args.X + args.nn + node);
+        cpa8(d + 2, args.X + 2 * args.nn + node);
+        cpa8(d + 3, args.unode + node);
+        cpa8(d + 4, args.unode + args.nn + node);
+        cpa8(d + 5, args.unode + 2 * args.nn + node);
+        int *m = sMetab + buf * kP2MT + tid * 7;
+        cpa4(m + 0, args.mask + (node & ~3));  // the aligned word holding the mask byte
+        cpa4(m + 1, args.rowptr0 + node);
+        cpa4(m + 2, args.rowlen + node);
+        cpa4(m + 3, args.dof + node);
+        cpa4(m + 4, args.dof + args.nn + node);
+        cpa4(m + 5, args.dof + 2 * args.nn + node);
+        m[6] = (node & 3) * 8;
         const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
-        uint16_t *sp = sPos + tid * NNE;
+        uint16_t *sp = sPosb + buf * kP2PS + tid * NNE;
 #pragma unroll
-        for (int b = 0; b < NNE; b++) sp[b] = pr[b];
+        for (int j = 0; j < NNE; j += 2) cpa4(sp + j, pr + j);
       }
     }
-    __syncthreads();
+    if (PLASTIC && tid < TE * NQP) {
+      const int el = tid / NQP, q = tid - el * NQP;
+      const long e = t1 + el;
+      if (e < ne) {
+        const long qp = e * NQP + q;
+        double *st = sStb + buf * kP2ST + tid * 7;
+#pragma unroll
+        for (int c = 0; c < 7; c++) cpa8(st + c, args.state_n + c * args.nqp + qp);
+      }
+    }
+    cpa_commit();
+  };
+  auto node_of = [&](long t1) -> int {
+    if (tid >= TE * NNE) return -1;
+    const int el = tid / NNE, a = tid - el * NNE;
+    const long e = t1 + el;
+    return (t1 < ne && e < ne) ? args.conn[(long)a * ne + e] : -1;
+  };
+
+  long tile0 = (long)blockIdx.x * TE;
+  int buf = 0;
+  if (tile0 < ne) prefetch(tile0, 0, node_of(tile0));
+  int next_node = node_of(tile0 + stride);
+  cpa_wait_all();
+  __syncthreads();
+
+  for (; tile0 < ne; tile0 += stride, buf ^= 1) {
+    const double *sXU = sXUb + buf * kP2XU;
+    const double *sSt = sStb + buf * kP2ST;
+    const int *sMeta = sMetab + buf * kP2MT;
+    const uint16_t *sPos = sPosb + buf * kP2PS;
 
     // ---------------- 1: quadrature points ----------------
     if (tid < TE * NQP) {
@@ -136,9 +187,10 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
           const long qp = e * NQP + q;
           double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
           if (PLASTIC) {
+            const double *st = sSt + tid * 7;
 #pragma unroll
-            for (int c = 0; c < 6; c++) Ast[c] = args.state_n[c * args.nqp + qp];
-            alpha = args.state_n[6 * args.nqp + qp];
+            for (int c = 0; c < 6; c++) Ast[c] = st[c];
+            alpha = st[6];
           }
           QpTangent t;
           double Anp1[6], alpha_np1;
@@ -210,13 +262,17 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
     }
     __syncthreads();
 
+    // the next tile's data lands while this tile's blocks are formed
+    if (tile0 + stride < ne) prefetch(tile0 + stride, buf ^ 1, next_node);
+    next_node = node_of(tile0 + 2 * stride);
+
     // ---------------- 3: column-split block rows + scatter ----------------
     {
       const int el = tid / 30, r = tid - el * 30;
       const int a = r / 3, k = r - a * 3;
       const long e = tile0 + el;
-      const int *mA = sMeta + (el * NNE + a) * 6;
-      const unsigned maskA = (e < ne) ? (unsigned)mA[0] : 0u;
+      const int *mA = sMeta + (el * NNE + a) * 7;
+      const unsigned maskA = (e < ne) ? ((unsigned)mA[0] >> mA[6]) & 0xFFu : 0u;
       if (maskA) {
         // the diagonal term (p_a . T_b) 1 enters entry (k, k): weights instead
         // of lane-dependent branches (the three lanes k of a warp stay converged)
@@ -275,7 +331,8 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
         const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
 #pragma unroll
         for (int b = 0; b < NNE; b++) {
-          const unsigned maskB = (unsigned)sMeta[(el * NNE + b) * 6];
+          const int *mB = sMeta + (el * NNE + b) * 7;
+          const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
           if (!((maskB >> k) & 1u)) continue;
           const long col = rp + posrow[b] + rank_of(maskB, k);
 #pragma unroll
@@ -286,6 +343,7 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
         }
       }
     }
+    cpa_wait_all();
     __syncthreads();
   }
 }

@@ -241,6 +241,14 @@ int upload(pgfem_gpu_ctx *c, T **d, const T *h, size_t n) {
   return PGFEM_GPU_OK;
 }
 
+// the free-component masks, padded to whole 4-byte words: kernels copy the
+// aligned word that holds a node's byte
+int upload_mask(pgfem_gpu_ctx *c, const std::vector<uint8_t> &mask) {
+  std::vector<uint8_t> padded(mask);
+  padded.resize((mask.size() + 3) & ~(size_t)3, 0);
+  return upload(c, &c->mask, padded.data(), padded.size());
+}
+
 void drop_events(pgfem_gpu_ctx *c) {
   for (auto &p : c->events) {
     cudaEventDestroy(p.first);
@@ -764,7 +772,7 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     }
   if ((r = upload(c, &c->X, X.data(), X.size())) || (r = upload(c, &c->dof, dof.data(), dof.size())) ||
       (r = upload(c, &c->rowptr0, rowptr0.data(), nn)) ||
-      (r = upload(c, &c->rowlen, rowlen.data(), nn)) || (r = upload(c, &c->mask, mask.data(), nn)) ||
+      (r = upload(c, &c->rowlen, rowlen.data(), nn)) || (r = upload_mask(c, mask)) ||
       (r = upload(c, &c->conn, conn.data(), conn.size())))
     return fail(r);
   if (m->F0 && (r = upload(c, &c->F0, m->F0, 9))) return fail(r);
