@@ -277,69 +277,74 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
         // the diagonal term (p_a . T_b) 1 enters entry (k, k): weights instead
         // of lane-dependent branches (the three lanes k of a warp stay converged)
         const double ek0 = k == 0 ? 1.0 : 0.0, ek1 = k == 1 ? 1.0 : 0.0, ek2 = k == 2 ? 1.0 : 0.0;
-        // points outer, the 10 column nodes inner: 30 independent accumulators
-        double acc[NNE][3];
-#pragma unroll
-        for (int b = 0; b < NNE; b++) acc[b][0] = acc[b][1] = acc[b][2] = 0.0;
+        // points outer, five column nodes inner (two halves): 15 independent
+        // accumulators per pass
+        const long rp = mA[1], rl = mA[2];
+        const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
         double Rk = 0.0;
 #pragma unroll 1
-        for (int q = 0; q < NQP; q++) {
-          const double *base = sVec + el * kP2ES + q * NNE * VS;
-          const double *L = base + a * VS;
-          const double2 l01 = *reinterpret_cast<const double2 *>(L);
-          const double pa0 = l01.x, pa1 = l01.y, pa2 = L[2];
-          const double2 s01 = *reinterpret_cast<const double2 *>(L + 12);
-          const double2 s2n0 = *reinterpret_cast<const double2 *>(L + 14);
-          const double2 n12 = *reinterpret_cast<const double2 *>(L + 16);
-          const double pak = L[k];
-          const double ha = sA1[el * NQP + q] * pak;
-          Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
+        for (int hb = 0; hb < 2; hb++) {
+          double acc[5][3];
 #pragma unroll
-          for (int b = 0; b < NNE; b++) {
-            const double *Rv = base + b * VS;
-            const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
-            const double pb2 = Rv[2];
-            const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
-            const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
-            const double dg = pa0 * Rv[9] + pa1 * t01.x + pa2 * t01.y;
-            double x0 = acc[b][0], x1 = acc[b][1], x2 = acc[b][2];
-            x0 = fma(r0.x, ha, x0);
-            x1 = fma(r0.y, ha, x1);
-            x2 = fma(pb2, ha, x2);
-            x0 = fma(pa0, Uk, x0);
-            x1 = fma(pa1, Uk, x1);
-            x2 = fma(pa2, Uk, x2);
-            x0 = fma(s01.x, pbk, x0);
-            x1 = fma(s01.y, pbk, x1);
-            x2 = fma(s2n0.x, pbk, x2);
-            if (PLASTIC) {
-              x0 = fma(s2n0.y, Wk, x0);
-              x1 = fma(n12.x, Wk, x1);
-              x2 = fma(n12.y, Wk, x2);
+          for (int j = 0; j < 5; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+#pragma unroll 1
+          for (int q = 0; q < NQP; q++) {
+            const double *base = sVec + el * kP2ES + q * NNE * VS;
+            const double *L = base + a * VS;
+            const double2 l01 = *reinterpret_cast<const double2 *>(L);
+            const double pa0 = l01.x, pa1 = l01.y, pa2 = L[2];
+            const double2 s01 = *reinterpret_cast<const double2 *>(L + 12);
+            const double2 s2n0 = *reinterpret_cast<const double2 *>(L + 14);
+            const double2 n12 = *reinterpret_cast<const double2 *>(L + 16);
+            const double pak = L[k];
+            const double ha = sA1[el * NQP + q] * pak;
+            if (hb == 0) Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
+#pragma unroll
+            for (int j = 0; j < 5; j++) {
+              const double *Rv = base + (5 * hb + j) * VS;
+              const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
+              const double pb2 = Rv[2];
+              const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
+              const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
+              const double dg = pa0 * Rv[9] + pa1 * t01.x + pa2 * t01.y;
+              double x0 = acc[j][0], x1 = acc[j][1], x2 = acc[j][2];
+              x0 = fma(r0.x, ha, x0);
+              x1 = fma(r0.y, ha, x1);
+              x2 = fma(pb2, ha, x2);
+              x0 = fma(pa0, Uk, x0);
+              x1 = fma(pa1, Uk, x1);
+              x2 = fma(pa2, Uk, x2);
+              x0 = fma(s01.x, pbk, x0);
+              x1 = fma(s01.y, pbk, x1);
+              x2 = fma(s2n0.x, pbk, x2);
+              if (PLASTIC) {
+                x0 = fma(s2n0.y, Wk, x0);
+                x1 = fma(n12.x, Wk, x1);
+                x2 = fma(n12.y, Wk, x2);
+              }
+              acc[j][0] = fma(ek0, dg, x0);
+              acc[j][1] = fma(ek1, dg, x1);
+              acc[j][2] = fma(ek2, dg, x2);
             }
-            acc[b][0] = fma(ek0, dg, x0);
-            acc[b][1] = fma(ek1, dg, x1);
-            acc[b][2] = fma(ek2, dg, x2);
+          }
+#pragma unroll
+          for (int j = 0; j < 5; j++) {
+            const int b = 5 * hb + j;
+            const int *mB = sMeta + (el * NNE + b) * 7;
+            const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
+            if (!((maskB >> k) & 1u)) continue;
+            const long col = rp + posrow[b] + rank_of(maskB, k);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+              if (!((maskA >> i) & 1u)) continue;
+              atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[j][i]);
+            }
           }
         }
         // residual component k of node a
         {
           const int id = mA[3 + k];
           if (id > 0) atomicAdd(&args.R[id - 1], Rk);
-        }
-        const long rp = mA[1], rl = mA[2];
-        const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
-#pragma unroll
-        for (int b = 0; b < NNE; b++) {
-          const int *mB = sMeta + (el * NNE + b) * 7;
-          const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
-          if (!((maskB >> k) & 1u)) continue;
-          const long col = rp + posrow[b] + rank_of(maskB, k);
-#pragma unroll
-          for (int i = 0; i < 3; i++) {
-            if (!((maskA >> i) & 1u)) continue;
-            atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[b][i]);
-          }
         }
       }
     }
