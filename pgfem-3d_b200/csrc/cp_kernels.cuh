@@ -267,15 +267,17 @@ struct CpArgs {
   double dt;
   int warm_k;                     // Newton iterations from the guess before the cold restart (0: max_iter)
   unsigned long long *fallbacks;  // cold restarts (or nullptr)
+  uint8_t *conv;                  // nqp: 1 when the point converged with an invertible M (or nullptr)
 };
 
-constexpr int kCpWarps = 2;  // warps per CTA of k_cp_update
+constexpr int kCpWarps = 4;      // warps per CTA of k_cp_update
+constexpr int kCpTanWarps = 2;   // warps per CTA of k_cp_tangent
 
 __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
   extern __shared__ double smem_cp[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double *Jm = smem_cp + warp * (100 + 90) * 32 + lane;  // 10x10 Jacobian
-  double *Bm = Jm + 100 * 32;                            // 10x9 right-hand sides
+  double *Jm = smem_cp + warp * (100 + 10) * 32 + lane;  // 10x10 Jacobian
+  double *Bm = Jm + 100 * 32;                            // right-hand side
   const unsigned FULL = 0xffffffffu;
   const long S = A.nqp;
   const double tol = A.mat.tol;
@@ -406,8 +408,50 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
 #pragma unroll
       for (int a = 0; a < kSlip; a++) A.out[(91 + a) * S + qp] = A.dt * gd[a];
       if (A.iters) A.iters[qp] = it;
-      // consistent dM/dF = -J^-1 dR/dF
-      if (conv && okM) {
+      if (A.conv) A.conv[qp] = (conv && okM) ? 1 : 0;
+      qp = -1;
+    }
+  }
+}
+
+inline size_t cp_update_smem() { return sizeof(double) * kCpWarps * (100 + 10) * 32; }
+
+// Consistent tangent of the converged local update, one lane per point:
+// dM/dF = -J^-1 dR/dF with d tau_a / dF = 2 F Z_a,
+// Z_a = pF_n^-1 M Ysym_a M^T pF_n^-T (the role of compute_dMdu,
+// src/plasticity_model.cc:578-881).  Reads the converged M and g from the
+// point record, writes dM/dF (81) into it; points that did not converge get a
+// zero tangent.  Every point does the same work, so no work stealing.
+__global__ void __launch_bounds__(32 * kCpTanWarps) k_cp_tangent(const CpArgs A) {
+  extern __shared__ double smem_ct[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double *Jm = smem_ct + warp * (100 + 90) * 32 + lane;  // 10x10 Jacobian
+  double *Bm = Jm + 100 * 32;                            // 10x9 right-hand sides
+  const long S = A.nqp;
+  for (long qp = (long)blockIdx.x * blockDim.x + threadIdx.x; qp < S; qp += (long)gridDim.x * blockDim.x) {
+    bool ok = A.conv[qp] != 0;
+    if (ok) {
+      CpPoint pt;
+      double Fq[9], pFni[9], pFn[9], M[9];
+      const long e = qp / A.nqp_e;
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        Fq[i] = A.F[i * S + qp];
+        pt.R[i] = A.Rcp[i * A.ne + e];
+        pFn[i] = A.state_n[i * S + qp];
+        M[i] = A.out[i * S + qp];
+      }
+      const double g = A.out[90 * S + qp];
+      pt.g_n = A.state_n[9 * S + qp];
+      pt.dt = A.dt;
+      inv3(pFn, pFni);
+      double Fe[9];
+      mm3(Fq, pFni, Fe);
+      mm3tn(Fe, Fe, pt.Cep);
+      double Res[10], gd[kSlip], dgd[kSlip], gdot = 0;
+      NeoHooke h;
+      ok = cp_residual(A.mat, pt, M, g, Res, h, gd, dgd, gdot);
+      if (ok) {
         cp_jacobian(A.mat, pt, M, g, h, gd, dgd, gdot, Jm);
         for (int i = 0; i < 90; i++) Bm[i * 32] = 0.0;
         double Ce[9], t[9], W[9];
@@ -428,22 +472,21 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
             for (int kl = 0; kl < 9; kl++) lm(Bm, 9, i, kl) -= cf * P[i] * 2.0 * dtF[kl];
           for (int kl = 0; kl < 9; kl++) lm(Bm, 9, 9, kl) -= -c * (gs - g) * sg * dgd[a] * 2.0 * dtF[kl];
         }
-        if (lane_solve(Jm, 10, Bm, 9)) {
+        ok = lane_solve(Jm, 10, Bm, 9);
+        if (ok) {
           for (int r = 0; r < 9; r++)
             for (int q = 0; q < 9; q++) A.out[(9 + r * 9 + q) * S + qp] = lm(Bm, 9, r, q);
         } else {
           atomicAdd(&A.status[3], 1ull);
-          for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
         }
-      } else {
-        for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
       }
-      qp = -1;
     }
+    if (!ok)
+      for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
   }
 }
 
-inline size_t cp_update_smem() { return sizeof(double) * kCpWarps * (100 + 90) * 32; }
+inline size_t cp_tangent_smem() { return sizeof(double) * kCpTanWarps * (100 + 90) * 32; }
 
 }  // namespace pgb
 

@@ -76,6 +76,7 @@ struct pgfem_gpu_ctx {
   double *cp_R = nullptr, *cp_F = nullptr, *cp_detJw = nullptr, *cp_out = nullptr, *cp_guess = nullptr;
   int *cp_iters = nullptr;
   unsigned *cp_counter = nullptr;
+  uint8_t *cp_conv = nullptr;  // per point: converged (the tangent kernel's input)
   bool cp_use_guess = false;
   // learned warm start: F at t_n, network features / predictions, cold restarts
   double *cp_Fn = nullptr;
@@ -264,7 +265,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
                   c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
-                  c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab,
+                  c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -546,6 +547,7 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   a.guess = (c->cp_use_guess || c->cp_net) ? c->cp_guess : nullptr;
   a.warm_k = c->cp_warm_k;
   a.fallbacks = c->cp_fallbacks;
+  a.conv = c->cp_conv;
   a.out = c->cp_out;
   a.iters = c->cp_iters;
   a.counter = c->cp_counter;
@@ -566,6 +568,18 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   const long grid = std::max<long>(1, std::min<long>(need, (long)g_num_sms * per_sm));
   k_cp_update<<<(unsigned)grid, 32 * kCpWarps, smem, s>>>(a);
   CK(cudaGetLastError());
+  {  // consistent tangent dM/dF of the converged points
+    const size_t tsm = cp_tangent_smem();
+    static bool tattr = false;
+    if (!tattr) {
+      CK(cudaFuncSetAttribute(k_cp_tangent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+      tattr = true;
+    }
+    const long tblk = 32 * kCpTanWarps;
+    const long tgrid = std::max<long>(1, std::min<long>((c->nqp + tblk - 1) / tblk, (long)g_num_sms * 16));
+    k_cp_tangent<<<(unsigned)tgrid, (unsigned)tblk, tsm, s>>>(a);
+    CK(cudaGetLastError());
+  }
   if (e0) {
     CK(cudaEventRecord(e1, s));
     c->events.emplace_back(e0, e1);
@@ -817,7 +831,7 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if ((r = upload(c, &c->cp_R, Rs.data(), Rs.size())) || (r = dalloc(c, &c->cp_F, (size_t)9 * ne)) ||
         (r = dalloc(c, &c->cp_detJw, ne)) || (r = dalloc(c, &c->cp_out, (size_t)kCpOut * c->nqp)) ||
         (r = dalloc(c, &c->cp_iters, c->nqp)) || (r = dalloc(c, &c->cp_counter, 1)) ||
-        (r = dalloc(c, &c->cp_fallbacks, 1)))
+        (r = dalloc(c, &c->cp_fallbacks, 1)) || (r = dalloc(c, &c->cp_conv, c->nqp)))
       return fail(r);
     std::vector<double> Fn((size_t)9 * c->nqp, 0.0);  // F at t_n: identity until the first commit
     for (long q = 0; q < c->nqp; q++) Fn[0 * c->nqp + q] = Fn[4 * c->nqp + q] = Fn[8 * c->nqp + q] = 1.0;
@@ -904,8 +918,8 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
-  if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, element (+ features, network, guess)
-    return c->cp_net ? 7 : 4;
+  if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, tangent, element (+ features, network, guess)
+    return c->cp_net ? 8 : 5;
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_CELLS && c->nne == 10) return 2;  // u expansion, cells
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
