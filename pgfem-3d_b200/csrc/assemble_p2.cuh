@@ -65,6 +65,228 @@ __device__ __forceinline__ void cpa8(void *dst, const void *src) {
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cpa_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
+// ---- the three phases as device functions (shared by both kernels) ----
+
+// Phase 1 for one quadrature point: Jacobian, F, constitutive update (state
+// n -> n+1 written to global memory) and the 38-double point record.
+// xu: the element's 10 nodes (x, u) in shared memory; st: 7 state doubles.
+template <bool PLASTIC>
+__device__ __forceinline__ void p2_point(const AsmArgs &args, const double *xu, const double *st, double *rec,
+                                         long e, int q) {
+  constexpr int NNE = 10, NQP = 4;
+  double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int b = 0; b < NNE; b++) {
+    const double g0 = args.shp.dNxi[q][b][0], g1 = args.shp.dNxi[q][b][1], g2 = args.shp.dNxi[q][b][2];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const double x = xu[b * 6 + i], u = xu[b * 6 + 3 + i];
+      dX[i * 3 + 0] += g0 * x;
+      dX[i * 3 + 1] += g1 * x;
+      dX[i * 3 + 2] += g2 * x;
+      dU[i * 3 + 0] += g0 * u;
+      dU[i * 3 + 1] += g1 * u;
+      dU[i * 3 + 2] += g2 * u;
+    }
+  }
+  const double detJ = det3(dX);
+  double dXi[9], F[9], Fi[9];
+  bool ok = detJ > 0.0 && inv3(dX, dXi);
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] + dU[i * 3 + 1] * dXi[1 * 3 + j] +
+                       dU[i * 3 + 2] * dXi[2 * 3 + j];
+    if (args.F0)
+#pragma unroll
+      for (int i = 0; i < 9; i++) F[i] += args.F0[i];
+  }
+  const double J = ok ? det3(F) : -1.0;
+  if (ok) ok = J > 0.0 && inv3(F, Fi);
+  if (!ok) {
+    atomicAdd(&args.status[0], 1ull);
+#pragma unroll
+    for (int i = 0; i < kRec; i++) rec[i] = 0.0;
+    return;
+  }
+  const long qp = e * NQP + q;
+  double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
+  if (PLASTIC) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) Ast[c] = st[c];
+    alpha = st[6];
+  }
+  QpTangent t;
+  double Anp1[6], alpha_np1;
+  spatial_update<PLASTIC>(args.mat, F, J, Ast, alpha, t, Anp1, &alpha_np1);
+  if (PLASTIC && args.state_np1) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) args.state_np1[c * args.nqp + qp] = Anp1[c];
+    args.state_np1[6 * args.nqp + qp] = alpha_np1;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      rec[i * 3 + j] =
+          dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] + dXi[i * 3 + 2] * Fi[2 * 3 + j];
+  rec[9] = detJ * args.shp.w[q];
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    rec[10 + i] = t.tau[i];
+    rec[16 + i] = t.s[i];
+    rec[22 + i] = t.n[i];
+    rec[28 + i] = t.D[i];
+  }
+  rec[34] = t.a1;
+  rec[35] = t.a2;
+  rec[36] = t.a4;
+  rec[37] = t.a5;
+}
+
+// Phase 2 for one (point, node): the 18-double vector record
+// [p, U, W, T, S, n p] (16-byte aligned pairs) and, for node 0, w a1 / 2.
+template <bool PLASTIC>
+__device__ __forceinline__ void p2_vectors(const AsmArgs &args, const double *rec, int q, int a, double *v,
+                                           double *a1_out) {
+  const double w = rec[9];
+  const double a1h = 0.5 * rec[34] * w, a2w = rec[35] * w, c23 = (2.0 / 3.0) * w;
+  const double g0 = args.shp.dNxi[q][a][0], g1 = args.shp.dNxi[q][a][1], g2 = args.shp.dNxi[q][a][2];
+  double p[3], sp[3], tp[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) p[j] = rec[0 * 3 + j] * g0 + rec[1 * 3 + j] * g1 + rec[2 * 3 + j] * g2;
+  smv(rec + 16, p, sp);
+  smv(rec + 10, p, tp);
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    v[j] = p[j];
+    v[3 + j] = a2w * p[j] - c23 * sp[j];
+    v[9 + j] = a1h * p[j] + w * tp[j];
+    v[12 + j] = -c23 * sp[j];
+  }
+  if (PLASTIC) {
+    const double a4w = rec[36] * w, a5w = rec[37] * w;
+    double np_[3], mp[3];
+    smv(rec + 22, p, np_);
+    smv(rec + 28, p, mp);
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+      v[6 + j] = a4w * np_[j] + a5w * mp[j];
+      v[15 + j] = np_[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < 3; j++) v[6 + j] = v[15 + j] = 0.0;
+  }
+  if (a == 0) *a1_out = a1h;
+}
+
+// Phase 3 for one lane (row node a, column component k of one element):
+// the entries (i, k) of K_ab for all b, scattered with FP64 reductions, and
+// the residual component k of node a.  vec: the element's vector records;
+// a1: its four w a1 / 2; meta / pos: its nodes' row metadata and positions.
+template <bool PLASTIC>
+__device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec, const double *a1,
+                                          const int *meta, const uint16_t *pos, int a, int k) {
+  constexpr int NNE = 10, NQP = 4, VS = kP2VS;
+  const int *mA = meta + a * 7;
+  const unsigned maskA = ((unsigned)mA[0] >> mA[6]) & 0xFFu;
+  if (!maskA) return;
+  // the diagonal term (p_a . T_b) 1 enters entry (k, k): weights instead of
+  // lane-dependent branches (the three lanes k of a warp stay converged)
+  const double ek0 = k == 0 ? 1.0 : 0.0, ek1 = k == 1 ? 1.0 : 0.0, ek2 = k == 2 ? 1.0 : 0.0;
+  const long rp = mA[1], rl = mA[2];
+  const uint16_t *posrow = pos + a * NNE;
+  double Rk = 0.0;
+  // points outer, five column nodes inner (two halves): 15 independent
+  // accumulators per pass
+#pragma unroll 1
+  for (int hb = 0; hb < 2; hb++) {
+    double acc[5][3];
+#pragma unroll
+    for (int j = 0; j < 5; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+#pragma unroll 1
+    for (int q = 0; q < NQP; q++) {
+      const double *base = vec + q * NNE * VS;
+      const double *L = base + a * VS;
+      const double2 l01 = *reinterpret_cast<const double2 *>(L);
+      const double pa0 = l01.x, pa1 = l01.y, pa2 = L[2];
+      const double2 s01 = *reinterpret_cast<const double2 *>(L + 12);
+      const double2 s2n0 = *reinterpret_cast<const double2 *>(L + 14);
+      const double2 n12 = *reinterpret_cast<const double2 *>(L + 16);
+      const double pak = L[k];
+      const double ha = a1[q] * pak;
+      if (hb == 0) Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
+#pragma unroll
+      for (int j = 0; j < 5; j++) {
+        const double *Rv = base + (5 * hb + j) * VS;
+        const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
+        const double pb2 = Rv[2];
+        const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
+        const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
+        const double dg = pa0 * Rv[9] + pa1 * t01.x + pa2 * t01.y;
+        double x0 = acc[j][0], x1 = acc[j][1], x2 = acc[j][2];
+        x0 = fma(r0.x, ha, x0);
+        x1 = fma(r0.y, ha, x1);
+        x2 = fma(pb2, ha, x2);
+        x0 = fma(pa0, Uk, x0);
+        x1 = fma(pa1, Uk, x1);
+        x2 = fma(pa2, Uk, x2);
+        x0 = fma(s01.x, pbk, x0);
+        x1 = fma(s01.y, pbk, x1);
+        x2 = fma(s2n0.x, pbk, x2);
+        if (PLASTIC) {
+          x0 = fma(s2n0.y, Wk, x0);
+          x1 = fma(n12.x, Wk, x1);
+          x2 = fma(n12.y, Wk, x2);
+        }
+        acc[j][0] = fma(ek0, dg, x0);
+        acc[j][1] = fma(ek1, dg, x1);
+        acc[j][2] = fma(ek2, dg, x2);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 5; j++) {
+      const int b = 5 * hb + j;
+      const int *mB = meta + b * 7;
+      const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
+      if (!((maskB >> k) & 1u)) continue;
+      const long col = rp + posrow[b] + rank_of(maskB, k);
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        if (!((maskA >> i) & 1u)) continue;
+        atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[j][i]);
+      }
+    }
+  }
+  const int id = mA[3 + k];
+  if (id > 0) atomicAdd(&args.R[id - 1], Rk);
+}
+
+// asynchronous copy of one element node's data and row metadata
+__device__ __forceinline__ void p2_fetch_node(const AsmArgs &args, long e, int a, int node, double *d, int *m,
+                                              uint16_t *sp) {
+  constexpr int NNE = 10;
+  cpa8(d + 0, args.X + node);
+  cpa8(d + 1, args.X + args.nn + node);
+  cpa8(d + 2, args.X + 2 * args.nn + node);
+  cpa8(d + 3, args.unode + node);
+  cpa8(d + 4, args.unode + args.nn + node);
+  cpa8(d + 5, args.unode + 2 * args.nn + node);
+  cpa4(m + 0, args.mask + (node & ~3));  // the aligned word holding the mask byte
+  cpa4(m + 1, args.rowptr0 + node);
+  cpa4(m + 2, args.rowlen + node);
+  cpa4(m + 3, args.dof + node);
+  cpa4(m + 4, args.dof + args.nn + node);
+  cpa4(m + 5, args.dof + 2 * args.nn + node);
+  m[6] = (node & 3) * 8;
+  const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
+#pragma unroll
+  for (int j = 0; j < NNE; j += 2) cpa4(sp + j, pr + j);
+}
+
 template <int MODEL>
 __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs args) {
   constexpr int NNE = 10, NQP = 4, TE = kP2TE, VS = kP2VS;
@@ -87,27 +309,9 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
     if (tid < TE * NNE) {
       const int el = tid / NNE, a = tid - el * NNE;
       const long e = t1 + el;
-      if (e < ne && node >= 0) {
-        double *d = sXUb + buf * kP2XU + tid * 6;
-        cpa8(d + 0, args.X + node);
-        cpa8(d + 1, args.X + args.nn + node);
-        cpa8(d + 2, args.X + 2 * args.nn + node);
-        cpa8(d + 3, args.unode + node);
-        cpa8(d + 4, args.unode + args.nn + node);
-        cpa8(d + 5, args.unode + 2 * args.nn + node);
-        int *m = sMetab + buf * kP2MT + tid * 7;
-        cpa4(m + 0, args.mask + (node & ~3));  // the aligned word holding the mask byte
-        cpa4(m + 1, args.rowptr0 + node);
-        cpa4(m + 2, args.rowlen + node);
-        cpa4(m + 3, args.dof + node);
-        cpa4(m + 4, args.dof + args.nn + node);
-        cpa4(m + 5, args.dof + 2 * args.nn + node);
-        m[6] = (node & 3) * 8;
-        const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
-        uint16_t *sp = sPosb + buf * kP2PS + tid * NNE;
-#pragma unroll
-        for (int j = 0; j < NNE; j += 2) cpa4(sp + j, pr + j);
-      }
+      if (e < ne && node >= 0)
+        p2_fetch_node(args, e, a, node, sXUb + buf * kP2XU + tid * 6, sMetab + buf * kP2MT + tid * 7,
+                      sPosb + buf * kP2PS + tid * NNE);
     }
     if (PLASTIC && tid < TE * NQP) {
       const int el = tid / NQP, q = tid - el * NQP;
@@ -145,120 +349,15 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
     if (tid < TE * NQP) {
       const int el = tid / NQP, q = tid - el * NQP;
       const long e = tile0 + el;
-      if (e < ne) {
-        const double *xu = sXU + el * NNE * 6;
-        double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll
-        for (int b = 0; b < NNE; b++) {
-          const double g0 = args.shp.dNxi[q][b][0], g1 = args.shp.dNxi[q][b][1], g2 = args.shp.dNxi[q][b][2];
-#pragma unroll
-          for (int i = 0; i < 3; i++) {
-            const double x = xu[b * 6 + i], u = xu[b * 6 + 3 + i];
-            dX[i * 3 + 0] += g0 * x;
-            dX[i * 3 + 1] += g1 * x;
-            dX[i * 3 + 2] += g2 * x;
-            dU[i * 3 + 0] += g0 * u;
-            dU[i * 3 + 1] += g1 * u;
-            dU[i * 3 + 2] += g2 * u;
-          }
-        }
-        double *rec = sRec + tid * kRec;
-        const double detJ = det3(dX);
-        double dXi[9], F[9], Fi[9];
-        bool ok = detJ > 0.0 && inv3(dX, dXi);
-        if (ok) {
-#pragma unroll
-          for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-              F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] +
-                             dU[i * 3 + 1] * dXi[1 * 3 + j] + dU[i * 3 + 2] * dXi[2 * 3 + j];
-          if (args.F0)
-#pragma unroll
-            for (int i = 0; i < 9; i++) F[i] += args.F0[i];
-        }
-        const double J = ok ? det3(F) : -1.0;
-        if (ok) ok = J > 0.0 && inv3(F, Fi);
-        if (!ok) {
-          atomicAdd(&args.status[0], 1ull);
-#pragma unroll
-          for (int i = 0; i < kRec; i++) rec[i] = 0.0;
-        } else {
-          const long qp = e * NQP + q;
-          double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
-          if (PLASTIC) {
-            const double *st = sSt + tid * 7;
-#pragma unroll
-            for (int c = 0; c < 6; c++) Ast[c] = st[c];
-            alpha = st[6];
-          }
-          QpTangent t;
-          double Anp1[6], alpha_np1;
-          spatial_update<PLASTIC>(args.mat, F, J, Ast, alpha, t, Anp1, &alpha_np1);
-          if (PLASTIC && args.state_np1) {
-#pragma unroll
-            for (int c = 0; c < 6; c++) args.state_np1[c * args.nqp + qp] = Anp1[c];
-            args.state_np1[6 * args.nqp + qp] = alpha_np1;
-          }
-#pragma unroll
-          for (int i = 0; i < 3; i++)
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-              rec[i * 3 + j] = dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] +
-                               dXi[i * 3 + 2] * Fi[2 * 3 + j];
-          rec[9] = detJ * args.shp.w[q];
-#pragma unroll
-          for (int i = 0; i < 6; i++) {
-            rec[10 + i] = t.tau[i];
-            rec[16 + i] = t.s[i];
-            rec[22 + i] = t.n[i];
-            rec[28 + i] = t.D[i];
-          }
-          rec[34] = t.a1;
-          rec[35] = t.a2;
-          rec[36] = t.a4;
-          rec[37] = t.a5;
-        }
-      }
+      if (e < ne) p2_point<PLASTIC>(args, sXU + el * NNE * 6, sSt + tid * 7, sRec + tid * kRec, e, q);
     }
     __syncthreads();
 
     // ---------------- 2: node vectors per point ----------------
     for (int it = tid; it < TE * NQP * NNE; it += kP2Threads) {
       const int eq = it / NNE, a = it - eq * NNE;  // eq = el * NQP + q
-      const int q = eq % NQP;
-      const double *rec = sRec + eq * kRec;
-      const double w = rec[9];
-      const double a1h = 0.5 * rec[34] * w, a2w = rec[35] * w, c23 = (2.0 / 3.0) * w;
-      const double g0 = args.shp.dNxi[q][a][0], g1 = args.shp.dNxi[q][a][1], g2 = args.shp.dNxi[q][a][2];
-      double p[3], sp[3], tp[3];
-#pragma unroll
-      for (int j = 0; j < 3; j++) p[j] = rec[0 * 3 + j] * g0 + rec[1 * 3 + j] * g1 + rec[2 * 3 + j] * g2;
-      smv(rec + 16, p, sp);
-      smv(rec + 10, p, tp);
-      double *v = sVec + (eq / NQP) * kP2ES + ((eq % NQP) * NNE + a) * VS;
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        v[j] = p[j];
-        v[3 + j] = a2w * p[j] - c23 * sp[j];
-        v[9 + j] = a1h * p[j] + w * tp[j];
-        v[12 + j] = -c23 * sp[j];
-      }
-      if (PLASTIC) {
-        const double a4w = rec[36] * w, a5w = rec[37] * w;
-        double np_[3], mp[3];
-        smv(rec + 22, p, np_);
-        smv(rec + 28, p, mp);
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-          v[6 + j] = a4w * np_[j] + a5w * mp[j];
-          v[15 + j] = np_[j];
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < 3; j++) v[6 + j] = v[15 + j] = 0.0;
-      }
-      if (a == 0) sA1[eq] = a1h;
+      p2_vectors<PLASTIC>(args, sRec + eq * kRec, eq % NQP, a,
+                          sVec + (eq / NQP) * kP2ES + ((eq % NQP) * NNE + a) * VS, sA1 + eq);
     }
     __syncthreads();
 
@@ -270,87 +369,189 @@ __global__ void __launch_bounds__(kP2Threads, 2) k_assemble_p2(const AsmArgs arg
     {
       const int el = tid / 30, r = tid - el * 30;
       const int a = r / 3, k = r - a * 3;
-      const long e = tile0 + el;
-      const int *mA = sMeta + (el * NNE + a) * 7;
-      const unsigned maskA = (e < ne) ? ((unsigned)mA[0] >> mA[6]) & 0xFFu : 0u;
-      if (maskA) {
-        // the diagonal term (p_a . T_b) 1 enters entry (k, k): weights instead
-        // of lane-dependent branches (the three lanes k of a warp stay converged)
-        const double ek0 = k == 0 ? 1.0 : 0.0, ek1 = k == 1 ? 1.0 : 0.0, ek2 = k == 2 ? 1.0 : 0.0;
-        // points outer, five column nodes inner (two halves): 15 independent
-        // accumulators per pass
-        const long rp = mA[1], rl = mA[2];
-        const uint16_t *posrow = sPos + (el * NNE + a) * NNE;
-        double Rk = 0.0;
-#pragma unroll 1
-        for (int hb = 0; hb < 2; hb++) {
-          double acc[5][3];
-#pragma unroll
-          for (int j = 0; j < 5; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
-#pragma unroll 1
-          for (int q = 0; q < NQP; q++) {
-            const double *base = sVec + el * kP2ES + q * NNE * VS;
-            const double *L = base + a * VS;
-            const double2 l01 = *reinterpret_cast<const double2 *>(L);
-            const double pa0 = l01.x, pa1 = l01.y, pa2 = L[2];
-            const double2 s01 = *reinterpret_cast<const double2 *>(L + 12);
-            const double2 s2n0 = *reinterpret_cast<const double2 *>(L + 14);
-            const double2 n12 = *reinterpret_cast<const double2 *>(L + 16);
-            const double pak = L[k];
-            const double ha = sA1[el * NQP + q] * pak;
-            if (hb == 0) Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
-#pragma unroll
-            for (int j = 0; j < 5; j++) {
-              const double *Rv = base + (5 * hb + j) * VS;
-              const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
-              const double pb2 = Rv[2];
-              const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
-              const double2 t01 = *reinterpret_cast<const double2 *>(Rv + 10);
-              const double dg = pa0 * Rv[9] + pa1 * t01.x + pa2 * t01.y;
-              double x0 = acc[j][0], x1 = acc[j][1], x2 = acc[j][2];
-              x0 = fma(r0.x, ha, x0);
-              x1 = fma(r0.y, ha, x1);
-              x2 = fma(pb2, ha, x2);
-              x0 = fma(pa0, Uk, x0);
-              x1 = fma(pa1, Uk, x1);
-              x2 = fma(pa2, Uk, x2);
-              x0 = fma(s01.x, pbk, x0);
-              x1 = fma(s01.y, pbk, x1);
-              x2 = fma(s2n0.x, pbk, x2);
-              if (PLASTIC) {
-                x0 = fma(s2n0.y, Wk, x0);
-                x1 = fma(n12.x, Wk, x1);
-                x2 = fma(n12.y, Wk, x2);
-              }
-              acc[j][0] = fma(ek0, dg, x0);
-              acc[j][1] = fma(ek1, dg, x1);
-              acc[j][2] = fma(ek2, dg, x2);
-            }
-          }
-#pragma unroll
-          for (int j = 0; j < 5; j++) {
-            const int b = 5 * hb + j;
-            const int *mB = sMeta + (el * NNE + b) * 7;
-            const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
-            if (!((maskB >> k) & 1u)) continue;
-            const long col = rp + posrow[b] + rank_of(maskB, k);
-#pragma unroll
-            for (int i = 0; i < 3; i++) {
-              if (!((maskA >> i) & 1u)) continue;
-              atomicAdd(&args.K[col + (long)rank_of(maskA, i) * rl], acc[j][i]);
-            }
-          }
-        }
-        // residual component k of node a
-        {
-          const int id = mA[3 + k];
-          if (id > 0) atomicAdd(&args.R[id - 1], Rk);
-        }
-      }
+      if (tile0 + el < ne)
+        p2_blocks<PLASTIC>(args, sVec + el * kP2ES, sA1 + el * NQP, sMeta + el * NNE * 7, sPos + el * NNE * NNE,
+                           a, k);
     }
     cpa_wait_all();
     __syncthreads();
   }
+}
+
+
+// ---- warp-specialised variant ---------------------------------------------
+//
+// Producer / consumer pipeline over tiles of 4 elements.  Warp 4 (producer)
+// runs the serial, latency-bound phases of tile i+1 -- the point updates
+// (lanes 0-15) and the vector records -- and issues the cp.async prefetch of
+// tile i+2's node data, while warps 0-3 (consumers) run the issue-bound block
+// phase and the reductions of tile i.  Hand-off through two mbarriers per
+// vector buffer (full: produced; empty: consumed), every wait bounded: a wait
+// that runs out sets status[3] and both roles leave the loop (their next
+// waits run out too), so a fault cannot hang the GPU.
+constexpr int kWTE = 4;                   // elements per tile
+constexpr int kWCons = 128;               // consumer threads (120 form blocks)
+constexpr int kWThreads = kWCons + 32;    // + one producer warp
+constexpr int kWXU = kWTE * 10 * 6, kWST = kWTE * 4 * 7, kWMT = kWTE * 10 * 7, kWPS = kWTE * 10 * 10;
+constexpr unsigned long long kWWaitNs = 2000000000ull;
+
+inline size_t p2ws_smem_bytes() {
+  return 64 + sizeof(double) * (2 * (size_t)kWXU + 2 * (size_t)kWST + (size_t)kWTE * 4 * kRec +
+                                2 * (size_t)kWTE * kP2ES + 2 * (size_t)kWTE * 4) +
+         sizeof(int) * 3 * (size_t)kWMT + sizeof(uint16_t) * 3 * (size_t)kWPS;
+}
+
+__device__ __forceinline__ unsigned long long w_gtimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void w_mb_init(uint64_t *b, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(b)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void w_mb_arrive(uint64_t *b) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(b))
+               : "memory");
+}
+// bounded wait for the completion of the phase with the given parity
+__device__ __forceinline__ bool w_mb_wait(uint64_t *b, unsigned parity) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(b);
+  const unsigned long long t0 = w_gtimer();
+  for (;;) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (w_gtimer() - t0 > kWWaitNs) return false;
+  }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2ws(const AsmArgs args) {
+  constexpr int NNE = 10, NQP = 4, TE = kWTE, VS = kP2VS;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ __align__(16) unsigned char wsm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(wsm);       // [2]
+  uint64_t *empty = full + 2;                                // [2]
+  double *sXU = reinterpret_cast<double *>(wsm + 64);        // [2][TE][NNE][6]
+  double *sSt = sXU + 2 * kWXU;                              // [2][TE][NQP][7]
+  double *sRec = sSt + 2 * kWST;                             // [TE][NQP][kRec]
+  double *sVec = sRec + TE * NQP * kRec;                     // [2][TE][kP2ES]
+  double *sA1 = sVec + 2 * TE * kP2ES;                       // [2][TE][NQP]
+  int *sMeta = reinterpret_cast<int *>(sA1 + 2 * TE * NQP);  // [3][TE*NNE][7]
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + 3 * kWMT);  // [3][TE*NNE][NNE]
+  const int tid = threadIdx.x;
+  const long ne = args.ne;
+  auto tile_e0 = [&](long i) -> long { return ((long)blockIdx.x + i * (long)gridDim.x) * TE; };
+  if (tid == 0) {
+    w_mb_init(&full[0], 32);
+    w_mb_init(&full[1], 32);
+    w_mb_init(&empty[0], kWCons);
+    w_mb_init(&empty[1], kWCons);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  bool fail = false;
+  if (tid >= kWCons) {
+    // ------------------------------ producer ------------------------------
+    const int pl = tid - kWCons;
+    auto load_nodes = [&](long i, int *nd) {
+      const long e0 = tile_e0(i);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int slot = pl + 32 * j;
+        nd[j] = -1;
+        if (slot < TE * NNE && e0 < ne) {
+          const int el = slot / NNE, a = slot - el * NNE;
+          const long e = e0 + el;
+          if (e < ne) nd[j] = args.conn[(long)a * ne + e];
+        }
+      }
+    };
+    auto issue = [&](long i, const int *nd) {
+      const long e0 = tile_e0(i);
+      const int bx = (int)(i & 1), bm = (int)(i % 3);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int slot = pl + 32 * j;
+        if (slot < TE * NNE && nd[j] >= 0) {
+          const int el = slot / NNE, a = slot - el * NNE;
+          p2_fetch_node(args, e0 + el, a, nd[j], sXU + bx * kWXU + slot * 6, sMeta + bm * kWMT + slot * 7,
+                        sPos + bm * kWPS + slot * NNE);
+        }
+      }
+      if (PLASTIC && pl < TE * NQP) {
+        const int el = pl / NQP, q = pl - el * NQP;
+        const long e = e0 + el;
+        if (e < ne) {
+          const long qp = e * NQP + q;
+          double *st = sSt + bx * kWST + pl * 7;
+#pragma unroll
+          for (int c = 0; c < 7; c++) cpa8(st + c, args.state_n + c * args.nqp + qp);
+        }
+      }
+      cpa_commit();
+    };
+    int nd[2], nd_next[2];
+    if (tile_e0(0) < ne) {
+      load_nodes(0, nd);
+      issue(0, nd);
+    }
+    load_nodes(1, nd_next);
+    for (long i = 0; tile_e0(i) < ne; i++) {
+      const int bx = (int)(i & 1);
+      if (i >= 2) {
+        const bool ok = w_mb_wait(&empty[bx], (unsigned)(((i - 2) >> 1) & 1));
+        if (__any_sync(0xffffffffu, !ok)) {
+          fail = true;
+          break;
+        }
+      }
+      cpa_wait_all();  // tile i's node data and state have landed
+      __syncwarp();
+      if (tile_e0(i + 1) < ne) issue(i + 1, nd_next);
+      load_nodes(i + 2, nd_next);
+      const long e0 = tile_e0(i);
+      if (pl < TE * NQP) {
+        const int el = pl / NQP, q = pl - el * NQP;
+        const long e = e0 + el;
+        if (e < ne) p2_point<PLASTIC>(args, sXU + bx * kWXU + el * NNE * 6, sSt + bx * kWST + pl * 7,
+                                      sRec + pl * kRec, e, q);
+      }
+      __syncwarp();
+      for (int it = pl; it < TE * NQP * NNE; it += 32) {
+        const int eq = it / NNE, a = it - eq * NNE;
+        const int el = eq / NQP, q = eq - el * NQP;
+        if (e0 + el < ne)
+          p2_vectors<PLASTIC>(args, sRec + eq * kRec, q, a, sVec + (bx * TE + el) * kP2ES + (q * NNE + a) * VS,
+                              sA1 + bx * TE * NQP + eq);
+      }
+      w_mb_arrive(&full[bx]);  // release: this lane's records are visible to the consumers
+    }
+    cpa_wait_all();
+  } else {
+    // ------------------------------ consumers ------------------------------
+    const int el = tid / 30, r = tid - el * 30;
+    const int a = r / 3, k = r - a * 3;
+    for (long i = 0; tile_e0(i) < ne; i++) {
+      const int bx = (int)(i & 1), bm = (int)(i % 3);
+      if (!w_mb_wait(&full[bx], (unsigned)((i >> 1) & 1))) {
+        fail = true;
+        break;
+      }
+      if (tid < TE * 30 && tile_e0(i) + el < ne)
+        p2_blocks<PLASTIC>(args, sVec + (bx * TE + el) * kP2ES, sA1 + bx * TE * NQP + el * NQP,
+                           sMeta + bm * kWMT + el * NNE * 7, sPos + bm * kWPS + el * NNE * NNE, a, k);
+      w_mb_arrive(&empty[bx]);
+    }
+  }
+  if (fail && (tid & 31) == 0) atomicAdd(&args.status[3], 1ull);
 }
 
 }  // namespace pgb

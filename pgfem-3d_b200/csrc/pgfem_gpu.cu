@@ -473,12 +473,36 @@ int launch_p2(const AsmArgs &a, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+template <int MODEL>
+int launch_p2ws(const AsmArgs &a, cudaStream_t s) {
+  const size_t smem = p2ws_smem_bytes();
+  auto kern = k_assemble_p2ws<MODEL>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long tiles = (a.ne + kWTE - 1) / kWTE;
+  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
+  kern<<<(unsigned)grid, kWThreads, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 template <bool ATOMIC, bool WANT_K, bool DENSE>
 int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
   // quadratic tets, R+K into the CSR with atomic scatter over all elements:
-  // the column-split kernel
-  if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS"))
-    return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
+  // the column-split kernel, warp-specialised (PGFEM_GPU_P2_SYNC selects the
+  // variant in which all threads run the three phases of a tile in turn)
+  if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS")) {
+    if (getenv("PGFEM_GPU_P2_SYNC"))
+      return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
+    return c->model == PGFEM_MODEL_J2 ? launch_p2ws<1>(a, s) : launch_p2ws<0>(a, s);
+  }
   // linear tets over all elements: the tuned schedule (elements per block,
   // work stealing)
   if (c->nne == 4 && ATOMIC && !DENSE && !a.elist && (c->sched_epb || c->sched_grab)) {

@@ -225,6 +225,35 @@ def test_tiled_first_touch_memset_and_untiled_agree(gpu, kind):
         check_K(K2, K, p.Ap, 1e-13)
 
 
+@pytest.mark.parametrize("model", ["j2", "he"])
+def test_quadratic_tet_kernel_variants_agree(gpu, model):
+    """The three R+K kernels for 10-node elements (the warp-specialised default,
+    the variant in which all threads run the phases of a tile in turn, and the
+    one-element-per-thread-block kernel) on 162 elements, so that the last
+    tile of every variant is partly empty; each against the oracle."""
+    import os
+    p = wl.j2_p2(n=3, seed=7, perturb=5e-3)
+    if model == "he":
+        p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.3)
+        p.state = None
+    assert p.conn.shape[0] % 8 == 2
+    ctx = p.context()
+    Ro, Ko, so = oracle_assemble(p)
+    for env in ({}, {"PGFEM_GPU_P2_SYNC": "1"}, {"PGFEM_GPU_ELEMENT_ROWS": "1"}):
+        os.environ.update(env)
+        try:
+            R, K, st = ctx.assemble_RK(p.u)
+        finally:
+            for k in env:
+                os.environ.pop(k, None)
+        assert st.ok(), (env, st.as_dict())
+        check_R(R, Ro)
+        check_K(K, Ko, p.Ap)
+        if so is not None:
+            sg = ctx.get_state(1)
+            assert np.abs(sg - so).max() <= TOL * np.abs(so).max(), env
+
+
 def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
     # number the nodes in reverse order (ids stay consecutive per node, but the
     # rows are no longer first touched in element order)
