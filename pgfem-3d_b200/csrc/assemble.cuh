@@ -72,6 +72,9 @@ struct AsmArgs {
   // before the launch); nullptr = static grid-stride order
   unsigned *ticket;
   int grab;
+  // point records written by the point-update kernel (kRec x nqp, structure
+  // of arrays), read by the two-kernel quadratic-tet assembly
+  const double *qrec;
   Mat mat;
   ShapeTable shp;
 };

@@ -1,5 +1,10 @@
-// assemble_p2.cuh -- fused FP64 R+K assembly of quadratic tets with
-// column-split block rows (default path for 10-node elements).
+// assemble_p2.cuh -- FP64 R+K assembly of quadratic tets with column-split
+// block rows.  Three kernels share the phases below: k_assemble_p2 (all
+// threads run the phases of a tile in turn), k_assemble_p2ws (one producer
+// warp runs phases 0-2 of the next tile while four consumer warps run phase 3)
+// and k_assemble_p2r, the default for 10-node elements: phase 1 runs first in
+// its own kernel (k_qp_update, one thread per point) and k_assemble_p2r is
+// the producer/consumer pipeline from the point records.
 //
 // Same operation as k_assemble (fd_residuals_MP + stiffmat_fd_MP for the
 // constitutive-model element, src/fd_residuals.cc:468-636,
@@ -60,6 +65,11 @@ __device__ __forceinline__ void cpa4(void *dst, const void *src) {
 }
 __device__ __forceinline__ void cpa8(void *dst, const void *src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa16(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
                : "memory");
 }
 __device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -148,17 +158,24 @@ __device__ __forceinline__ void p2_point(const AsmArgs &args, const double *xu, 
 
 // Phase 2 for one (point, node): the 18-double vector record
 // [p, U, W, T, S, n p] (16-byte aligned pairs) and, for node 0, w a1 / 2.
-template <bool PLASTIC>
+// RS: stride between consecutive values of the point record (1: one record
+// per point, contiguous; 16: structure of arrays over a tile's 16 points)
+template <bool PLASTIC, int RS = 1>
 __device__ __forceinline__ void p2_vectors(const AsmArgs &args, const double *rec, int q, int a, double *v,
                                            double *a1_out) {
-  const double w = rec[9];
-  const double a1h = 0.5 * rec[34] * w, a2w = rec[35] * w, c23 = (2.0 / 3.0) * w;
+  const double w = rec[9 * RS];
+  const double a1h = 0.5 * rec[34 * RS] * w, a2w = rec[35 * RS] * w, c23 = (2.0 / 3.0) * w;
   const double g0 = args.shp.dNxi[q][a][0], g1 = args.shp.dNxi[q][a][1], g2 = args.shp.dNxi[q][a][2];
-  double p[3], sp[3], tp[3];
+  double p[3], sp[3], tp[3], S6[6];
 #pragma unroll
-  for (int j = 0; j < 3; j++) p[j] = rec[0 * 3 + j] * g0 + rec[1 * 3 + j] * g1 + rec[2 * 3 + j] * g2;
-  smv(rec + 16, p, sp);
-  smv(rec + 10, p, tp);
+  for (int j = 0; j < 3; j++)
+    p[j] = rec[(0 * 3 + j) * RS] * g0 + rec[(1 * 3 + j) * RS] * g1 + rec[(2 * 3 + j) * RS] * g2;
+#pragma unroll
+  for (int c = 0; c < 6; c++) S6[c] = rec[(16 + c) * RS];
+  smv(S6, p, sp);
+#pragma unroll
+  for (int c = 0; c < 6; c++) S6[c] = rec[(10 + c) * RS];
+  smv(S6, p, tp);
 #pragma unroll
   for (int j = 0; j < 3; j++) {
     v[j] = p[j];
@@ -167,10 +184,14 @@ __device__ __forceinline__ void p2_vectors(const AsmArgs &args, const double *re
     v[12 + j] = -c23 * sp[j];
   }
   if (PLASTIC) {
-    const double a4w = rec[36] * w, a5w = rec[37] * w;
+    const double a4w = rec[36 * RS] * w, a5w = rec[37 * RS] * w;
     double np_[3], mp[3];
-    smv(rec + 22, p, np_);
-    smv(rec + 28, p, mp);
+#pragma unroll
+    for (int c = 0; c < 6; c++) S6[c] = rec[(22 + c) * RS];
+    smv(S6, p, np_);
+#pragma unroll
+    for (int c = 0; c < 6; c++) S6[c] = rec[(28 + c) * RS];
+    smv(S6, p, mp);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
       v[6 + j] = a4w * np_[j] + a5w * mp[j];
@@ -187,7 +208,9 @@ __device__ __forceinline__ void p2_vectors(const AsmArgs &args, const double *re
 // the entries (i, k) of K_ab for all b, scattered with FP64 reductions, and
 // the residual component k of node a.  vec: the element's vector records;
 // a1: its four w a1 / 2; meta / pos: its nodes' row metadata and positions.
-template <bool PLASTIC>
+// NB: column nodes per pass (5: two passes, fewer registers; 10: one pass,
+// the row node's vectors loaded once per point)
+template <bool PLASTIC, int NB = 5>
 __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec, const double *a1,
                                           const int *meta, const uint16_t *pos, int a, int k) {
   constexpr int NNE = 10, NQP = 4, VS = kP2VS;
@@ -200,13 +223,12 @@ __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec
   const long rp = mA[1], rl = mA[2];
   const uint16_t *posrow = pos + a * NNE;
   double Rk = 0.0;
-  // points outer, five column nodes inner (two halves): 15 independent
-  // accumulators per pass
+  // points outer, NB column nodes inner: 3 NB independent accumulators per pass
 #pragma unroll 1
-  for (int hb = 0; hb < 2; hb++) {
-    double acc[5][3];
+  for (int hb = 0; hb < NNE / NB; hb++) {
+    double acc[NB][3];
 #pragma unroll
-    for (int j = 0; j < 5; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
+    for (int j = 0; j < NB; j++) acc[j][0] = acc[j][1] = acc[j][2] = 0.0;
 #pragma unroll 1
     for (int q = 0; q < NQP; q++) {
       const double *base = vec + q * NNE * VS;
@@ -220,8 +242,8 @@ __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec
       const double ha = a1[q] * pak;
       if (hb == 0) Rk += L[9 + k] - ha;  // w tau p_a = T_a - a1/2 w p_a
 #pragma unroll
-      for (int j = 0; j < 5; j++) {
-        const double *Rv = base + (5 * hb + j) * VS;
+      for (int j = 0; j < NB; j++) {
+        const double *Rv = base + (NB * hb + j) * VS;
         const double2 r0 = *reinterpret_cast<const double2 *>(Rv + 0);
         const double pb2 = Rv[2];
         const double pbk = Rv[k], Uk = Rv[3 + k], Wk = PLASTIC ? Rv[6 + k] : 0.0;
@@ -248,8 +270,8 @@ __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec
       }
     }
 #pragma unroll
-    for (int j = 0; j < 5; j++) {
-      const int b = 5 * hb + j;
+    for (int j = 0; j < NB; j++) {
+      const int b = NB * hb + j;
       const int *mB = meta + b * 7;
       const unsigned maskB = ((unsigned)mB[0] >> mB[6]) & 0xFFu;
       if (!((maskB >> k) & 1u)) continue;
@@ -266,15 +288,9 @@ __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec
 }
 
 // asynchronous copy of one element node's data and row metadata
-__device__ __forceinline__ void p2_fetch_node(const AsmArgs &args, long e, int a, int node, double *d, int *m,
+__device__ __forceinline__ void p2_fetch_meta(const AsmArgs &args, long e, int a, int node, int *m,
                                               uint16_t *sp) {
   constexpr int NNE = 10;
-  cpa8(d + 0, args.X + node);
-  cpa8(d + 1, args.X + args.nn + node);
-  cpa8(d + 2, args.X + 2 * args.nn + node);
-  cpa8(d + 3, args.unode + node);
-  cpa8(d + 4, args.unode + args.nn + node);
-  cpa8(d + 5, args.unode + 2 * args.nn + node);
   cpa4(m + 0, args.mask + (node & ~3));  // the aligned word holding the mask byte
   cpa4(m + 1, args.rowptr0 + node);
   cpa4(m + 2, args.rowlen + node);
@@ -285,6 +301,17 @@ __device__ __forceinline__ void p2_fetch_node(const AsmArgs &args, long e, int a
   const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
 #pragma unroll
   for (int j = 0; j < NNE; j += 2) cpa4(sp + j, pr + j);
+}
+
+__device__ __forceinline__ void p2_fetch_node(const AsmArgs &args, long e, int a, int node, double *d, int *m,
+                                              uint16_t *sp) {
+  cpa8(d + 0, args.X + node);
+  cpa8(d + 1, args.X + args.nn + node);
+  cpa8(d + 2, args.X + 2 * args.nn + node);
+  cpa8(d + 3, args.unode + node);
+  cpa8(d + 4, args.unode + args.nn + node);
+  cpa8(d + 5, args.unode + 2 * args.nn + node);
+  p2_fetch_meta(args, e, a, node, m, sp);
 }
 
 template <int MODEL>
@@ -547,6 +574,133 @@ __global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2ws(const AsmArgs ar
       }
       if (tid < TE * 30 && tile_e0(i) + el < ne)
         p2_blocks<PLASTIC>(args, sVec + (bx * TE + el) * kP2ES, sA1 + bx * TE * NQP + el * NQP,
+                           sMeta + bm * kWMT + el * NNE * 7, sPos + bm * kWPS + el * NNE * NNE, a, k);
+      w_mb_arrive(&empty[bx]);
+    }
+  }
+  if (fail && (tid & 31) == 0) atomicAdd(&args.status[3], 1ull);
+}
+
+
+// ---- two-kernel variant: point records from HBM --------------------------
+//
+// The point updates run first in their own kernel (k_qp_update, one thread
+// per point at full occupancy, records as structure of arrays).  This kernel
+// is the pipeline above without them: the producer warp copies a tile's 16
+// point records (38 x 16 doubles, 16-byte cp.async chunks) and its CSR row
+// metadata two tiles ahead and builds the vector records of tile i+1 while the
+// consumer warps run the blocks and reductions of tile i.  Same hand-off and
+// bounded waits as k_assemble_p2ws.
+constexpr int kRRT = kWTE * 4;  // points per tile
+
+inline size_t p2r_smem_bytes() {
+  return 64 + sizeof(double) * (2 * (size_t)kRec * kRRT + 2 * (size_t)kWTE * kP2ES + 2 * (size_t)kRRT) +
+         sizeof(int) * 3 * (size_t)kWMT + sizeof(uint16_t) * 3 * (size_t)kWPS;
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2r(const AsmArgs args) {
+  constexpr int NNE = 10, NQP = 4, TE = kWTE, VS = kP2VS, RT = kRRT;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ __align__(16) unsigned char wsm[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(wsm);       // [2]
+  uint64_t *empty = full + 2;                                // [2]
+  double *sRec = reinterpret_cast<double *>(wsm + 64);       // [2][kRec][RT]
+  double *sVec = sRec + 2 * kRec * RT;                       // [2][TE][kP2ES]
+  double *sA1 = sVec + 2 * TE * kP2ES;                       // [2][TE][NQP]
+  int *sMeta = reinterpret_cast<int *>(sA1 + 2 * RT);        // [3][TE*NNE][7]
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + 3 * kWMT);  // [3][TE*NNE][NNE]
+  const int tid = threadIdx.x;
+  const long ne = args.ne;
+  auto tile_e0 = [&](long i) -> long { return ((long)blockIdx.x + i * (long)gridDim.x) * TE; };
+  if (tid == 0) {
+    w_mb_init(&full[0], 32);
+    w_mb_init(&full[1], 32);
+    w_mb_init(&empty[0], kWCons);
+    w_mb_init(&empty[1], kWCons);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  bool fail = false;
+  if (tid >= kWCons) {
+    // ------------------------------ producer ------------------------------
+    const int pl = tid - kWCons;
+    auto load_nodes = [&](long i, int *nd) {
+      const long e0 = tile_e0(i);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int slot = pl + 32 * j;
+        nd[j] = -1;
+        if (slot < TE * NNE && e0 < ne) {
+          const int el = slot / NNE, a = slot - el * NNE;
+          const long e = e0 + el;
+          if (e < ne) nd[j] = args.conn[(long)a * ne + e];
+        }
+      }
+    };
+    auto issue = [&](long i, const int *nd) {
+      const long e0 = tile_e0(i);
+      const int bx = (int)(i & 1), bm = (int)(i % 3);
+#pragma unroll
+      for (int j = 0; j < 2; j++) {
+        const int slot = pl + 32 * j;
+        if (slot < TE * NNE && nd[j] >= 0) {
+          const int el = slot / NNE, a = slot - el * NNE;
+          p2_fetch_meta(args, e0 + el, a, nd[j], sMeta + bm * kWMT + slot * 7, sPos + bm * kWPS + slot * NNE);
+        }
+      }
+      // records: kRec rows of RT consecutive points, in 16-byte chunks (two
+      // points of one element each; nqp = 4 ne keeps every chunk aligned)
+      const long qp0 = e0 * NQP;
+      for (int ch = pl; ch < kRec * RT / 2; ch += 32) {
+        const int c = ch / (RT / 2), part = ch - c * (RT / 2);
+        if (e0 + part / 2 < ne)
+          cpa16(sRec + (bx * kRec + c) * RT + part * 2, args.qrec + (long)c * args.nqp + qp0 + part * 2);
+      }
+      cpa_commit();
+    };
+    int nd[2], nd_next[2];
+    if (tile_e0(0) < ne) {
+      load_nodes(0, nd);
+      issue(0, nd);
+    }
+    load_nodes(1, nd_next);
+    for (long i = 0; tile_e0(i) < ne; i++) {
+      const int bx = (int)(i & 1);
+      if (i >= 2) {
+        const bool ok = w_mb_wait(&empty[bx], (unsigned)(((i - 2) >> 1) & 1));
+        if (__any_sync(0xffffffffu, !ok)) {
+          fail = true;
+          break;
+        }
+      }
+      cpa_wait_all();  // tile i's records and metadata have landed
+      __syncwarp();
+      if (tile_e0(i + 1) < ne) issue(i + 1, nd_next);
+      load_nodes(i + 2, nd_next);
+      const long e0 = tile_e0(i);
+      for (int it = pl; it < RT * NNE; it += 32) {
+        const int eq = it / NNE, a = it - eq * NNE;
+        const int el = eq / NQP, q = eq - el * NQP;
+        if (e0 + el < ne)
+          p2_vectors<PLASTIC, RT>(args, sRec + bx * kRec * RT + eq, q, a,
+                                  sVec + (bx * TE + el) * kP2ES + (q * NNE + a) * VS, sA1 + bx * RT + eq);
+      }
+      w_mb_arrive(&full[bx]);  // release: this lane's vectors are visible to the consumers
+    }
+    cpa_wait_all();
+  } else {
+    // ------------------------------ consumers ------------------------------
+    const int el = tid / 30, r = tid - el * 30;
+    const int a = r / 3, k = r - a * 3;
+    for (long i = 0; tile_e0(i) < ne; i++) {
+      const int bx = (int)(i & 1), bm = (int)(i % 3);
+      if (!w_mb_wait(&full[bx], (unsigned)((i >> 1) & 1))) {
+        fail = true;
+        break;
+      }
+      if (tid < TE * 30 && tile_e0(i) + el < ne)
+        p2_blocks<PLASTIC, 10>(args, sVec + (bx * TE + el) * kP2ES, sA1 + bx * RT + el * NQP,
                            sMeta + bm * kWMT + el * NNE * 7, sPos + bm * kWPS + el * NNE * NNE, a, k);
       w_mb_arrive(&empty[bx]);
     }

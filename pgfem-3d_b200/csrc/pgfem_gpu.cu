@@ -331,30 +331,35 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+// Point updates of all quadrature points into c->qrec (allocated on first use).
 template <int NNE, int NQP, int MODEL>
-int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
-  if (!c->qrec) {  // point records of the two-kernel mode, allocated on first use
+int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
+  if (!c->qrec) {
     int r = dalloc(c, &c->qrec, (size_t)kQRec * c->nqp);
     if (r) return r;
   }
-  {
-    QpArgs q{};
-    q.X = c->X;
-    q.unode = c->unode;
-    q.conn = c->conn;
-    q.nn = c->nn;
-    q.ne = c->ne;
-    q.nqp = c->nqp;
-    q.F0 = c->F0;
-    q.state_n = c->state_n;
-    q.state_np1 = c->state_np1;
-    q.qrec = c->qrec;
-    q.status = c->status;
-    q.mat = c->mat;
-    q.shp = c->shp;
-    k_qp_update<NNE, NQP, MODEL><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
-    CK(cudaGetLastError());
-  }
+  QpArgs q{};
+  q.X = c->X;
+  q.unode = c->unode;
+  q.conn = c->conn;
+  q.nn = c->nn;
+  q.ne = c->ne;
+  q.nqp = c->nqp;
+  q.F0 = c->F0;
+  q.state_n = c->state_n;
+  q.state_np1 = c->state_np1;
+  q.qrec = c->qrec;
+  q.status = c->status;
+  q.mat = c->mat;
+  q.shp = c->shp;
+  k_qp_update<NNE, NQP, MODEL><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+template <int NNE, int NQP, int MODEL>
+int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
+  if (int r = launch_qp_update<NNE, NQP, MODEL>(c, s)) return r;
   const size_t smem = tiles_smem_bytes<NNE, NQP>(c->nslots_max);
   auto kern = k_assemble_tiles<NNE, NQP, MODEL>;
   constexpr int T = tile_threads<NNE>();
@@ -493,15 +498,42 @@ int launch_p2ws(const AsmArgs &a, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+// quadratic tets in two kernels: point updates into c->qrec, then the
+// pipelined assembly from the records
+template <int MODEL>
+int launch_p2r(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+  if (int r = launch_qp_update<10, 4, MODEL>(c, s)) return r;
+  AsmArgs a = a0;
+  a.qrec = c->qrec;
+  const size_t smem = p2r_smem_bytes();
+  auto kern = k_assemble_p2r<MODEL>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWThreads, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long tiles = (a.ne + kWTE - 1) / kWTE;
+  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
+  kern<<<(unsigned)grid, kWThreads, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 template <bool ATOMIC, bool WANT_K, bool DENSE>
-int dispatch(const pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
+int dispatch(pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
   // quadratic tets, R+K into the CSR with atomic scatter over all elements:
   // the column-split kernel, warp-specialised (PGFEM_GPU_P2_SYNC selects the
   // variant in which all threads run the three phases of a tile in turn)
   if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS")) {
     if (getenv("PGFEM_GPU_P2_SYNC"))
       return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
-    return c->model == PGFEM_MODEL_J2 ? launch_p2ws<1>(a, s) : launch_p2ws<0>(a, s);
+    if (getenv("PGFEM_GPU_P2_FUSED"))
+      return c->model == PGFEM_MODEL_J2 ? launch_p2ws<1>(a, s) : launch_p2ws<0>(a, s);
+    return c->model == PGFEM_MODEL_J2 ? launch_p2r<1>(c, a, s) : launch_p2r<0>(c, a, s);
   }
   // linear tets over all elements: the tuned schedule (elements per block,
   // work stealing)
@@ -946,6 +978,9 @@ int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
     return c->cp_net ? 8 : 5;
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_CELLS && c->nne == 10) return 2;  // u expansion, cells
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
+  if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_ELEMENT_ROWS") &&
+      !getenv("PGFEM_GPU_P2_SYNC") && !getenv("PGFEM_GPU_P2_FUSED"))
+    return 3;  // u expansion, point updates, pipelined R+K assembly
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
 }

@@ -227,9 +227,11 @@ def test_tiled_first_touch_memset_and_untiled_agree(gpu, kind):
 
 @pytest.mark.parametrize("model", ["j2", "he"])
 def test_quadratic_tet_kernel_variants_agree(gpu, model):
-    """The three R+K kernels for 10-node elements (the warp-specialised default,
-    the variant in which all threads run the phases of a tile in turn, and the
-    one-element-per-thread-block kernel) on 162 elements, so that the last
+    """The R+K paths for 10-node elements -- the default (point updates in
+    their own kernel, then the warp-specialised assembly from the point
+    records), the single-kernel warp-specialised variant, the variant in which
+    all threads run the phases of a tile in turn, and the
+    one-element-per-thread-block kernel -- on 162 elements, so that the last
     tile of every variant is partly empty; each against the oracle."""
     import os
     p = wl.j2_p2(n=3, seed=7, perturb=5e-3)
@@ -239,7 +241,7 @@ def test_quadratic_tet_kernel_variants_agree(gpu, model):
     assert p.conn.shape[0] % 8 == 2
     ctx = p.context()
     Ro, Ko, so = oracle_assemble(p)
-    for env in ({}, {"PGFEM_GPU_P2_SYNC": "1"}, {"PGFEM_GPU_ELEMENT_ROWS": "1"}):
+    for env in ({}, {"PGFEM_GPU_P2_FUSED": "1"}, {"PGFEM_GPU_P2_SYNC": "1"}, {"PGFEM_GPU_ELEMENT_ROWS": "1"}):
         os.environ.update(env)
         try:
             R, K, st = ctx.assemble_RK(p.u)
