@@ -691,7 +691,9 @@ __global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2r(const AsmArgs arg
     cpa_wait_all();
   } else {
     // ------------------------------ consumers ------------------------------
-    const int el = tid / 30, r = tid - el * 30;
+    // one warp per element (lanes 30 and 31 idle): the column-node loads of
+    // a warp are broadcasts from a single record
+    const int el = tid >> 5, r = tid & 31;
     const int a = r / 3, k = r - a * 3;
     for (long i = 0; tile_e0(i) < ne; i++) {
       const int bx = (int)(i & 1), bm = (int)(i % 3);
@@ -699,7 +701,7 @@ __global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2r(const AsmArgs arg
         fail = true;
         break;
       }
-      if (tid < TE * 30 && tile_e0(i) + el < ne)
+      if (r < 30 && tile_e0(i) + el < ne)
         p2_blocks<PLASTIC, 10>(args, sVec + (bx * TE + el) * kP2ES, sA1 + bx * RT + el * NQP,
                            sMeta + bm * kWMT + el * NNE * 7, sPos + bm * kWPS + el * NNE * NNE, a, k);
       w_mb_arrive(&empty[bx]);
