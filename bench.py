@@ -165,8 +165,9 @@ def measured_hbm_gbs():
 
 
 def traffic_per_launch():
-    """dram bytes per launch of the assembly kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "k_assemble_p2_j2_p2_traffic.txt")
+    """dram bytes of one R+K iterate's two kernels (point updates, then the
+    assembly) from the committed ncu summary of the J2 quadratic-tet workload."""
+    path = os.path.join(ROOT, "profiles", "k_assemble_p2r_j2_p2_traffic.txt")
     if not os.path.exists(path):
         return None
     for ln in open(path):
@@ -271,7 +272,8 @@ def run_ours(args, ws, rank, local):
     assert st.ok()
     e2e_value = ws * p.nqp * n_e2e / e2e_s
 
-    # roofline of the dominant kernel (the fused assembly kernel)
+    # roofline of the assembly kernels (quadratic tets: the point-update kernel
+    # and the R+K assembly kernel together; linear tets: the fused kernel)
     k_ms = kms / max(kcalls, 1)
     flops = (2.5e3 if he else FLOP_PER_QP) * p.nqp
     nbytes = alg_bytes(p.X.shape[0], p.ndof, p.ne, p.nqp, p.nnz)
@@ -284,8 +286,9 @@ def run_ours(args, ws, rank, local):
         roof = {"bound": "hbm", "achieved": nbytes / (k_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                 "peak_source": hbm_src}
     roof["frac"] = roof["achieved"] / roof["peak"]
-    tr = traffic_per_launch()
-    roof["traffic"] = tr
+    roof["kernel"] = ("k_assemble<4,1,0> (fused R+K)" if he else
+                      "k_qp_update<10,4,1> + k_assemble_p2r<1> (point updates, then R+K)")
+    roof["traffic"] = None if he else traffic_per_launch()
     roof["kernel_ms"] = k_ms
     roof["roofline_ms"] = 1e3 * max(t_fp64, t_hbm)
     roof["frac_of_roofline_step"] = max(t_fp64, t_hbm) / (ms_step * 1e-3)
