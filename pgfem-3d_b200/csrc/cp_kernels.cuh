@@ -106,7 +106,23 @@ __device__ __forceinline__ void schmid(const double *R, int a, double *P) {
     for (int j = 0; j < 3; j++) P[i * 3 + j] = s[i] * n[j];
 }
 
-__device__ __forceinline__ double flow_pow(double r, double e) { return pow(r, e); }
+// |tau/g|^(1/m - 1) of the power-law flow rule.  When the exponent is a small
+// non-negative integer (m = 0.05 gives 19) it is formed by binary
+// exponentiation (repeated squaring: seven multiplies for 19, a few ulp from
+// the correctly rounded power); otherwise pow.  The exponent is the same for
+// every lane, so the branch does not diverge.
+__device__ __forceinline__ double flow_pow(double r, double e) {
+  const int n = (int)e;
+  if ((double)n == e && n >= 0 && n <= 64) {
+    double x = r, y = 1.0;
+    for (int k = n; k; k >>= 1) {
+      if (k & 1) y *= x;
+      x *= x;
+    }
+    return y;
+  }
+  return pow(r, e);
+}
 
 // Residual of the local problem at (M, g).  Returns false on an invalid state.
 struct CpPoint {
