@@ -310,6 +310,76 @@ int pgfem_gpu_cp_training_pairs(pgfem_gpu_ctx *ctx, float *d_x, float *d_t);
 /* Points of the last assembly that fell back to the cold start. */
 int pgfem_gpu_get_cp_fallbacks(pgfem_gpu_ctx *ctx, long *n);
 
+/* ---- linear solve and Newton-Raphson on the device ------------------------
+ * The consumer of K.  The reference solves K dd_u = f with hypre
+ * (src/solvers/hypre/Hypre.cc:147-194): BiCGSTAB (src/solvers/hypre/BCGStab.cc)
+ * preconditioned by diagonal scaling (src/solvers/hypre/ScaleDiag.cc: 1/K_ii,
+ * 1.1 where |K_ii| <= 1e-5), inside its Newton-Raphson loop
+ * (src/Newton_Raphson.cc:931-1330).  A solver holds the CSR pattern on the
+ * device (Ap, Ai of one rank, columns sorted, column id = row id on the
+ * diagonal) and its Krylov work vectors; K values are passed per call. */
+enum { PGFEM_SOLVER_BCG_STAB = 1 };                          /* SOLVER_BCG_STAB */
+enum { PGFEM_PRECOND_NONE = 0, PGFEM_PRECOND_DIAG_SCALE = 1 }; /* PRECOND_DIAG_SCALE */
+
+typedef struct {
+  int solver;      /* PGFEM_SOLVER_BCG_STAB */
+  int precond;     /* PGFEM_PRECOND_* */
+  int maxit;       /* iteration cap (the reference's sol->maxit) */
+  double tol;      /* relative residual ||b - K x|| / ||b|| to reach (sol->err) */
+  int check_every; /* iterations queued between host convergence checks; <= 0: 8 */
+} pgfem_solver_opts;
+
+typedef struct {
+  int iters;       /* BiCGSTAB iterations (SOLVER_INFO n_iter) */
+  double res_norm; /* final relative residual of the recurrence (SOLVER_INFO res_norm) */
+  int converged;   /* res_norm <= tol */
+  int breakdown;   /* a BiCGSTAB denominator vanished or a value was not finite */
+} pgfem_solve_info;
+
+typedef struct pgfem_gpu_solver pgfem_gpu_solver;
+
+/* Copies the pattern to the device; EPATTERN when a column id is out of
+ * range, ENODEV without an sm_100 device. */
+int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfem_solver_opts *opts,
+                            pgfem_gpu_solver **solver);
+int pgfem_gpu_solver_destroy(pgfem_gpu_solver *solver);
+long pgfem_gpu_solver_device_bytes(const pgfem_gpu_solver *solver);
+/* y = K x on `stream` (device pointers; asynchronous). */
+int pgfem_gpu_spmv(pgfem_gpu_solver *solver, const double *d_K, const double *d_x, double *d_y, void *stream);
+/* K x = b by preconditioned BiCGSTAB; d_x holds the initial guess on entry.
+ * Synchronises `stream` at each convergence check. */
+int pgfem_gpu_solve(pgfem_gpu_solver *solver, const double *d_K, const double *d_b, double *d_x,
+                    pgfem_solve_info *info, void *stream);
+
+#define PGFEM_NEWTON_HISTORY 32
+typedef struct {
+  int iter_max;         /* Newton iteration cap (sol->iter_max) */
+  double nor_min;       /* converged when ||R|| / ||R_0|| <= nor_min (sol->nor_min) */
+  double computer_zero; /* ... or when ||R|| <= computer_zero (sol->computer_zero) */
+} pgfem_newton_opts;
+
+typedef struct {
+  int iters;          /* Newton iterations (solves) taken */
+  int converged;
+  int lin_iters;      /* BiCGSTAB iterations summed over the solves */
+  int lin_failed;     /* a linear solve missed its tolerance */
+  long elem_failures; /* element/point failures reported by the assemblies */
+  double nor, nor2;   /* last ||R|| / ||R_0|| and ||R|| */
+  double nor_hist[PGFEM_NEWTON_HISTORY]; /* ||R|| / ||R_0|| per iteration */
+} pgfem_newton_info;
+
+/* One load step of full Newton-Raphson (stiffness every iteration, no line
+ * search): from the free-DOF displacement d_u (updated in place) and the
+ * prescribed values of the step, assemble R and K on the device
+ * (pgfem_gpu_assemble_RK_device), solve K du = -R with the solver, u += du,
+ * until the reference's test nor = ||R|| / ||R_0|| <= nor_min or
+ * ||R|| <= computer_zero (src/Newton_Raphson.cc:1203-1217, 1323).  The state
+ * at t_{n+1} in the context is the one of the last assembly: commit it with
+ * pgfem_gpu_commit_state after a converged step.  Returns a negative code
+ * on usage/CUDA errors; non-convergence is reported in info. */
+int pgfem_gpu_newton_step(pgfem_gpu_ctx *ctx, pgfem_gpu_solver *solver, double *d_u, const double *d_u_presc,
+                          double dt, const pgfem_newton_opts *opts, pgfem_newton_info *info, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

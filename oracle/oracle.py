@@ -189,6 +189,36 @@ class Problem:
         return err, R, K, snp1
 
 
+def newton_step(P, mat, u0, u_presc=None, state_n=None, dt=0.0, iter_max=10, nor_min=1e-10,
+                computer_zero=1e-15, nthreads=8):
+    """One load step of full Newton-Raphson on the CPU, the checker of
+    pgfem_gpu_newton_step: the reference's loop (src/Newton_Raphson.cc:931-1330
+    with FNR = 1, no line search) -- assemble R and K, nor = ||R|| / ||R_0||
+    (:1203-1217), stop when nor <= nor_min or ||R|| <= computer_zero (:1323),
+    else solve K du = -R (here a sparse direct solve) and u += du.
+    Returns (u, [nor per iteration], converged, state_np1)."""
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.linalg import spsolve
+    u = np.array(u0, dtype=np.float64, copy=True)
+    hist, NORM = [], 1.0
+    for it in range(iter_max + 1):
+        err, R, K, snp1 = P.assemble(mat, u, u_presc, state_n=state_n, dt=dt, nthreads=nthreads)
+        if err:
+            return u, hist, False, snp1
+        nor2 = float(np.linalg.norm(R))
+        if it == 0:
+            NORM = nor2 if nor2 > computer_zero else (computer_zero if computer_zero > 0 else 1.0)
+        nor = nor2 / NORM
+        hist.append(nor)
+        if nor <= nor_min or nor2 <= computer_zero:
+            return u, hist, True, snp1
+        if it >= iter_max:
+            return u, hist, False, snp1
+        Km = csr_matrix((K, P.Ai, P.Ap), shape=(P.ndof, P.ndof))
+        u = u + spsolve(Km.tocsc(), -R)
+    return u, hist, False, snp1
+
+
 def from_workload(p):
     """Oracle Problem + material for a pgfem-3d_b200 workloads.Problem."""
     return Problem(p.X, p.conn, p.ids, p.ndof, p.Ap, p.Ai, F0=p.F0, R_cp=p.R_cp), from_pg_material(p.mat)

@@ -1,0 +1,536 @@
+// solver.cu -- linear solve and Newton-Raphson load step on the device.
+//
+// The consumer of the assembled operator.  The reference hands K and the
+// residual to hypre (src/solvers/hypre/Hypre.cc:147-194) and iterates
+// Newton-Raphson around it (src/Newton_Raphson.cc:931-1330).  Here:
+//
+//  - CSR SpMV, one warp per row: the row's values and column ids are read
+//    contiguously (12 bytes per non-zero from HBM), the vector is gathered
+//    through L2; the Krylov dot products that follow a product are fused into
+//    it (per-block partial sums);
+//  - BiCGSTAB (BCGStab.cc) with right preconditioning by diagonal scaling
+//    (ScaleDiag.cc: 1/K_ii, or 1.1 where |K_ii| <= 1e-5) or none.  All Krylov
+//    scalars live in device memory and are formed by one-block finalize
+//    kernels, so an iteration is a fixed sequence of launches with no host
+//    round trip; every kernel returns at once when the device-side `done`
+//    flag is set (converged or broken down), so the host queues several
+//    iterations between convergence checks.  Reductions sum per-block
+//    partials in a fixed order: the result does not depend on timing;
+//  - pgfem_gpu_newton_step: full Newton (stiffness every iteration, FNR = 1)
+//    for one load step through the public assembly entry point, converged
+//    when ||R|| / ||R_0|| <= nor_min or ||R|| <= computer_zero (the
+//    reference's nor / nor2 test, :1203-1217, 1323).  No line search.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+#include "pgfem_gpu.h"
+
+namespace {
+
+constexpr int kBlk = 256;            // threads per block of every vector kernel
+constexpr int kFin = 1024;           // threads of the one-block finalize kernels
+constexpr int kBlocksPerSm = 8;      // grid-stride grids: 8 blocks per SM
+constexpr double kDiagThresh = 1e-5, kDiagReplace = 1.1;  // ScaleDiag.cc constants
+
+// Device-resident BiCGSTAB state.
+struct Scalars {
+  double rho, rho_new, alpha, omega;
+  double bnorm2, rnorm2, tol2;
+  int iter, done, breakdown, pad;
+};
+
+enum Stage { kInit = 0, kAlpha = 1, kOmega = 2, kRho = 3, kNorm = 4 };
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Block sum of two values into part0/part1[blockIdx.x] (thread 0 writes).
+__device__ __forceinline__ void block_partials(double d0, double d1, double *part0, double *part1) {
+  __shared__ double s0[kBlk / 32], s1[kBlk / 32];
+  d0 = warp_sum(d0);
+  d1 = warp_sum(d1);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) {
+    s0[w] = d0;
+    s1[w] = d1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < kBlk / 32; i++) {
+      a += s0[i];
+      b += s1[i];
+    }
+    if (part0) part0[blockIdx.x] = a;
+    if (part1) part1[blockIdx.x] = b;
+  }
+}
+
+// y = K x; with w0: partial (w0, y); with self: partial (y, y).
+// One warp per row, grid-stride over rows.
+__global__ void __launch_bounds__(kBlk) k_spmv(long n, const int *__restrict__ Ap, const int *__restrict__ Ai,
+                                               const double *__restrict__ K, const double *__restrict__ x,
+                                               double *__restrict__ y, const double *__restrict__ w0, int self,
+                                               double *part0, double *part1, const Scalars *S) {
+  if (S && S->done) return;
+  const int lane = threadIdx.x & 31;
+  const long warp0 = ((long)blockIdx.x * kBlk + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * kBlk) >> 5;
+  double d0 = 0.0, d1 = 0.0;
+  for (long i = warp0; i < n; i += nwarps) {
+    const int b = Ap[i], e = Ap[i + 1];
+    double acc = 0.0;
+    for (int j = b + lane; j < e; j += 32) acc = fma(K[j], x[Ai[j]], acc);
+    acc = warp_sum(acc);
+    if (lane == 0) {
+      y[i] = acc;
+      if (w0) d0 = fma(w0[i], acc, d0);
+      if (self) d1 = fma(acc, acc, d1);
+    }
+  }
+  if (part0 || part1) block_partials(d0, d1, part0, part1);
+}
+
+// dinv[i] = 1 / K_ii (|K_ii| > thresh), else the replacement; 1 without
+// preconditioning.
+__global__ void k_diag_scale(long n, const long *__restrict__ dpos, const double *__restrict__ K, int precond,
+                             double *__restrict__ dinv) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double v = 1.0;
+    if (precond == PGFEM_PRECOND_DIAG_SCALE) {
+      const double d = dpos[i] >= 0 ? K[dpos[i]] : 0.0;
+      v = fabs(d) > kDiagThresh ? 1.0 / d : kDiagReplace;
+    }
+    dinv[i] = v;
+  }
+}
+
+// r = b - Ax (Ax in r on entry), rh = r, p = v = 0; partials (r, r), (b, b).
+__global__ void __launch_bounds__(kBlk) k_init(long n, const double *__restrict__ b, double *__restrict__ r,
+                                               double *__restrict__ rh, double *__restrict__ p,
+                                               double *__restrict__ v, double *part0, double *part1) {
+  double d0 = 0.0, d1 = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    const double ri = b[i] - r[i];
+    r[i] = ri;
+    rh[i] = ri;
+    p[i] = 0.0;
+    v[i] = 0.0;
+    d0 = fma(ri, ri, d0);
+    d1 = fma(b[i], b[i], d1);
+  }
+  block_partials(d0, d1, part0, part1);
+}
+
+// p = r + beta (p - omega v), ph = dinv p  (first iteration: p = r).
+__global__ void __launch_bounds__(kBlk) k_update_p(long n, const double *__restrict__ r, double *__restrict__ p,
+                                                   const double *__restrict__ v, const double *__restrict__ dinv,
+                                                   double *__restrict__ ph, const Scalars *S) {
+  if (S->done) return;
+  const double beta = S->iter == 0 ? 0.0 : (S->rho_new / S->rho) * (S->alpha / S->omega);
+  const double om = S->omega;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    const double pi = S->iter == 0 ? r[i] : r[i] + beta * (p[i] - om * v[i]);
+    p[i] = pi;
+    ph[i] = dinv[i] * pi;
+  }
+}
+
+// s = r - alpha v, sh = dinv s  (s stored in place of r).
+__global__ void __launch_bounds__(kBlk) k_update_s(long n, double *__restrict__ r, const double *__restrict__ v,
+                                                   const double *__restrict__ dinv, double *__restrict__ sh,
+                                                   const Scalars *S) {
+  if (S->done) return;
+  const double al = S->alpha;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    const double si = r[i] - al * v[i];
+    r[i] = si;
+    sh[i] = dinv[i] * si;
+  }
+}
+
+// x += alpha ph + omega sh, r = s - omega t; partials (rh, r), (r, r).
+__global__ void __launch_bounds__(kBlk) k_update_xr(long n, double *__restrict__ x, const double *__restrict__ ph,
+                                                    const double *__restrict__ sh, double *__restrict__ r,
+                                                    const double *__restrict__ t, const double *__restrict__ rh,
+                                                    double *part0, double *part1, const Scalars *S) {
+  if (S->done) return;
+  const double al = S->alpha, om = S->omega;
+  double d0 = 0.0, d1 = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    x[i] += al * ph[i] + om * sh[i];
+    const double ri = r[i] - om * t[i];
+    r[i] = ri;
+    d0 = fma(rh[i], ri, d0);
+    d1 = fma(ri, ri, d1);
+  }
+  block_partials(d0, d1, part0, part1);
+}
+
+// One block: sums the partials in a fixed order and advances the scalars.
+__global__ void __launch_bounds__(kFin) k_finalize(int nblocks, const double *part0, const double *part1, int stage,
+                                                   Scalars *S, double *out) {
+  if (stage != kInit && stage != kNorm && S->done) return;
+  __shared__ double s0[kFin], s1[kFin];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nblocks; i += kFin) {
+    a += part0[i];
+    if (part1) b += part1[i];
+  }
+  s0[threadIdx.x] = a;
+  s1[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = kFin / 2; o; o >>= 1) {
+    if (threadIdx.x < o) {
+      s0[threadIdx.x] += s0[threadIdx.x + o];
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x) return;
+  const double d0 = s0[0], d1 = s1[0];
+  switch (stage) {
+    case kInit:  // d0 = (r, r), d1 = (b, b)
+      S->rho = S->alpha = S->omega = 1.0;
+      S->rho_new = d0;
+      S->rnorm2 = d0;
+      S->bnorm2 = d1;
+      S->iter = 0;
+      S->breakdown = 0;
+      S->done = (d0 <= S->tol2 * d1) ? 1 : 0;
+      break;
+    case kAlpha:  // d0 = (rh, v)
+      if (d0 == 0.0 || !isfinite(d0)) {
+        S->breakdown = 1;
+        S->done = 1;
+      } else {
+        S->alpha = S->rho_new / d0;
+      }
+      break;
+    case kOmega:  // d0 = (t, s), d1 = (t, t)
+      if (d1 == 0.0 || !isfinite(d1)) {
+        S->breakdown = 1;
+        S->done = 1;
+      } else {
+        S->omega = d0 / d1;
+      }
+      break;
+    case kRho:  // d0 = (rh, r), d1 = (r, r)
+      S->rho = S->rho_new;
+      S->rho_new = d0;
+      S->rnorm2 = d1;
+      S->iter += 1;
+      if (!isfinite(d1)) {
+        S->breakdown = 1;
+        S->done = 1;
+      } else if (d1 <= S->tol2 * S->bnorm2) {
+        S->done = 1;
+      } else if (d0 == 0.0 || S->omega == 0.0) {
+        S->breakdown = 1;
+        S->done = 1;
+      }
+      break;
+    case kNorm:  // plain dot product into *out
+      *out = d0;
+      break;
+  }
+}
+
+// y = a x + y  /  y = a x
+__global__ void k_axpy(long n, double a, const double *__restrict__ x, double *__restrict__ y, int overwrite) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    y[i] = overwrite ? a * x[i] : fma(a, x[i], y[i]);
+}
+
+// x = -x
+__global__ void k_negate(long n, double *x) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) x[i] = -x[i];
+}
+
+__global__ void __launch_bounds__(kBlk) k_dot(long n, const double *__restrict__ a, const double *__restrict__ b,
+                                              double *part0) {
+  double d = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) d = fma(a[i], b[i], d);
+  block_partials(d, 0.0, part0, nullptr);
+}
+
+// Position of the diagonal entry of every row (-1 when the row has none).
+void find_diagonal(const int *Ap, const int *Ai, long n, long *dpos) {
+  for (long i = 0; i < n; i++) {
+    dpos[i] = -1;
+    int lo = Ap[i], hi = Ap[i + 1];
+    while (lo < hi) {  // columns sorted ascending
+      const int mid = (lo + hi) >> 1;
+      if (Ai[mid] < i) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < Ap[i + 1] && Ai[lo] == i) dpos[i] = lo;
+  }
+}
+
+int g_sms = 0;
+int grid_size() {
+  if (!g_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sms <= 0) g_sms = 148;
+  }
+  return g_sms * kBlocksPerSm;
+}
+
+int device_ok() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return 0;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  return major >= 10;
+}
+
+}  // namespace
+
+struct pgfem_gpu_solver {
+  long n = 0, nnz = 0;
+  pgfem_solver_opts opts{};
+  int grid = 0;
+  int *Ap = nullptr, *Ai = nullptr;
+  long *dpos = nullptr;
+  double *dinv = nullptr, *r = nullptr, *rh = nullptr, *p = nullptr, *v = nullptr, *ph = nullptr, *sh = nullptr,
+         *t = nullptr;
+  double *part0 = nullptr, *part1 = nullptr, *dot_out = nullptr;
+  Scalars *S = nullptr;
+  Scalars *hS = nullptr;  // pinned host copy
+  // Newton buffers (allocated by the first newton_step)
+  double *R = nullptr, *K = nullptr, *du = nullptr;
+  long bytes = 0;
+};
+
+namespace {
+
+template <class T>
+int salloc(pgfem_gpu_solver *s, T **p, size_t n) {
+  if (cudaMalloc((void **)p, (n ? n : 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return PGFEM_GPU_ENOMEM;
+  }
+  s->bytes += (long)((n ? n : 1) * sizeof(T));
+  return PGFEM_GPU_OK;
+}
+
+void release(pgfem_gpu_solver *s) {
+  void *ptrs[] = {s->Ap, s->Ai, s->dpos, s->dinv, s->r, s->rh, s->p, s->v, s->ph, s->sh, s->t,
+                  s->part0, s->part1, s->dot_out, s->S, s->R, s->K, s->du};
+  for (void *p : ptrs)
+    if (p) cudaFree(p);
+  if (s->hS) cudaFreeHost(s->hS);
+}
+
+#define SK(x)                         \
+  do {                                \
+    if ((x) != cudaSuccess) {         \
+      cudaGetLastError();             \
+      return PGFEM_GPU_ECUDA;         \
+    }                                 \
+  } while (0)
+
+int ew_grid(const pgfem_gpu_solver *s) {
+  const long need = (s->n + kBlk - 1) / kBlk;
+  return (int)(need < s->grid ? (need > 0 ? need : 1) : s->grid);
+}
+
+// ||a||^2 or (a, b) on the stream into s->dot_out (device)
+int dot_device(pgfem_gpu_solver *s, const double *a, const double *b, cudaStream_t st) {
+  const int g = ew_grid(s);
+  k_dot<<<g, kBlk, 0, st>>>(s->n, a, b, s->part0);
+  k_finalize<<<1, kFin, 0, st>>>(g, s->part0, nullptr, kNorm, s->S, s->dot_out);
+  SK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+int solve_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x, pgfem_solve_info *info,
+               cudaStream_t st) {
+  const long n = s->n;
+  const int g = ew_grid(s);
+  const int gs = s->grid;  // SpMV grid (warp per row, grid-stride)
+  // tolerance into the device scalars, preconditioner, initial residual
+  Scalars init{};
+  init.tol2 = s->opts.tol * s->opts.tol;
+  SK(cudaMemcpyAsync(s->S, &init, sizeof(Scalars), cudaMemcpyHostToDevice, st));
+  k_diag_scale<<<g, kBlk, 0, st>>>(n, s->dpos, K, s->opts.precond, s->dinv);
+  k_spmv<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, x, s->r, nullptr, 0, nullptr, nullptr, nullptr);
+  k_init<<<g, kBlk, 0, st>>>(n, b, s->r, s->rh, s->p, s->v, s->part0, s->part1);
+  k_finalize<<<1, kFin, 0, st>>>(g, s->part0, s->part1, kInit, s->S, nullptr);
+  SK(cudaGetLastError());
+  const int every = s->opts.check_every > 0 ? s->opts.check_every : 8;
+  int queued = 0;
+  for (;;) {
+    const int k = (s->opts.maxit - queued) < every ? (s->opts.maxit - queued) : every;
+    for (int it = 0; it < k; it++) {
+      k_update_p<<<g, kBlk, 0, st>>>(n, s->r, s->p, s->v, s->dinv, s->ph, s->S);
+      k_spmv<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, s->ph, s->v, s->rh, 0, s->part0, nullptr, s->S);
+      k_finalize<<<1, kFin, 0, st>>>(gs, s->part0, nullptr, kAlpha, s->S, nullptr);
+      k_update_s<<<g, kBlk, 0, st>>>(n, s->r, s->v, s->dinv, s->sh, s->S);
+      k_spmv<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, s->sh, s->t, s->r, 1, s->part0, s->part1, s->S);
+      k_finalize<<<1, kFin, 0, st>>>(gs, s->part0, s->part1, kOmega, s->S, nullptr);
+      k_update_xr<<<g, kBlk, 0, st>>>(n, x, s->ph, s->sh, s->r, s->t, s->rh, s->part0, s->part1, s->S);
+      k_finalize<<<1, kFin, 0, st>>>(g, s->part0, s->part1, kRho, s->S, nullptr);
+    }
+    SK(cudaGetLastError());
+    queued += k;
+    SK(cudaMemcpyAsync(s->hS, s->S, sizeof(Scalars), cudaMemcpyDeviceToHost, st));
+    SK(cudaStreamSynchronize(st));
+    if (s->hS->done || queued >= s->opts.maxit) break;
+  }
+  const Scalars &h = *s->hS;
+  if (info) {
+    info->iters = h.iter;
+    info->res_norm = h.bnorm2 > 0.0 ? std::sqrt(h.rnorm2 / h.bnorm2) : std::sqrt(h.rnorm2);
+    info->converged = (h.done && !h.breakdown && h.rnorm2 <= init.tol2 * h.bnorm2) ? 1 : 0;
+    info->breakdown = h.breakdown;
+  }
+  return PGFEM_GPU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfem_solver_opts *opts,
+                            pgfem_gpu_solver **out) {
+  if (!out) return PGFEM_GPU_EINVAL;
+  *out = nullptr;
+  if (!Ap || !Ai || nrows <= 0 || !opts || opts->maxit <= 0 || !(opts->tol > 0.0) ||
+      opts->solver != PGFEM_SOLVER_BCG_STAB ||
+      (opts->precond != PGFEM_PRECOND_NONE && opts->precond != PGFEM_PRECOND_DIAG_SCALE))
+    return PGFEM_GPU_EINVAL;
+  if (Ap[0] != 0) return PGFEM_GPU_EINVAL;
+  for (long i = 0; i < nrows; i++)
+    if (Ap[i + 1] < Ap[i]) return PGFEM_GPU_EINVAL;
+  const long nnz = Ap[nrows];
+  for (long j = 0; j < nnz; j++)
+    if (Ai[j] < 0 || Ai[j] >= nrows) return PGFEM_GPU_EPATTERN;
+  if (!device_ok()) return PGFEM_GPU_ENODEV;
+  pgfem_gpu_solver *s = new pgfem_gpu_solver();
+  s->n = nrows;
+  s->nnz = nnz;
+  s->opts = *opts;
+  s->grid = grid_size();
+  long *hdpos = new long[nrows];
+  find_diagonal(Ap, Ai, nrows, hdpos);
+  int r = PGFEM_GPU_OK;
+  if ((r = salloc(s, &s->Ap, nrows + 1)) || (r = salloc(s, &s->Ai, nnz)) || (r = salloc(s, &s->dpos, nrows)) ||
+      (r = salloc(s, &s->dinv, nrows)) || (r = salloc(s, &s->r, nrows)) || (r = salloc(s, &s->rh, nrows)) ||
+      (r = salloc(s, &s->p, nrows)) || (r = salloc(s, &s->v, nrows)) || (r = salloc(s, &s->ph, nrows)) ||
+      (r = salloc(s, &s->sh, nrows)) || (r = salloc(s, &s->t, nrows)) || (r = salloc(s, &s->part0, s->grid)) ||
+      (r = salloc(s, &s->part1, s->grid)) || (r = salloc(s, &s->dot_out, 1)) || (r = salloc(s, &s->S, 1))) {
+    delete[] hdpos;
+    release(s);
+    delete s;
+    return r;
+  }
+  if (cudaMallocHost((void **)&s->hS, sizeof(Scalars)) != cudaSuccess ||
+      cudaMemcpy(s->Ap, Ap, sizeof(int) * (nrows + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->Ai, Ai, sizeof(int) * nnz, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(s->dpos, hdpos, sizeof(long) * nrows, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    delete[] hdpos;
+    release(s);
+    delete s;
+    return PGFEM_GPU_ECUDA;
+  }
+  delete[] hdpos;
+  *out = s;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_solver_destroy(pgfem_gpu_solver *s) {
+  if (!s) return PGFEM_GPU_EINVAL;
+  release(s);
+  delete s;
+  return PGFEM_GPU_OK;
+}
+
+long pgfem_gpu_solver_device_bytes(const pgfem_gpu_solver *s) { return s ? s->bytes : -1; }
+
+int pgfem_gpu_spmv(pgfem_gpu_solver *s, const double *d_K, const double *d_x, double *d_y, void *stream) {
+  if (!s || !d_K || !d_x || !d_y) return PGFEM_GPU_EINVAL;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_spmv<<<s->grid, kBlk, 0, st>>>(s->n, s->Ap, s->Ai, d_K, d_x, d_y, nullptr, 0, nullptr, nullptr, nullptr);
+  SK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_solve(pgfem_gpu_solver *s, const double *d_K, const double *d_b, double *d_x,
+                    pgfem_solve_info *info, void *stream) {
+  if (!s || !d_K || !d_b || !d_x) return PGFEM_GPU_EINVAL;
+  return solve_impl(s, d_K, d_b, d_x, info, (cudaStream_t)stream);
+}
+
+int pgfem_gpu_newton_step(pgfem_gpu_ctx *ctx, pgfem_gpu_solver *s, double *d_u, const double *d_u_presc,
+                          double dt, const pgfem_newton_opts *o, pgfem_newton_info *info, void *stream) {
+  if (!ctx || !s || !d_u || !o || !info || o->iter_max <= 0 || !(o->nor_min > 0.0)) return PGFEM_GPU_EINVAL;
+  if (pgfem_gpu_nnz(ctx) != s->nnz) return PGFEM_GPU_EPATTERN;
+  std::memset(info, 0, sizeof(*info));
+  cudaStream_t st = (cudaStream_t)stream;
+  int r;
+  if (!s->R && ((r = salloc(s, &s->R, s->n)) || (r = salloc(s, &s->K, s->nnz)) || (r = salloc(s, &s->du, s->n))))
+    return r;
+  const int g = ew_grid(s);
+  double NORM = 0.0;
+  for (int iter = 0;; iter++) {
+    if ((r = pgfem_gpu_assemble_RK_device(ctx, d_u, d_u_presc, dt, s->R, s->K, stream))) return r;
+    if ((r = dot_device(s, s->R, s->R, st))) return r;
+    double nrm2 = 0.0;
+    SK(cudaMemcpyAsync(&nrm2, s->dot_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+    SK(cudaStreamSynchronize(st));
+    pgfem_gpu_status es;
+    if ((r = pgfem_gpu_read_status(ctx, &es, 1))) return r;
+    info->elem_failures += es.inverted + es.nonconverged + es.bad_diagonal + es.other;
+    const double nor2 = std::sqrt(nrm2);
+    if (iter == 0) NORM = nor2 > o->computer_zero ? nor2 : (o->computer_zero > 0.0 ? o->computer_zero : 1.0);
+    const double nor = nor2 / NORM;
+    if (iter < PGFEM_NEWTON_HISTORY) info->nor_hist[iter] = nor;
+    info->iters = iter;
+    info->nor = nor;
+    info->nor2 = nor2;
+    if (!std::isfinite(nor) || info->elem_failures) {
+      info->converged = 0;
+      return PGFEM_GPU_OK;
+    }
+    if (nor <= o->nor_min || nor2 <= o->computer_zero) {
+      info->converged = 1;
+      return PGFEM_GPU_OK;
+    }
+    if (iter >= o->iter_max) {
+      info->converged = 0;
+      return PGFEM_GPU_OK;
+    }
+    // K du = -R, du from zero
+    k_negate<<<g, kBlk, 0, st>>>(s->n, s->R);
+    SK(cudaMemsetAsync(s->du, 0, sizeof(double) * s->n, st));
+    SK(cudaGetLastError());
+    pgfem_solve_info si{};
+    if ((r = solve_impl(s, s->K, s->R, s->du, &si, st))) return r;
+    info->lin_iters += si.iters;
+    if (!si.converged) {
+      info->lin_failed = 1;
+      info->converged = 0;
+      return PGFEM_GPU_OK;
+    }
+    k_axpy<<<g, kBlk, 0, st>>>(s->n, 1.0, s->du, d_u, 0);
+    SK(cudaGetLastError());
+  }
+}
+
+}  // extern "C"

@@ -113,6 +113,12 @@ def lib():
             "pgfem_gpu_graph_launch": (C.c_int, [_P, _P]),
             "pgfem_gpu_graph_destroy": (C.c_int, [_P]),
             "pgfem_gpu_autotune": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, C.c_int, _P, _P, _P]),
+            "pgfem_gpu_solver_create": (C.c_int, [_P, _P, C.c_long, _P, _P]),
+            "pgfem_gpu_solver_destroy": (C.c_int, [_P]),
+            "pgfem_gpu_solver_device_bytes": (C.c_long, [_P]),
+            "pgfem_gpu_spmv": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_gpu_solve": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_newton_step": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -495,3 +501,76 @@ class Graph:
         if getattr(self, "h", None) and _lib is not None:
             _lib.pgfem_gpu_graph_destroy(self.h)
             self.h = None
+
+
+# ---- linear solve and Newton-Raphson --------------------------------------
+SOLVER_BCG_STAB = 1
+PRECOND_NONE, PRECOND_DIAG_SCALE = 0, 1
+NEWTON_HISTORY = 32
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("maxit", C.c_int), ("tol", C.c_double),
+                ("check_every", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("res_norm", C.c_double), ("converged", C.c_int), ("breakdown", C.c_int)]
+
+
+class NewtonOpts(C.Structure):
+    _fields_ = [("iter_max", C.c_int), ("nor_min", C.c_double), ("computer_zero", C.c_double)]
+
+
+class NewtonInfo(C.Structure):
+    _fields_ = [("iters", C.c_int), ("converged", C.c_int), ("lin_iters", C.c_int), ("lin_failed", C.c_int),
+                ("elem_failures", C.c_long), ("nor", C.c_double), ("nor2", C.c_double),
+                ("nor_hist", C.c_double * NEWTON_HISTORY)]
+
+    def history(self):
+        return [self.nor_hist[i] for i in range(min(self.iters + 1, NEWTON_HISTORY))]
+
+
+class Solver:
+    """Device linear solver over one CSR pattern (pgfem_gpu_solver_*)."""
+
+    def __init__(self, Ap, Ai, nrows, precond=PRECOND_DIAG_SCALE, maxit=5000, tol=1e-10, check_every=8):
+        self._Ap = np.ascontiguousarray(Ap, dtype=np.int32)
+        self._Ai = np.ascontiguousarray(Ai, dtype=np.int32)
+        self.n = int(nrows)
+        self.nnz = int(self._Ap[-1])
+        self.opts = SolverOpts(SOLVER_BCG_STAB, precond, maxit, tol, check_every)
+        h = C.c_void_p()
+        _check("pgfem_gpu_solver_create", lib().pgfem_gpu_solver_create(_ptr(self._Ap), _ptr(self._Ai), self.n,
+                                                                        C.byref(self.opts), C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().pgfem_gpu_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self):
+        return lib().pgfem_gpu_solver_device_bytes(self.h)
+
+    def spmv(self, d_K, d_x, d_y, stream=None):
+        _check("pgfem_gpu_spmv", lib().pgfem_gpu_spmv(self.h, d_K, d_x, d_y, stream))
+
+    def solve(self, d_K, d_b, d_x, stream=None):
+        info = SolveInfo()
+        _check("pgfem_gpu_solve", lib().pgfem_gpu_solve(self.h, d_K, d_b, d_x, C.byref(info), stream))
+        return info
+
+    def newton_step(self, ctx, d_u, d_presc=None, dt=0.0, iter_max=10, nor_min=1e-10, computer_zero=1e-15,
+                    stream=None):
+        o = NewtonOpts(iter_max, nor_min, computer_zero)
+        info = NewtonInfo()
+        _check("pgfem_gpu_newton_step", lib().pgfem_gpu_newton_step(ctx.h, self.h, d_u, d_presc, dt, C.byref(o),
+                                                                    C.byref(info), stream))
+        return info

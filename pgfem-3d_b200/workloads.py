@@ -97,6 +97,31 @@ def he_p1(n=10, seed=0):
     return Problem("he_p1_n%d" % n, X, conn, ids, ndof, Ap, Ai, mat, u, meta=dict(n=n, seed=seed))
 
 
+def tension(n=4, nne=4, model="he", stretch=0.01):
+    """Uniaxial tension of the unit cube for a Newton-Raphson load step: the
+    x = 0 face fixed, the x-displacement of the x = 1 face prescribed
+    (one prescribed value, u_presc[0] = stretch), every other DOF free and
+    starting from zero.  model "he" (neo-Hookean) or "j2" (state at identity)."""
+    X, conn, _ = pg.mesh_box_tet(n, nne)
+    nn = X.shape[0]
+    codes = np.zeros((nn, 3), dtype=np.int64)
+    codes[X[:, 0] == 0.0] = 1
+    codes[X[:, 0] == 1.0, 0] = -1
+    ids, ndof = pg.generate_dof_ids(conn, nn, codes)
+    Ap, Ai = pg.psparse_apai(conn, ids, ndof)
+    if model == "he":
+        mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.3)
+        state = None
+    else:
+        mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
+        nqp = conn.shape[0] * (4 if nne == 10 else 1)
+        state = np.zeros((nqp, 10))
+        state[:, [0, 4, 8]] = 1.0
+    return Problem("tension_%s_p%d_n%d" % (model, 1 if nne == 4 else 2, n), X, conn, ids, ndof, Ap, Ai, mat,
+                   np.zeros(ndof), u_presc=np.array([stretch]), state=state,
+                   meta=dict(n=n, stretch=stretch, model=model))
+
+
 def j2_yield_strain(E=200e3, nu=0.3, sigma_y=250.0):
     mu = E / (2.0 * (1.0 + nu))
     return sigma_y / (2.0 * mu)
