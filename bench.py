@@ -726,6 +726,151 @@ def run_rve(args, ws, rank, local):
     return out
 
 
+NR_METRIC = "Newton-Raphson load steps/sec (device assembly + GMRES), SpMV % of HBM roofline"
+
+
+def run_nr(args, ws, rank, local):
+    """One Newton-Raphson load step on the device (the consumer of K): J2
+    quadratic tets, `--nr-n`^3 cells, x = 0 face fixed, x = 1 face pulled to
+    `--nr-stretch` in one step from the linear predictor u_x = stretch x; each
+    Newton iteration assembles R and K on the device and solves K du = -R with
+    GMRES(kdim) + diagonal scaling (pgfem_gpu_newton_step).  A step = state
+    reset, u = predictor, the whole Newton loop.  Roofline: the CSR SpMV that dominates the
+    solve, timed alone on the step's K (HBM-bound: 12 bytes per non-zero)."""
+    import torch
+
+    import pgfem_gpu as pg
+    import workloads as wl
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    t0 = time.perf_counter()
+    p = wl.tension(n=args.nr_n, nne=10, model="j2", stretch=args.nr_stretch, predictor=True)
+    ctx = p.context()
+    solver = pg.Solver(p.Ap, p.Ai, p.ndof, maxit=args.nr_maxit, kdim=args.nr_kdim, tol=args.nr_tol)
+    log("[rank %d] tension J2 P2 n=%d: %d elements, %d DOFs, %d nnz, set up in %.1f s"
+        % (rank, args.nr_n, p.ne, p.ndof, p.nnz, time.perf_counter() - t0))
+    hbm_peak, hbm_src = measured_hbm_gbs()
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    d_u0 = torch.from_numpy(p.u.copy()).to(dev)
+    d_u = torch.empty_like(d_u0)
+    d_p = torch.from_numpy(p.u_presc.copy()).to(dev)
+    infos = []
+
+    def step():
+        ctx.reset_state()
+        d_u.copy_(d_u0)
+        info = solver.newton_step(ctx, d_u.data_ptr(), d_p.data_ptr(), iter_max=20, nor_min=args.nr_nor_min,
+                                  stream=sh)
+        assert info.converged and info.elem_failures == 0, (info.iters, info.history())
+        return info
+
+    for _ in range(args.warmup):
+        infos.append(step())
+    nsteps = max(1, min(args.steps, args.nr_steps))
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(nsteps):
+        infos.append(step())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clocks = clk.stop()
+    ms_step = allreduce_max(e0.elapsed_time(e1), ws) / nsteps
+    info = infos[-1]
+    # split: the assemblies of the step, timed alone
+    d_R = torch.empty(p.ndof, dtype=torch.float64, device=dev)
+    d_K = torch.empty(p.nnz, dtype=torch.float64, device=dev)
+    ctx.set_timing(True)
+    ctx.kernel_time(reset=True)
+    for _ in range(3):
+        ctx.assemble_RK_device(d_u.data_ptr(), d_p.data_ptr(), d_R.data_ptr(), d_K.data_ptr(), sh)
+    kms, kc = ctx.kernel_time(reset=True)
+    ctx.set_timing(False)
+    asm_ms = kms / max(kc, 1)
+    # SpMV alone on the converged K (inputs larger than L2 when 12 nnz > 126 MB)
+    d_x = torch.rand(p.ndof, dtype=torch.float64, device=dev)
+    d_y = torch.empty_like(d_x)
+    for _ in range(5):
+        solver.spmv(d_K.data_ptr(), d_x.data_ptr(), d_y.data_ptr(), sh)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    nsp = 50
+    s0.record(stream)
+    for _ in range(nsp):
+        solver.spmv(d_K.data_ptr(), d_x.data_ptr(), d_y.data_ptr(), sh)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    spmv_ms = s0.elapsed_time(s1) / nsp
+    spmv_bytes = 12.0 * p.nnz + 4.0 * (p.ndof + 1) + 16.0 * p.ndof
+    roof = {"bound": "hbm", "achieved": spmv_bytes / (spmv_ms * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+            "peak_source": hbm_src, "kernel": "k_spmv (CSR, warp per row)", "kernel_ms": spmv_ms,
+            "alg_bytes": spmv_bytes, "traffic": None}
+    roof["frac"] = roof["achieved"] / roof["peak"]
+    # kernels of one step: per assembly its kernels + the norm (2); per solve the
+    # negation, the diagonal scaling and the final residual (5); per GMRES cycle
+    # 6; per queued Arnoldi step 11 (steps are queued 8 at a time, so a cycle
+    # queues at most 7 beyond its last step)
+    solves = info.iters
+    cycles = solves + info.lin_iters // max(args.nr_kdim, 1)
+    launches = (info.iters + 1) * (ctx.launches_per_assembly() + 2) + 5 * solves + 6 * cycles \
+        + 11 * (info.lin_iters + 7 * cycles)
+    out = {"metric": NR_METRIC, "value": 1e3 / ms_step, "unit": "steps/s", "n_gpus": ws, "steps": nsteps,
+           "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic (structured mesh, uniaxial tension)",
+           "config": {"workload": "one Newton-Raphson load step, J2 quadratic tets, %d^3 cells x 6 (%d elements, "
+                                  "%d DOFs, %d nnz), uniaxial stretch %.4g in one step from the linear "
+                                  "predictor, full Newton to ||R||/||R0|| <= %.0e, GMRES(%d) + diagonal "
+                                  "scaling to %.0e"
+                                  % (args.nr_n, p.ne, p.ndof, p.nnz, args.nr_stretch, args.nr_nor_min,
+                                     args.nr_kdim, args.nr_tol),
+                      "newton_iterations": info.iters, "linear_iterations": info.lin_iters,
+                      "residual_history": info.history(),
+                      "assembly_ms": asm_ms, "assembly_share": info.iters and (info.iters + 1) * asm_ms / ms_step,
+                      "spmv_ms": spmv_ms,
+                      "l2": "K values + column ids %.0f MB (L2 126 MB)" % (12e-6 * p.nnz),
+                      "parallelism": "replicas%d" % ws if ws > 1 else "1 GPU"},
+           "roofline": roof, "clocks": clocks,
+           "e2e": {"value": 1e3 / ms_step, "unit": "steps/s", "h2d_bytes_per_step": 8 * len(p.u_presc),
+                   "d2h_bytes_per_step": 0, "note": "the step's input is the prescribed value (the predictor and "
+                                                    "the state are reset on the device); nothing returns to the "
+                                                    "host but the convergence flags"},
+           "gpu_launches": int(nsteps * launches)}
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        from scipy.sparse import csr_matrix
+        from scipy.sparse.linalg import LinearOperator, bicgstab
+        P, mat = oracle.from_workload(p)
+        nth = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        P.assemble(mat, p.u, p.u_presc, state_n=p.state, nthreads=nth)
+        t_asm = time.perf_counter() - t0
+        Km = csr_matrix((d_K.cpu().numpy(), p.Ai, p.Ap), shape=(p.ndof, p.ndof))
+        dinv = 1.0 / Km.diagonal()
+        M = LinearOperator(Km.shape, matvec=lambda v: dinv * v)
+        b = np.random.default_rng(0).normal(size=p.ndof)
+        nit = 20
+        t0 = time.perf_counter()
+        bicgstab(Km, b, rtol=1e-30, maxiter=nit, M=M)
+        t_it = (time.perf_counter() - t0) / nit
+        t_cpu = (info.iters + 1) * t_asm + info.lin_iters * t_it
+        out["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "steps/s", "cores": nth, "kind": "port",
+                               "sample": "one R+K assembly of the step (CPU oracle, %d threads, %.2f s) and %d "
+                                         "BiCGSTAB iterations (scipy, diagonal scaling, %.3f s each), scaled to "
+                                         "the step's %d assemblies and %d linear iterations"
+                                         % (nth, t_asm, nit, t_it, info.iters + 1, info.lin_iters)}
+    solver.close()
+    ctx.close()
+    return out
+
+
 def run_reference(args, ws, rank):
     import workloads as wl
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -775,7 +920,15 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles", "cells"])
-    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch"])
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch",
+                                                         "nr_step"])
+    ap.add_argument("--nr-n", type=int, default=16)
+    ap.add_argument("--nr-stretch", type=float, default=0.003)
+    ap.add_argument("--nr-tol", type=float, default=1e-8)
+    ap.add_argument("--nr-maxit", type=int, default=20000)
+    ap.add_argument("--nr-nor-min", type=float, default=1e-8)
+    ap.add_argument("--nr-steps", type=int, default=1)
+    ap.add_argument("--nr-kdim", type=int, default=100)
     ap.add_argument("--nrve", type=int, default=256)
     ap.add_argument("--train-n", type=int, default=32)
     ap.add_argument("--train-epochs", type=int, default=30)
@@ -798,6 +951,8 @@ def main():
         out = run_cp_warm(args, ws, rank, local)
     elif args.workload == "rve_batch":
         out = run_rve(args, ws, rank, local)
+    elif args.workload == "nr_step":
+        out = run_nr(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
     if rank == 0:

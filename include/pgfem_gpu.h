@@ -312,41 +312,48 @@ int pgfem_gpu_get_cp_fallbacks(pgfem_gpu_ctx *ctx, long *n);
 
 /* ---- linear solve and Newton-Raphson on the device ------------------------
  * The consumer of K.  The reference solves K dd_u = f with hypre
- * (src/solvers/hypre/Hypre.cc:147-194): BiCGSTAB (src/solvers/hypre/BCGStab.cc)
- * preconditioned by diagonal scaling (src/solvers/hypre/ScaleDiag.cc: 1/K_ii,
- * 1.1 where |K_ii| <= 1e-5), inside its Newton-Raphson loop
+ * (src/solvers/hypre/Hypre.cc:147-194): GMRES (src/solvers/hypre/GMRes.cc, the
+ * default) or BiCGSTAB (src/solvers/hypre/BCGStab.cc), preconditioned by
+ * diagonal scaling (src/solvers/hypre/ScaleDiag.cc: 1/K_ii, 1.1 where
+ * |K_ii| <= 1e-5), inside its Newton-Raphson loop
  * (src/Newton_Raphson.cc:931-1330).  A solver holds the CSR pattern on the
  * device (Ap, Ai of one rank, columns sorted, column id = row id on the
- * diagonal) and its Krylov work vectors; K values are passed per call. */
-enum { PGFEM_SOLVER_BCG_STAB = 1 };                          /* SOLVER_BCG_STAB */
-enum { PGFEM_PRECOND_NONE = 0, PGFEM_PRECOND_DIAG_SCALE = 1 }; /* PRECOND_DIAG_SCALE */
+ * diagonal) and its Krylov work vectors; K values are passed per call.
+ * Solver and preconditioner ids keep the values of the reference's
+ * enumerations (include/enumerations.h:35-45, 87-94). */
+enum { PGFEM_SOLVER_GMRES = 0, PGFEM_SOLVER_BCG_STAB = 1 };      /* SOLVER_GMRES, SOLVER_BCG_STAB */
+enum { PGFEM_PRECOND_NONE = 4, PGFEM_PRECOND_DIAG_SCALE = 5 };  /* PRECOND_NONE, PRECOND_DIAG_SCALE */
+#define PGFEM_GMRES_MAX_KDIM 1000 /* largest Krylov dimension of a GMRES solver (ELIMIT beyond) */
 
 typedef struct {
-  int solver;      /* PGFEM_SOLVER_BCG_STAB */
-  int precond;     /* PGFEM_PRECOND_* */
-  int maxit;       /* iteration cap (the reference's sol->maxit) */
+  int solver;      /* PGFEM_SOLVER_GMRES or PGFEM_SOLVER_BCG_STAB */
+  int precond;     /* PGFEM_PRECOND_NONE or PGFEM_PRECOND_DIAG_SCALE */
+  int maxit;       /* iteration cap (the reference's -maxit, default 1000) */
+  int kdim;        /* GMRES restart length (-kdim, default 500); the basis takes (kdim + 1) * nrows doubles */
   double tol;      /* relative residual ||b - K x|| / ||b|| to reach (sol->err) */
   int check_every; /* iterations queued between host convergence checks; <= 0: 8 */
 } pgfem_solver_opts;
 
 typedef struct {
-  int iters;       /* BiCGSTAB iterations (SOLVER_INFO n_iter) */
-  double res_norm; /* final relative residual of the recurrence (SOLVER_INFO res_norm) */
-  int converged;   /* res_norm <= tol */
-  int breakdown;   /* a BiCGSTAB denominator vanished or a value was not finite */
+  int iters;       /* iterations (GMRES: Arnoldi steps over all cycles; SOLVER_INFO n_iter) */
+  double res_norm; /* final relative residual (GMRES: ||b - K x|| / ||b|| recomputed; BiCGSTAB: of the
+                      recurrence) (SOLVER_INFO res_norm) */
+  int converged;   /* the method's residual reached tol */
+  int breakdown;   /* a denominator vanished or a value was not finite */
 } pgfem_solve_info;
 
 typedef struct pgfem_gpu_solver pgfem_gpu_solver;
 
-/* Copies the pattern to the device; EPATTERN when a column id is out of
- * range, ENODEV without an sm_100 device. */
+/* Copies the pattern to the device and allocates the work vectors; EPATTERN
+ * when a column id is out of range, ELIMIT for kdim > PGFEM_GMRES_MAX_KDIM,
+ * ENODEV without an sm_100 device. */
 int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfem_solver_opts *opts,
                             pgfem_gpu_solver **solver);
 int pgfem_gpu_solver_destroy(pgfem_gpu_solver *solver);
 long pgfem_gpu_solver_device_bytes(const pgfem_gpu_solver *solver);
 /* y = K x on `stream` (device pointers; asynchronous). */
 int pgfem_gpu_spmv(pgfem_gpu_solver *solver, const double *d_K, const double *d_x, double *d_y, void *stream);
-/* K x = b by preconditioned BiCGSTAB; d_x holds the initial guess on entry.
+/* K x = b by the solver's method; d_x holds the initial guess on entry.
  * Synchronises `stream` at each convergence check. */
 int pgfem_gpu_solve(pgfem_gpu_solver *solver, const double *d_K, const double *d_b, double *d_x,
                     pgfem_solve_info *info, void *stream);

@@ -8,14 +8,19 @@
 //    contiguously (12 bytes per non-zero from HBM), the vector is gathered
 //    through L2; the Krylov dot products that follow a product are fused into
 //    it (per-block partial sums);
-//  - BiCGSTAB (BCGStab.cc) with right preconditioning by diagonal scaling
-//    (ScaleDiag.cc: 1/K_ii, or 1.1 where |K_ii| <= 1e-5) or none.  All Krylov
-//    scalars live in device memory and are formed by one-block finalize
-//    kernels, so an iteration is a fixed sequence of launches with no host
-//    round trip; every kernel returns at once when the device-side `done`
-//    flag is set (converged or broken down), so the host queues several
-//    iterations between convergence checks.  Reductions sum per-block
-//    partials in a fixed order: the result does not depend on timing;
+//  - restarted GMRES(kdim) (GMRes.cc, the reference's default solver) and
+//    BiCGSTAB (BCGStab.cc), both right-preconditioned by diagonal scaling
+//    (ScaleDiag.cc: 1/K_ii, or 1.1 where |K_ii| <= 1e-5) or not at all.  GMRES
+//    orthogonalises by classical Gram-Schmidt applied twice (the dot products
+//    against the basis in one pass, eight vectors per register tile) and keeps
+//    the Hessenberg matrix, the Givens rotations and the residual estimate in
+//    device memory, advanced by one-thread kernels.  All Krylov scalars live
+//    in device memory, so an iteration is a fixed sequence of launches with
+//    no host round trip; every kernel returns at once when the device-side
+//    `done` flag is set (converged, end of a GMRES cycle, or broken down), so
+//    the host queues several iterations between checks.  Reductions sum
+//    per-block partials in a fixed order: the result does not depend on
+//    timing;
 //  - pgfem_gpu_newton_step: full Newton (stiffness every iteration, FNR = 1)
 //    for one load step through the public assembly entry point, converged
 //    when ||R|| / ||R_0|| <= nor_min or ||R|| <= computer_zero (the
@@ -260,6 +265,256 @@ __global__ void __launch_bounds__(kBlk) k_dot(long n, const double *__restrict__
   block_partials(d, 0.0, part0, nullptr);
 }
 
+// ---- GMRES ----------------------------------------------------------------
+constexpr int kTile = 8;  // basis vectors per register tile of the dot products
+
+struct GState {
+  double beta0, bnorm, tol;
+  int j;          // Arnoldi steps completed in this cycle
+  int m;          // Krylov dimension
+  int done, converged, breakdown, pad;
+};
+
+// w = K (dinv o V[j]), j = G->j (one warp per row)
+__global__ void __launch_bounds__(kBlk) k_spmv_basis(long n, const int *__restrict__ Ap, const int *__restrict__ Ai,
+                                                     const double *__restrict__ K, const double *__restrict__ dinv,
+                                                     const double *__restrict__ V, double *__restrict__ w,
+                                                     const GState *G) {
+  if (G->done) return;
+  const double *x = V + (long)G->j * n;
+  const int lane = threadIdx.x & 31;
+  const long warp0 = ((long)blockIdx.x * kBlk + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * kBlk) >> 5;
+  for (long i = warp0; i < n; i += nwarps) {
+    const int b = Ap[i], e = Ap[i + 1];
+    double acc = 0.0;
+    for (int jj = b + lane; jj < e; jj += 32) {
+      const int c = Ai[jj];
+      acc = fma(K[jj], dinv[c] * x[c], acc);
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) w[i] = acc;
+  }
+}
+
+// partials part[t * nblk + block] = (V[t], w) over the block's chunk, t <= j
+__global__ void __launch_bounds__(kBlk) k_multidot(long n, const double *__restrict__ V, const double *__restrict__ w,
+                                                   double *part, const GState *G) {
+  if (G->done) return;
+  __shared__ double sm[kBlk / 32][kTile];
+  const int nt = G->j + 1;
+  const long chunk = (n + gridDim.x - 1) / gridDim.x;
+  const long i0 = (long)blockIdx.x * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
+  for (int t0 = 0; t0 < nt; t0 += kTile) {
+    double acc[kTile];
+#pragma unroll
+    for (int u = 0; u < kTile; u++) acc[u] = 0.0;
+    for (long i = i0 + threadIdx.x; i < i1; i += kBlk) {
+      const double wi = w[i];
+#pragma unroll
+      for (int u = 0; u < kTile; u++)
+        if (t0 + u < nt) acc[u] = fma(V[(long)(t0 + u) * n + i], wi, acc[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < kTile; u++) acc[u] = warp_sum(acc[u]);
+    const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
+    if (l == 0)
+#pragma unroll
+      for (int u = 0; u < kTile; u++) sm[wp][u] = acc[u];
+    __syncthreads();
+    if (threadIdx.x < kTile && t0 + threadIdx.x < nt) {
+      double sum = 0.0;
+      for (int q = 0; q < kBlk / 32; q++) sum += sm[q][threadIdx.x];
+      part[(long)(t0 + threadIdx.x) * gridDim.x + blockIdx.x] = sum;
+    }
+    __syncthreads();
+  }
+}
+
+// h[t] = sum of the partials (one warp per t); column j of H gets h
+// (accumulate: +=), htmp gets h for the following update of w.
+__global__ void __launch_bounds__(kFin) k_multidot_fin(int nblk, const double *part, double *H, double *htmp,
+                                                       int accumulate, const GState *G) {
+  if (G->done) return;
+  const int nt = G->j + 1, m1 = G->m + 1;
+  const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
+  for (int t = wp; t < nt; t += kFin / 32) {
+    double sum = 0.0;
+    for (int b = l; b < nblk; b += 32) sum += part[(long)t * nblk + b];
+    sum = warp_sum(sum);
+    if (l == 0) {
+      htmp[t] = sum;
+      double &h = H[(long)G->j * m1 + t];
+      h = accumulate ? h + sum : sum;
+    }
+  }
+}
+
+// w -= sum_{t <= j} V[t] htmp[t]
+__global__ void k_multiaxpy(long n, const double *__restrict__ V, double *__restrict__ w,
+                            const double *__restrict__ htmp, const GState *G) {
+  if (G->done) return;
+  const int nt = G->j + 1;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double acc = w[i];
+    for (int t = 0; t < nt; t++) acc = fma(-V[(long)t * n + i], htmp[t], acc);
+    w[i] = acc;
+  }
+}
+
+// partials of (w, w) unless the cycle is over
+__global__ void __launch_bounds__(kBlk) k_gdot(long n, const double *__restrict__ w, double *part0,
+                                               const GState *G) {
+  if (G->done) return;
+  double d = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) d = fma(w[i], w[i], d);
+  block_partials(d, 0.0, part0, nullptr);
+}
+
+// H[j+1, j] = ||w|| (one block)
+__global__ void __launch_bounds__(kFin) k_gnorm_fin(int nblk, const double *part0, double *H, const GState *G) {
+  if (G->done) return;
+  __shared__ double s0[kFin];
+  double a = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += kFin) a += part0[i];
+  s0[threadIdx.x] = a;
+  __syncthreads();
+  for (int o = kFin / 2; o; o >>= 1) {
+    if (threadIdx.x < o) s0[threadIdx.x] += s0[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) H[(long)G->j * (G->m + 1) + G->j + 1] = sqrt(s0[0]);
+}
+
+// V[j+1] = w / H[j+1, j] (zero when the new direction vanished)
+__global__ void k_gscale(long n, double *__restrict__ V, const double *__restrict__ w, const double *H,
+                         const GState *G) {
+  if (G->done) return;
+  const double h = H[(long)G->j * (G->m + 1) + G->j + 1];
+  const double inv = h > 0.0 ? 1.0 / h : 0.0;
+  double *v = V + (long)(G->j + 1) * n;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+    v[i] = w[i] * inv;
+}
+
+// One thread: apply the previous rotations to column j, form rotation j,
+// update the residual estimate |g[j+1]|, advance j, end the cycle when it is
+// converged, full, or broken down.
+__global__ void k_givens(double *H, double *cs, double *sn, double *g, GState *G) {
+  if (G->done) return;
+  const int j = G->j, m1 = G->m + 1;
+  double *h = H + (long)j * m1;
+  for (int t = 0; t < j; t++) {
+    const double a = cs[t] * h[t] + sn[t] * h[t + 1];
+    h[t + 1] = -sn[t] * h[t] + cs[t] * h[t + 1];
+    h[t] = a;
+  }
+  const double hn = h[j + 1];
+  const double d = hypot(h[j], hn);
+  if (!(d > 0.0) || !isfinite(d)) {
+    G->breakdown = 1;
+    G->done = 1;
+    return;
+  }
+  cs[j] = h[j] / d;
+  sn[j] = hn / d;
+  h[j] = d;
+  h[j + 1] = 0.0;
+  g[j + 1] = -sn[j] * g[j];
+  g[j] = cs[j] * g[j];
+  G->j = j + 1;
+  if (fabs(g[j + 1]) <= G->tol * G->bnorm || hn == 0.0) {
+    G->converged = 1;
+    G->done = 1;
+  } else if (G->j >= G->m) {
+    G->done = 1;
+  }
+}
+
+// Cycle start: V[0] = b - w (w = K x), partials (r, r), (b, b).
+__global__ void __launch_bounds__(kBlk) k_ginit(long n, const double *__restrict__ b, const double *__restrict__ w,
+                                                double *__restrict__ V, double *part0, double *part1) {
+  double d0 = 0.0, d1 = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    const double ri = b[i] - w[i];
+    V[i] = ri;
+    d0 = fma(ri, ri, d0);
+    d1 = fma(b[i], b[i], d1);
+  }
+  block_partials(d0, d1, part0, part1);
+}
+
+// One block: beta0 = ||r0||, g = (beta0, 0, ...), j = 0.
+__global__ void __launch_bounds__(kFin) k_ginit_fin(int nblk, const double *part0, const double *part1, double *g,
+                                                    GState *G) {
+  __shared__ double s0[kFin], s1[kFin];
+  double a = 0.0, b = 0.0;
+  for (int i = threadIdx.x; i < nblk; i += kFin) {
+    a += part0[i];
+    b += part1[i];
+  }
+  s0[threadIdx.x] = a;
+  s1[threadIdx.x] = b;
+  __syncthreads();
+  for (int o = kFin / 2; o; o >>= 1) {
+    if (threadIdx.x < o) {
+      s0[threadIdx.x] += s0[threadIdx.x + o];
+      s1[threadIdx.x] += s1[threadIdx.x + o];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x) return;
+  G->beta0 = sqrt(s0[0]);
+  G->bnorm = sqrt(s1[0]);
+  G->j = 0;
+  G->breakdown = 0;
+  G->converged = (G->beta0 <= G->tol * G->bnorm) ? 1 : 0;
+  G->done = G->converged || !isfinite(G->beta0);
+  if (!isfinite(G->beta0)) G->breakdown = 1;
+  g[0] = G->beta0;
+}
+
+// V[0] /= beta0
+__global__ void k_gscale0(long n, double *V, const GState *G) {
+  if (G->done) return;
+  const double inv = 1.0 / G->beta0;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) V[i] *= inv;
+}
+
+// One thread: y = H(0:k, 0:k)^-1 g(0:k), k = j (upper triangular after the
+// rotations).
+__global__ void k_backsolve(const double *H, const double *g, double *y, const GState *G) {
+  const int k = G->j, m1 = G->m + 1;
+  for (int t = k - 1; t >= 0; t--) {
+    double a = g[t];
+    for (int q = t + 1; q < k; q++) a -= H[(long)q * m1 + t] * y[q];
+    const double d = H[(long)t * m1 + t];
+    y[t] = d != 0.0 ? a / d : 0.0;
+  }
+}
+
+// x += dinv o (V y) over the cycle's k = j basis vectors
+__global__ void k_gupdate_x(long n, const double *__restrict__ V, const double *__restrict__ y,
+                            const double *__restrict__ dinv, double *__restrict__ x, const GState *G) {
+  const int k = G->j;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int t = 0; t < k; t++) acc = fma(V[(long)t * n + i], y[t], acc);
+    x[i] = fma(dinv[i], acc, x[i]);
+  }
+}
+
+// partials of ||b - w||^2 (true residual, w = K x)
+__global__ void __launch_bounds__(kBlk) k_resid(long n, const double *__restrict__ b, const double *__restrict__ w,
+                                                double *part0) {
+  double d = 0.0;
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    const double r = b[i] - w[i];
+    d = fma(r, r, d);
+  }
+  block_partials(d, 0.0, part0, nullptr);
+}
+
 // Position of the diagonal entry of every row (-1 when the row has none).
 void find_diagonal(const int *Ap, const int *Ai, long n, long *dpos) {
   for (long i = 0; i < n; i++) {
@@ -310,6 +565,11 @@ struct pgfem_gpu_solver {
   double *part0 = nullptr, *part1 = nullptr, *dot_out = nullptr;
   Scalars *S = nullptr;
   Scalars *hS = nullptr;  // pinned host copy
+  // GMRES
+  double *V = nullptr, *H = nullptr, *cs = nullptr, *sn = nullptr, *g = nullptr, *y = nullptr, *htmp = nullptr,
+         *w = nullptr, *gpart = nullptr;
+  GState *G = nullptr;
+  GState *hG = nullptr;
   // Newton buffers (allocated by the first newton_step)
   double *R = nullptr, *K = nullptr, *du = nullptr;
   long bytes = 0;
@@ -330,10 +590,12 @@ int salloc(pgfem_gpu_solver *s, T **p, size_t n) {
 
 void release(pgfem_gpu_solver *s) {
   void *ptrs[] = {s->Ap, s->Ai, s->dpos, s->dinv, s->r, s->rh, s->p, s->v, s->ph, s->sh, s->t,
-                  s->part0, s->part1, s->dot_out, s->S, s->R, s->K, s->du};
+                  s->part0, s->part1, s->dot_out, s->S, s->R, s->K, s->du, s->V, s->H,
+                  s->cs, s->sn, s->g, s->y, s->htmp, s->w, s->gpart, s->G};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (s->hS) cudaFreeHost(s->hS);
+  if (s->hG) cudaFreeHost(s->hG);
 }
 
 #define SK(x)                         \
@@ -358,8 +620,8 @@ int dot_device(pgfem_gpu_solver *s, const double *a, const double *b, cudaStream
   return PGFEM_GPU_OK;
 }
 
-int solve_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x, pgfem_solve_info *info,
-               cudaStream_t st) {
+int bicg_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x, pgfem_solve_info *info,
+              cudaStream_t st) {
   const long n = s->n;
   const int g = ew_grid(s);
   const int gs = s->grid;  // SpMV grid (warp per row, grid-stride)
@@ -402,6 +664,83 @@ int solve_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x,
   return PGFEM_GPU_OK;
 }
 
+int gmres_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x, pgfem_solve_info *info,
+               cudaStream_t st) {
+  const long n = s->n;
+  const int g = ew_grid(s), gs = s->grid, m = s->opts.kdim;
+  const int every = s->opts.check_every > 0 ? s->opts.check_every : 8;
+  k_diag_scale<<<g, kBlk, 0, st>>>(n, s->dpos, K, s->opts.precond, s->dinv);
+  GState init{};
+  init.tol = s->opts.tol;
+  init.m = m;
+  SK(cudaMemcpyAsync(s->G, &init, sizeof(GState), cudaMemcpyHostToDevice, st));
+  int total = 0, cycles = 0;
+  bool converged = false, breakdown = false;
+  while (true) {
+    // cycle start from the current x
+    k_spmv<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, x, s->w, nullptr, 0, nullptr, nullptr, nullptr);
+    k_ginit<<<g, kBlk, 0, st>>>(n, b, s->w, s->V, s->part0, s->part1);
+    k_ginit_fin<<<1, kFin, 0, st>>>(g, s->part0, s->part1, s->g, s->G);
+    k_gscale0<<<g, kBlk, 0, st>>>(n, s->V, s->G);
+    SK(cudaGetLastError());
+    int steps = 0;
+    for (;;) {
+      int k = every;
+      if (k > m - steps) k = m - steps;
+      if (k > s->opts.maxit - total - steps) k = s->opts.maxit - total - steps;
+      for (int it = 0; it < k; it++) {
+        k_spmv_basis<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, s->dinv, s->V, s->w, s->G);
+        for (int pass = 0; pass < 2; pass++) {
+          k_multidot<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->gpart, s->G);
+          k_multidot_fin<<<1, kFin, 0, st>>>(g, s->gpart, s->H, s->htmp, pass, s->G);
+          k_multiaxpy<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->htmp, s->G);
+        }
+        k_gdot<<<g, kBlk, 0, st>>>(n, s->w, s->part0, s->G);
+        k_gnorm_fin<<<1, kFin, 0, st>>>(g, s->part0, s->H, s->G);
+        k_gscale<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->H, s->G);
+        k_givens<<<1, 1, 0, st>>>(s->H, s->cs, s->sn, s->g, s->G);
+      }
+      SK(cudaGetLastError());
+      steps += k;
+      SK(cudaMemcpyAsync(s->hG, s->G, sizeof(GState), cudaMemcpyDeviceToHost, st));
+      SK(cudaStreamSynchronize(st));
+      if (s->hG->done || k <= 0 || steps >= m || total + steps >= s->opts.maxit) break;
+    }
+    // x += D V y over the steps of this cycle
+    k_backsolve<<<1, 1, 0, st>>>(s->H, s->g, s->y, s->G);
+    k_gupdate_x<<<g, kBlk, 0, st>>>(n, s->V, s->y, s->dinv, x, s->G);
+    SK(cudaGetLastError());
+    SK(cudaMemcpyAsync(s->hG, s->G, sizeof(GState), cudaMemcpyDeviceToHost, st));
+    SK(cudaStreamSynchronize(st));
+    total += s->hG->j;
+    cycles++;
+    converged = s->hG->converged != 0;
+    breakdown = s->hG->breakdown != 0;
+    if (converged || breakdown || total >= s->opts.maxit || s->hG->j == 0) break;
+  }
+  // true relative residual ||b - K x|| / ||b||
+  k_spmv<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, x, s->w, nullptr, 0, nullptr, nullptr, nullptr);
+  k_resid<<<g, kBlk, 0, st>>>(n, b, s->w, s->part0);
+  k_finalize<<<1, kFin, 0, st>>>(g, s->part0, nullptr, kNorm, s->S, s->dot_out);
+  SK(cudaGetLastError());
+  double rr = 0.0;
+  SK(cudaMemcpyAsync(&rr, s->dot_out, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SK(cudaStreamSynchronize(st));
+  if (info) {
+    const double bn = s->hG->bnorm;
+    info->iters = total;
+    info->res_norm = bn > 0.0 ? std::sqrt(rr) / bn : std::sqrt(rr);
+    info->converged = converged ? 1 : 0;
+    info->breakdown = breakdown ? 1 : 0;
+  }
+  return PGFEM_GPU_OK;
+}
+
+int solve_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x, pgfem_solve_info *info,
+               cudaStream_t st) {
+  return s->opts.solver == PGFEM_SOLVER_GMRES ? gmres_impl(s, K, b, x, info, st) : bicg_impl(s, K, b, x, info, st);
+}
+
 }  // namespace
 
 extern "C" {
@@ -411,9 +750,11 @@ int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfe
   if (!out) return PGFEM_GPU_EINVAL;
   *out = nullptr;
   if (!Ap || !Ai || nrows <= 0 || !opts || opts->maxit <= 0 || !(opts->tol > 0.0) ||
-      opts->solver != PGFEM_SOLVER_BCG_STAB ||
+      (opts->solver != PGFEM_SOLVER_BCG_STAB && opts->solver != PGFEM_SOLVER_GMRES) ||
       (opts->precond != PGFEM_PRECOND_NONE && opts->precond != PGFEM_PRECOND_DIAG_SCALE))
     return PGFEM_GPU_EINVAL;
+  if (opts->solver == PGFEM_SOLVER_GMRES && opts->kdim <= 0) return PGFEM_GPU_EINVAL;
+  if (opts->solver == PGFEM_SOLVER_GMRES && opts->kdim > PGFEM_GMRES_MAX_KDIM) return PGFEM_GPU_ELIMIT;
   if (Ap[0] != 0) return PGFEM_GPU_EINVAL;
   for (long i = 0; i < nrows; i++)
     if (Ap[i + 1] < Ap[i]) return PGFEM_GPU_EINVAL;
@@ -433,13 +774,21 @@ int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfe
       (r = salloc(s, &s->dinv, nrows)) || (r = salloc(s, &s->r, nrows)) || (r = salloc(s, &s->rh, nrows)) ||
       (r = salloc(s, &s->p, nrows)) || (r = salloc(s, &s->v, nrows)) || (r = salloc(s, &s->ph, nrows)) ||
       (r = salloc(s, &s->sh, nrows)) || (r = salloc(s, &s->t, nrows)) || (r = salloc(s, &s->part0, s->grid)) ||
-      (r = salloc(s, &s->part1, s->grid)) || (r = salloc(s, &s->dot_out, 1)) || (r = salloc(s, &s->S, 1))) {
+      (r = salloc(s, &s->part1, s->grid)) || (r = salloc(s, &s->dot_out, 1)) || (r = salloc(s, &s->S, 1)) ||
+      (opts->solver == PGFEM_SOLVER_GMRES &&
+       ((r = salloc(s, &s->V, (size_t)(opts->kdim + 1) * nrows)) ||
+        (r = salloc(s, &s->H, (size_t)(opts->kdim + 1) * opts->kdim)) || (r = salloc(s, &s->cs, opts->kdim)) ||
+        (r = salloc(s, &s->sn, opts->kdim)) || (r = salloc(s, &s->g, opts->kdim + 1)) ||
+        (r = salloc(s, &s->y, opts->kdim)) || (r = salloc(s, &s->htmp, opts->kdim + 1)) ||
+        (r = salloc(s, &s->w, nrows)) || (r = salloc(s, &s->gpart, (size_t)(opts->kdim + 1) * s->grid)) ||
+        (r = salloc(s, &s->G, 1))))) {
     delete[] hdpos;
     release(s);
     delete s;
     return r;
   }
   if (cudaMallocHost((void **)&s->hS, sizeof(Scalars)) != cudaSuccess ||
+      cudaMallocHost((void **)&s->hG, sizeof(GState)) != cudaSuccess ||
       cudaMemcpy(s->Ap, Ap, sizeof(int) * (nrows + 1), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(s->Ai, Ai, sizeof(int) * nnz, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(s->dpos, hdpos, sizeof(long) * nrows, cudaMemcpyHostToDevice) != cudaSuccess) {

@@ -504,14 +504,15 @@ class Graph:
 
 
 # ---- linear solve and Newton-Raphson --------------------------------------
-SOLVER_BCG_STAB = 1
-PRECOND_NONE, PRECOND_DIAG_SCALE = 0, 1
+SOLVER_GMRES, SOLVER_BCG_STAB = 0, 1
+PRECOND_NONE, PRECOND_DIAG_SCALE = 4, 5
+GMRES_MAX_KDIM = 1000
 NEWTON_HISTORY = 32
 
 
 class SolverOpts(C.Structure):
-    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("maxit", C.c_int), ("tol", C.c_double),
-                ("check_every", C.c_int)]
+    _fields_ = [("solver", C.c_int), ("precond", C.c_int), ("maxit", C.c_int), ("kdim", C.c_int),
+                ("tol", C.c_double), ("check_every", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -534,12 +535,13 @@ class NewtonInfo(C.Structure):
 class Solver:
     """Device linear solver over one CSR pattern (pgfem_gpu_solver_*)."""
 
-    def __init__(self, Ap, Ai, nrows, precond=PRECOND_DIAG_SCALE, maxit=5000, tol=1e-10, check_every=8):
+    def __init__(self, Ap, Ai, nrows, solver=SOLVER_GMRES, precond=PRECOND_DIAG_SCALE, maxit=5000, kdim=100,
+                 tol=1e-10, check_every=8):
         self._Ap = np.ascontiguousarray(Ap, dtype=np.int32)
         self._Ai = np.ascontiguousarray(Ai, dtype=np.int32)
         self.n = int(nrows)
         self.nnz = int(self._Ap[-1])
-        self.opts = SolverOpts(SOLVER_BCG_STAB, precond, maxit, tol, check_every)
+        self.opts = SolverOpts(solver, precond, maxit, kdim, tol, check_every)
         h = C.c_void_p()
         _check("pgfem_gpu_solver_create", lib().pgfem_gpu_solver_create(_ptr(self._Ap), _ptr(self._Ai), self.n,
                                                                         C.byref(self.opts), C.byref(h)))

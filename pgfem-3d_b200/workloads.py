@@ -97,11 +97,12 @@ def he_p1(n=10, seed=0):
     return Problem("he_p1_n%d" % n, X, conn, ids, ndof, Ap, Ai, mat, u, meta=dict(n=n, seed=seed))
 
 
-def tension(n=4, nne=4, model="he", stretch=0.01):
+def tension(n=4, nne=4, model="he", stretch=0.01, predictor=False):
     """Uniaxial tension of the unit cube for a Newton-Raphson load step: the
     x = 0 face fixed, the x-displacement of the x = 1 face prescribed
-    (one prescribed value, u_presc[0] = stretch), every other DOF free and
-    starting from zero.  model "he" (neo-Hookean) or "j2" (state at identity)."""
+    (one prescribed value, u_presc[0] = stretch), every other DOF free,
+    starting from zero or, with predictor, from the linear field
+    u_x = stretch * x.  model "he" (neo-Hookean) or "j2" (state at identity)."""
     X, conn, _ = pg.mesh_box_tet(n, nne)
     nn = X.shape[0]
     codes = np.zeros((nn, 3), dtype=np.int64)
@@ -117,8 +118,12 @@ def tension(n=4, nne=4, model="he", stretch=0.01):
         nqp = conn.shape[0] * (4 if nne == 10 else 1)
         state = np.zeros((nqp, 10))
         state[:, [0, 4, 8]] = 1.0
+    disp = np.zeros((nn, 3))
+    if predictor:
+        disp[:, 0] = stretch * X[:, 0]
+    u = nodal_to_free(ids, disp) if ndof else np.zeros(0)
     return Problem("tension_%s_p%d_n%d" % (model, 1 if nne == 4 else 2, n), X, conn, ids, ndof, Ap, Ai, mat,
-                   np.zeros(ndof), u_presc=np.array([stretch]), state=state,
+                   u, u_presc=np.array([stretch]), state=state,
                    meta=dict(n=n, stretch=stretch, model=model))
 
 

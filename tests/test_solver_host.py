@@ -24,10 +24,13 @@ def test_bad_pattern_is_rejected_before_device_work():
     with pytest.raises(pg.PgfemError) as e:
         _create(Ap, p.Ai, p.ndof)
     assert pg.ERRORS[e.value.code] == "EINVAL"
-    for kw in (dict(maxit=0), dict(tol=0.0), dict(precond=7)):
+    for kw in (dict(maxit=0), dict(tol=0.0), dict(precond=7), dict(solver=3), dict(kdim=0)):
         with pytest.raises(pg.PgfemError) as e:
             _create(p.Ap, p.Ai, p.ndof, **kw)
         assert pg.ERRORS[e.value.code] == "EINVAL", kw
+    with pytest.raises(pg.PgfemError) as e:
+        _create(p.Ap, p.Ai, p.ndof, kdim=pg.GMRES_MAX_KDIM + 1)
+    assert pg.ERRORS[e.value.code] == "ELIMIT"
 
 
 def test_no_cpu_fallback():
