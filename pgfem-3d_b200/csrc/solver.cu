@@ -297,12 +297,17 @@ __global__ void __launch_bounds__(kBlk) k_spmv_basis(long n, const int *__restri
   }
 }
 
-// partials part[t * nblk + block] = (V[t], w) over the block's chunk, t <= j
+// partials part[t * nblk + block] = (V[t], w), t <= j.  Each warp walks its
+// own slice of the block's rows through all tiles of kTile basis vectors and
+// keeps its sums in shared memory, so warps never wait for each other between
+// tiles; one barrier at the end combines the warps.
+constexpr int kMdWarps = kBlk / 32;
 __global__ void __launch_bounds__(kBlk) k_multidot(long n, const double *__restrict__ V, const double *__restrict__ w,
                                                    double *part, const GState *G) {
   if (G->done) return;
-  __shared__ double sm[kBlk / 32][kTile];
+  extern __shared__ double smd[];  // [kMdWarps][nt]
   const int nt = G->j + 1;
+  const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
   const long chunk = (n + gridDim.x - 1) / gridDim.x;
   const long i0 = (long)blockIdx.x * chunk, i1 = i0 + chunk < n ? i0 + chunk : n;
   for (int t0 = 0; t0 < nt; t0 += kTile) {
@@ -316,20 +321,20 @@ __global__ void __launch_bounds__(kBlk) k_multidot(long n, const double *__restr
         if (t0 + u < nt) acc[u] = fma(V[(long)(t0 + u) * n + i], wi, acc[u]);
     }
 #pragma unroll
-    for (int u = 0; u < kTile; u++) acc[u] = warp_sum(acc[u]);
-    const int wp = threadIdx.x >> 5, l = threadIdx.x & 31;
-    if (l == 0)
-#pragma unroll
-      for (int u = 0; u < kTile; u++) sm[wp][u] = acc[u];
-    __syncthreads();
-    if (threadIdx.x < kTile && t0 + threadIdx.x < nt) {
-      double sum = 0.0;
-      for (int q = 0; q < kBlk / 32; q++) sum += sm[q][threadIdx.x];
-      part[(long)(t0 + threadIdx.x) * gridDim.x + blockIdx.x] = sum;
+    for (int u = 0; u < kTile; u++) {
+      const double v = warp_sum(acc[u]);
+      if (l == 0 && t0 + u < nt) smd[wp * nt + t0 + u] = v;
     }
-    __syncthreads();
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < nt; t += kBlk) {
+    double sum = 0.0;
+    for (int q = 0; q < kMdWarps; q++) sum += smd[q * nt + t];
+    part[(long)t * gridDim.x + blockIdx.x] = sum;
   }
 }
+
+inline size_t multidot_smem(int nt) { return sizeof(double) * kMdWarps * (size_t)nt; }
 
 // h[t] = sum of the partials (one warp per t); column j of H gets h
 // (accumulate: +=), htmp gets h for the following update of w.
@@ -350,25 +355,29 @@ __global__ void __launch_bounds__(kFin) k_multidot_fin(int nblk, const double *p
   }
 }
 
-// w -= sum_{t <= j} V[t] htmp[t]
-__global__ void k_multiaxpy(long n, const double *__restrict__ V, double *__restrict__ w,
-                            const double *__restrict__ htmp, const GState *G) {
+// w -= sum_{t <= j} V[t] htmp[t]; with norm: partials of (w, w) of the result
+// (the second Gram-Schmidt pass and ||w|| in one sweep)
+__global__ void __launch_bounds__(kBlk) k_multiaxpy(long n, const double *__restrict__ V, double *__restrict__ w,
+                                                    const double *__restrict__ htmp, double *part0,
+                                                    const GState *G) {
   if (G->done) return;
   const int nt = G->j + 1;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double acc = w[i];
-    for (int t = 0; t < nt; t++) acc = fma(-V[(long)t * n + i], htmp[t], acc);
-    w[i] = acc;
-  }
-}
-
-// partials of (w, w) unless the cycle is over
-__global__ void __launch_bounds__(kBlk) k_gdot(long n, const double *__restrict__ w, double *part0,
-                                               const GState *G) {
-  if (G->done) return;
   double d = 0.0;
-  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) d = fma(w[i], w[i], d);
-  block_partials(d, 0.0, part0, nullptr);
+  for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
+    double a0 = w[i], a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int t = 0;
+    for (; t + 4 <= nt; t += 4) {
+      a0 = fma(-V[(long)t * n + i], htmp[t], a0);
+      a1 = fma(-V[(long)(t + 1) * n + i], htmp[t + 1], a1);
+      a2 = fma(-V[(long)(t + 2) * n + i], htmp[t + 2], a2);
+      a3 = fma(-V[(long)(t + 3) * n + i], htmp[t + 3], a3);
+    }
+    for (; t < nt; t++) a0 = fma(-V[(long)t * n + i], htmp[t], a0);
+    const double r = (a0 + a1) + (a2 + a3);
+    w[i] = r;
+    d = fma(r, r, d);
+  }
+  if (part0) block_partials(d, 0.0, part0, nullptr);
 }
 
 // H[j+1, j] = ||w|| (one block)
@@ -668,6 +677,7 @@ int gmres_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x,
                cudaStream_t st) {
   const long n = s->n;
   const int g = ew_grid(s), gs = s->grid, m = s->opts.kdim;
+  const int gm = g < g_sms * 4 ? g : g_sms * 4;  // one wave of the dot kernel
   const int every = s->opts.check_every > 0 ? s->opts.check_every : 8;
   k_diag_scale<<<g, kBlk, 0, st>>>(n, s->dpos, K, s->opts.precond, s->dinv);
   GState init{};
@@ -689,13 +699,15 @@ int gmres_impl(pgfem_gpu_solver *s, const double *K, const double *b, double *x,
       if (k > m - steps) k = m - steps;
       if (k > s->opts.maxit - total - steps) k = s->opts.maxit - total - steps;
       for (int it = 0; it < k; it++) {
+        // the basis has steps + it + 1 vectors at this step (host-known count
+        // sizes the dot kernel's shared memory; the kernels read j themselves)
+        const int nt = steps + it + 1;
         k_spmv_basis<<<gs, kBlk, 0, st>>>(n, s->Ap, s->Ai, K, s->dinv, s->V, s->w, s->G);
         for (int pass = 0; pass < 2; pass++) {
-          k_multidot<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->gpart, s->G);
-          k_multidot_fin<<<1, kFin, 0, st>>>(g, s->gpart, s->H, s->htmp, pass, s->G);
-          k_multiaxpy<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->htmp, s->G);
+          k_multidot<<<gm, kBlk, multidot_smem(nt), st>>>(n, s->V, s->w, s->gpart, s->G);
+          k_multidot_fin<<<1, kFin, 0, st>>>(gm, s->gpart, s->H, s->htmp, pass, s->G);
+          k_multiaxpy<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->htmp, pass ? s->part0 : nullptr, s->G);
         }
-        k_gdot<<<g, kBlk, 0, st>>>(n, s->w, s->part0, s->G);
         k_gnorm_fin<<<1, kFin, 0, st>>>(g, s->part0, s->H, s->G);
         k_gscale<<<g, kBlk, 0, st>>>(n, s->V, s->w, s->H, s->G);
         k_givens<<<1, 1, 0, st>>>(s->H, s->cs, s->sn, s->g, s->G);
@@ -762,6 +774,12 @@ int pgfem_gpu_solver_create(const int *Ap, const int *Ai, long nrows, const pgfe
   for (long j = 0; j < nnz; j++)
     if (Ai[j] < 0 || Ai[j] >= nrows) return PGFEM_GPU_EPATTERN;
   if (!device_ok()) return PGFEM_GPU_ENODEV;
+  if (opts->solver == PGFEM_SOLVER_GMRES &&
+      cudaFuncSetAttribute(k_multidot, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)multidot_smem(opts->kdim + 1)) != cudaSuccess) {
+    cudaGetLastError();
+    return PGFEM_GPU_ECUDA;
+  }
   pgfem_gpu_solver *s = new pgfem_gpu_solver();
   s->n = nrows;
   s->nnz = nnz;
