@@ -109,9 +109,10 @@ __device__ __forceinline__ void p2_point(const AsmArgs &args, const double *xu, 
       for (int j = 0; j < 3; j++)
         F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] + dU[i * 3 + 1] * dXi[1 * 3 + j] +
                        dU[i * 3 + 2] * dXi[2 * 3 + j];
-    if (args.F0)
+    const double *F0 = args.elem_group ? args.F0_tab + 9 * (long)args.elem_group[e] : args.F0;
+    if (F0)
 #pragma unroll
-      for (int i = 0; i < 9; i++) F[i] += args.F0[i];
+      for (int i = 0; i < 9; i++) F[i] += F0[i];
   }
   const double J = ok ? det3(F) : -1.0;
   if (ok) ok = J > 0.0 && inv3(F, Fi);
@@ -210,10 +211,12 @@ __device__ __forceinline__ void p2_vectors(const AsmArgs &args, const double *re
 // a1: its four w a1 / 2; meta / pos: its nodes' row metadata and positions.
 // NB: column nodes per pass (5: two passes, fewer registers; 10: one pass,
 // the row node's vectors loaded once per point)
-template <bool PLASTIC, int NB = 5>
+// NNE, NQP: nodes and quadrature points of the element (10, 4 quadratic tets;
+// 4, 1 linear tets).
+template <bool PLASTIC, int NB = 5, int NNE = 10, int NQP = 4>
 __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec, const double *a1,
                                           const int *meta, const uint16_t *pos, int a, int k) {
-  constexpr int NNE = 10, NQP = 4, VS = kP2VS;
+  constexpr int VS = kP2VS;
   const int *mA = meta + a * 7;
   const unsigned maskA = ((unsigned)mA[0] >> mA[6]) & 0xFFu;
   if (!maskA) return;
@@ -708,6 +711,107 @@ __global__ void __launch_bounds__(kWThreads, 3) k_assemble_p2r(const AsmArgs arg
     }
   }
   if (fail && (tid & 31) == 0) atomicAdd(&args.status[3], 1ull);
+}
+
+
+// ---- linear tets: column-split assembly from point records ----------------
+//
+// The linear-tet counterpart of k_assemble_p2r for the default R+K path
+// (configs 1 and 5): the point updates run first in k_qp_update<4, 1, MODEL>
+// (one thread per point, records in HBM); this kernel takes tiles of TE
+// elements -- claimed `grab` tiles at a time from a ticket when a work-stealing
+// schedule is set, else grid-stride -- and runs in turn
+//   0  the tile's point records (structure of arrays, coalesced) and the CSR
+//      metadata of its (element, node) pairs into shared memory;
+//   2  item (element, node): the vector record (p, U, W, T, S, n p);
+//   3  thread (element, row node a, column component k): the entries
+//      (a, i; b, k) of K_ab for i = 0..2 and the four column nodes b, and the
+//      residual; the three lanes k of one (element, a) are adjacent, so each
+//      FP64 reduction instruction writes three consecutive doubles of a CSR
+//      row segment (the per-node kernel writes one double per sector).
+constexpr int kP1ES = 4 * kP2VS + 2;  // doubles per element of vector records (even, bank-spread)
+
+inline size_t p1r_smem_bytes(int TE) {
+  return sizeof(double) * ((size_t)kRec * TE + (size_t)TE * kP1ES + TE) + sizeof(int) * (size_t)TE * 4 * 7 +
+         sizeof(uint16_t) * (size_t)TE * 16;
+}
+
+template <int MODEL, int TE>
+__global__ void __launch_bounds__(TE * 12) k_assemble_p1r(const AsmArgs args) {
+  constexpr int NNE = 4, VS = kP2VS, NT = TE * 12;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ __align__(16) double p1s[];
+  double *sRec = p1s;                                                   // [kRec][TE]
+  double *sVec = sRec + kRec * TE;                                      // [TE][kP1ES]
+  double *sA1 = sVec + TE * kP1ES;                                      // [TE]
+  int *sMeta = reinterpret_cast<int *>(sA1 + TE);                       // [TE][NNE][7]
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + TE * NNE * 7);  // [TE][NNE][NNE]
+  const int tid = threadIdx.x;
+  const long ne = args.ne;
+  __shared__ long s_claim;
+  long claim_end = 0;
+  long tile0 = (long)blockIdx.x * TE;
+  if (args.ticket) {
+    if (tid == 0) s_claim = (long)atomicAdd(args.ticket, (unsigned)args.grab) * TE;
+    __syncthreads();
+    tile0 = s_claim;
+    claim_end = tile0 + (long)args.grab * TE;
+    __syncthreads();
+  }
+  while (tile0 < ne) {
+    // phase 0: records and metadata
+    for (int t = tid; t < kRec * TE; t += NT) {
+      const int c = t / TE, el = t - c * TE;
+      const long e = tile0 + el;
+      sRec[t] = e < ne ? args.qrec[(long)c * args.nqp + e] : 0.0;  // one point per element
+    }
+    if (tid < TE * NNE) {
+      const int el = tid / NNE, a = tid - el * NNE;
+      const long e = tile0 + el;
+      if (e < ne) {
+        const int node = args.conn[(long)a * ne + e];
+        int *m = sMeta + tid * 7;
+        m[0] = args.mask[node];
+        m[1] = args.rowptr0[node];
+        m[2] = args.rowlen[node];
+        m[3] = args.dof[node];
+        m[4] = args.dof[args.nn + node];
+        m[5] = args.dof[2 * args.nn + node];
+        m[6] = 0;
+        const uint16_t *pr = args.pos + (e * NNE + a) * NNE;
+#pragma unroll
+        for (int b = 0; b < NNE; b++) sPos[tid * NNE + b] = pr[b];
+      }
+    }
+    __syncthreads();
+    // phase 2: vector records
+    if (tid < TE * NNE) {
+      const int el = tid / NNE, a = tid - el * NNE;
+      if (tile0 + el < ne) p2_vectors<PLASTIC, TE>(args, sRec + el, 0, a, sVec + el * kP1ES + a * VS, sA1 + el);
+    }
+    __syncthreads();
+    // phase 3: column-split blocks and reductions
+    {
+      const int el = tid / 12, r = tid - el * 12;
+      const int a = r / 3, k = r - a * 3;
+      if (tile0 + el < ne)
+        p2_blocks<PLASTIC, 4, 4, 1>(args, sVec + el * kP1ES, sA1 + el, sMeta + el * NNE * 7,
+                                    sPos + el * NNE * NNE, a, k);
+    }
+    __syncthreads();
+    if (args.ticket) {
+      tile0 += TE;
+      if (tile0 >= claim_end) {
+        if (tid == 0) s_claim = (long)atomicAdd(args.ticket, (unsigned)args.grab) * TE;
+        __syncthreads();
+        tile0 = s_claim;
+        claim_end = tile0 + (long)args.grab * TE;
+        __syncthreads();
+      }
+    } else {
+      tile0 += (long)gridDim.x * TE;
+    }
+  }
 }
 
 }  // namespace pgb

@@ -41,6 +41,8 @@ struct QpArgs {
   const int *conn;      // NNE*ne (SoA)
   long nn, ne, nqp;
   const double *F0;
+  const int *elem_group;  // FE2 batches: element -> group (or nullptr)
+  const double *F0_tab;   // group -> macro deformation (9)
   const double *state_n;
   double *state_np1;
   double *qrec;         // kQRec*nqp (SoA)
@@ -84,9 +86,10 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
       for (int j = 0; j < 3; j++)
         F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] + dU[i * 3 + 1] * dXi[1 * 3 + j] +
                        dU[i * 3 + 2] * dXi[2 * 3 + j];
-    if (A.F0)
+    const double *F0 = A.elem_group ? A.F0_tab + 9 * (long)A.elem_group[e] : A.F0;
+    if (F0)
 #pragma unroll
-      for (int i = 0; i < 9; i++) F[i] += A.F0[i];
+      for (int i = 0; i < 9; i++) F[i] += F0[i];
   }
   const double J = ok ? det3(F) : -1.0;
   if (ok) ok = J > 0.0 && inv3(F, Fi);

@@ -346,6 +346,8 @@ int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   q.ne = c->ne;
   q.nqp = c->nqp;
   q.F0 = c->F0;
+  q.elem_group = c->elem_group;
+  q.F0_tab = c->F0_tab;
   q.state_n = c->state_n;
   q.state_np1 = c->state_np1;
   q.qrec = c->qrec;
@@ -523,6 +525,47 @@ int launch_p2r(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+// linear tets in two kernels: point updates into c->qrec, then the column-split
+// assembly from the records with the context's schedule (elements per block,
+// work stealing)
+template <int MODEL, int TE>
+int launch_p1r_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+  AsmArgs a = a0;
+  a.qrec = c->qrec;
+  if (c->sched_grab > 0) {
+    a.ticket = c->sched_ticket;
+    a.grab = c->sched_grab;
+  }
+  const size_t smem = p1r_smem_bytes(TE);
+  auto kern = k_assemble_p1r<MODEL, TE>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TE * 12, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long tiles = (a.ne + TE - 1) / TE;
+  long grid = std::min<long>(tiles, (long)g_num_sms * per_sm * 8);
+  if (a.ticket) {  // persistent: every CTA resident, tiles claimed from the ticket
+    CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), s));
+    grid = std::min<long>(tiles, (long)g_num_sms * per_sm);
+  }
+  kern<<<(unsigned)std::max<long>(1, grid), TE * 12, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+template <int MODEL>
+int launch_p1r(pgfem_gpu_ctx *c, const AsmArgs &a, cudaStream_t s) {
+  if (int r = launch_qp_update<4, 1, MODEL>(c, s)) return r;
+  if (c->sched_epb == 16) return launch_p1r_te<MODEL, 16>(c, a, s);
+  if (c->sched_epb == 64) return launch_p1r_te<MODEL, 64>(c, a, s);
+  return launch_p1r_te<MODEL, 32>(c, a, s);
+}
+
 template <bool ATOMIC, bool WANT_K, bool DENSE>
 int dispatch(pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
   // quadratic tets, R+K into the CSR with atomic scatter over all elements:
@@ -535,6 +578,11 @@ int dispatch(pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
       return c->model == PGFEM_MODEL_J2 ? launch_p2ws<1>(a, s) : launch_p2ws<0>(a, s);
     return c->model == PGFEM_MODEL_J2 ? launch_p2r<1>(c, a, s) : launch_p2r<0>(c, a, s);
   }
+  // linear tets, R+K into the CSR with atomic scatter over all elements: the
+  // point kernel + column-split assembly with the context's schedule
+  // (PGFEM_GPU_P1_NODE selects the per-node kernel below)
+  if (c->nne == 4 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_P1_NODE"))
+    return c->model == PGFEM_MODEL_J2 ? launch_p1r<1>(c, a, s) : launch_p1r<0>(c, a, s);
   // linear tets over all elements: the tuned schedule (elements per block,
   // work stealing)
   if (c->nne == 4 && ATOMIC && !DENSE && !a.elist && (c->sched_epb || c->sched_grab)) {
@@ -981,6 +1029,8 @@ int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_ELEMENT_ROWS") &&
       !getenv("PGFEM_GPU_P2_SYNC") && !getenv("PGFEM_GPU_P2_FUSED"))
     return 3;  // u expansion, point updates, pipelined R+K assembly
+  if (c->nne == 4 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_P1_NODE"))
+    return 3;  // u expansion, point updates, column-split R+K assembly
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
 }

@@ -279,7 +279,8 @@ class RveBatch(Problem):
         ids[ids > 0] -= d0
         Ap = (self.Ap[d0:d1 + 1] - self.Ap[d0]).astype(np.int32)
         Ai = (self.Ai[self.Ap[d0]:self.Ap[d1]] - d0).astype(np.int32)
-        state = None if self.state is None else self.state[e0:e1]
+        ni = self.nint
+        state = None if self.state is None else self.state[e0 * ni:e1 * ni]
         return Problem("%s_rve%d" % (self.name, r), self.X[n0:n1], conn, ids, d1 - d0, Ap, Ai, self.mat,
                        self.u[d0:d1].copy(), state=state, F0=self.F0s[r].copy(), meta=dict(n=int(self.n_r[r])))
 
@@ -289,13 +290,14 @@ class RveBatch(Problem):
         return ctx
 
 
-def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3, subset=None):
+def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3, subset=None, nne=4):
     """Config 5: nrve periodic unit cubes, n_r^3 cells x 6 linear tets with n_r
     uniform in nmin..nmax, macro F0 = sym(U(-0.02, 0.02)^{3x3}) per RVE, a
     seeded periodic fluctuation field of amplitude fluct * h_r, J2 material
     (E 200 GPa, nu 0.3, yield 250 MPa, H 2 GPa), state at identity.
     subset: indices of the RVEs to build (a rank's shard); sizes, macro
-    deformations and fluctuations are those of the full batch."""
+    deformations and fluctuations are those of the full batch.  nne 10 builds
+    quadratic tets (4 points per element) instead."""
     ns_all = nmin + np.minimum((splitmix64(seed, nrve, stream=7) * (nmax - nmin + 1)).astype(np.int64),
                                nmax - nmin)
     A_all = (2.0 * splitmix64(seed, 9 * nrve, stream=8) - 1.0).reshape(nrve, 3, 3) * 0.02
@@ -304,7 +306,7 @@ def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3, subset=None)
     Xs, conns, idss, node_off, elem_off, dof_off = [], [], [], [0], [0], [0]
     us = []
     for r, n in zip(sel, ns):
-        X, conn, Pr = pg.mesh_box_tet(int(n), 4, periodic=True)
+        X, conn, Pr = pg.mesh_box_tet(int(n), nne, periodic=True)
         nn = X.shape[0]
         ids, ndof = pg.generate_dof_ids(conn, nn, np.zeros((nn, 3), dtype=np.int64), Pr=Pr)
         Xs.append(X)
@@ -327,7 +329,7 @@ def rve_batch(nrve=256, seed=RVE_SEED, nmin=8, nmax=24, fluct=1e-3, subset=None)
     F0s = (0.5 * (A + np.transpose(A, (0, 2, 1)))).reshape(len(sel), 9)
     u = np.concatenate(us)
     mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
-    state = np.zeros((conn.shape[0], 10))
+    state = np.zeros((conn.shape[0] * (4 if nne == 10 else 1), 10))
     state[:, [0, 4, 8]] = 1.0
     p = RveBatch("rve_batch_%d" % nrve, X, conn, ids, ndof, Ap, Ai, mat, u, state=state,
                  meta=dict(nrve=nrve, seed=seed, nmin=nmin, nmax=nmax, subset=sel.tolist()))

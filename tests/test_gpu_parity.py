@@ -256,6 +256,41 @@ def test_quadratic_tet_kernel_variants_agree(gpu, model):
             assert np.abs(sg - so).max() <= TOL * np.abs(so).max(), env
 
 
+@pytest.mark.parametrize("model", ["j2", "he"])
+def test_linear_tet_kernel_variants_agree(gpu, model):
+    """The R+K paths for 4-node elements -- the default (point kernel, then the
+    column-split assembly) with each schedule (elements per block 16/32/64,
+    static or work stealing) and the per-node kernel -- on 5^3 x 6 = 750
+    elements, so that the last tile of every block size is partly empty;
+    each against the oracle."""
+    import os
+    p = wl.he_p1(5, seed=4)
+    p.u = p.u * 0.3
+    if model == "j2":
+        p.mat = pg.material(pg.MODEL_J2, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0)
+        p.state = np.zeros((p.nqp, 10))
+        p.state[:, [0, 4, 8]] = 1.0
+    assert p.ne % 16 and p.ne % 32 and p.ne % 64
+    ctx = p.context()
+    Ro, Ko, so = oracle_assemble(p)
+    if so is not None:
+        assert (so[:, 9] > 0).any()
+    runs = [(epb, grab, {}) for epb in (16, 32, 64) for grab in (0, 2)] + [(0, 0, {"PGFEM_GPU_P1_NODE": "1"})]
+    for epb, grab, env in runs:
+        ctx.set_schedule(epb, grab)
+        os.environ.update(env)
+        try:
+            R, K, st = ctx.assemble_RK(p.u)
+        finally:
+            for k in env:
+                os.environ.pop(k, None)
+        assert st.ok(), (epb, grab, env, st.as_dict())
+        check_R(R, Ro)
+        check_K(K, Ko, p.Ap)
+        if so is not None:
+            assert np.abs(ctx.get_state(1) - so).max() <= TOL * np.abs(so).max(), (epb, grab, env)
+
+
 def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
     # number the nodes in reverse order (ids stay consecutive per node, but the
     # rows are no longer first touched in element order)

@@ -81,3 +81,23 @@ def test_schedules_and_graph_replay_agree(gpu, batch):
     g.destroy()
     with pytest.raises(pg.PgfemError):
         ctx.set_schedule(24, 1)
+
+
+def test_quadratic_tet_groups_use_their_own_macro_deformation(gpu):
+    """Mesh groups on a quadratic-tet context: each RVE of the batch sees its
+    own macro F through the default two-kernel path (the point kernel applies
+    the group's F0); every RVE equals the oracle run on it alone."""
+    p = wl.rve_batch(nrve=3, nmin=2, nmax=3, seed=11, nne=10)
+    assert len(set(map(tuple, np.round(p.F0s, 12)))) == 3
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    S = ctx.get_state(1)
+    for r in range(len(p.n_r)):
+        q = p.rve(r)
+        Ro, Ko, so = _oracle_rve(q)
+        d0, d1 = p.dof_off[r], p.dof_off[r + 1]
+        check_R(R[d0:d1], Ro)
+        check_K(K[p.Ap[d0]:p.Ap[d1]], Ko, q.Ap)
+        e0, e1 = p.elem_off[r] * 4, p.elem_off[r + 1] * 4
+        assert np.abs(S[e0:e1] - so).max() <= TOL * np.abs(so).max()
