@@ -690,24 +690,35 @@ void scatter(const orc_problem *P, long e, const double *fe, const double *lk, d
   }
 }
 
-// Greedy element colouring: no two elements of one colour share a node.
+// Greedy element colouring: no two elements of one colour share a free DOF
+// (the rows of R and K they add into).  Sharing a node implies sharing its
+// DOFs, and on periodic meshes distinct slave and master nodes share DOF ids,
+// so the test is on DOF ids, not node ids.
 std::vector<std::vector<long>> colour_elements(const orc_problem *P, long e0, long e1) {
   std::vector<std::vector<long>> colours;
-  std::vector<std::vector<char>> used;  // per colour: node mask (lazy)
+  std::vector<std::vector<char>> used;  // per colour: free-DOF mask (lazy)
+  auto touches = [&](long e, const std::vector<char> &mask) {
+    for (int a = 0; a < P->nne; a++)
+      for (int c = 0; c < 3; c++) {
+        const long id = P->id[(long)P->conn[e * P->nne + a] * 3 + c];
+        if (id > 0 && mask[id - 1]) return true;
+      }
+    return false;
+  };
   for (long e = e0; e < e1; e++) {
     size_t c = 0;
-    for (; c < colours.size(); c++) {
-      bool ok = true;
-      for (int a = 0; a < P->nne && ok; a++)
-        if (used[c][P->conn[e * P->nne + a]]) ok = false;
-      if (ok) break;
-    }
+    for (; c < colours.size(); c++)
+      if (!touches(e, used[c])) break;
     if (c == colours.size()) {
       colours.emplace_back();
-      used.emplace_back(P->nn, 0);
+      used.emplace_back(std::max<long>(P->ndof, 1), 0);
     }
     colours[c].push_back(e);
-    for (int a = 0; a < P->nne; a++) used[c][P->conn[e * P->nne + a]] = 1;
+    for (int a = 0; a < P->nne; a++)
+      for (int k = 0; k < 3; k++) {
+        const long id = P->id[(long)P->conn[e * P->nne + a] * 3 + k];
+        if (id > 0) used[c][id - 1] = 1;
+      }
   }
   return colours;
 }

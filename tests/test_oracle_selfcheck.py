@@ -6,6 +6,7 @@
   4-nested compute_stiffness_matrix assembly
 - patch test: an affine displacement gives zero residual on interior DOFs
 - rigid rotation leaves S unchanged; HE and J2 elastic K are symmetric
+- the threaded assembly equals the serial one, periodic cells included
 """
 import numpy as np
 import pytest
@@ -87,6 +88,22 @@ def test_multithreaded_assembly_equals_serial():
     _, R4, K4, _ = P.assemble(mat, p.u, state_n=p.state, nthreads=4)
     assert np.linalg.norm(R4 - R1) <= 1e-13 * np.linalg.norm(R1)
     assert np.linalg.norm(K4 - K1) <= 1e-13 * np.linalg.norm(K1)
+
+
+def test_multithreaded_assembly_on_periodic_cell_equals_serial():
+    """Periodic cells map distinct slave and master nodes to one DOF: the
+    threaded assembly's element colours must keep elements that share a DOF
+    apart, not only elements that share a node (repeated, since a race shows
+    only on some runs)."""
+    b = wl.rve_batch(nrve=9, nmin=3, nmax=7, seed=5)
+    for r in range(len(b.n_r)):
+        q = b.rve(r)
+        P, mat = oracle.from_workload(q)
+        _, R1, K1, _ = P.assemble(mat, q.u, state_n=q.state, nthreads=1)
+        for _ in range(6):
+            _, R8, K8, _ = P.assemble(mat, q.u, state_n=q.state, nthreads=8)
+            assert np.abs(R8 - R1).max() <= 1e-13 * np.abs(R1).max()
+            assert np.abs(K8 - K1).max() <= 1e-13 * np.abs(K1).max()
 
 
 @pytest.mark.parametrize("nne", [4, 10])
