@@ -814,4 +814,150 @@ __global__ void __launch_bounds__(TE * 12) k_assemble_p1r(const AsmArgs args) {
   }
 }
 
+
+// ---- linear tets: warp-specialised column-split assembly (default) ---------
+//
+// k_assemble_p1r as a producer/consumer pipeline: the last warp (producer)
+// claims tiles of TE elements (from the ticket, `grab` at a time, when a
+// work-stealing schedule is set; else grid-stride), copies a tile's point
+// records and CSR metadata with cp.async one tile ahead, builds its vector
+// records and hands it over with the tile's first element in shared memory
+// (-1: no more tiles); TE/2 consumer warps (16 lanes per element, 12 used)
+// form the column-split blocks and issue the reductions.  Hand-off through the
+// bounded mbarrier waits of k_assemble_p2ws (a wait that runs out sets
+// status[3] and ends the loops).  Records are copied 8 bytes at a time: with
+// an odd element count a 16-byte chunk of a record row would be misaligned.
+template <int TE>
+constexpr int p1ws_threads() { return TE * 16 + 32; }
+
+inline size_t p1ws_smem_bytes(int TE) {
+  return 64 + sizeof(double) * (2 * (size_t)kRec * TE + 2 * (size_t)TE * kP1ES + 2 * (size_t)TE) +
+         sizeof(int) * 3 * (size_t)TE * 4 * 7 + sizeof(uint16_t) * 3 * (size_t)TE * 16;
+}
+
+__device__ __forceinline__ void p1_fetch_meta(const AsmArgs &args, long e, int a, int node, int *m,
+                                              uint16_t *sp) {
+  cpa4(m + 0, args.mask + (node & ~3));  // the aligned word holding the mask byte
+  cpa4(m + 1, args.rowptr0 + node);
+  cpa4(m + 2, args.rowlen + node);
+  cpa4(m + 3, args.dof + node);
+  cpa4(m + 4, args.dof + args.nn + node);
+  cpa4(m + 5, args.dof + 2 * args.nn + node);
+  m[6] = (node & 3) * 8;
+  cpa8(sp, args.pos + (e * 4 + a) * 4);  // the four uint16 column positions of (e, a)
+}
+
+template <int MODEL, int TE>
+__global__ void __launch_bounds__(p1ws_threads<TE>()) k_assemble_p1ws(const AsmArgs args) {
+  constexpr int NNE = 4, VS = kP2VS, NC = TE * 16;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ __align__(16) unsigned char p1w[];
+  uint64_t *full = reinterpret_cast<uint64_t *>(p1w);     // [2]
+  uint64_t *empty = full + 2;                              // [2]
+  long *sTile = reinterpret_cast<long *>(p1w + 32);        // [2] first element of the handed-over tile
+  double *sRec = reinterpret_cast<double *>(p1w + 64);     // [2][kRec][TE]
+  double *sVec = sRec + 2 * kRec * TE;                     // [2][TE][kP1ES]
+  double *sA1 = sVec + 2 * TE * kP1ES;                     // [2][TE]
+  int *sMeta = reinterpret_cast<int *>(sA1 + 2 * TE);      // [3][TE][NNE][7]
+  uint16_t *sPos = reinterpret_cast<uint16_t *>(sMeta + 3 * TE * NNE * 7);  // [3][TE][NNE][NNE]
+  const int tid = threadIdx.x;
+  const long ne = args.ne;
+  if (tid == 0) {
+    w_mb_init(&full[0], 32);
+    w_mb_init(&full[1], 32);
+    w_mb_init(&empty[0], NC);
+    w_mb_init(&empty[1], NC);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  bool fail = false;
+  if (tid >= NC) {
+    // ------------------------------ producer ------------------------------
+    const int pl = tid - NC;
+    long claim_next = 0, claim_end = 0, grid_next = (long)blockIdx.x * TE;
+    auto next_tile = [&]() -> long {  // first element of the next tile (>= ne: none)
+      if (!args.ticket) {
+        const long t = grid_next;
+        grid_next += (long)gridDim.x * TE;
+        return t;
+      }
+      if (claim_next >= claim_end) {
+        unsigned c = 0;
+        if (pl == 0) c = atomicAdd(args.ticket, (unsigned)args.grab);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        claim_next = (long)c * TE;
+        claim_end = claim_next + (long)args.grab * TE;
+      }
+      const long t = claim_next;
+      claim_next += TE;
+      return t;
+    };
+    auto issue = [&](long t0, int slot, int bm) {
+      for (int u = pl; u < TE * NNE; u += 32) {
+        const int el = u / NNE, a = u - el * NNE;
+        const long e = t0 + el;
+        if (e < ne) {
+          const int node = args.conn[(long)a * ne + e];
+          p1_fetch_meta(args, e, a, node, sMeta + (bm * TE * NNE + u) * 7, sPos + (bm * TE * NNE + u) * NNE);
+        }
+      }
+      for (int u = pl; u < kRec * TE; u += 32) {
+        const int c = u / TE, el = u - c * TE;
+        const long e = t0 + el;
+        if (e < ne) cpa8(sRec + (slot * kRec + c) * TE + el, args.qrec + (long)c * args.nqp + e);
+      }
+      cpa_commit();
+    };
+    long t_cur = next_tile();
+    if (t_cur < ne) issue(t_cur, 0, 0);
+    for (long i = 0;; i++) {
+      const int bx = (int)(i & 1);
+      if (i >= 2) {
+        const bool ok = w_mb_wait(&empty[bx], (unsigned)(((i - 2) >> 1) & 1));
+        if (__any_sync(0xffffffffu, !ok)) {
+          fail = true;
+          break;
+        }
+      }
+      if (t_cur >= ne) {  // no more tiles: tell the consumers
+        if (pl == 0) sTile[bx] = -1;
+        w_mb_arrive(&full[bx]);
+        break;
+      }
+      cpa_wait_all();  // tile i's records and metadata have landed
+      __syncwarp();
+      const long t_nxt = next_tile();
+      if (t_nxt < ne) issue(t_nxt, (int)((i + 1) & 1), (int)((i + 1) % 3));
+      for (int u = pl; u < TE * NNE; u += 32) {
+        const int el = u / NNE, a = u - el * NNE;
+        if (t_cur + el < ne)
+          p2_vectors<PLASTIC, TE>(args, sRec + bx * kRec * TE + el, 0, a,
+                                  sVec + (bx * TE + el) * kP1ES + a * VS, sA1 + bx * TE + el);
+      }
+      if (pl == 0) sTile[bx] = t_cur;
+      w_mb_arrive(&full[bx]);  // release: vectors and the tile index are visible to the consumers
+      t_cur = t_nxt;
+    }
+    cpa_wait_all();
+  } else {
+    // ------------------------------ consumers ------------------------------
+    const int el = tid >> 4, r = tid & 15;
+    const int a = r / 3, k = r - a * 3;
+    for (long i = 0;; i++) {
+      const int bx = (int)(i & 1), bm = (int)(i % 3);
+      if (!w_mb_wait(&full[bx], (unsigned)((i >> 1) & 1))) {
+        fail = true;
+        break;
+      }
+      const long t0 = sTile[bx];
+      if (t0 < 0) break;
+      if (r < 12 && t0 + el < ne)
+        p2_blocks<PLASTIC, 4, 4, 1>(args, sVec + (bx * TE + el) * kP1ES, sA1 + bx * TE + el,
+                                    sMeta + (bm * TE + el) * NNE * 7, sPos + (bm * TE + el) * NNE * NNE, a, k);
+      w_mb_arrive(&empty[bx]);
+    }
+  }
+  if (fail && (tid & 31) == 0) atomicAdd(&args.status[3], 1ull);
+}
+
 }  // namespace pgb

@@ -558,12 +558,48 @@ int launch_p1r_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
+template <int MODEL, int TE>
+int launch_p1ws_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+  AsmArgs a = a0;
+  a.qrec = c->qrec;
+  if (c->sched_grab > 0) {
+    a.ticket = c->sched_ticket;
+    a.grab = c->sched_grab;
+  }
+  const size_t smem = p1ws_smem_bytes(TE);
+  auto kern = k_assemble_p1ws<MODEL, TE>;
+  constexpr int nt = p1ws_threads<TE>();
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, nt, smem));
+  if (per_sm < 1) per_sm = 1;
+  if (!g_num_sms) grid_for(1, 1, 1);
+  const long tiles = (a.ne + TE - 1) / TE;
+  if (a.ticket) CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), s));
+  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
+  kern<<<(unsigned)grid, nt, smem, s>>>(a);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+// elements per block of the schedule -> the pipeline's tile: 16 -> 8, 32 (or
+// unset) -> 16, 64 -> 32 elements (the consumer warps of a CTA hold two
+// elements each)
 template <int MODEL>
 int launch_p1r(pgfem_gpu_ctx *c, const AsmArgs &a, cudaStream_t s) {
   if (int r = launch_qp_update<4, 1, MODEL>(c, s)) return r;
-  if (c->sched_epb == 16) return launch_p1r_te<MODEL, 16>(c, a, s);
-  if (c->sched_epb == 64) return launch_p1r_te<MODEL, 64>(c, a, s);
-  return launch_p1r_te<MODEL, 32>(c, a, s);
+  if (getenv("PGFEM_GPU_P1_SYNC")) {  // all threads run the phases of a tile in turn
+    if (c->sched_epb == 16) return launch_p1r_te<MODEL, 16>(c, a, s);
+    if (c->sched_epb == 64) return launch_p1r_te<MODEL, 64>(c, a, s);
+    return launch_p1r_te<MODEL, 32>(c, a, s);
+  }
+  if (c->sched_epb == 16) return launch_p1ws_te<MODEL, 8>(c, a, s);
+  if (c->sched_epb == 64) return launch_p1ws_te<MODEL, 32>(c, a, s);
+  return launch_p1ws_te<MODEL, 16>(c, a, s);
 }
 
 template <bool ATOMIC, bool WANT_K, bool DENSE>

@@ -259,10 +259,11 @@ def test_quadratic_tet_kernel_variants_agree(gpu, model):
 @pytest.mark.parametrize("model", ["j2", "he"])
 def test_linear_tet_kernel_variants_agree(gpu, model):
     """The R+K paths for 4-node elements -- the default (point kernel, then the
-    column-split assembly) with each schedule (elements per block 16/32/64,
-    static or work stealing) and the per-node kernel -- on 5^3 x 6 = 750
-    elements, so that the last tile of every block size is partly empty;
-    each against the oracle."""
+    warp-specialised column-split assembly) with each schedule (elements per
+    block 16/32/64, static or work stealing), the variant in which all threads
+    run the phases of a tile in turn, and the per-node kernel -- on
+    5^3 x 6 = 750 elements, so that the last tile of every tile size is partly
+    empty; each against the oracle."""
     import os
     p = wl.he_p1(5, seed=4)
     p.u = p.u * 0.3
@@ -275,7 +276,9 @@ def test_linear_tet_kernel_variants_agree(gpu, model):
     Ro, Ko, so = oracle_assemble(p)
     if so is not None:
         assert (so[:, 9] > 0).any()
-    runs = [(epb, grab, {}) for epb in (16, 32, 64) for grab in (0, 2)] + [(0, 0, {"PGFEM_GPU_P1_NODE": "1"})]
+    runs = [(epb, grab, {}) for epb in (16, 32, 64) for grab in (0, 2)]
+    runs += [(32, 0, {"PGFEM_GPU_P1_SYNC": "1"}), (16, 2, {"PGFEM_GPU_P1_SYNC": "1"}),
+             (0, 0, {"PGFEM_GPU_P1_NODE": "1"})]
     for epb, grab, env in runs:
         ctx.set_schedule(epb, grab)
         os.environ.update(env)
