@@ -70,6 +70,10 @@ typedef struct {
   double G0, g0, gs_0, gamma_dot_s, w; /* CP saturation hardening */
   double cp_tol;         /* CP local residual tolerance */
   int cp_max_iter;       /* CP local iteration cap */
+  int dev_pot;           /* HE deviatoric potential, the reference's devPotFlag (src/new_potentials.cc:79-156):
+                            0 or 1 Mooney-Rivlin with m01 = 0 (neo-Hookean, m10 = G/2); 2 linear,
+                            S_dev = G (C - I) (devStress_Linear :364-375).  HE only; 2 runs the
+                            per-node element kernel on every R/K path (no tile or cell modes). */
 } pgfem_material_desc;
 
 typedef struct {

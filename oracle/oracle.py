@@ -76,8 +76,11 @@ def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0,
                        cp_max_iter, dev_pot)
 
 
-def from_pg_material(m, dev_pot=1):
-    """Oracle material from a pgfem_gpu.MaterialDesc (same field meanings)."""
+def from_pg_material(m, dev_pot=None):
+    """Oracle material from a pgfem_gpu.MaterialDesc (same field meanings; the
+    deviatoric potential flag is taken from the record unless given)."""
+    if dev_pot is None:
+        dev_pot = 2 if getattr(m, "dev_pot", 1) == 2 else 1
     return material(m.model, m.E, m.nu, m.sigma_y, m.H, m.gamma_dot_0, m.m, m.G0, m.g0, m.gs_0,
                     m.gamma_dot_s, m.w, m.cp_tol, m.cp_max_iter, dev_pot)
 

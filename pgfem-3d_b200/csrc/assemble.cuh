@@ -22,6 +22,10 @@
 // threads form their node's spatial vectors per point and scatter R.
 // Phase 3: node thread a forms the 3x3 blocks K_ab for b = 0..NNE-1, summed
 // over the points, and scatters them through the element->CSR node-block map.
+//
+// MODEL: 0 HE (neo-Hookean), 1 J2, 3 HE with the linear deviatoric potential,
+// whose tangent adds w G [b_ik (p_a . b p_b) + (b p_b)_i (b p_a)_k] to K_ab
+// (b = F F^T in the record's n slot, b p_a in the vector record's n p slot).
 #pragma once
 #include <cstdint>
 
@@ -220,7 +224,10 @@ __global__ void __launch_bounds__(TEP *NNE)
           }
           QpTangent t;
           double Anp1[6], alpha_np1;
-          spatial_update<PLASTIC>(args.mat, F, J, A, alpha, t, Anp1, &alpha_np1);
+          if (MODEL == 3)
+            linear_dev_update(args.mat, F, J, t);
+          else
+            spatial_update<PLASTIC>(args.mat, F, J, A, alpha, t, Anp1, &alpha_np1);
           if (PLASTIC && args.state_np1) {
 #pragma unroll
             for (int c = 0; c < 6; c++) args.state_np1[c * args.nqp + qp] = Anp1[c];
@@ -272,6 +279,13 @@ __global__ void __launch_bounds__(TEP *NNE)
         v[3] = sp[0];
         v[4] = sp[1];
         v[5] = sp[2];
+        if (MODEL == 3) {
+          double bp[3];
+          smv(rec + 22, p, bp);
+          v[6] = bp[0];
+          v[7] = bp[1];
+          v[8] = bp[2];
+        }
         if (PLASTIC) {
           double np_[3], Dp[3];
           smv(rec + 22, p, np_);
@@ -355,6 +369,17 @@ __global__ void __launch_bounds__(TEP *NNE)
             for (int i = 0; i < 3; i++)
 #pragma unroll
               for (int k = 0; k < 3; k++) acc[i * 3 + k] += npa[i] * (a4 * npb[k] + a5 * Dpb[k]);
+          }
+          if (MODEL == 3) {
+            const double wG = w * args.mat.mu;
+            const double *b = rec + 22;  // Voigt xx yy zz yz xz xy
+            const double bpa[3] = {va[6], va[7], va[8]}, bpb[3] = {vb[6], vb[7], vb[8]};
+            const double pbb = wG * (pa[0] * bpb[0] + pa[1] * bpb[1] + pa[2] * bpb[2]);
+            const double bf[9] = {b[0], b[5], b[4], b[5], b[1], b[3], b[4], b[3], b[2]};
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+              for (int k = 0; k < 3; k++) acc[i * 3 + k] += bf[i * 3 + k] * pbb + wG * bpb[i] * bpa[k];
           }
         }
         if (DENSE) {

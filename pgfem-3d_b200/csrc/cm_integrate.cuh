@@ -37,7 +37,11 @@ __global__ void k_cm_integrate(Mat mat, long nqp, const double *F_all, const dou
   }
   QpTangent t;
   double Anp1[6], alpha_np1;
-  spatial_update<PLASTIC>(mat, F, J, A, alpha, t, Anp1, &alpha_np1);
+  const bool linear_dev = !PLASTIC && mat.dev_pot == 2;
+  if (linear_dev)
+    linear_dev_update(mat, F, J, t);  // t.n = b, pulled back to the identity below
+  else
+    spatial_update<PLASTIC>(mat, F, J, A, alpha, t, Anp1, &alpha_np1);
   if (PLASTIC) {
     double *s = state_np1 + q * 10;
     s[0] = Anp1[0]; s[1] = Anp1[5]; s[2] = Anp1[4];
@@ -66,6 +70,7 @@ __global__ void k_cm_integrate(Mat mat, long nqp, const double *F_all, const dou
           double v = t.a1 * 0.5 * (sv(Ci, i, k) * sv(Ci, j, l) + sv(Ci, i, l) * sv(Ci, j, k)) +
                      t.a2 * cij * ckl - (2.0 / 3.0) * (sv(Ss, i, j) * ckl + cij * sv(Ss, k, l));
           if (PLASTIC) v += sv(Sn, i, j) * (t.a4 * sv(Sn, k, l) + t.a5 * sv(SD, k, l));
+          if (linear_dev) v += mat.mu * (sv(Sn, i, k) * sv(Sn, j, l) + sv(Sn, i, l) * sv(Sn, j, k));
           L[i * 27 + j * 9 + k * 3 + l] = v;
         }
 }

@@ -13,6 +13,13 @@
 //      U_Common volumetric potential (:553-604) as combined in
 //      src/displacement_based_element.cc:1368-1445, pushed forward:
 //      tau = mu dev(J^-2/3 F F^T) + kappa J (J-1) 1.
+//  HE, linear deviatoric potential (devPotFlag 2, devStress_Linear /
+//      matStiff_Linear, src/new_potentials.cc:364-375, 434-452): S = G (C - I)
+//      + kappa J (J-1) C^-1, L = 2G I + volumetric part; pushed forward
+//      tau = G (b^2 - b) + kappa J (J-1) 1 and
+//      c = G (b_ik b_jl + b_il b_jk) + a1 I + a2 1(x)1, which is not of the
+//      form above: the per-node element kernel adds the b-term itself
+//      (template model 3), from b = F F^T carried in the tangent's n slot.
 //  J2  (CM_J2P_PARAM, src/cm_j2_plasticity.cc:184-214, damage off): the
 //      isochoric-split radial return of Simo (1988) / Simo & Hughes (1998)
 //      Box 9.1 with linear isotropic hardening, state (Cp^-1, eqps), and the
@@ -24,6 +31,7 @@ namespace pgb {
 
 struct Mat {
   int model;
+  int dev_pot;  // HE deviatoric potential: 2 linear, otherwise neo-Hookean
   double mu, kappa, sy, H;
   // crystal plasticity
   double gdot0, m, G0, g0, gs0, gdots, w, tol;
@@ -187,6 +195,35 @@ __device__ __forceinline__ void spatial_update(const Mat &mat, const double *F, 
   o.tau[2] += pJ;
   o.a1 = 2.0 * mubar * r - 2.0 * kap * J * (J - 1.0);
   o.a2 = kap * J * (2.0 * J - 1.0) - (2.0 / 3.0) * mubar * r;
+}
+
+// HE with the linear deviatoric potential at one point: tau, the volumetric
+// tangent coefficients (s = n = D = 0, a4 = a5 = 0) and b = F F^T in o.n.
+__device__ __forceinline__ void linear_dev_update(const Mat &mat, const double *F, double J,
+                                                  QpTangent &o) {
+  const double G = mat.mu, kap = mat.kappa;
+  const double I6[6] = {1, 1, 1, 0, 0, 0};
+  double b[6];
+  push_sym(F, I6, b);
+  double b2[6];
+  b2[0] = b[0] * b[0] + b[5] * b[5] + b[4] * b[4];
+  b2[1] = b[5] * b[5] + b[1] * b[1] + b[3] * b[3];
+  b2[2] = b[4] * b[4] + b[3] * b[3] + b[2] * b[2];
+  b2[3] = b[5] * b[4] + b[1] * b[3] + b[3] * b[2];
+  b2[4] = b[0] * b[4] + b[5] * b[3] + b[4] * b[2];
+  b2[5] = b[0] * b[5] + b[5] * b[1] + b[4] * b[3];
+  const double pJ = kap * J * (J - 1.0);
+#pragma unroll
+  for (int i = 0; i < 6; i++) {
+    o.tau[i] = G * (b2[i] - b[i]) + (i < 3 ? pJ : 0.0);
+    o.s[i] = 0.0;
+    o.n[i] = b[i];
+    o.D[i] = 0.0;
+  }
+  o.a1 = -2.0 * kap * J * (J - 1.0);
+  o.a2 = kap * J * (2.0 * J - 1.0);
+  o.a4 = 0.0;
+  o.a5 = 0.0;
 }
 
 }  // namespace pgb

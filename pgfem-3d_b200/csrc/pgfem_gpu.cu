@@ -167,6 +167,7 @@ ShapeTable make_shape(int nne) {
 Mat make_mat(const pgfem_material_desc *m) {
   Mat r{};
   r.model = m->model;
+  r.dev_pot = m->model == PGFEM_MODEL_HE && m->dev_pot == 2 ? 2 : 1;
   r.mu = m->E / (2.0 * (1.0 + m->nu));
   r.kappa = (2 * r.mu * (1 + m->nu)) / (3 * (1 - 2 * m->nu));
   r.sy = m->sigma_y;
@@ -604,6 +605,11 @@ int launch_p1r(pgfem_gpu_ctx *c, const AsmArgs &a, cudaStream_t s) {
 
 template <bool ATOMIC, bool WANT_K, bool DENSE>
 int dispatch(pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
+  // HE with the linear deviatoric potential: its tangent is carried by the
+  // per-node kernel only (template model 3), for every call of this context
+  if (c->mat.dev_pot == 2)
+    return c->nne == 4 ? launch_asm<4, 1, 3, ATOMIC, WANT_K, DENSE>(a, nitems, s)
+                       : launch_asm<10, 4, 3, ATOMIC, WANT_K, DENSE>(a, nitems, s);
   // quadratic tets, R+K into the CSR with atomic scatter over all elements:
   // the column-split kernel, warp-specialised (PGFEM_GPU_P2_SYNC selects the
   // variant in which all threads run the three phases of a tile in turn)
@@ -816,23 +822,39 @@ int read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, bool clear) {
 
 // Greedy colouring: elements of one colour share no node, so their R and K
 // updates touch disjoint rows and need no atomics.
+// Greedy element colours for the plain-add scatter: no two elements of one
+// colour share a free DOF, i.e. a row of R and K.  (Periodic meshes map
+// distinct slave and master nodes to one DOF, so sharing no node is not
+// enough.)
 void build_colours(const pgfem_mesh_desc *m, std::vector<int> &elems, std::vector<long> &off) {
   std::vector<int> colour(m->ne, -1);
   std::vector<std::vector<uint8_t>> used;
   int ncol = 0;
+  auto dof_of = [&](long e, int a, int k) {  // 1-based free DOF id, 0 for fixed / prescribed
+    const long id = m->dof_id[(long)m->conn[e * m->nne + a] * 3 + k];
+    return id > 0 && id <= m->ndof ? id : 0L;
+  };
   for (long e = 0; e < m->ne; e++) {
     int c = 0;
     for (; c < ncol; c++) {
       bool ok = true;
-      for (int a = 0; a < m->nne && ok; a++) ok = !used[c][m->conn[e * m->nne + a]];
+      for (int a = 0; a < m->nne && ok; a++)
+        for (int k = 0; k < 3 && ok; k++) {
+          const long id = dof_of(e, a, k);
+          ok = !(id > 0 && used[c][id - 1]);
+        }
       if (ok) break;
     }
     if (c == ncol) {
-      used.emplace_back(m->nn, 0);
+      used.emplace_back(std::max<long>(1, m->ndof), 0);
       ncol++;
     }
     colour[e] = c;
-    for (int a = 0; a < m->nne; a++) used[c][m->conn[e * m->nne + a]] = 1;
+    for (int a = 0; a < m->nne; a++)
+      for (int k = 0; k < 3; k++) {
+        const long id = dof_of(e, a, k);
+        if (id > 0) used[c][id - 1] = 1;
+      }
   }
   off.assign(ncol + 1, 0);
   for (long e = 0; e < m->ne; e++) off[colour[e] + 1]++;
@@ -860,6 +882,8 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
       m->nn <= 0 || m->ne <= 0 || nrows != m->ndof || !Ap || !Ai)
     return PGFEM_GPU_EINVAL;
   if (mat->model < 0 || mat->model > 2) return PGFEM_GPU_EINVAL;
+  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE))
+    return PGFEM_GPU_EINVAL;
   if (mat->model == PGFEM_MODEL_CP && (m->nne != 4 || !m->R_cp || !(mat->m > 0) || !(mat->g0 > 0) ||
                                        !(mat->gs_0 > mat->g0)))
     return PGFEM_GPU_EINVAL;
@@ -978,8 +1002,9 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if ((r = upload(c, &c->cp_Fn, Fn.data(), Fn.size()))) return fail(r);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
   }
-  // tiled assembly plan (HE / J2)
-  if (c->model != PGFEM_MODEL_CP && !getenv("PGFEM_GPU_NO_TILES")) {
+  // tiled assembly plan (HE / J2; not for the linear deviatoric potential,
+  // which only the per-node kernel carries)
+  if (c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2 && !getenv("PGFEM_GPU_NO_TILES")) {
     std::vector<int> first_dof(nn, -1);
     for (long n = 0; n < nn; n++)
       for (int j = 0; j < 3 && first_dof[n] < 0; j++)
@@ -1060,6 +1085,8 @@ int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
   if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, tangent, element (+ features, network, guess)
     return c->cp_net ? 8 : 5;
+  if (c->mat.dev_pot == 2)  // u expansion + per-node kernel launches (one per colour in colour mode)
+    return 1 + (c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1);
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_CELLS && c->nne == 10) return 2;  // u expansion, cells
   if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
   if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_ELEMENT_ROWS") &&
@@ -1345,6 +1372,8 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
                            double *L, int *qp_status) {
   if (!mat || nqp < 0 || (nqp && (!F || !S))) return PGFEM_GPU_EINVAL;
   if (mat->model != PGFEM_MODEL_HE && mat->model != PGFEM_MODEL_J2) return PGFEM_GPU_EINVAL;
+  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE))
+    return PGFEM_GPU_EINVAL;
   if (mat->model == PGFEM_MODEL_J2 && nqp && (!state_n || !state_np1)) return PGFEM_GPU_EINVAL;
   int r = check_device();
   if (r) return r;

@@ -29,7 +29,8 @@ class MaterialDesc(C.Structure):
                 ("sigma_y", C.c_double), ("H", C.c_double),
                 ("gamma_dot_0", C.c_double), ("m", C.c_double), ("G0", C.c_double),
                 ("g0", C.c_double), ("gs_0", C.c_double), ("gamma_dot_s", C.c_double),
-                ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int)]
+                ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int),
+                ("dev_pot", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -144,9 +145,11 @@ def _check(fn, r):
 
 
 def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0, G0=0.0, g0=0.0,
-             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25):
+             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1):
+    """Material record; dev_pot is the reference's devPotFlag for HE (1
+    neo-Hookean, 2 linear deviatoric potential)."""
     return MaterialDesc(model, E, nu, sigma_y, H, gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w,
-                        cp_tol, cp_max_iter)
+                        cp_tol, cp_max_iter, dev_pot)
 
 
 # ---------------------------------------------------------------- setup ----

@@ -350,3 +350,55 @@ def test_cells_mode_is_for_quadratic_tets_only(gpu):
     ctx = wl.he_p1(4).context()
     with pytest.raises(pg.PgfemError):
         ctx.set_scatter_mode(pg.SCATTER_CELLS)
+
+
+@pytest.mark.parametrize("nne", [4, 10])
+def test_linear_deviatoric_potential_matches_oracle(gpu, nne):
+    """HE with the reference's linear deviatoric potential (devPotFlag 2,
+    S_dev = G (C - I)) at finite strain (30 % stretch, random perturbation,
+    prescribed face): R and K through the atomic and the colour scatter, the
+    R-only call, the element-level entry points and the constitutive level
+    equal the oracle with the same flag (1e-10)."""
+    p = wl.tension(n=3, nne=nne, model="he", stretch=0.3, predictor=True)
+    rng = np.random.default_rng(3)
+    p.u = p.u + rng.uniform(-0.02, 0.02, p.u.shape)
+    p.mat.dev_pot = 2
+    Ro, Ko, _ = oracle_assemble(p)
+    # the b-term is not negligible: the neo-Hookean K differs at O(1)
+    P_, _ = oracle.from_workload(p)
+    _, _, Kn, _ = P_.assemble(oracle.from_pg_material(p.mat, dev_pot=1), p.u, p.u_presc)
+    assert np.linalg.norm(Kn - Ko) > 0.05 * np.linalg.norm(Ko)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u, p.u_presc)
+    assert st.ok(), st.as_dict()
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    check_R(ctx.assemble_R(p.u, p.u_presc)[0], Ro)
+    ctx.set_scatter_mode(pg.SCATTER_COLOUR)
+    Rc, Kc, _ = ctx.assemble_RK(p.u, p.u_presc)
+    check_R(Rc, Ro)
+    check_K(Kc, Ko, p.Ap)
+    for mode in (pg.SCATTER_TILES, pg.SCATTER_CELLS):
+        with pytest.raises(pg.PgfemError):
+            ctx.set_scatter_mode(mode)
+    # element level: the dense element blocks assemble to the same K
+    elems = np.arange(p.conn.shape[0])
+    lk, fe, _ = ctx.stiffmatel_fd(elems, p.u, p.u_presc)
+    nd = nne * 3
+    Kd = np.zeros((p.ndof, p.ndof))
+    for e in elems:
+        idx = np.array([p.ids[p.conn[e, a], j] for a in range(nne) for j in range(3)])
+        m = idx > 0
+        Kd[np.ix_(idx[m] - 1, idx[m] - 1)] += lk[e].reshape(nd, nd)[np.ix_(m, m)]
+    rows = np.repeat(np.arange(p.ndof), np.diff(p.Ap))
+    assert np.abs(Kd[rows, p.Ai] - Ko).max() <= TOL * np.abs(Ko).max()
+    # constitutive level
+    F = np.eye(3)[None] + rng.uniform(-0.2, 0.2, (16, 3, 3))
+    S, L, _, q = pg.cm_integrate(p.mat, F.reshape(16, 9))
+    assert (q == 0).all()
+    om = oracle.from_pg_material(p.mat)
+    for i in range(16):
+        err, So, Lo, _, _ = oracle.cm_update(om, F[i])
+        assert err == 0
+        assert np.abs(S[i] - So.ravel()).max() <= TOL * np.abs(So).max()
+        assert np.abs(sym_L(L[i]) - sym_L(Lo)).max() <= TOL * np.abs(sym_L(Lo)).max()
