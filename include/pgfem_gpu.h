@@ -38,6 +38,7 @@ extern "C" {
 #define PGFEM_GPU_ENODEV (-5)   /* no usable sm_100 device */
 #define PGFEM_GPU_ELIMIT (-6)   /* size beyond a fixed limit of the entry point */
 #define PGFEM_GPU_ETIMEOUT (-7) /* a bounded device-side wait ran out (kernel returned early) */
+#define PGFEM_GPU_EFORMAT (-8)  /* input file missing or malformed (pgfem_input_last_error says where) */
 
 /* Constitutive models (the Model_parameters families on the path). */
 enum {
@@ -390,6 +391,101 @@ typedef struct {
  * on usage/CUDA errors; non-convergence is reported in info. */
 int pgfem_gpu_newton_step(pgfem_gpu_ctx *ctx, pgfem_gpu_solver *solver, double *d_u, const double *d_u_presc,
                           double dt, const pgfem_newton_opts *opts, pgfem_newton_info *info, void *stream);
+
+/* ---- input files (host only) ----------------------------------------------
+ * Readers of PGFem3D's own input files, so that the reference's inputs drive
+ * this library: mesh files <base><r>.in of read_input_file
+ * (src/read_input_file.cc:268-415, non-legacy formats), solver files
+ * (read_solver_file, :556-700), model_params.in (read_model_parameters_list,
+ * src/constitutive_model.cc:1171-1309) and crystal orientation files
+ * (plasticity_model_read_orientations, src/plasticity_model.cc:1260-1337).
+ * Errors: PGFEM_GPU_EFORMAT with a message from pgfem_input_last_error(). */
+const char *pgfem_input_last_error(void);
+
+typedef struct pgfem_input pgfem_input;
+typedef struct {
+  long nn, ne;          /* merged mesh */
+  int nne;              /* 4 or 10 (one element type per mesh) */
+  long npres;           /* prescribed values (support code -k takes defl[k-1]) */
+  int nmat;             /* material lines */
+  long nconc, norient;  /* material geometry sizes */
+  long lin_maxit;       /* header line 2: linear solver iterations, tolerance, zero */
+  double lin_err, lim_zero;
+  long nln, nel_s, nel_v; /* nodal / surface / volume load counts (not applied on this path) */
+} pgfem_input_info;
+
+/* Reads <base><r>.in for r = 0..nparts-1 and merges the partitions into one
+ * mesh: a partition-boundary node (Gnn >= 0) is one node whichever files list
+ * it, an interior node (Gnn = -1) belongs to its file; nodes are numbered in
+ * order of first appearance (partition, then local id), elements partition
+ * by partition.  Partitions must agree on shared nodes, supports, prescribed
+ * values and materials.  The supports come from the mesh files (not from a
+ * BC directory). */
+int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out);
+int pgfem_input_get_info(const pgfem_input *in, pgfem_input_info *info);
+/* X[nn*3], conn[ne*nne] (0-based merged ids), codes[nn*3] support codes
+ * (0 free, 1 fixed, -k prescribed: the pgfem_generate_dof_ids input),
+ * defl[npres]. */
+int pgfem_input_get_mesh(const pgfem_input *in, double *X, int *conn, long *codes, double *defl);
+/* Per element (each may be NULL): mat[ne*2], hom[ne*2] (matrix, fibre),
+ * partition and id within the partition. */
+int pgfem_input_get_elements(const pgfem_input *in, long *mat, long *hom, int *part, long *local_id);
+/* vals[nmat*13] = Ex Ey Ez Gyz Gxz Gxy nyz nxz nxy ax ay az sig, and the
+ * potential flags (devPotFlag, volPotFlag) per material. */
+int pgfem_input_get_materials(const pgfem_input *in, double *vals, int *dev_pot, int *vol_pot);
+/* Crystal orientations <base>_<r>.in (one per partition): angles[ne*3]
+ * (phi, theta, psi) per merged element, NAN where no line sets one; a line
+ * with a negative element id sets every element of material `ip` of its
+ * partition.  euler_type: the file's "# EulerAngleType: k" (0 if absent). */
+int pgfem_input_read_orientations(const pgfem_input *in, const char *base, double *angles, int *euler_type);
+void pgfem_input_destroy(pgfem_input *in);
+/* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
+ * composition the reference states at src/plasticity_model.cc:1252-1255; its
+ * rotation_matrix_of_Euler_angles lives in an absent library). */
+int pgfem_euler_rotation(long n, const double *angles, double *R);
+
+typedef struct {
+  double nor_min;        /* Newton tolerance */
+  long iter_max, npres, FNR;
+  double dAL0, dALMAX;   /* arc length (FNR 2, 3) */
+  int physicsno, max_NR_staggering, max_subdivision; /* FNR 4 */
+  long nt;               /* time steps: times[nt+1] */
+  long n_print;          /* output steps */
+  long n_load;           /* steps with a load increment */
+  long n_incr;           /* increments per load step (npd, or npres when npd < 0) */
+} pgfem_solver_file;
+/* Reads a solver file; arrays may be NULL (call once with NULL for the
+ * sizes): times[nt+1], print_steps[n_print], load_steps[n_load],
+ * load_incr[n_load*n_incr], the prescribed-value increments the reference
+ * reads while stepping, one per prescribed value of the mesh: pass the
+ * mesh's npres as npd (the header's npres is a different count). */
+int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *sf, double *times,
+                                 long *print_steps, long *load_steps, double *load_incr);
+
+/* model_type values of model_params.in (include/constitutive_model.h:42-54) */
+enum {
+  PGFEM_CM_HYPER_ELASTICITY = 0,
+  PGFEM_CM_CRYSTAL_PLASTICITY = 1,
+  PGFEM_CM_BPA_PLASTICITY = 2,
+  PGFEM_CM_ISO_VISCOUS_DAMAGE = 3,
+  PGFEM_CM_J2_PLASTICITY_DAMAGE = 4,
+  PGFEM_CM_UQCM = 100
+};
+typedef struct {
+  int mat_id, model_type, uq;
+  int np;                 /* parameters in p: CP 7 (gamma_dot_0 m G0 g0 gs_0 gamma_dot_s w);
+                             J2 14 (beta hp k0, mu w_max P1 P2 Yin, da db_p db_m va vb_p vb_m) */
+  double p[16];
+  int unit_cell;          /* CP slip system */
+  int ort_option[3];      /* CP orientation option (2: from files ort_file_<r>.in; 3: ort_angles) */
+  char ort_file[256];
+  double ort_angles[3];
+  int solver_set;         /* CP local solver block present */
+  int max_itr_stag, max_itr_hardening, max_itr_M, max_subdivision;
+  double tol_hardening, tol_M, computer_zero;
+} pgfem_model_params;
+/* Reads up to max_entries entries (n = entries in the file). */
+int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model_params *out, int *n);
 
 #ifdef __cplusplus
 }

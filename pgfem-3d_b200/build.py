@@ -18,7 +18,7 @@ OUT = os.path.join(HERE, "libpgfem_gpu.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 CU_SOURCES = ["pgfem_gpu.cu", "cp_kernels.cu", "mlp_kernels.cu", "rve_batch.cu", "solver.cu"]
-CXX_SOURCES = ["setup_host.cpp"]
+CXX_SOURCES = ["setup_host.cpp", "input_reader.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,589 @@
+// input_reader.cpp -- readers of PGFem3D's input files for the assembly path.
+//
+// Mesh files <base><r>.in (read_input_file, src/read_input_file.cc:268-415,
+// non-legacy formats: nodes src/node.cc:78-160, supports and prescribed
+// values src/in.cc:29-191, elements src/element.cc:168-199 and 256-330,
+// materials src/in.cc:195-223, material geometry and loads
+// src/in.cc:225-290), merged over partitions r = 0..P-1 into one mesh;
+// solver files <base><r>.in.st (read_solver_file / read_time_steps /
+// compute_times_load, src/read_input_file.cc:517-700, src/load.cc:29-60);
+// model_params.in (read_model_parameters_list, src/constitutive_model.cc:
+// 1171-1309, with the CP / J2 / HE parameter blocks of src/plasticity_model.cc:
+// 945-1040, src/cm_j2_plasticity.cc:865-900, src/plasticity_model_none.cc:293);
+// crystal orientation files <base>_<r>.in (plasticity_model_read_orientations,
+// src/plasticity_model.cc:1260-1337).
+//
+// Tokens are whitespace separated; a token that starts with '#' begins a
+// comment that runs to the end of its line (the effect of the reference's
+// scan_for_valid_line between fscanf calls); '{' and '}' are tokens of their
+// own.
+#include <algorithm>
+#include <cctype>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/pgfem_gpu.h"
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(const std::string &msg) {
+  g_err = msg;
+  return PGFEM_GPU_EFORMAT;
+}
+
+struct Tokens {
+  std::string s, path;
+  size_t i = 0;
+
+  bool load(const std::string &p) {
+    path = p;
+    FILE *f = fopen(p.c_str(), "rb");
+    if (!f) return false;
+    char buf[65536];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, n);
+    fclose(f);
+    return true;
+  }
+  void skip() {
+    for (;;) {
+      while (i < s.size() && isspace((unsigned char)s[i])) i++;
+      if (i < s.size() && s[i] == '#') {
+        while (i < s.size() && s[i] != '\n') i++;
+        continue;
+      }
+      return;
+    }
+  }
+  bool eof() {
+    skip();
+    return i >= s.size();
+  }
+  bool next(std::string &t) {
+    skip();
+    if (i >= s.size()) return false;
+    if (s[i] == '{' || s[i] == '}') {
+      t.assign(1, s[i++]);
+      return true;
+    }
+    const size_t b = i;
+    while (i < s.size() && !isspace((unsigned char)s[i]) && s[i] != '{' && s[i] != '}') i++;
+    t = s.substr(b, i - b);
+    return true;
+  }
+  bool num(double &v) {
+    std::string t;
+    if (!next(t)) return false;
+    char *end = nullptr;
+    v = strtod(t.c_str(), &end);
+    return end && *end == 0 && !t.empty();
+  }
+  bool num(long &v) {
+    std::string t;
+    if (!next(t)) return false;
+    char *end = nullptr;
+    v = strtol(t.c_str(), &end, 10);
+    return end && *end == 0 && !t.empty();
+  }
+  bool num(int &v) {
+    long l;
+    if (!num(l)) return false;
+    v = (int)l;
+    return true;
+  }
+  // peek whether the next token is an integer (without consuming it)
+  bool peek_int() {
+    const size_t keep = i;
+    long v;
+    const bool ok = num(v);
+    i = keep;
+    return ok;
+  }
+  std::string where() const {
+    const long line = 1 + (long)std::count(s.begin(), s.begin() + (long)std::min(i, s.size()), '\n');
+    return path + ":" + std::to_string(line);
+  }
+};
+
+}  // namespace
+
+struct pgfem_input {
+  pgfem_input_info info{};
+  std::vector<double> X;
+  std::vector<int> conn;
+  std::vector<long> codes, elem_mat, elem_hom, elem_local;
+  std::vector<int> elem_part;
+  std::vector<double> defl, mat_vals, cf, ee;
+  std::vector<int> dev_pot, vol_pot;
+  int nparts = 0;
+  std::vector<long> part_elem_off;  // merged element index of each partition's first element
+};
+
+namespace {
+
+struct Part {
+  long nn = 0, ndofn = 0, ne = 0, lin_maxit = 0, nmat = 0, nconc = 0, norient = 0;
+  double lin_err = 0, lim_zero = 0;
+  std::vector<long> toe, gnn, dom;
+  std::vector<double> X;
+  std::vector<long> codes;
+  std::vector<double> defl;
+  std::vector<long> conn, emat, ehom;
+  std::vector<double> mats, cf, ee;
+  std::vector<int> devp, volp;
+  long nln = 0, nel_s = 0, nel_v = 0;
+};
+
+int read_part(const std::string &path, Part &p) {
+  Tokens t;
+  if (!t.load(path)) return fail("cannot open " + path);
+  auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
+  if (!t.num(p.nn) || !t.num(p.ndofn) || !t.num(p.ne)) return bad("header (nn ndofn ne)");
+  if (!t.num(p.lin_maxit) || !t.num(p.lin_err) || !t.num(p.lim_zero)) return bad("solver header");
+  if (!t.num(p.nmat) || !t.num(p.nconc) || !t.num(p.norient)) return bad("material header");
+  if (p.nn <= 0 || p.ne < 0 || p.nmat < 0 || p.nconc < 0 || p.norient < 0) return bad("header sizes");
+  if (p.ndofn != 3) return fail(path + ": ndofn " + std::to_string(p.ndofn) + " (the mechanical path has 3)");
+  p.toe.resize(p.ne);
+  for (long e = 0; e < p.ne; e++)
+    if (!t.num(p.toe[e])) return bad("element type line");
+  // nodes: Gnn Dom id x y z model_type model_id pr
+  p.gnn.assign(p.nn, -2);
+  p.dom.assign(p.nn, 0);
+  p.X.assign(3 * p.nn, 0.0);
+  for (long k = 0; k < p.nn; k++) {
+    long g, d, id, mt, mid, pr;
+    double x[3];
+    if (!t.num(g) || !t.num(d) || !t.num(id) || !t.num(x[0]) || !t.num(x[1]) || !t.num(x[2]) || !t.num(mt) ||
+        !t.num(mid) || !t.num(pr))
+      return bad("node line");
+    if (id < 0 || id >= p.nn || p.gnn[id] != -2) return bad("node id");
+    p.gnn[id] = g;
+    p.dom[id] = d;
+    for (int j = 0; j < 3; j++) p.X[3 * id + j] = x[j];
+  }
+  // supports and prescribed values
+  long nsup;
+  if (!t.num(nsup) || nsup < 0) return bad("support count");
+  p.codes.assign(3 * p.nn, 0);
+  for (long k = 0; k < nsup; k++) {
+    long n;
+    if (!t.num(n) || n < 0 || n >= p.nn) return bad("support node");
+    for (int j = 0; j < 3; j++)
+      if (!t.num(p.codes[3 * n + j])) return bad("support code");
+  }
+  long npd;
+  if (!t.num(npd) || npd < 0) return bad("prescribed count");
+  p.defl.resize(npd);
+  for (long k = 0; k < npd; k++)
+    if (!t.num(p.defl[k])) return bad("prescribed value");
+  for (long n = 0; n < p.nn; n++)
+    for (int j = 0; j < 3; j++) {
+      const long c = p.codes[3 * n + j];
+      if (c < -npd || c > 1) return bad("support code range");
+    }
+  // elements: id nodes[toe] ftype fid pr bnd_id[4] bnd_type[4]
+  long nne = p.ne ? p.toe[0] : 0;
+  for (long e = 0; e < p.ne; e++)
+    if (p.toe[e] != nne) return fail(path + ": mixed element types (one type per mesh on this path)");
+  if (p.ne && nne != 4 && nne != 10)
+    return fail(path + ": element type " + std::to_string(nne) + " (linear or quadratic tets on this path)");
+  p.conn.assign(p.ne * nne, -1);
+  std::vector<char> seen(p.ne, 0);
+  for (long k = 0; k < p.ne; k++) {
+    long id;
+    if (!t.num(id) || id < 0 || id >= p.ne || seen[id]) return bad("element id");
+    seen[id] = 1;
+    for (long a = 0; a < nne; a++) {
+      long n;
+      if (!t.num(n) || n < 0 || n >= p.nn) return bad("element node");
+      p.conn[id * nne + a] = n;
+    }
+    for (int k2 = 0; k2 < 11; k2++) {
+      long v;
+      if (!t.num(v)) return bad("element face data");
+    }
+  }
+  // element materials: id mat[2] hom[2]
+  p.emat.assign(2 * p.ne, 0);
+  p.ehom.assign(2 * p.ne, 0);
+  for (long k = 0; k < p.ne; k++) {
+    long id;
+    if (!t.num(id) || id < 0 || id >= p.ne) return bad("element material id");
+    if (!t.num(p.emat[2 * id]) || !t.num(p.emat[2 * id + 1]) || !t.num(p.ehom[2 * id]) ||
+        !t.num(p.ehom[2 * id + 1]))
+      return bad("element material");
+    if (p.emat[2 * id] < 0 || p.emat[2 * id] >= std::max(1L, p.nmat)) return bad("element material index");
+  }
+  // materials: Ex Ey Ez Gyz Gxz Gxy nyz nxz nxy ax ay az sig devPotFlag volPotFlag
+  p.mats.assign(13 * p.nmat, 0.0);
+  p.devp.assign(p.nmat, 0);
+  p.volp.assign(p.nmat, 0);
+  for (long m = 0; m < p.nmat; m++) {
+    for (int j = 0; j < 13; j++)
+      if (!t.num(p.mats[13 * m + j])) return bad("material line");
+    if (!t.num(p.devp[m]) || !t.num(p.volp[m])) return bad("material potential flags");
+  }
+  // material geometry
+  p.cf.assign(p.nconc, 0.0);
+  for (long k = 0; k < p.nconc; k++)
+    if (!t.num(p.cf[k])) return bad("concentration");
+  p.ee.assign(9 * p.norient, 0.0);
+  for (long k = 0; k < 9 * p.norient; k++)
+    if (!t.num(p.ee[k])) return bad("orientation");
+  {
+    long SH;
+    double a1, a2;
+    if (!t.num(SH) || !t.num(a1) || !t.num(a2)) return bad("material geometry (SH a1 a2)");
+  }
+  // loads: counted and stepped over (nodal and element loads are not on this path)
+  if (!t.num(p.nln) || p.nln < 0) return bad("nodal load count");
+  for (long k = 0; k < p.nln; k++) {
+    double v;
+    for (int j = 0; j < 4; j++)
+      if (!t.num(v)) return bad("nodal load");
+  }
+  if (!t.num(p.nel_s) || p.nel_s < 0) return bad("surface load count");
+  const int nsur = nne == 10 ? 6 : 3;
+  for (long k = 0; k < p.nel_s; k++) {
+    double v;
+    for (int j = 0; j < 1 + nsur + 3; j++)
+      if (!t.num(v)) return bad("surface load");
+  }
+  if (!t.num(p.nel_v) || p.nel_v < 0) return bad("volume load count");
+  return PGFEM_GPU_OK;
+}
+
+bool close(double a, double b) { return std::fabs(a - b) <= 1e-12 * std::max(1.0, std::max(std::fabs(a), std::fabs(b))); }
+
+}  // namespace
+
+extern "C" {
+
+const char *pgfem_input_last_error(void) { return g_err.c_str(); }
+
+int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
+  if (!base || nparts < 1 || !out) return PGFEM_GPU_EINVAL;
+  *out = nullptr;
+  std::vector<Part> parts(nparts);
+  for (int r = 0; r < nparts; r++) {
+    const int e = read_part(std::string(base) + std::to_string(r) + ".in", parts[r]);
+    if (e) return e;
+  }
+  auto *in = new pgfem_input();
+  in->nparts = nparts;
+  const Part &p0 = parts[0];
+  pgfem_input_info &I = in->info;
+  I.nne = 0;
+  for (const Part &p : parts)
+    if (p.ne) {
+      I.nne = (int)p.toe[0];
+      break;
+    }
+  I.npres = (long)p0.defl.size();
+  I.nmat = (int)p0.nmat;
+  I.nconc = p0.nconc;
+  I.norient = p0.norient;
+  I.lin_maxit = p0.lin_maxit;
+  I.lin_err = p0.lin_err;
+  I.lim_zero = p0.lim_zero;
+  auto reject = [&](const std::string &m) {
+    delete in;
+    return fail(m);
+  };
+  // merged node numbering: partition-boundary nodes (Gnn >= 0) by Gnn,
+  // interior nodes (Gnn = -1) per partition; first appearance order
+  std::map<long, long> gmap;
+  std::vector<std::vector<long>> lmap(nparts);
+  for (int r = 0; r < nparts; r++) {
+    const Part &p = parts[r];
+    if (p.ne && p.toe[0] != I.nne) return reject("partitions with different element types");
+    if ((long)p.defl.size() != I.npres) return reject("partitions with different prescribed value counts");
+    for (long k = 0; k < I.npres; k++)
+      if (!close(p.defl[k], p0.defl[k])) return reject("partitions with different prescribed values");
+    if (p.nmat != p0.nmat) return reject("partitions with different material counts");
+    for (size_t k = 0; k < p.mats.size(); k++)
+      if (!close(p.mats[k], p0.mats[k])) return reject("partitions with different materials");
+    for (long m = 0; m < p.nmat; m++)
+      if (p.devp[m] != p0.devp[m] || p.volp[m] != p0.volp[m]) return reject("partitions with different materials");
+    lmap[r].assign(p.nn, -1);
+    for (long n = 0; n < p.nn; n++) {
+      long id;
+      bool fresh = true;
+      if (p.gnn[n] >= 0) {
+        auto it = gmap.find(p.gnn[n]);
+        if (it != gmap.end()) {
+          id = it->second;
+          fresh = false;
+        } else {
+          id = (long)in->X.size() / 3;
+          gmap[p.gnn[n]] = id;
+        }
+      } else {
+        id = (long)in->X.size() / 3;
+      }
+      lmap[r][n] = id;
+      if (fresh) {
+        for (int j = 0; j < 3; j++) {
+          in->X.push_back(p.X[3 * n + j]);
+          in->codes.push_back(p.codes[3 * n + j]);
+        }
+      } else {
+        for (int j = 0; j < 3; j++) {
+          if (!close(in->X[3 * id + j], p.X[3 * n + j]))
+            return reject("partition-boundary node " + std::to_string(p.gnn[n]) + " with different coordinates");
+          long &c = in->codes[3 * id + j];
+          if (c == 0) c = p.codes[3 * n + j];
+          else if (p.codes[3 * n + j] != 0 && p.codes[3 * n + j] != c)
+            return reject("partition-boundary node " + std::to_string(p.gnn[n]) + " with different supports");
+        }
+      }
+    }
+  }
+  I.nn = (long)in->X.size() / 3;
+  in->part_elem_off.assign(nparts + 1, 0);
+  for (int r = 0; r < nparts; r++) {
+    const Part &p = parts[r];
+    in->part_elem_off[r + 1] = in->part_elem_off[r] + p.ne;
+    for (long e = 0; e < p.ne; e++) {
+      for (int a = 0; a < I.nne; a++) in->conn.push_back((int)lmap[r][p.conn[e * I.nne + a]]);
+      in->elem_mat.push_back(p.emat[2 * e]);
+      in->elem_mat.push_back(p.emat[2 * e + 1]);
+      in->elem_hom.push_back(p.ehom[2 * e]);
+      in->elem_hom.push_back(p.ehom[2 * e + 1]);
+      in->elem_part.push_back(r);
+      in->elem_local.push_back(e);
+    }
+    I.nln += p.nln;
+    I.nel_s += p.nel_s;
+    I.nel_v += p.nel_v;
+  }
+  I.ne = in->part_elem_off[nparts];
+  in->defl = p0.defl;
+  in->mat_vals = p0.mats;
+  in->dev_pot = p0.devp;
+  in->vol_pot = p0.volp;
+  in->cf = p0.cf;
+  in->ee = p0.ee;
+  *out = in;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_info(const pgfem_input *in, pgfem_input_info *info) {
+  if (!in || !info) return PGFEM_GPU_EINVAL;
+  *info = in->info;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_mesh(const pgfem_input *in, double *X, int *conn, long *codes, double *defl) {
+  if (!in || !X || !conn || !codes || (in->info.npres && !defl)) return PGFEM_GPU_EINVAL;
+  memcpy(X, in->X.data(), sizeof(double) * in->X.size());
+  memcpy(conn, in->conn.data(), sizeof(int) * in->conn.size());
+  memcpy(codes, in->codes.data(), sizeof(long) * in->codes.size());
+  if (in->info.npres) memcpy(defl, in->defl.data(), sizeof(double) * in->defl.size());
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_elements(const pgfem_input *in, long *mat, long *hom, int *part, long *local_id) {
+  if (!in) return PGFEM_GPU_EINVAL;
+  const size_t ne = (size_t)in->info.ne;
+  if (mat) memcpy(mat, in->elem_mat.data(), sizeof(long) * 2 * ne);
+  if (hom) memcpy(hom, in->elem_hom.data(), sizeof(long) * 2 * ne);
+  if (part) memcpy(part, in->elem_part.data(), sizeof(int) * ne);
+  if (local_id) memcpy(local_id, in->elem_local.data(), sizeof(long) * ne);
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_materials(const pgfem_input *in, double *vals, int *dev_pot, int *vol_pot) {
+  if (!in || (in->info.nmat && (!vals || !dev_pot || !vol_pot))) return PGFEM_GPU_EINVAL;
+  if (!in->info.nmat) return PGFEM_GPU_OK;
+  memcpy(vals, in->mat_vals.data(), sizeof(double) * in->mat_vals.size());
+  memcpy(dev_pot, in->dev_pot.data(), sizeof(int) * in->dev_pot.size());
+  memcpy(vol_pot, in->vol_pot.data(), sizeof(int) * in->vol_pot.size());
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_read_orientations(const pgfem_input *in, const char *base, double *angles, int *euler_type) {
+  if (!in || !base || !angles) return PGFEM_GPU_EINVAL;
+  const long ne = in->info.ne;
+  for (long k = 0; k < 3 * ne; k++) angles[k] = NAN;
+  int etype = 0;
+  for (int r = 0; r < in->nparts; r++) {
+    const std::string path = std::string(base) + "_" + std::to_string(r) + ".in";
+    FILE *f = fopen(path.c_str(), "r");
+    if (!f) return fail("cannot open " + path);
+    const long e0 = in->part_elem_off[r], npe = in->part_elem_off[r + 1] - e0;
+    char line[1024];
+    long lineno = 0;
+    while (fgets(line, sizeof line, f)) {
+      lineno++;
+      if (line[0] == '#') {  // "# EulerAngleType: k"
+        const char *key = strstr(line, "EulerAngleType:");
+        if (key) etype = atoi(key + strlen("EulerAngleType:"));
+        continue;
+      }
+      long e, ip;
+      double a[3];
+      const int got = sscanf(line, "%ld %ld %lf %lf %lf", &e, &ip, a, a + 1, a + 2);
+      if (got <= 0) continue;  // blank line
+      if (got != 5) {
+        fclose(f);
+        return fail(path + ":" + std::to_string(lineno) + ": bad orientation line");
+      }
+      if (e < 0) {  // every element of material `ip` of this partition
+        for (long k = 0; k < npe; k++)
+          if (in->elem_mat[2 * (e0 + k)] == ip)
+            for (int j = 0; j < 3; j++) angles[3 * (e0 + k) + j] = a[j];
+      } else {
+        if (e >= npe || ip != 0) {  // one integration point per linear tet
+          fclose(f);
+          return fail(path + ":" + std::to_string(lineno) + ": element or point out of range");
+        }
+        for (int j = 0; j < 3; j++) angles[3 * (e0 + e) + j] = a[j];
+      }
+    }
+    fclose(f);
+  }
+  if (euler_type) *euler_type = etype;
+  return PGFEM_GPU_OK;
+}
+
+void pgfem_input_destroy(pgfem_input *in) { delete in; }
+
+int pgfem_euler_rotation(long n, const double *angles, double *R) {
+  if (n < 0 || (n && (!angles || !R))) return PGFEM_GPU_EINVAL;
+  for (long k = 0; k < n; k++) {
+    const double ph = angles[3 * k], th = angles[3 * k + 1], ps = angles[3 * k + 2];
+    const double cx = cos(ph), sx = sin(ph), cy = cos(th), sy = sin(th), cz = cos(ps), sz = sin(ps);
+    const double Ax[9] = {1, 0, 0, 0, cx, -sx, 0, sx, cx};
+    const double Ay[9] = {cy, 0, sy, 0, 1, 0, -sy, 0, cy};
+    const double Az[9] = {cz, -sz, 0, sz, cz, 0, 0, 0, 1};
+    double T[9];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        T[i * 3 + j] = Ay[i * 3] * Ax[j] + Ay[i * 3 + 1] * Ax[3 + j] + Ay[i * 3 + 2] * Ax[6 + j];
+    double *Rk = R + 9 * k;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++)
+        Rk[i * 3 + j] = Az[i * 3] * T[j] + Az[i * 3 + 1] * T[3 + j] + Az[i * 3 + 2] * T[6 + j];
+  }
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *sf, double *times,
+                                 long *print_steps, long *load_steps, double *load_incr) {
+  if (!path || !sf) return PGFEM_GPU_EINVAL;
+  Tokens t;
+  if (!t.load(path)) return fail(std::string("cannot open ") + path);
+  auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
+  pgfem_solver_file s{};
+  if (!t.num(s.nor_min) || !t.num(s.iter_max) || !t.num(s.npres) || !t.num(s.FNR)) return bad("solver line");
+  if (s.FNR == 2 || s.FNR == 3)
+    if (!t.num(s.dAL0) || !t.num(s.dALMAX)) return bad("arc-length line");
+  if (s.FNR == 4) {
+    if (!t.num(s.physicsno) || !t.num(s.max_NR_staggering) || s.physicsno < 1) return bad("multiphysics line");
+    for (int k = 0; k < s.physicsno; k++) {
+      int sub, setr;
+      if (!t.num(sub) || !t.num(setr)) return bad("per-physics solver line");
+      if (k == 0) s.max_subdivision = sub;
+      if (setr) {
+        double du;
+        if (!t.num(du)) return bad("initial residual scale");
+      }
+    }
+  }
+  if (!t.num(s.nt) || s.nt < 0) return bad("time step count");
+  for (long k = 0; k <= s.nt; k++) {
+    double v;
+    if (!t.num(v)) return bad("time");
+    if (times) times[k] = v;
+  }
+  if (!t.num(s.n_print) || s.n_print < 0) return bad("output step count");
+  for (long k = 0; k < s.n_print; k++) {
+    long v;
+    if (!t.num(v)) return bad("output step");
+    if (print_steps) print_steps[k] = v;
+  }
+  if (!t.num(s.n_load) || s.n_load < 0) return bad("load step count");
+  for (long k = 0; k < s.n_load; k++) {
+    long v;
+    if (!t.num(v)) return bad("load step");
+    if (load_steps) load_steps[k] = v;
+  }
+  // prescribed-value increments, one per prescribed value of the mesh per
+  // load step (the reference reads them while stepping; all of them here)
+  s.n_incr = npd >= 0 ? npd : s.npres;
+  for (long k = 0; k < s.n_load * s.n_incr; k++) {
+    double v;
+    if (!t.num(v)) return bad("load increment");
+    if (load_incr) load_incr[k] = v;
+  }
+  *sf = s;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model_params *out, int *n) {
+  if (!path || !n || max_entries < 0 || (max_entries && !out)) return PGFEM_GPU_EINVAL;
+  Tokens t;
+  if (!t.load(path)) return fail(std::string("cannot open ") + path);
+  auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
+  int count;
+  if (!t.num(count) || count < 0) return bad("entry count");
+  int k = 0;
+  for (; k < count; k++) {
+    pgfem_model_params m{};
+    std::string tok;
+    if (!t.num(m.mat_id) || !t.num(m.model_type)) return bad("entry header (mat_id model_type)");
+    if (!t.next(tok) || tok != "{") return bad("opening brace");
+    if (m.model_type == PGFEM_CM_UQCM) {
+      if (!t.num(m.model_type)) return bad("UQ model type");
+      m.uq = 1;
+    }
+    if (m.mat_id >= 0 && m.model_type == PGFEM_CM_CRYSTAL_PLASTICITY) {
+      // gamma_dot_0 m G0 g0 gs_0 gamma_dot_s w; unit cell; orientation option (+ its data)
+      for (int j = 0; j < 7; j++)
+        if (!t.num(m.p[j])) return bad("crystal plasticity parameters");
+      m.np = 7;
+      if (!t.num(m.unit_cell) || !t.num(m.ort_option[0])) return bad("slip system / orientation option");
+      if (m.ort_option[0] == 0 && !t.num(m.ort_option[1])) return bad("orientation option");
+      if (m.ort_option[0] == 2) {
+        std::string f;
+        if (!t.next(f) || f == "}" || f.size() >= sizeof(m.ort_file)) return bad("orientation file");
+        strcpy(m.ort_file, f.c_str());
+      }
+      if (m.ort_option[0] == 3)
+        for (int j = 0; j < 3; j++)
+          if (!t.num(m.ort_angles[j])) return bad("orientation angles");
+      if (t.peek_int()) {
+        int set;
+        t.num(set);
+        if (set) {
+          m.solver_set = 1;
+          if (!t.num(m.max_itr_stag) || !t.num(m.max_itr_hardening) || !t.num(m.max_itr_M) ||
+              !t.num(m.max_subdivision) || !t.num(m.tol_hardening) || !t.num(m.tol_M) || !t.num(m.computer_zero))
+            return bad("crystal plasticity solver parameters");
+        }
+      }
+    } else if (m.mat_id >= 0 && m.model_type == PGFEM_CM_J2_PLASTICITY_DAMAGE) {
+      // beta hp k0; damage mu w_max P1 P2 Yin; da db_p db_m va vb_p vb_m
+      for (int j = 0; j < 14; j++)
+        if (!t.num(m.p[j])) return bad("J2 plasticity parameters");
+      m.np = 14;
+    }
+    // the rest of the block (other models, or data this path does not use)
+    while (t.next(tok) && tok != "}") {
+    }
+    if (tok != "}") return bad("closing brace");
+    if (k < max_entries) out[k] = m;
+  }
+  *n = k;
+  return PGFEM_GPU_OK;
+}
+
+}  // extern "C"

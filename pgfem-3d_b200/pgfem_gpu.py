@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(HERE, "libpgfem_gpu.so")
 MODEL_HE, MODEL_J2, MODEL_CP = 0, 1, 2
 SCATTER_ATOMIC, SCATTER_COLOUR, SCATTER_TILES, SCATTER_CELLS = 0, 1, 2, 3
 
-ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT", -7: "ETIMEOUT"}
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT", -7: "ETIMEOUT",
+          -8: "EFORMAT"}
 
 
 class PgfemError(RuntimeError):
@@ -120,6 +121,17 @@ def lib():
             "pgfem_gpu_spmv": (C.c_int, [_P, _P, _P, _P, _P]),
             "pgfem_gpu_solve": (C.c_int, [_P, _P, _P, _P, _P, _P]),
             "pgfem_gpu_newton_step": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P]),
+            "pgfem_input_last_error": (C.c_char_p, []),
+            "pgfem_input_read_mesh": (C.c_int, [C.c_char_p, C.c_int, _P]),
+            "pgfem_input_get_info": (C.c_int, [_P, _P]),
+            "pgfem_input_get_mesh": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_input_get_elements": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_input_get_materials": (C.c_int, [_P, _P, _P, _P]),
+            "pgfem_input_read_orientations": (C.c_int, [_P, C.c_char_p, _P, _P]),
+            "pgfem_input_destroy": (None, [_P]),
+            "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
+            "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
+            "pgfem_input_read_model_params": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -579,3 +591,141 @@ class Solver:
         _check("pgfem_gpu_newton_step", lib().pgfem_gpu_newton_step(ctx.h, self.h, d_u, d_presc, dt, C.byref(o),
                                                                     C.byref(info), stream))
         return info
+
+
+# ------------------------------------------------------------ input files ----
+class InputInfo(C.Structure):
+    _fields_ = [("nn", C.c_long), ("ne", C.c_long), ("nne", C.c_int), ("npres", C.c_long), ("nmat", C.c_int),
+                ("nconc", C.c_long), ("norient", C.c_long), ("lin_maxit", C.c_long), ("lin_err", C.c_double),
+                ("lim_zero", C.c_double), ("nln", C.c_long), ("nel_s", C.c_long), ("nel_v", C.c_long)]
+
+
+class SolverFile(C.Structure):
+    _fields_ = [("nor_min", C.c_double), ("iter_max", C.c_long), ("npres", C.c_long), ("FNR", C.c_long),
+                ("dAL0", C.c_double), ("dALMAX", C.c_double), ("physicsno", C.c_int),
+                ("max_NR_staggering", C.c_int), ("max_subdivision", C.c_int), ("nt", C.c_long),
+                ("n_print", C.c_long), ("n_load", C.c_long), ("n_incr", C.c_long)]
+
+
+class ModelParams(C.Structure):
+    _fields_ = [("mat_id", C.c_int), ("model_type", C.c_int), ("uq", C.c_int), ("np", C.c_int),
+                ("p", C.c_double * 16), ("unit_cell", C.c_int), ("ort_option", C.c_int * 3),
+                ("ort_file", C.c_char * 256), ("ort_angles", C.c_double * 3), ("solver_set", C.c_int),
+                ("max_itr_stag", C.c_int), ("max_itr_hardening", C.c_int), ("max_itr_M", C.c_int),
+                ("max_subdivision", C.c_int), ("tol_hardening", C.c_double), ("tol_M", C.c_double),
+                ("computer_zero", C.c_double)]
+
+
+CM_HYPER_ELASTICITY, CM_CRYSTAL_PLASTICITY, CM_J2_PLASTICITY_DAMAGE = 0, 1, 4
+
+
+def _check_input(fn, r):
+    if r < 0:
+        e = PgfemError(fn, r)
+        e.args = (e.args[0] + ": " + lib().pgfem_input_last_error().decode(),)
+        raise e
+    return r
+
+
+class InputMesh:
+    """A PGFem3D mesh read from its <base><r>.in files (pgfem_input_read_mesh),
+    partitions merged: X (nn,3), conn (ne,nne), codes (nn,3) support codes,
+    defl (npres,), per-element material / partition data, material lines."""
+
+    def __init__(self, base, nparts=1):
+        h = C.c_void_p()
+        _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh(base.encode(), nparts, C.byref(h)))
+        try:
+            info = InputInfo()
+            _check("pgfem_input_get_info", lib().pgfem_input_get_info(h, C.byref(info)))
+            self.info = info
+            nn, ne, nne = info.nn, info.ne, info.nne
+            self.X = np.zeros((nn, 3))
+            self.conn = np.zeros((ne, nne), dtype=np.int32)
+            self.codes = np.zeros((nn, 3), dtype=np.int64)
+            self.defl = np.zeros(info.npres)
+            _check("pgfem_input_get_mesh", lib().pgfem_input_get_mesh(h, _ptr(self.X), _ptr(self.conn),
+                                                                      _ptr(self.codes), _ptr(self.defl)))
+            self.elem_mat = np.zeros((ne, 2), dtype=np.int64)
+            self.elem_hom = np.zeros((ne, 2), dtype=np.int64)
+            self.elem_part = np.zeros(ne, dtype=np.int32)
+            self.elem_local = np.zeros(ne, dtype=np.int64)
+            _check("pgfem_input_get_elements", lib().pgfem_input_get_elements(
+                h, _ptr(self.elem_mat), _ptr(self.elem_hom), _ptr(self.elem_part), _ptr(self.elem_local)))
+            self.materials = np.zeros((info.nmat, 13))
+            self.dev_pot = np.zeros(info.nmat, dtype=np.int32)
+            self.vol_pot = np.zeros(info.nmat, dtype=np.int32)
+            _check("pgfem_input_get_materials", lib().pgfem_input_get_materials(
+                h, _ptr(self.materials), _ptr(self.dev_pot), _ptr(self.vol_pot)))
+            self._h = h
+        except Exception:
+            lib().pgfem_input_destroy(h)
+            raise
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pgfem_input_destroy(self._h)
+            self._h = None
+
+    def orientations(self, base):
+        """(angles (ne,3), EulerAngleType) from <base>_<r>.in."""
+        a = np.zeros((self.info.ne, 3))
+        et = C.c_int()
+        _check_input("pgfem_input_read_orientations",
+                     lib().pgfem_input_read_orientations(self._h, base.encode(), _ptr(a), C.byref(et)))
+        return a, et.value
+
+    def material(self, imat=0, model=MODEL_HE, **kw):
+        """pgfem_material_desc from material line imat: E = Ex, nu = nyz (the
+        isotropic entries), dev_pot = devPotFlag for HE; keywords add or
+        override fields (J2 / CP parameters)."""
+        m = self.materials[imat]
+        args = dict(E=m[0], nu=m[6])
+        if model == MODEL_HE:
+            args["dev_pot"] = int(self.dev_pot[imat])
+        args.update(kw)
+        return material(model, **args)
+
+    def dof_setup(self):
+        """(ids, ndof, Ap, Ai) of the merged mesh (generate_dof_ids + Psparse_ApAi)."""
+        ids, ndof = generate_dof_ids(self.conn, self.X.shape[0], self.codes)
+        Ap, Ai = psparse_apai(self.conn, ids, ndof)
+        return ids, ndof, Ap, Ai
+
+
+def read_solver_file(path, npd=-1):
+    """Returns (SolverFile, times, print_steps, load_steps, load_incr (n_load, n_incr));
+    npd = the mesh's prescribed-value count (InputMesh.info.npres)."""
+    sf = SolverFile()
+    _check_input("pgfem_input_read_solver_file",
+                 lib().pgfem_input_read_solver_file(path.encode(), npd, C.byref(sf), None, None, None, None))
+    times = np.zeros(sf.nt + 1)
+    ps = np.zeros(sf.n_print, dtype=np.int64)
+    ls = np.zeros(sf.n_load, dtype=np.int64)
+    li = np.zeros((sf.n_load, sf.n_incr))
+    _check_input("pgfem_input_read_solver_file", lib().pgfem_input_read_solver_file(
+        path.encode(), npd, C.byref(sf), _ptr(times), _ptr(ps), _ptr(ls), _ptr(li)))
+    return sf, times, ps, ls, li
+
+
+def read_model_params(path, max_entries=64):
+    out = (ModelParams * max_entries)()
+    n = C.c_int()
+    _check_input("pgfem_input_read_model_params",
+                 lib().pgfem_input_read_model_params(path.encode(), max_entries, out, C.byref(n)))
+    return [out[i] for i in range(min(n.value, max_entries))]
+
+
+def cp_material(mp, E, nu, cp_tol=1e-10, cp_max_iter=25):
+    """pgfem_material_desc of a crystal plasticity model_params entry."""
+    assert mp.model_type == CM_CRYSTAL_PLASTICITY and mp.np == 7
+    p = list(mp.p)[:7]
+    return material(MODEL_CP, E=E, nu=nu, gamma_dot_0=p[0], m=p[1], G0=p[2], g0=p[3], gs_0=p[4],
+                    gamma_dot_s=p[5], w=p[6], cp_tol=cp_tol, cp_max_iter=cp_max_iter)
+
+
+def euler_rotation(angles):
+    a = np.ascontiguousarray(angles, dtype=np.float64).reshape(-1, 3)
+    R = np.zeros((a.shape[0], 3, 3))
+    _check("pgfem_euler_rotation", lib().pgfem_euler_rotation(a.shape[0], _ptr(a), _ptr(R)))
+    return R
