@@ -462,6 +462,37 @@ typedef struct {
 int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *sf, double *times,
                                  long *print_steps, long *load_steps, double *load_incr);
 
+/* ---- restart files --------------------------------------------------------
+ * One rank's restart file in the reference's layout (write_restart_constitutive_model /
+ * read_restart_constitutive_model, src/restart.cc:187-300): per node the pairs
+ * "u_nm1 u_n" of x, y, z (total displacements, prescribed values included),
+ * then per element its point count and per point the model block of
+ * write_restart: HE (src/plasticity_model_none.cc:298-311) Fn, Fnm1 = 18
+ * doubles; CP (src/plasticity_model.cc:883-942) Fn, Fnm1, pFn, pFnm1,
+ * tau_n[12], gamma_dot_n[12], g_n, g_nm1, L_n, L_nm1 = 64 doubles.  J2 has no
+ * restart here: the reference's J2 block carries damage variables of a model
+ * this path does not carry.  File name convention of the reference:
+ * <dir>/STEP_<step %06d>/<name>_<rank>_<step>.res. */
+int pgfem_restart_block_size(int model);
+/* Host-only formatting / parsing: u_nm1, u_n nodal AoS (nn*3), blocks
+ * (ne*n_ip*block_size).  The parser rejects a file whose node, element or
+ * point counts do not match (EFORMAT). */
+int pgfem_restart_format(const char *path, long nn, long ne, int n_ip, int model, const double *u_nm1,
+                         const double *u_n, const double *blocks);
+int pgfem_restart_parse(const char *path, long nn, long ne, int n_ip, int model, double *u_nm1, double *u_n,
+                        double *blocks);
+/* Context level.  Write: u_nm1, u_n free-DOF displacements at t_{n-1}, t_n
+ * with their prescribed values; F per point is computed from them on the
+ * device; CP pFn, g_n from the committed state (t_n) and pFnm1, g_nm1 from
+ * state_nm1 (host AoS nqp*10 as pgfem_gpu_get_state, the state before the
+ * last commit; NULL = the state at t_n); tau_n, gamma_dot_n, L_n, L_nm1 are
+ * not carried by this path and are written as 0.  Read: returns the free-DOF
+ * displacements u_nm1, u_n (the caller's vectors) and, for CP, sets the state
+ * at t_n (pFn, g_n) and F at t_n from the file; the other fields are not used. */
+int pgfem_gpu_write_restart(pgfem_gpu_ctx *ctx, const char *path, const double *u_nm1, const double *u_n,
+                            const double *presc_nm1, const double *presc_n, const double *state_nm1);
+int pgfem_gpu_read_restart(pgfem_gpu_ctx *ctx, const char *path, double *u_nm1, double *u_n);
+
 /* model_type values of model_params.in (include/constitutive_model.h:42-54) */
 enum {
   PGFEM_CM_HYPER_ELASTICITY = 0,

@@ -5,8 +5,10 @@
 // src/integration.cc:378-423): FCC {111}<110> slip, resolved shear
 // tau_a = s_a . (Ce S) n_a, gamma_dot_a = gamma_dot_0 sgn(tau_a)|tau_a/g|^(1/m),
 // M = pF_n pF_{n+1}^-1 = I - dt sum gamma_dot_a P_a, saturation hardening
-// g - g_n - dt G0 gamma_dot (gs - g)/(gs - g0) = 0 (w = 0), neo-Hookean +
-// U_Common elasticity at Ce = M^T Ce' M.  The local problem in x = (M, g) is
+// g - g_n - dt G0 gamma_dot (gs - g)/(gs - g0) = 0 with the rate-dependent
+// saturation stress gs = gs_0 (gamma_dot / gamma_dot_s)^w (src/integration.cc:
+// 394-402; gs = gs_0 for w = 0), neo-Hookean + U_Common elasticity at
+// Ce = M^T Ce' M.  The local problem in x = (M, g) is
 // solved by Newton with backtracking from the elastic predictor or from a
 // supplied initial guess; at convergence the consistent dM/dF is formed.
 //
@@ -130,6 +132,20 @@ struct CpPoint {
   double g_n, dt;
 };
 
+// Saturation stress gs(gamma_dot) and dRg = d R_g / d gamma_dot (through gs as
+// well): -dt G0 [(gs - g)/(gs - g0) + w gs (g - g0)/(gs - g0)^2].
+struct CpHard {
+  double gs, dRg;
+};
+__device__ __forceinline__ CpHard cp_hardening(const Mat &mat, double gdot, double g, double dt) {
+  CpHard h;
+  const bool rate = mat.w > 0.0 && gdot > 0.0;
+  h.gs = rate ? mat.gs0 * pow(gdot / mat.gdots, mat.w) : mat.gs0;
+  const double d = h.gs - mat.g0;
+  h.dRg = -dt * mat.G0 * ((h.gs - g) / d + (rate ? mat.w * h.gs * (g - mat.g0) / (d * d) : 0.0));
+  return h;
+}
+
 __device__ __forceinline__ bool cp_residual(const Mat &mat, const CpPoint &pt, const double *M, double g,
                                             double *Res, NeoHooke &h, double *gd, double *dgd, double &gdot) {
   double t[9], Ce[9];
@@ -155,7 +171,8 @@ __device__ __forceinline__ bool cp_residual(const Mat &mat, const CpPoint &pt, c
 #pragma unroll
     for (int i = 0; i < 9; i++) Res[i] += pt.dt * gd[a] * P[i];
   }
-  Res[9] = g - pt.g_n - pt.dt * mat.G0 * gdot * (mat.gs0 - g) / (mat.gs0 - mat.g0);
+  const double gs = cp_hardening(mat, gdot, g, pt.dt).gs;
+  Res[9] = g - pt.g_n - pt.dt * mat.G0 * gdot * (gs - g) / (gs - mat.g0);
   return true;
 }
 
@@ -241,7 +258,8 @@ __device__ void cp_jacobian(const Mat &mat, const CpPoint &pt, const double *M, 
   double t[9], Ce[9], CepM[9];
   mm3(pt.Cep, M, CepM);
   mm3tn(M, CepM, Ce);
-  const double gs = mat.gs0, g0 = mat.g0, c = pt.dt * mat.G0 / (gs - g0);
+  const CpHard hd = cp_hardening(mat, gdot, g, pt.dt);
+  const double c = pt.dt * mat.G0 / (hd.gs - mat.g0);
   for (int r = 0; r < 10; r++)
     for (int q = 0; q < 10; q++) lm(Jm, 10, r, q) = (r == q && r < 9) ? 1.0 : 0.0;
   double dgdM[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -262,8 +280,8 @@ __device__ void cp_jacobian(const Mat &mat, const CpPoint &pt, const double *M, 
 #pragma unroll
     for (int j = 0; j < 9; j++) dgdM[j] += sg * dgd[a] * dtau[j];
   }
-  for (int j = 0; j < 9; j++) lm(Jm, 10, 9, j) = -c * (gs - g) * dgdM[j];
-  lm(Jm, 10, 9, 9) = 1.0 + c * gdot + c * (gs - g) * gdot / (mat.m * g);
+  for (int j = 0; j < 9; j++) lm(Jm, 10, 9, j) = hd.dRg * dgdM[j];
+  lm(Jm, 10, 9, 9) = 1.0 + c * gdot - hd.dRg * gdot / (mat.m * g);
 }
 
 struct CpArgs {
@@ -474,7 +492,7 @@ __global__ void __launch_bounds__(32 * kCpTanWarps) k_cp_tangent(const CpArgs A)
         mm3(pt.Cep, M, t);
         mm3tn(M, t, Ce);
         mm3(pFni, M, W);
-        const double gs = A.mat.gs0, c = A.dt * A.mat.G0 / (gs - A.mat.g0);
+        const double dRg = cp_hardening(A.mat, gdot, g, A.dt).dRg;
         for (int a = 0; a < kSlip; a++) {
           double P[9], Y[9], t1[9], Z[9], dtF[9];
           schmid(pt.R, a, P);
@@ -486,7 +504,7 @@ __global__ void __launch_bounds__(32 * kCpTanWarps) k_cp_tangent(const CpArgs A)
           const double cf = A.dt * dgd[a];
           for (int i = 0; i < 9; i++)
             for (int kl = 0; kl < 9; kl++) lm(Bm, 9, i, kl) -= cf * P[i] * 2.0 * dtF[kl];
-          for (int kl = 0; kl < 9; kl++) lm(Bm, 9, 9, kl) -= -c * (gs - g) * sg * dgd[a] * 2.0 * dtF[kl];
+          for (int kl = 0; kl < 9; kl++) lm(Bm, 9, 9, kl) -= dRg * sg * dgd[a] * 2.0 * dtF[kl];
         }
         ok = lane_solve(Jm, 10, Bm, 9);
         if (ok) {

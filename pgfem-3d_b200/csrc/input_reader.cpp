@@ -587,3 +587,87 @@ int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Restart files of one rank (write_restart_constitutive_model /
+// read_restart_constitutive_model, src/restart.cc:187-300): per node the pairs
+// "u_nm1 u_n" of x, y, z on one line; then per element its point count and per
+// point the model's block of write_restart -- HE (HE_PARAM::write_restart,
+// src/plasticity_model_none.cc:298-311): Fn, Fnm1; CP (CP_PARAM::write_restart,
+// src/plasticity_model.cc:883-911): Fn, Fnm1, pFn, pFnm1 (cm_write_tensor_restart,
+// src/constitutive_model.cc:4005-4013, one tensor of 9 per line), tau_n[12],
+// gamma_dot_n[12], then g_n g_nm1 L_n L_nm1.  Numbers in %.17e.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int pgfem_restart_block_size(int model) {
+  switch (model) {
+    case PGFEM_MODEL_HE: return 18;
+    case PGFEM_MODEL_CP: return 4 * 9 + 12 + 12 + 4;
+    default: return -1;
+  }
+}
+
+int pgfem_restart_format(const char *path, long nn, long ne, int n_ip, int model, const double *u_nm1,
+                         const double *u_n, const double *blocks) {
+  const int bs = pgfem_restart_block_size(model);
+  if (!path || nn < 0 || ne < 0 || n_ip < 1 || bs < 0 || (nn && (!u_nm1 || !u_n)) || (ne && !blocks))
+    return PGFEM_GPU_EINVAL;
+  FILE *f = fopen(path, "w");
+  if (!f) return fail(std::string("cannot create ") + path);
+  for (long a = 0; a < nn; a++) {
+    for (int b = 0; b < 3; b++) fprintf(f, "%.17e %.17e ", u_nm1[3 * a + b], u_n[3 * a + b]);
+    fprintf(f, "\n");
+  }
+  auto tensor = [&](const double *t) {
+    fprintf(f, "%.17e %.17e %.17e %.17e %.17e %.17e %.17e %.17e %.17e\n", t[0], t[1], t[2], t[3], t[4], t[5], t[6],
+            t[7], t[8]);
+  };
+  for (long e = 0; e < ne; e++) {
+    fprintf(f, "%d\n", n_ip);
+    for (int q = 0; q < n_ip; q++) {
+      const double *b = blocks + ((size_t)e * n_ip + q) * bs;
+      tensor(b);
+      tensor(b + 9);
+      if (model == PGFEM_MODEL_CP) {
+        tensor(b + 18);
+        tensor(b + 27);
+        for (int k = 0; k < 12; k++) fprintf(f, "%.17e ", b[36 + k]);
+        fprintf(f, "\n");
+        for (int k = 0; k < 12; k++) fprintf(f, "%.17e ", b[48 + k]);
+        fprintf(f, "\n");
+        fprintf(f, "%.17e %.17e %.17e %.17e\n", b[60], b[61], b[62], b[63]);
+      }
+    }
+  }
+  const bool ok = !ferror(f);
+  fclose(f);
+  return ok ? PGFEM_GPU_OK : fail(std::string("write error on ") + path);
+}
+
+int pgfem_restart_parse(const char *path, long nn, long ne, int n_ip, int model, double *u_nm1, double *u_n,
+                        double *blocks) {
+  const int bs = pgfem_restart_block_size(model);
+  if (!path || nn < 0 || ne < 0 || n_ip < 1 || bs < 0 || (nn && (!u_nm1 || !u_n)) || (ne && !blocks))
+    return PGFEM_GPU_EINVAL;
+  Tokens t;
+  if (!t.load(path)) return fail(std::string("cannot open ") + path);
+  auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
+  for (long a = 0; a < nn; a++)
+    for (int b = 0; b < 3; b++)
+      if (!t.num(u_nm1[3 * a + b]) || !t.num(u_n[3 * a + b])) return bad("nodal displacement");
+  for (long e = 0; e < ne; e++) {
+    long nip;
+    if (!t.num(nip)) return bad("point count");
+    if (nip != n_ip) return bad("point count (element type)");
+    for (int q = 0; q < n_ip; q++) {
+      double *b = blocks + ((size_t)e * n_ip + q) * bs;
+      for (int k = 0; k < bs; k++)
+        if (!t.num(b[k])) return bad(model == PGFEM_MODEL_CP ? "crystal plasticity block" : "hyperelastic block");
+    }
+  }
+  if (!t.eof()) return bad("trailing data (mesh or model does not match the file)");
+  return PGFEM_GPU_OK;
+}
+
+}  // extern "C"

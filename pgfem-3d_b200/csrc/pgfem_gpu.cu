@@ -192,6 +192,37 @@ int device_state_size(int model) {
   }
 }
 
+// F = I + grad_X u (+ the element group's macro F0) at every point, AoS
+// [ne * nqp_e][9] (compute_deformation_gradient of the restart writer's Fn).
+__global__ void k_point_F(const double *X, const int *conn, long nn, long ne, int nne, int nqp_e,
+                          const double *unode, ShapeTable shp, const double *F0, const int *elem_group,
+                          const double *F0_tab, double *F_out) {
+  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (t >= ne * nqp_e) return;
+  const long e = t / nqp_e;
+  const int q = (int)(t % nqp_e);
+  double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int a = 0; a < nne; a++) {
+    const long n = conn[(long)a * ne + e];
+    for (int i = 0; i < 3; i++) {
+      const double x = X[i * nn + n], u = unode[i * nn + n];
+      for (int c = 0; c < 3; c++) {
+        dX[i * 3 + c] += shp.dNxi[q][a][c] * x;
+        dU[i * 3 + c] += shp.dNxi[q][a][c] * u;
+      }
+    }
+  }
+  double dXi[9], F[9];
+  const bool ok = inv3(dX, dXi);
+  const double *G0 = elem_group ? F0_tab + 9 * (long)elem_group[e] : F0;
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++)
+      F[i * 3 + j] = ok ? (i == j ? 1.0 : 0.0) + dU[i * 3] * dXi[j] + dU[i * 3 + 1] * dXi[3 + j] +
+                              dU[i * 3 + 2] * dXi[6 + j] + (G0 ? G0[i * 3 + j] : 0.0)
+                        : 0.0;
+  for (int k = 0; k < 9; k++) F_out[t * 9 + k] = F[k];
+}
+
 __global__ void k_expand_u(const int *dof, long nn, const double *u, const double *presc,
                            double *unode) {
   const long n = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -1255,6 +1286,112 @@ int pgfem_gpu_reset_state(pgfem_gpu_ctx *c) {
     CK(cudaMemcpyAsync(c->state_np1, c->state_n, sizeof(double) * c->nstate * c->nqp,
                        cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+static int ensure_scratch(pgfem_gpu_ctx *c, bool wantK);
+
+// Nodal totals (AoS nn*3) and point F (AoS nqp*9) of a free-DOF displacement
+// and the prescribed values.
+static int nodal_and_F(pgfem_gpu_ctx *c, const double *u, const double *presc, std::vector<double> &nodal,
+                       std::vector<double> &F) {
+  int r = ensure_scratch(c, false);
+  if (r) return r;
+  cudaStream_t s = c->stream;
+  if (c->ndof) CK(cudaMemcpyAsync(c->d_u, u, sizeof(double) * c->ndof, cudaMemcpyHostToDevice, s));
+  if (c->npres && presc) CK(cudaMemcpyAsync(c->d_presc, presc, sizeof(double) * c->npres, cudaMemcpyHostToDevice, s));
+  const long n3 = 3 * c->nn;
+  k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, c->d_u, presc ? c->d_presc : nullptr,
+                                                          c->unode);
+  CK(cudaGetLastError());
+  double *dF = nullptr;
+  if (cudaMalloc(&dF, sizeof(double) * 9 * c->nqp) != cudaSuccess) {
+    cudaGetLastError();
+    return PGFEM_GPU_ENOMEM;
+  }
+  k_point_F<<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(c->X, c->conn, c->nn, c->ne, c->nne, c->nqp_e, c->unode,
+                                                             c->shp, c->F0, c->elem_group, c->F0_tab, dF);
+  std::vector<double> soa((size_t)n3);
+  F.resize((size_t)9 * c->nqp);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(soa.data(), c->unode, sizeof(double) * n3, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(F.data(), dF, sizeof(double) * 9 * c->nqp, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaFree(dF);
+  if (e != cudaSuccess) return PGFEM_GPU_ECUDA;
+  nodal.resize((size_t)n3);
+  for (long n = 0; n < c->nn; n++)
+    for (int b = 0; b < 3; b++) nodal[3 * n + b] = soa[(size_t)b * c->nn + n];
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_nm1, const double *u_n,
+                            const double *presc_nm1, const double *presc_n, const double *state_nm1) {
+  if (!c || !path || (c->ndof && (!u_nm1 || !u_n)) || (c->npres && (!presc_nm1 || !presc_n)))
+    return PGFEM_GPU_EINVAL;
+  if (c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  std::vector<double> un1, un, Fn1, Fn;
+  int r;
+  if ((r = nodal_and_F(c, u_nm1, presc_nm1, un1, Fn1)) || (r = nodal_and_F(c, u_n, presc_n, un, Fn))) return r;
+  const int bs = pgfem_restart_block_size(c->model);
+  std::vector<double> blocks((size_t)bs * c->nqp, 0.0);
+  std::vector<double> st;
+  if (c->model == PGFEM_MODEL_CP) {
+    st.resize((size_t)10 * c->nqp);
+    if ((r = pgfem_gpu_get_state(c, 0, st.data()))) return r;
+  }
+  for (long q = 0; q < c->nqp; q++) {
+    double *b = blocks.data() + (size_t)bs * q;
+    for (int k = 0; k < 9; k++) {
+      b[k] = Fn[9 * q + k];
+      b[9 + k] = Fn1[9 * q + k];
+    }
+    if (c->model == PGFEM_MODEL_CP) {
+      const double *sn = st.data() + 10 * q, *sm = state_nm1 ? state_nm1 + 10 * q : sn;
+      for (int k = 0; k < 9; k++) {
+        b[18 + k] = sn[k];
+        b[27 + k] = sm[k];
+      }
+      // tau_n, gamma_dot_n and L are not carried by this path: written as 0
+      b[60] = sn[9];
+      b[61] = sm[9];
+    }
+  }
+  return pgfem_restart_format(path, c->nn, c->ne, c->nqp_e, c->model, un1.data(), un.data(), blocks.data());
+}
+
+int pgfem_gpu_read_restart(pgfem_gpu_ctx *c, const char *path, double *u_nm1, double *u_n) {
+  if (!c || !path || (c->ndof && (!u_nm1 || !u_n))) return PGFEM_GPU_EINVAL;
+  if (c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
+  const int bs = pgfem_restart_block_size(c->model);
+  std::vector<double> un1((size_t)3 * c->nn), un((size_t)3 * c->nn), blocks((size_t)bs * c->nqp);
+  int r = pgfem_restart_parse(path, c->nn, c->ne, c->nqp_e, c->model, un1.data(), un.data(), blocks.data());
+  if (r) return r;
+  std::vector<int> dof((size_t)3 * c->nn);
+  CK(cudaMemcpyAsync(dof.data(), c->dof, sizeof(int) * dof.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (long n = 0; n < c->nn; n++)
+    for (int b = 0; b < 3; b++) {
+      const int id = dof[(size_t)b * c->nn + n];
+      if (id > 0) {
+        u_nm1[id - 1] = un1[3 * n + b];
+        u_n[id - 1] = un[3 * n + b];
+      }
+    }
+  if (c->model == PGFEM_MODEL_CP) {
+    std::vector<double> st((size_t)10 * c->nqp), Fs((size_t)9 * c->nqp);
+    for (long q = 0; q < c->nqp; q++) {
+      const double *b = blocks.data() + (size_t)bs * q;
+      for (int k = 0; k < 9; k++) {
+        st[10 * q + k] = b[18 + k];
+        Fs[(size_t)k * c->nqp + q] = b[k];
+      }
+      st[10 * q + 9] = b[60];
+    }
+    if ((r = pgfem_gpu_set_state(c, st.data()))) return r;
+    CK(cudaMemcpyAsync(c->cp_Fn, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
   return PGFEM_GPU_OK;
 }
 

@@ -132,6 +132,11 @@ def lib():
             "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
             "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
             "pgfem_input_read_model_params": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
+            "pgfem_restart_block_size": (C.c_int, [C.c_int]),
+            "pgfem_restart_format": (C.c_int, [C.c_char_p, C.c_long, C.c_long, C.c_int, C.c_int, _P, _P, _P]),
+            "pgfem_restart_parse": (C.c_int, [C.c_char_p, C.c_long, C.c_long, C.c_int, C.c_int, _P, _P, _P]),
+            "pgfem_gpu_write_restart": (C.c_int, [_P, C.c_char_p, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_read_restart": (C.c_int, [_P, C.c_char_p, _P, _P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -729,3 +734,45 @@ def euler_rotation(angles):
     R = np.zeros((a.shape[0], 3, 3))
     _check("pgfem_euler_rotation", lib().pgfem_euler_rotation(a.shape[0], _ptr(a), _ptr(R)))
     return R
+
+
+# --------------------------------------------------------------- restart ----
+def restart_block_size(model):
+    return lib().pgfem_restart_block_size(model)
+
+
+def restart_format(path, model, u_nm1, u_n, blocks):
+    """One rank's restart file: u_nm1, u_n nodal (nn,3); blocks (ne, n_ip, block_size)."""
+    u_nm1 = np.ascontiguousarray(u_nm1, dtype=np.float64)
+    u_n = np.ascontiguousarray(u_n, dtype=np.float64)
+    blocks = np.ascontiguousarray(blocks, dtype=np.float64)
+    _check_input("pgfem_restart_format", lib().pgfem_restart_format(
+        path.encode(), u_n.shape[0], blocks.shape[0], blocks.shape[1], model, _ptr(u_nm1), _ptr(u_n), _ptr(blocks)))
+
+
+def restart_parse(path, model, nn, ne, n_ip):
+    bs = _check("pgfem_restart_block_size", restart_block_size(model))
+    u_nm1 = np.zeros((nn, 3))
+    u_n = np.zeros((nn, 3))
+    blocks = np.zeros((ne, n_ip, bs))
+    _check_input("pgfem_restart_parse", lib().pgfem_restart_parse(
+        path.encode(), nn, ne, n_ip, model, _ptr(u_nm1), _ptr(u_n), _ptr(blocks)))
+    return u_nm1, u_n, blocks
+
+
+def write_restart(ctx, path, u_nm1, u_n, presc_nm1=None, presc_n=None, state_nm1=None):
+    u_nm1 = np.ascontiguousarray(u_nm1, dtype=np.float64)
+    u_n = np.ascontiguousarray(u_n, dtype=np.float64)
+    pn1 = None if presc_nm1 is None else np.ascontiguousarray(presc_nm1, dtype=np.float64)
+    pn = None if presc_n is None else np.ascontiguousarray(presc_n, dtype=np.float64)
+    sm = None if state_nm1 is None else np.ascontiguousarray(state_nm1, dtype=np.float64)
+    _check_input("pgfem_gpu_write_restart", lib().pgfem_gpu_write_restart(
+        ctx.h, path.encode(), _ptr(u_nm1), _ptr(u_n), _ptr(pn1), _ptr(pn), _ptr(sm)))
+
+
+def read_restart(ctx, path):
+    """Returns the free-DOF (u_nm1, u_n); CP contexts take the state at t_n from the file."""
+    u_nm1 = np.zeros(ctx.ndof)
+    u_n = np.zeros(ctx.ndof)
+    _check_input("pgfem_gpu_read_restart", lib().pgfem_gpu_read_restart(ctx.h, path.encode(), _ptr(u_nm1), _ptr(u_n)))
+    return u_nm1, u_n

@@ -7,10 +7,11 @@ Reads, with this library's own input readers (pgfem_input_*), the reference's
 box_8CPU_tension/box_<r>.in (257 linear tets, merged into one mesh),
 model_params.in (crystal plasticity parameters), CO/co_<r>.in (grain
 orientations) and box_0.in.st_tension (time steps and the prescribed-value
-increments of the first load steps), and writes
-tests/golden/cp_box_tension.json.  The file carries inputs only: the
-reference's own results for this case come from an elastic law and a local
-solver that live in an absent library, so no reference numbers are stored.
+increments of its 49 load steps) and the reference's own output of that run,
+ref_out_tension/box_<r>_49.res (restart files of step 49: per element the
+plastic deformation gradient pF_n and the slip resistance g_n, read with this
+library's restart parser and put in merged element order), and writes
+tests/golden/cp_box_tension.json.
 """
 import json
 import os
@@ -21,7 +22,7 @@ sys.path.insert(0, os.path.join(HERE, "..", "..", "pgfem-3d_b200"))
 
 import pgfem_gpu as pg  # noqa: E402
 
-NSTEPS = 3
+NSTEPS = 49
 
 
 def main(ref):
@@ -31,13 +32,25 @@ def main(ref):
              if x.model_type == pg.CM_CRYSTAL_PLASTICITY]
     angles, etype = m.orientations(os.path.join(cp, mp.ort_file.decode()))
     sf, times, _, load_steps, incr = pg.read_solver_file(os.path.join(cp, "box_0.in.st_tension"), m.info.npres)
+    pF49 = [None] * m.info.ne
+    g49 = [None] * m.info.ne
+    for r in range(8):
+        with open(os.path.join(cp, "box_8CPU_tension", "box_%d.in" % r)) as f:
+            nn, _, ne = map(int, f.readline().split())
+        _, _, b = pg.restart_parse(os.path.join(cp, "ref_out_tension", "box_%d_49.res" % r), pg.MODEL_CP, nn, ne, 1)
+        for e in range(m.info.ne):
+            if m.elem_part[e] == r:
+                blk = b[m.elem_local[e], 0]
+                pF49[e] = blk[18:27].tolist()
+                g49[e] = float(blk[60])
     d = dict(X=m.X.tolist(), conn=m.conn.tolist(), codes=m.codes.tolist(), defl=m.defl.tolist(),
              Ex=float(m.materials[0, 0]), nyz=float(m.materials[0, 6]), devPotFlag=int(m.dev_pot[0]),
              volPotFlag=int(m.vol_pot[0]), cp_params=list(mp.p)[:mp.np], euler_type=etype,
-             angles=angles.tolist(), nor_min=sf.nor_min, times=times[:NSTEPS + 1].tolist(),
+             angles=angles.tolist(), nor_min=sf.nor_min, times=times.tolist(),
              load_steps=load_steps[:NSTEPS].tolist(), load_incr=incr[:NSTEPS].tolist(),
+             ref_step=49, ref_pF=pF49, ref_g=g49,
              source="verification_tests/crystal_plasticity/{box_8CPU_tension/box_<r>.in, model_params.in, "
-                    "CO/co_<r>.in, box_0.in.st_tension}")
+                    "CO/co_<r>.in, box_0.in.st_tension, ref_out_tension/box_<r>_49.res}")
     out = os.path.join(HERE, "cp_box_tension.json")
     with open(out, "w") as f:
         json.dump(d, f, indent=0)

@@ -1,0 +1,115 @@
+"""Restart files from and into a device context (pgfem_gpu_write_restart /
+pgfem_gpu_read_restart) in the reference's per-rank layout.
+
+- crystal plasticity box (the reference's own inputs): after three device load
+  steps the written file holds the total nodal displacements of t_{n-1} and
+  t_n, F from them, pF and g at t_n (committed state) and t_{n-1} (the state
+  before the last commit), zeros for the fields this path does not carry;
+  a fresh context that reads it returns the same displacements and state,
+  and its next load step equals the original context's (to the rounding of
+  the atomic scatter's summation order, 1e-12)
+- hyperelastic box patch test: the converged affine stretch writes
+  Fn = diag(2, 1, 1) at every point and Fnm1 = I
+- a J2 context has no restart (EINVAL)
+"""
+import numpy as np
+import pytest
+
+import pgfem_gpu as pg
+from test_oracle_golden import cp_box, cp_box_steps
+
+pytestmark = pytest.mark.gpu
+
+DN4 = np.array([[-1.0, -1, -1], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+
+
+def nodal(ids, u, presc):
+    out = np.zeros(ids.shape)
+    free = ids > 0
+    out[free] = u[ids[free] - 1]
+    pres = ids < 0
+    out[pres] = presc[-ids[pres] - 1]
+    return out
+
+
+def F_linear_tets(X, conn, un):
+    dX = np.einsum("eai,ac->eic", X[conn], DN4)
+    dU = np.einsum("eai,ac->eic", un[conn], DN4)
+    return np.eye(3) + dU @ np.linalg.inv(dX)
+
+
+def test_crystal_plasticity_restart_round_trip(gpu, tmp_path):
+    import torch
+    d, X, conn, ids, ndof, Ap, Ai, R_cp, mat = cp_box()
+    npres = len(d["defl"])
+
+    def context():
+        return pg.Context(X, conn, ids, ndof, Ap, Ai, mat, npres=npres, R_cp=R_cp)
+
+    ctx = context()
+    s = pg.Solver(Ap, Ai, ndof, maxit=5000, kdim=100, tol=1e-13)
+    du = torch.zeros(ndof, dtype=torch.float64, device="cuda")
+    steps = list(cp_box_steps(d))
+    hist = []
+    for dt, presc in steps[:3]:
+        prev_state = ctx.get_state(0)
+        info = s.newton_step(ctx, du.data_ptr(), torch.from_numpy(presc).cuda().data_ptr(), dt=dt, iter_max=20,
+                             nor_min=1e-10)
+        assert info.converged
+        ctx.commit_state()
+        hist.append((du.cpu().numpy(), presc))
+    (u1, p1), (u2, p2) = hist[-2], hist[-1]
+    path = str(tmp_path / "box_0_3.res")
+    pg.write_restart(ctx, path, u1, u2, p1, p2, state_nm1=prev_state)
+    a, b, blocks = pg.restart_parse(path, pg.MODEL_CP, X.shape[0], conn.shape[0], 1)
+    assert np.array_equal(a, nodal(ids, u1, p1)) and np.array_equal(b, nodal(ids, u2, p2))
+    st = ctx.get_state(0)
+    blk = blocks[:, 0]
+    assert np.abs(blk[:, 0:9] - F_linear_tets(X, conn, b).reshape(-1, 9)).max() <= 1e-14
+    assert np.abs(blk[:, 9:18] - F_linear_tets(X, conn, a).reshape(-1, 9)).max() <= 1e-14
+    assert np.array_equal(blk[:, 18:27], st[:, :9]) and np.array_equal(blk[:, 60], st[:, 9])
+    assert np.array_equal(blk[:, 27:36], prev_state[:, :9]) and np.array_equal(blk[:, 61], prev_state[:, 9])
+    assert not blk[:, 36:60].any() and not blk[:, 62:64].any()
+    # a fresh context resumes from the file
+    ctx2 = context()
+    r1, r2 = pg.read_restart(ctx2, path)
+    assert np.array_equal(r1, u1) and np.array_equal(r2, u2)
+    assert np.array_equal(ctx2.get_state(0), st)
+    dt, presc = steps[3]
+    dp = torch.from_numpy(presc).cuda()
+    du2 = torch.from_numpy(r2.copy()).cuda()
+    i1 = s.newton_step(ctx, du.data_ptr(), dp.data_ptr(), dt=dt, iter_max=20, nor_min=1e-10)
+    i2 = s.newton_step(ctx2, du2.data_ptr(), dp.data_ptr(), dt=dt, iter_max=20, nor_min=1e-10)
+    assert i1.converged and i2.converged and len(i1.history()) == len(i2.history())
+    assert np.allclose(i1.history(), i2.history(), rtol=1e-9, atol=1e-15)
+    assert torch.allclose(du, du2, rtol=0, atol=1e-12 * float(du.abs().max()))
+    s1, s2 = ctx.get_state(1), ctx2.get_state(1)
+    assert np.abs(s1 - s2).max() <= 1e-12 * np.abs(s1).max()
+
+
+def test_hyperelastic_restart_holds_the_deformation(gpu, tmp_path):
+    import torch
+    from test_gpu_box_fixture import box
+    d, X, conn, ids, ndof, Ap, Ai, mat, defl = box(tmp_path, "LT")
+    ctx = pg.Context(X, conn, ids, ndof, Ap, Ai, mat, npres=len(defl))
+    s = pg.Solver(Ap, Ai, ndof, maxit=2000, kdim=100, tol=1e-13)
+    du = torch.zeros(ndof, dtype=torch.float64, device="cuda")
+    info = s.newton_step(ctx, du.data_ptr(), torch.from_numpy(defl.copy()).cuda().data_ptr(), iter_max=30,
+                         nor_min=1e-13)
+    assert info.converged
+    u = du.cpu().numpy()
+    path = str(tmp_path / "box_LT_0_1.res")
+    pg.write_restart(ctx, path, np.zeros(ndof), u, np.zeros_like(defl), defl)
+    _, b, blocks = pg.restart_parse(path, pg.MODEL_HE, X.shape[0], conn.shape[0], 1)
+    assert np.abs(blocks[:, 0, 0:9] - np.diag([1.0 + defl[0], 1.0, 1.0]).ravel()).max() <= 1e-10
+    assert np.abs(blocks[:, 0, 9:18] - np.eye(3).ravel()).max() == 0.0
+    r1, r2 = pg.read_restart(ctx, path)
+    assert not r1.any() and np.array_equal(r2, u)
+
+
+def test_j2_context_has_no_restart(gpu, tmp_path):
+    import workloads as wl
+    p = wl.j2_p2(n=2, seed=1)
+    ctx = p.context()
+    with pytest.raises(pg.PgfemError, match="EINVAL"):
+        pg.write_restart(ctx, str(tmp_path / "j2.res"), p.u, p.u)

@@ -1,5 +1,11 @@
 """Pins the CPU oracle to the reference's own known answers.
 
+(1) box patch test (below); (2) the crystal plasticity tension case of
+verification_tests/crystal_plasticity: its 8-partition mesh, grain
+orientations, parameters and 50 load steps, against the state the reference
+wrote in its step-49 restart files (slip resistance and plastic deformation
+gradient of every element).
+
 The reference's box patch test (tests/box/tension_disp, run by
 tests/box/common.sh.in) stretches the unit box to twice its length with the
 lateral DOFs held (verification_tests/box_patch_{LT,QT}/tension_disp inputs)
@@ -67,3 +73,56 @@ def test_box_tension_disp_matches_reference_output(lq):
     err, S, _, _, _ = oracle.cm_update(mat, F)
     assert err == 0
     assert abs(S[0, 0] - d["expected_S_xx"]) <= 1e-14 * abs(d["expected_S_xx"]) + 1e-14
+
+
+# The reference's crystal plasticity tension case writes its state after 50
+# load steps (tests/golden/make_cp_box_fixture.py); its local solver stops at
+# 1e-5 and its elasticity lives in an absent library, so agreement is judged
+# at the size of those tolerances (measured: g 6.5e-5 relative, pF 1.7e-5).
+CP_REF_G_RTOL = 2e-4
+CP_REF_PF_ATOL = 5e-5
+
+
+def cp_box():
+    import pgfem_gpu as pg
+    d = json.load(open(os.path.join(GOLDEN, "cp_box_tension.json")))
+    X = np.array(d["X"])
+    conn = np.array(d["conn"], dtype=np.int32)
+    ids, ndof = oracle.generate_dof_ids(conn, X.shape[0], np.array(d["codes"], dtype=np.int64))
+    Ap, Ai = oracle.psparse_apai(conn, ids, ndof)
+    R_cp = pg.euler_rotation(np.array(d["angles"])).reshape(-1, 9)
+    p = d["cp_params"]
+    mat = pg.material(pg.MODEL_CP, E=d["Ex"], nu=d["nyz"], gamma_dot_0=p[0], m=p[1], G0=p[2], g0=p[3], gs_0=p[4],
+                      gamma_dot_s=p[5], w=p[6])
+    return d, X, conn, ids, ndof, Ap, Ai, R_cp, mat
+
+
+def cp_box_steps(d):
+    """(dt, prescribed values) of each solve: the mesh's values first, then one
+    increment per load step (times has one more entry than the solves)."""
+    presc = np.array(d["defl"])
+    for k in range(len(d["times"]) - 1):
+        yield d["times"][k + 1] - d["times"][k], presc.copy()
+        if k < len(d["load_incr"]):
+            presc = presc + np.array(d["load_incr"][k])
+
+
+def test_crystal_plasticity_box_matches_reference_restart():
+    d, X, conn, ids, ndof, Ap, Ai, R_cp, mat = cp_box()
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai, R_cp=R_cp)
+    om = oracle.from_pg_material(mat)
+    st = np.zeros((conn.shape[0], 10))
+    st[:, [0, 4, 8]] = 1.0
+    st[:, 9] = d["cp_params"][3]
+    u = np.zeros(ndof)
+    nsolve = 0
+    for dt, presc in cp_box_steps(d):
+        u, h, ok, st = oracle.newton_step(P, om, u, presc, state_n=st, dt=dt, iter_max=20, nor_min=1e-10)
+        assert ok, h
+        nsolve += 1
+    assert nsolve == d["ref_step"] + 1 == 50
+    g_ref, pF_ref = np.array(d["ref_g"]), np.array(d["ref_pF"])
+    assert np.abs(st[:, 9] - g_ref).max() <= CP_REF_G_RTOL * g_ref.max()
+    assert np.abs(st[:, :9] - pF_ref).max() <= CP_REF_PF_ATOL
+    # the comparison is sharp: the plastic part of pF is 200x the tolerance
+    assert np.abs(pF_ref - np.eye(3).ravel()).max() > 200 * CP_REF_PF_ATOL

@@ -1,0 +1,34 @@
+"""Restart files in the reference's layout (host code, CPU): the formatter
+and parser of one rank's file (src/restart.cc:187-300 with the HE and CP
+write_restart blocks) round-trip bit-exactly through %.17e; files whose node,
+element or point counts or model do not match are rejected (EFORMAT)."""
+import numpy as np
+import pytest
+
+import pgfem_gpu as pg
+
+
+@pytest.mark.parametrize("model,bs", [(pg.MODEL_HE, 18), (pg.MODEL_CP, 64)])
+def test_round_trip(tmp_path, model, bs):
+    assert pg.restart_block_size(model) == bs
+    rng = np.random.default_rng(model)
+    nn, ne, nip = 14, 24, (1 if model == pg.MODEL_CP else 4)
+    u1, u2 = rng.normal(size=(nn, 3)), rng.normal(size=(nn, 3))
+    blocks = rng.normal(size=(ne, nip, bs)) * 10.0 ** rng.integers(-12, 12, size=(ne, nip, bs)).astype(float)
+    path = str(tmp_path / "box_0_7.res")
+    pg.restart_format(path, model, u1, u2, blocks)
+    lines = open(path).read().split("\n")
+    assert len(lines[0].split()) == 6 and lines[nn].strip() == str(nip)
+    a, b, c = pg.restart_parse(path, model, nn, ne, nip)
+    assert np.array_equal(a, u1) and np.array_equal(b, u2) and np.array_equal(c, blocks)
+    with pytest.raises(pg.PgfemError, match="EFORMAT.*point count"):
+        pg.restart_parse(path, model, nn, ne, nip + 1)
+    with pytest.raises(pg.PgfemError, match="EFORMAT"):
+        pg.restart_parse(path, model, nn, ne + 1, nip)
+    with pytest.raises(pg.PgfemError, match="EFORMAT.*trailing"):
+        pg.restart_parse(path, model, nn, ne - 1, nip)
+    other = pg.MODEL_HE if model == pg.MODEL_CP else pg.MODEL_CP
+    with pytest.raises(pg.PgfemError, match="EFORMAT"):
+        pg.restart_parse(path, other, nn, ne, nip)
+    with pytest.raises(pg.PgfemError, match="EINVAL"):
+        pg.restart_parse(path, pg.MODEL_J2, nn, ne, nip)
