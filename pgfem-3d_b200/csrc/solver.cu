@@ -314,6 +314,8 @@ __global__ void __launch_bounds__(kBlk) k_multidot(long n, const double *__restr
     double acc[kTile];
 #pragma unroll
     for (int u = 0; u < kTile; u++) acc[u] = 0.0;
+    // two rows per pass: sixteen loads in flight, same summation order
+#pragma unroll 2
     for (long i = i0 + threadIdx.x; i < i1; i += kBlk) {
       const double wi = w[i];
 #pragma unroll
@@ -366,6 +368,8 @@ __global__ void __launch_bounds__(kBlk) k_multiaxpy(long n, const double *__rest
   for (long i = blockIdx.x * (long)kBlk + threadIdx.x; i < n; i += (long)gridDim.x * kBlk) {
     double a0 = w[i], a1 = 0.0, a2 = 0.0, a3 = 0.0;
     int t = 0;
+    // eight basis loads in flight per pass, same summation order
+#pragma unroll 2
     for (; t + 4 <= nt; t += 4) {
       a0 = fma(-V[(long)t * n + i], htmp[t], a0);
       a1 = fma(-V[(long)(t + 1) * n + i], htmp[t + 1], a1);
