@@ -438,6 +438,11 @@ int pgfem_input_get_materials(const pgfem_input *in, double *vals, int *dev_pot,
  * with a negative element id sets every element of material `ip` of its
  * partition.  euler_type: the file's "# EulerAngleType: k" (0 if absent). */
 int pgfem_input_read_orientations(const pgfem_input *in, const char *base, double *angles, int *euler_type);
+/* Partition `part` of the merged mesh: its node and element counts and the
+ * merged id of each of its local nodes (node_map[nn], may be NULL); its
+ * elements are the merged elements [sum of earlier ne, + ne).  This is what
+ * maps per-rank files (restart files, outputs) onto the merged mesh. */
+int pgfem_input_get_partition(const pgfem_input *in, int part, long *nn, long *ne, long *node_map);
 void pgfem_input_destroy(pgfem_input *in);
 /* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
  * composition the reference states at src/plasticity_model.cc:1252-1255; its

@@ -124,6 +124,7 @@ struct pgfem_input {
   std::vector<int> dev_pot, vol_pot;
   int nparts = 0;
   std::vector<long> part_elem_off;  // merged element index of each partition's first element
+  std::vector<std::vector<long>> node_map;  // per partition: merged id of each local node
 };
 
 namespace {
@@ -365,6 +366,7 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
     I.nel_v += p.nel_v;
   }
   I.ne = in->part_elem_off[nparts];
+  in->node_map = std::move(lmap);
   in->defl = p0.defl;
   in->mat_vals = p0.mats;
   in->dev_pot = p0.devp;
@@ -451,6 +453,15 @@ int pgfem_input_read_orientations(const pgfem_input *in, const char *base, doubl
     fclose(f);
   }
   if (euler_type) *euler_type = etype;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_partition(const pgfem_input *in, int part, long *nn, long *ne, long *node_map) {
+  if (!in || part < 0 || part >= in->nparts) return PGFEM_GPU_EINVAL;
+  const std::vector<long> &m = in->node_map[part];
+  if (nn) *nn = (long)m.size();
+  if (ne) *ne = in->part_elem_off[part + 1] - in->part_elem_off[part];
+  if (node_map) memcpy(node_map, m.data(), sizeof(long) * m.size());
   return PGFEM_GPU_OK;
 }
 

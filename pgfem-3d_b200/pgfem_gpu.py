@@ -129,6 +129,7 @@ def lib():
             "pgfem_input_get_materials": (C.c_int, [_P, _P, _P, _P]),
             "pgfem_input_read_orientations": (C.c_int, [_P, C.c_char_p, _P, _P]),
             "pgfem_input_destroy": (None, [_P]),
+            "pgfem_input_get_partition": (C.c_int, [_P, C.c_int, _P, _P, _P]),
             "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
             "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
             "pgfem_input_read_model_params": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
@@ -671,6 +672,16 @@ class InputMesh:
         if getattr(self, "_h", None) and _lib is not None:
             _lib.pgfem_input_destroy(self._h)
             self._h = None
+
+    def partition(self, part):
+        """(node_map (merged id of each local node), first element, element count) of a partition."""
+        nn, ne = C.c_long(), C.c_long()
+        _check("pgfem_input_get_partition", lib().pgfem_input_get_partition(self._h, part, C.byref(nn), C.byref(ne),
+                                                                          None))
+        nm = np.zeros(nn.value, dtype=np.int64)
+        _check("pgfem_input_get_partition", lib().pgfem_input_get_partition(self._h, part, None, None, _ptr(nm)))
+        e0 = int(np.searchsorted(self.elem_part, part))
+        return nm, e0, ne.value
 
     def orientations(self, base):
         """(angles (ne,3), EulerAngleType) from <base>_<r>.in."""

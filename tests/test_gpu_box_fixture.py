@@ -83,7 +83,7 @@ def test_box_tension_disp_on_the_gpu_matches_reference_output(gpu, tmp_path, lq)
 
 def test_crystal_plasticity_box_load_steps_match_oracle_and_reference(gpu):
     import torch
-    from test_oracle_golden import CP_REF_G_RTOL, CP_REF_PF_ATOL, cp_box, cp_box_steps
+    from test_oracle_golden import CP_REF_G_RTOL, CP_REF_PF_ATOL, CP_REF_U_ATOL, cp_box, cp_box_steps, nodal_total
     d, X, conn, ids, ndof, Ap, Ai, R_cp, mat = cp_box()
     ctx = pg.Context(X, conn, ids, ndof, Ap, Ai, mat, npres=len(d["defl"]), R_cp=R_cp)
     P = oracle.Problem(X, conn, ids, ndof, Ap, Ai, R_cp=R_cp)
@@ -112,3 +112,4 @@ def test_crystal_plasticity_box_load_steps_match_oracle_and_reference(gpu):
     sg = ctx.get_state(0)
     assert np.abs(sg[:, 9] - g_ref).max() <= CP_REF_G_RTOL * g_ref.max()
     assert np.abs(sg[:, :9] - pF_ref).max() <= CP_REF_PF_ATOL
+    assert np.abs(nodal_total(ids, du.cpu().numpy(), presc) - np.array(d["ref_u"])).max() <= CP_REF_U_ATOL

@@ -72,6 +72,10 @@ def test_partitions_merge_to_the_original_mesh(tmp_path, nne):
                 orig[g] = o
                 assert loc[int(o)] >= 0
     assert (orig >= 0).all() and len(set(orig)) == nn
+    for r in range(len(parts)):  # the partition maps: local node -> merged node
+        nm, e0, ne_r = m.partition(r)
+        assert ne_r == len(parts[r]) and e0 == sum(len(p) for p in parts[:r])
+        assert np.array_equal(orig[nm], maps[r])
     assert np.array_equal(m.X, X[orig])
     assert np.array_equal(m.codes, codes[orig])
     assert np.array_equal(orig[m.conn], conn[np.concatenate(parts)])

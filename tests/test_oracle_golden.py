@@ -3,8 +3,8 @@
 (1) box patch test (below); (2) the crystal plasticity tension case of
 verification_tests/crystal_plasticity: its 8-partition mesh, grain
 orientations, parameters and 50 load steps, against the state the reference
-wrote in its step-49 restart files (slip resistance and plastic deformation
-gradient of every element).
+wrote in its step-49 restart files (nodal displacements, slip resistance and
+plastic deformation gradient of every element).
 
 The reference's box patch test (tests/box/tension_disp, run by
 tests/box/common.sh.in) stretches the unit box to twice its length with the
@@ -78,9 +78,19 @@ def test_box_tension_disp_matches_reference_output(lq):
 # The reference's crystal plasticity tension case writes its state after 50
 # load steps (tests/golden/make_cp_box_fixture.py); its local solver stops at
 # 1e-5 and its elasticity lives in an absent library, so agreement is judged
-# at the size of those tolerances (measured: g 6.5e-5 relative, pF 1.7e-5).
+# at the size of those tolerances (measured: g 6.5e-5 relative, pF 1.7e-5,
+# nodal displacements 1.3e-6 of at most 1.0e-2).
 CP_REF_G_RTOL = 2e-4
 CP_REF_PF_ATOL = 5e-5
+CP_REF_U_ATOL = 5e-6
+
+
+def nodal_total(ids, u, presc):
+    """Nodal displacements (nn, 3): free DOFs from u, prescribed ones from presc."""
+    out = np.zeros(ids.shape)
+    out[ids > 0] = u[ids[ids > 0] - 1]
+    out[ids < 0] = presc[-ids[ids < 0] - 1]
+    return out
 
 
 def cp_box():
@@ -116,6 +126,7 @@ def test_crystal_plasticity_box_matches_reference_restart():
     st[:, 9] = d["cp_params"][3]
     u = np.zeros(ndof)
     nsolve = 0
+    presc = None
     for dt, presc in cp_box_steps(d):
         u, h, ok, st = oracle.newton_step(P, om, u, presc, state_n=st, dt=dt, iter_max=20, nor_min=1e-10)
         assert ok, h
@@ -124,5 +135,6 @@ def test_crystal_plasticity_box_matches_reference_restart():
     g_ref, pF_ref = np.array(d["ref_g"]), np.array(d["ref_pF"])
     assert np.abs(st[:, 9] - g_ref).max() <= CP_REF_G_RTOL * g_ref.max()
     assert np.abs(st[:, :9] - pF_ref).max() <= CP_REF_PF_ATOL
+    assert np.abs(nodal_total(ids, u, presc) - np.array(d["ref_u"])).max() <= CP_REF_U_ATOL
     # the comparison is sharp: the plastic part of pF is 200x the tolerance
     assert np.abs(pF_ref - np.eye(3).ravel()).max() > 200 * CP_REF_PF_ATOL
