@@ -149,8 +149,14 @@ def test_he_stiffness_symmetric():
     assert np.abs(lk - lk.T).max() <= 1e-10 * np.abs(lk).max()
 
 
-def test_cp_tangent_matches_central_differences():
+@pytest.mark.parametrize("w", [0.0, 0.005])
+def test_cp_tangent_matches_central_differences(w):
+    """w > 0: the saturation stress depends on the slip rate, and its
+    derivative enters the local Jacobian and the tangent."""
     p = wl.cp_p1(n=3, seed=2, ngrains=4)
+    if w:
+        p.mat.w = w
+        p.mat.gamma_dot_s = 5e10
     P, mat = oracle.from_workload(p)
     st = p.state.copy()
     for s in range(1, 5):  # load to a plastic state
