@@ -412,16 +412,24 @@ typedef struct {
   long lin_maxit;       /* header line 2: linear solver iterations, tolerance, zero */
   double lin_err, lim_zero;
   long nln, nel_s, nel_v; /* nodal / surface / volume load counts (not applied on this path) */
+  long nperiodic;       /* nodes that are periodic images of another (pgfem_input_get_periodic) */
 } pgfem_input_info;
 
 /* Reads <base><r>.in for r = 0..nparts-1 and merges the partitions into one
  * mesh: a partition-boundary node (Gnn >= 0) is one node whichever files list
- * it, an interior node (Gnn = -1) belongs to its file; nodes are numbered in
- * order of first appearance (partition, then local id), elements partition
- * by partition.  Partitions must agree on shared nodes, supports, prescribed
- * values and materials.  The supports come from the mesh files (not from a
- * BC directory). */
+ * it at the same position, an interior node (Gnn = -1) belongs to its file;
+ * nodes that share a global number at different positions are periodic
+ * images (periodic micro-structures), kept as nodes of their own and linked to
+ * the first image (pgfem_input_get_periodic).  Nodes are numbered in order of
+ * first appearance (partition, then local id), elements partition by
+ * partition.  Partitions must agree on supports, prescribed values and
+ * materials.  The supports come from the mesh files. */
 int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out);
+/* The same with the supports and prescribed values of a BC directory
+ * (src/read_input_file.cc:320-360): <bc_base>_<r>.bc per partition and
+ * <bc_base>.bcv (e.g. bc_base = "<input dir>/BC/Mechanical"); the mesh files'
+ * own supports sections are read and ignored, as the reference does. */
+int pgfem_input_read_mesh_bc(const char *base, int nparts, const char *bc_base, pgfem_input **out);
 int pgfem_input_get_info(const pgfem_input *in, pgfem_input_info *info);
 /* X[nn*3], conn[ne*nne] (0-based merged ids), codes[nn*3] support codes
  * (0 free, 1 fixed, -k prescribed: the pgfem_generate_dof_ids input),
@@ -443,6 +451,8 @@ int pgfem_input_read_orientations(const pgfem_input *in, const char *base, doubl
  * elements are the merged elements [sum of earlier ne, + ne).  This is what
  * maps per-rank files (restart files, outputs) onto the merged mesh. */
 int pgfem_input_get_partition(const pgfem_input *in, int part, long *nn, long *ne, long *node_map);
+/* Pr[nn]: periodic master of each node or -1 (the pgfem_generate_dof_ids Pr input). */
+int pgfem_input_get_periodic(const pgfem_input *in, long *Pr);
 void pgfem_input_destroy(pgfem_input *in);
 /* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
  * composition the reference states at src/plasticity_model.cc:1252-1255; its

@@ -125,6 +125,7 @@ struct pgfem_input {
   int nparts = 0;
   std::vector<long> part_elem_off;  // merged element index of each partition's first element
   std::vector<std::vector<long>> node_map;  // per partition: merged id of each local node
+  std::vector<long> Pr;                      // periodic master of each merged node, -1 if none
 };
 
 namespace {
@@ -261,6 +262,38 @@ int read_part(const std::string &path, Part &p) {
   return PGFEM_GPU_OK;
 }
 
+// Supports from <bc_base>_<r>.bc (count, then "node c0 c1 c2" lines) and the
+// prescribed values from <bc_base>.bcv (count, values): the BC-directory
+// variant of read_input_file (src/read_input_file.cc:320-360, read_Dirichlet_BCs /
+// read_Dirichlet_BCs_values, src/in.cc:29-168), which replaces the mesh file's
+// own supports section.
+int read_bc_files(const std::string &bc_base, int r, Part &p) {
+  Tokens v;
+  const std::string fv = bc_base + ".bcv";
+  if (!v.load(fv)) return fail("cannot open " + fv);
+  long npd;
+  if (!v.num(npd) || npd < 0) return fail("bad prescribed count at " + v.where());
+  p.defl.assign(npd, 0.0);
+  for (long k = 0; k < npd; k++)
+    if (!v.num(p.defl[k])) return fail("bad prescribed value at " + v.where());
+  Tokens t;
+  const std::string fb = bc_base + "_" + std::to_string(r) + ".bc";
+  if (!t.load(fb)) return fail("cannot open " + fb);
+  long nsup;
+  if (!t.num(nsup) || nsup < 0) return fail("bad support count at " + t.where());
+  p.codes.assign(3 * p.nn, 0);
+  for (long k = 0; k < nsup; k++) {
+    long n;
+    if (!t.num(n) || n < 0 || n >= p.nn) return fail("bad support node at " + t.where());
+    for (int j = 0; j < 3; j++) {
+      long c;
+      if (!t.num(c) || c < -npd || c > 1) return fail("bad support code at " + t.where());
+      p.codes[3 * n + j] = c;
+    }
+  }
+  return PGFEM_GPU_OK;
+}
+
 bool close(double a, double b) { return std::fabs(a - b) <= 1e-12 * std::max(1.0, std::max(std::fabs(a), std::fabs(b))); }
 
 }  // namespace
@@ -270,11 +303,16 @@ extern "C" {
 const char *pgfem_input_last_error(void) { return g_err.c_str(); }
 
 int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
+  return pgfem_input_read_mesh_bc(base, nparts, nullptr, out);
+}
+
+int pgfem_input_read_mesh_bc(const char *base, int nparts, const char *bc_base, pgfem_input **out) {
   if (!base || nparts < 1 || !out) return PGFEM_GPU_EINVAL;
   *out = nullptr;
   std::vector<Part> parts(nparts);
   for (int r = 0; r < nparts; r++) {
-    const int e = read_part(std::string(base) + std::to_string(r) + ".in", parts[r]);
+    int e = read_part(std::string(base) + std::to_string(r) + ".in", parts[r]);
+    if (!e && bc_base) e = read_bc_files(bc_base, r, parts[r]);
     if (e) return e;
   }
   auto *in = new pgfem_input();
@@ -298,9 +336,14 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
     delete in;
     return fail(m);
   };
-  // merged node numbering: partition-boundary nodes (Gnn >= 0) by Gnn,
-  // interior nodes (Gnn = -1) per partition; first appearance order
-  std::map<long, long> gmap;
+  // merged node numbering: partition-boundary nodes (Gnn >= 0) by Gnn and
+  // position, interior nodes (Gnn = -1) per partition; first appearance
+  // order.  Nodes that share a global number at different positions are
+  // periodic images: each becomes a node of its own, linked to the first
+  // image as its periodic master -- the reference's rule (a node's periodic
+  // master is the first node with the same global number,
+  // generate_local_dof_ids, src/generate_dof_ids.cc:81-96).
+  std::map<long, std::vector<long>> gmap;
   std::vector<std::vector<long>> lmap(nparts);
   for (int r = 0; r < nparts; r++) {
     const Part &p = parts[r];
@@ -315,19 +358,23 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
       if (p.devp[m] != p0.devp[m] || p.volp[m] != p0.volp[m]) return reject("partitions with different materials");
     lmap[r].assign(p.nn, -1);
     for (long n = 0; n < p.nn; n++) {
-      long id;
+      long id = (long)in->X.size() / 3, master = -1;
       bool fresh = true;
       if (p.gnn[n] >= 0) {
-        auto it = gmap.find(p.gnn[n]);
-        if (it != gmap.end()) {
-          id = it->second;
-          fresh = false;
-        } else {
-          id = (long)in->X.size() / 3;
-          gmap[p.gnn[n]] = id;
+        std::vector<long> &images = gmap[p.gnn[n]];
+        for (long cand : images) {
+          bool same = true;
+          for (int j = 0; j < 3 && same; j++) same = close(in->X[3 * cand + j], p.X[3 * n + j]);
+          if (same) {
+            id = cand;
+            fresh = false;
+            break;
+          }
         }
-      } else {
-        id = (long)in->X.size() / 3;
+        if (fresh) {
+          if (!images.empty()) master = images[0];
+          images.push_back(id);
+        }
       }
       lmap[r][n] = id;
       if (fresh) {
@@ -335,10 +382,10 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
           in->X.push_back(p.X[3 * n + j]);
           in->codes.push_back(p.codes[3 * n + j]);
         }
+        in->Pr.push_back(master);
+        if (master >= 0) I.nperiodic++;
       } else {
         for (int j = 0; j < 3; j++) {
-          if (!close(in->X[3 * id + j], p.X[3 * n + j]))
-            return reject("partition-boundary node " + std::to_string(p.gnn[n]) + " with different coordinates");
           long &c = in->codes[3 * id + j];
           if (c == 0) c = p.codes[3 * n + j];
           else if (p.codes[3 * n + j] != 0 && p.codes[3 * n + j] != c)
@@ -453,6 +500,12 @@ int pgfem_input_read_orientations(const pgfem_input *in, const char *base, doubl
     fclose(f);
   }
   if (euler_type) *euler_type = etype;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_get_periodic(const pgfem_input *in, long *Pr) {
+  if (!in || !Pr) return PGFEM_GPU_EINVAL;
+  memcpy(Pr, in->Pr.data(), sizeof(long) * in->Pr.size());
   return PGFEM_GPU_OK;
 }
 

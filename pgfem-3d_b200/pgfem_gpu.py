@@ -123,6 +123,7 @@ def lib():
             "pgfem_gpu_newton_step": (C.c_int, [_P, _P, _P, _P, C.c_double, _P, _P, _P]),
             "pgfem_input_last_error": (C.c_char_p, []),
             "pgfem_input_read_mesh": (C.c_int, [C.c_char_p, C.c_int, _P]),
+            "pgfem_input_read_mesh_bc": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, _P]),
             "pgfem_input_get_info": (C.c_int, [_P, _P]),
             "pgfem_input_get_mesh": (C.c_int, [_P, _P, _P, _P, _P]),
             "pgfem_input_get_elements": (C.c_int, [_P, _P, _P, _P, _P]),
@@ -130,6 +131,7 @@ def lib():
             "pgfem_input_read_orientations": (C.c_int, [_P, C.c_char_p, _P, _P]),
             "pgfem_input_destroy": (None, [_P]),
             "pgfem_input_get_partition": (C.c_int, [_P, C.c_int, _P, _P, _P]),
+            "pgfem_input_get_periodic": (C.c_int, [_P, _P]),
             "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
             "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
             "pgfem_input_read_model_params": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
@@ -603,7 +605,8 @@ class Solver:
 class InputInfo(C.Structure):
     _fields_ = [("nn", C.c_long), ("ne", C.c_long), ("nne", C.c_int), ("npres", C.c_long), ("nmat", C.c_int),
                 ("nconc", C.c_long), ("norient", C.c_long), ("lin_maxit", C.c_long), ("lin_err", C.c_double),
-                ("lim_zero", C.c_double), ("nln", C.c_long), ("nel_s", C.c_long), ("nel_v", C.c_long)]
+                ("lim_zero", C.c_double), ("nln", C.c_long), ("nel_s", C.c_long), ("nel_v", C.c_long),
+                ("nperiodic", C.c_long)]
 
 
 class SolverFile(C.Structure):
@@ -638,9 +641,12 @@ class InputMesh:
     partitions merged: X (nn,3), conn (ne,nne), codes (nn,3) support codes,
     defl (npres,), per-element material / partition data, material lines."""
 
-    def __init__(self, base, nparts=1):
+    def __init__(self, base, nparts=1, bc_base=None):
+        """bc_base: supports and prescribed values from <bc_base>_<r>.bc and
+        <bc_base>.bcv (a BC directory) instead of the mesh files."""
         h = C.c_void_p()
-        _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh(base.encode(), nparts, C.byref(h)))
+        _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh_bc(
+            base.encode(), nparts, None if bc_base is None else bc_base.encode(), C.byref(h)))
         try:
             info = InputInfo()
             _check("pgfem_input_get_info", lib().pgfem_input_get_info(h, C.byref(info)))
@@ -658,6 +664,8 @@ class InputMesh:
             self.elem_local = np.zeros(ne, dtype=np.int64)
             _check("pgfem_input_get_elements", lib().pgfem_input_get_elements(
                 h, _ptr(self.elem_mat), _ptr(self.elem_hom), _ptr(self.elem_part), _ptr(self.elem_local)))
+            self.Pr = np.zeros(nn, dtype=np.int64)
+            _check("pgfem_input_get_periodic", lib().pgfem_input_get_periodic(h, _ptr(self.Pr)))
             self.materials = np.zeros((info.nmat, 13))
             self.dev_pot = np.zeros(info.nmat, dtype=np.int32)
             self.vol_pot = np.zeros(info.nmat, dtype=np.int32)
@@ -703,8 +711,10 @@ class InputMesh:
         return material(model, **args)
 
     def dof_setup(self):
-        """(ids, ndof, Ap, Ai) of the merged mesh (generate_dof_ids + Psparse_ApAi)."""
-        ids, ndof = generate_dof_ids(self.conn, self.X.shape[0], self.codes)
+        """(ids, ndof, Ap, Ai) of the merged mesh (generate_dof_ids with the
+        periodic links + Psparse_ApAi)."""
+        Pr = self.Pr if self.info.nperiodic else None
+        ids, ndof = generate_dof_ids(self.conn, self.X.shape[0], self.codes, Pr)
         Ap, Ai = psparse_apai(self.conn, ids, ndof)
         return ids, ndof, Ap, Ai
 

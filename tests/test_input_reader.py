@@ -81,13 +81,14 @@ def test_partitions_merge_to_the_original_mesh(tmp_path, nne):
     assert np.array_equal(orig[m.conn], conn[np.concatenate(parts)])
 
 
-def test_partitions_must_agree(tmp_path):
+def test_shared_number_at_two_positions_is_a_periodic_image(tmp_path):
     X, conn, _ = pg.mesh_box_tet(2, 4)
     codes = np.zeros((X.shape[0], 3), dtype=np.int64)
     parts = np.split(np.arange(conn.shape[0]), [20])
     base = str(tmp_path / "bad_")
     maps = write_partitions(base, X, conn, codes, [], [material_line(2e5, 0.3, 1, 99)], parts)
-    # move a shared node in partition 1's file
+    # move a shared node in partition 1's file: the same global number at
+    # another position is a periodic image of the first (its DOFs are shared)
     shared = set(np.unique(conn[parts[0]])) & set(np.unique(conn[parts[1]]))
     n = sorted(shared)[0]
     X2 = X.copy()
@@ -98,7 +99,25 @@ def test_partitions_must_agree(tmp_path):
     gnn = np.array([v if v in shared else -1 for v in maps[1]])
     write_mesh(base + "1.in", Xl, lconn, codes[maps[1]], [], [material_line(2e5, 0.3, 1, 99)], gnn=gnn,
                dom=np.zeros(len(maps[1]), dtype=int))
-    with pytest.raises(pg.PgfemError, match="EFORMAT.*coordinates"):
+    m = pg.InputMesh(base, 2)
+    assert m.info.nn == X.shape[0] + 1 and m.info.nperiodic == 1
+    img = int(np.where(m.Pr >= 0)[0][0])
+    assert np.allclose(m.X[img], X2[n]) and np.allclose(m.X[m.Pr[img]], X[n])
+    ids, ndof, _, _ = m.dof_setup()
+    assert np.array_equal(ids[img], ids[m.Pr[img]]) and ndof == 3 * X.shape[0]
+    # one node with different supports in the two files is an error
+    maps = write_partitions(base, X, conn, codes, [0.5], [material_line(2e5, 0.3, 1, 99)], parts)
+    c1 = codes[maps[1]].copy()
+    c1[list(maps[1]).index(n)] = [-1, 0, 0]
+    write_mesh(base + "1.in", X[maps[1]], np.vectorize(loc.get)(conn[parts[1]]), c1, [0.5],
+               [material_line(2e5, 0.3, 1, 99)], gnn=gnn, dom=np.zeros(len(maps[1]), dtype=int))
+    c0 = codes[maps[0]].copy()
+    c0[list(maps[0]).index(n)] = [1, 1, 1]
+    loc0 = {int(v): i for i, v in enumerate(maps[0])}
+    gnn0 = np.array([v if v in shared else -1 for v in maps[0]])
+    write_mesh(base + "0.in", X[maps[0]], np.vectorize(loc0.get)(conn[parts[0]]), c0, [0.5],
+               [material_line(2e5, 0.3, 1, 99)], gnn=gnn0, dom=np.zeros(len(maps[0]), dtype=int))
+    with pytest.raises(pg.PgfemError, match="EFORMAT.*different supports"):
         pg.InputMesh(base, 2)
 
 
@@ -213,3 +232,70 @@ def test_orientations_and_rotations(tmp_path):
     assert np.allclose(np.einsum("kij,kil->kjl", R, R), np.eye(3), atol=1e-14)
     with pytest.raises(pg.PgfemError, match="EFORMAT.*co_9"):
         pg.InputMesh(base, 2).orientations(str(tmp_path / "co_9"))
+
+
+def test_bc_directory_supports(tmp_path):
+    """Supports and prescribed values from a BC directory (<bc>_<r>.bc,
+    <bc>.bcv) replace the mesh files' own sections."""
+    X, conn, _ = pg.mesh_box_tet(3, 4)
+    nn = X.shape[0]
+    codes = np.zeros((nn, 3), dtype=np.int64)
+    codes[X[:, 0] == 0.0] = 1
+    codes[X[:, 0] == 1.0, 0] = -1
+    codes[X[:, 0] == 1.0, 1] = -2
+    parts = np.split(np.arange(conn.shape[0]), [50, 110])
+    base = str(tmp_path / "cube_")
+    maps = write_partitions(base, X, conn, np.zeros_like(codes), [], [material_line(2e5, 0.3, 1, 99)], parts)
+    bc = tmp_path / "BC"
+    bc.mkdir()
+    (bc / "Mechanical.bcv").write_text("2\n0.25\n-0.125\n")
+    for r, nodes in enumerate(maps):
+        sup = [i for i, n in enumerate(nodes) if codes[n].any()]
+        (bc / ("Mechanical_%d.bc" % r)).write_text(
+            "%d\n" % len(sup) + "".join("%4d  %d %d %d\n" % (i, *codes[nodes[i]]) for i in sup))
+    plain = pg.InputMesh(base, 3)
+    assert not plain.codes.any() and plain.info.npres == 0
+    m = pg.InputMesh(base, 3, bc_base=str(bc / "Mechanical"))
+    assert m.info.npres == 2 and list(m.defl) == [0.25, -0.125]
+    orig = np.zeros(nn, dtype=int)
+    for r in range(3):
+        orig[m.partition(r)[0]] = maps[r]
+    assert np.array_equal(m.codes, codes[orig])
+    ids, ndof, Ap, Ai = m.dof_setup()
+    assert ndof == 3 * nn - 3 * (X[:, 0] == 0.0).sum() - 2 * (X[:, 0] == 1.0).sum()
+    (bc / "Mechanical_1.bc").write_text("1\n0  -3 0 0\n")
+    with pytest.raises(pg.PgfemError, match="EFORMAT.*support code"):
+        pg.InputMesh(base, 3, bc_base=str(bc / "Mechanical"))
+
+
+def test_reference_fe2_micro_structure():
+    """The reference's periodic FE2 micro-structure (tube-shear case, three
+    partitions, BC directory; tests/golden/make_fe2_micro_fixture.py): the
+    merged mesh carries the periodic links of its shared global numbers, the
+    product's DOF ids and CSR pattern with those links equal the oracle's, and
+    the oracle assembles it under a macro deformation."""
+    import json
+    import os
+    d = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "fe2_micro_pack.json")))
+    X = np.array(d["X"])
+    conn = np.array(d["conn"], dtype=np.int32)
+    codes = np.array(d["codes"], dtype=np.int64)
+    Pr = np.array(d["Pr"], dtype=np.int64)
+    assert X.shape == (360, 3) and conn.shape == (1350, 4) and (Pr >= 0).sum() == 94
+    # images sit one cell length apart along the axes
+    off = X[Pr >= 0] - X[Pr[Pr >= 0]]
+    assert np.allclose(np.abs(off), np.round(np.abs(off))) and (np.abs(off).sum(1) >= 1).all()
+    ids, ndof = pg.generate_dof_ids(conn, X.shape[0], codes, Pr)
+    ido, ndofo = oracle.generate_dof_ids(conn, X.shape[0], codes, Pr)
+    assert ndof == ndofo == 726 and np.array_equal(ids, ido)
+    sl = np.where(Pr >= 0)[0]
+    assert np.array_equal(ids[sl], ids[Pr[sl]])
+    Ap, Ai = pg.psparse_apai(conn, ids, ndof)
+    Apo, Aio = oracle.psparse_apai(conn, ido, ndofo)
+    assert np.array_equal(Ap, Apo) and np.array_equal(Ai[:Ap[-1]], Aio[:Apo[-1]])
+    F0 = np.array([[0.01, 0.004, 0.0], [0.004, -0.005, 0.002], [0.0, 0.002, 0.003]])
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai, F0=F0.ravel())
+    mat = oracle.material(oracle.HE, E=d["Ex"], nu=d["nyz"])
+    u = np.random.default_rng(0).uniform(-1e-4, 1e-4, ndof)
+    err, R, K, _ = P.assemble(mat, u, np.array(d["defl"]))
+    assert err == 0 and np.isfinite(R).all() and np.isfinite(K).all() and np.abs(R).max() > 0
