@@ -456,7 +456,9 @@ int pgfem_input_get_periodic(const pgfem_input *in, long *Pr);
 void pgfem_input_destroy(pgfem_input *in);
 /* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
  * composition the reference states at src/plasticity_model.cc:1252-1255; its
- * rotation_matrix_of_Euler_angles lives in an absent library). */
+ * rotation_matrix_of_Euler_angles lives in an absent library).  With this R
+ * the reference's crystal plasticity tension case reproduces its own restart
+ * output; the transpose does not. */
 int pgfem_euler_rotation(long n, const double *angles, double *R);
 
 typedef struct {
