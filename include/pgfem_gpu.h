@@ -457,8 +457,10 @@ void pgfem_input_destroy(pgfem_input *in);
 /* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
  * composition the reference states at src/plasticity_model.cc:1252-1255; its
  * rotation_matrix_of_Euler_angles lives in an absent library).  With this R
- * the reference's crystal plasticity tension case reproduces its own restart
- * output; the transpose does not. */
+ * the reference's crystal plasticity tension case (EulerAngleType 0)
+ * reproduces its own restart output; the transpose does not.  Other
+ * EulerAngleType values select conventions of that library that no reference
+ * output pins; callers check the type pgfem_input_read_orientations returns. */
 int pgfem_euler_rotation(long n, const double *angles, double *R);
 
 typedef struct {
