@@ -477,7 +477,9 @@ typedef struct {
  * sizes): times[nt+1], print_steps[n_print], load_steps[n_load],
  * load_incr[n_load*n_incr], the prescribed-value increments the reference
  * reads while stepping, one per prescribed value of the mesh: pass the
- * mesh's npres as npd (the header's npres is a different count). */
+ * mesh's npres as npd (the header's npres is a different count).  A file that
+ * ends after the output steps has its load history in a load directory, which
+ * is not read (n_load = 0). */
 int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *sf, double *times,
                                  long *print_steps, long *load_steps, double *load_incr);
 

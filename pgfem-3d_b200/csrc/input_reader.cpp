@@ -574,6 +574,14 @@ int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *
     if (!t.num(v)) return bad("output step");
     if (print_steps) print_steps[k] = v;
   }
+  // no load section: the history is in a load directory (<input>/load/<physics>.load,
+  // src/read_input_file.cc:646-673), not read here
+  if (t.eof()) {
+    s.n_load = 0;
+    s.n_incr = npd >= 0 ? npd : s.npres;
+    *sf = s;
+    return PGFEM_GPU_OK;
+  }
   if (!t.num(s.n_load) || s.n_load < 0) return bad("load step count");
   for (long k = 0; k < s.n_load; k++) {
     long v;

@@ -154,6 +154,9 @@ def test_solver_files(tmp_path):
     r.write_text("1e-6 8 0 4\n1 3\n\n6 1 0.25\n\n2\n0 1 2\n\n1\n2\n\n0\n")
     sf, t, ps, ls, li = pg.read_solver_file(str(r))
     assert (sf.FNR, sf.physicsno, sf.max_NR_staggering, sf.max_subdivision, sf.nt) == (4, 1, 3, 6, 2)
+    r.write_text("1e-5 10 4 1 \n\n3\n0 1 2 3 \n\n3\n0 1 2 \n")  # load history in a load directory
+    sf, t, ps, ls, li = pg.read_solver_file(str(r), 0)
+    assert (sf.nt, sf.n_print, sf.n_load) == (3, 3, 0) and list(ps) == [0, 1, 2]
     r.write_text("1e-6 8 0 1\n\n3\n0 1\n")
     with pytest.raises(pg.PgfemError, match="EFORMAT.*time"):
         pg.read_solver_file(str(r))
