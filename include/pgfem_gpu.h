@@ -430,6 +430,17 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out);
  * <bc_base>.bcv (e.g. bc_base = "<input dir>/BC/Mechanical"); the mesh files'
  * own supports sections are read and ignored, as the reference does. */
 int pgfem_input_read_mesh_bc(const char *base, int nparts, const char *bc_base, pgfem_input **out);
+/* Multiphysics meshes: one supports section per physics in the order of
+ * multiphysics.in, ndim[k] codes per node (1 heat transfer, 3 mechanics);
+ * section `mech` (ndim 3) is kept.  With bc_base the mesh file holds a single
+ * supports section, which the BC directory's files replace (the reference's
+ * layout, src/read_input_file.cc:320-360). */
+int pgfem_input_read_mesh_mp(const char *base, int nparts, const char *bc_base, int nphys, const int *ndim,
+                             int mech, pgfem_input **out);
+/* multiphysics.in (read_multiphysics_settings, src/PGFem3D_data_structure.cc:
+ * 680-780): per physics in file order its id (0 mechanical, 1 thermal) and
+ * degrees of freedom per node; n = number of physics. */
+int pgfem_input_read_multiphysics(const char *path, int max_phys, int *ids, int *ndim, int *n);
 int pgfem_input_get_info(const pgfem_input *in, pgfem_input_info *info);
 /* X[nn*3], conn[ne*nne] (0-based merged ids), codes[nn*3] support codes
  * (0 free, 1 fixed, -k prescribed: the pgfem_generate_dof_ids input),

@@ -143,7 +143,17 @@ struct Part {
   long nln = 0, nel_s = 0, nel_v = 0;
 };
 
-int read_part(const std::string &path, Part &p) {
+// Physics layout of a mesh file: one supports section per physics, in the
+// order of multiphysics.in, each with ndim codes per node; the mechanical
+// section (ndim 3) is the one kept.
+struct PhysLayout {
+  int nphys = 1;
+  std::vector<int> ndim{3};
+  int mech = 0;
+  bool multiphysics = false;  // the header's ndofn then counts every physics
+};
+
+int read_part(const std::string &path, Part &p, const PhysLayout &L) {
   Tokens t;
   if (!t.load(path)) return fail("cannot open " + path);
   auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
@@ -151,7 +161,8 @@ int read_part(const std::string &path, Part &p) {
   if (!t.num(p.lin_maxit) || !t.num(p.lin_err) || !t.num(p.lim_zero)) return bad("solver header");
   if (!t.num(p.nmat) || !t.num(p.nconc) || !t.num(p.norient)) return bad("material header");
   if (p.nn <= 0 || p.ne < 0 || p.nmat < 0 || p.nconc < 0 || p.norient < 0) return bad("header sizes");
-  if (p.ndofn != 3) return fail(path + ": ndofn " + std::to_string(p.ndofn) + " (the mechanical path has 3)");
+  if (!L.multiphysics && p.ndofn != 3)
+    return fail(path + ": ndofn " + std::to_string(p.ndofn) + " (the mechanical path has 3)");
   p.toe.resize(p.ne);
   for (long e = 0; e < p.ne; e++)
     if (!t.num(p.toe[e])) return bad("element type line");
@@ -170,21 +181,36 @@ int read_part(const std::string &path, Part &p) {
     p.dom[id] = d;
     for (int j = 0; j < 3; j++) p.X[3 * id + j] = x[j];
   }
-  // supports and prescribed values
-  long nsup;
-  if (!t.num(nsup) || nsup < 0) return bad("support count");
+  // supports and prescribed values, one section per physics (read_supports,
+  // src/read_input_file.cc:362-370); the mechanical section is kept
+  long npd = 0;
   p.codes.assign(3 * p.nn, 0);
-  for (long k = 0; k < nsup; k++) {
-    long n;
-    if (!t.num(n) || n < 0 || n >= p.nn) return bad("support node");
-    for (int j = 0; j < 3; j++)
-      if (!t.num(p.codes[3 * n + j])) return bad("support code");
+  for (int ph = 0; ph < L.nphys; ph++) {
+    const bool keep = ph == L.mech;
+    const int nd = L.ndim[ph];
+    long nsup;
+    if (!t.num(nsup) || nsup < 0) return bad("support count");
+    for (long k = 0; k < nsup; k++) {
+      long n;
+      if (!t.num(n) || n < 0 || n >= p.nn) return bad("support node");
+      for (int j = 0; j < nd; j++) {
+        long c;
+        if (!t.num(c)) return bad("support code");
+        if (keep) p.codes[3 * n + j] = c;
+      }
+    }
+    long np_;
+    if (!t.num(np_) || np_ < 0) return bad("prescribed count");
+    if (keep) {
+      npd = np_;
+      p.defl.resize(npd);
+    }
+    for (long k = 0; k < np_; k++) {
+      double v;
+      if (!t.num(v)) return bad("prescribed value");
+      if (keep) p.defl[k] = v;
+    }
   }
-  long npd;
-  if (!t.num(npd) || npd < 0) return bad("prescribed count");
-  p.defl.resize(npd);
-  for (long k = 0; k < npd; k++)
-    if (!t.num(p.defl[k])) return bad("prescribed value");
   for (long n = 0; n < p.nn; n++)
     for (int j = 0; j < 3; j++) {
       const long c = p.codes[3 * n + j];
@@ -307,11 +333,27 @@ int pgfem_input_read_mesh(const char *base, int nparts, pgfem_input **out) {
 }
 
 int pgfem_input_read_mesh_bc(const char *base, int nparts, const char *bc_base, pgfem_input **out) {
-  if (!base || nparts < 1 || !out) return PGFEM_GPU_EINVAL;
+  const int ndim = 3;
+  return pgfem_input_read_mesh_mp(base, nparts, bc_base, 1, &ndim, 0, out);
+}
+
+int pgfem_input_read_mesh_mp(const char *base, int nparts, const char *bc_base, int nphys, const int *ndim,
+                             int mech, pgfem_input **out) {
+  if (!base || nparts < 1 || !out || nphys < 1 || !ndim || mech < 0 || mech >= nphys || ndim[mech] != 3)
+    return PGFEM_GPU_EINVAL;
+  for (int k = 0; k < nphys; k++)
+    if (ndim[k] < 1 || ndim[k] > 3) return PGFEM_GPU_EINVAL;
+  PhysLayout L;
+  if (!bc_base) {
+    L.nphys = nphys;
+    L.ndim.assign(ndim, ndim + nphys);
+    L.mech = mech;
+  }  // with a BC directory the mesh file holds one supports section, read and replaced
+  L.multiphysics = nphys > 1;
   *out = nullptr;
   std::vector<Part> parts(nparts);
   for (int r = 0; r < nparts; r++) {
-    int e = read_part(std::string(base) + std::to_string(r) + ".in", parts[r]);
+    int e = read_part(std::string(base) + std::to_string(r) + ".in", parts[r], L);
     if (!e && bc_base) e = read_bc_files(bc_base, r, parts[r]);
     if (e) return e;
   }
@@ -537,6 +579,36 @@ int pgfem_euler_rotation(long n, const double *angles, double *R) {
       for (int j = 0; j < 3; j++)
         Rk[i * 3 + j] = Az[i * 3] * T[j] + Az[i * 3 + 1] * T[3 + j] + Az[i * 3 + 2] * T[6 + j];
   }
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_read_multiphysics(const char *path, int max_phys, int *ids, int *ndim, int *n) {
+  if (!path || !n || max_phys < 0 || (max_phys && (!ids || !ndim))) return PGFEM_GPU_EINVAL;
+  Tokens t;
+  if (!t.load(path)) return fail(std::string("cannot open ") + path);
+  auto bad = [&](const char *what) { return fail(std::string("bad ") + what + " at " + t.where()); };
+  int np;
+  if (!t.num(np) || np < 1) return bad("physics count");
+  for (int k = 0; k < np; k++) {
+    int id, nd, nc, nv;
+    std::string name;
+    if (!t.num(id) || !t.next(name) || !t.num(nd)) return bad("physics line (id name ndim)");
+    if (!t.num(nc) || nc < 0) return bad("coupling count");
+    for (int j = 0; j < nc; j++) {
+      int c;
+      if (!t.num(c)) return bad("coupled physics id");
+    }
+    if (!t.num(nv) || nv < 0) return bad("output variable count");
+    for (int j = 0; j < nv; j++) {
+      int v;
+      if (!t.num(v)) return bad("output variable id");
+    }
+    if (k < max_phys) {
+      ids[k] = id;
+      ndim[k] = nd;
+    }
+  }
+  *n = np;
   return PGFEM_GPU_OK;
 }
 

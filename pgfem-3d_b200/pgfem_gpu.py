@@ -124,6 +124,8 @@ def lib():
             "pgfem_input_last_error": (C.c_char_p, []),
             "pgfem_input_read_mesh": (C.c_int, [C.c_char_p, C.c_int, _P]),
             "pgfem_input_read_mesh_bc": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, _P]),
+            "pgfem_input_read_mesh_mp": (C.c_int, [C.c_char_p, C.c_int, C.c_char_p, C.c_int, _P, C.c_int, _P]),
+            "pgfem_input_read_multiphysics": (C.c_int, [C.c_char_p, C.c_int, _P, _P, _P]),
             "pgfem_input_get_info": (C.c_int, [_P, _P]),
             "pgfem_input_get_mesh": (C.c_int, [_P, _P, _P, _P, _P]),
             "pgfem_input_get_elements": (C.c_int, [_P, _P, _P, _P, _P]),
@@ -641,12 +643,20 @@ class InputMesh:
     partitions merged: X (nn,3), conn (ne,nne), codes (nn,3) support codes,
     defl (npres,), per-element material / partition data, material lines."""
 
-    def __init__(self, base, nparts=1, bc_base=None):
+    def __init__(self, base, nparts=1, bc_base=None, physics=None):
         """bc_base: supports and prescribed values from <bc_base>_<r>.bc and
-        <bc_base>.bcv (a BC directory) instead of the mesh files."""
+        <bc_base>.bcv (a BC directory) instead of the mesh files.  physics:
+        (ids, ndim) of a multiphysics mesh (read_multiphysics); the mechanical
+        supports section (id 0) is kept."""
         h = C.c_void_p()
-        _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh_bc(
-            base.encode(), nparts, None if bc_base is None else bc_base.encode(), C.byref(h)))
+        bc = None if bc_base is None else bc_base.encode()
+        if physics is None:
+            _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh_bc(base.encode(), nparts, bc, C.byref(h)))
+        else:
+            ids, nd = physics
+            nd = np.ascontiguousarray(nd, dtype=np.int32)
+            _check_input("pgfem_input_read_mesh", lib().pgfem_input_read_mesh_mp(
+                base.encode(), nparts, bc, len(nd), _ptr(nd), list(ids).index(0), C.byref(h)))
         try:
             info = InputInfo()
             _check("pgfem_input_get_info", lib().pgfem_input_get_info(h, C.byref(info)))
@@ -717,6 +727,16 @@ class InputMesh:
         ids, ndof = generate_dof_ids(self.conn, self.X.shape[0], self.codes, Pr)
         Ap, Ai = psparse_apai(self.conn, ids, ndof)
         return ids, ndof, Ap, Ai
+
+
+def read_multiphysics(path, max_phys=16):
+    """(ids, ndim) per physics in file order (0 mechanical, 1 thermal)."""
+    ids = np.zeros(max_phys, dtype=np.int32)
+    nd = np.zeros(max_phys, dtype=np.int32)
+    n = C.c_int()
+    _check_input("pgfem_input_read_multiphysics",
+                 lib().pgfem_input_read_multiphysics(path.encode(), max_phys, _ptr(ids), _ptr(nd), C.byref(n)))
+    return ids[:n.value].tolist(), nd[:n.value].tolist()
 
 
 def read_solver_file(path, npd=-1):

@@ -20,9 +20,12 @@ def material_line(Ex, nu, dev_pot, vol_pot, Ey=0.0, Ez=0.0, G=0.0):
     return " ".join("%.17g" % x for x in v) + " %d %d" % (dev_pot, vol_pot)
 
 
-def write_mesh(path, X, conn, codes, defl, mat_lines, gnn=None, dom=None, elem_mat=None, local_order=None):
+def write_mesh(path, X, conn, codes, defl, mat_lines, gnn=None, dom=None, elem_mat=None, local_order=None,
+               before=()):
     """One mesh file.  gnn/dom per local node (default: Gnn = id, Dom = 0);
-    local_order: the order in which node lines are written (default 0..nn-1)."""
+    local_order: the order in which node lines are written (default 0..nn-1);
+    before: supports sections of other physics written ahead of the
+    mechanical one, each (codes (nn, ndim), values)."""
     nn, ne, nne = X.shape[0], conn.shape[0], conn.shape[1]
     gnn = np.arange(nn) if gnn is None else gnn
     dom = np.zeros(nn, dtype=int) if dom is None else dom
@@ -32,6 +35,11 @@ def write_mesh(path, X, conn, codes, defl, mat_lines, gnn=None, dom=None, elem_m
          " ".join([str(nne)] * ne), ""]
     for i in order:
         L.append("%d %d %d  %.17g %.17g %.17g 1 %d     0" % (gnn[i], dom[i], i, X[i, 0], X[i, 1], X[i, 2], i + 1))
+    for c_other, v_other in before:
+        c_other = np.asarray(c_other).reshape(nn, -1)
+        s_other = [i for i in range(nn) if np.any(c_other[i] != 0)]
+        L += ["", str(len(s_other))] + ["%d %s" % (i, " ".join(str(int(c)) for c in c_other[i])) for i in s_other]
+        L += ["", str(len(v_other)), " ".join("%.17g" % v for v in v_other)]
     sup = [i for i in range(nn) if np.any(codes[i] != 0)]
     L += ["", str(len(sup))] + ["%d  %d %d %d " % (i, *codes[i]) for i in sup]
     L += ["", str(len(defl)), " ".join("%.17g" % v for v in defl), ""]

@@ -302,3 +302,35 @@ def test_reference_fe2_micro_structure():
     u = np.random.default_rng(0).uniform(-1e-4, 1e-4, ndof)
     err, R, K, _ = P.assemble(mat, u, np.array(d["defl"]))
     assert err == 0 and np.isfinite(R).all() and np.isfinite(K).all() and np.abs(R).max() > 0
+
+
+def test_multiphysics_mesh_keeps_the_mechanical_supports(tmp_path):
+    """A heat-transfer + mechanics mesh (multiphysics.in lists heat transfer
+    first): the thermal supports section (one code per node) is stepped over
+    and the mechanical one kept."""
+    (tmp_path / "multiphysics.in").write_text("""# physics
+2
+1 heat_transfer 1
+0
+2
+0 1
+# mechanics
+0 solid_mechanics 3
+1 1
+4
+0 3 6 11
+""")
+    ids, nd = pg.read_multiphysics(str(tmp_path / "multiphysics.in"))
+    assert (ids, nd) == ([1, 0], [1, 3])
+    X, conn, _ = pg.mesh_box_tet(2, 4)
+    nn = X.shape[0]
+    codes = np.zeros((nn, 3), dtype=np.int64)
+    codes[X[:, 2] == 0.0] = 1
+    codes[X[:, 2] == 1.0, 2] = -1
+    tcodes = np.where(X[:, 0] == 0.0, -1, 0)
+    write_mesh(str(tmp_path / "mp_0.in"), X, conn, codes, [0.05], [material_line(2e5, 0.3, 1, 99)],
+               before=[(tcodes, [300.0])])
+    m = pg.InputMesh(str(tmp_path / "mp_"), 1, physics=(ids, nd))
+    assert np.array_equal(m.codes, codes) and list(m.defl) == [0.05]
+    with pytest.raises(pg.PgfemError, match="EFORMAT"):
+        pg.InputMesh(str(tmp_path / "mp_"), 1)  # read as single-physics: the layout does not fit
