@@ -513,6 +513,11 @@ int pgfem_restart_format(const char *path, long nn, long ne, int n_ip, int model
                          const double *u_n, const double *blocks);
 int pgfem_restart_parse(const char *path, long nn, long ne, int n_ip, int model, double *u_nm1, double *u_n,
                         double *blocks);
+/* One file per partition of a merged mesh, as the reference's ranks write
+ * them: <name>_<r>_<step>.res with the partition's nodes (its node map) and
+ * elements, from merged nodal u_nm1, u_n (nn*3) and blocks (ne*n_ip*block). */
+int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int step, int model, int n_ip,
+                                   const double *u_nm1, const double *u_n, const double *blocks);
 /* Context level.  Write: u_nm1, u_n free-DOF displacements at t_{n-1}, t_n
  * with their prescribed values; F per point is computed from them on the
  * device; CP pFn, g_n from the committed state (t_n) and pFnm1, g_nm1 from

@@ -815,3 +815,28 @@ int pgfem_restart_parse(const char *path, long nn, long ne, int n_ip, int model,
 }
 
 }  // extern "C"
+
+extern "C" {
+
+int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int step, int model, int n_ip,
+                                   const double *u_nm1, const double *u_n, const double *blocks) {
+  const int bs = pgfem_restart_block_size(model);
+  if (!in || !name || step < 0 || n_ip < 1 || bs < 0 || !u_nm1 || !u_n || !blocks) return PGFEM_GPU_EINVAL;
+  for (int r = 0; r < in->nparts; r++) {
+    const std::vector<long> &nm = in->node_map[r];
+    const long e0 = in->part_elem_off[r], ne = in->part_elem_off[r + 1] - e0;
+    std::vector<double> a(3 * nm.size()), b(3 * nm.size());
+    for (size_t i = 0; i < nm.size(); i++)
+      for (int j = 0; j < 3; j++) {
+        a[3 * i + j] = u_nm1[3 * nm[i] + j];
+        b[3 * i + j] = u_n[3 * nm[i] + j];
+      }
+    const std::string path = std::string(name) + "_" + std::to_string(r) + "_" + std::to_string(step) + ".res";
+    const int e = pgfem_restart_format(path.c_str(), (long)nm.size(), ne, n_ip, model, a.data(), b.data(),
+                                       blocks + (size_t)e0 * n_ip * bs);
+    if (e) return e;
+  }
+  return PGFEM_GPU_OK;
+}
+
+}  // extern "C"

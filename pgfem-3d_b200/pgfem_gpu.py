@@ -141,6 +141,7 @@ def lib():
             "pgfem_restart_format": (C.c_int, [C.c_char_p, C.c_long, C.c_long, C.c_int, C.c_int, _P, _P, _P]),
             "pgfem_restart_parse": (C.c_int, [C.c_char_p, C.c_long, C.c_long, C.c_int, C.c_int, _P, _P, _P]),
             "pgfem_gpu_write_restart": (C.c_int, [_P, C.c_char_p, _P, _P, _P, _P, _P]),
+            "pgfem_restart_write_partitions": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.c_int, _P, _P, _P]),
             "pgfem_gpu_read_restart": (C.c_int, [_P, C.c_char_p, _P, _P]),
         }
         for name, (res, args) in sig.items():
@@ -799,6 +800,16 @@ def restart_parse(path, model, nn, ne, n_ip):
     _check_input("pgfem_restart_parse", lib().pgfem_restart_parse(
         path.encode(), nn, ne, n_ip, model, _ptr(u_nm1), _ptr(u_n), _ptr(blocks)))
     return u_nm1, u_n, blocks
+
+
+def restart_write_partitions(inp, name, step, model, u_nm1, u_n, blocks):
+    """Per-partition restart files <name>_<r>_<step>.res of an InputMesh from
+    merged nodal u_nm1, u_n (nn, 3) and blocks (ne, n_ip, block_size)."""
+    u_nm1 = np.ascontiguousarray(u_nm1, dtype=np.float64)
+    u_n = np.ascontiguousarray(u_n, dtype=np.float64)
+    blocks = np.ascontiguousarray(blocks, dtype=np.float64)
+    _check_input("pgfem_restart_write_partitions", lib().pgfem_restart_write_partitions(
+        inp._h, name.encode(), step, model, blocks.shape[1], _ptr(u_nm1), _ptr(u_n), _ptr(blocks)))
 
 
 def write_restart(ctx, path, u_nm1, u_n, presc_nm1=None, presc_n=None, state_nm1=None):

@@ -32,3 +32,26 @@ def test_round_trip(tmp_path, model, bs):
         pg.restart_parse(path, other, nn, ne, nip)
     with pytest.raises(pg.PgfemError, match="EINVAL"):
         pg.restart_parse(path, pg.MODEL_J2, nn, ne, nip)
+
+
+def test_partition_files_of_a_merged_mesh(tmp_path):
+    """Per-partition files (the reference's one file per rank) from a merged
+    mesh: each holds its partition's nodes and elements; parsed back with the
+    partition sizes they equal the merged arrays sliced by the node maps."""
+    from input_files import material_line, write_partitions
+    X, conn, _ = pg.mesh_box_tet(2, 4)
+    parts = np.split(np.arange(conn.shape[0]), [17, 30])
+    base = str(tmp_path / "box_")
+    write_partitions(base, X, conn, np.zeros((X.shape[0], 3), dtype=np.int64), [], [material_line(2e5, 0.3, 1, 2)],
+                     parts)
+    m = pg.InputMesh(base, 3)
+    rng = np.random.default_rng(3)
+    nn, ne = m.info.nn, m.info.ne
+    u1, u2 = rng.normal(size=(nn, 3)), rng.normal(size=(nn, 3))
+    blocks = rng.normal(size=(ne, 1, 64))
+    name = str(tmp_path / "box")
+    pg.restart_write_partitions(m, name, 49, pg.MODEL_CP, u1, u2, blocks)
+    for r in range(3):
+        nm, e0, ne_r = m.partition(r)
+        a, b, c = pg.restart_parse("%s_%d_49.res" % (name, r), pg.MODEL_CP, len(nm), ne_r, 1)
+        assert np.array_equal(a, u1[nm]) and np.array_equal(b, u2[nm]) and np.array_equal(c, blocks[e0:e0 + ne_r])
