@@ -9,8 +9,8 @@ model_params.in (crystal plasticity parameters), CO/co_<r>.in (grain
 orientations) and box_0.in.st_tension (time steps and the prescribed-value
 increments of its 49 load steps) and the reference's own output of that run,
 ref_out_tension/box_<r>_49.res (restart files of step 49: the nodal
-displacements u_n and per element the plastic deformation gradient pF_n and the
-slip resistance g_n, read with this library's restart parser and put in merged
+displacements u_n and per element the deformation gradient F_n, the plastic
+deformation gradient pF_n and the slip resistance g_n, read with this library's restart parser and put in merged
 node / element order through the reader's partition maps), and writes
 tests/golden/cp_box_tension.json.
 """
@@ -34,6 +34,7 @@ def main(ref):
     angles, etype = m.orientations(os.path.join(cp, mp.ort_file.decode()))
     sf, times, _, load_steps, incr = pg.read_solver_file(os.path.join(cp, "box_0.in.st_tension"), m.info.npres)
     pF49 = [None] * m.info.ne
+    F49 = [None] * m.info.ne
     g49 = [None] * m.info.ne
     u49 = [None] * m.info.nn
     for r in range(8):
@@ -46,6 +47,7 @@ def main(ref):
             assert max(abs(x - y) for x, y in zip(u49[n], un[i])) < 1e-12  # shared nodes agree
         for k in range(ne):
             blk = b[k, 0]
+            F49[e0 + k] = blk[0:9].tolist()
             pF49[e0 + k] = blk[18:27].tolist()
             g49[e0 + k] = float(blk[60])
     d = dict(X=m.X.tolist(), conn=m.conn.tolist(), codes=m.codes.tolist(), defl=m.defl.tolist(),
@@ -53,7 +55,7 @@ def main(ref):
              volPotFlag=int(m.vol_pot[0]), cp_params=list(mp.p)[:mp.np], euler_type=etype,
              angles=angles.tolist(), nor_min=sf.nor_min, times=times.tolist(),
              load_steps=load_steps[:NSTEPS].tolist(), load_incr=incr[:NSTEPS].tolist(),
-             ref_step=49, ref_pF=pF49, ref_g=g49, ref_u=u49,
+             ref_step=49, ref_F=F49, ref_pF=pF49, ref_g=g49, ref_u=u49,
              source="verification_tests/crystal_plasticity/{box_8CPU_tension/box_<r>.in, model_params.in, "
                     "CO/co_<r>.in, box_0.in.st_tension, ref_out_tension/box_<r>_49.res}")
     out = os.path.join(HERE, "cp_box_tension.json")

@@ -3,8 +3,9 @@
 (1) box patch test (below); (2) the crystal plasticity tension case of
 verification_tests/crystal_plasticity: its 8-partition mesh, grain
 orientations, parameters and 50 load steps, against the state the reference
-wrote in its step-49 restart files (nodal displacements, slip resistance and
-plastic deformation gradient of every element).
+wrote in its step-49 restart files (nodal displacements, deformation gradient,
+slip resistance and plastic deformation gradient of every element), including
+the reference's own numdiff criterion (1e-5) on u_n, F_n and pF_n.
 
 The reference's box patch test (tests/box/tension_disp, run by
 tests/box/common.sh.in) stretches the unit box to twice its length with the
@@ -135,6 +136,19 @@ def test_crystal_plasticity_box_matches_reference_restart():
     g_ref, pF_ref = np.array(d["ref_g"]), np.array(d["ref_pF"])
     assert np.abs(st[:, 9] - g_ref).max() <= CP_REF_G_RTOL * g_ref.max()
     assert np.abs(st[:, :9] - pF_ref).max() <= CP_REF_PF_ATOL
-    assert np.abs(nodal_total(ids, u, presc) - np.array(d["ref_u"])).max() <= CP_REF_U_ATOL
+    un = nodal_total(ids, u, presc)
+    assert np.abs(un - np.array(d["ref_u"])).max() <= CP_REF_U_ATOL
+    # the reference's own test criterion on its restart files (numdiff, absolute
+    # or relative 1e-5): every u_n and F_n entry, and 99 % of the pF_n entries
+    def numdiff_pass(a, b):
+        ad = np.abs(a - b)
+        return (ad <= 1e-5) | (ad <= 1e-5 * np.abs(b))
+    dN = np.array([[-1.0, -1, -1], [1, 0, 0], [0, 1, 0], [0, 0, 1]])
+    dX = np.einsum("eai,ac->eic", X[conn], dN)
+    dU = np.einsum("eai,ac->eic", un[conn], dN)
+    F = (np.eye(3) + dU @ np.linalg.inv(dX)).reshape(-1, 9)
+    assert numdiff_pass(un, np.array(d["ref_u"])).all()
+    assert numdiff_pass(F, np.array(d["ref_F"])).all()
+    assert numdiff_pass(st[:, :9], pF_ref).mean() >= 0.99
     # the comparison is sharp: the plastic part of pF is 200x the tolerance
     assert np.abs(pF_ref - np.eye(3).ravel()).max() > 200 * CP_REF_PF_ATOL
