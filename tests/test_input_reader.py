@@ -334,3 +334,41 @@ def test_multiphysics_mesh_keeps_the_mechanical_supports(tmp_path):
     assert np.array_equal(m.codes, codes) and list(m.defl) == [0.05]
     with pytest.raises(pg.PgfemError, match="EFORMAT"):
         pg.InputMesh(str(tmp_path / "mp_"), 1)  # read as single-physics: the layout does not fit
+
+
+def test_entry_points_reject_bad_arguments(tmp_path):
+    """Null handles, null outputs and out-of-range arguments return EINVAL
+    (no crash) from every reader and restart entry point."""
+    import ctypes as C
+    L = pg.lib()
+    EINVAL = -1
+    h = C.c_void_p()
+    assert L.pgfem_input_read_mesh(None, 1, C.byref(h)) == EINVAL
+    assert L.pgfem_input_read_mesh(b"x_", 0, C.byref(h)) == EINVAL
+    assert L.pgfem_input_read_mesh(b"x_", 1, None) == EINVAL
+    one = np.array([3], dtype=np.int32)
+    assert L.pgfem_input_read_mesh_mp(b"x_", 1, None, 1, one.ctypes.data, 1, C.byref(h)) == EINVAL  # mech out of range
+    bad = np.array([2], dtype=np.int32)
+    assert L.pgfem_input_read_mesh_mp(b"x_", 1, None, 1, bad.ctypes.data, 0, C.byref(h)) == EINVAL  # mechanics needs 3
+    assert L.pgfem_input_get_info(None, None) == EINVAL
+    assert L.pgfem_input_get_mesh(None, None, None, None, None) == EINVAL
+    assert L.pgfem_input_get_elements(None, None, None, None, None) == EINVAL
+    assert L.pgfem_input_get_periodic(None, None) == EINVAL
+    assert L.pgfem_input_get_partition(None, 0, None, None, None) == EINVAL
+    assert L.pgfem_input_read_orientations(None, b"co", None, None) == EINVAL
+    assert L.pgfem_euler_rotation(-1, None, None) == EINVAL
+    n = C.c_int()
+    assert L.pgfem_input_read_model_params(None, 0, None, C.byref(n)) == EINVAL
+    assert L.pgfem_input_read_multiphysics(None, 0, None, None, C.byref(n)) == EINVAL
+    assert L.pgfem_input_read_solver_file(None, -1, None, None, None, None, None) == EINVAL
+    assert L.pgfem_restart_block_size(pg.MODEL_J2) < 0
+    assert L.pgfem_restart_format(None, 1, 1, 1, pg.MODEL_HE, None, None, None) == EINVAL
+    assert L.pgfem_restart_parse(b"x.res", 1, 1, 0, pg.MODEL_HE, None, None, None) == EINVAL
+    assert L.pgfem_restart_write_partitions(None, b"x", 0, pg.MODEL_CP, 1, None, None, None) == EINVAL
+    # a valid handle with a partition out of range
+    from input_files import write_box_fixture
+    base = str(tmp_path / "box_")
+    write_box_fixture(base, "LT")
+    m = pg.InputMesh(base, 1)
+    assert L.pgfem_input_get_partition(m._h, 1, None, None, None) == EINVAL
+    assert L.pgfem_input_get_partition(m._h, -1, None, None, None) == EINVAL
