@@ -167,7 +167,7 @@ def measured_hbm_gbs():
 def traffic_per_launch():
     """dram bytes of one R+K iterate's two kernels (point updates, then the
     assembly) from the committed ncu summary of the J2 quadratic-tet workload."""
-    path = os.path.join(ROOT, "profiles", "k_assemble_p2r_j2_p2_traffic.txt")
+    path = os.path.join(ROOT, "profiles", "k_assemble_p2m_j2_p2_traffic.txt")
     if not os.path.exists(path):
         return None
     for ln in open(path):
@@ -210,8 +210,7 @@ def run_ours(args, ws, rank, local):
     ctx = p.context()
     log("[rank %d] context (device copy + element->CSR map) %.1f s, %.2f GB on device"
         % (rank, time.perf_counter() - t0, ctx.device_bytes() / 1e9))
-    ctx.set_scatter_mode({"atomic": pg.SCATTER_ATOMIC, "colour": pg.SCATTER_COLOUR,
-                          "tiles": pg.SCATTER_TILES, "cells": pg.SCATTER_CELLS}[args.scatter])
+    ctx.set_scatter_mode({"atomic": pg.SCATTER_ATOMIC, "colour": pg.SCATTER_COLOUR}[args.scatter])
     fp64_peak = pg.fp64_peak_tflops()
     hbm_peak, hbm_src = measured_hbm_gbs()
 
@@ -287,7 +286,7 @@ def run_ours(args, ws, rank, local):
                 "peak_source": hbm_src}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["kernel"] = ("k_assemble<4,1,0> (fused R+K)" if he else
-                      "k_qp_update<10,4,1> + k_assemble_p2r<1> (point updates, then R+K)")
+                      "k_qp_update<10,4,1,1> + k_assemble_p2m<1> (point updates, then R+K on the FP64 tensor cores)")
     roof["traffic"] = None if he else traffic_per_launch()
     roof["kernel_ms"] = k_ms
     roof["roofline_ms"] = 1e3 * max(t_fp64, t_hbm)
@@ -919,7 +918,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour", "tiles", "cells"])
+    ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour"])
     ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch",
                                                          "nr_step"])
     ap.add_argument("--nr-n", type=int, default=16)

@@ -52,16 +52,9 @@ enum {
 int pgfem_gpu_state_size(int model);
 
 /* Scatter modes:
- *  ATOMIC  one fused kernel, FP64 atomic adds per element entry (default);
- *  COLOUR  element colours with plain adds (deterministic summation order);
- *  TILES   point-update kernel + persistent tile kernel that combines the
- *          blocks of a cell of elements in shared memory, issues address-
- *          ordered reductions and zero-fills the CSR rows a tile touches first
- *          instead of a full memset (2.3x less DRAM traffic per iterate);
- *  CELLS   quadratic tets: one fused kernel per Kuhn cell of 6 elements --
- *          point updates in registers, node-pair blocks combined in shared
- *          memory, address-ordered coalesced reductions. */
-enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1, PGFEM_SCATTER_TILES = 2, PGFEM_SCATTER_CELLS = 3 };
+ *  ATOMIC  FP64 atomic adds of every element entry (default);
+ *  COLOUR  element colours with plain adds (deterministic summation order). */
+enum { PGFEM_SCATTER_ATOMIC = 0, PGFEM_SCATTER_COLOUR = 1 };
 
 typedef struct {
   int model;

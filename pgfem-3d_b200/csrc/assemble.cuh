@@ -79,6 +79,10 @@ struct AsmArgs {
   // point records written by the point-update kernel (kRec x nqp, structure
   // of arrays), read by the two-kernel quadratic-tet assembly
   const double *qrec;
+  // per-element scatter blocks of the tensor-core quadratic-tet kernel
+  // (kEBW int32 words per element: row bases, residual indices, node-pair
+  // positions, free masks)
+  const int *eblk;
   Mat mat;
   ShapeTable shp;
 };

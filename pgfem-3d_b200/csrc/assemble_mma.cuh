@@ -1,0 +1,480 @@
+// assemble_mma.cuh -- FP64 R+K assembly of quadratic tets with the element
+// contraction on the FP64 tensor cores (mma.sync .m8n8k4 .f64).
+//
+// Same operation as the other assembly kernels (fd_residuals_MP +
+// stiffmat_fd_MP for the constitutive-model element, src/fd_residuals.cc:
+// 468-636, src/stiffmat_fd.cc:831-993), in two kernels:
+//
+//  k_qp_update<..., YREC = true>  one thread per quadrature point: F, the
+//      constitutive update (run_integration_algorithm,
+//      src/constitutive_model.cc:1100-1129; state n -> n+1) and a 40-double
+//      point record (structure of arrays) holding the matrices the element
+//      contraction needs:
+//        G = (dX/dxi)^-1 F^-1      (p_a = G^T dN_a/dxi = F^-T grad_X N_a)
+//        T' = a1 w/2 1 + w tau,  U' = w a2 1 - 2/3 w s,  W' = w (a4 n + a5 dev(n^2)),
+//        s'' = -2/3 w s,  n,  h = a1 w / 2
+//      for the spatial tangent c = a1 I + a2 1(x)1 - 2/3 (s(x)1 + 1(x)s)
+//      + a4 n(x)n + a5 n(x)dev(n^2) (cm_models.cuh) and w = det(dX/dxi) x weight.
+//
+//  k_assemble_p2m  persistent grid over tiles of 4 consecutive elements, four
+//      warps per CTA, one element per warp in the contraction.  With the
+//      vectors p, T = T'p, U = U'p, W = W'p, h p of node b at point q, the
+//      element block K_ab[i][k] (compute_stiffness_matrix,
+//      src/constitutive_model.cc:1520-1616, in spatial form) is
+//        K_ab[i][k] = sum_q sum_j p_a[j] Y_q[j][(b,i,k)],
+//        Y_q[j][(b,i,k)] = d_jk h p_b[i] + d_ij U_b[k] + s''_ij p_b[k]
+//                          + n_ij W_b[k] + d_ik T_b[j],
+//      and the residual R_a[i] = sum_q sum_j p_a[j] w tau_ij
+//      (compute_residual_vector, :1628-1662): one GEMM per element,
+//        C (96 x 10) = Y^T (96 x 12) P (12 x 10),  P[(q,j)][a] = p_qa[j],
+//      whose 96 rows are (i, b, k) in blocks of 32 per i (30 K columns, the
+//      residual, one pad) and whose 12-deep contraction runs over (q, j).
+//   Y  all threads: item (element, point, column node b) builds its 27 Y
+//      values and its p into shared memory (Y in the A-fragment order of the
+//      mma, so that each fragment load is 32 consecutive doubles), and the
+//      column offsets of node b's block in the rows of the element's nodes;
+//   C  warp per element: 36 mma.m8n8k4 for row nodes a = 0..7; rows 8 and 9
+//      from the same A fragments with FP64 FMAs (partial sums over the lane's
+//      contraction indices, combined by two shuffles);
+//   S  FP64 reductions of the 900 K entries and 30 R entries into the CSR
+//      through the node-block map (fd_res_assemble, src/fd_residuals.cc:58-73;
+//      PLoc_Sparse, src/PLoc_Sparse.cc:15-175).  Per reduction instruction a
+//      warp writes eight consecutive entries of four CSR rows.
+#pragma once
+#include <cstdint>
+
+#include "assemble.cuh"
+
+namespace pgb {
+
+constexpr int kQRec = kRec;  // point record of the linear-tet path: G 9, w, tau 6, s 6, n 6, dev(n^2) 6, a1 a2 a4 a5
+constexpr int kYRec = 40;  // point record of the tensor-core path: G 9, T' 6, U' 6, W' 6, s'' 6, n 6, h
+
+struct QpArgs {
+  const double *X;      // 3*nn
+  const double *unode;  // 3*nn
+  const int *conn;      // NNE*ne (SoA)
+  long nn, ne, nqp;
+  const double *F0;
+  const int *elem_group;  // FE2 batches: element -> group (or nullptr)
+  const double *F0_tab;   // group -> macro deformation (9)
+  const double *state_n;
+  double *state_np1;
+  double *qrec;         // kQRec*nqp or kYRec*nqp (SoA)
+  unsigned long long *status;
+  // processing order: record slot e' holds element perm[e'] (nullptr: e' = e);
+  // the state stays in element order
+  const int *perm;
+  Mat mat;
+  ShapeTable shp;
+};
+
+template <int NNE, int NQP, int MODEL, bool YREC = false>
+__global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
+  constexpr bool PLASTIC = (MODEL == 1);
+  constexpr int NR = YREC ? kYRec : kQRec;
+  const long qs = blockIdx.x * (long)blockDim.x + threadIdx.x;  // record slot
+  if (qs >= A.nqp) return;
+  const long es = qs / NQP;
+  const int q = (int)(qs - es * NQP);
+  const long e = A.perm ? (long)A.perm[es] : es;
+  const long qp = e * NQP + q;  // state index
+  double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int b = 0; b < NNE; b++) {
+    const int n = A.conn[(long)b * A.ne + e];
+    const double g0 = A.shp.dNxi[q][b][0], g1 = A.shp.dNxi[q][b][1], g2 = A.shp.dNxi[q][b][2];
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const double x = A.X[i * A.nn + n], u = A.unode[i * A.nn + n];
+      dX[i * 3 + 0] += g0 * x;
+      dX[i * 3 + 1] += g1 * x;
+      dX[i * 3 + 2] += g2 * x;
+      dU[i * 3 + 0] += g0 * u;
+      dU[i * 3 + 1] += g1 * u;
+      dU[i * 3 + 2] += g2 * u;
+    }
+  }
+  double *rec = A.qrec;
+  const long S = A.nqp;
+  const double detJ = det3(dX);
+  double dXi[9], F[9], Fi[9];
+  bool ok = detJ > 0.0 && inv3(dX, dXi);
+  if (ok) {
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+      for (int j = 0; j < 3; j++)
+        F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] + dU[i * 3 + 1] * dXi[1 * 3 + j] +
+                       dU[i * 3 + 2] * dXi[2 * 3 + j];
+    const double *F0 = A.elem_group ? A.F0_tab + 9 * (long)A.elem_group[e] : A.F0;
+    if (F0)
+#pragma unroll
+      for (int i = 0; i < 9; i++) F[i] += F0[i];
+  }
+  const double J = ok ? det3(F) : -1.0;
+  if (ok) ok = J > 0.0 && inv3(F, Fi);
+  if (!ok) {
+    atomicAdd(&A.status[0], 1ull);
+#pragma unroll
+    for (int c = 0; c < NR; c++) rec[c * S + qs] = 0.0;
+    return;
+  }
+  double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
+  if (PLASTIC) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) Ast[c] = A.state_n[c * S + qp];
+    alpha = A.state_n[6 * S + qp];
+  }
+  QpTangent t;
+  double Anp1[6], alpha_np1;
+  spatial_update<PLASTIC>(A.mat, F, J, Ast, alpha, t, Anp1, &alpha_np1);
+  if (PLASTIC && A.state_np1) {
+#pragma unroll
+    for (int c = 0; c < 6; c++) A.state_np1[c * S + qp] = Anp1[c];
+    A.state_np1[6 * S + qp] = alpha_np1;
+  }
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+      rec[(i * 3 + j) * S + qs] =
+          dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] + dXi[i * 3 + 2] * Fi[2 * 3 + j];
+  const double w = detJ * A.shp.w[q];
+  if (YREC) {
+    const double h = 0.5 * t.a1 * w, c23 = (2.0 / 3.0) * w;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      const double d = c < 3 ? 1.0 : 0.0;
+      rec[(9 + c) * S + qs] = h * d + w * t.tau[c];
+      rec[(15 + c) * S + qs] = w * t.a2 * d - c23 * t.s[c];
+      rec[(21 + c) * S + qs] = w * (t.a4 * t.n[c] + t.a5 * t.D[c]);
+      rec[(27 + c) * S + qs] = -c23 * t.s[c];
+      rec[(33 + c) * S + qs] = t.n[c];
+    }
+    rec[39 * S + qs] = h;
+  } else {
+    rec[9 * S + qs] = w;
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      rec[(10 + c) * S + qs] = t.tau[c];
+      rec[(16 + c) * S + qs] = t.s[c];
+      rec[(22 + c) * S + qs] = t.n[c];
+      rec[(28 + c) * S + qs] = t.D[c];
+    }
+    rec[34 * S + qs] = t.a1;
+    rec[35 * S + qs] = t.a2;
+    rec[36 * S + qs] = t.a4;
+    rec[37 * S + qs] = t.a5;
+  }
+}
+
+// ---- tensor-core element assembly ------------------------------------------
+
+constexpr int kMTE = 4;                 // elements per tile (one per warp)
+constexpr int kMThreads = 32 * kMTE;    // 128
+constexpr int kMPts = kMTE * 4;         // points per tile
+// Y doubles per element: [kstep 3][row tile 12][lane 32], and P doubles per
+// element: [a 10][t 12]; both padded so that the item stores of a half-warp
+// (four column-node pairs x four points, possibly of two elements) hit 16
+// distinct banks
+constexpr int kMY = 3 * 12 * 32 + 12;
+constexpr int kMP = 10 * 12 + 4;
+constexpr int kMCS = 36;                // column-table row stride (words): lane loads hit 32 banks
+constexpr int kMCol = 10 * kMCS;        // column table per element: [a 10][rr = 3 b + k, 30 -> R, 31 -> pad]
+constexpr int kMMeta = kMTE * 10;       // (element, node) pairs per tile
+constexpr int kMColR = -2;              // column-table marker of the residual row
+// Per-element scatter block (int32 words, 464 bytes so that it copies in 16-byte chunks):
+//   [0, 30)    row base of (node a, component i): CSR offset of the row, -1 if not free
+//   [30, 60)   residual index of (a, i): free DOF id - 1, -1 if not free
+//   [60, 110)  node-pair positions pos[a][b] (uint16, column offset of b's block in a's rows)
+//   [110, 113) free-component masks of the ten nodes (bytes)
+constexpr int kEBW = 116;
+constexpr int kEBPos = 60, kEBMask = 110;
+
+inline size_t p2m_smem_bytes() {
+  return sizeof(double) * ((size_t)kMTE * kMY + (size_t)kMTE * kMP + (size_t)kYRec * kMPts) +
+         sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW;
+}
+
+// Builds the scatter blocks of all 10-node elements from the node arrays and
+// the element->CSR node-block map (thread per element).
+// Block slot e' holds element perm[e'] (the processing order).
+__global__ void k_build_eblock(const int *conn, long ne, const int *dof, long nn, const int *rowptr0,
+                               const int *rowlen, const uint8_t *mask, const uint16_t *pos, const int *perm,
+                               int *eb) {
+  const long es = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (es >= ne) return;
+  const long e = perm ? (long)perm[es] : es;
+  int *o = eb + es * kEBW;
+  uint16_t *o16 = reinterpret_cast<uint16_t *>(o + kEBPos);
+  uint8_t *o8 = reinterpret_cast<uint8_t *>(o + kEBMask);
+  for (int a = 0; a < 10; a++) {
+    const int n = conn[(long)a * ne + e];
+    const unsigned mk = mask[n];
+    for (int i = 0; i < 3; i++) {
+      const bool fr = (mk >> i) & 1u;
+      o[a * 3 + i] = fr ? rowptr0[n] + __popc(mk & ((1u << i) - 1u)) * rowlen[n] : -1;
+      o[30 + a * 3 + i] = fr ? dof[i * nn + n] - 1 : -1;
+    }
+    for (int b = 0; b < 10; b++) o16[a * 10 + b] = pos[(e * 10 + a) * 10 + b];
+    o8[a] = (uint8_t)mk;
+  }
+  o8[10] = o8[11] = 0;
+  o[113] = o[114] = o[115] = 0;
+}
+
+// index of Y[t][r] (t = 3q + j, r = 32 i + 3 b + k) in the fragment-ordered buffer
+__device__ __forceinline__ int y_idx(int t, int r) {
+  return (((t >> 2) * 12 + (r >> 3)) << 5) + ((r & 7) << 2) + (t & 3);
+}
+
+// D (8x8) += A (8x4, row) B (4x8, col), FP64.  Lane l holds A[l/4][l%4],
+// B[l%4][l/4], and C[l/4][2 (l%4) + c] in c<c>.
+__device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cpa4m(void *dst, const void *src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cpa16m(void *dst, const void *src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src)
+               : "memory");
+}
+
+// Item (point q, column nodes b0 and b0 + 5) of one element: p_b into P, the
+// 27 values Y_q[j][(b, i, k)] of each column node and, for b0 = 0, the
+// residual rows Y_q[j][32 i + 30] = w tau_ij.  rec: the point's record fields
+// with stride RS; dN: the shape-function derivatives of the point.
+// Y[t][r] sits at y_idx(t, r) = tb(t) + 128 i + gk(3 b + k) for r = 32 i + 3 b + k.
+template <bool PLASTIC, int RS>
+__device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3], int q, int b0, double *Y,
+                                         double *P) {
+  double G[9], Tm[6], Um[6], Wm[6], s2[6], nn[6];
+#pragma unroll
+  for (int c = 0; c < 9; c++) G[c] = rec[c * RS];
+#pragma unroll
+  for (int c = 0; c < 6; c++) {
+    Tm[c] = rec[(9 + c) * RS];
+    Um[c] = rec[(15 + c) * RS];
+    Wm[c] = PLASTIC ? rec[(21 + c) * RS] : 0.0;
+    s2[c] = rec[(27 + c) * RS];
+    nn[c] = PLASTIC ? rec[(33 + c) * RS] : 0.0;
+  }
+  const double h = rec[39 * RS];
+  int tb[3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    const int t = 3 * q + j;
+    tb[j] = (t >> 2) * 384 + (t & 3);
+  }
+  // full 3x3 index of a Voigt-stored symmetric matrix (xx yy zz yz xz xy)
+  auto vo = [](int i, int j) { return i == j ? i : 6 - i - j; };
+#pragma unroll
+  for (int half = 0; half < 2; half++) {
+    const int b = b0 + 5 * half;
+    const double g0 = dN[b][0], g1 = dN[b][1], g2 = dN[b][2];
+    double p[3], T[3], U[3], W[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int j = 0; j < 3; j++) p[j] = G[j] * g0 + G[3 + j] * g1 + G[6 + j] * g2;
+    smv(Tm, p, T);
+    smv(Um, p, U);
+    if (PLASTIC) smv(Wm, p, W);
+    int gk[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const int x = 3 * b + k;
+      gk[k] = ((x >> 3) << 5) + ((x & 7) << 2);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        double *Yjk = Y + tb[j] + gk[k];
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double y = s2[vo(i, j)] * p[k];
+          if (PLASTIC) y = fma(nn[vo(i, j)], W[k], y);
+          if (j == k) y = fma(h, p[i], y);
+          if (i == j) y += U[k];
+          if (i == k) y += T[j];
+          Yjk[128 * i] = y;
+        }
+      }
+      P[b * 12 + 3 * q + j] = p[j];
+    }
+  }
+  if (b0 == 0) {
+    // w tau = T' - h 1 (row r = 32 i + 30: offset 128 i + 120)
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) Y[tb[j] + 128 * i + 120] = Tm[vo(i, j)] - (i == j ? h : 0.0);
+  }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs args) {
+  constexpr int NNE = 10, NQP = 4, TE = kMTE, NT = kMThreads;
+  constexpr bool PLASTIC = (MODEL == 1);
+  extern __shared__ __align__(16) double msm[];
+  double *sY = msm;                                          // [TE][kMY]
+  double *sP = sY + TE * kMY;                                // [TE][kMP]
+  double *sRec = sP + TE * kMP;                              // [kYRec][kMPts]
+  int *sCol = reinterpret_cast<int *>(sRec + kYRec * kMPts);  // [TE][10][kMCS]
+  int *sEB = sCol + TE * kMCol;                              // [2][TE][kEBW]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long ne = args.ne;
+  const long stride = (long)gridDim.x * TE;
+  // pad rows r = 32 i + 31 of Y stay zero; the column table marks the
+  // residual row (rr = 30) and the pad row (rr = 31)
+  for (int x = tid; x < TE * 12; x += NT) {
+    const int el = x / 12, t = x - el * 12;
+#pragma unroll
+    for (int i = 0; i < 3; i++) sY[el * kMY + y_idx(t, 32 * i + 31)] = 0.0;
+  }
+  for (int x = tid; x < TE * 10; x += NT) {
+    sCol[x * kMCS + 30] = kMColR;
+    sCol[x * kMCS + 31] = -1;
+  }
+
+  // asynchronous copies of one tile's point records and scatter blocks
+  // (16-byte chunks; nqp = 4 ne keeps every record chunk aligned)
+  auto issue = [&](long e0, int buf) {
+    const long qp0 = e0 * NQP;
+    for (int ch = tid; ch < kYRec * kMPts / 2; ch += NT) {
+      const int c = ch / (kMPts / 2), part = ch - c * (kMPts / 2);
+      if (e0 + part / 2 < ne) cpa16m(sRec + c * kMPts + part * 2, args.qrec + (long)c * args.nqp + qp0 + part * 2);
+    }
+    if (tid < TE * (kEBW / 4)) {
+      const int el = tid / (kEBW / 4), ch = tid - el * (kEBW / 4);
+      if (e0 + el < ne) cpa16m(sEB + (buf * TE + el) * kEBW + 4 * ch, args.eblk + (e0 + el) * kEBW + 4 * ch);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+
+  long e0 = (long)blockIdx.x * TE;
+  if (e0 < ne) issue(e0, 0);
+
+  for (int it = 0; e0 < ne; it++, e0 += stride) {
+    const int mb = it & 1;
+    asm volatile("cp.async.wait_all;" ::: "memory");
+    __syncthreads();  // records and scatter blocks of this tile landed; previous tile's C/S done
+    // ---- Y: items (element, column-node pair, point), point fastest ----
+    if (tid < TE * 20) {
+      const int el = tid / 20, rem = tid - el * 20;
+      const int bp = rem >> 2, q = rem & 3;
+      if (e0 + el < ne) {
+        p2m_item<PLASTIC, kMPts>(sRec + el * NQP + q, args.shp.dNxi[q], q, bp, sY + el * kMY, sP + el * kMP);
+        // column offsets of node b's block inside the rows of nodes a = q, q+4, q+8
+        const int *eb = sEB + (mb * TE + el) * kEBW;
+        const uint16_t *pos16 = reinterpret_cast<const uint16_t *>(eb + kEBPos);
+        const uint8_t *mk8 = reinterpret_cast<const uint8_t *>(eb + kEBMask);
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+          const int b = bp + 5 * half;
+          const unsigned maskB = mk8[b];
+          int *ct = sCol + el * kMCol + 3 * b;
+#pragma unroll
+          for (int x4 = 0; x4 < 3; x4++) {
+            const int a = q + 4 * x4;
+            if (a < NNE) {
+              const int pab = pos16[a * 10 + b];
+#pragma unroll
+              for (int k = 0; k < 3; k++)
+                ct[a * kMCS + k] = ((maskB >> k) & 1u) ? pab + rank_of(maskB, k) : -1;
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();  // Y, P and column offsets complete; the record buffer is free
+    // ---- prefetch the next tile's records and scatter blocks ----
+    if (e0 + stride < ne) issue(e0 + stride, mb ^ 1);
+    // ---- C: the element's GEMM on the FP64 tensor cores ----
+    // m8n8k4 for row nodes a = 0..7 (12 row tiles of 8 Y rows, 3 steps over
+    // the contraction); rows 8 and 9 from the same A fragments with FP64 FMAs
+    const int el = warp;
+    if (e0 + el >= ne) continue;
+    const double *Y = sY + el * kMY;
+    const double *P = sP + el * kMP;
+    const int rho = lane >> 2, u = lane & 3;
+    double acc[12][2], r8[12], r9[12];
+#pragma unroll
+    for (int m = 0; m < 12; m++) acc[m][0] = acc[m][1] = r8[m] = r9[m] = 0.0;
+#pragma unroll
+    for (int s = 0; s < 3; s++) {
+      const double bf = P[rho * 12 + 4 * s + u];
+      const double p8 = P[8 * 12 + 4 * s + u], p9 = P[9 * 12 + 4 * s + u];
+#pragma unroll
+      for (int m = 0; m < 12; m++) {
+        const double af = Y[(s * 12 + m) * 32 + lane];
+        dmma884(acc[m][0], acc[m][1], af, bf);
+        r8[m] = fma(p8, af, r8[m]);
+        r9[m] = fma(p9, af, r9[m]);
+      }
+    }
+    // rows 8, 9: sum the four lanes of a row group
+#pragma unroll
+    for (int m = 0; m < 12; m++) {
+      r8[m] += __shfl_xor_sync(0xffffffffu, r8[m], 1);
+      r9[m] += __shfl_xor_sync(0xffffffffu, r9[m], 1);
+      r8[m] += __shfl_xor_sync(0xffffffffu, r8[m], 2);
+      r9[m] += __shfl_xor_sync(0xffffffffu, r9[m], 2);
+    }
+    // ---- S: reductions into the CSR ----
+    // C[r][a], r = 8 m + rho = 32 i + rr: K entry (row i of node a, column rr
+    // of the column table) or, for rr = 30, the residual of (a, i); one
+    // reduction instruction per value, its target selected.
+    const int *eb = sEB + (mb * TE + el) * kEBW;
+    const int *ct = sCol + el * kMCol;
+    auto dst = [&](int rb, int rd, int cv) -> double * {
+      if (rb < 0) return nullptr;  // component i of node a is not free
+      if (cv >= 0) return args.K + (rb + cv);
+      return cv == kMColR ? args.R + rd : nullptr;
+    };
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+      const int a = 2 * u + c;
+      int rb[3], rd[3], cv[4];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        rb[i] = eb[a * 3 + i];
+        rd[i] = eb[30 + a * 3 + i];
+      }
+#pragma unroll
+      for (int mq = 0; mq < 4; mq++) cv[mq] = ct[a * kMCS + 8 * mq + rho];
+#pragma unroll
+      for (int m = 0; m < 12; m++) {
+        double *d = dst(rb[m >> 2], rd[m >> 2], cv[m & 3]);
+        if (d) atomicAdd(d, acc[m][c]);
+      }
+    }
+    {
+      // lane u of a row group takes the row tile m = 4 mm + u (row i = mm)
+      const int rr = 8 * u + rho;
+      const int cv8 = ct[8 * kMCS + rr], cv9 = ct[9 * kMCS + rr];
+#pragma unroll
+      for (int mm = 0; mm < 3; mm++) {
+        double v8 = r8[4 * mm], v9 = r9[4 * mm];
+#pragma unroll
+        for (int x = 1; x < 4; x++) {
+          v8 = u == x ? r8[4 * mm + x] : v8;
+          v9 = u == x ? r9[4 * mm + x] : v9;
+        }
+        double *d8 = dst(eb[24 + mm], eb[54 + mm], cv8);
+        double *d9 = dst(eb[27 + mm], eb[57 + mm], cv9);
+        if (d8) atomicAdd(d8, v8);
+        if (d9) atomicAdd(d9, v9);
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+}  // namespace pgb

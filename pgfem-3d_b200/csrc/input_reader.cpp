@@ -27,7 +27,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/pgfem_gpu.h"
+#include "pgfem_gpu.h"
 
 namespace {
 

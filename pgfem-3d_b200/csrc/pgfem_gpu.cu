@@ -20,10 +20,8 @@
 #include <vector>
 
 #include "assemble.cuh"
-#include "tile_plan.hpp"
-#include "assemble_tiles.cuh"
-#include "assemble_cells.cuh"
-#include "assemble_p2.cuh"
+#include "assemble_mma.cuh"
+#include "assemble_p1.cuh"
 #include "cm_integrate.cuh"
 #include "cp_kernels.cuh"
 #include "peak_probe.cuh"
@@ -58,20 +56,14 @@ struct pgfem_gpu_ctx {
   std::vector<long> colour_off;  // offsets into colour element list
   int *colour_elems = nullptr;
   long bytes = 0;
-  // tiled assembly plan (device copies)
-  bool tiles = false;
-  int tile_zero_mode = 0, nslots_max = 0;
-  long ntiles = 0;
-  int *t_nodes = nullptr;
-  uint8_t *t_nl = nullptr, *t_lnode = nullptr;
-  uint16_t *t_slot = nullptr, *t_aoff = nullptr;
-  long long *t_soff = nullptr, *t_zlo = nullptr, *t_zhi = nullptr;
-  uint32_t *t_sinfo = nullptr;
-  int *t_deps = nullptr;
-  uint8_t *t_allfree = nullptr;
-  unsigned *t_flags = nullptr, *t_ticket = nullptr;
-  unsigned epoch = 0;
-  double *qrec = nullptr;  // point records (kQRec x nqp)
+  double *qrec = nullptr;  // point records (kYRec x nqp for 10-node elements, kQRec x nqp for 4-node)
+  int *eblk = nullptr;     // scatter blocks of 10-node elements (kEBW words each), processing order
+  // tensor-core quadratic-tet path: processing order (slot -> element), and a
+  // second stream with fork/join events on which K is zeroed while the point
+  // kernel runs
+  int *perm = nullptr;
+  cudaStream_t zstream = nullptr;
+  cudaEvent_t zfork = nullptr, zjoin = nullptr;
   // crystal plasticity
   double *cp_R = nullptr, *cp_F = nullptr, *cp_detJw = nullptr, *cp_out = nullptr, *cp_guess = nullptr;
   int *cp_iters = nullptr;
@@ -294,13 +286,15 @@ void release(pgfem_gpu_ctx *c) {
   drop_events(c);
   void *ptrs[] = {c->X, c->conn, c->dof, c->rowptr0, c->rowlen, c->mask, c->pos, c->unode, c->F0,
                   c->state_n, c->state_np1, c->status, c->d_u, c->d_presc, c->d_R, c->d_K,
-                  c->colour_elems, c->t_nodes, c->t_nl, c->t_lnode, c->t_slot, c->t_aoff, c->t_soff,
-                  c->t_zlo, c->t_zhi, c->t_sinfo, c->t_deps, c->t_flags, c->t_ticket, c->qrec, c->t_allfree,
+                  c->colour_elems, c->qrec, c->eblk, c->perm,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket};
   for (void *p : ptrs)
     if (p) cudaFree(p);
+  if (c->zfork) cudaEventDestroy(c->zfork);
+  if (c->zjoin) cudaEventDestroy(c->zjoin);
+  if (c->zstream) cudaStreamDestroy(c->zstream);
   if (c->stream) cudaStreamDestroy(c->stream);
 }
 
@@ -363,11 +357,14 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
   return PGFEM_GPU_OK;
 }
 
-// Point updates of all quadrature points into c->qrec (allocated on first use).
+// Point updates of all quadrature points into c->qrec (allocated on first use;
+// 40-double records for the tensor-core quadratic-tet kernel, 38 for the
+// linear-tet kernels).
 template <int NNE, int NQP, int MODEL>
 int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
+  constexpr bool YREC = NNE == 10;
   if (!c->qrec) {
-    int r = dalloc(c, &c->qrec, (size_t)kQRec * c->nqp);
+    int r = dalloc(c, &c->qrec, (size_t)(YREC ? kYRec : kQRec) * c->nqp);
     if (r) return r;
   }
   QpArgs q{};
@@ -384,175 +381,42 @@ int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   q.state_np1 = c->state_np1;
   q.qrec = c->qrec;
   q.status = c->status;
+  if (YREC) q.perm = c->perm;
   q.mat = c->mat;
   q.shp = c->shp;
-  k_qp_update<NNE, NQP, MODEL><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
+  k_qp_update<NNE, NQP, MODEL, YREC><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
   CK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }
 
-template <int NNE, int NQP, int MODEL>
-int launch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
-  if (int r = launch_qp_update<NNE, NQP, MODEL>(c, s)) return r;
-  const size_t smem = tiles_smem_bytes<NNE, NQP>(c->nslots_max);
-  auto kern = k_assemble_tiles<NNE, NQP, MODEL>;
-  constexpr int T = tile_threads<NNE>();
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (!g_num_sms) grid_for(1, 1, 1);
-  const long grid = std::max<long>(1, std::min<long>(c->ntiles, (long)g_num_sms * per_sm));
-  TileArgs a{};
-  a.dof = c->dof;
-  a.rowptr0 = c->rowptr0;
-  a.rowlen = c->rowlen;
-  a.mask = c->mask;
-  a.nn = c->nn;
-  a.ne = c->ne;
-  a.nqp = c->nqp;
-  a.qrec = c->qrec;
-  a.tile_nodes = c->t_nodes;
-  a.tile_nl = c->t_nl;
-  a.elem_lnode = c->t_lnode;
-  a.elem_slot = c->t_slot;
-  a.slot_off = c->t_soff;
-  a.slot_info = c->t_sinfo;
-  a.aoff = c->t_aoff;
-  a.zlo = c->t_zlo;
-  a.zhi = c->t_zhi;
-  a.deps = c->t_deps;
-  a.allfree = c->t_allfree;
-  a.flags = c->t_flags;
-  a.ticket = c->t_ticket;
-  a.epoch = ++c->epoch;
-  a.zero_mode = c->tile_zero_mode;
-  a.zahead = (int)std::min<long>(c->ntiles, std::max<long>(64, (3 * grid) / 2));
-  a.ntiles = c->ntiles;
-  a.nslots_max = c->nslots_max;
-  a.R = d_R;
-  a.K = d_K;
-  a.status = c->status;
-  a.shp = c->shp;
-  CK(cudaMemsetAsync(c->t_ticket, 0, sizeof(unsigned), s));
-  kern<<<(unsigned)grid, T, smem, s>>>(a);
-  CK(cudaGetLastError());
-  return PGFEM_GPU_OK;
-}
-
+// quadratic tets in two kernels: point updates into c->qrec (40-double
+// records; K zeroed meanwhile on the context's second stream), then the
+// tensor-core element assembly from the records
 template <int MODEL>
-int launch_cells(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
-  const size_t smem = cells_smem_bytes(c->nslots_max);
-  auto kern = k_assemble_cells<MODEL>;
-  CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kCellThreads, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (!g_num_sms) grid_for(1, 1, 1);
-  const long grid = std::max<long>(1, std::min<long>(c->ntiles, (long)g_num_sms * per_sm));
-  CellArgs a{};
-  a.X = c->X;
-  a.unode = c->unode;
-  a.conn = c->conn;
-  a.nn = c->nn;
-  a.ne = c->ne;
-  a.nqp = c->nqp;
-  a.F0 = c->F0;
-  a.state_n = c->state_n;
-  a.state_np1 = c->state_np1;
-  a.dof = c->dof;
-  a.rowptr0 = c->rowptr0;
-  a.rowlen = c->rowlen;
-  a.mask = c->mask;
-  a.tile_nodes = c->t_nodes;
-  a.tile_nl = c->t_nl;
-  a.elem_lnode = c->t_lnode;
-  a.elem_slot = c->t_slot;
-  a.slot_off = c->t_soff;
-  a.slot_info = c->t_sinfo;
-  a.aoff = c->t_aoff;
-  a.allfree = c->t_allfree;
-  a.ntiles = c->ntiles;
-  a.nslots_max = c->nslots_max;
-  a.R = d_R;
-  a.K = d_K;
-  a.status = c->status;
-  a.mat = c->mat;
-  a.shp = c->shp;
-  kern<<<(unsigned)grid, kCellThreads, smem, s>>>(a);
-  CK(cudaGetLastError());
-  return PGFEM_GPU_OK;
-}
-
-int dispatch_tiles(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s) {
-  if (c->scatter_mode == PGFEM_SCATTER_CELLS)
-    return c->model == PGFEM_MODEL_J2 ? launch_cells<1>(c, d_R, d_K, s) : launch_cells<0>(c, d_R, d_K, s);
-  if (c->nne == 4)
-    return c->model == PGFEM_MODEL_J2 ? launch_tiles<4, 1, 1>(c, d_R, d_K, s) : launch_tiles<4, 1, 0>(c, d_R, d_K, s);
-  return c->model == PGFEM_MODEL_J2 ? launch_tiles<10, 4, 1>(c, d_R, d_K, s) : launch_tiles<10, 4, 0>(c, d_R, d_K, s);
-}
-
-template <int MODEL>
-int launch_p2(const AsmArgs &a, cudaStream_t s) {
-  const size_t smem = p2_smem_bytes();
-  auto kern = k_assemble_p2<MODEL>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kP2Threads, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (!g_num_sms) grid_for(1, 1, 1);
-  const long tiles = (a.ne + kP2TE - 1) / kP2TE;
-  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
-  kern<<<(unsigned)grid, kP2Threads, smem, s>>>(a);
-  CK(cudaGetLastError());
-  return PGFEM_GPU_OK;
-}
-
-template <int MODEL>
-int launch_p2ws(const AsmArgs &a, cudaStream_t s) {
-  const size_t smem = p2ws_smem_bytes();
-  auto kern = k_assemble_p2ws<MODEL>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWThreads, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (!g_num_sms) grid_for(1, 1, 1);
-  const long tiles = (a.ne + kWTE - 1) / kWTE;
-  const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
-  kern<<<(unsigned)grid, kWThreads, smem, s>>>(a);
-  CK(cudaGetLastError());
-  return PGFEM_GPU_OK;
-}
-
-// quadratic tets in two kernels: point updates into c->qrec, then the
-// pipelined assembly from the records
-template <int MODEL>
-int launch_p2r(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+int launch_p2m(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+  CK(cudaEventRecord(c->zfork, s));
+  CK(cudaStreamWaitEvent(c->zstream, c->zfork, 0));
+  CK(cudaMemsetAsync(a0.K, 0, sizeof(double) * c->nnz, c->zstream));
+  CK(cudaEventRecord(c->zjoin, c->zstream));
   if (int r = launch_qp_update<10, 4, MODEL>(c, s)) return r;
+  CK(cudaStreamWaitEvent(s, c->zjoin, 0));
   AsmArgs a = a0;
   a.qrec = c->qrec;
-  const size_t smem = p2r_smem_bytes();
-  auto kern = k_assemble_p2r<MODEL>;
+  a.eblk = c->eblk;
+  const size_t smem = p2m_smem_bytes();
+  auto kern = k_assemble_p2m<MODEL>;
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr_set = true;
   }
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kWThreads, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMThreads, smem));
   if (per_sm < 1) per_sm = 1;
   if (!g_num_sms) grid_for(1, 1, 1);
-  const long tiles = (a.ne + kWTE - 1) / kWTE;
+  const long tiles = (a.ne + kMTE - 1) / kMTE;
   const long grid = std::max<long>(1, std::min<long>(tiles, (long)g_num_sms * per_sm));
-  kern<<<(unsigned)grid, kWThreads, smem, s>>>(a);
+  kern<<<(unsigned)grid, kMThreads, smem, s>>>(a);
   CK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }
@@ -560,36 +424,6 @@ int launch_p2r(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
 // linear tets in two kernels: point updates into c->qrec, then the column-split
 // assembly from the records with the context's schedule (elements per block,
 // work stealing)
-template <int MODEL, int TE>
-int launch_p1r_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
-  AsmArgs a = a0;
-  a.qrec = c->qrec;
-  if (c->sched_grab > 0) {
-    a.ticket = c->sched_ticket;
-    a.grab = c->sched_grab;
-  }
-  const size_t smem = p1r_smem_bytes(TE);
-  auto kern = k_assemble_p1r<MODEL, TE>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
-  int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TE * 12, smem));
-  if (per_sm < 1) per_sm = 1;
-  if (!g_num_sms) grid_for(1, 1, 1);
-  const long tiles = (a.ne + TE - 1) / TE;
-  long grid = std::min<long>(tiles, (long)g_num_sms * per_sm * 8);
-  if (a.ticket) {  // persistent: every CTA resident, tiles claimed from the ticket
-    CK(cudaMemsetAsync(a.ticket, 0, sizeof(unsigned), s));
-    grid = std::min<long>(tiles, (long)g_num_sms * per_sm);
-  }
-  kern<<<(unsigned)std::max<long>(1, grid), TE * 12, smem, s>>>(a);
-  CK(cudaGetLastError());
-  return PGFEM_GPU_OK;
-}
-
 template <int MODEL, int TE>
 int launch_p1ws_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
   AsmArgs a = a0;
@@ -624,11 +458,6 @@ int launch_p1ws_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
 template <int MODEL>
 int launch_p1r(pgfem_gpu_ctx *c, const AsmArgs &a, cudaStream_t s) {
   if (int r = launch_qp_update<4, 1, MODEL>(c, s)) return r;
-  if (getenv("PGFEM_GPU_P1_SYNC")) {  // all threads run the phases of a tile in turn
-    if (c->sched_epb == 16) return launch_p1r_te<MODEL, 16>(c, a, s);
-    if (c->sched_epb == 64) return launch_p1r_te<MODEL, 64>(c, a, s);
-    return launch_p1r_te<MODEL, 32>(c, a, s);
-  }
   if (c->sched_epb == 16) return launch_p1ws_te<MODEL, 8>(c, a, s);
   if (c->sched_epb == 64) return launch_p1ws_te<MODEL, 32>(c, a, s);
   return launch_p1ws_te<MODEL, 16>(c, a, s);
@@ -642,19 +471,12 @@ int dispatch(pgfem_gpu_ctx *c, const AsmArgs &a, long nitems, cudaStream_t s) {
     return c->nne == 4 ? launch_asm<4, 1, 3, ATOMIC, WANT_K, DENSE>(a, nitems, s)
                        : launch_asm<10, 4, 3, ATOMIC, WANT_K, DENSE>(a, nitems, s);
   // quadratic tets, R+K into the CSR with atomic scatter over all elements:
-  // the column-split kernel, warp-specialised (PGFEM_GPU_P2_SYNC selects the
-  // variant in which all threads run the three phases of a tile in turn)
-  if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_ELEMENT_ROWS")) {
-    if (getenv("PGFEM_GPU_P2_SYNC"))
-      return c->model == PGFEM_MODEL_J2 ? launch_p2<1>(a, s) : launch_p2<0>(a, s);
-    if (getenv("PGFEM_GPU_P2_FUSED"))
-      return c->model == PGFEM_MODEL_J2 ? launch_p2ws<1>(a, s) : launch_p2ws<0>(a, s);
-    return c->model == PGFEM_MODEL_J2 ? launch_p2r<1>(c, a, s) : launch_p2r<0>(c, a, s);
-  }
+  // the point kernel + the tensor-core element assembly
+  if (c->nne == 10 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R)
+    return c->model == PGFEM_MODEL_J2 ? launch_p2m<1>(c, a, s) : launch_p2m<0>(c, a, s);
   // linear tets, R+K into the CSR with atomic scatter over all elements: the
   // point kernel + column-split assembly with the context's schedule
-  // (PGFEM_GPU_P1_NODE selects the per-node kernel below)
-  if (c->nne == 4 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R && !getenv("PGFEM_GPU_P1_NODE"))
+  if (c->nne == 4 && ATOMIC && WANT_K && !DENSE && !a.elist && a.R)
     return c->model == PGFEM_MODEL_J2 ? launch_p1r<1>(c, a, s) : launch_p1r<0>(c, a, s);
   // linear tets over all elements: the tuned schedule (elements per block,
   // work stealing)
@@ -786,14 +608,18 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   return PGFEM_GPU_OK;
 }
 
+// Whether an R+K call of this context runs the tensor-core quadratic-tet
+// path (the branch of dispatch() for 10-node elements, atomic scatter).
+bool uses_p2m(const pgfem_gpu_ctx *c) {
+  return c->eblk && c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2 && c->scatter_mode == PGFEM_SCATTER_ATOMIC;
+}
+
 // One assembly on device buffers (zeroing R and K first).
 int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
                     double *d_K, cudaStream_t s, double dt = 0.0) {
-  const bool use_cells = c->tiles && d_K && c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_CELLS;
-  const bool use_tiles = c->tiles && d_K && (c->scatter_mode == PGFEM_SCATTER_TILES || use_cells);
   if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
-  if (d_K && !(use_tiles && !use_cells && c->tile_zero_mode))
-    CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
+  // the tensor-core quadratic-tet path zeroes K itself, beside its point kernel
+  if (d_K && !(uses_p2m(c) && d_R)) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
   {
     const long n3 = 3 * c->nn;
     k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
@@ -818,9 +644,7 @@ int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, 
     CK(cudaEventRecord(e0, s));
   }
   int r = PGFEM_GPU_OK;
-  if (use_tiles) {
-    r = dispatch_tiles(c, d_R, d_K, s);
-  } else if (c->scatter_mode == PGFEM_SCATTER_COLOUR && c->colour_elems) {
+  if (c->scatter_mode == PGFEM_SCATTER_COLOUR && c->colour_elems) {
     for (size_t k = 0; k + 1 < c->colour_off.size() && !r; k++) {
       a.elist = c->colour_elems + c->colour_off[k];
       a.nlist = c->colour_off[k + 1] - c->colour_off[k];
@@ -893,6 +717,58 @@ void build_colours(const pgfem_mesh_desc *m, std::vector<int> &elems, std::vecto
   elems.resize(m->ne);
   std::vector<long> fill(off.begin(), off.end() - 1);
   for (long e = 0; e < m->ne; e++) elems[fill[colour[e]]++] = (int)e;
+}
+
+// Element processing order of the tensor-core quadratic-tet kernel: columns
+// of 32 x 32 element-size bins across the two shorter axes of the bounding
+// box, swept along the longest axis, bins in lexicographic order inside a
+// column (element centroids from the four vertex nodes; element size h =
+// (6 V / ne)^(1/3)).  Nearby elements share CSR rows, so in this order a row's
+// contributions arrive within about one column layer and its cache lines stay
+// in L2 between them (in the mesh's own order a whole cross-section is live).
+// Any permutation gives the same sums; this one only shapes the traffic.
+std::vector<int> locality_order(const pgfem_mesh_desc *m) {
+  const long ne = m->ne;
+  std::vector<double> cen((size_t)3 * ne);
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (long e = 0; e < ne; e++)
+    for (int d = 0; d < 3; d++) {
+      double x = 0.0;
+      for (int a = 0; a < 4; a++) x += m->X[(long)m->conn[e * m->nne + a] * 3 + d];
+      x *= 0.25;
+      cen[(size_t)3 * e + d] = x;
+      lo[d] = std::min(lo[d], x);
+      hi[d] = std::max(hi[d], x);
+    }
+  double vol = 1.0;
+  for (int d = 0; d < 3; d++) vol *= std::max(hi[d] - lo[d], 1e-300);
+  const double h = std::max(std::cbrt(6.0 * vol / (double)ne), 1e-300);
+  int sw = 2;  // sweep axis: the longest (ties: the last)
+  for (int d = 1; d >= 0; d--)
+    if (hi[d] - lo[d] > hi[sw] - lo[sw]) sw = d;
+  const int c1 = sw == 0 ? 1 : 0, c2 = sw == 2 ? 1 : 2;
+  auto bin = [&](long e, int d) {
+    const double v = (cen[(size_t)3 * e + d] - lo[d]) / h;
+    return (long)std::min(std::max(v, 0.0), 1.0e6);
+  };
+  const long nb1 = (long)((hi[c1] - lo[c1]) / h) + 1, nb2 = (long)((hi[c2] - lo[c2]) / h) + 1;
+  const long nbs = (long)((hi[sw] - lo[sw]) / h) + 1, T = 32;
+  const long nc2 = (nb2 + T - 1) / T;
+  std::vector<std::pair<unsigned long long, int>> key((size_t)ne);
+  for (long e = 0; e < ne; e++) {
+    const long b1 = bin(e, c1), b2 = bin(e, c2), bs = bin(e, sw);
+    const unsigned long long col = (unsigned long long)((b1 / T) * nc2 + b2 / T);
+    key[e].first = ((col * (unsigned long long)nbs + (unsigned long long)bs) * (unsigned long long)nb1 +
+                    (unsigned long long)b1) * (unsigned long long)nb2 + (unsigned long long)b2;
+    key[e].second = (int)e;
+  }
+  std::stable_sort(key.begin(), key.end(),
+                   [](const std::pair<unsigned long long, int> &x, const std::pair<unsigned long long, int> &y) {
+                     return x.first < y.first;
+                   });
+  std::vector<int> perm((size_t)ne);
+  for (long e = 0; e < ne; e++) perm[e] = key[e].second;
+  return perm;
 }
 
 }  // namespace
@@ -1018,6 +894,21 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if (ce != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
     if (herr) return fail(PGFEM_GPU_EPATTERN);
   }
+  // tensor-core quadratic-tet path: processing order, scatter blocks in that
+  // order, the second stream that zeroes K
+  if (m->nne == 10 && c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2) {
+    std::vector<int> perm = locality_order(m);
+    if ((r = upload(c, &c->perm, perm.data(), perm.size())) || (r = dalloc(c, &c->eblk, (size_t)ne * kEBW)))
+      return fail(r);
+    if (cudaStreamCreateWithFlags(&c->zstream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->zfork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->zjoin, cudaEventDisableTiming) != cudaSuccess)
+      return fail(PGFEM_GPU_ECUDA);
+    k_build_eblock<<<(unsigned)((ne + 127) / 128), 128, 0, c->stream>>>(c->conn, ne, c->dof, nn, c->rowptr0,
+                                                                       c->rowlen, c->mask, c->pos, c->perm, c->eblk);
+    if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(c->stream) != cudaSuccess)
+      return fail(PGFEM_GPU_ECUDA);
+  }
   // crystal plasticity buffers (rotations SoA, F, point outputs)
   if (c->model == PGFEM_MODEL_CP) {
     std::vector<double> Rs((size_t)9 * ne);
@@ -1032,40 +923,6 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     for (long q = 0; q < c->nqp; q++) Fn[0 * c->nqp + q] = Fn[4 * c->nqp + q] = Fn[8 * c->nqp + q] = 1.0;
     if ((r = upload(c, &c->cp_Fn, Fn.data(), Fn.size()))) return fail(r);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
-  }
-  // tiled assembly plan (HE / J2; not for the linear deviatoric potential,
-  // which only the per-node kernel carries)
-  if (c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2 && !getenv("PGFEM_GPU_NO_TILES")) {
-    std::vector<int> first_dof(nn, -1);
-    for (long n = 0; n < nn; n++)
-      for (int j = 0; j < 3 && first_dof[n] < 0; j++)
-        if (m->dof_id[n * 3 + j] > 0) first_dof[n] = (int)m->dof_id[n * 3 + j] - 1;
-    std::vector<int> conn_em(m->conn, m->conn + (size_t)ne * m->nne);
-    TilePlan P;
-    const int TE = m->nne == 10 ? TileCfg<10>::TE : TileCfg<4>::TE;
-    if (!build_tile_plan(P, TE, m->nne, ne, conn_em, first_dof, mask, Ap, Ai, m->ndof))
-      return fail(PGFEM_GPU_EPATTERN);
-    c->ntiles = P.ntiles;
-    c->nslots_max = P.nslots_max;
-    c->tile_zero_mode = P.first_touch ? 1 : 0;
-    if (getenv("PGFEM_GPU_TILE_MEMSET")) c->tile_zero_mode = 0;
-    if ((r = upload(c, &c->t_nodes, P.tile_nodes.data(), P.tile_nodes.size())) ||
-        (r = upload(c, &c->t_nl, P.tile_nl.data(), P.tile_nl.size())) ||
-        (r = upload(c, &c->t_lnode, P.elem_lnode.data(), P.elem_lnode.size())) ||
-        (r = upload(c, &c->t_slot, P.elem_slot.data(), P.elem_slot.size())) ||
-        (r = upload(c, &c->t_soff, P.slot_off.data(), P.slot_off.size())) ||
-        (r = upload(c, &c->t_sinfo, P.slot_info.data(), std::max<size_t>(1, P.slot_info.size()))) ||
-        (r = upload(c, &c->t_aoff, P.aoff.data(), P.aoff.size())) ||
-        (r = upload(c, &c->t_zlo, P.zlo.data(), P.zlo.size())) ||
-        (r = upload(c, &c->t_zhi, P.zhi.data(), P.zhi.size())) ||
-        (r = upload(c, &c->t_deps, P.deps.data(), P.deps.size())) ||
-        (r = upload(c, &c->t_allfree, P.allfree.data(), P.allfree.size())) ||
-        (r = dalloc(c, &c->t_flags, P.ntiles)) || (r = dalloc(c, &c->t_ticket, 1)))
-      return fail(r);
-    if (cudaMemsetAsync(c->t_flags, 0, sizeof(unsigned) * P.ntiles, c->stream) != cudaSuccess ||
-        cudaStreamSynchronize(c->stream) != cudaSuccess)
-      return fail(PGFEM_GPU_ECUDA);
-    c->tiles = true;
   }
   // default state: identity Cp^-1 / pF, zero eqps, g = g0
   if (c->nstate) {
@@ -1100,11 +957,7 @@ int pgfem_gpu_destroy(pgfem_gpu_ctx *c) {
 }
 
 int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
-  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR && mode != PGFEM_SCATTER_TILES &&
-             mode != PGFEM_SCATTER_CELLS))
-    return PGFEM_GPU_EINVAL;
-  if ((mode == PGFEM_SCATTER_TILES || mode == PGFEM_SCATTER_CELLS) && !c->tiles) return PGFEM_GPU_EINVAL;
-  if (mode == PGFEM_SCATTER_CELLS && c->nne != 10) return PGFEM_GPU_EINVAL;
+  if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR)) return PGFEM_GPU_EINVAL;
   c->scatter_mode = mode;
   return PGFEM_GPU_OK;
 }
@@ -1118,12 +971,9 @@ int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
     return c->cp_net ? 8 : 5;
   if (c->mat.dev_pot == 2)  // u expansion + per-node kernel launches (one per colour in colour mode)
     return 1 + (c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1);
-  if (c->tiles && c->scatter_mode == PGFEM_SCATTER_CELLS && c->nne == 10) return 2;  // u expansion, cells
-  if (c->tiles && c->scatter_mode == PGFEM_SCATTER_TILES) return 3;  // u expansion, point update, tiles
-  if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_ELEMENT_ROWS") &&
-      !getenv("PGFEM_GPU_P2_SYNC") && !getenv("PGFEM_GPU_P2_FUSED"))
-    return 3;  // u expansion, point updates, pipelined R+K assembly
-  if (c->nne == 4 && c->scatter_mode == PGFEM_SCATTER_ATOMIC && !getenv("PGFEM_GPU_P1_NODE"))
+  if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC)
+    return 3;  // u expansion, point updates, tensor-core R+K assembly
+  if (c->nne == 4 && c->scatter_mode == PGFEM_SCATTER_ATOMIC)
     return 3;  // u expansion, point updates, column-split R+K assembly
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
   return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpgfem_gpu.so")
 
 MODEL_HE, MODEL_J2, MODEL_CP = 0, 1, 2
-SCATTER_ATOMIC, SCATTER_COLOUR, SCATTER_TILES, SCATTER_CELLS = 0, 1, 2, 3
+SCATTER_ATOMIC, SCATTER_COLOUR = 0, 1
 
 ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "EPATTERN", -5: "ENODEV", -6: "ELIMIT", -7: "ETIMEOUT",
           -8: "EFORMAT"}

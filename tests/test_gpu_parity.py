@@ -189,82 +189,40 @@ def test_pattern_mismatch_is_rejected(gpu):
     assert ei.value.code == -4
 
 
-def _ctx_with_env(p, **env):
-    import os
-    old = {k: os.environ.get(k) for k in env}
-    try:
-        for k, v in env.items():
-            os.environ[k] = v
-        return p.context()
-    finally:
-        for k, v in old.items():
-            if v is None:
-                os.environ.pop(k, None)
-            else:
-                os.environ[k] = v
-
-
-@pytest.mark.parametrize("kind", ["j2_p2", "he_p1"])
-def test_tiled_first_touch_memset_and_untiled_agree(gpu, kind):
-    p = wl.j2_p2(n=4, seed=2, perturb=1e-4) if kind == "j2_p2" else wl.he_p1(6, seed=3)
-    ref = _ctx_with_env(p, PGFEM_GPU_NO_TILES="1")
-    Ru, Ku, _ = ref.assemble_RK(p.u)
-    with pytest.raises(pg.PgfemError):
-        ref.set_scatter_mode(pg.SCATTER_TILES)  # no tile plan in this context
-    for env in ({}, {"PGFEM_GPU_TILE_MEMSET": "1"}):
-        ctx = _ctx_with_env(p, **env)
-        ctx.set_scatter_mode(pg.SCATTER_TILES)
-        R, K, st = ctx.assemble_RK(p.u)
-        assert st.ok(), st.as_dict()
-        check_R(R, Ru, 1e-12)
-        check_K(K, Ku, p.Ap, 1e-12)
-        # repeated calls (flags carry an epoch; no reset between calls)
-        R2, K2, st2 = ctx.assemble_RK(p.u)
-        assert st2.ok()
-        check_R(R2, R, 1e-13)
-        check_K(K2, K, p.Ap, 1e-13)
-
-
 @pytest.mark.parametrize("model", ["j2", "he"])
-def test_quadratic_tet_kernel_variants_agree(gpu, model):
-    """The R+K paths for 10-node elements -- the default (point updates in
-    their own kernel, then the warp-specialised assembly from the point
-    records), the single-kernel warp-specialised variant, the variant in which
-    all threads run the phases of a tile in turn, and the
-    one-element-per-thread-block kernel -- on 162 elements, so that the last
-    tile of every variant is partly empty; each against the oracle."""
-    import os
+def test_quadratic_tet_ragged_tile_and_repeat(gpu, model):
+    """The quadratic-tet R+K path (point kernel, then the tensor-core element
+    assembly over tiles of four elements) on 162 elements, so that the last
+    tile is partly empty, against the oracle; a second call on the same
+    context gives the same R and K (the record and Y buffers carry nothing
+    over between calls)."""
     p = wl.j2_p2(n=3, seed=7, perturb=5e-3)
     if model == "he":
         p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.3)
         p.state = None
-    assert p.conn.shape[0] % 8 == 2
+    assert p.conn.shape[0] % 4 == 2
     ctx = p.context()
+    assert ctx.launches_per_assembly() == 3
     Ro, Ko, so = oracle_assemble(p)
-    for env in ({}, {"PGFEM_GPU_P2_FUSED": "1"}, {"PGFEM_GPU_P2_SYNC": "1"}, {"PGFEM_GPU_ELEMENT_ROWS": "1"}):
-        os.environ.update(env)
-        try:
-            R, K, st = ctx.assemble_RK(p.u)
-        finally:
-            for k in env:
-                os.environ.pop(k, None)
-        assert st.ok(), (env, st.as_dict())
-        check_R(R, Ro)
-        check_K(K, Ko, p.Ap)
-        if so is not None:
-            sg = ctx.get_state(1)
-            assert np.abs(sg - so).max() <= TOL * np.abs(so).max(), env
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    if so is not None:
+        sg = ctx.get_state(1)
+        assert np.abs(sg - so).max() <= TOL * np.abs(so).max()
+    R2, K2, st2 = ctx.assemble_RK(p.u)
+    assert st2.ok()
+    check_R(R2, R, 1e-13)
+    check_K(K2, K, p.Ap, 1e-13)
 
 
 @pytest.mark.parametrize("model", ["j2", "he"])
-def test_linear_tet_kernel_variants_agree(gpu, model):
-    """The R+K paths for 4-node elements -- the default (point kernel, then the
-    warp-specialised column-split assembly) with each schedule (elements per
-    block 16/32/64, static or work stealing), the variant in which all threads
-    run the phases of a tile in turn, and the per-node kernel -- on
-    5^3 x 6 = 750 elements, so that the last tile of every tile size is partly
-    empty; each against the oracle."""
-    import os
+def test_linear_tet_schedules_agree(gpu, model):
+    """The linear-tet R+K path (point kernel, then the warp-specialised
+    column-split assembly) with each schedule -- elements per block 16/32/64,
+    static or work stealing -- on 5^3 x 6 = 750 elements, so that the last
+    tile of every tile size is partly empty; each against the oracle."""
     p = wl.he_p1(5, seed=4)
     p.u = p.u * 0.3
     if model == "j2":
@@ -276,29 +234,24 @@ def test_linear_tet_kernel_variants_agree(gpu, model):
     Ro, Ko, so = oracle_assemble(p)
     if so is not None:
         assert (so[:, 9] > 0).any()
-    runs = [(epb, grab, {}) for epb in (16, 32, 64) for grab in (0, 2)]
-    runs += [(32, 0, {"PGFEM_GPU_P1_SYNC": "1"}), (16, 2, {"PGFEM_GPU_P1_SYNC": "1"}),
-             (0, 0, {"PGFEM_GPU_P1_NODE": "1"})]
-    for epb, grab, env in runs:
-        ctx.set_schedule(epb, grab)
-        os.environ.update(env)
-        try:
+    for epb in (16, 32, 64):
+        for grab in (0, 2):
+            ctx.set_schedule(epb, grab)
             R, K, st = ctx.assemble_RK(p.u)
-        finally:
-            for k in env:
-                os.environ.pop(k, None)
-        assert st.ok(), (epb, grab, env, st.as_dict())
-        check_R(R, Ro)
-        check_K(K, Ko, p.Ap)
-        if so is not None:
-            assert np.abs(ctx.get_state(1) - so).max() <= TOL * np.abs(so).max(), (epb, grab, env)
+            assert st.ok(), (epb, grab, st.as_dict())
+            check_R(R, Ro)
+            check_K(K, Ko, p.Ap)
+            if so is not None:
+                assert np.abs(ctx.get_state(1) - so).max() <= TOL * np.abs(so).max(), (epb, grab)
 
 
-def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
-    # number the nodes in reverse order (ids stay consecutive per node, but the
-    # rows are no longer first touched in element order)
+@pytest.mark.parametrize("nne", [4, 10])
+def test_non_first_visit_numbering_matches_oracle(gpu, nne):
+    """Nodes numbered in reverse order (ids stay consecutive per node, but rows
+    are no longer first touched in element order): the default R+K path
+    against the oracle."""
     import pgfem_gpu as pgm
-    X, conn, _ = pgm.mesh_box_tet(3, 10)
+    X, conn, _ = pgm.mesh_box_tet(3, nne)
     nn = X.shape[0]
     ids = np.zeros((nn, 3), dtype=np.int64)
     order = np.arange(nn)[::-1]
@@ -309,11 +262,11 @@ def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
     disp = (2 * r - 1) * 1e-4 / 3 + np.outer(X[:, 0], [wl.j2_yield_strain(), 0, 0])
     u = wl.nodal_to_free(ids, disp)
     mat = pg.material(pg.MODEL_J2, sigma_y=250.0, H=2000.0)
-    state = np.zeros((conn.shape[0] * 4, 10))
+    nqp = conn.shape[0] * (4 if nne == 10 else 1)
+    state = np.zeros((nqp, 10))
     state[:, [0, 4, 8]] = 1.0
     prob = wl.Problem("rev", X, conn, ids, ndof, Ap, Ai, mat, u, state=state)
     ctx = prob.context()
-    ctx.set_scatter_mode(pg.SCATTER_TILES)
     R, K, st = ctx.assemble_RK(u)
     assert st.ok()
     Ro, Ko, _ = oracle_assemble(prob)
@@ -321,35 +274,11 @@ def test_non_first_visit_numbering_falls_back_and_matches_oracle(gpu):
     check_K(K, Ko, Ap)
 
 
-@pytest.mark.parametrize("n,stretch,perturb,model", [(3, None, 1e-4, "j2"), (4, 4e-3, 5e-3, "j2"),
-                                                      (3, None, 1e-4, "he")])
-def test_cells_mode_matches_oracle(gpu, n, stretch, perturb, model):
-    """Fused one-cell-per-CTA kernel (quadratic tets) against the oracle; a
-    second call on the same buffers gives the same result."""
-    p = wl.j2_p2(n=n, seed=11, stretch=stretch, perturb=perturb)
-    if model == "he":
-        p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.3)
-        p.state = None
-    ctx = p.context()
-    ctx.set_scatter_mode(pg.SCATTER_CELLS)
-    assert ctx.launches_per_assembly() == 2
-    R, K, st = ctx.assemble_RK(p.u)
-    assert st.ok(), st.as_dict()
-    Ro, Ko, so = oracle_assemble(p)
-    check_R(R, Ro)
-    check_K(K, Ko, p.Ap)
-    if so is not None:
-        sg = ctx.get_state(1)
-        assert np.abs(sg - so).max() <= TOL * np.abs(so).max()
-    R2, K2, _ = ctx.assemble_RK(p.u)
-    check_R(R2, R, 1e-13)
-    check_K(K2, K, p.Ap, 1e-13)
-
-
-def test_cells_mode_is_for_quadratic_tets_only(gpu):
+def test_scatter_modes_other_than_atomic_and_colour_are_rejected(gpu):
     ctx = wl.he_p1(4).context()
-    with pytest.raises(pg.PgfemError):
-        ctx.set_scatter_mode(pg.SCATTER_CELLS)
+    for mode in (2, 3, -1):
+        with pytest.raises(pg.PgfemError):
+            ctx.set_scatter_mode(mode)
 
 
 @pytest.mark.parametrize("nne", [4, 10])
@@ -378,9 +307,6 @@ def test_linear_deviatoric_potential_matches_oracle(gpu, nne):
     Rc, Kc, _ = ctx.assemble_RK(p.u, p.u_presc)
     check_R(Rc, Ro)
     check_K(Kc, Ko, p.Ap)
-    for mode in (pg.SCATTER_TILES, pg.SCATTER_CELLS):
-        with pytest.raises(pg.PgfemError):
-            ctx.set_scatter_mode(mode)
     # element level: the dense element blocks assemble to the same K
     elems = np.arange(p.conn.shape[0])
     lk, fe, _ = ctx.stiffmatel_fd(elems, p.u, p.u_presc)
