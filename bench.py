@@ -871,16 +871,20 @@ def run_nr(args, ws, rank, local):
 
 
 def run_reference(args, ws, rank):
-    import workloads as wl
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     if rank != 0:
         return None
     nth = os.cpu_count() or 1
     # the same workload restricted to an element sample: the first cells of
-    # the n^3 mesh in element order (identical per-element work)
-    p = wl.j2_p2(n=args.n, seed=1, max_cells_z=args.ref_layers)
-    P, mat = oracle.from_workload(p)
+    # the n^3 mesh in element order (identical per-element work), built by the
+    # oracle's own mesher, DOF numbering and CSR pattern (no product code)
+    P, mat, u, state = oracle.j2_p2_problem(args.n, seed=1, max_cells_z=args.ref_layers)
+
+    class _W:  # the attributes the timing below reads
+        pass
+    p = _W()
+    p.u, p.state, p.ne, p.nint = u, state, int(P.conn.shape[0]), 4
     per_step = min(10.0, 150.0 / max(1, args.steps + args.warmup))
     t0 = time.perf_counter()
     P.assemble(mat, p.u, state_n=p.state, e1=min(p.ne, 256), nthreads=nth)

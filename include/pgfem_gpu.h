@@ -67,7 +67,11 @@ typedef struct {
   int dev_pot;           /* HE deviatoric potential, the reference's devPotFlag (src/new_potentials.cc:79-156):
                             0 or 1 Mooney-Rivlin with m01 = 0 (neo-Hookean, m10 = G/2); 2 linear,
                             S_dev = G (C - I) (devStress_Linear :364-375).  HE only; 2 runs the
-                            per-node element kernel on every R/K path (no tile or cell modes). */
+                            per-node element kernel on every R/K path. */
+  int vol_pot;           /* HE and J2 volumetric potential U(J), the reference's volPotFlag
+                            (src/new_potentials.cc:185-300, 553-640): 99 (or <= 0) U_Common
+                            0.5 (J-1)^2; 2 Doll-Schweizerhof 0.5 (exp(J-1) - ln J - 1); 3
+                            Doll-Schweizerhof 0.5 (J-1) ln J.  Other values: PGFEM_GPU_EINVAL. */
 } pgfem_material_desc;
 
 typedef struct {
@@ -119,6 +123,13 @@ int pgfem_gpu_create(const pgfem_mesh_desc *mesh, const pgfem_material_desc *mat
                      const int *Ai, long nrows, pgfem_gpu_ctx **ctx);
 int pgfem_gpu_destroy(pgfem_gpu_ctx *ctx);
 int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *ctx, int mode);
+/* Tests of the failure path (no counterpart in the reference): the bound of
+ * the producer/consumer hand-off waits of the linear-tet R+K kernel (seconds,
+ * default 2) and, with stall_next_assembly, the next such assembly's producer
+ * warps withhold their first hand-off: the consumers' waits run out, every
+ * warp leaves its loop (no trap), status.other counts it, and later calls are
+ * unaffected. */
+int pgfem_gpu_set_wait_test(pgfem_gpu_ctx *ctx, double limit_s, int stall_next_assembly);
 /* Device bytes held by the context (mesh, map, state, scratch). */
 long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *ctx);
 long pgfem_gpu_nnz(const pgfem_gpu_ctx *ctx);
@@ -163,6 +174,11 @@ int pgfem_gpu_kernel_time(pgfem_gpu_ctx *ctx, double *ms, long *ncalls, int rese
  * chain kernel over every SM; the FP64 roofline denominator.  No counterpart
  * in the reference. */
 int pgfem_gpu_fp64_peak(double *tflops);
+
+/* Compute capability the library's kernels were compiled for, as reported by
+ * the CUDA runtime for one of them (major * 10 + minor: 100 for sm_100a).  No
+ * counterpart in the reference. */
+int pgfem_gpu_binary_version(int *version);
 
 /* ---- crystal plasticity local solver -------------------------------------
  * Initial guess of the local Newton per quadrature point (host AoS nqp*10:
@@ -211,7 +227,8 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
  * d_state_n / d_state_np1 [10][nqp] (pF 9, g), optional d_dgam [12][nqp]
  * slip increments dt*gamma_dot_a and d_iters [nqp] Newton iteration counts.
  * Asynchronous on `stream` unless st != NULL, in which case the call waits
- * for the stream and returns the failure counts.
+ * for the stream and returns the failure counts (so st must be NULL while
+ * the stream is being captured into a graph: PGFEM_GPU_EINVAL otherwise).
  * Its working memory (about 3.4 MB: per-point Newton record, ticket counter,
  * failure counters) is one fixed array in the library's device image, held
  * by every GPU that loads the library until the process exits; each call
@@ -221,7 +238,10 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
  *    same device) share the array and race: order them on one stream;
  *  - the first call on each device performs a one-time set-up (looks up the
  *    array's device address, sets the kernel's shared-memory limit); make
- *    that first call before any stream capture. */
+ *    that first call before any stream capture;
+ *  - the set-up is kept per device ordinal, for the device's primary context
+ *    (the CUDA runtime's default): call it from threads that use the primary
+ *    context, not from a driver-API context created with cuCtxCreate. */
 int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, const double *d_F,
                                    const double *d_R_cp, const double *d_state_n, double dt,
                                    double *d_state_np1, double *d_dgam, int *d_iters,
@@ -285,6 +305,12 @@ int pgfem_mlp_get_scaling(const pgfem_mlp *m, float *x_mean, float *x_inv_std, f
 /* scaling from data: feature mean / standard deviation, target RMS */
 int pgfem_mlp_fit_scaling(pgfem_mlp *m, long n, const float *d_x, const float *d_t);
 int pgfem_mlp_predict_device(pgfem_mlp *m, long n, const float *d_x, float *d_y, void *stream);
+/* Tests of the failure path (no counterpart in the reference): the bound of
+ * the network kernels' tensor-core completion waits (seconds, default 2) and,
+ * with stall_next_forward, the next forward pass withholds each CTA's first
+ * MMA chain so that its wait runs out: the kernel returns early (TMEM released,
+ * no trap) and the call reports PGFEM_GPU_ETIMEOUT; later calls are unaffected. */
+int pgfem_mlp_set_wait_test(pgfem_mlp *m, double limit_s, int stall_next_forward);
 int pgfem_mlp_predict(pgfem_mlp *m, long n, const float *x, float *y); /* host buffers */
 /* loss 1/(2n) sum |out - t/y_std|^2 over all n rows and its gradient (host buffers) */
 int pgfem_mlp_loss_grad(pgfem_mlp *m, long n, const float *x, const float *t, float *grad, double *loss);
@@ -516,9 +542,14 @@ int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int 
  * device; CP pFn, g_n from the committed state (t_n) and pFnm1, g_nm1 from
  * state_nm1 (host AoS nqp*10 as pgfem_gpu_get_state, the state before the
  * last commit; NULL = the state at t_n); tau_n, gamma_dot_n, L_n, L_nm1 are
- * not carried by this path and are written as 0.  Read: returns the free-DOF
- * displacements u_nm1, u_n (the caller's vectors) and, for CP, sets the state
- * at t_n (pFn, g_n) and F at t_n from the file; the other fields are not used. */
+ * not carried by this path and are written as 0.  J2: the plastic stress of
+ * the reference's block is pS = G (I - Cp^-1) of this path's state (zero in
+ * the initial state, as the reference initialises it), ep_n / ep_nm1 the
+ * equivalent plastic strain, gam_n = sqrt(3/2) (ep_n - ep_nm1), the damage
+ * variables w, X, H, gam_nm1 and the damage flag 0 (damage is not carried).
+ * Read: returns the free-DOF displacements u_nm1, u_n (the caller's vectors)
+ * and sets the state at t_n from the file (CP: pFn, g_n and F at t_n; J2:
+ * Cp^-1 = I - pSn / G and ep_n); the other fields are not used. */
 int pgfem_gpu_write_restart(pgfem_gpu_ctx *ctx, const char *path, const double *u_nm1, const double *u_n,
                             const double *presc_nm1, const double *presc_n, const double *state_nm1);
 int pgfem_gpu_read_restart(pgfem_gpu_ctx *ctx, const char *path, double *u_nm1, double *u_n);
@@ -547,6 +578,15 @@ typedef struct {
 } pgfem_model_params;
 /* Reads up to max_entries entries (n = entries in the file). */
 int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model_params *out, int *n);
+/* Material of a J2 entry (CM_J2P_PARAM::read_param, src/cm_j2_plasticity.cc:
+ * 865-932): E, nu and vol_pot (volPotFlag) from the mesh file's material line,
+ * sigma_y = k0 and H = hp from the entry (yield function ||dev tau|| -
+ * sqrt(2/3) (k0 + hp ep), linear isotropic hardening).  Returns
+ * PGFEM_GPU_EINVAL for beta != 0 (only the reference driver's beta = 0 is
+ * carried) and for active damage (mu != 0); the damage parameters are
+ * otherwise unused (damage off). */
+int pgfem_input_j2_material(const pgfem_model_params *mp, double E, double nu, int vol_pot,
+                            pgfem_material_desc *out);
 
 #ifdef __cplusplus
 }

@@ -21,7 +21,7 @@ class OrcMaterial(C.Structure):
                 ("gamma_dot_0", C.c_double), ("m", C.c_double), ("G0", C.c_double),
                 ("g0", C.c_double), ("gs_0", C.c_double), ("gamma_dot_s", C.c_double),
                 ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int),
-                ("dev_pot", C.c_int)]
+                ("dev_pot", C.c_int), ("vol_pot", C.c_int)]
 
 
 class OrcProblem(C.Structure):
@@ -71,9 +71,9 @@ def _p(a):
 
 
 def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0, G0=0.0, g0=0.0,
-             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1):
+             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1, vol_pot=99):
     return OrcMaterial(model, E, nu, sigma_y, H, gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w, cp_tol,
-                       cp_max_iter, dev_pot)
+                       cp_max_iter, dev_pot, vol_pot)
 
 
 def from_pg_material(m, dev_pot=None):
@@ -82,7 +82,7 @@ def from_pg_material(m, dev_pot=None):
     if dev_pot is None:
         dev_pot = 2 if getattr(m, "dev_pot", 1) == 2 else 1
     return material(m.model, m.E, m.nu, m.sigma_y, m.H, m.gamma_dot_0, m.m, m.G0, m.g0, m.gs_0,
-                    m.gamma_dot_s, m.w, m.cp_tol, m.cp_max_iter, dev_pot)
+                    m.gamma_dot_s, m.w, m.cp_tol, m.cp_max_iter, dev_pot, getattr(m, "vol_pot", 99))
 
 
 def state_size(model):
@@ -220,6 +220,85 @@ def newton_step(P, mat, u0, u_presc=None, state_n=None, dt=0.0, iter_max=10, nor
         Km = csr_matrix((K, P.Ai, P.Ap), shape=(P.ndof, P.ndof))
         u = u + spsolve(Km.tocsc(), -R)
     return u, hist, False, snp1
+
+
+# ---------------------------------------------------------------------------
+# Synthetic workload built without the product library (the CPU arm of the
+# benchmark times the oracle on it, so that no product code is loaded there).
+# ---------------------------------------------------------------------------
+# Kuhn split of the unit cube into 6 tets along the (0,0,0)-(1,1,1) diagonal
+# (one tet per axis permutation, oriented to a positive volume) and the
+# quadratic-tet edge nodes in FEMLIB's order (FEMLIB/src/femlib.cc:163-176).
+_KUHN_PERM = [(0, 1, 2), (0, 2, 1), (1, 0, 2), (1, 2, 0), (2, 0, 1), (2, 1, 0)]
+_KUHN_SIGN = [1, -1, -1, 1, 1, -1]
+_EDGES = [(0, 1), (1, 2), (0, 2), (0, 3), (1, 3), (2, 3)]
+
+
+def mesh_box_tet(n, nne):
+    """Structured n^3 unit-cube mesh, 6 Kuhn tets per cell, node-lexicographic
+    numbering on the lattice (n or 2n intervals), cell-major element order."""
+    N = n if nne == 4 else 2 * n
+    L = N + 1
+    s = 1 if nne == 4 else 2
+    k, j, i = np.meshgrid(np.arange(L), np.arange(L), np.arange(L), indexing="ij")
+    X = np.stack([i.ravel() / N, j.ravel() / N, k.ravel() / N], axis=1)
+    cells = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij"), axis=-1).reshape(-1, 3)
+    cells = cells[:, ::-1]  # (ci, cj, ck) with ci fastest
+    conn = np.zeros((6 * n ** 3, nne), dtype=np.int64)
+    for t in range(6):
+        v = np.zeros((4, 3), dtype=np.int64)
+        v[1, _KUHN_PERM[t][0]] = 1
+        v[2] = v[1]
+        v[2, _KUHN_PERM[t][1]] += 1
+        v[3] = 1
+        if _KUHN_SIGN[t] < 0:
+            v[[1, 2]] = v[[2, 1]]
+        lat = [s * (cells + v[a]) for a in range(4)]
+        if nne == 10:
+            lat += [(lat[a] + lat[b]) // 2 for a, b in _EDGES]
+        for a in range(nne):
+            conn[t::6, a] = lat[a][:, 0] + L * (lat[a][:, 1] + L * lat[a][:, 2])
+    return X, conn.astype(np.int32)
+
+
+def splitmix64(seed, n, stream=0):
+    """n uniform doubles in [0,1) from splitmix64(seed, stream, index)."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(n, dtype=np.uint64)
+        z = (np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15) + np.uint64(stream) * np.uint64(0xD1B54A32D192ED03)
+             + (idx + np.uint64(1)) * np.uint64(0x9E3779B97F4A7C15))
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+
+
+def j2_p2_problem(n, seed=1, perturb=1e-4, max_cells_z=None, E=200e3, nu=0.3, sigma_y=250.0, H=2000.0):
+    """The J2 quadratic-tet workload (n^3 cells, stretch at the yield onset
+    sigma_y / 2 mu along x plus a seeded perturbation of perturb * h), or its
+    first max_cells_z layers of cells, built with the oracle's own mesher, DOF
+    numbering and CSR pattern.  Returns (Problem, material, u, state_n)."""
+    X, conn = mesh_box_tet(n, 10)
+    r = splitmix64(seed, X.shape[0] * 3).reshape(-1, 3)
+    if max_cells_z is not None and max_cells_z < n:
+        conn = conn[:6 * n * n * max_cells_z]
+        used = np.unique(conn)
+        remap = np.full(X.shape[0], -1, dtype=np.int64)
+        remap[used] = np.arange(len(used))
+        X, r, conn = X[used], r[used], remap[conn].astype(np.int32)
+    ids, ndof = generate_dof_ids(conn, X.shape[0], np.zeros((X.shape[0], 3), dtype=np.int64))
+    Ap, Ai = psparse_apai(conn, ids, ndof)
+    a = perturb * (1.0 / n)
+    mu = E / (2.0 * (1.0 + nu))
+    disp = (2.0 * r - 1.0) * a
+    disp[:, 0] += sigma_y / (2.0 * mu) * X[:, 0]
+    u = np.zeros(ndof)
+    m = ids > 0
+    u[ids[m] - 1] = disp[m]
+    state = np.zeros((conn.shape[0] * 4, 10))
+    state[:, [0, 4, 8]] = 1.0
+    mat = material(J2, E=E, nu=nu, sigma_y=sigma_y, H=H)
+    return Problem(X, conn, ids, ndof, Ap, Ai), mat, u, state
 
 
 def from_workload(p):

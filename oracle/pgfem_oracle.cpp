@@ -196,8 +196,25 @@ void deformation_gradient(int nne, const double *u, const double *dN, double *F)
 // ---------------------------------------------------------------------------
 struct Elast {
   double G, nu, m10, m01, kappa;
-  int dev_pot;
+  int dev_pot, vol_pot;
 };
+
+// U'(J), U''(J) of the volumetric potentials (src/new_potentials.cc:553-622).
+void vol_derivs(int vol_pot, double J, double &dU, double &d2U) {
+  switch (vol_pot) {
+    case 2:  // U_Doll_Schweizerhof_7 = 0.5 (exp(J-1) - ln J - 1)
+      dU = (std::exp(-1 + J) - 1. / J) * .5;
+      d2U = (std::exp(-1 + J) + 1. / (J * J)) * .5;
+      break;
+    case 3:  // U_Doll_Schweizerhof_8 = 0.5 (J-1) ln J
+      dU = (-1 + J) / (2. * J) + std::log(J) * .5;
+      d2U = 1. / J - (-1 + J) / (2. * J * J);
+      break;
+    default:  // 99: U_Common = 0.5 (J-1)^2
+      dU = J - 1.0;
+      d2U = 1.0;
+  }
+}
 
 Elast make_elast(const orc_material *m) {
   Elast e;
@@ -207,6 +224,7 @@ Elast make_elast(const orc_material *m) {
   e.m01 = 0.0;
   e.kappa = (2 * e.G * (1 + e.nu)) / (3 * (1 - 2 * e.nu));
   e.dev_pot = m->dev_pot == 2 ? 2 : 1;
+  e.vol_pot = (m->vol_pot == 2 || m->vol_pot == 3) && m->model != 2 ? m->vol_pot : 99;
   return e;
 }
 
@@ -218,7 +236,8 @@ void he_stress_stiffness(const Elast &el, const double *C, double J, double *S, 
   const double trC = C[0] + C[4] + C[8];
   double CC = 0;
   for (int i = 0; i < 9; i++) CC += C[i] * C[i];
-  const double dUdJ = J - 1.0, d2UdJ2 = 1.0;
+  double dUdJ, d2UdJ2;
+  vol_derivs(el.vol_pot, J, dUdJ, d2UdJ2);
   if (el.dev_pot == 2) {  // devStress_Linear / matStiff_Linear, src/new_potentials.cc:364-375, 434-452
     for (int i = 0; i < 9; i++) S[i] = el.G * (C[i] - I[i]) + el.kappa * J * dUdJ * invC[i];
     if (!L) return;
@@ -271,7 +290,7 @@ void he_stress_stiffness(const Elast &el, const double *C, double J, double *S, 
 // Inelasticity" (1998) Box 9.1, written in the material description with the
 // state (Cp^-1, eqps): b_e_trial = J^{-2/3} F Cp^-1 F^T, radial return of
 // s = mu dev(b_e), b_e_{n+1} = s/mu + (tr b_e_trial / 3) 1.  The volumetric
-// part is the reference's U_Common potential (kappa J (J-1) C^-1).  The
+// part is kappa J U'(J) C^-1 with the material's potential (vol_derivs).  The
 // tangent L = 2 dS/dC is the exact derivative of this update (the published
 // Box 9.2 tangent is its symmetrised form); it is checked against central
 // differences in tests/.
@@ -309,7 +328,9 @@ void j2_update(const Elast &el, double sy, double Hh, const double *F, const dou
     dgam = f / (2.0 * mubar * beta0);
     r = 1.0 - f / (beta0 * q);
   }
-  const double pJ = kap * J * (J - 1.0);
+  double dU, d2U;
+  vol_derivs(el.vol_pot, J, dU, d2U);
+  const double pJ = kap * J * dU;
   for (int i = 0; i < 9; i++) S[i] = pJ * Ci[i] + r * Str[i];
 
   if (state_np1) {
@@ -324,7 +345,7 @@ void j2_update(const Elast &el, double sy, double Hh, const double *F, const dou
   }
   if (!L) return;
   // L_vol in the reference's DISP form (C^-1_ik C^-1_lj product).
-  const double cvol1 = kap * (J * (J - 1.0) + J * J), cvol2 = 2.0 * kap * J * (J - 1.0);
+  const double cvol1 = kap * (J * dU + J * J * d2U), cvol2 = 2.0 * kap * J * dU;
   double dq[9] = {0}, dr[9] = {0};
   if (plastic) {
     const double c = mu * mu * J23 * J23 / (2.0 * q);

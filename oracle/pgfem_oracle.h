@@ -42,6 +42,8 @@ typedef struct {
   int dev_pot;                  /* deviatoric potential flag of src/new_potentials.cc:79-156:
                                    1 (or 0) Mooney-Rivlin with m10 = G/2, m01 = 0 (neo-Hookean),
                                    2 Linear (S_dev = G (C - I)) */
+  int vol_pot;                  /* volumetric potential flag (src/new_potentials.cc:185-300, 553-640):
+                                   99 (or <= 0) U_Common, 2 / 3 Doll-Schweizerhof; HE and J2 */
 } orc_material;
 
 typedef struct {

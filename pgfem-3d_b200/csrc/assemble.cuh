@@ -83,6 +83,10 @@ struct AsmArgs {
   // (kEBW int32 words per element: row bases, residual indices, node-pair
   // positions, free masks)
   const int *eblk;
+  // bound of the pipelined kernels' hand-off waits (ns), and the failure-path
+  // test switch: the producer withholds its first hand-off
+  unsigned long long wait_ns;
+  int stall;
   Mat mat;
   ShapeTable shp;
 };

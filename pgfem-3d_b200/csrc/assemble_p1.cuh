@@ -187,7 +187,7 @@ __device__ __forceinline__ void p2_blocks(const AsmArgs &args, const double *vec
 // Every wait is bounded: a wait that runs out sets status[3] and both roles
 // leave their loops (their next waits run out too), so a fault cannot hang
 // the GPU.
-constexpr unsigned long long kWWaitNs = 2000000000ull;
+constexpr unsigned long long kWWaitNs = 2000000000ull;  // default bound of a hand-off wait
 
 __device__ __forceinline__ unsigned long long w_gtimer() {
   unsigned long long t;
@@ -204,7 +204,7 @@ __device__ __forceinline__ void w_mb_arrive(uint64_t *b) {
                : "memory");
 }
 // bounded wait for the completion of the phase with the given parity
-__device__ __forceinline__ bool w_mb_wait(uint64_t *b, unsigned parity) {
+__device__ __forceinline__ bool w_mb_wait(uint64_t *b, unsigned parity, unsigned long long limit) {
   const unsigned a = (unsigned)__cvta_generic_to_shared(b);
   const unsigned long long t0 = w_gtimer();
   for (;;) {
@@ -216,7 +216,7 @@ __device__ __forceinline__ bool w_mb_wait(uint64_t *b, unsigned parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (w_gtimer() - t0 > kWWaitNs) return false;
+    if (w_gtimer() - t0 > limit) return false;
   }
 }
 
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(p1ws_threads<TE>()) k_assemble_p1ws(const AsmA
     for (long i = 0;; i++) {
       const int bx = (int)(i & 1);
       if (i >= 2) {
-        const bool ok = w_mb_wait(&empty[bx], (unsigned)(((i - 2) >> 1) & 1));
+        const bool ok = w_mb_wait(&empty[bx], (unsigned)(((i - 2) >> 1) & 1), args.wait_ns);
         if (__any_sync(0xffffffffu, !ok)) {
           fail = true;
           break;
@@ -346,7 +346,9 @@ __global__ void __launch_bounds__(p1ws_threads<TE>()) k_assemble_p1ws(const AsmA
                                   sVec + (bx * TE + el) * kP1ES + a * VS, sA1 + bx * TE + el);
       }
       if (pl == 0) sTile[bx] = t_cur;
-      w_mb_arrive(&full[bx]);  // release: vectors and the tile index are visible to the consumers
+      // release: vectors and the tile index are visible to the consumers (the
+      // failure-path test withholds lane 0's first arrive: the phase never completes)
+      if (!(args.stall && i == 0 && pl == 0)) w_mb_arrive(&full[bx]);
       t_cur = t_nxt;
     }
     cpa_wait_all();
@@ -356,7 +358,7 @@ __global__ void __launch_bounds__(p1ws_threads<TE>()) k_assemble_p1ws(const AsmA
     const int a = r / 3, k = r - a * 3;
     for (long i = 0;; i++) {
       const int bx = (int)(i & 1), bm = (int)(i % 3);
-      if (!w_mb_wait(&full[bx], (unsigned)((i >> 1) & 1))) {
+      if (!w_mb_wait(&full[bx], (unsigned)((i >> 1) & 1), args.wait_ns)) {
         fail = true;
         break;
       }

@@ -12,7 +12,8 @@
 //      Mooney-Rivlin with m01 = 0 (src/new_potentials.cc:333-432) plus the
 //      U_Common volumetric potential (:553-604) as combined in
 //      src/displacement_based_element.cc:1368-1445, pushed forward:
-//      tau = mu dev(J^-2/3 F F^T) + kappa J (J-1) 1.
+//      tau = mu dev(J^-2/3 F F^T) + kappa J U'(J) 1 (U the material's
+//      volumetric potential: U_Common or a Doll-Schweizerhof form).
 //  HE, linear deviatoric potential (devPotFlag 2, devStress_Linear /
 //      matStiff_Linear, src/new_potentials.cc:364-375, 434-452): S = G (C - I)
 //      + kappa J (J-1) C^-1, L = 2G I + volumetric part; pushed forward
@@ -32,6 +33,7 @@ namespace pgb {
 struct Mat {
   int model;
   int dev_pot;  // HE deviatoric potential: 2 linear, otherwise neo-Hookean
+  int vol_pot;  // volumetric potential: 99 U_Common, 2 / 3 Doll-Schweizerhof (src/new_potentials.cc:553-640)
   double mu, kappa, sy, H;
   // crystal plasticity
   double gdot0, m, G0, g0, gs0, gdots, w, tol;
@@ -41,6 +43,23 @@ struct Mat {
 struct Sym {
   double v[6];
 };
+
+// U'(J) and U''(J) of the volumetric potential (src/new_potentials.cc:553-622):
+// 99 U_Common 0.5 (J-1)^2; 2 0.5 (exp(J-1) - ln J - 1); 3 0.5 (J-1) ln J.
+__device__ __forceinline__ void vol_derivs(int vol_pot, double J, double &dU, double &d2U) {
+  if (vol_pot == 2) {
+    const double e = exp(J - 1.0), iJ = 1.0 / J;
+    dU = 0.5 * (e - iJ);
+    d2U = 0.5 * (e + iJ * iJ);
+  } else if (vol_pot == 3) {
+    const double iJ = 1.0 / J;
+    dU = 0.5 * (J - 1.0) * iJ + 0.5 * log(J);
+    d2U = iJ - 0.5 * (J - 1.0) * iJ * iJ;
+  } else {
+    dU = J - 1.0;
+    d2U = 1.0;
+  }
+}
 
 __device__ __forceinline__ double sdot(const double *a, const double *b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + 2.0 * (a[3] * b[3] + a[4] * b[4] + a[5] * b[5]);
@@ -125,7 +144,9 @@ __device__ __forceinline__ void spatial_update(const Mat &mat, const double *F, 
   str[0] -= mubar;
   str[1] -= mubar;
   str[2] -= mubar;
-  const double pJ = kap * J * (J - 1.0);
+  double dU, d2U;
+  vol_derivs(mat.vol_pot, J, dU, d2U);
+  const double pJ = kap * J * dU;
   double r = 1.0;
   o.a4 = 0.0;
   o.a5 = 0.0;
@@ -193,8 +214,8 @@ __device__ __forceinline__ void spatial_update(const Mat &mat, const double *F, 
   o.tau[0] += pJ;
   o.tau[1] += pJ;
   o.tau[2] += pJ;
-  o.a1 = 2.0 * mubar * r - 2.0 * kap * J * (J - 1.0);
-  o.a2 = kap * J * (2.0 * J - 1.0) - (2.0 / 3.0) * mubar * r;
+  o.a1 = 2.0 * mubar * r - 2.0 * pJ;
+  o.a2 = kap * (J * dU + J * J * d2U) - (2.0 / 3.0) * mubar * r;
 }
 
 // HE with the linear deviatoric potential at one point: tau, the volumetric
@@ -212,7 +233,9 @@ __device__ __forceinline__ void linear_dev_update(const Mat &mat, const double *
   b2[3] = b[5] * b[4] + b[1] * b[3] + b[3] * b[2];
   b2[4] = b[0] * b[4] + b[5] * b[3] + b[4] * b[2];
   b2[5] = b[0] * b[5] + b[5] * b[1] + b[4] * b[3];
-  const double pJ = kap * J * (J - 1.0);
+  double dU, d2U;
+  vol_derivs(mat.vol_pot, J, dU, d2U);
+  const double pJ = kap * J * dU;
 #pragma unroll
   for (int i = 0; i < 6; i++) {
     o.tau[i] = G * (b2[i] - b[i]) + (i < 3 ? pJ : 0.0);
@@ -220,8 +243,8 @@ __device__ __forceinline__ void linear_dev_update(const Mat &mat, const double *
     o.n[i] = b[i];
     o.D[i] = 0.0;
   }
-  o.a1 = -2.0 * kap * J * (J - 1.0);
-  o.a2 = kap * J * (2.0 * J - 1.0);
+  o.a1 = -2.0 * pJ;
+  o.a2 = kap * (J * dU + J * J * d2U);
   o.a4 = 0.0;
   o.a5 = 0.0;
 }

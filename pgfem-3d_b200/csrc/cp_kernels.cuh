@@ -580,6 +580,12 @@ struct CpElemArgs {
   const double *state_n;
   const double *out;  // kCpOut * ne
   double *R, *K;
+  // element level (stiffmatel_fd / resid_on_elem): the listed elements' dense
+  // element vector fe[nlist][12] and matrix lk[nlist][12][12] (idx_K order,
+  // every DOF of the element) instead of the CSR scatter; lk may be nullptr
+  const int *elist;
+  long nlist;
+  double *lk_out, *fe_out;
   Mat mat;
 };
 
@@ -589,8 +595,18 @@ struct CpElemArgs {
 // written through the first Piola stress P = pJ F M S M^T of the element:
 // R_a = w P grad N_a and dR_a/du = w dP grad N_a.
 __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
-  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (e >= A.ne) return;
+  const long it = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const bool dense = A.elist != nullptr;
+  if (it >= (dense ? A.nlist : A.ne)) return;
+  const long e = dense ? (long)A.elist[it] : it;
+  double *fe = dense ? A.fe_out + it * 12 : nullptr;
+  double *lk = dense && A.lk_out ? A.lk_out + it * 144 : nullptr;
+  if (dense) {  // zero outputs for an inverted element (counted by the F kernel)
+#pragma unroll
+    for (int k = 0; k < 12; k++) fe[k] = 0.0;
+    if (lk)
+      for (int k = 0; k < 144; k++) lk[k] = 0.0;
+  }
   const long S = A.ne;
   const double w = A.detJw[e];
   if (!(w > 0.0)) return;
@@ -645,14 +661,23 @@ __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
 #pragma unroll
     for (int i = 0; i < 3; i++)
       Re[a * 3 + i] = w * pJ * (Pk[i * 3] * gN[a][0] + Pk[i * 3 + 1] * gN[a][1] + Pk[i * 3 + 2] * gN[a][2]);
-  const unsigned mk[4] = {A.mask[nd[0]], A.mask[nd[1]], A.mask[nd[2]], A.mask[nd[3]]};
+  // dense element outputs take every DOF of the element
+  const unsigned mk[4] = {dense ? 7u : A.mask[nd[0]], dense ? 7u : A.mask[nd[1]], dense ? 7u : A.mask[nd[2]],
+                          dense ? 7u : A.mask[nd[3]]};
+  if (dense) {
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+    for (int k = 0; k < 12; k++) fe[k] = Re[k];
+    if (!lk) return;
+  } else {
 #pragma unroll
-    for (int i = 0; i < 3; i++) {
-      const int id = A.dof[i * A.nn + nd[a]];
-      if (id > 0) atomicAdd(A.R + (id - 1), Re[a * 3 + i]);
-    }
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int id = A.dof[i * A.nn + nd[a]];
+        if (id > 0) atomicAdd(A.R + (id - 1), Re[a * 3 + i]);
+      }
+    if (!A.K) return;
+  }
   // tangent columns (node wn, component gc)
   for (int wn = 0; wn < 4; wn++) {
     if (!mk[wn]) continue;
@@ -712,6 +737,14 @@ __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
         for (int k = 0; k < 3; k++) trMdM += Mi[i * 3 + k] * dM[k * 3 + i];
 #pragma unroll
       for (int i = 0; i < 9; i++) dP[i] = w * pJ * (dP[i] + q3[i] - trMdM * Pk[i]);
+      if (dense) {  // column (wn, gc) of the element matrix, idx_K order
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+          for (int i = 0; i < 3; i++)
+            lk[(a * 3 + i) * 12 + wn * 3 + gc] =
+                dP[i * 3] * gN[a][0] + dP[i * 3 + 1] * gN[a][1] + dP[i * 3 + 2] * gN[a][2];
+        continue;
+      }
       // scatter the column into the rows of the element's nodes
       const long pcol = (e * 4 + 0) * 4 + wn;  // pos of (a, wn) at (e*4 + a)*4 + wn
       for (int a = 0; a < 4; a++) {

@@ -730,6 +730,34 @@ int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model
   return PGFEM_GPU_OK;
 }
 
+// The material of a J2 entry (CM_J2P_PARAM::read_param,
+// src/cm_j2_plasticity.cc:865-932: G and nu from the mesh file's material line,
+// then beta hp k0 and the damage block).  Elasticity is the spatial
+// neo-Hookean form with the material line's volumetric potential; the return
+// map is J2 with yield function ||dev tau|| - sqrt(2/3) (k0 + hp ep) and linear
+// isotropic hardening: sigma_y = k0, H = hp.  beta = 0 (the reference's own
+// driver value, tests/constitutive_model/cm_j2_plasticity_driver.cc:64-83) is
+// the only hardening mix carried; damage must be off (mu = 0: the damage
+// variable never evolves).  Other values return PGFEM_GPU_EINVAL.
+int pgfem_input_j2_material(const pgfem_model_params *mp, double E, double nu, int vol_pot,
+                            pgfem_material_desc *out) {
+  if (!mp || !out || mp->model_type != PGFEM_CM_J2_PLASTICITY_DAMAGE || mp->np != 14) return PGFEM_GPU_EINVAL;
+  const double beta = mp->p[0], hp = mp->p[1], k0 = mp->p[2], mu = mp->p[3];
+  if (beta != 0.0 || mu != 0.0 || !(k0 > 0.0) || !(hp >= 0.0) || !(E > 0.0) || !(nu > -1.0 && nu < 0.5))
+    return PGFEM_GPU_EINVAL;
+  if (!(vol_pot <= 0 || vol_pot == 2 || vol_pot == 3 || vol_pot == 99)) return PGFEM_GPU_EINVAL;
+  pgfem_material_desc m{};
+  m.model = PGFEM_MODEL_J2;
+  m.E = E;
+  m.nu = nu;
+  m.sigma_y = k0;
+  m.H = hp;
+  m.dev_pot = 1;
+  m.vol_pot = vol_pot <= 0 ? 99 : vol_pot;
+  *out = m;
+  return PGFEM_GPU_OK;
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
@@ -740,7 +768,10 @@ int pgfem_input_read_model_params(const char *path, int max_entries, pgfem_model
 // src/plasticity_model_none.cc:298-311): Fn, Fnm1; CP (CP_PARAM::write_restart,
 // src/plasticity_model.cc:883-911): Fn, Fnm1, pFn, pFnm1 (cm_write_tensor_restart,
 // src/constitutive_model.cc:4005-4013, one tensor of 9 per line), tau_n[12],
-// gamma_dot_n[12], then g_n g_nm1 L_n L_nm1.  Numbers in %.17e.
+// gamma_dot_n[12], then g_n g_nm1 L_n L_nm1; J2 (CM_J2P_PARAM::write_restart,
+// src/cm_j2_plasticity.cc:784-808): Fn, pSn, Fnm1, pSnm1, then w_n w_nm1 X_n
+// X_nm1 H_n H_nm1 ep_n ep_nm1 gam_n gam_nm1 on one line and the damage flag
+// (an integer) on the next.  Numbers in %.17e.
 // ---------------------------------------------------------------------------
 extern "C" {
 
@@ -748,6 +779,7 @@ int pgfem_restart_block_size(int model) {
   switch (model) {
     case PGFEM_MODEL_HE: return 18;
     case PGFEM_MODEL_CP: return 4 * 9 + 12 + 12 + 4;
+    case PGFEM_MODEL_J2: return 4 * 9 + 10 + 1;
     default: return -1;
   }
 }
@@ -773,6 +805,12 @@ int pgfem_restart_format(const char *path, long nn, long ne, int n_ip, int model
       const double *b = blocks + ((size_t)e * n_ip + q) * bs;
       tensor(b);
       tensor(b + 9);
+      if (model == PGFEM_MODEL_J2) {
+        tensor(b + 18);
+        tensor(b + 27);
+        for (int k = 0; k < 10; k++) fprintf(f, k < 9 ? "%.17e " : "%.17e\n", b[36 + k]);
+        fprintf(f, "%d\n", (int)b[46]);
+      }
       if (model == PGFEM_MODEL_CP) {
         tensor(b + 18);
         tensor(b + 27);
@@ -807,7 +845,10 @@ int pgfem_restart_parse(const char *path, long nn, long ne, int n_ip, int model,
     for (int q = 0; q < n_ip; q++) {
       double *b = blocks + ((size_t)e * n_ip + q) * bs;
       for (int k = 0; k < bs; k++)
-        if (!t.num(b[k])) return bad(model == PGFEM_MODEL_CP ? "crystal plasticity block" : "hyperelastic block");
+        if (!t.num(b[k]))
+          return bad(model == PGFEM_MODEL_CP   ? "crystal plasticity block"
+                     : model == PGFEM_MODEL_J2 ? "J2 plasticity block"
+                                               : "hyperelastic block");
     }
   }
   if (!t.eof()) return bad("trailing data (mesh or model does not match the file)");

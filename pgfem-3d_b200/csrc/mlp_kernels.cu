@@ -29,7 +29,9 @@ struct pgfem_mlp {
   double *loss = nullptr;
   float h_scale[kScale];
   long adam_t = 0;
-  pgb::mlp::MlpDev dev_view() const { return {w, bias, scale, err}; }
+  uint64_t wait_ns = pgb::mlp::kWaitNs;
+  int stall = 0;  // the next forward pass withholds its first MMA chain (failure-path tests)
+  pgb::mlp::MlpDev dev_view() const { return {w, bias, scale, err, wait_ns, 0}; }
 };
 
 namespace {
@@ -253,6 +255,13 @@ int pgfem_mlp_fit_scaling(pgfem_mlp *m, long n, const float *d_x, const float *d
   return pgfem_mlp_set_scaling(m, xm, xs, ys);
 }
 
+int pgfem_mlp_set_wait_test(pgfem_mlp *m, double limit_s, int stall_next_forward) {
+  if (!m || !(limit_s > 0.0) || limit_s > 60.0) return PGFEM_GPU_EINVAL;
+  m->wait_ns = (uint64_t)(limit_s * 1e9);
+  m->stall = stall_next_forward ? 1 : 0;
+  return PGFEM_GPU_OK;
+}
+
 int pgfem_mlp_predict_device(pgfem_mlp *m, long n, const float *d_x, float *d_y, void *stream) {
   if (!m || n < 0 || (n && (!d_x || !d_y))) return PGFEM_GPU_EINVAL;
   if (n == 0) return PGFEM_GPU_OK;
@@ -260,7 +269,10 @@ int pgfem_mlp_predict_device(pgfem_mlp *m, long n, const float *d_x, float *d_y,
   if (r) return r;
   const long tiles = (n + kTile - 1) / kTile;
   const unsigned grid = (unsigned)std::min<long>(tiles, num_sms());
-  k_mlp_forward<<<grid, kThreads, kInfSmem, (cudaStream_t)stream>>>(m->dev_view(), n, d_x, d_y);
+  pgb::mlp::MlpDev dv = m->dev_view();
+  dv.stall = m->stall;
+  m->stall = 0;
+  k_mlp_forward<<<grid, kThreads, kInfSmem, (cudaStream_t)stream>>>(dv, n, d_x, d_y);
   MCK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }

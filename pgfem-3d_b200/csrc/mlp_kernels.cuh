@@ -62,9 +62,11 @@ struct MlpDev {
   const float *b;          // kNPB
   const float *scale;      // kScale
   unsigned *err;           // bit 0: an mbarrier wait ran out
+  uint64_t wait_ns;        // bound of every mbarrier wait
+  int stall;               // test of the failure path: the first tile's first MMA chain is not issued
 };
 
-constexpr uint64_t kWaitNs = 2000000000ull;  // bound of every mbarrier wait (2 s)
+constexpr uint64_t kWaitNs = 2000000000ull;  // default bound of every mbarrier wait (2 s)
 
 // ---------------------------------------------------------------- helpers --
 
@@ -130,8 +132,8 @@ __device__ __forceinline__ void mbar_init(uint32_t a, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Bounded wait for the completion of phase `parity`; false after kWaitNs.
-__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
+// Bounded wait for the completion of phase `parity`; false after `limit` ns.
+__device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity, uint64_t limit) {
   const uint64_t t0 = gtimer();
   for (;;) {
     uint32_t ok;
@@ -142,7 +144,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t a, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (gtimer() - t0 > kWaitNs) return false;
+    if (gtimer() - t0 > limit) return false;
   }
 }
 
@@ -275,7 +277,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     __syncthreads();
     tc_after();
     for (int l = 0; l < 4 && !fail; l++) {
-      if (tid == 0) {
+      // (with m.stall the CTA's first chain and its commit are not issued: the
+      // wait below runs out with no MMA in flight)
+      if (tid == 0 && !(m.stall && l == 0 && t == blockIdx.x)) {
         if (l == 0)
           mma_chain(tbase, kmajor(ab + sX0, kInP), kmajor(ab + sW1, kInP), kInP / 16, ID_H);
         else if (l < 3)
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           mma_chain(tbase, kmajor(ab + sH1, kH), kmajor(ab + sW4, kH), kH / 16, ID_O);
         mma_commit(mb);
       }
-      const bool ok = mbar_wait(mb, phase);
+      const bool ok = mbar_wait(mb, phase, m.wait_ns);
       phase ^= 1;
       if (__syncthreads_or(!ok)) {
         fail = true;
@@ -308,7 +312,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
   }
   if (fail) {
-    mbar_wait(mb, phase ^ 1u);  // bounded: let a late MMA finish before its TMEM is released
+    mbar_wait(mb, phase ^ 1u, m.wait_ns);  // bounded: let a late MMA finish before its TMEM is released
     if (tid == 0) atomicOr(m.err, 1u);
   }
   tc_before();
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_after();
   };
   auto wait_mma = [&]() -> bool {
-    const bool ok = mbar_wait(mb, phase);
+    const bool ok = mbar_wait(mb, phase, m.wait_ns);
     phase ^= 1;
     if (__syncthreads_or(!ok)) return false;
     tc_after();
@@ -503,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1)
     dw_rows(cZ1, kIn, oW1);
   } while (false);
   if (fail) {
-    mbar_wait(mb, phase ^ 1u);  // bounded: let a late MMA finish before its TMEM is released
+    mbar_wait(mb, phase ^ 1u, m.wait_ns);  // bounded: let a late MMA finish before its TMEM is released
     if (tid == 0) atomicOr(m.err, 1u);
   }
   tc_before();

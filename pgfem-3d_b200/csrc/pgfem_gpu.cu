@@ -82,6 +82,9 @@ struct pgfem_gpu_ctx {
   int ngroups = 0;
   unsigned *sched_ticket = nullptr;
   int sched_epb = 0, sched_grab = 0;  // elements per block (0: default), tiles per steal (0: static)
+  // failure-path tests: bound of the hand-off waits, one-shot withheld hand-off
+  unsigned long long wait_ns = 2000000000ull;
+  int stall_next = 0;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -160,6 +163,7 @@ Mat make_mat(const pgfem_material_desc *m) {
   Mat r{};
   r.model = m->model;
   r.dev_pot = m->model == PGFEM_MODEL_HE && m->dev_pot == 2 ? 2 : 1;
+  r.vol_pot = (m->vol_pot == 2 || m->vol_pot == 3) && m->model != PGFEM_MODEL_CP ? m->vol_pot : 99;
   r.mu = m->E / (2.0 * (1.0 + m->nu));
   r.kappa = (2 * r.mu * (1 + m->nu)) / (3 * (1 - 2 * m->nu));
   r.sy = m->sigma_y;
@@ -319,6 +323,7 @@ AsmArgs base_args(const pgfem_gpu_ctx *c) {
   a.shp = c->shp;
   a.elem_group = c->elem_group;
   a.F0_tab = c->F0_tab;
+  a.wait_ns = c->wait_ns;
   return a;
 }
 
@@ -428,6 +433,8 @@ template <int MODEL, int TE>
 int launch_p1ws_te(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
   AsmArgs a = a0;
   a.qrec = c->qrec;
+  a.stall = c->stall_next;
+  c->stall_next = 0;
   if (c->sched_grab > 0) {
     a.ticket = c->sched_ticket;
     a.grab = c->sched_grab;
@@ -514,7 +521,18 @@ int ensure_K_scratch(pgfem_gpu_ctx *c) {
   return dalloc(c, &c->d_K, std::max<long>(1, c->nnz));
 }
 
-int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStream_t s) {
+// element-level outputs of assemble_cp: the listed elements' dense blocks
+struct CpElemList {
+  const int *list;
+  long n;
+  double *lk, *fe;
+};
+
+// The CP path: F per element, the local Newton (optionally from the network's
+// guess), the consistent tangent, then the element stage -- scattered into the
+// CSR (d_R, d_K) or, with el, the listed elements' dense blocks.
+int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStream_t s,
+                const CpElemList *el = nullptr) {
   k_cp_F<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(c->X, c->unode, c->conn, c->nn, c->ne, c->F0, c->cp_F,
                                                           c->cp_detJw, c->status);
   CK(cudaGetLastError());
@@ -583,7 +601,7 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
     CK(cudaEventRecord(e1, s));
     c->events.emplace_back(e0, e1);
   }
-  if (d_K || d_R) {
+  if (d_K || d_R || el) {
     CpElemArgs b{};
     b.X = c->X;
     b.conn = c->conn;
@@ -601,6 +619,15 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
     b.R = d_R;
     b.K = d_K;
     b.mat = c->mat;
+    if (el) {  // element level: dense blocks of the listed elements
+      b.elist = el->list;
+      b.nlist = el->n;
+      b.lk_out = el->lk;
+      b.fe_out = el->fe;
+      k_cp_element<<<(unsigned)((el->n + 127) / 128), 128, 0, s>>>(b);
+      CK(cudaGetLastError());
+      return PGFEM_GPU_OK;
+    }
     if (!d_K) return PGFEM_GPU_EINVAL;
     k_cp_element<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(b);
     CK(cudaGetLastError());
@@ -720,13 +747,16 @@ void build_colours(const pgfem_mesh_desc *m, std::vector<int> &elems, std::vecto
 }
 
 // Element processing order of the tensor-core quadratic-tet kernel: columns
-// of 32 x 32 element-size bins across the two shorter axes of the bounding
+// of 6 x 6 element-size bins across the two shorter axes of the bounding
 // box, swept along the longest axis, bins in lexicographic order inside a
 // column (element centroids from the four vertex nodes; element size h =
 // (6 V / ne)^(1/3)).  Nearby elements share CSR rows, so in this order a row's
 // contributions arrive within about one column layer and its cache lines stay
 // in L2 between them (in the mesh's own order a whole cross-section is live).
-// Any permutation gives the same sums; this one only shapes the traffic.
+// Any permutation gives the same sums; this one only shapes the traffic.  The
+// width was measured on the 64^3-cell quadratic-tet mesh: 6 bins 6.56, 4 bins
+// 6.85, 8 bins 6.87, 12 bins 7.54, 32 bins 7.67 ms per R+K iterate, one
+// cross-section 8.24 ms.
 std::vector<int> locality_order(const pgfem_mesh_desc *m) {
   const long ne = m->ne;
   std::vector<double> cen((size_t)3 * ne);
@@ -752,7 +782,7 @@ std::vector<int> locality_order(const pgfem_mesh_desc *m) {
     return (long)std::min(std::max(v, 0.0), 1.0e6);
   };
   const long nb1 = (long)((hi[c1] - lo[c1]) / h) + 1, nb2 = (long)((hi[c2] - lo[c2]) / h) + 1;
-  const long nbs = (long)((hi[sw] - lo[sw]) / h) + 1, T = 32;
+  const long nbs = (long)((hi[sw] - lo[sw]) / h) + 1, T = 6;
   const long nc2 = (nb2 + T - 1) / T;
   std::vector<std::pair<unsigned long long, int>> key((size_t)ne);
   for (long e = 0; e < ne; e++) {
@@ -789,7 +819,8 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
       m->nn <= 0 || m->ne <= 0 || nrows != m->ndof || !Ap || !Ai)
     return PGFEM_GPU_EINVAL;
   if (mat->model < 0 || mat->model > 2) return PGFEM_GPU_EINVAL;
-  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE))
+  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE) ||
+      !(mat->vol_pot <= 0 || mat->vol_pot == 99 || ((mat->vol_pot == 2 || mat->vol_pot == 3) && mat->model != PGFEM_MODEL_CP)))
     return PGFEM_GPU_EINVAL;
   if (mat->model == PGFEM_MODEL_CP && (m->nne != 4 || !m->R_cp || !(mat->m > 0) || !(mat->g0 > 0) ||
                                        !(mat->gs_0 > mat->g0)))
@@ -962,6 +993,13 @@ int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
   return PGFEM_GPU_OK;
 }
 
+int pgfem_gpu_set_wait_test(pgfem_gpu_ctx *c, double limit_s, int stall_next_assembly) {
+  if (!c || !(limit_s > 0.0) || limit_s > 60.0) return PGFEM_GPU_EINVAL;
+  c->wait_ns = (unsigned long long)(limit_s * 1e9);
+  c->stall_next = stall_next_assembly ? 1 : 0;
+  return PGFEM_GPU_OK;
+}
+
 long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *c) { return c ? c->bytes : -1; }
 long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
@@ -1077,6 +1115,16 @@ int pgfem_gpu_fp64_peak(double *tflops) {
   return fp64_peak_probe(tflops);
 }
 
+int pgfem_gpu_binary_version(int *version) {
+  if (!version) return PGFEM_GPU_EINVAL;
+  int r = check_device();
+  if (r) return r;
+  cudaFuncAttributes fa;
+  CK(cudaFuncGetAttributes(&fa, k_expand_u));
+  *version = fa.binaryVersion;
+  return PGFEM_GPU_OK;
+}
+
 int pgfem_gpu_set_state(pgfem_gpu_ctx *c, const double *st) {
   if (!c || !st) return PGFEM_GPU_EINVAL;
   if (!c->nstate) return PGFEM_GPU_OK;
@@ -1179,19 +1227,36 @@ int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_
                             const double *presc_nm1, const double *presc_n, const double *state_nm1) {
   if (!c || !path || (c->ndof && (!u_nm1 || !u_n)) || (c->npres && (!presc_nm1 || !presc_n)))
     return PGFEM_GPU_EINVAL;
-  if (c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
   std::vector<double> un1, un, Fn1, Fn;
   int r;
   if ((r = nodal_and_F(c, u_nm1, presc_nm1, un1, Fn1)) || (r = nodal_and_F(c, u_n, presc_n, un, Fn))) return r;
   const int bs = pgfem_restart_block_size(c->model);
   std::vector<double> blocks((size_t)bs * c->nqp, 0.0);
   std::vector<double> st;
-  if (c->model == PGFEM_MODEL_CP) {
+  if (c->model == PGFEM_MODEL_CP || c->model == PGFEM_MODEL_J2) {
     st.resize((size_t)10 * c->nqp);
     if ((r = pgfem_gpu_get_state(c, 0, st.data()))) return r;
   }
   for (long q = 0; q < c->nqp; q++) {
     double *b = blocks.data() + (size_t)bs * q;
+    if (c->model == PGFEM_MODEL_J2) {
+      // the reference's plastic stress pS <-> this path's Cp^-1: pS = G (I - Cp^-1)
+      // (zero in the initial state, as the reference's set_init_vals); the damage
+      // variables are written at their undamaged values, gam_n = sqrt(3/2)(ep_n - ep_nm1)
+      const double *sn = st.data() + 10 * q, *sm = state_nm1 ? state_nm1 + 10 * q : sn;
+      const double G = c->mat.mu;
+      for (int k = 0; k < 9; k++) {
+        const double I = (k % 4 == 0) ? 1.0 : 0.0;
+        b[k] = Fn[9 * q + k];
+        b[9 + k] = G * (I - sn[k]);
+        b[18 + k] = Fn1[9 * q + k];
+        b[27 + k] = G * (I - sm[k]);
+      }
+      b[42] = sn[9];
+      b[43] = sm[9];
+      b[44] = std::sqrt(1.5) * (sn[9] - sm[9]);
+      continue;
+    }
     for (int k = 0; k < 9; k++) {
       b[k] = Fn[9 * q + k];
       b[9 + k] = Fn1[9 * q + k];
@@ -1212,7 +1277,6 @@ int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_
 
 int pgfem_gpu_read_restart(pgfem_gpu_ctx *c, const char *path, double *u_nm1, double *u_n) {
   if (!c || !path || (c->ndof && (!u_nm1 || !u_n))) return PGFEM_GPU_EINVAL;
-  if (c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
   const int bs = pgfem_restart_block_size(c->model);
   std::vector<double> un1((size_t)3 * c->nn), un((size_t)3 * c->nn), blocks((size_t)bs * c->nqp);
   int r = pgfem_restart_parse(path, c->nn, c->ne, c->nqp_e, c->model, un1.data(), un.data(), blocks.data());
@@ -1241,6 +1305,16 @@ int pgfem_gpu_read_restart(pgfem_gpu_ctx *c, const char *path, double *u_nm1, do
     if ((r = pgfem_gpu_set_state(c, st.data()))) return r;
     CK(cudaMemcpyAsync(c->cp_Fn, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+  }
+  if (c->model == PGFEM_MODEL_J2) {  // Cp^-1 = I - pS / G, eqps = ep_n
+    std::vector<double> st((size_t)10 * c->nqp);
+    const double G = c->mat.mu;
+    for (long q = 0; q < c->nqp; q++) {
+      const double *b = blocks.data() + (size_t)bs * q;
+      for (int k = 0; k < 9; k++) st[10 * q + k] = ((k % 4 == 0) ? 1.0 : 0.0) - b[9 + k] / G;
+      st[10 * q + 9] = b[42];
+    }
+    if ((r = pgfem_gpu_set_state(c, st.data()))) return r;
   }
   return PGFEM_GPU_OK;
 }
@@ -1293,9 +1367,8 @@ int pgfem_gpu_read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, int clear) {
 }
 
 static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
-                         const double *presc, double *lk, double *fe, pgfem_gpu_status *st) {
+                         const double *presc, double dt, double *lk, double *fe, pgfem_gpu_status *st) {
   if (!c || nel < 0 || (nel && (!elems || !fe)) || !u || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
-  if (c->model == PGFEM_MODEL_CP) return PGFEM_GPU_EINVAL;
   if (nel == 0) return PGFEM_GPU_OK;
   for (long i = 0; i < nel; i++)
     if (elems[i] < 0 || elems[i] >= c->ne) return PGFEM_GPU_EINVAL;
@@ -1324,12 +1397,19 @@ static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const do
   const long n3 = 3 * c->nn;
   k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, c->stream>>>(c->dof, c->nn, c->d_u,
                                                                    c->npres ? c->d_presc : nullptr, c->unode);
-  AsmArgs a = base_args(c);
-  a.elist = d_el;
-  a.nlist = nel;
-  a.lk_out = d_lk;
-  a.fe_out = d_fe;
-  r = lk ? dispatch<false, true, true>(c, a, nel, c->stream) : dispatch<false, false, true>(c, a, nel, c->stream);
+  if (c->model == PGFEM_MODEL_CP) {
+    // the local update runs for every point of the context (its state at
+    // t_{n+1} is that of an assembly at u), then the listed elements' blocks
+    CpElemList L{d_el, nel, d_lk, d_fe};
+    r = assemble_cp(c, nullptr, nullptr, dt, c->stream, &L);
+  } else {
+    AsmArgs a = base_args(c);
+    a.elist = d_el;
+    a.nlist = nel;
+    a.lk_out = d_lk;
+    a.fe_out = d_fe;
+    r = lk ? dispatch<false, true, true>(c, a, nel, c->stream) : dispatch<false, false, true>(c, a, nel, c->stream);
+  }
   if (!r) {
     cudaMemcpyAsync(fe, d_fe, sizeof(double) * nel * nd, cudaMemcpyDeviceToHost, c->stream);
     if (lk) cudaMemcpyAsync(lk, d_lk, sizeof(double) * nel * nd * nd, cudaMemcpyDeviceToHost, c->stream);
@@ -1343,15 +1423,13 @@ static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const do
 int pgfem_gpu_stiffmatel_fd(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
                             const double *presc, double dt, double *lk, double *fe,
                             pgfem_gpu_status *st) {
-  (void)dt;
   if (!lk) return PGFEM_GPU_EINVAL;
-  return element_level(c, nel, elems, u, presc, lk, fe, st);
+  return element_level(c, nel, elems, u, presc, dt, lk, fe, st);
 }
 
 int pgfem_gpu_resid_on_elem(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
                             const double *presc, double dt, double *fe, pgfem_gpu_status *st) {
-  (void)dt;
-  return element_level(c, nel, elems, u, presc, nullptr, fe, st);
+  return element_level(c, nel, elems, u, presc, dt, nullptr, fe, st);
 }
 
 int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const double *F, double dt,
@@ -1359,7 +1437,8 @@ int pgfem_gpu_cm_integrate(const pgfem_material_desc *mat, long nqp, const doubl
                            double *L, int *qp_status) {
   if (!mat || nqp < 0 || (nqp && (!F || !S))) return PGFEM_GPU_EINVAL;
   if (mat->model != PGFEM_MODEL_HE && mat->model != PGFEM_MODEL_J2) return PGFEM_GPU_EINVAL;
-  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE))
+  if (mat->dev_pot < 0 || mat->dev_pot > 2 || (mat->dev_pot == 2 && mat->model != PGFEM_MODEL_HE) ||
+      !(mat->vol_pot <= 0 || mat->vol_pot == 99 || ((mat->vol_pot == 2 || mat->vol_pot == 3) && mat->model != PGFEM_MODEL_CP)))
     return PGFEM_GPU_EINVAL;
   if (mat->model == PGFEM_MODEL_J2 && nqp && (!state_n || !state_np1)) return PGFEM_GPU_EINVAL;
   int r = check_device();
@@ -1585,11 +1664,16 @@ int pgfem_gpu_cp_integrate_noalloc(const pgfem_material_desc *mat, long nqp, con
   int dev = 0;
   CK(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kNaMaxDevices) return PGFEM_GPU_ENODEV;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (st) {  // reading the counts back waits for the stream: not allowed while it is captured
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(s, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return PGFEM_GPU_EINVAL;
+  }
   NaDevice *d = nullptr;
   if ((r = noalloc_setup(dev, &d))) return r;
   if (st) *st = pgfem_gpu_status{};
   if (nqp == 0) return PGFEM_GPU_OK;
-  cudaStream_t s = (cudaStream_t)stream;
   // the ticket counter and the failure counters must start at zero; the work
   // record is written in full for every point before it is read
   CK(cudaMemsetAsync(d->scratch, 0, sizeof(double) * kNaHeader, s));

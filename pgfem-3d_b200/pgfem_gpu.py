@@ -31,7 +31,7 @@ class MaterialDesc(C.Structure):
                 ("gamma_dot_0", C.c_double), ("m", C.c_double), ("G0", C.c_double),
                 ("g0", C.c_double), ("gs_0", C.c_double), ("gamma_dot_s", C.c_double),
                 ("w", C.c_double), ("cp_tol", C.c_double), ("cp_max_iter", C.c_int),
-                ("dev_pot", C.c_int)]
+                ("dev_pot", C.c_int), ("vol_pot", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -71,6 +71,8 @@ def lib():
             "pgfem_gpu_create": (C.c_int, [_P, _P, _P, _P, C.c_long, _P]),
             "pgfem_gpu_destroy": (C.c_int, [_P]),
             "pgfem_gpu_set_scatter_mode": (C.c_int, [_P, C.c_int]),
+            "pgfem_gpu_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
+            "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_device_bytes": (C.c_long, [_P]),
             "pgfem_gpu_nnz": (C.c_long, [_P]),
             "pgfem_gpu_set_state": (C.c_int, [_P, _P]),
@@ -88,6 +90,7 @@ def lib():
             "pgfem_gpu_set_timing": (C.c_int, [_P, C.c_int]),
             "pgfem_gpu_kernel_time": (C.c_int, [_P, _P, _P, C.c_int]),
             "pgfem_gpu_fp64_peak": (C.c_int, [_P]),
+            "pgfem_gpu_binary_version": (C.c_int, [_P]),
             "pgfem_gpu_set_cp_guess": (C.c_int, [_P, _P]),
             "pgfem_gpu_get_cp_iterations": (C.c_int, [_P, _P, _P]),
             "pgfem_gpu_cp_integrate_noalloc": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_double, _P, _P, _P, _P,
@@ -136,6 +139,7 @@ def lib():
             "pgfem_input_get_periodic": (C.c_int, [_P, _P]),
             "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
             "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
+            "pgfem_input_j2_material": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _P]),
             "pgfem_input_read_model_params": (C.c_int, [C.c_char_p, C.c_int, _P, _P]),
             "pgfem_restart_block_size": (C.c_int, [C.c_int]),
             "pgfem_restart_format": (C.c_int, [C.c_char_p, C.c_long, C.c_long, C.c_int, C.c_int, _P, _P, _P]),
@@ -168,11 +172,12 @@ def _check(fn, r):
 
 
 def material(model, E=200e3, nu=0.3, sigma_y=0.0, H=0.0, gamma_dot_0=0.0, m=1.0, G0=0.0, g0=0.0,
-             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1):
+             gs_0=0.0, gamma_dot_s=1.0, w=0.0, cp_tol=1e-10, cp_max_iter=25, dev_pot=1, vol_pot=99):
     """Material record; dev_pot is the reference's devPotFlag for HE (1
-    neo-Hookean, 2 linear deviatoric potential)."""
+    neo-Hookean, 2 linear deviatoric potential), vol_pot its volPotFlag for HE
+    and J2 (99 U_Common, 2 and 3 the Doll-Schweizerhof forms)."""
     return MaterialDesc(model, E, nu, sigma_y, H, gamma_dot_0, m, G0, g0, gs_0, gamma_dot_s, w,
-                        cp_tol, cp_max_iter, dev_pot)
+                        cp_tol, cp_max_iter, dev_pot, vol_pot)
 
 
 # ---------------------------------------------------------------- setup ----
@@ -258,6 +263,11 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    def set_wait_test(self, limit_s, stall_next=False):
+        """Failure-path tests: hand-off wait bound (s) of the linear-tet R+K
+        kernel; stall_next withholds the next assembly's first hand-off."""
+        _check("pgfem_gpu_set_wait_test", lib().pgfem_gpu_set_wait_test(self.h, limit_s, int(stall_next)))
 
     def set_scatter_mode(self, mode):
         _check("pgfem_gpu_set_scatter_mode", lib().pgfem_gpu_set_scatter_mode(self.h, mode))
@@ -398,6 +408,13 @@ class Context:
         return fe, st
 
 
+def binary_version():
+    """Compute capability the library's kernels were built for (100 = sm_100a)."""
+    v = C.c_int(0)
+    _check("pgfem_gpu_binary_version", lib().pgfem_gpu_binary_version(C.byref(v)))
+    return v.value
+
+
 def fp64_peak_tflops():
     t = C.c_double()
     _check("pgfem_gpu_fp64_peak", lib().pgfem_gpu_fp64_peak(C.byref(t)))
@@ -469,6 +486,11 @@ class Mlp:
         p = np.ascontiguousarray(p, dtype=np.float32)
         assert p.size == self.num_params()
         _check("pgfem_mlp_set_params", lib().pgfem_mlp_set_params(self.h, _ptr(p)))
+
+    def set_wait_test(self, limit_s, stall_next=False):
+        """Failure-path tests: tensor-core completion wait bound (s); stall_next
+        withholds the next forward pass's first MMA chain per CTA."""
+        _check("pgfem_mlp_set_wait_test", lib().pgfem_mlp_set_wait_test(self.h, limit_s, int(stall_next)))
 
     def set_scaling(self, x_mean, x_std, y_std):
         a = [np.ascontiguousarray(v, dtype=np.float32) for v in (x_mean, x_std, y_std)]
@@ -712,12 +734,14 @@ class InputMesh:
 
     def material(self, imat=0, model=MODEL_HE, **kw):
         """pgfem_material_desc from material line imat: E = Ex, nu = nyz (the
-        isotropic entries), dev_pot = devPotFlag for HE; keywords add or
-        override fields (J2 / CP parameters)."""
+        isotropic entries), dev_pot = devPotFlag for HE, vol_pot = volPotFlag
+        for HE and J2; keywords add or override fields (J2 / CP parameters)."""
         m = self.materials[imat]
         args = dict(E=m[0], nu=m[6])
         if model == MODEL_HE:
             args["dev_pot"] = int(self.dev_pot[imat])
+        if model in (MODEL_HE, MODEL_J2) and int(self.vol_pot[imat]) in (2, 3):
+            args["vol_pot"] = int(self.vol_pot[imat])
         args.update(kw)
         return material(model, **args)
 
@@ -769,6 +793,14 @@ def cp_material(mp, E, nu, cp_tol=1e-10, cp_max_iter=25):
     p = list(mp.p)[:7]
     return material(MODEL_CP, E=E, nu=nu, gamma_dot_0=p[0], m=p[1], G0=p[2], g0=p[3], gs_0=p[4],
                     gamma_dot_s=p[5], w=p[6], cp_tol=cp_tol, cp_max_iter=cp_max_iter)
+
+
+def j2_material(mp, E, nu, vol_pot=99):
+    """pgfem_material_desc of a J2 model_params entry (sigma_y = k0, H = hp;
+    EINVAL for beta != 0 or active damage)."""
+    out = MaterialDesc()
+    _check("pgfem_input_j2_material", lib().pgfem_input_j2_material(C.byref(mp), E, nu, vol_pot, C.byref(out)))
+    return out
 
 
 def euler_rotation(angles):

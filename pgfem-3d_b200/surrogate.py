@@ -62,11 +62,15 @@ def train(x, t, seed=0, epochs=30, batch=8192, lr=2e-3, lr_min=2e-5):
     return m, hist, time.time() - t0
 
 
-def guess_from_prediction(p, y, state_n):
+def guess_from_prediction(p, y, state_n, points=None):
     """Newton guess (nqp x 10: M0 9, g0) from predicted slip increments y (nqp x 12),
-    the same arithmetic as the device kernel k_cp_guess (numpy, FP64)."""
+    the same arithmetic as the device kernel k_cp_guess (numpy, FP64); with
+    points, y and state_n are those of the listed points only."""
     s, n = wl.fcc_slip_systems()
     R = p.R_cp.reshape(-1, 3, 3)
+    if points is not None:
+        R = R[np.asarray(points)]
+        state_n = np.asarray(state_n)[np.asarray(points)] if len(state_n) == p.R_cp.shape[0] else state_n
     rs = np.einsum("eij,aj->eai", R, s)
     rn = np.einsum("eij,aj->eai", R, n)
     P = np.einsum("eai,eaj->eaij", rs, rn)

@@ -1,6 +1,6 @@
 """Generates the box patch-test fixtures from the PGFem3D source tree.
 
-    python tests/golden/make_box_fixtures.py [/path/to/pgfem3d]
+    python tests/golden/make_box_fixtures.py /path/to/pgfem3d
 
 Reads the reference's 1-rank tension_disp inputs
 (verification_tests/box_patch_{LT,QT}/tension_disp/inputs/box_*_1CPU/box_*_0.in)
@@ -76,4 +76,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path of the PGFem3D source tree>" % sys.argv[0])
+    main(sys.argv[1])

@@ -1,6 +1,6 @@
 """Generates the crystal-plasticity box fixture from the PGFem3D source tree.
 
-    python tests/golden/make_cp_box_fixture.py [/path/to/pgfem3d]
+    python tests/golden/make_cp_box_fixture.py /path/to/pgfem3d
 
 Reads, with this library's own input readers (pgfem_input_*), the reference's
 8-partition tension case verification_tests/crystal_plasticity:
@@ -65,4 +65,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path of the PGFem3D source tree>" % sys.argv[0])
+    main(sys.argv[1])

@@ -1,6 +1,6 @@
 """Generates the FE2 micro-structure fixture from the PGFem3D source tree.
 
-    python tests/golden/make_fe2_micro_fixture.py [/path/to/pgfem3d]
+    python tests/golden/make_fe2_micro_fixture.py /path/to/pgfem3d
 
 Reads, with this library's own input readers (pgfem_input_read_mesh_bc), the
 reference's periodic micro-structure of the tube-shear FE2 case,
@@ -35,4 +35,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python %s <path of the PGFem3D source tree>" % sys.argv[0])
+    main(sys.argv[1])

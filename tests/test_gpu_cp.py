@@ -80,3 +80,45 @@ def test_cp_warm_start_same_answer_fewer_iterations(gpu):
     assert cv.all()
     assert np.abs(s1 - so).max() <= TOL * np.abs(so).max()
     ctx.set_cp_guess(None)
+
+
+def test_cp_element_level_entry_points(gpu):
+    """stiffmatel_fd / resid_on_elem for crystal plasticity (the reference's
+    stiffness_el_constitutive_model_1f with compute_dMdu,
+    src/constitutive_model.cc:2545-2676, src/plasticity_model.cc:867-881): the
+    dense element blocks of listed elements (every element DOF, idx_K order)
+    equal the oracle's element at the same state and load step (1e-10), and
+    assemble into the CSR K of the assembly call."""
+    p = wl.cp_p1(n=4, seed=2, ngrains=8)
+    ctx = p.context()
+    P, mat = oracle.from_workload(p)
+    ctx.assemble_RK(p.displacement(1), dt=p.dt)
+    ctx.commit_state()
+    st_n = ctx.get_state(0)
+    u = p.displacement(2)
+    elems = np.array([0, 5, 77, 200, p.ne - 1])
+    lk, fe, st = ctx.stiffmatel_fd(elems, u, dt=p.dt)
+    fe2, st2 = ctx.resid_on_elem(elems, u, dt=p.dt)
+    assert st.ok() and st2.ok()
+    for k, e in enumerate(elems):
+        ue = np.zeros(12)
+        for a in range(4):
+            for j in range(3):
+                i = p.ids[p.conn[e, a], j]
+                ue[a * 3 + j] = u[i - 1] if i > 0 else 0.0
+        err, feo, lko, _ = P.element(mat, e, ue, st_n[e], dt=p.dt)
+        assert err == 0
+        assert np.linalg.norm(fe[k] - feo) <= TOL * np.linalg.norm(feo)
+        assert np.linalg.norm(fe2[k] - feo) <= TOL * np.linalg.norm(feo)
+        assert np.linalg.norm(lk[k].ravel() - lko.ravel()) <= TOL * np.linalg.norm(lko)
+    # the blocks of all elements assemble into the assembly's K
+    allel = np.arange(p.ne)
+    lka, _, _ = ctx.stiffmatel_fd(allel, u, dt=p.dt)
+    R, K, _ = ctx.assemble_RK(u, dt=p.dt)
+    Kd = np.zeros((p.ndof, p.ndof))
+    for e in allel:
+        idx = np.array([p.ids[p.conn[e, a], j] for a in range(4) for j in range(3)])
+        m = idx > 0
+        Kd[np.ix_(idx[m] - 1, idx[m] - 1)] += lka[e].reshape(12, 12)[np.ix_(m, m)]
+    rows = np.repeat(np.arange(p.ndof), np.diff(p.Ap))
+    assert np.abs(Kd[rows, p.Ai] - K).max() <= 1e-10 * np.abs(K).max()

@@ -328,3 +328,59 @@ def test_linear_deviatoric_potential_matches_oracle(gpu, nne):
         assert err == 0
         assert np.abs(S[i] - So.ravel()).max() <= TOL * np.abs(So).max()
         assert np.abs(sym_L(L[i]) - sym_L(Lo)).max() <= TOL * np.abs(sym_L(Lo)).max()
+
+
+@pytest.mark.parametrize("nne,model,vol_pot", [(10, "j2", 2), (10, "j2", 3), (4, "j2", 3), (4, "he", 2),
+                                               (10, "he", 3)])
+def test_volumetric_potentials_match_oracle(gpu, nne, model, vol_pot):
+    """The reference's Doll-Schweizerhof volumetric potentials (volPotFlag 2,
+    3) at finite volume change, every R+K path of the element type (the
+    tensor-core quadratic-tet kernel, the linear-tet column-split kernel), the
+    R-only call and the constitutive level, against the oracle (1e-10)."""
+    p = wl.tension(n=3, nne=nne, model=model, stretch=0.05, predictor=True)
+    rng = np.random.default_rng(vol_pot)
+    p.u = p.u + rng.uniform(-0.01, 0.01, p.u.shape)
+    p.mat.vol_pot = vol_pot
+    Ro, Ko, so = oracle_assemble(p)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u, p.u_presc)
+    assert st.ok(), st.as_dict()
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    if so is not None:
+        assert np.abs(ctx.get_state(1) - so).max() <= TOL * np.abs(so).max()
+    check_R(ctx.assemble_R(p.u, p.u_presc)[0], Ro)
+    F = np.eye(3)[None] + rng.uniform(-0.1, 0.1, (8, 3, 3))
+    st = None
+    if model == "j2":
+        st = np.zeros((8, 10))
+        st[:, [0, 4, 8]] = 1.0
+    S, L, _, q = pg.cm_integrate(p.mat, F.reshape(8, 9), st)
+    assert (q == 0).all()
+    om = oracle.from_pg_material(p.mat)
+    for i in range(8):
+        err, So, Lo, _, _ = oracle.cm_update(om, F[i], None if st is None else st[i])
+        assert err == 0
+        assert np.abs(S[i] - So.ravel()).max() <= TOL * np.abs(So).max()
+
+
+def test_reference_j2_parameter_block_through_the_gpu(gpu, tmp_path):
+    """A model_params.in J2 entry with the reference driver's parameters (beta
+    0, hp 300, k0 0.5, damage off; G 6, nu 0.49 from the material line,
+    volPotFlag 2) goes reader -> material -> GPU assembly of quadratic tets
+    stretched past yield, equal to the oracle with the same material (1e-10)."""
+    f = tmp_path / "model_params.in"
+    f.write_text("1\n0 4\n{\n0.0 300.0 0.5\n0.0 1.0 0.0 0.0 0.0\n0 0 0 0 0 0\n}\n")
+    (j2,) = pg.read_model_params(str(f))
+    G, nu = 6.0, 0.49
+    mat = pg.j2_material(j2, 2 * G * (1 + nu), nu, vol_pot=2)
+    p = wl.j2_p2(n=3, seed=5, stretch=0.08, perturb=5e-3)
+    p.mat = mat
+    Ro, Ko, so = oracle_assemble(p)
+    assert (so[:, 9] > 0).mean() > 0.5
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    assert np.abs(ctx.get_state(1) - so).max() <= TOL * np.abs(so).max()

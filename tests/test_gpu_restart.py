@@ -10,7 +10,9 @@ pgfem_gpu_read_restart) in the reference's per-rank layout.
   the atomic scatter's summation order, 1e-12)
 - hyperelastic box patch test: the converged affine stretch writes
   Fn = diag(2, 1, 1) at every point and Fnm1 = I
-- a J2 context has no restart (EINVAL)
+- J2 quadratic tets past yield: the written file holds the reference's J2
+  block (pS = G (I - Cp^-1), ep, gam); a fresh context that reads it holds the
+  same state (1e-14) and assembles the same R and K (1e-12)
 """
 import numpy as np
 import pytest
@@ -108,9 +110,33 @@ def test_hyperelastic_restart_holds_the_deformation(gpu, tmp_path):
     assert not r1.any() and np.array_equal(r2, u)
 
 
-def test_j2_context_has_no_restart(gpu, tmp_path):
+def test_j2_restart_round_trip(gpu, tmp_path):
     import workloads as wl
-    p = wl.j2_p2(n=2, seed=1)
+    p = wl.j2_p2(n=2, seed=1, stretch=6e-3, perturb=2e-2)
     ctx = p.context()
-    with pytest.raises(pg.PgfemError, match="EINVAL"):
-        pg.write_restart(ctx, str(tmp_path / "j2.res"), p.u, p.u)
+    s0 = ctx.get_state(0)
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok()
+    ctx.commit_state()
+    s1 = ctx.get_state(0)
+    assert (s1[:, 9] > 0).any()
+    path = str(tmp_path / "j2_0_1.res")
+    zero = np.zeros(p.ndof)
+    pg.write_restart(ctx, path, zero, p.u, state_nm1=s0)
+    nn, ne = p.X.shape[0], p.conn.shape[0]
+    a, b, blocks = pg.restart_parse(path, pg.MODEL_J2, nn, ne, 4)
+    G = 200e3 / (2 * 1.3)
+    blk = blocks.reshape(-1, 47)
+    assert np.allclose(blk[:, 9:18], G * (np.eye(3).ravel() - s1[:, :9]), rtol=0, atol=1e-9 * G)
+    assert np.array_equal(blk[:, 42], s1[:, 9]) and not blk[:, 43].any()
+    assert np.allclose(blk[:, 44], np.sqrt(1.5) * s1[:, 9], rtol=1e-14, atol=0)
+    assert not blk[:, [36, 37, 38, 39, 40, 41, 45, 46]].any()
+    ctx2 = p.context()
+    r1, r2 = pg.read_restart(ctx2, path)
+    assert not r1.any() and np.allclose(r2, p.u, rtol=0, atol=0)
+    assert np.abs(ctx2.get_state(0) - s1).max() <= 1e-14 * max(1.0, np.abs(s1).max())
+    u3 = p.u * 1.1
+    Ra, Ka, _ = ctx.assemble_RK(u3)
+    Rb, Kb, _ = ctx2.assemble_RK(u3)
+    assert np.linalg.norm(Rb - Ra) <= 1e-12 * np.linalg.norm(Ra)
+    assert np.linalg.norm(Kb - Ka) <= 1e-12 * np.linalg.norm(Ka)

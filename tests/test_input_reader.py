@@ -202,6 +202,30 @@ def test_model_params(tmp_path):
         pg.read_model_params(str(p))
 
 
+def test_j2_material_from_the_reference_parameter_block(tmp_path):
+    """A J2 entry (beta hp k0 / damage / split-damage lines, the reference's own
+    driver values: beta 0, hp 300, k0 0.5, damage off) gives sigma_y = k0,
+    H = hp, E and nu from the mesh's material line and its volumetric potential;
+    beta != 0 and active damage (mu != 0) are refused."""
+    p = tmp_path / "model_params.in"
+    block = "1\n0 4\n{\n%s %s %s\n%s 1.0 0.0 0.0 0.0\n0 0 0 0 0 0\n}\n"
+    p.write_text(block % (0.0, 300.0, 0.5, 0.0))
+    (j2,) = pg.read_model_params(str(p))
+    G, nu = 6.0, 0.49
+    E = 2 * G * (1 + nu)
+    m = pg.j2_material(j2, E, nu, vol_pot=2)
+    assert (m.model, m.sigma_y, m.H, m.vol_pot, m.dev_pot) == (pg.MODEL_J2, 0.5, 300.0, 2, 1)
+    assert (m.E, m.nu) == (E, nu)
+    assert pg.j2_material(j2, E, nu, vol_pot=0).vol_pot == 99
+    for beta, mu in ((0.5, 0.0), (0.0, 1.0)):
+        p.write_text(block % (beta, 300.0, 0.5, mu))
+        (j2b,) = pg.read_model_params(str(p))
+        with pytest.raises(pg.PgfemError, match="EINVAL"):
+            pg.j2_material(j2b, E, nu)
+    with pytest.raises(pg.PgfemError, match="EINVAL"):
+        pg.j2_material(j2, E, nu, vol_pot=5)
+
+
 def test_orientations_and_rotations(tmp_path):
     X, conn, _ = pg.mesh_box_tet(2, 4)
     ne = conn.shape[0]
@@ -361,7 +385,8 @@ def test_entry_points_reject_bad_arguments(tmp_path):
     assert L.pgfem_input_read_model_params(None, 0, None, C.byref(n)) == EINVAL
     assert L.pgfem_input_read_multiphysics(None, 0, None, None, C.byref(n)) == EINVAL
     assert L.pgfem_input_read_solver_file(None, -1, None, None, None, None, None) == EINVAL
-    assert L.pgfem_restart_block_size(pg.MODEL_J2) < 0
+    assert L.pgfem_restart_block_size(7) < 0
+    assert L.pgfem_input_j2_material(None, C.c_double(1.0), C.c_double(0.3), 99, None) == EINVAL
     assert L.pgfem_restart_format(None, 1, 1, 1, pg.MODEL_HE, None, None, None) == EINVAL
     assert L.pgfem_restart_parse(b"x.res", 1, 1, 0, pg.MODEL_HE, None, None, None) == EINVAL
     assert L.pgfem_restart_write_partitions(None, b"x", 0, pg.MODEL_CP, 1, None, None, None) == EINVAL

@@ -152,3 +152,26 @@ def test_crystal_plasticity_box_matches_reference_restart():
     assert numdiff_pass(st[:, :9], pF_ref).mean() >= 0.99
     # the comparison is sharp: the plastic part of pF is 200x the tolerance
     assert np.abs(pF_ref - np.eye(3).ravel()).max() > 200 * CP_REF_PF_ATOL
+
+
+@pytest.mark.parametrize("nne", [4, 10])
+def test_oracle_mesher_equals_product_mesher(nne):
+    """The oracle's restated box mesher (used by the CPU arm of the benchmark
+    so that it loads no product code) gives the product mesher's nodes and
+    connectivity."""
+    import pgfem_gpu as pg
+    Xp, cp, _ = pg.mesh_box_tet(3, nne)
+    Xo, co = oracle.mesh_box_tet(3, nne)
+    assert np.array_equal(cp, co)
+    assert np.array_equal(Xp, Xo)
+
+
+@pytest.mark.parametrize("layers", [None, 2])
+def test_oracle_j2_workload_equals_product_workload(layers):
+    import workloads as wl
+    p = wl.j2_p2(n=3, seed=1, max_cells_z=layers)
+    P, mat, u, state = oracle.j2_p2_problem(3, seed=1, max_cells_z=layers)
+    assert np.array_equal(P.ids, p.ids) and P.ndof == p.ndof
+    assert np.array_equal(P.Ap, p.Ap) and np.array_equal(P.Ai, p.Ai)
+    assert np.array_equal(u, p.u) and np.array_equal(state, p.state)
+    assert np.array_equal(P.X, p.X) and np.array_equal(P.conn, p.conn)

@@ -24,11 +24,12 @@ def rot(a, b, c):
     return Rz(a) @ Rx(b) @ Rz(c)
 
 
-def small_problem(kind, n=2, stretch=None):
+def small_problem(kind, n=2, stretch=None, vol_pot=99):
     if kind == "he":
         p = wl.he_p1(n=n, seed=7)
     else:
         p = wl.j2_p2(n=n, seed=3, stretch=stretch, perturb=2e-2)
+    p.mat.vol_pot = vol_pot
     P, mat = oracle.from_workload(p)
     return p, P, mat
 
@@ -42,9 +43,12 @@ def elem_u(p, e, u):
     return ue
 
 
-@pytest.mark.parametrize("kind,stretch", [("he", None), ("j2", 1e-4), ("j2", 6e-3)])
-def test_tangent_matches_central_differences(kind, stretch):
-    p, P, mat = small_problem(kind, stretch=stretch)
+@pytest.mark.parametrize("kind,stretch,vol_pot", [("he", None, 99), ("j2", 1e-4, 99), ("j2", 6e-3, 99),
+                                                   ("he", None, 2), ("he", None, 3), ("j2", 6e-3, 2),
+                                                   ("j2", 6e-3, 3)])
+def test_tangent_matches_central_differences(kind, stretch, vol_pot):
+    """Also for the Doll-Schweizerhof volumetric potentials (volPotFlag 2, 3)."""
+    p, P, mat = small_problem(kind, stretch=stretch, vol_pot=vol_pot)
     rng = np.random.default_rng(0)
     for e in rng.choice(p.ne, 4, replace=False):
         ue = elem_u(p, e, p.u)
@@ -70,9 +74,10 @@ def test_j2_plastic_points_exist_in_plastic_case():
     assert (snp1[:, 9] > 0).mean() > 0.5
 
 
-@pytest.mark.parametrize("kind,stretch", [("he", None), ("j2", None), ("j2", 6e-3)])
-def test_bform_equals_reference_form(kind, stretch):
-    p, P, mat = small_problem(kind, n=3, stretch=stretch)
+@pytest.mark.parametrize("kind,stretch,vol_pot", [("he", None, 99), ("j2", None, 99), ("j2", 6e-3, 99),
+                                                   ("he", None, 2), ("j2", 6e-3, 3)])
+def test_bform_equals_reference_form(kind, stretch, vol_pot):
+    p, P, mat = small_problem(kind, n=3, stretch=stretch, vol_pot=vol_pot)
     err, R, K, s1 = P.assemble(mat, p.u, state_n=p.state)
     err2, R2, K2, s2 = P.assemble(mat, p.u, state_n=p.state, bform=True)
     assert err == 0 and err2 == 0
@@ -230,3 +235,14 @@ def cp_guess_from_slip(p, dgam):
     P = np.einsum("eai,eaj->eaij", rs, rn)
     M0 = np.eye(3)[None] - np.einsum("ea,eaij->eij", dgam, P)
     return np.concatenate([M0.reshape(-1, 9), np.zeros((len(M0), 1))], axis=1)
+
+
+@pytest.mark.parametrize("vol_pot", [2, 3])
+def test_volumetric_potentials_change_the_answer(vol_pot):
+    """The Doll-Schweizerhof potentials are really used (R differs from the
+    U_Common answer at finite volume change)."""
+    p, P, mat = small_problem("j2", stretch=6e-3, vol_pot=99)
+    _, R0, _, _ = P.assemble(mat, p.u, state_n=p.state)
+    p2, P2, mat2 = small_problem("j2", stretch=6e-3, vol_pot=vol_pot)
+    _, R1, _, _ = P2.assemble(mat2, p2.u, state_n=p2.state)
+    assert np.linalg.norm(R1 - R0) > 1e-6 * np.linalg.norm(R0)
