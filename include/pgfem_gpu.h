@@ -130,6 +130,27 @@ int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *ctx, int mode);
  * warp leaves its loop (no trap), status.other counts it, and later calls are
  * unaffected. */
 int pgfem_gpu_set_wait_test(pgfem_gpu_ctx *ctx, double limit_s, int stall_next_assembly);
+
+/* ---- surface loads (Neumann boundary conditions) ------------------------
+ * Replaces the NeumannBoundaryElement lists (include/PGFem3D_data_structure.h:
+ * 32-120, built by construct_list_of_boundary_elements,
+ * src/PGFem3D_data_structure.cc:825-895, from the NBC/<physics>.nbc features
+ * read in src/read_input_file.cc:168-214) and their quasi-static terms
+ * (compute_Neumann_boundary_conditions, src/fd_residuals.cc:123-273;
+ * compute_Neumann_boundary_conditions_stiffnes_mat, src/stiffmat_fd.cc:
+ * 359-500), which every residual and R+K call and the element-level calls
+ * then add after the element integrals.
+ * Face k: element elem[k] (0-based), local face face[k] (0..3, FEMLIB's
+ * Tet2Tri numbering: {0,2,1}, {0,1,3}, {1,2,3}, {0,3,2}), feature feature[k].
+ * Feature f: load_type[f] values (1: pressure p along the face's unit
+ * normal, 2 or 3: traction components), load_np1[3f .. 3f+2] at t_{n+1} (the
+ * host evaluates the load functions; unused entries are ignored).  nface = 0
+ * clears.  Returns PGFEM_GPU_EINVAL for an element, face, feature or type out
+ * of range.  set_neumann_loads replaces only the values (same nfeature). */
+int pgfem_gpu_set_neumann(pgfem_gpu_ctx *ctx, long nface, const long *elem, const int *face,
+                          const int *feature, int nfeature, const int *load_type, const double *load_np1);
+int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *ctx, int nfeature, const double *load_np1);
+
 /* Device bytes held by the context (mesh, map, state, scratch). */
 long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *ctx);
 long pgfem_gpu_nnz(const pgfem_gpu_ctx *ctx);

@@ -27,7 +27,9 @@ class OrcMaterial(C.Structure):
 class OrcProblem(C.Structure):
     _fields_ = [("nn", C.c_long), ("ne", C.c_long), ("nne", C.c_int),
                 ("X", C.c_void_p), ("conn", C.c_void_p), ("id", C.c_void_p), ("ndof", C.c_long),
-                ("Ap", C.c_void_p), ("Ai", C.c_void_p), ("F0", C.c_void_p), ("R_cp", C.c_void_p)]
+                ("Ap", C.c_void_p), ("Ai", C.c_void_p), ("F0", C.c_void_p), ("R_cp", C.c_void_p),
+                ("nbc_off", C.c_void_p), ("nbc_face", C.c_void_p), ("nbc_type", C.c_void_p),
+                ("nbc_load", C.c_void_p)]
 
 
 _lib = None
@@ -154,6 +156,28 @@ class Problem:
         self.s = OrcProblem(self.X.shape[0], self.conn.shape[0], self.conn.shape[1], _p(self.X),
                             _p(self.conn), _p(self.ids), ndof, _p(self.Ap), _p(self.Ai), _p(self.F0),
                             _p(self.R_cp))
+
+    def set_neumann(self, elem, face, load_type, load):
+        """Surface loads on element faces (the reference's NeumannBoundaryElement
+        list, src/PGFem3D_data_structure.cc:825-895, flattened to one entry per
+        face): elem (0-based), local face 0..3, number of load values (1 pressure,
+        2..3 traction) and the values at t_{n+1} (nface x 3).  Empty lists clear."""
+        elem = np.asarray(elem, dtype=np.int64).ravel()
+        if elem.size == 0:
+            self.nbc = None
+            self.s.nbc_off = self.s.nbc_face = self.s.nbc_type = self.s.nbc_load = None
+            return
+        order = np.argsort(elem, kind="stable")
+        ne = self.conn.shape[0]
+        off = np.zeros(ne + 1, dtype=np.int64)
+        np.add.at(off, elem + 1, 1)
+        off = np.cumsum(off)
+        face = np.ascontiguousarray(np.asarray(face, dtype=np.int32).ravel()[order])
+        ltype = np.ascontiguousarray(np.asarray(load_type, dtype=np.int32).ravel()[order])
+        load = np.ascontiguousarray(np.asarray(load, dtype=np.float64).reshape(-1, 3)[order])
+        self.nbc = (off, face, ltype, load)
+        self.s.nbc_off, self.s.nbc_face, self.s.nbc_type, self.s.nbc_load = (_p(off), _p(face), _p(ltype),
+                                                                             _p(load))
 
     @property
     def nnz(self):

@@ -464,6 +464,150 @@ void compute_stiffness_matrix(double *lk, int nne, const double *dN, double detJ
     }
 }
 
+// ---------------------------------------------------------------------------
+// Neumann (surface-load) terms of one element, quasi-static:
+// compute_Neumann_boundary_conditions (src/fd_residuals.cc:123-273) and
+// compute_Neumann_boundary_conditions_stiffnes_mat (src/stiffmat_fd.cc:
+// 359-500), both run at the end of the element routine (:439-440 and :602-604).
+// The boundary FEMLIB (FEMLIB/src/femlib.cc): face node lists Tet2Tri /
+// QTet2QTri (:85-86), the volume-coordinate maps kez_map_Tet (:97-100) and
+// set_tet2tri (:796-815), the triangle rules TriIntegrationPoints1/3 (:619-635;
+// the boundary takes the volume element's integration order, which FEMLIB
+// raises to 1 for quadratic tets: 1 point on linear faces, 3 on quadratic),
+// elem_basis_S (:1578-1612: volume N and dN/dX at the point) and
+// PGFem3D_dNdX_Vol2Bnd (:486-541: face Jacobian |dX/dxi_1 x dX/dxi_2| and unit
+// normal from the face's own basis, compute_dN_dkez :229-246, evaluated at the
+// volume coordinates picked through kez_map).
+//
+// Residual, per point and face node a (volume node V2B[a]), component i:
+//   f[a,i] += N_a w (-1) J (F^-T PN)_i,  PN = p n (pressure), t (traction)
+// Stiffness, only the component-diagonal entries (a,d; c,d):
+//   k[a,d; c,d] += N_a w (-1) J FIT_d,
+//   FIT_i = (tr(F^-1 ST) F^-1_ji - dFIdF_ijkl ST_kl) PN'_j,
+//   dFIdF_ijkl = -F^-1_jk F^-1_li,  ST_kl = delta_dk dN/dX_{c',l}
+// which is 2 g_d (F^-T PN')_d with g_m = sum_l F^-1_lm dN/dX_{c',l}.  As in the
+// reference, the shape tensor is taken at volume node c' = c (the face-local
+// index, src/stiffmat_fd.cc:486-488), and for a pressure PN' = (p n_0, 0, p n_2)
+// (only load value 0 is read and copied to component 2, :419-423, then
+// multiplied component-wise by n, :442-445).  Face 3 of the tet: the table maps
+// its points onto the plane zet = 0 (face 0's plane) while its nodes are
+// {0, 3, 2}; the restatement keeps that.
+// ---------------------------------------------------------------------------
+const int kTet2Tri[4][3] = {{0, 2, 1}, {0, 1, 3}, {1, 2, 3}, {0, 3, 2}};
+const int kQTet2QTri[4][6] = {{0, 2, 1, 6, 5, 4}, {0, 1, 3, 4, 8, 7}, {1, 2, 3, 5, 9, 8}, {0, 3, 2, 7, 9, 6}};
+const int kKezMapTet[4][3] = {{1, 0, 2}, {0, 2, 1}, {0, 1, 2}, {0, 1, 2}};
+
+// Volume shape functions, PGFem3D_N (FEMLIB/src/femlib.cc:158-177).
+void shape_N(int nne, double ksi, double eta, double zet, double *N) {
+  const double l0 = 1.0 - ksi - eta - zet;
+  if (nne == 4) {
+    N[0] = l0;
+    N[1] = ksi;
+    N[2] = eta;
+    N[3] = zet;
+    return;
+  }
+  N[0] = (2.0 * l0 - 1.0) * l0;
+  N[1] = (2.0 * ksi - 1.0) * ksi;
+  N[2] = (2.0 * eta - 1.0) * eta;
+  N[3] = (2.0 * zet - 1.0) * zet;
+  N[4] = 4.0 * l0 * ksi;
+  N[5] = 4.0 * ksi * eta;
+  N[6] = 4.0 * l0 * eta;
+  N[7] = 4.0 * l0 * zet;
+  N[8] = 4.0 * ksi * zet;
+  N[9] = 4.0 * eta * zet;
+}
+
+// Face basis derivatives (nb x 2), compute_dN_dkez for TRIANGLE / QTRIANGLE.
+void face_dN(int nb, double ksi, double eta, double *d) {
+  if (nb == 3) {
+    const double t[6] = {-1, -1, 1, 0, 0, 1};
+    std::memcpy(d, t, sizeof(t));
+    return;
+  }
+  d[0] = 4.0 * eta + 4.0 * ksi - 3.0;
+  d[1] = 4.0 * eta + 4.0 * ksi - 3.0;
+  d[2] = 4.0 * ksi - 1.0;
+  d[3] = 0.0;
+  d[4] = 0.0;
+  d[5] = 4.0 * eta - 1.0;
+  d[6] = 4.0 - 8.0 * ksi - 4.0 * eta;
+  d[7] = -4.0 * ksi;
+  d[8] = 4.0 * eta;
+  d[9] = 4.0 * ksi;
+  d[10] = -4.0 * eta;
+  d[11] = 4.0 - 4.0 * ksi - 8.0 * eta;
+}
+
+void neumann_faces(const orc_problem *P, long e, const double *Xe, const double *u_e, double *fe,
+                   double *lk) {
+  const int nne = P->nne, nd = nne * 3, nb = nne == 10 ? 6 : 3;
+  const int npt = nne == 10 ? 3 : 1;
+  const double gk1[1] = {1.0 / 3.0}, ge1[1] = {1.0 / 3.0}, w1[1] = {0.5};
+  const double gk3[3] = {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0}, ge3[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+  const double w3[3] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0};
+  const double *gk = npt == 3 ? gk3 : gk1, *ge = npt == 3 ? ge3 : ge1, *wt = npt == 3 ? w3 : w1;
+  for (long k = P->nbc_off[e]; k < P->nbc_off[e + 1]; k++) {
+    const int f = P->nbc_face[k], type = P->nbc_type[k];
+    const int *v2b = nne == 10 ? kQTet2QTri[f] : kTet2Tri[f];
+    const int *km = kKezMapTet[f];
+    double Pv[3] = {0.0, 0.0, 0.0};
+    for (int i = 0; i < type && i < 3; i++) Pv[i] = P->nbc_load[k * 3 + i];
+    if (type == 1) Pv[2] = Pv[0];  // Pv[1] stays 0
+    for (int ip = 0; ip < npt; ip++) {
+      double kez[3] = {0.0, 0.0, 0.0};
+      kez[km[0]] = gk[ip];
+      kez[km[1]] = ge[ip];
+      if (f == 2) kez[km[2]] = 1.0 - gk[ip] - ge[ip];
+      double N[10], dN[30];
+      shape_N(nne, kez[0], kez[1], kez[2], N);
+      int terr = 0;
+      PGFem3D_dNdX(nne, kez[0], kez[1], kez[2], Xe, dN, &terr);
+      double db[12];
+      face_dN(nb, kez[km[0]], kez[km[1]], db);
+      double dX[6] = {0, 0, 0, 0, 0, 0};  // dX(ib, ic), ic = 0, 1
+      for (int ib = 0; ib < 3; ib++)
+        for (int ic = 0; ic < 2; ic++)
+          for (int ia = 0; ia < nb; ia++) dX[ib * 2 + ic] += db[ia * 2 + ic] * Xe[v2b[ia] * 3 + ib];
+      const double v0 = dX[2] * dX[5] - dX[3] * dX[4];
+      const double v1 = dX[1] * dX[4] - dX[0] * dX[5];
+      const double v2 = dX[0] * dX[3] - dX[1] * dX[2];
+      const double Jf = std::sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+      const double n[3] = {v0 / Jf, v1 / Jf, v2 / Jf};
+      const double detJxW = Jf * wt[ip];
+      double F[9], FI[9];
+      deformation_gradient(nne, u_e, dN, F);
+      const double J = det3x3(F);
+      inv3x3(F, FI);
+      double PN[3], PNk[3];
+      for (int i = 0; i < 3; i++) {
+        PN[i] = type == 1 ? Pv[0] * n[i] : Pv[i];
+        PNk[i] = type == 1 ? Pv[i] * n[i] : Pv[i];
+      }
+      double FTP[3], FTPk[3];  // F^-T PN
+      for (int i = 0; i < 3; i++) {
+        FTP[i] = FI[0 * 3 + i] * PN[0] + FI[1 * 3 + i] * PN[1] + FI[2 * 3 + i] * PN[2];
+        FTPk[i] = FI[0 * 3 + i] * PNk[0] + FI[1 * 3 + i] * PNk[1] + FI[2 * 3 + i] * PNk[2];
+      }
+      for (int ia = 0; ia < nb; ia++) {
+        const int a = v2b[ia];
+        const double s = N[a] * detJxW * (-1.0) * J;
+        for (int i = 0; i < 3; i++) fe[a * 3 + i] += s * FTP[i];
+        if (!lk) continue;
+        for (int ic = 0; ic < nb; ic++) {
+          const int c = v2b[ic];
+          for (int d = 0; d < 3; d++) {
+            double g = 0.0;  // shape tensor of volume node ic
+            for (int l = 0; l < 3; l++) g += FI[l * 3 + d] * dN[ic * 3 + l];
+            lk[(a * 3 + d) * nd + c * 3 + d] += s * 2.0 * g * FTPk[d];
+          }
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -583,6 +727,9 @@ int orc_element(const orc_problem *P, const orc_material *mat, long e, const dou
   if (lk && !err)
     for (int a = 0; a < nd; a++)
       if (!std::isnormal(lk[a * nd + a])) err++;
+  // surface loads after the element integrals (src/fd_residuals.cc:439,
+  // src/stiffmat_fd.cc:602)
+  if (!err && P->nbc_off) neumann_faces(P, e, Xe, u_e, fe, lk);
   return err;
 }
 

@@ -56,6 +56,17 @@ typedef struct {
   const int *Ap, *Ai;           /* CSR pattern of the free DOFs (0-based) */
   const double *F0;             /* macro deformation-gradient increment added to F (FE2), or NULL */
   const double *R_cp;           /* CP: ne*9 crystal rotation per element (row-major), or NULL */
+  /* Neumann faces (surface loads), or nbc_off == NULL for none: the faces of
+   * element e are k = nbc_off[e] .. nbc_off[e+1]-1, each with its local face
+   * nbc_face[k] (0..3, FEMLIB's Tet2Tri numbering), the number of load values
+   * nbc_type[k] (1: pressure along the face normal, 2 or 3: traction) and the
+   * values at t_{n+1} nbc_load[3k .. 3k+2].  Added to the element's residual and
+   * stiffness after the element integrals (src/fd_residuals.cc:123-273,
+   * src/stiffmat_fd.cc:359-500). */
+  const long *nbc_off;
+  const int *nbc_face;
+  const int *nbc_type;
+  const double *nbc_load;
 } orc_problem;
 
 /* Reference: src/generate_dof_ids.cc:69-171 (generate_local_dof_ids) and

@@ -24,6 +24,7 @@
 #include "assemble_p1.cuh"
 #include "cm_integrate.cuh"
 #include "cp_kernels.cuh"
+#include "neumann.cuh"
 #include "peak_probe.cuh"
 #include "pgfem_gpu.h"
 
@@ -85,6 +86,13 @@ struct pgfem_gpu_ctx {
   // failure-path tests: bound of the hand-off waits, one-shot withheld hand-off
   unsigned long long wait_ns = 2000000000ull;
   int stall_next = 0;
+  // surface loads: faces sorted by element, their features' load type and
+  // values, per-element face offsets (ne+1)
+  long nbc_nface = 0, nbc_bytes = 0;
+  int nbc_nfeat = 0;
+  int *nbc_elem = nullptr, *nbc_feat = nullptr, *nbc_type = nullptr, *nbc_off = nullptr;
+  uint8_t *nbc_face = nullptr;
+  double *nbc_load = nullptr;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -293,7 +301,8 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->qrec, c->eblk, c->perm,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
-                  c->sched_ticket};
+                  c->sched_ticket, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
+                  c->nbc_load};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->zfork) cudaEventDestroy(c->zfork);
@@ -635,6 +644,59 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
   return PGFEM_GPU_OK;
 }
 
+NbcArgs nbc_args(const pgfem_gpu_ctx *c) {
+  NbcArgs A{};
+  A.X = c->X;
+  A.conn = c->conn;
+  A.dof = c->dof;
+  A.rowptr0 = c->rowptr0;
+  A.rowlen = c->rowlen;
+  A.mask = c->mask;
+  A.pos = c->pos;
+  A.nn = c->nn;
+  A.ne = c->ne;
+  A.unode = c->unode;
+  A.nface = c->nbc_nface;
+  A.face_elem = c->nbc_elem;
+  A.face_id = c->nbc_face;
+  A.face_feat = c->nbc_feat;
+  A.feat_type = c->nbc_type;
+  A.feat_load = c->nbc_load;
+  A.elem_face_off = c->nbc_off;
+  return A;
+}
+
+// Surface-load terms after the element kernels (same stream): into R and K
+// (K may be null: residual only), or into the dense blocks of listed elements.
+int launch_neumann(pgfem_gpu_ctx *c, double *d_R, double *d_K, cudaStream_t s, const int *elist = nullptr,
+                   long nlist = 0, double *lk = nullptr, double *fe = nullptr) {
+  if (!c->nbc_nface) return PGFEM_GPU_OK;
+  NbcArgs A = nbc_args(c);
+  if (elist) {
+    if (!nlist) return PGFEM_GPU_OK;
+    A.elist = elist;
+    A.nlist = nlist;
+    A.lk_out = lk;
+    A.fe_out = fe;
+    const unsigned g = (unsigned)((nlist + 127) / 128);
+    if (c->nne == 10)
+      lk ? k_neumann_dense<10, true><<<g, 128, 0, s>>>(A) : k_neumann_dense<10, false><<<g, 128, 0, s>>>(A);
+    else
+      lk ? k_neumann_dense<4, true><<<g, 128, 0, s>>>(A) : k_neumann_dense<4, false><<<g, 128, 0, s>>>(A);
+  } else {
+    if (!d_R && !d_K) return PGFEM_GPU_OK;
+    A.R = d_R;
+    A.K = d_K;
+    const unsigned g = (unsigned)((c->nbc_nface + 127) / 128);
+    if (c->nne == 10)
+      d_K ? k_neumann<10, true><<<g, 128, 0, s>>>(A) : k_neumann<10, false><<<g, 128, 0, s>>>(A);
+    else
+      d_K ? k_neumann<4, true><<<g, 128, 0, s>>>(A) : k_neumann<4, false><<<g, 128, 0, s>>>(A);
+  }
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 // Whether an R+K call of this context runs the tensor-core quadratic-tet
 // path (the branch of dispatch() for 10-node elements, atomic scatter).
 bool uses_p2m(const pgfem_gpu_ctx *c) {
@@ -653,13 +715,16 @@ int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, 
     CK(cudaGetLastError());
   }
   if (c->model == PGFEM_MODEL_CP) {
+    int r;
     if (!d_K) {  // residual only: the tangent columns are skipped by a scratch K
-      int r = ensure_K_scratch(c);
+      r = ensure_K_scratch(c);
       if (r) return r;
       CK(cudaMemsetAsync(c->d_K, 0, sizeof(double) * c->nnz, s));
-      return assemble_cp(c, d_R, c->d_K, dt, s);
+      r = assemble_cp(c, d_R, c->d_K, dt, s);
+    } else {
+      r = assemble_cp(c, d_R, d_K, dt, s);
     }
-    return assemble_cp(c, d_R, d_K, dt, s);
+    return r ? r : launch_neumann(c, d_R, d_K, s);
   }
   AsmArgs a = base_args(c);
   a.R = d_R;
@@ -685,7 +750,7 @@ int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, 
     CK(cudaEventRecord(e1, s));
     c->events.emplace_back(e0, e1);
   }
-  return r;
+  return r ? r : launch_neumann(c, d_R, d_K, s);
 }
 
 int read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, bool clear) {
@@ -993,6 +1058,75 @@ int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
   return PGFEM_GPU_OK;
 }
 
+int pgfem_gpu_set_neumann(pgfem_gpu_ctx *c, long nface, const long *elem, const int *face,
+                          const int *feature, int nfeature, const int *load_type, const double *load_np1) {
+  if (!c || nface < 0 || nfeature < 0 || (nface && (!elem || !face || !feature || !nfeature)) ||
+      (nfeature && (!load_type || !load_np1)))
+    return PGFEM_GPU_EINVAL;
+  for (long k = 0; k < nface; k++)
+    if (elem[k] < 0 || elem[k] >= c->ne || face[k] < 0 || face[k] > 3 || feature[k] < 0 || feature[k] >= nfeature)
+      return PGFEM_GPU_EINVAL;
+  for (int f = 0; f < nfeature; f++)
+    if (load_type[f] < 1 || load_type[f] > 3) return PGFEM_GPU_EINVAL;
+  CK(cudaStreamSynchronize(c->stream));  // earlier assemblies may still read the old lists
+  int *old[] = {c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off};
+  for (int *p : old)
+    if (p) cudaFree(p);
+  if (c->nbc_face) cudaFree(c->nbc_face);
+  if (c->nbc_load) cudaFree(c->nbc_load);
+  c->nbc_elem = c->nbc_feat = c->nbc_type = c->nbc_off = nullptr;
+  c->nbc_face = nullptr;
+  c->nbc_load = nullptr;
+  c->nbc_nface = 0;
+  c->nbc_nfeat = 0;
+  c->bytes -= c->nbc_bytes;
+  c->nbc_bytes = 0;
+  if (!nface) return PGFEM_GPU_OK;
+  const long bytes0 = c->bytes;
+  // faces in element order (stable), per-element offsets
+  std::vector<long> order(nface);
+  for (long k = 0; k < nface; k++) order[k] = k;
+  std::stable_sort(order.begin(), order.end(), [&](long x, long y) { return elem[x] < elem[y]; });
+  std::vector<int> fe_(nface), ff(nface), off(c->ne + 1, 0);
+  std::vector<uint8_t> fi(nface);
+  for (long k = 0; k < nface; k++) {
+    fe_[k] = (int)elem[order[k]];
+    fi[k] = (uint8_t)face[order[k]];
+    ff[k] = feature[order[k]];
+    off[fe_[k] + 1]++;
+  }
+  for (long e = 0; e < c->ne; e++) off[e + 1] += off[e];
+  std::vector<double> ld((size_t)3 * nfeature);
+  for (int f = 0; f < nfeature; f++)
+    for (int i = 0; i < 3; i++) ld[(size_t)3 * f + i] = i < load_type[f] ? load_np1[(size_t)3 * f + i] : 0.0;
+  int r;
+  if ((r = upload(c, &c->nbc_elem, fe_.data(), fe_.size())) || (r = upload(c, &c->nbc_face, fi.data(), fi.size())) ||
+      (r = upload(c, &c->nbc_feat, ff.data(), ff.size())) || (r = upload(c, &c->nbc_type, load_type, nfeature)) ||
+      (r = upload(c, &c->nbc_load, ld.data(), ld.size())) || (r = upload(c, &c->nbc_off, off.data(), off.size()))) {
+    c->nbc_bytes = c->bytes - bytes0;  // freed by the next call or at destroy
+    return r;
+  }
+  c->nbc_bytes = c->bytes - bytes0;
+  CK(cudaStreamSynchronize(c->stream));
+  c->nbc_nface = nface;
+  c->nbc_nfeat = nfeature;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *c, int nfeature, const double *load_np1) {
+  if (!c || nfeature != c->nbc_nfeat || (nfeature && !load_np1)) return PGFEM_GPU_EINVAL;
+  if (!nfeature) return PGFEM_GPU_OK;
+  std::vector<int> t(nfeature);
+  CK(cudaMemcpyAsync(t.data(), c->nbc_type, sizeof(int) * nfeature, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<double> ld((size_t)3 * nfeature);
+  for (int f = 0; f < nfeature; f++)
+    for (int i = 0; i < 3; i++) ld[(size_t)3 * f + i] = i < t[f] ? load_np1[(size_t)3 * f + i] : 0.0;
+  CK(cudaMemcpyAsync(c->nbc_load, ld.data(), sizeof(double) * ld.size(), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
 int pgfem_gpu_set_wait_test(pgfem_gpu_ctx *c, double limit_s, int stall_next_assembly) {
   if (!c || !(limit_s > 0.0) || limit_s > 60.0) return PGFEM_GPU_EINVAL;
   c->wait_ns = (unsigned long long)(limit_s * 1e9);
@@ -1005,16 +1139,17 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *c) { return c ? c->nnz : -1; }
 
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *c) {
   if (!c) return -1;
+  const int nbc = c->nbc_nface ? 1 : 0;  // the surface-load kernel
   if (c->model == PGFEM_MODEL_CP)  // u expansion, F, local Newton, tangent, element (+ features, network, guess)
-    return c->cp_net ? 8 : 5;
+    return (c->cp_net ? 8 : 5) + nbc;
   if (c->mat.dev_pot == 2)  // u expansion + per-node kernel launches (one per colour in colour mode)
-    return 1 + (c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1);
+    return 1 + (c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1) + nbc;
   if (c->nne == 10 && c->scatter_mode == PGFEM_SCATTER_ATOMIC)
-    return 3;  // u expansion, point updates, tensor-core R+K assembly
+    return 3 + nbc;  // u expansion, point updates, tensor-core R+K assembly
   if (c->nne == 4 && c->scatter_mode == PGFEM_SCATTER_ATOMIC)
-    return 3;  // u expansion, point updates, column-split R+K assembly
+    return 3 + nbc;  // u expansion, point updates, column-split R+K assembly
   const int nasm = c->scatter_mode == PGFEM_SCATTER_COLOUR ? (int)c->colour_off.size() - 1 : 1;
-  return 1 + nasm;  // u expansion + assembly launches (memsets are not kernels of ours)
+  return 1 + nasm + nbc;  // u expansion + assembly launches (memsets are not kernels of ours)
 }
 
 int pgfem_gpu_set_cp_guess(pgfem_gpu_ctx *c, const double *guess) {
@@ -1410,6 +1545,7 @@ static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const do
     a.fe_out = d_fe;
     r = lk ? dispatch<false, true, true>(c, a, nel, c->stream) : dispatch<false, false, true>(c, a, nel, c->stream);
   }
+  if (!r) r = launch_neumann(c, nullptr, nullptr, c->stream, d_el, nel, d_lk, d_fe);
   if (!r) {
     cudaMemcpyAsync(fe, d_fe, sizeof(double) * nel * nd, cudaMemcpyDeviceToHost, c->stream);
     if (lk) cudaMemcpyAsync(lk, d_lk, sizeof(double) * nel * nd * nd, cudaMemcpyDeviceToHost, c->stream);

@@ -72,6 +72,8 @@ def lib():
             "pgfem_gpu_destroy": (C.c_int, [_P]),
             "pgfem_gpu_set_scatter_mode": (C.c_int, [_P, C.c_int]),
             "pgfem_gpu_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
+            "pgfem_gpu_set_neumann": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_int, _P, _P]),
+            "pgfem_gpu_set_neumann_loads": (C.c_int, [_P, C.c_int, _P]),
             "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_device_bytes": (C.c_long, [_P]),
             "pgfem_gpu_nnz": (C.c_long, [_P]),
@@ -268,6 +270,27 @@ class Context:
         """Failure-path tests: hand-off wait bound (s) of the linear-tet R+K
         kernel; stall_next withholds the next assembly's first hand-off."""
         _check("pgfem_gpu_set_wait_test", lib().pgfem_gpu_set_wait_test(self.h, limit_s, int(stall_next)))
+
+    def set_neumann(self, elem, face, feature, load_type, load_np1):
+        """Surface loads (the reference's NBC features, src/fd_residuals.cc:123-273):
+        face k is local face face[k] (0..3) of element elem[k] with feature
+        feature[k]; feature f has load_type[f] values (1 pressure, 2..3 traction)
+        in load_np1[f] (3 each).  Empty elem clears."""
+        el = np.ascontiguousarray(elem, dtype=np.int64).ravel()
+        fc = np.ascontiguousarray(face, dtype=np.int32).ravel()
+        ft = np.ascontiguousarray(feature, dtype=np.int32).ravel()
+        lt = np.ascontiguousarray(load_type, dtype=np.int32).ravel()
+        ld = np.ascontiguousarray(np.reshape(load_np1, (-1, 3)) if len(lt) else np.zeros((0, 3)),
+                                  dtype=np.float64)
+        if not (len(el) == len(fc) == len(ft)) or len(ld) != len(lt):
+            raise ValueError("set_neumann: array lengths differ")
+        self._nbc_keep = (el, fc, ft, lt, ld)
+        _check("pgfem_gpu_set_neumann", lib().pgfem_gpu_set_neumann(self.h, len(el), _ptr(el), _ptr(fc), _ptr(ft),
+                                                                      len(lt), _ptr(lt), _ptr(ld)))
+
+    def set_neumann_loads(self, load_np1):
+        ld = np.ascontiguousarray(np.reshape(load_np1, (-1, 3)), dtype=np.float64)
+        _check("pgfem_gpu_set_neumann_loads", lib().pgfem_gpu_set_neumann_loads(self.h, len(ld), _ptr(ld)))
 
     def set_scatter_mode(self, mode):
         _check("pgfem_gpu_set_scatter_mode", lib().pgfem_gpu_set_scatter_mode(self.h, mode))

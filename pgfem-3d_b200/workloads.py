@@ -80,6 +80,20 @@ def nodal_to_free(ids, disp):
     return u
 
 
+# local faces of a tet by their vertex nodes (FEMLIB's Tet2Tri numbering)
+TET_FACES = np.array([[0, 2, 1], [0, 1, 3], [1, 2, 3], [0, 3, 2]])
+
+
+def box_faces(X, conn, axis, value, tol=1e-12):
+    """The element faces lying on the plane X[axis] = value: (elem, face)
+    arrays, face the local face 0..3 whose three vertex nodes are on it (the
+    synthetic meshes' stand-in for the reference's boundary features)."""
+    on = np.abs(X[:, axis] - value) <= tol
+    hit = on[conn[:, TET_FACES]].all(axis=2)  # (ne, 4)
+    e, f = np.nonzero(hit)
+    return e.astype(np.int64), f.astype(np.int32)
+
+
 def he_p1(n=10, seed=0):
     X, conn, Pr = pg.mesh_box_tet(n, 4)
     nn = X.shape[0]
