@@ -504,7 +504,48 @@ int pgfem_input_read_orientations(const pgfem_input *in, const char *base, doubl
 int pgfem_input_get_partition(const pgfem_input *in, int part, long *nn, long *ne, long *node_map);
 /* Pr[nn]: periodic master of each node or -1 (the pgfem_generate_dof_ids Pr input). */
 int pgfem_input_get_periodic(const pgfem_input *in, long *Pr);
+/* The boundary feature of each element face, read from the element lines
+ * (bnd_type[4], bnd_id[4], src/element.cc:168-199): bnd_type[ne*4] and
+ * bnd_id[ne*4] (each may be NULL), merged element order, local faces 0..3. */
+int pgfem_input_get_element_faces(const pgfem_input *in, int *bnd_type, int *bnd_id);
 void pgfem_input_destroy(pgfem_input *in);
+
+/* Surface-load files: <ipath>/NBC/<physics>.nbc (read_Neumann_boundary_conditions,
+ * src/read_input_file.cc:168-214): a feature count, then per feature its
+ * type, id, number of load values (1 pressure, 2..3 traction) and one file
+ * name per value, whose first line is the load as an expression of time t
+ * (read_loads, src/PGFem3D_data_structure.cc:934-948).  A missing directory
+ * or file means no surface loads (an empty set, as in the reference).  The
+ * reference evaluates the expressions with the exprtk library
+ * (string_function_of_time, src/utils.cc:3423-3440); this library evaluates
+ * the arithmetic subset pgfem_load_expression documents and rejects the rest
+ * (EFORMAT).  A feature listed twice is rejected too: the reference would
+ * then load face 0 of the element with feature 0 (its list has more rows
+ * than flagged faces, src/PGFem3D_data_structure.cc:870-891). */
+typedef struct pgfem_nbc pgfem_nbc;
+int pgfem_input_read_nbc(const char *ipath, const char *physics, pgfem_nbc **out);
+/* Feature count and, per feature (arrays may be NULL), type, id, load type. */
+int pgfem_nbc_get_features(const pgfem_nbc *nbc, int *nfeature, int *ftype, int *fid, int *load_type);
+/* The loaded faces of the mesh (construct_list_of_boundary_elements,
+ * src/PGFem3D_data_structure.cc:825-895): every element face whose
+ * (bnd_type, bnd_id) is a feature's (type, id), in element then face order;
+ * nface receives the count (elem/face/feature may be NULL to count first).
+ * The arrays are pgfem_gpu_set_neumann's. */
+int pgfem_nbc_faces(const pgfem_nbc *nbc, const pgfem_input *in, long *nface, long *elem, int *face, int *feature);
+/* The features' load values at time t (compute_load_values,
+ * src/PGFem3D_data_structure.cc:956-972): load[nfeature*3], entries past a
+ * feature's load type 0; pgfem_gpu_set_neumann_loads' input. */
+int pgfem_nbc_load_values(const pgfem_nbc *nbc, double t, double *load);
+void pgfem_nbc_destroy(pgfem_nbc *nbc);
+/* One load expression at time t (names case-insensitive, comments # and //
+ * to the end of the line and slash-star blocks skipped): numbers, t, pi,
+ * epsilon, inf, true, false;
+ * + - * / % ^ (right associative, above unary minus), comparisons (< <= > >=
+ * == = != <>), and / or / not (also && || & |), c ? a : b; functions if(c,a,b),
+ * min, max (1 or more arguments), clamp(lo,x,hi), pow, atan2, hypot, mod, abs,
+ * sgn, sqrt, exp, log, log10, log2, floor, ceil, round, trunc, frac, sin, cos,
+ * tan, asin, acos, atan, sinh, cosh, tanh; an optional trailing ';'. */
+int pgfem_load_expression(const char *expr, double t, double *value);
 /* R = Az(psi) Ay(theta) Ax(phi), right-handed rotations about the axes (the
  * composition the reference states at src/plasticity_model.cc:1252-1255; its
  * rotation_matrix_of_Euler_angles lives in an absent library).  With this R

@@ -122,6 +122,7 @@ struct pgfem_input {
   std::vector<int> elem_part;
   std::vector<double> defl, mat_vals, cf, ee;
   std::vector<int> dev_pot, vol_pot;
+  std::vector<int> bnd_id, bnd_type;  // 4 per element: the faces' boundary features
   int nparts = 0;
   std::vector<long> part_elem_off;  // merged element index of each partition's first element
   std::vector<std::vector<long>> node_map;  // per partition: merged id of each local node
@@ -138,6 +139,7 @@ struct Part {
   std::vector<long> codes;
   std::vector<double> defl;
   std::vector<long> conn, emat, ehom;
+  std::vector<int> bid, btype;  // per element and face: boundary feature id and type
   std::vector<double> mats, cf, ee;
   std::vector<int> devp, volp;
   long nln = 0, nel_s = 0, nel_v = 0;
@@ -223,6 +225,8 @@ int read_part(const std::string &path, Part &p, const PhysLayout &L) {
   if (p.ne && nne != 4 && nne != 10)
     return fail(path + ": element type " + std::to_string(nne) + " (linear or quadratic tets on this path)");
   p.conn.assign(p.ne * nne, -1);
+  p.bid.assign(4 * p.ne, 0);
+  p.btype.assign(4 * p.ne, 0);
   std::vector<char> seen(p.ne, 0);
   for (long k = 0; k < p.ne; k++) {
     long id;
@@ -233,10 +237,14 @@ int read_part(const std::string &path, Part &p, const PhysLayout &L) {
       if (!t.num(n) || n < 0 || n >= p.nn) return bad("element node");
       p.conn[id * nne + a] = n;
     }
-    for (int k2 = 0; k2 < 11; k2++) {
+    for (int k2 = 0; k2 < 3; k2++) {  // ftype fid pr
       long v;
       if (!t.num(v)) return bad("element face data");
     }
+    for (int f = 0; f < 4; f++)
+      if (!t.num(p.bid[4 * id + f])) return bad("element face feature id");
+    for (int f = 0; f < 4; f++)
+      if (!t.num(p.btype[4 * id + f])) return bad("element face feature type");
   }
   // element materials: id mat[2] hom[2]
   p.emat.assign(2 * p.ne, 0);
@@ -449,6 +457,10 @@ int pgfem_input_read_mesh_mp(const char *base, int nparts, const char *bc_base, 
       in->elem_hom.push_back(p.ehom[2 * e + 1]);
       in->elem_part.push_back(r);
       in->elem_local.push_back(e);
+      for (int f = 0; f < 4; f++) {
+        in->bnd_id.push_back(p.bid[4 * e + f]);
+        in->bnd_type.push_back(p.btype[4 * e + f]);
+      }
     }
     I.nln += p.nln;
     I.nel_s += p.nel_s;
@@ -879,5 +891,386 @@ int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int 
   }
   return PGFEM_GPU_OK;
 }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Surface loads: NBC/<physics>.nbc (read_Neumann_boundary_conditions,
+// src/read_input_file.cc:168-214; NeumannBoundaryElement::read_loads,
+// src/PGFem3D_data_structure.cc:934-948), the element faces they load
+// (construct_list_of_boundary_elements, :825-895, from the elements' face
+// features, src/element.cc:168-199) and their load values at a time
+// (compute_load_values, :956-972).  The reference evaluates each load file's
+// first line with the exprtk library as a function of t with exprtk's
+// constants (string_function_of_time, src/utils.cc:3423-3440); this reader
+// evaluates the arithmetic subset written below (comments, numbers, t, pi, epsilon, inf,
+// + - * / % ^, comparisons, and / or, "c ? a : b", if(c, a, b), min, max,
+// clamp, abs, sgn, sqrt, exp, log, log10, log2, pow, hypot, floor, ceil,
+// round, trunc, frac, sin, cos, tan, asin, acos, atan, atan2, sinh, cosh,
+// tanh), and rejects anything else with EFORMAT rather than guessing.
+// ---------------------------------------------------------------------------
+struct pgfem_nbc {
+  std::vector<int> ftype, fid, ltype;
+  std::vector<std::string> expr;  // 3 per feature, load_type of them set
+};
+
+namespace {
+
+struct Expr {
+  const std::string &s;
+  double t;
+  size_t i = 0;
+  std::string err;
+
+  Expr(const std::string &src, double tv) : s(src), t(tv) {}
+  // white space and comments (# or // to the end of the line, /* ... */)
+  void ws() {
+    for (;;) {
+      while (i < s.size() && isspace((unsigned char)s[i])) i++;
+      if (i < s.size() && (s[i] == '#' || s.compare(i, 2, "//") == 0)) {
+        while (i < s.size() && s[i] != '\n') i++;
+      } else if (s.compare(i, 2, "/*") == 0) {
+        const size_t e = s.find("*/", i + 2);
+        i = e == std::string::npos ? s.size() : e + 2;
+      } else {
+        return;
+      }
+    }
+  }
+  bool eat(const char *tok) {
+    ws();
+    const size_t n = strlen(tok);
+    if (s.compare(i, n, tok) != 0) return false;
+    // a word operator must not run into an identifier
+    if (isalpha((unsigned char)tok[0]) && i + n < s.size() && (isalnum((unsigned char)s[i + n]) || s[i + n] == '_'))
+      return false;
+    i += n;
+    return true;
+  }
+  bool fail_at(const std::string &m) {
+    if (err.empty()) err = m + " at column " + std::to_string(i + 1);
+    return false;
+  }
+  bool ternary(double &v) {
+    if (!logic_or(v)) return false;
+    if (eat("?")) {
+      double a, b;
+      if (!ternary(a)) return false;
+      if (!eat(":")) return fail_at("expected ':'");
+      if (!ternary(b)) return false;
+      v = v != 0.0 ? a : b;
+    }
+    return true;
+  }
+  bool logic_or(double &v) {
+    if (!logic_and(v)) return false;
+    for (;;) {
+      if (eat("||") || eat("or") || eat("|")) {
+        double w;
+        if (!logic_and(w)) return false;
+        v = (v != 0.0 || w != 0.0) ? 1.0 : 0.0;
+      } else {
+        return true;
+      }
+    }
+  }
+  bool logic_and(double &v) {
+    if (!compare(v)) return false;
+    for (;;) {
+      if (eat("&&") || eat("and") || eat("&")) {
+        double w;
+        if (!compare(w)) return false;
+        v = (v != 0.0 && w != 0.0) ? 1.0 : 0.0;
+      } else {
+        return true;
+      }
+    }
+  }
+  bool compare(double &v) {
+    if (!additive(v)) return false;
+    for (;;) {
+      int op;
+      if (eat("<=")) op = 0;
+      else if (eat(">=")) op = 1;
+      else if (eat("==")) op = 2;
+      else if (eat("!=") || eat("<>")) op = 3;
+      else if (eat("<")) op = 4;
+      else if (eat(">")) op = 5;
+      else if (eat("=")) op = 2;
+      else return true;
+      double w;
+      if (!additive(w)) return false;
+      const bool r[6] = {v <= w, v >= w, v == w, v != w, v < w, v > w};
+      v = r[op] ? 1.0 : 0.0;
+    }
+  }
+  bool additive(double &v) {
+    if (!multiplicative(v)) return false;
+    for (;;) {
+      if (eat("+")) {
+        double w;
+        if (!multiplicative(w)) return false;
+        v += w;
+      } else if (eat("-")) {
+        double w;
+        if (!multiplicative(w)) return false;
+        v -= w;
+      } else {
+        return true;
+      }
+    }
+  }
+  bool multiplicative(double &v) {
+    if (!unary(v)) return false;
+    for (;;) {
+      if (eat("*")) {
+        double w;
+        if (!unary(w)) return false;
+        v *= w;
+      } else if (eat("/")) {
+        double w;
+        if (!unary(w)) return false;
+        v /= w;
+      } else if (eat("%")) {
+        double w;
+        if (!unary(w)) return false;
+        v = std::fmod(v, w);
+      } else {
+        return true;
+      }
+    }
+  }
+  bool unary(double &v) {
+    if (eat("-")) {
+      if (!unary(v)) return false;
+      v = -v;
+      return true;
+    }
+    if (eat("+")) return unary(v);
+    if (eat("not")) {
+      if (!unary(v)) return false;
+      v = v == 0.0 ? 1.0 : 0.0;
+      return true;
+    }
+    return power(v);
+  }
+  bool power(double &v) {
+    if (!primary(v)) return false;
+    if (eat("^")) {
+      double w;
+      if (!unary(w)) return false;  // right associative
+      v = std::pow(v, w);
+    }
+    return true;
+  }
+  bool args(std::vector<double> &a) {
+    if (!eat("(")) return fail_at("expected '('");
+    if (eat(")")) return true;
+    for (;;) {
+      double v;
+      if (!ternary(v)) return false;
+      a.push_back(v);
+      if (eat(")")) return true;
+      if (!eat(",")) return fail_at("expected ',' or ')'");
+    }
+  }
+  bool primary(double &v) {
+    ws();
+    if (i >= s.size()) return fail_at("unexpected end");
+    if (eat("(")) {
+      if (!ternary(v)) return false;
+      if (!eat(")")) return fail_at("expected ')'");
+      return true;
+    }
+    const char c = s[i];
+    if (isdigit((unsigned char)c) || c == '.') {
+      const char *b = s.c_str() + i;
+      char *end = nullptr;
+      v = strtod(b, &end);
+      if (end == b) return fail_at("bad number");
+      i += (size_t)(end - b);
+      return true;
+    }
+    if (!isalpha((unsigned char)c) && c != '_') return fail_at(std::string("unexpected '") + c + "'");
+    const size_t b = i;
+    while (i < s.size() && (isalnum((unsigned char)s[i]) || s[i] == '_')) i++;
+    std::string w = s.substr(b, i - b);
+    for (char &ch : w) ch = (char)tolower((unsigned char)ch);
+    if (w == "t") return v = t, true;
+    if (w == "pi") return v = 3.14159265358979323846, true;
+    if (w == "epsilon") return v = 2.220446049250313e-16, true;
+    if (w == "inf") return v = HUGE_VAL, true;
+    if (w == "true") return v = 1.0, true;
+    if (w == "false") return v = 0.0, true;
+    std::vector<double> a;
+    const size_t at = b;
+    if (!args(a)) return false;
+    auto need = [&](size_t n) {
+      if (a.size() == n) return true;
+      i = at;
+      return fail_at(w + " takes " + std::to_string(n) + " argument(s)");
+    };
+    if (w == "min" || w == "max") {
+      if (a.empty()) return need(1);
+      v = a[0];
+      for (double x : a) v = w == "min" ? std::min(v, x) : std::max(v, x);
+      return true;
+    }
+    if (w == "if") return need(3) && (v = a[0] != 0.0 ? a[1] : a[2], true);
+    if (w == "clamp") return need(3) && (v = std::min(std::max(a[1], a[0]), a[2]), true);
+    if (w == "pow") return need(2) && (v = std::pow(a[0], a[1]), true);
+    if (w == "atan2") return need(2) && (v = std::atan2(a[0], a[1]), true);
+    if (w == "hypot") return need(2) && (v = std::hypot(a[0], a[1]), true);
+    if (w == "mod") return need(2) && (v = std::fmod(a[0], a[1]), true);
+    if (!need(1)) return false;
+    const double x = a[0];
+    if (w == "abs") v = std::fabs(x);
+    else if (w == "sgn") v = x > 0 ? 1.0 : (x < 0 ? -1.0 : 0.0);
+    else if (w == "sqrt") v = std::sqrt(x);
+    else if (w == "exp") v = std::exp(x);
+    else if (w == "log") v = std::log(x);
+    else if (w == "log10") v = std::log10(x);
+    else if (w == "log2") v = std::log2(x);
+    else if (w == "floor") v = std::floor(x);
+    else if (w == "ceil") v = std::ceil(x);
+    else if (w == "round") v = std::round(x);
+    else if (w == "trunc") v = std::trunc(x);
+    else if (w == "frac") v = x - std::trunc(x);
+    else if (w == "sin") v = std::sin(x);
+    else if (w == "cos") v = std::cos(x);
+    else if (w == "tan") v = std::tan(x);
+    else if (w == "asin") v = std::asin(x);
+    else if (w == "acos") v = std::acos(x);
+    else if (w == "atan") v = std::atan(x);
+    else if (w == "sinh") v = std::sinh(x);
+    else if (w == "cosh") v = std::cosh(x);
+    else if (w == "tanh") v = std::tanh(x);
+    else {
+      i = at;
+      return fail_at("unknown function or name '" + w + "'");
+    }
+    return true;
+  }
+  // a whole expression, optionally ended by ';'
+  bool run(double &v) {
+    if (!ternary(v)) return false;
+    eat(";");
+    ws();
+    if (i != s.size()) return fail_at("trailing text");
+    return true;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int pgfem_input_get_element_faces(const pgfem_input *in, int *bnd_type, int *bnd_id) {
+  if (!in) return PGFEM_GPU_EINVAL;
+  if (bnd_type) std::copy(in->bnd_type.begin(), in->bnd_type.end(), bnd_type);
+  if (bnd_id) std::copy(in->bnd_id.begin(), in->bnd_id.end(), bnd_id);
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_load_expression(const char *expr, double t, double *value) {
+  if (!expr || !value) return PGFEM_GPU_EINVAL;
+  const std::string s(expr);
+  Expr x(s, t);
+  double v = 0.0;
+  if (!x.run(v)) return fail("load expression \"" + s + "\": " + x.err);
+  *value = v;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_input_read_nbc(const char *ipath, const char *physics, pgfem_nbc **out) {
+  if (!ipath || !physics || !out) return PGFEM_GPU_EINVAL;
+  *out = nullptr;
+  auto *nb = new pgfem_nbc();
+  const std::string dir = std::string(ipath) + "/NBC";
+  Tokens t;
+  if (!t.load(dir + "/" + physics + ".nbc")) {  // no NBC directory or file: no surface loads
+    *out = nb;
+    return PGFEM_GPU_OK;
+  }
+  auto reject = [&](const std::string &m) {
+    delete nb;
+    return fail(m);
+  };
+  long nf;
+  if (!t.num(nf) || nf < 0) return reject("bad feature count at " + t.where());
+  for (long f = 0; f < nf; f++) {
+    int ft, fi, lt;
+    if (!t.num(ft) || !t.num(fi) || !t.num(lt)) return reject("bad feature line at " + t.where());
+    if (lt < 1 || lt > 3) return reject("load type " + std::to_string(lt) + " at " + t.where() + " (1 to 3 values)");
+    for (long g = 0; g < f; g++)
+      if (nb->ftype[g] == ft && nb->fid[g] == fi)
+        return reject("feature (" + std::to_string(ft) + ", " + std::to_string(fi) + ") listed twice at " + t.where());
+    nb->ftype.push_back(ft);
+    nb->fid.push_back(fi);
+    nb->ltype.push_back(lt);
+    for (int k = 0; k < 3; k++) {
+      std::string line;
+      if (k < lt) {
+        std::string fn;
+        if (!t.next(fn)) return reject("missing load file name at " + t.where());
+        FILE *fp = fopen((dir + "/" + fn).c_str(), "rb");
+        if (!fp) return reject("cannot open " + dir + "/" + fn);
+        int ch;
+        while ((ch = fgetc(fp)) != EOF && ch != '\n') line.push_back((char)ch);
+        fclose(fp);
+        double v;
+        Expr x(line, 0.0);
+        if (!x.run(v)) return reject(dir + "/" + fn + ": " + x.err);
+      }
+      nb->expr.push_back(line);
+    }
+  }
+  *out = nb;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_nbc_get_features(const pgfem_nbc *nb, int *nfeature, int *ftype, int *fid, int *load_type) {
+  if (!nb) return PGFEM_GPU_EINVAL;
+  const size_t n = nb->ftype.size();
+  if (nfeature) *nfeature = (int)n;
+  if (ftype) std::copy(nb->ftype.begin(), nb->ftype.end(), ftype);
+  if (fid) std::copy(nb->fid.begin(), nb->fid.end(), fid);
+  if (load_type) std::copy(nb->ltype.begin(), nb->ltype.end(), load_type);
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_nbc_faces(const pgfem_nbc *nb, const pgfem_input *in, long *nface, long *elem, int *face, int *feature) {
+  if (!nb || !in || !nface) return PGFEM_GPU_EINVAL;
+  long k = 0;
+  for (long e = 0; e < in->info.ne; e++)
+    for (int f = 0; f < 4; f++) {
+      int hit = -1;
+      for (size_t g = 0; g < nb->ftype.size(); g++)
+        if (nb->ftype[g] == in->bnd_type[4 * e + f] && nb->fid[g] == in->bnd_id[4 * e + f]) hit = (int)g;
+      if (hit < 0) continue;
+      if (elem) elem[k] = e;
+      if (face) face[k] = f;
+      if (feature) feature[k] = hit;
+      k++;
+    }
+  *nface = k;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_nbc_load_values(const pgfem_nbc *nb, double t, double *load) {
+  if (!nb || !load) return PGFEM_GPU_EINVAL;
+  for (size_t f = 0; f < nb->ftype.size(); f++)
+    for (int k = 0; k < 3; k++) {
+      double v = 0.0;
+      if (k < nb->ltype[f]) {
+        Expr x(nb->expr[3 * f + k], t);
+        if (!x.run(v)) return fail("load expression \"" + nb->expr[3 * f + k] + "\": " + x.err);
+      }
+      load[3 * f + k] = v;
+    }
+  return PGFEM_GPU_OK;
+}
+
+void pgfem_nbc_destroy(pgfem_nbc *nb) { delete nb; }
 
 }  // extern "C"

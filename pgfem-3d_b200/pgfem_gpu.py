@@ -139,6 +139,13 @@ def lib():
             "pgfem_input_destroy": (None, [_P]),
             "pgfem_input_get_partition": (C.c_int, [_P, C.c_int, _P, _P, _P]),
             "pgfem_input_get_periodic": (C.c_int, [_P, _P]),
+            "pgfem_input_get_element_faces": (C.c_int, [_P, _P, _P]),
+            "pgfem_input_read_nbc": (C.c_int, [C.c_char_p, C.c_char_p, _P]),
+            "pgfem_nbc_get_features": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_nbc_faces": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+            "pgfem_nbc_load_values": (C.c_int, [_P, C.c_double, _P]),
+            "pgfem_nbc_destroy": (None, [_P]),
+            "pgfem_load_expression": (C.c_int, [C.c_char_p, C.c_double, _P]),
             "pgfem_euler_rotation": (C.c_int, [C.c_long, _P, _P]),
             "pgfem_input_read_solver_file": (C.c_int, [C.c_char_p, C.c_long, _P, _P, _P, _P, _P]),
             "pgfem_input_j2_material": (C.c_int, [_P, C.c_double, C.c_double, C.c_int, _P]),
@@ -768,6 +775,13 @@ class InputMesh:
         args.update(kw)
         return material(model, **args)
 
+    def element_faces(self):
+        """(bnd_type, bnd_id), each (ne, 4): the boundary feature of every face."""
+        bt = np.zeros((self.info.ne, 4), dtype=np.int32)
+        bi = np.zeros((self.info.ne, 4), dtype=np.int32)
+        _check("pgfem_input_get_element_faces", lib().pgfem_input_get_element_faces(self._h, _ptr(bt), _ptr(bi)))
+        return bt, bi
+
     def dof_setup(self):
         """(ids, ndof, Ap, Ai) of the merged mesh (generate_dof_ids with the
         periodic links + Psparse_ApAi)."""
@@ -775,6 +789,51 @@ class InputMesh:
         ids, ndof = generate_dof_ids(self.conn, self.X.shape[0], self.codes, Pr)
         Ap, Ai = psparse_apai(self.conn, ids, ndof)
         return ids, ndof, Ap, Ai
+
+
+class NbcFile:
+    """Surface loads of <ipath>/NBC/<physics>.nbc (pgfem_input_read_nbc):
+    features (type, id, load type), the loaded faces of a mesh and the load
+    values at a time -- the inputs of Context.set_neumann / set_neumann_loads."""
+
+    def __init__(self, ipath, physics="Mechanical"):
+        h = C.c_void_p()
+        _check_input("pgfem_input_read_nbc", lib().pgfem_input_read_nbc(ipath.encode(), physics.encode(), C.byref(h)))
+        self._h = h
+        n = C.c_int()
+        _check("pgfem_nbc_get_features", lib().pgfem_nbc_get_features(h, C.byref(n), None, None, None))
+        self.ftype = np.zeros(n.value, dtype=np.int32)
+        self.fid = np.zeros(n.value, dtype=np.int32)
+        self.load_type = np.zeros(n.value, dtype=np.int32)
+        _check("pgfem_nbc_get_features", lib().pgfem_nbc_get_features(h, None, _ptr(self.ftype), _ptr(self.fid),
+                                                                      _ptr(self.load_type)))
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.pgfem_nbc_destroy(self._h)
+            self._h = None
+
+    def faces(self, mesh):
+        """(elem, face, feature) of the faces of an InputMesh these features load."""
+        n = C.c_long()
+        _check("pgfem_nbc_faces", lib().pgfem_nbc_faces(self._h, mesh._h, C.byref(n), None, None, None))
+        el = np.zeros(n.value, dtype=np.int64)
+        fc = np.zeros(n.value, dtype=np.int32)
+        ft = np.zeros(n.value, dtype=np.int32)
+        _check("pgfem_nbc_faces", lib().pgfem_nbc_faces(self._h, mesh._h, C.byref(n), _ptr(el), _ptr(fc), _ptr(ft)))
+        return el, fc, ft
+
+    def load_values(self, t):
+        v = np.zeros((len(self.ftype), 3))
+        _check_input("pgfem_nbc_load_values", lib().pgfem_nbc_load_values(self._h, t, _ptr(v)))
+        return v
+
+
+def load_expression(expr, t):
+    """Value of a load expression of time t (pgfem_load_expression)."""
+    v = C.c_double()
+    _check_input("pgfem_load_expression", lib().pgfem_load_expression(expr.encode(), t, C.byref(v)))
+    return v.value
 
 
 def read_multiphysics(path, max_phys=16):

@@ -21,11 +21,12 @@ def material_line(Ex, nu, dev_pot, vol_pot, Ey=0.0, Ez=0.0, G=0.0):
 
 
 def write_mesh(path, X, conn, codes, defl, mat_lines, gnn=None, dom=None, elem_mat=None, local_order=None,
-               before=()):
+               before=(), bnd=None):
     """One mesh file.  gnn/dom per local node (default: Gnn = id, Dom = 0);
     local_order: the order in which node lines are written (default 0..nn-1);
     before: supports sections of other physics written ahead of the
-    mechanical one, each (codes (nn, ndim), values)."""
+    mechanical one, each (codes (nn, ndim), values); bnd: (bnd_type, bnd_id),
+    each (ne, 4), the boundary feature of every element face (default 0)."""
     nn, ne, nne = X.shape[0], conn.shape[0], conn.shape[1]
     gnn = np.arange(nn) if gnn is None else gnn
     dom = np.zeros(nn, dtype=int) if dom is None else dom
@@ -43,8 +44,10 @@ def write_mesh(path, X, conn, codes, defl, mat_lines, gnn=None, dom=None, elem_m
     sup = [i for i in range(nn) if np.any(codes[i] != 0)]
     L += ["", str(len(sup))] + ["%d  %d %d %d " % (i, *codes[i]) for i in sup]
     L += ["", str(len(defl)), " ".join("%.17g" % v for v in defl), ""]
+    bt, bi = (np.zeros((ne, 4), dtype=int),) * 2 if bnd is None else bnd
     for e in range(ne):
-        L.append("%d  %s  4 1 0  0 0 0 0  0 0 0 0" % (e, " ".join(str(int(n)) for n in conn[e])))
+        L.append("%d  %s  4 1 0  %s  %s" % (e, " ".join(str(int(n)) for n in conn[e]),
+                                           " ".join(str(int(v)) for v in bi[e]), " ".join(str(int(v)) for v in bt[e])))
     L.append("")
     L += ["%d  %d 0 %d 0 " % (e, elem_mat[e], elem_mat[e]) for e in range(ne)]
     L += [""] + list(mat_lines) + ["", "1.000000 ",

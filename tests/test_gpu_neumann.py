@@ -182,3 +182,34 @@ def test_bad_faces_rejected(gpu):
     with pytest.raises(pg.PgfemError):  # wrong number of features
         ctx.set_neumann_loads(np.zeros((2, 3)))
     ctx.close()
+
+
+def test_input_files_drive_surface_loads(gpu, tmp_path):
+    """A mesh with face features and NBC files read through the input API,
+    the loaded faces and their load values at t handed to the context."""
+    from test_nbc_reader import _box_input, _write_nbc
+    tmp = str(tmp_path)
+    base, X, conn, _, _ = _box_input(tmp, nne=10, n=2)
+    _write_nbc(tmp, ["2", "2 5 3 tx ty tz", "2 7 1 p"], {"tx": "100*t", "ty": "20", "tz": "-50*t",
+                                                        "p": "if(t < 1, 30*t, 30)"})
+    mesh = pg.InputMesh(base)
+    nb = pg.NbcFile(tmp)
+    ids, ndof, Ap, Ai = mesh.dof_setup()
+    mat = mesh.material(0)
+    ctx = pg.Context(mesh.X, mesh.conn, ids, ndof, Ap, Ai, mat)
+    el, fc, ft = nb.faces(mesh)
+    ctx.set_neumann(el, fc, ft, nb.load_type, nb.load_values(0.0))
+    u = 1e-3 * np.random.default_rng(2).uniform(-1, 1, ndof)
+    P = oracle.Problem(mesh.X, mesh.conn, ids, ndof, Ap, Ai)
+    om = oracle.from_pg_material(mat)
+    for t in (0.5, 2.0):
+        loads = nb.load_values(t)
+        ctx.set_neumann_loads(loads)
+        R, K, st = ctx.assemble_RK(u)
+        assert st.ok()
+        P.set_neumann(el, fc, nb.load_type[ft], loads[ft])
+        err, Ro, Ko, _ = P.assemble(om, u)
+        assert err == 0
+        check_R(R, Ro)
+        check_K(K, Ko, Ap)
+    ctx.close()
