@@ -511,13 +511,23 @@ def run_cp_warm(args, ws, rank, local):
     clk = ClockSampler(local)
     clk.start()
     time.sleep(0.3)
-    ms_c, upd_c, it_c = timed()
-    R_c = d_R.cpu().numpy()
-    s_c = ctx.get_state(1)
+    # plain and warm runs alternate; the speed-ups are reported as the median
+    # and the range over the repeats
+    runs = []
     ctx.set_cp_warm_limit(args.warm_k)
-    ctx.set_cp_surrogate(net)
-    ms_w, upd_w, it_w = timed()
+    for r in range(max(1, args.repeats)):
+        ctx.set_cp_surrogate(None)
+        ms_c, upd_c, it_c = timed()
+        if r == 0:
+            R_c = d_R.cpu().numpy()
+            s_c = ctx.get_state(1)
+        ctx.set_cp_surrogate(net)
+        ms_w, upd_w, it_w = timed()
+        runs.append((ms_c, ms_w, upd_c, upd_w))
     clocks = clk.stop()
+    runs = np.array(runs)
+    ms_c, ms_w, upd_c, upd_w = (float(np.median(runs[:, k])) for k in range(4))
+    sp_it, sp_upd = runs[:, 0] / runs[:, 1], runs[:, 2] / runs[:, 3]
     launches = ctx.launches_per_assembly()  # with the network attached
     fb = ctx.cp_fallbacks()
     R_w = d_R.cpu().numpy()
@@ -546,9 +556,13 @@ def run_cp_warm(args, ws, rank, local):
                                   "(cold-start fallback after %d iterations)"
                                   % (args.cp_n, p.ne, args.cp_step, wl.CP_STEPS, args.warm_k),
                       "plain_value": ws * p.nqp / (ms_c * 1e-3), "plain_ms_per_step": ms_c,
-                      "speedup_rk_iterate": ms_c / ms_w,
+                      "repeats": int(len(runs)),
+                      "speedup_rk_iterate": float(np.median(sp_it)),
+                      "speedup_rk_iterate_range": [float(sp_it.min()), float(sp_it.max())],
                       "local_update_ms": {"plain": upd_c, "warm": upd_w},
-                      "speedup_local_update": upd_c / upd_w,
+                      "speedup_local_update": float(np.median(sp_upd)),
+                      "speedup_local_update_range": [float(sp_upd.min()), float(sp_upd.max())],
+                      "speedup_runs": [[float(a), float(b)] for a, b in zip(sp_it, sp_upd)],
                       "iterations_mean": {"plain": float(it_c.mean()), "warm": float(it_w.mean())},
                       "iterations_hist": {"plain": np.bincount(it_c).tolist(), "warm": np.bincount(it_w).tolist()},
                       "fallbacks": fb, "warm_vs_plain_state_rel": state_rel, "warm_vs_plain_R_rel": R_rel,
@@ -936,6 +950,7 @@ def main():
     ap.add_argument("--train-n", type=int, default=32)
     ap.add_argument("--train-epochs", type=int, default=30)
     ap.add_argument("--warm-k", type=int, default=6)
+    ap.add_argument("--repeats", type=int, default=5, help="cp_warm: alternating plain / warm runs (median, range)")
     ap.add_argument("--cp-n", type=int, default=48)
     ap.add_argument("--cp-step", type=int, default=10)
     args = ap.parse_args()
