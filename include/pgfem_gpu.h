@@ -179,6 +179,26 @@ int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *ctx, const double *u, const double *u_p
 int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc,
                                  double dt, double *d_R, double *d_K, void *stream);
 int pgfem_gpu_read_status(pgfem_gpu_ctx *ctx, pgfem_gpu_status *st, int clear);
+/* Transient (inertia) element, mid-point rule: what fd_residuals_MP /
+ * stiffmat_fd_MP compute when the material density exceeds 1e-16
+ * (src/fd_residuals.cc:494-500, src/stiffmat_fd.cc:549-565; residual_with_inertia
+ * / stiffness_with_inertia, src/dynamics.cc:183-432, with the CM parts of
+ * src/constitutive_model.cc:1905-2170, 2803-2958).  Host buffers: free-DOF
+ * displacements and prescribed values at t_{n+1}, t_n, t_{n-1}; alpha of the
+ * mid-point rule (0..1), dt_np1 = t_{n+1} - t_n, dt_n = t_n - t_{n-1}, the
+ * density rho.  Output R[ndof] and K[nnz] (K may be NULL):
+ *   R = -dt_np1 (1 - alpha) R(u_{n+alpha}) - dt_n alpha R(u_{n-1+alpha}) - f_i
+ *   K = -M / dt_np1 - alpha (1 - alpha) dt_np1 K(u_{n+alpha})
+ * with R(u), K(u) the quasi-static element integrals, f_i the inertia force of
+ * rho (dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1}) / (dt_np1 dt_n) and M
+ * the consistent mass (rho N_A N_C) on the element's own quadrature rule.  With
+ * |rho| < 1e-16 this is the quasi-static R, K at u_{n+1}, as in the reference.
+ * Hyperelastic contexts without surface loads or macro deformation only
+ * (PGFEM_GPU_EINVAL otherwise).  The status counts both mid-point assemblies. */
+int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *ctx, const double *u_np1, const double *u_n,
+                                    const double *u_nm1, const double *presc_np1, const double *presc_n,
+                                    const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
+                                    double *R, double *K, pgfem_gpu_status *st);
 /* Launch count of the kernels of one assemble_RK call (for accounting). */
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *ctx);
 

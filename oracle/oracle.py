@@ -59,6 +59,8 @@ def lib():
                                              C.c_long, C.c_int]),
             "orc_cp_update_batch": (C.c_long, [_P, C.c_long, _P, C.c_double, _P, _P, _P, _P, _P, _P, _P,
                                                _P, C.c_int, _P]),
+            "orc_assemble_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                                                 C.c_double, C.c_double, _P, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -214,6 +216,19 @@ class Problem:
             err = lib().orc_assemble(C.byref(self.s), C.byref(mat), _p(u), _p(up), dt, _p(sn), _p(snp1), _p(R),
                                      _p(K), e0, e1, nthreads, None)
         return err, R, K, snp1
+
+
+def assemble_transient(P, mat, u_np1, u_n, u_nm1, alpha, dt_np1, dt_n, rho, p_np1=None, p_n=None, p_nm1=None,
+                       want_K=True):
+    """Transient (mid-point rule) R, K of the hyperelastic element: the oracle's
+    orc_assemble_transient.  Returns (err, R, K)."""
+    R = np.zeros(P.ndof)
+    K = np.zeros(P.nnz) if want_K else None
+    arr = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+           for a in (u_np1, u_n, u_nm1, p_np1, p_n, p_nm1)]
+    err = lib().orc_assemble_transient(C.byref(P.s), C.byref(mat), *[_p(a) for a in arr], alpha, dt_np1, dt_n, rho,
+                                       _p(R), _p(K))
+    return err, R, K
 
 
 def newton_step(P, mat, u0, u_presc=None, state_n=None, dt=0.0, iter_max=10, nor_min=1e-10,

@@ -945,6 +945,96 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 
 #include "orc_bform.inc"
 
+// ---------------------------------------------------------------------------
+// Transient (inertia) 1-field element of the hyperelastic model, one rank:
+// residual_with_inertia / stiffness_with_inertia (src/dynamics.cc:183-432),
+// which PGFem3D runs instead of the quasi-static element whenever the
+// material density exceeds 1e-16 (src/stiffmat_fd.cc:549-565,
+// src/fd_residuals.cc:494-500), with the constitutive-model parts
+// residuals_el_constitutive_model_w_inertia_1f (src/constitutive_model.cc:
+// 2803-2958), residuals_el_constitutive_model_n_plus_alpha (:1905-1978) and
+// stiffness_el_constitutive_model_w_inertia_1f (:2024-2170).  For HE the
+// plastic parts are the identity (HE_PARAM::get_pF,
+// src/plasticity_model_none.cc:282-291), and F at t_n, t_{n-1} are those of the
+// given displacements.  mid(a, b) = (1 - alpha) a + alpha b (mid_point_rule,
+// src/utils.cc:3213-3223).
+//   f  = -dt_np1 (1 - alpha) r(F(n+alpha)) - dt_n alpha r(F(n-1+alpha)) - f_i
+//   f_i[a,b] = rho / (dt_np1 dt_n) sum_q N_a du_b w,
+//       du = sum_c N_c (dt_n u_np1 - (dt_np1 + dt_n) u_n + dt_np1 u_nm1)_c
+//   k  = -rho / dt_np1 sum_q N_a N_c w delta_bd - alpha (1 - alpha) dt_np1 k(F(n+alpha))
+// with r, k the quasi-static element integrals at the given F (M = I); the
+// body force of the manufactured-solution tests is zero here.
+// ---------------------------------------------------------------------------
+extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                      const double *u_n, const double *u_nm1, const double *p_np1,
+                                      const double *p_n, const double *p_nm1, double alpha, double dt_np1,
+                                      double dt_n, double rho, double *R, double *K) {
+  if (mat->model != ORC_MODEL_HE) return 1;
+  const int nne = P->nne, nd = nne * 3;
+  int err = 0;
+  Quad qr = quad_rule(nne);
+  for (long e = 0; e < P->ne; e++) {
+    double u2[30], u1[30], u0[30], Xe[30];
+    gather_u(P, e, u_np1, p_np1, u2);
+    gather_u(P, e, u_n, p_n, u1);
+    gather_u(P, e, u_nm1, p_nm1, u0);
+    for (int a = 0; a < nne; a++)
+      for (int i = 0; i < 3; i++) Xe[a * 3 + i] = P->X[(long)P->conn[e * nne + a] * 3 + i];
+    std::vector<double> fe(nd, 0.0), fi(nd, 0.0), lk(K ? nd * nd : 0, 0.0), kI(K ? nd * nd : 0, 0.0),
+        lk1(K ? nd * nd : 0, 0.0);
+    double I3[9];
+    ident(I3);
+    int eerr = 0;
+    for (int ip = 0; ip < qr.nint && !eerr; ip++) {
+      double dN[30], N[10];
+      int terr = 0;
+      const double detJ = PGFem3D_dNdX(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], Xe, dN, &terr);
+      if (terr) { eerr += terr; break; }
+      const double w = detJ * qr.w[ip];
+      shape_N(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], N);
+      double F2[9], F1[9], F0[9], Fnpa[9], Fnma[9];
+      deformation_gradient(nne, u2, dN, F2);
+      deformation_gradient(nne, u1, dN, F1);
+      deformation_gradient(nne, u0, dN, F0);
+      for (int i = 0; i < 9; i++) {
+        Fnpa[i] = (1.0 - alpha) * F1[i] + alpha * F2[i];
+        Fnma[i] = (1.0 - alpha) * F0[i] + alpha * F1[i];
+      }
+      if (det3x3(Fnpa) <= 0.0 || det3x3(Fnma) <= 0.0) { eerr += 1; break; }  // getJacobian
+      double S[9], L[81], st[10];
+      if (orc_cm_update(mat, Fnpa, 0.0, nullptr, nullptr, st, S, K ? L : nullptr, nullptr)) { eerr++; break; }
+      compute_residual_vector(fe.data(), nne, dN, w, Fnpa, I3, I3, S, -dt_np1 * (1.0 - alpha));
+      if (K) {
+        double FrTFr[9];
+        matmulTN(Fnpa, Fnpa, FrTFr);
+        std::vector<double> dMdu(nd * 9, 0.0);
+        compute_stiffness_matrix(lk1.data(), nne, dN, w, Fnpa, I3, I3, I3, FrTFr, I3, S, L, dMdu.data(), 1.0);
+      }
+      double S0[9];
+      if (orc_cm_update(mat, Fnma, 0.0, nullptr, nullptr, st, S0, nullptr, nullptr)) { eerr++; break; }
+      compute_residual_vector(fe.data(), nne, dN, w, Fnma, I3, I3, S0, -dt_n * alpha);
+      // inertia (DISP_resid_w_inertia_el, src/dynamics.cc:78-181; mass of
+      // stiffness_with_inertia, :383-396)
+      double du[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < nne; a++)
+        for (int b = 0; b < 3; b++)
+          du[b] += N[a] * (dt_n * u2[a * 3 + b] - (dt_np1 + dt_n) * u1[a * 3 + b] + dt_np1 * u0[a * 3 + b]);
+      for (int a = 0; a < nne; a++)
+        for (int b = 0; b < 3; b++) fi[a * 3 + b] += rho / dt_np1 / dt_n * N[a] * du[b] * w;
+      if (K)
+        for (int a = 0; a < nne; a++)
+          for (int c = 0; c < nne; c++)
+            for (int b = 0; b < 3; b++) kI[(a * 3 + b) * nd + c * 3 + b] += rho / dt_np1 * N[a] * N[c] * w;
+    }
+    if (eerr) { err += eerr; continue; }
+    for (int i = 0; i < nd; i++) fe[i] -= fi[i];
+    if (K)
+      for (int i = 0; i < nd * nd; i++) lk[i] = -kI[i] - alpha * (1.0 - alpha) * dt_np1 * lk1[i];
+    scatter(P, e, fe.data(), K ? lk.data() : nullptr, R, K);
+  }
+  return err;
+}
+
 extern "C" long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, double dt,
                                     const double *Rcp, const double *state_n, const double *M0,
                                     const double *g_guess, double *state_np1, int *iters, double *dgam,

@@ -136,6 +136,19 @@ long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, dou
                          double *state_np1, int *iters, double *dgam, int *converged, int warm_k,
                          int *fallback);
 
+/* Transient (inertia, mid-point rule) R and K of the hyperelastic 1-field
+ * element (residual_with_inertia / stiffness_with_inertia,
+ * src/dynamics.cc:183-432, with the CM parts of src/constitutive_model.cc:
+ * 1905-2170, 2803-2958), which the reference runs when the density exceeds
+ * 1e-16.  Displacements (free DOFs) and prescribed values at t_{n+1}, t_n and
+ * t_{n-1}; alpha of the mid-point rule, the step sizes dt_{n+1} = t_{n+1} - t_n
+ * and dt_n = t_n - t_{n-1}, the density.  R and K are accumulated (caller
+ * zeroes them); K may be NULL.  HE only (returns 1 otherwise). */
+int orc_assemble_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                           const double *u_n, const double *u_nm1, const double *p_np1,
+                           const double *p_n, const double *p_nm1, double alpha, double dt_np1,
+                           double dt_n, double rho, double *R, double *K);
+
 /* Number of quadrature points per element for nne (1 for 4, 4 for 10). */
 int orc_nint(int nne);
 

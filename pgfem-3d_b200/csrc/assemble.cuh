@@ -39,6 +39,7 @@ constexpr int kVec = 15;  // doubles per (point, node) vector record
 struct ShapeTable {
   double dNxi[4][10][3];  // dN/dxi at the quadrature points
   double w[4];            // quadrature weights
+  double N[4][10];        // shape functions at the quadrature points
 };
 
 struct AsmArgs {

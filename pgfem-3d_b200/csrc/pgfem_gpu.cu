@@ -25,6 +25,7 @@
 #include "cm_integrate.cuh"
 #include "cp_kernels.cuh"
 #include "neumann.cuh"
+#include "transient.cuh"
 #include "peak_probe.cuh"
 #include "pgfem_gpu.h"
 
@@ -93,6 +94,9 @@ struct pgfem_gpu_ctx {
   int *nbc_elem = nullptr, *nbc_feat = nullptr, *nbc_type = nullptr, *nbc_off = nullptr;
   uint8_t *nbc_face = nullptr;
   double *nbc_load = nullptr;
+  // transient calls: u and prescribed values at t_{n+1}, t_n, t_{n-1}, a
+  // mid-point / combination vector of each, the second residual
+  double *tr_buf = nullptr;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -143,6 +147,7 @@ ShapeTable make_shape(int nne) {
     for (int a = 0; a < 4; a++)
       for (int c = 0; c < 3; c++) t.dNxi[0][a][c] = d[a][c];
     t.w[0] = 1.0 / 6.0;
+    for (int a = 0; a < 4; a++) t.N[0][a] = 0.25;  // PGFem3D_N at the centroid
     return t;
   }
   const double A = 0.58541020, B = 0.13819660;
@@ -163,6 +168,12 @@ ShapeTable make_shape(int nne) {
     for (int a = 0; a < 10; a++)
       for (int c = 0; c < 3; c++) t.dNxi[q][a][c] = d[a][c];
     t.w[q] = (1.0 / 4.0) / 6.0;
+    // PGFem3D_N (FEMLIB/src/femlib.cc:164-177)
+    const double l0 = 1.0 - ksi - eta - zet;
+    const double N[10] = {(2.0 * l0 - 1.0) * l0, (2.0 * ksi - 1.0) * ksi, (2.0 * eta - 1.0) * eta,
+                          (2.0 * zet - 1.0) * zet, 4.0 * l0 * ksi, 4.0 * ksi * eta, 4.0 * l0 * eta,
+                          4.0 * l0 * zet, 4.0 * ksi * zet, 4.0 * eta * zet};
+    for (int a = 0; a < 10; a++) t.N[q][a] = N[a];
   }
   return t;
 }
@@ -302,7 +313,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
-                  c->nbc_load};
+                  c->nbc_load, c->tr_buf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->zfork) cudaEventDestroy(c->zfork);
@@ -1488,6 +1499,82 @@ int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *c, const double *u, const double *presc
                           double *R, double *K, pgfem_gpu_status *st) {
   if (!K) return PGFEM_GPU_EINVAL;
   return assemble_host(c, u, presc, R, K, st, dt);
+}
+
+int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
+                                    const double *u_nm1, const double *presc_np1, const double *presc_n,
+                                    const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
+                                    double *R, double *K, pgfem_gpu_status *st) {
+  if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
+    return PGFEM_GPU_EINVAL;
+  if (c->model != PGFEM_MODEL_HE || c->nbc_nface || c->F0 || c->elem_group) return PGFEM_GPU_EINVAL;
+  if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
+    return PGFEM_GPU_EINVAL;
+  // below the reference's density threshold the element is the quasi-static one
+  if (std::fabs(rho) < 1.0e-16) return assemble_host(c, u_np1, presc_np1, R, K, st, dt_np1);
+  int r = ensure_scratch(c, K != nullptr);
+  if (r) return r;
+  const long nd = std::max<long>(1, c->ndof), np = std::max<long>(1, c->npres);
+  if (!c->tr_buf && (r = dalloc(c, &c->tr_buf, (size_t)5 * nd + 4 * np))) return r;
+  double *tu2 = c->tr_buf, *tu1 = tu2 + nd, *tu0 = tu1 + nd, *tua = tu0 + nd, *tR2 = tua + nd;
+  double *tp2 = tR2 + nd, *tp1 = tp2 + np, *tp0 = tp1 + np, *tpa = tp0 + np;
+  cudaStream_t s = c->stream;
+  const size_t bu = sizeof(double) * c->ndof, bp = sizeof(double) * c->npres;
+  CK(cudaMemcpyAsync(tu2, u_np1, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu1, u_n, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu0, u_nm1, bu, cudaMemcpyHostToDevice, s));
+  if (c->npres) {
+    CK(cudaMemcpyAsync(tp2, presc_np1, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp1, presc_n, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp0, presc_nm1, bp, cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), s));
+  const unsigned gu = (unsigned)((nd + 255) / 256), gp = (unsigned)((np + 255) / 256);
+  double *pres = c->npres ? tpa : nullptr;
+  // quasi-static R and K at u_{n+a}
+  k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
+  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
+  CK(cudaGetLastError());
+  if ((r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1))) return r;
+  // quasi-static R at u_{n-1+a}
+  k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, c->ndof);
+  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, c->npres);
+  CK(cudaGetLastError());
+  if ((r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n))) return r;
+  // the mid-point combination
+  k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
+  if (K) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
+                                                                       nullptr, 0.0, c->nnz);
+  // inertia: v = dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1} at the nodes
+  k_comb3<<<gu, 256, 0, s>>>(tua, tu2, dt_n, tu1, -(dt_np1 + dt_n), tu0, dt_np1, c->ndof);
+  if (c->npres) k_comb3<<<gp, 256, 0, s>>>(tpa, tp2, dt_n, tp1, -(dt_np1 + dt_n), tp0, dt_np1, c->npres);
+  {
+    const long n3 = 3 * c->nn;
+    k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, tua, pres, c->unode);
+  }
+  InertiaArgs ia{};
+  ia.X = c->X;
+  ia.conn = c->conn;
+  ia.dof = c->dof;
+  ia.rowptr0 = c->rowptr0;
+  ia.rowlen = c->rowlen;
+  ia.mask = c->mask;
+  ia.pos = c->pos;
+  ia.nn = c->nn;
+  ia.ne = c->ne;
+  ia.vnode = c->unode;
+  ia.cR = rho / (dt_np1 * dt_n);
+  ia.cK = rho / dt_np1;
+  ia.R = c->d_R;
+  ia.K = K ? c->d_K : nullptr;
+  ia.shp = c->shp;
+  const unsigned ge = (unsigned)((c->ne + 127) / 128);
+  if (c->nne == 10) k_inertia<10, 4><<<ge, 128, 0, s>>>(ia);
+  else k_inertia<4, 1><<<ge, 128, 0, s>>>(ia);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(R, c->d_R, bu, cudaMemcpyDeviceToHost, s));
+  if (K) CK(cudaMemcpyAsync(K, c->d_K, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost, s));
+  return read_status(c, st, false);
 }
 
 int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc,

@@ -73,6 +73,8 @@ def lib():
             "pgfem_gpu_set_scatter_mode": (C.c_int, [_P, C.c_int]),
             "pgfem_gpu_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_set_neumann": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_int, _P, _P]),
+            "pgfem_gpu_assemble_RK_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                                                          C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_gpu_set_neumann_loads": (C.c_int, [_P, C.c_int, _P]),
             "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_device_bytes": (C.c_long, [_P]),
@@ -343,6 +345,21 @@ class Context:
         st = Status()
         _check("pgfem_gpu_assemble_RK", lib().pgfem_gpu_assemble_RK(
             self.h, _ptr(u), _ptr(self._presc(u_presc)), dt, _ptr(R), _ptr(K), C.byref(st)))
+        return R, K, st
+
+    def assemble_RK_transient(self, u_np1, u_n, u_nm1, alpha, dt_np1, dt_n, rho, presc=(None, None, None),
+                              want_K=True):
+        """Transient (mid-point rule) R and K of a hyperelastic context
+        (pgfem_gpu_assemble_RK_transient); presc = prescribed values at
+        t_{n+1}, t_n, t_{n-1}.  Returns (R, K or None, Status)."""
+        us = [np.ascontiguousarray(v, dtype=np.float64) for v in (u_np1, u_n, u_nm1)]
+        ps = [self._presc(v) for v in presc]
+        R = np.zeros(self.ndof)
+        K = np.zeros(self.nnz) if want_K else None
+        st = Status()
+        _check("pgfem_gpu_assemble_RK_transient", lib().pgfem_gpu_assemble_RK_transient(
+            self.h, *[_ptr(v) for v in us], *[_ptr(v) for v in ps], alpha, dt_np1, dt_n, rho, _ptr(R), _ptr(K),
+            C.byref(st)))
         return R, K, st
 
     def assemble_RK_device(self, d_u, d_presc, d_R, d_K, stream, dt=0.0):

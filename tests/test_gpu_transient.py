@@ -1,0 +1,89 @@
+"""The transient (inertia, mid-point rule) element on the GPU against the
+oracle, through the C ABI (pgfem_gpu_assemble_RK_transient; the reference's
+residual_with_inertia / stiffness_with_inertia, src/dynamics.cc:183-432, for
+the hyperelastic model): linear tets with a fixed face, quadratic tets with
+prescribed displacements (values at three times), two alphas and unequal
+steps, R and K at the parity tolerance (1e-10); below the density threshold
+the call is the quasi-static assembly at t_{n+1}; J2 contexts, contexts with
+surface loads and bad time parameters are rejected."""
+import numpy as np
+import pytest
+
+import oracle
+import pgfem_gpu as pg
+import workloads as wl
+from test_gpu_parity import check_K, check_R
+
+pytestmark = pytest.mark.gpu
+
+
+def _three_states(p, seed, amp=2e-3):
+    rng = np.random.default_rng(seed)
+    h = 1.0 / p.meta["n"]
+    us = [p.u * (k + 1) / 3 + amp * h * rng.uniform(-1, 1, p.ndof) for k in range(3)]
+    ps = None
+    if p.u_presc is not None:
+        ps = [p.u_presc * (k + 1) / 3 for k in range(3)]
+    return us, ps
+
+
+@pytest.mark.parametrize("maker,alpha", [("p1", 0.5), ("p1", 0.8), ("p2", 0.5), ("p2", 0.3)])
+def test_transient_matches_oracle(gpu, maker, alpha):
+    if maker == "p1":
+        p = wl.he_p1(n=4, seed=2)
+    else:
+        p = wl.tension(n=3, nne=10, model="he", stretch=0.004, predictor=True)
+    us, ps = _three_states(p, seed=7)
+    dt1, dt0 = 0.02, 0.015
+    rho = 2.0e4  # inertia and stiffness terms of one order (E 200e3, h ~ 0.3, dt ~ 0.02)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho,
+                                         presc=(ps[2], ps[1], ps[0]) if ps else (None, None, None))
+    assert st.ok(), st.as_dict()
+    P, mat = oracle.from_workload(p)
+    args = dict(p_np1=ps[2], p_n=ps[1], p_nm1=ps[0]) if ps else {}
+    err, Ro, Ko = oracle.assemble_transient(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, **args)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    # both the inertia and the quasi-static parts carry weight
+    _, R0, K0 = oracle.assemble_transient(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, 0.0, **args)
+    assert np.linalg.norm(Ro - R0) > 0.05 * np.linalg.norm(Ro)
+    assert np.linalg.norm(R0) > 0.05 * np.linalg.norm(Ro)
+    # residual only
+    R1, K1, st1 = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho,
+                                            presc=(ps[2], ps[1], ps[0]) if ps else (None, None, None),
+                                            want_K=False)
+    assert K1 is None and st1.ok()
+    check_R(R1, Ro)
+    ctx.close()
+
+
+def test_below_density_threshold_is_quasi_static(gpu):
+    p = wl.he_p1(n=3, seed=4)
+    us, _ = _three_states(p, seed=2)
+    ctx = p.context()
+    R, K, st = ctx.assemble_RK_transient(us[2], us[1], us[0], 0.5, 0.1, 0.1, 1e-17)
+    Rs, Ks, _ = ctx.assemble_RK(us[2])
+    check_R(R, Rs, 1e-13)  # two atomic-scatter assemblies: the summation order differs
+    check_K(K, Ks, p.Ap, 1e-13)
+    ctx.close()
+
+
+def test_transient_rejections(gpu):
+    p = wl.he_p1(n=2, seed=1)
+    us, _ = _three_states(p, seed=1)
+    ctx = p.context()
+    for a, d1, d0 in [(-0.1, 0.1, 0.1), (1.5, 0.1, 0.1), (0.5, 0.0, 0.1), (0.5, 0.1, -1.0)]:
+        with pytest.raises(pg.PgfemError):
+            ctx.assemble_RK_transient(us[2], us[1], us[0], a, d1, d0, 1.0)
+    e, f = wl.box_faces(p.X, p.conn, 0, 1.0)
+    ctx.set_neumann(e, f, np.zeros(len(e), dtype=np.int32), [1], [[1.0, 0, 0]])
+    with pytest.raises(pg.PgfemError):
+        ctx.assemble_RK_transient(us[2], us[1], us[0], 0.5, 0.1, 0.1, 1.0)
+    ctx.close()
+    q = wl.j2_p2(n=2, seed=1)
+    cq = q.context()
+    with pytest.raises(pg.PgfemError):
+        cq.assemble_RK_transient(q.u, q.u, q.u, 0.5, 0.1, 0.1, 1.0)
+    cq.close()
