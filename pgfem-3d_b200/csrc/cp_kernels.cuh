@@ -450,77 +450,347 @@ __global__ void __launch_bounds__(32 * kCpWarps) k_cp_update(const CpArgs A) {
 
 inline size_t cp_update_smem() { return sizeof(double) * kCpWarps * (100 + 10) * 32; }
 
-// Consistent tangent of the converged local update, one lane per point:
-// dM/dF = -J^-1 dR/dF with d tau_a / dF = 2 F Z_a,
-// Z_a = pF_n^-1 M Ysym_a M^T pF_n^-T (the role of compute_dMdu,
-// src/plasticity_model.cc:578-881).  Reads the converged M and g from the
-// point record, writes dM/dF (81) into it; points that did not converge get a
-// zero tangent.  Every point does the same work, so no work stealing.
-__global__ void __launch_bounds__(32 * kCpTanWarps) k_cp_tangent(const CpArgs A) {
-  extern __shared__ double smem_ct[];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double *Jm = smem_ct + warp * (100 + 90) * 32 + lane;  // 10x10 Jacobian
-  double *Bm = Jm + 100 * 32;                            // 10x9 right-hand sides
-  const long S = A.nqp;
-  for (long qp = (long)blockIdx.x * blockDim.x + threadIdx.x; qp < S; qp += (long)gridDim.x * blockDim.x) {
-    bool ok = A.conv[qp] != 0;
-    if (ok) {
-      CpPoint pt;
-      double Fq[9], pFni[9], pFn[9], M[9];
-      const long e = qp / A.nqp_e;
+// ---- consistent tangent, four lanes per point -------------------------------
+
+// Sample-frame slip direction and normal of system a (unit vectors).
+__device__ __forceinline__ void slip_sn(const double *R, int a, double *sv, double *nv) {
+  const double is2 = 0.70710678118654752440, is3 = 0.57735026918962576451;
 #pragma unroll
-      for (int i = 0; i < 9; i++) {
-        Fq[i] = A.F[i * S + qp];
-        pt.R[i] = A.Rcp[i * A.ne + e];
-        pFn[i] = A.state_n[i * S + qp];
-        M[i] = A.out[i * S + qp];
-      }
-      const double g = A.out[90 * S + qp];
-      pt.g_n = A.state_n[9 * S + qp];
-      pt.dt = A.dt;
-      inv3(pFn, pFni);
-      double Fe[9];
-      mm3(Fq, pFni, Fe);
-      mm3tn(Fe, Fe, pt.Cep);
-      double Res[10], gd[kSlip], dgd[kSlip], gdot = 0;
-      NeoHooke h;
-      ok = cp_residual(A.mat, pt, M, g, Res, h, gd, dgd, gdot);
-      if (ok) {
-        cp_jacobian(A.mat, pt, M, g, h, gd, dgd, gdot, Jm);
-        for (int i = 0; i < 90; i++) Bm[i * 32] = 0.0;
-        double Ce[9], t[9], W[9];
-        mm3(pt.Cep, M, t);
-        mm3tn(M, t, Ce);
-        mm3(pFni, M, W);
-        const double dRg = cp_hardening(A.mat, gdot, g, A.dt).dRg;
-        for (int a = 0; a < kSlip; a++) {
-          double P[9], Y[9], t1[9], Z[9], dtF[9];
-          schmid(pt.R, a, P);
-          ysym(A.mat, h, Ce, P, Y);
-          mm3(W, Y, t1);
-          mm3nt(t1, W, Z);  // Z = pFn^-1 M Ysym M^T pFn^-T
-          mm3(Fq, Z, dtF);
-          const double sg = gd[a] < 0 ? -1.0 : 1.0;
-          const double cf = A.dt * dgd[a];
-          for (int i = 0; i < 9; i++)
-            for (int kl = 0; kl < 9; kl++) lm(Bm, 9, i, kl) -= cf * P[i] * 2.0 * dtF[kl];
-          for (int kl = 0; kl < 9; kl++) lm(Bm, 9, 9, kl) -= dRg * sg * dgd[a] * 2.0 * dtF[kl];
-        }
-        ok = lane_solve(Jm, 10, Bm, 9);
-        if (ok) {
-          for (int r = 0; r < 9; r++)
-            for (int q = 0; q < 9; q++) A.out[(9 + r * 9 + q) * S + qp] = lm(Bm, 9, r, q);
-        } else {
-          atomicAdd(&A.status[3], 1ull);
-        }
-      }
-    }
-    if (!ok)
-      for (int r = 0; r < 81; r++) A.out[(9 + r) * S + qp] = 0.0;
+  for (int i = 0; i < 3; i++) {
+    sv[i] = (R[i * 3] * c_slip_s[a][0] + R[i * 3 + 1] * c_slip_s[a][1] + R[i * 3 + 2] * c_slip_s[a][2]) * is2;
+    nv[i] = (R[i * 3] * c_slip_n[a][0] + R[i * 3 + 1] * c_slip_n[a][1] + R[i * 3 + 2] * c_slip_n[a][2]) * is3;
   }
 }
 
-inline size_t cp_tangent_smem() { return sizeof(double) * kCpTanWarps * (100 + 90) * 32; }
+// Sum of v over the four lanes of a point (every lane gets the same bits).
+__device__ __forceinline__ double quad_sum(unsigned qm, double v) {
+  v += __shfl_xor_sync(qm, v, 1);
+  v += __shfl_xor_sync(qm, v, 2);
+  return v;
+}
+
+// symmetric 3x3 in Voigt order (xx yy zz yz xz xy): y = A x
+__device__ __forceinline__ void symv6(const double *A, const double *x, double *y) {
+  y[0] = A[0] * x[0] + A[5] * x[1] + A[4] * x[2];
+  y[1] = A[5] * x[0] + A[1] * x[1] + A[3] * x[2];
+  y[2] = A[4] * x[0] + A[3] * x[1] + A[2] * x[2];
+}
+
+// Ysym of slip system (s, n) for the neo-Hookean + U_Common law from the
+// shared per-point state (Ce, Ce^-1 in Voigt form; a = mu detC^-1/3, pv =
+// kappa J (J - 1), trC, J), by the rank-one Schmid structure P = s n^T:
+// sym(P S) = sym(s w^T) with w = S n, and dS[X] for X = sym(c n^T), c = Ce s
+// (nh_dS with Ci:X = n . Ci c and Ci X Ci = sym(p q^T), p = Ci c, q = Ci n).
+// The same tensor as ysym; tau = s . (Ce S) n is returned too.
+__device__ __forceinline__ double ysym_sn(const Mat &mat, const double *C6, const double *Ci, double a, double pv,
+                                          double trC, double J, const double *sv, const double *nv, double *Y) {
+  double c[3], p[3], q[3], w[3];
+  symv6(C6, sv, c);
+  symv6(Ci, c, p);
+  symv6(Ci, nv, q);
+#pragma unroll
+  for (int i = 0; i < 3; i++) w[i] = a * (nv[i] - trC / 3.0 * q[i]) + pv * q[i];
+  const double sn = sv[0] * nv[0] + sv[1] * nv[1] + sv[2] * nv[2];
+  const double trX = c[0] * nv[0] + c[1] * nv[1] + c[2] * nv[2];
+  const double CiX = nv[0] * p[0] + nv[1] * p[1] + nv[2] * p[2];
+  const double dpv = mat.kappa * (2.0 * J - 1.0) * 0.5 * J * CiX;
+  const int vi[6] = {0, 1, 2, 1, 0, 0}, vj[6] = {0, 1, 2, 2, 2, 1};
+#pragma unroll
+  for (int v = 0; v < 6; v++) {
+    const int i = vi[v], j = vj[v];
+    const double d = i == j ? 1.0 : 0.0;
+    const double cxc = 0.5 * (p[i] * q[j] + q[i] * p[j]);
+    const double y = 0.5 * (sv[i] * w[j] + w[i] * sv[j]) +
+                     a * (-CiX / 3.0 * (d - trC / 3.0 * Ci[v]) - trX / 3.0 * Ci[v] + trC / 3.0 * cxc) +
+                     dpv * Ci[v] - pv * cxc;
+    Y[i * 3 + j] = y;
+    Y[j * 3 + i] = y;
+  }
+  return a * (trX - trC / 3.0 * sn) + pv * sn;  // tau
+}
+
+// Shared region of one point of k_cp_tangent (doubles): [0, 100) the
+// Jacobian rows, [100, 190) the right-hand sides (10 x 9, row-major), [190,
+// 234) exchange records of four slip systems, then the crystal rotation, W =
+// pF_n^-1 M, F, Ce (Voigt), Ce^-1 (Voigt), Ce' M and five scalars.  The
+// stride is 2 mod 16 doubles (the eight points of a warp on distinct banks).
+constexpr int kCtQS = 290;
+constexpr int kCtJ = 0, kCtB = 100, kCtX = 190, kCtR = 234, kCtW = 243, kCtF = 252, kCtCe = 261, kCtCi = 267,
+              kCtCM = 273, kCtSc = 282;
+constexpr int kCtPts = 8 * kCpTanWarps;  // points per CTA
+
+// Consistent tangent of the converged local update, four lanes per point:
+// dM/dF = -J^-1 dR/dF with d tau_a / dF = 2 F Z_a, Z_a = pF_n^-1 M Ysym_a M^T
+// pF_n^-T (the role of compute_dMdu, src/plasticity_model.cc:578-881).  The
+// Jacobian rows and the nine right-hand sides are built in rounds of four
+// slip-system records (each lane forms the record of one system per round,
+// every lane adds the four records to its rows sub, sub + 4, sub + 8), the
+// pivoted elimination splits rows over the lanes, the back substitution the
+// nine columns.  Points that did not converge, or whose Jacobian is singular
+// (counted in status[3]), get a zero tangent.  Every point does the same work:
+// a uniform grid over the points, four lanes each.
+__global__ void __launch_bounds__(32 * kCpTanWarps, 6) k_cp_tangent(const CpArgs A) {
+  extern __shared__ double smem_ct[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int sub = lane & 3, qd = lane >> 2;
+  const unsigned qm = 0xFu << (lane & ~3);
+  double *reg = smem_ct + (warp * 8 + qd) * kCtQS;
+  const long S = A.nqp;
+  const double dt = A.dt, im = 1.0 / A.mat.m;
+  const long nquads = (long)gridDim.x * kCtPts;
+  for (long qp = (long)blockIdx.x * kCtPts + warp * 8 + qd; qp < S; qp += nquads) {
+    bool ok = A.conv[qp] != 0;
+    double g = 0.0, gsum = 0.0;
+    if (ok) {
+      // point set-up (every lane computes, lane 0 stores as it goes): F, W =
+      // pF_n^-1 M, Ce' M, Ce, its inverse and the stress scalars
+      __syncwarp(qm);  // the previous point's reads of the region are done
+      const long e = qp / A.nqp_e;
+      double M[9], pFni[9], C6[6];
+#pragma unroll
+      for (int i = 0; i < 9; i++) M[i] = A.out[i * S + qp];
+      g = A.out[90 * S + qp];
+      {
+        double pFn[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) pFn[i] = A.state_n[i * S + qp];
+        inv3(pFn, pFni);
+      }
+      {
+        double W[9];
+        mm3(pFni, M, W);
+        if (sub == 0)
+#pragma unroll
+          for (int i = 0; i < 9; i++) reg[kCtW + i] = W[i];
+      }
+      {
+        double Fq[9], Fe[9], Cep[9], CepM[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) Fq[i] = A.F[i * S + qp];
+        if (sub == 0)
+#pragma unroll
+          for (int i = 0; i < 9; i++) reg[kCtF + i] = Fq[i];
+        mm3(Fq, pFni, Fe);
+        mm3tn(Fe, Fe, Cep);
+        mm3(Cep, M, CepM);
+        if (sub == 0)
+#pragma unroll
+          for (int i = 0; i < 9; i++) reg[kCtCM + i] = CepM[i];
+        double Ce[9];
+        mm3tn(M, CepM, Ce);
+        C6[0] = Ce[0], C6[1] = Ce[4], C6[2] = Ce[8], C6[3] = Ce[5], C6[4] = Ce[2], C6[5] = Ce[1];
+      }
+      const double detC = C6[0] * (C6[1] * C6[2] - C6[3] * C6[3]) - C6[5] * (C6[5] * C6[2] - C6[3] * C6[4]) +
+                          C6[4] * (C6[5] * C6[3] - C6[1] * C6[4]);
+      ok = detC > 0.0 && g > 0.0;
+      if (ok) {
+        const double J = sqrt(detC), a = A.mat.mu / cbrt(detC), pv = A.mat.kappa * J * (J - 1.0);
+        const double trC = C6[0] + C6[1] + C6[2], id = 1.0 / detC;
+        if (sub == 0) {
+          reg[kCtCi + 0] = (C6[1] * C6[2] - C6[3] * C6[3]) * id;
+          reg[kCtCi + 1] = (C6[0] * C6[2] - C6[4] * C6[4]) * id;
+          reg[kCtCi + 2] = (C6[0] * C6[1] - C6[5] * C6[5]) * id;
+          reg[kCtCi + 3] = (C6[4] * C6[5] - C6[0] * C6[3]) * id;
+          reg[kCtCi + 4] = (C6[5] * C6[3] - C6[1] * C6[4]) * id;
+          reg[kCtCi + 5] = (C6[3] * C6[4] - C6[2] * C6[5]) * id;
+#pragma unroll
+          for (int i = 0; i < 6; i++) reg[kCtCe + i] = C6[i];
+          reg[kCtSc] = a;
+          reg[kCtSc + 1] = pv;
+          reg[kCtSc + 2] = trC;
+          reg[kCtSc + 3] = J;
+#pragma unroll
+          for (int i = 0; i < 9; i++) reg[kCtR + i] = A.Rcp[i * A.ne + e];
+        }
+        __syncwarp(qm);
+        // the own systems' slip rates: the hardening slope needs their sum
+#pragma unroll 1
+        for (int k = 0; k < 3; k++) {
+          double sv[3], nv[3], c[3];
+          slip_sn(reg + kCtR, 4 * k + sub, sv, nv);
+          symv6(C6, sv, c);
+          const double sn = sv[0] * nv[0] + sv[1] * nv[1] + sv[2] * nv[2];
+          const double tau = a * ((c[0] * nv[0] + c[1] * nv[1] + c[2] * nv[2]) - trC / 3.0 * sn) + pv * sn;
+          gsum += fabs(A.mat.gdot0 * (tau / g) * flow_pow(fabs(tau / g), im - 1.0));
+        }
+      }
+    }
+    ok = __shfl_sync(qm, ok, lane & ~3) != 0;  // the quad agrees (identical inputs)
+    if (ok) {
+      gsum = quad_sum(qm, gsum);
+      const CpHard hd = cp_hardening(A.mat, gsum, g, dt);
+      // own rows: J identity (row 9 zero), B zero
+#pragma unroll
+      for (int r = 0; r < 3; r++) {
+        const int i = sub + 4 * r;
+        if (i < 10) {
+#pragma unroll
+          for (int j = 0; j < 10; j++) reg[kCtJ + i * 10 + j] = (i == j && i < 9) ? 1.0 : 0.0;
+#pragma unroll
+          for (int j = 0; j < 9; j++) reg[kCtB + i * 9 + j] = 0.0;
+        }
+      }
+      __syncwarp(qm);
+      const double a = reg[kCtSc], pv = reg[kCtSc + 1], trC = reg[kCtSc + 2], J = reg[kCtSc + 3];
+      const double *R = reg + kCtR;
+      // pass 0: Jacobian rows (records dtau, gd, dgd); pass 1: right-hand
+      // sides (records 2 dtF, cf, dRg sg dgd)
+#pragma unroll 1
+      for (int pass = 0; pass < 2; pass++) {
+#pragma unroll 1
+        for (int k = 0; k < 3; k++) {
+          {
+            const int sa = 4 * k + sub;
+            double sv[3], nv[3], Y[9], out9[9];
+            slip_sn(R, sa, sv, nv);
+            const double tau = ysym_sn(A.mat, reg + kCtCe, reg + kCtCi, a, pv, trC, J, sv, nv, Y);
+            const double pw = flow_pow(fabs(tau / g), im - 1.0);
+            const double gd = A.mat.gdot0 * (tau / g) * pw, dgd = A.mat.gdot0 * im / g * pw;
+            double *x = reg + kCtX + sub * 11;
+            if (pass == 0) {
+              mm3(reg + kCtCM, Y, out9);  // dtau = 2 Ce'M Ysym
+#pragma unroll
+              for (int i = 0; i < 9; i++) x[i] = 2.0 * out9[i];
+              x[9] = gd;
+              x[10] = dgd;
+            } else {
+              double t1[9], Z[9];
+              mm3(reg + kCtW, Y, t1);
+              mm3nt(t1, reg + kCtW, Z);  // Z = pF_n^-1 M Ysym M^T pF_n^-T
+              mm3(reg + kCtF, Z, out9);   // dtF
+              const double sg = gd < 0 ? -1.0 : 1.0;
+#pragma unroll
+              for (int i = 0; i < 9; i++) x[i] = 2.0 * out9[i];
+              x[9] = dt * dgd;            // cf
+              x[10] = hd.dRg * sg * dgd;  // row 9 weight
+            }
+          }
+          __syncwarp(qm);
+          // the round's four systems into the own rows: the Schmid entries of
+          // the own rows first, then one row at a time
+          double Pr[4][3];
+#pragma unroll 1
+          for (int o = 0; o < 4; o++) {
+            double sv[3], nv[3];
+            slip_sn(R, 4 * k + o, sv, nv);
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+              const int i = sub + 4 * r, ii = i / 3, jj = i - 3 * ii;  // run-time row: select, do not index
+              const double Pv = (ii == 0 ? sv[0] : (ii == 1 ? sv[1] : sv[2])) *
+                                (jj == 0 ? nv[0] : (jj == 1 ? nv[1] : nv[2]));
+#pragma unroll
+              for (int oo = 0; oo < 4; oo++)
+                if (oo == o) Pr[oo][r] = Pv;
+            }
+          }
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            const int i = sub + 4 * r;
+            if (i >= 10) continue;
+#pragma unroll 1
+            for (int o = 0; o < 4; o++) {
+              const double *x = reg + kCtX + o * 11;
+              const double Pi = o == 0 ? Pr[0][r] : (o == 1 ? Pr[1][r] : (o == 2 ? Pr[2][r] : Pr[3][r]));
+              if (pass == 0) {
+                double *row = reg + kCtJ + i * 10;
+                const double gd = x[9], dgd = x[10];
+                if (i == 9) {
+                  const double sgd = (gd < 0 ? -1.0 : 1.0) * dgd;
+#pragma unroll
+                  for (int j = 0; j < 9; j++) row[j] += sgd * x[j];
+                } else {
+                  const double cf = dt * dgd, cg = dt * (-gd / (A.mat.m * g));
+#pragma unroll
+                  for (int j = 0; j < 9; j++) row[j] += cf * Pi * x[j];
+                  row[9] += cg * Pi;
+                }
+              } else {
+                double *row = reg + kCtB + i * 9;
+                const double wgt = i == 9 ? x[10] : x[9] * Pi;
+#pragma unroll
+                for (int j = 0; j < 9; j++) row[j] -= wgt * x[j];
+              }
+            }
+          }
+          __syncwarp(qm);  // the records are read before the next round overwrites them
+        }
+        if (pass == 0 && sub == 1) {  // row 9 of the Jacobian
+          const double c = dt * A.mat.G0 / (hd.gs - A.mat.g0);
+          double *row = reg + kCtJ + 90;
+#pragma unroll
+          for (int j = 0; j < 9; j++) row[j] = hd.dRg * row[j];
+          row[9] = 1.0 + c * gsum - hd.dRg * gsum / (A.mat.m * g);
+        }
+        __syncwarp(qm);
+      }
+      // pivoted elimination: rows i = sub (mod 4), swaps over the 19 columns
+      double *Am = reg + kCtJ, *Bm = reg + kCtB;
+#pragma unroll 1
+      for (int k = 0; k < 10 && ok; k++) {
+        double best = -1.0;
+        int p = k;
+        for (int i = k + ((sub - k) & 3); i < 10; i += 4) {
+          const double v = fabs(Am[i * 10 + k]);
+          if (v > best) {
+            best = v;
+            p = i;
+          }
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+          const double ob = __shfl_xor_sync(qm, best, o);
+          const int op = __shfl_xor_sync(qm, p, o);
+          if (ob > best || (ob == best && op < p)) {
+            best = ob;
+            p = op;
+          }
+        }
+        if (!(best > 0.0)) {
+          ok = false;
+          break;
+        }
+        if (p != k) {
+          for (int j = sub; j < 19; j += 4) {
+            double *x = j < 10 ? Am + k * 10 + j : Bm + k * 9 + (j - 10);
+            double *y = j < 10 ? Am + p * 10 + j : Bm + p * 9 + (j - 10);
+            const double t = *x;
+            *x = *y;
+            *y = t;
+          }
+          __syncwarp(qm);
+        }
+        const double inv = 1.0 / Am[k * 10 + k];
+        for (int i = k + 1 + ((sub - k - 1) & 3); i < 10; i += 4) {
+          const double f = Am[i * 10 + k] * inv;
+          if (f == 0.0) continue;
+          for (int j = k; j < 10; j++) Am[i * 10 + j] -= f * Am[k * 10 + j];
+          for (int j = 0; j < 9; j++) Bm[i * 9 + j] -= f * Bm[k * 9 + j];
+        }
+        __syncwarp(qm);
+      }
+      if (ok) {
+        // back substitution, columns c = sub (mod 4), and the output
+        for (int c = sub; c < 9; c += 4) {
+          for (int k = 9; k >= 0; k--) {
+            const double inv = 1.0 / Am[k * 10 + k];
+            double v = Bm[k * 9 + c];
+            for (int i = k + 1; i < 10; i++) v -= Am[k * 10 + i] * Bm[i * 9 + c];
+            Bm[k * 9 + c] = v * inv;
+          }
+#pragma unroll
+          for (int r = 0; r < 9; r++) A.out[(9 + r * 9 + c) * S + qp] = Bm[r * 9 + c];
+        }
+      } else if (sub == 0) {
+        atomicAdd(&A.status[3], 1ull);
+      }
+    }
+    if (!ok)
+      for (int r = sub; r < 81; r += 4) A.out[(9 + r) * S + qp] = 0.0;
+    __syncwarp(qm);
+  }
+}
+
+inline size_t cp_tangent_smem() { return sizeof(double) * kCtPts * kCtQS; }
 
 }  // namespace pgb
 

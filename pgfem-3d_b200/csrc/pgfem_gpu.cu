@@ -612,9 +612,11 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
       CK(cudaFuncSetAttribute(k_cp_tangent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
       tattr = true;
     }
-    const long tblk = 32 * kCpTanWarps;
-    const long tgrid = std::max<long>(1, std::min<long>((c->nqp + tblk - 1) / tblk, (long)g_num_sms * 16));
-    k_cp_tangent<<<(unsigned)tgrid, (unsigned)tblk, tsm, s>>>(a);
+    int tper = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&tper, k_cp_tangent, 32 * kCpTanWarps, tsm));
+    if (tper < 1) tper = 1;
+    const long tgrid = std::max<long>(1, std::min<long>((c->nqp + kCtPts - 1) / kCtPts, (long)g_num_sms * tper));
+    k_cp_tangent<<<(unsigned)tgrid, 32 * kCpTanWarps, tsm, s>>>(a);
     CK(cudaGetLastError());
   }
   if (e0) {
