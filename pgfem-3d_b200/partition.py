@@ -185,9 +185,13 @@ class DistributedAssembly:
     """
 
     def __init__(self, X, conn, ids, ndof, Ap, Ai, backend, group=None):
+        import torch
         import torch.distributed as dist
         self.dist = dist
         self.group = group
+        # NCCL moves device buffers, gloo host buffers
+        self.dev = (torch.device("cuda", torch.cuda.current_device())
+                    if dist.get_backend(group) == "nccl" else torch.device("cpu"))
         nparts = dist.get_world_size(group)
         rank = dist.get_rank(group)
         self.plan = RankPlan(X, conn, ids, ndof, Ap, Ai, nparts, rank)
@@ -231,10 +235,10 @@ class DistributedAssembly:
                 continue
             want = allreq[q].get(rank)
             if want is not None and want.size:
-                t = torch.from_numpy(np.ascontiguousarray(u_owned[want - p.row0]))
+                t = torch.from_numpy(np.ascontiguousarray(u_owned[want - p.row0])).to(self.dev)
                 ops.append(dist.P2POp(dist.isend, t, q, group=self.group))
             if q in need:
-                bufs[q] = torch.zeros(sum(len(m) for _, m, _ in need[q]), dtype=torch.float64)
+                bufs[q] = torch.zeros(sum(len(m) for _, m, _ in need[q]), dtype=torch.float64, device=self.dev)
                 ops.append(dist.P2POp(dist.irecv, bufs[q], q, group=self.group))
         if ops:
             for w in dist.batch_isend_irecv(ops):
@@ -246,7 +250,7 @@ class DistributedAssembly:
             ul[mine] = u_owned[pc.gdof[mine] - p.row0]
             out.append(ul)
         for q, lst in need.items():
-            v = bufs[q].numpy()
+            v = bufs[q].cpu().numpy()
             o = 0
             for ip, m, _ in lst:
                 out[ip][m] = v[o:o + len(m)]
@@ -267,7 +271,7 @@ class DistributedAssembly:
         ops, keep = [], []
         recvbufs = {}
         for q, (rpos, kpos) in self.recv.items():
-            recvbufs[q] = torch.zeros(len(rpos) + len(kpos), dtype=torch.float64)
+            recvbufs[q] = torch.zeros(len(rpos) + len(kpos), dtype=torch.float64, device=self.dev)
             ops.append(dist.P2POp(dist.irecv, recvbufs[q], q, group=self.group))
         works = []
         for ip, pc in enumerate(p.pieces):
@@ -276,7 +280,8 @@ class DistributedAssembly:
             status = np.maximum(status, np.asarray(st, dtype=np.int64))
             if ip == 0:  # after the first piece (the boundary piece when there is one)
                 for q, (rq, kq) in p.send.items():
-                    b = torch.from_numpy(np.ascontiguousarray(np.concatenate([results[0][0][rq], results[0][1][kq]])))
+                    b = torch.from_numpy(np.ascontiguousarray(np.concatenate([results[0][0][rq],
+                                                                              results[0][1][kq]]))).to(self.dev)
                     keep.append(b)
                     ops.append(dist.P2POp(dist.isend, b, q, group=self.group))
                 if ops:
@@ -288,9 +293,40 @@ class DistributedAssembly:
         for w in works:
             w.wait()
         for q, (rpos, kpos) in self.recv.items():
-            v = recvbufs[q].numpy()
+            v = recvbufs[q].cpu().numpy()
             np.add.at(R, rpos, v[:len(rpos)])
             np.add.at(K, kpos, v[len(rpos):])
-        st = torch.from_numpy(status.copy())
+        st = torch.from_numpy(status.copy()).to(self.dev)
         dist.all_reduce(st, op=dist.ReduceOp.MAX, group=self.group)
-        return R, K, st.numpy()
+        return R, K, st.cpu().numpy()
+
+
+class DeviceBackend:
+    """Piece assembly on this library's device contexts: one context per
+    piece (created at its first call), the piece's element state taken from the
+    global per-point state array, R and K of the piece from
+    pgfem_gpu_assemble_RK."""
+
+    def __init__(self, mat, state=None, nint=1, npres=0, dt=0.0, R_cp=None):
+        self.mat, self.state, self.nint, self.npres, self.dt, self.R_cp = mat, state, nint, npres, dt, R_cp
+        self.ctx = {}
+
+    def context(self, pc):
+        c = self.ctx.get(id(pc))
+        if c is None:
+            Rcp = None if self.R_cp is None else self.R_cp[pc.elems]
+            c = pg.Context(pc.X, pc.conn, pc.ids, pc.ndof, pc.Ap, pc.Ai, self.mat, npres=self.npres, R_cp=Rcp)
+            if self.state is not None:
+                rows = (pc.elems[:, None] * self.nint + np.arange(self.nint)).ravel()
+                c.set_state(self.state[rows])
+            self.ctx[id(pc)] = c
+        return c
+
+    def __call__(self, pc, u_local, u_presc):
+        R, K, st = self.context(pc).assemble_RK(u_local, u_presc, dt=self.dt)
+        return R, K, np.array([st.inverted, st.nonconverged, st.bad_diagonal, st.other], dtype=np.int64)
+
+    def close(self):
+        for c in self.ctx.values():
+            c.close()
+        self.ctx = {}
