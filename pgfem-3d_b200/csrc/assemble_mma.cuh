@@ -44,11 +44,18 @@
 #include <cstdint>
 
 #include "assemble.cuh"
+#include "assemble_p1.cuh"  // bounded mbarrier waits
 
 namespace pgb {
 
 constexpr int kQRec = kRec;  // point record of the linear-tet path: G 9, w, tau 6, s 6, n 6, dev(n^2) 6, a1 a2 a4 a5
 constexpr int kYRec = 40;  // point record of the tensor-core path: G 9, T' 6, U' 6, W' 6, s'' 6, n 6, h
+constexpr int kMPtsT = 16;  // points per record tile (the assembly tile: 4 elements x 4 points)
+
+// index of field c of record slot qs in the tiled layout of the tensor-core path
+__host__ __device__ __forceinline__ long yrec_idx(long qs, int c) {
+  return ((qs >> 4) * kYRec + c) * kMPtsT + (qs & (kMPtsT - 1));
+}
 
 struct QpArgs {
   const double *X;      // 3*nn
@@ -60,7 +67,8 @@ struct QpArgs {
   const double *F0_tab;   // group -> macro deformation (9)
   const double *state_n;
   double *state_np1;
-  double *qrec;         // kQRec*nqp or kYRec*nqp (SoA)
+  double *qrec;         // kQRec*nqp (SoA) or, for 10-node elements, kYRec doubles per point in
+                        // tiles of kMPtsT points ([tile][field][point], padded to whole tiles)
   unsigned long long *status;
   // processing order: record slot e' holds element perm[e'] (nullptr: e' = e);
   // the state stays in element order
@@ -117,7 +125,7 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   if (!ok) {
     atomicAdd(&A.status[0], 1ull);
 #pragma unroll
-    for (int c = 0; c < NR; c++) rec[c * S + qs] = 0.0;
+    for (int c = 0; c < NR; c++) rec[YREC ? yrec_idx(qs, c) : c * S + qs] = 0.0;
     return;
   }
   double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
@@ -138,7 +146,7 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      rec[(i * 3 + j) * S + qs] =
+      rec[YREC ? yrec_idx(qs, i * 3 + j) : (i * 3 + j) * S + qs] =
           dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] + dXi[i * 3 + 2] * Fi[2 * 3 + j];
   const double w = detJ * A.shp.w[q];
   if (YREC) {
@@ -146,13 +154,13 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
 #pragma unroll
     for (int c = 0; c < 6; c++) {
       const double d = c < 3 ? 1.0 : 0.0;
-      rec[(9 + c) * S + qs] = h * d + w * t.tau[c];
-      rec[(15 + c) * S + qs] = w * t.a2 * d - c23 * t.s[c];
-      rec[(21 + c) * S + qs] = w * (t.a4 * t.n[c] + t.a5 * t.D[c]);
-      rec[(27 + c) * S + qs] = -c23 * t.s[c];
-      rec[(33 + c) * S + qs] = t.n[c];
+      rec[yrec_idx(qs, 9 + c)] = h * d + w * t.tau[c];
+      rec[yrec_idx(qs, 15 + c)] = w * t.a2 * d - c23 * t.s[c];
+      rec[yrec_idx(qs, 21 + c)] = w * (t.a4 * t.n[c] + t.a5 * t.D[c]);
+      rec[yrec_idx(qs, 27 + c)] = -c23 * t.s[c];
+      rec[yrec_idx(qs, 33 + c)] = t.n[c];
     }
-    rec[39 * S + qs] = h;
+    rec[yrec_idx(qs, 39)] = h;
   } else {
     rec[9 * S + qs] = w;
 #pragma unroll
@@ -194,7 +202,25 @@ constexpr int kEBPos = 60, kEBMask = 110;
 
 inline size_t p2m_smem_bytes() {
   return sizeof(double) * ((size_t)kMTE * kMY + (size_t)kMTE * kMP + (size_t)kYRec * kMPts) +
-         sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW;
+         sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW + 2 * sizeof(uint64_t);
+}
+
+// bytes of one tile's copies: its point records and its elements' scatter blocks
+constexpr unsigned kMTileBytes = (unsigned)(sizeof(double) * kYRec * kMPtsT + sizeof(int) * kMTE * kEBW);
+
+// one-dimensional bulk copy global -> shared through the tensor memory
+// accelerator, completing on an mbarrier (16-byte aligned, size a multiple of 16)
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          (unsigned)__cvta_generic_to_shared(dst)),
+      "l"(src), "r"(bytes), "r"((unsigned)__cvta_generic_to_shared(bar))
+      : "memory");
+}
+__device__ __forceinline__ void mb_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(bar)),
+               "r"(bytes)
+               : "memory");
 }
 
 // Builds the scatter blocks of all 10-node elements from the node arrays and
@@ -328,6 +354,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
   double *sRec = sP + TE * kMP;                              // [kYRec][kMPts]
   int *sCol = reinterpret_cast<int *>(sRec + kYRec * kMPts);  // [TE][10][kMCS]
   int *sEB = sCol + TE * kMCol;                              // [2][TE][kEBW]
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(sEB + 2 * TE * kEBW);  // [2]: tile copies landed
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long ne = args.ne;
   const long stride = (long)gridDim.x * TE;
@@ -343,28 +370,39 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     sCol[x * kMCS + 31] = -1;
   }
 
-  // asynchronous copies of one tile's point records and scatter blocks
-  // (16-byte chunks; nqp = 4 ne keeps every record chunk aligned)
-  auto issue = [&](long e0, int buf) {
-    const long qp0 = e0 * NQP;
-    for (int ch = tid; ch < kYRec * kMPts / 2; ch += NT) {
-      const int c = ch / (kMPts / 2), part = ch - c * (kMPts / 2);
-      if (e0 + part / 2 < ne) cpa16m(sRec + c * kMPts + part * 2, args.qrec + (long)c * args.nqp + qp0 + part * 2);
-    }
-    if (tid < TE * (kEBW / 4)) {
-      const int el = tid / (kEBW / 4), ch = tid - el * (kEBW / 4);
-      if (e0 + el < ne) cpa16m(sEB + (buf * TE + el) * kEBW + 4 * ch, args.eblk + (e0 + el) * kEBW + 4 * ch);
-    }
-    asm volatile("cp.async.commit_group;" ::: "memory");
+  // one tile's point records (5120 contiguous bytes of the tiled layout) and
+  // its elements' scatter blocks (1856 contiguous bytes) by two bulk copies of
+  // the tensor memory accelerator, completing on mbar[buf]; the buffers are
+  // padded to whole tiles, so a partial last tile copies whole too
+  if (tid == 0) {
+    w_mb_init(&mbar[0], 1);
+    w_mb_init(&mbar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](long e0, int buf) {  // thread 0
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the generic reads of the buffers
+    mb_expect_tx(&mbar[buf], kMTileBytes);
+    bulk_g2s(sRec, args.qrec + (e0 / TE) * (long)(kYRec * kMPtsT), sizeof(double) * kYRec * kMPtsT, &mbar[buf]);
+    bulk_g2s(sEB + buf * TE * kEBW, args.eblk + e0 * kEBW, sizeof(int) * TE * kEBW, &mbar[buf]);
   };
 
   long e0 = (long)blockIdx.x * TE;
-  if (e0 < ne) issue(e0, 0);
+  if (e0 < ne && tid == 0) issue(e0, 0);
 
   for (int it = 0; e0 < ne; it++, e0 += stride) {
     const int mb = it & 1;
-    asm volatile("cp.async.wait_all;" ::: "memory");
-    __syncthreads();  // records and scatter blocks of this tile landed; previous tile's C/S done
+    // this tile's copies landed (bounded wait: a wait that runs out is
+    // counted in status[3] and every thread leaves, after waiting -- again
+    // bounded -- for the copies still in flight)
+    const bool landed = w_mb_wait(&mbar[mb], (unsigned)((it >> 1) & 1), args.wait_ns);
+    if (__syncthreads_or(!landed)) {  // also: previous tile's C/S done
+      if (tid == 0) {
+        atomicAdd(&args.status[3], 1ull);
+        w_mb_wait(&mbar[mb], (unsigned)((it >> 1) & 1), args.wait_ns);
+      }
+      break;
+    }
     // ---- Y: items (element, column-node pair, point), point fastest ----
     if (tid < TE * 20) {
       const int el = tid / 20, rem = tid - el * 20;
@@ -395,7 +433,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     }
     __syncthreads();  // Y, P and column offsets complete; the record buffer is free
     // ---- prefetch the next tile's records and scatter blocks ----
-    if (e0 + stride < ne) issue(e0 + stride, mb ^ 1);
+    if (e0 + stride < ne && tid == 0) issue(e0 + stride, mb ^ 1);
     // ---- C: the element's GEMM on the FP64 tensor cores ----
     // m8n8k4 for row nodes a = 0..7 (12 row tiles of 8 Y rows, 3 steps over
     // the contraction); rows 8 and 9 from the same A fragments with FP64 FMAs
@@ -474,7 +512,6 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       }
     }
   }
-  asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 }  // namespace pgb

@@ -388,8 +388,9 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
 template <int NNE, int NQP, int MODEL>
 int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   constexpr bool YREC = NNE == 10;
-  if (!c->qrec) {
-    int r = dalloc(c, &c->qrec, (size_t)(YREC ? kYRec : kQRec) * c->nqp);
+  if (!c->qrec) {  // the tiled layout of the 10-node records is padded to whole tiles
+    const size_t npts = YREC ? (size_t)((c->nqp + kMPtsT - 1) / kMPtsT) * kMPtsT : (size_t)c->nqp;
+    int r = dalloc(c, &c->qrec, (size_t)(YREC ? kYRec : kQRec) * npts);
     if (r) return r;
   }
   QpArgs q{};
@@ -1007,7 +1008,7 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
   // order, the second stream that zeroes K
   if (m->nne == 10 && c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2) {
     std::vector<int> perm = locality_order(m);
-    if ((r = upload(c, &c->perm, perm.data(), perm.size())) || (r = dalloc(c, &c->eblk, (size_t)ne * kEBW)))
+    if ((r = upload(c, &c->perm, perm.data(), perm.size())) || (r = dalloc(c, &c->eblk, (size_t)((ne + kMTE - 1) / kMTE) * kMTE * kEBW)))
       return fail(r);
     if (cudaStreamCreateWithFlags(&c->zstream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->zfork, cudaEventDisableTiming) != cudaSuccess ||
