@@ -602,9 +602,9 @@ int pgfem_input_read_solver_file(const char *path, long npd, pgfem_solver_file *
  * then per element its point count and per point the model block of
  * write_restart: HE (src/plasticity_model_none.cc:298-311) Fn, Fnm1 = 18
  * doubles; CP (src/plasticity_model.cc:883-942) Fn, Fnm1, pFn, pFnm1,
- * tau_n[12], gamma_dot_n[12], g_n, g_nm1, L_n, L_nm1 = 64 doubles.  J2 has no
- * restart here: the reference's J2 block carries damage variables of a model
- * this path does not carry.  File name convention of the reference:
+ * tau_n[12], gamma_dot_n[12], g_n, g_nm1, L_n, L_nm1 = 64 doubles; J2
+ * (src/cm_j2_plasticity.cc:784-808) Fn, pSn, Fnm1, pSnm1, w, X, H, ep_n, ep_nm1,
+ * gam_n, gam_nm1, the damage flag = 47 doubles.  File name convention of the reference:
  * <dir>/STEP_<step %06d>/<name>_<rank>_<step>.res. */
 int pgfem_restart_block_size(int model);
 /* Host-only formatting / parsing: u_nm1, u_n nodal AoS (nn*3), blocks
@@ -623,8 +623,9 @@ int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int 
  * with their prescribed values; F per point is computed from them on the
  * device; CP pFn, g_n from the committed state (t_n) and pFnm1, g_nm1 from
  * state_nm1 (host AoS nqp*10 as pgfem_gpu_get_state, the state before the
- * last commit; NULL = the state at t_n); tau_n, gamma_dot_n, L_n, L_nm1 are
- * not carried by this path and are written as 0.  J2: the plastic stress of
+ * last commit; NULL = the state at t_n); tau_n and gamma_dot_n from F_n, pF_n
+ * and g_n (pgfem_cp_resolved_shear); L_n, L_nm1 (a multiplier of the
+ * reference's integrator) written as 0.  J2: the plastic stress of
  * the reference's block is pS = G (I - Cp^-1) of this path's state (zero in
  * the initial state, as the reference initialises it), ep_n / ep_nm1 the
  * equivalent plastic strain, gam_n = sqrt(3/2) (ep_n - ep_nm1), the damage
@@ -634,6 +635,15 @@ int pgfem_restart_write_partitions(const pgfem_input *in, const char *name, int 
  * Cp^-1 = I - pSn / G and ep_n); the other fields are not used. */
 int pgfem_gpu_write_restart(pgfem_gpu_ctx *ctx, const char *path, const double *u_nm1, const double *u_n,
                             const double *presc_nm1, const double *presc_n, const double *state_nm1);
+/* Host: the crystal plasticity restart fields tau_n and gamma_dot_n of n
+ * points from F (n*9), pF (n*9), g (n) and the crystal rotation R (n*9), all
+ * row-major: tau = s . (Ce S) n per slip system at Ce = pF^-T F^T F pF^-1 and
+ * gamma_dot = gamma_dot_0 (tau/g) |tau/g|^(1/m - 1), written (n*12 each) in the
+ * order and sign of the systems in the reference's restart files (the order of
+ * its integrator, taken from its own output: every element of its crystal
+ * plasticity tension case).  gdot may be NULL. */
+int pgfem_cp_resolved_shear(const pgfem_material_desc *mat, long n, const double *F, const double *pF,
+                            const double *g, const double *R, double *tau, double *gdot);
 int pgfem_gpu_read_restart(pgfem_gpu_ctx *ctx, const char *path, double *u_nm1, double *u_n);
 
 /* model_type values of model_params.in (include/constitutive_model.h:42-54) */

@@ -1372,6 +1372,87 @@ static int nodal_and_F(pgfem_gpu_ctx *c, const double *u, const double *presc, s
   return PGFEM_GPU_OK;
 }
 
+// Slip systems of the reference's restart output in terms of this library's
+// FCC table: system a of the file is sign * (system kRefSys[a] here), as its
+// own restart files show (every element of its crystal plasticity tension
+// case, ref_out_tension/box_<r>_49.res).
+static const int kRefSys[12] = {2, 0, 1, 5, 4, 3, 8, 6, 7, 9, 10, 11};
+static const double kRefSgn[12] = {1, -1, 1, 1, 1, -1, 1, 1, -1, 1, 1, 1};
+// host copies of the FCC slip table of cp_kernels.cuh (directions <110>,
+// normals {111}, unnormalised) and the 3x3 helpers the host needs
+static const double kHostSlipS[12][3] = {{0, 1, -1}, {1, 0, -1}, {1, -1, 0}, {0, 1, -1}, {1, 0, 1}, {1, 1, 0},
+                                         {0, 1, 1},  {1, 0, -1}, {1, 1, 0},  {0, 1, 1},  {1, 0, 1}, {1, -1, 0}};
+static const double kHostSlipN[12][3] = {{1, 1, 1},  {1, 1, 1},  {1, 1, 1},  {-1, 1, 1}, {-1, 1, 1}, {-1, 1, 1},
+                                         {1, -1, 1}, {1, -1, 1}, {1, -1, 1}, {1, 1, -1}, {1, 1, -1}, {1, 1, -1}};
+static double h_det3(const double *a) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) + a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+static bool h_inv3(const double *a, double *b) {
+  const double d = h_det3(a);
+  if (d == 0.0 || !std::isfinite(d)) return false;
+  const double id = 1.0 / d;
+  b[0] = (a[4] * a[8] - a[5] * a[7]) * id, b[1] = (a[2] * a[7] - a[1] * a[8]) * id;
+  b[2] = (a[1] * a[5] - a[2] * a[4]) * id, b[3] = (a[5] * a[6] - a[3] * a[8]) * id;
+  b[4] = (a[0] * a[8] - a[2] * a[6]) * id, b[5] = (a[2] * a[3] - a[0] * a[5]) * id;
+  b[6] = (a[3] * a[7] - a[4] * a[6]) * id, b[7] = (a[1] * a[6] - a[0] * a[7]) * id;
+  b[8] = (a[0] * a[4] - a[1] * a[3]) * id;
+  return true;
+}
+static void h_mm3(const double *A, const double *B, double *C, bool transA) {  // C = op(A) B
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      double v = 0.0;
+      for (int k = 0; k < 3; k++) v += (transA ? A[k * 3 + i] : A[i * 3 + k]) * B[k * 3 + j];
+      C[i * 3 + j] = v;
+    }
+}
+
+static int cp_resolved_shear_mat(const Mat &m, long n, const double *F, const double *pF, const double *g,
+                                 const double *R, double *tau, double *gdot) {
+  for (long q = 0; q < n; q++) {
+    double pFi[9], Fe[9], C[9], Ci[9];
+    if (!h_inv3(pF + 9 * q, pFi)) return PGFEM_GPU_EINVAL;
+    h_mm3(F + 9 * q, pFi, Fe, false);
+    h_mm3(Fe, Fe, C, true);
+    const double detC = h_det3(C);
+    if (!(detC > 0.0) || !h_inv3(C, Ci)) return PGFEM_GPU_EINVAL;
+    // neo-Hookean + U_Common: S = mu detC^-1/3 (I - trC/3 C^-1) + kappa J (J - 1) C^-1
+    const double J = std::sqrt(detC), a = m.mu / std::cbrt(detC), pv = m.kappa * J * (J - 1.0);
+    const double trC = C[0] + C[4] + C[8];
+    double S[9], CS[9];
+    for (int i = 0; i < 9; i++) S[i] = a * ((i % 4 == 0 ? 1.0 : 0.0) - trC / 3.0 * Ci[i]) + pv * Ci[i];
+    h_mm3(C, S, CS, false);
+    double t[12];
+    const double *Rq = R + 9 * q, is2 = 0.70710678118654752440, is3 = 0.57735026918962576451;
+    for (int sy = 0; sy < 12; sy++) {  // sample-frame s = R s0, n = R n0; tau = s . (C S) n
+      double sv[3], nv[3];
+      for (int i = 0; i < 3; i++) {
+        sv[i] = (Rq[i * 3] * kHostSlipS[sy][0] + Rq[i * 3 + 1] * kHostSlipS[sy][1] + Rq[i * 3 + 2] * kHostSlipS[sy][2]) * is2;
+        nv[i] = (Rq[i * 3] * kHostSlipN[sy][0] + Rq[i * 3 + 1] * kHostSlipN[sy][1] + Rq[i * 3 + 2] * kHostSlipN[sy][2]) * is3;
+      }
+      double v = 0.0;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) v += CS[i * 3 + j] * (sv[i] * nv[j]);
+      t[sy] = v;
+    }
+    for (int k = 0; k < 12; k++) {
+      const double tk = kRefSgn[k] * t[kRefSys[k]];
+      tau[12 * q + k] = tk;
+      if (gdot) {  // the flow rule at t_n: gamma_dot_0 (tau/g) |tau/g|^(1/m - 1)
+        const double r = tk / g[q];
+        gdot[12 * q + k] = m.gdot0 * r * std::pow(std::fabs(r), 1.0 / m.m - 1.0);
+      }
+    }
+  }
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_cp_resolved_shear(const pgfem_material_desc *mat, long n, const double *F, const double *pF,
+                            const double *g, const double *R, double *tau, double *gdot) {
+  if (!mat || n < 0 || (n && (!F || !pF || !g || !R || !tau))) return PGFEM_GPU_EINVAL;
+  return cp_resolved_shear_mat(make_mat(mat), n, F, pF, g, R, tau, gdot);
+}
+
 int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_nm1, const double *u_n,
                             const double *presc_nm1, const double *presc_n, const double *state_nm1) {
   if (!c || !path || (c->ndof && (!u_nm1 || !u_n)) || (c->npres && (!presc_nm1 || !presc_n)))
@@ -1381,10 +1462,28 @@ int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_
   if ((r = nodal_and_F(c, u_nm1, presc_nm1, un1, Fn1)) || (r = nodal_and_F(c, u_n, presc_n, un, Fn))) return r;
   const int bs = pgfem_restart_block_size(c->model);
   std::vector<double> blocks((size_t)bs * c->nqp, 0.0);
-  std::vector<double> st;
+  std::vector<double> st, taus, gdots;
   if (c->model == PGFEM_MODEL_CP || c->model == PGFEM_MODEL_J2) {
     st.resize((size_t)10 * c->nqp);
     if ((r = pgfem_gpu_get_state(c, 0, st.data()))) return r;
+  }
+  if (c->model == PGFEM_MODEL_CP) {  // resolved shears and slip rates at t_n
+    std::vector<double> Rs((size_t)9 * c->ne), Rq((size_t)9 * c->nqp), pFq((size_t)9 * c->nqp), gq(c->nqp);
+    CK(cudaMemcpyAsync(Rs.data(), c->cp_R, sizeof(double) * Rs.size(), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    for (long q = 0; q < c->nqp; q++) {
+      const long e = q / c->nqp_e;
+      for (int i = 0; i < 9; i++) {
+        Rq[9 * q + i] = Rs[(size_t)i * c->ne + e];
+        pFq[9 * q + i] = st[10 * q + i];
+      }
+      gq[q] = st[10 * q + 9];
+    }
+    taus.resize((size_t)12 * c->nqp);
+    gdots.resize((size_t)12 * c->nqp);
+    if ((r = cp_resolved_shear_mat(c->mat, c->nqp, Fn.data(), pFq.data(), gq.data(), Rq.data(), taus.data(),
+                                   gdots.data())))
+      return r;
   }
   for (long q = 0; q < c->nqp; q++) {
     double *b = blocks.data() + (size_t)bs * q;
@@ -1416,9 +1515,12 @@ int pgfem_gpu_write_restart(pgfem_gpu_ctx *c, const char *path, const double *u_
         b[18 + k] = sn[k];
         b[27 + k] = sm[k];
       }
-      // tau_n, gamma_dot_n and L are not carried by this path: written as 0
+      for (int k = 0; k < 12; k++) {
+        b[36 + k] = taus[(size_t)12 * q + k];
+        b[48 + k] = gdots[(size_t)12 * q + k];
+      }
       b[60] = sn[9];
-      b[61] = sm[9];
+      b[61] = sm[9];  // L_n, L_nm1 (a multiplier of the reference's integrator): 0
     }
   }
   return pgfem_restart_format(path, c->nn, c->ne, c->nqp_e, c->model, un1.data(), un.data(), blocks.data());

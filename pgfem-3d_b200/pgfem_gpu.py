@@ -73,6 +73,7 @@ def lib():
             "pgfem_gpu_set_scatter_mode": (C.c_int, [_P, C.c_int]),
             "pgfem_gpu_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_set_neumann": (C.c_int, [_P, C.c_long, _P, _P, _P, C.c_int, _P, _P]),
+            "pgfem_cp_resolved_shear": (C.c_int, [_P, C.c_long, _P, _P, _P, _P, _P, _P]),
             "pgfem_gpu_assemble_RK_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                           C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_gpu_set_neumann_loads": (C.c_int, [_P, C.c_int, _P]),
@@ -844,6 +845,20 @@ class NbcFile:
         v = np.zeros((len(self.ftype), 3))
         _check_input("pgfem_nbc_load_values", lib().pgfem_nbc_load_values(self._h, t, _ptr(v)))
         return v
+
+
+def cp_resolved_shear(mat, F, pF, g, R):
+    """(tau, gamma_dot), each (n, 12), of crystal plasticity points in the
+    order and sign of the reference's restart files (pgfem_cp_resolved_shear)."""
+    F = np.ascontiguousarray(np.reshape(F, (-1, 9)), dtype=np.float64)
+    pF = np.ascontiguousarray(np.reshape(pF, (-1, 9)), dtype=np.float64)
+    g = np.ascontiguousarray(np.ravel(g), dtype=np.float64)
+    R = np.ascontiguousarray(np.reshape(R, (-1, 9)), dtype=np.float64)
+    n = len(F)
+    tau, gd = np.zeros((n, 12)), np.zeros((n, 12))
+    _check("pgfem_cp_resolved_shear", lib().pgfem_cp_resolved_shear(C.byref(mat), n, _ptr(F), _ptr(pF), _ptr(g),
+                                                                      _ptr(R), _ptr(tau), _ptr(gd)))
+    return tau, gd
 
 
 def load_expression(expr, t):

@@ -10,7 +10,8 @@ orientations) and box_0.in.st_tension (time steps and the prescribed-value
 increments of its 49 load steps) and the reference's own output of that run,
 ref_out_tension/box_<r>_49.res (restart files of step 49: the nodal
 displacements u_n and per element the deformation gradient F_n, the plastic
-deformation gradient pF_n and the slip resistance g_n, read with this library's restart parser and put in merged
+deformation gradient pF_n, the slip resistance g_n and the per-system resolved
+shear tau_n and slip rate gamma_dot_n, read with this library's restart parser and put in merged
 node / element order through the reader's partition maps), and writes
 tests/golden/cp_box_tension.json.
 """
@@ -36,6 +37,8 @@ def main(ref):
     pF49 = [None] * m.info.ne
     F49 = [None] * m.info.ne
     g49 = [None] * m.info.ne
+    tau49 = [None] * m.info.ne
+    gd49 = [None] * m.info.ne
     u49 = [None] * m.info.nn
     for r in range(8):
         node_map, e0, ne = m.partition(r)
@@ -50,12 +53,14 @@ def main(ref):
             F49[e0 + k] = blk[0:9].tolist()
             pF49[e0 + k] = blk[18:27].tolist()
             g49[e0 + k] = float(blk[60])
+            tau49[e0 + k] = blk[36:48].tolist()
+            gd49[e0 + k] = blk[48:60].tolist()
     d = dict(X=m.X.tolist(), conn=m.conn.tolist(), codes=m.codes.tolist(), defl=m.defl.tolist(),
              Ex=float(m.materials[0, 0]), nyz=float(m.materials[0, 6]), devPotFlag=int(m.dev_pot[0]),
              volPotFlag=int(m.vol_pot[0]), cp_params=list(mp.p)[:mp.np], euler_type=etype,
              angles=angles.tolist(), nor_min=sf.nor_min, times=times.tolist(),
              load_steps=load_steps[:NSTEPS].tolist(), load_incr=incr[:NSTEPS].tolist(),
-             ref_step=49, ref_F=F49, ref_pF=pF49, ref_g=g49, ref_u=u49,
+             ref_step=49, ref_F=F49, ref_pF=pF49, ref_g=g49, ref_u=u49, ref_tau=tau49, ref_gdot=gd49,
              source="verification_tests/crystal_plasticity/{box_8CPU_tension/box_<r>.in, model_params.in, "
                     "CO/co_<r>.in, box_0.in.st_tension, ref_out_tension/box_<r>_49.res}")
     out = os.path.join(HERE, "cp_box_tension.json")

@@ -4,7 +4,9 @@ pgfem_gpu_read_restart) in the reference's per-rank layout.
 - crystal plasticity box (the reference's own inputs): after three device load
   steps the written file holds the total nodal displacements of t_{n-1} and
   t_n, F from them, pF and g at t_n (committed state) and t_{n-1} (the state
-  before the last commit), zeros for the fields this path does not carry;
+  before the last commit), tau_n and gamma_dot_n of the state at t_n in the
+  reference's system order (pgfem_cp_resolved_shear, pinned to the
+  reference's own restart output on the CPU), zero L_n, L_nm1;
   a fresh context that reads it returns the same displacements and state,
   and its next load step equals the original context's (to the rounding of
   the atomic scatter's summation order, 1e-12)
@@ -71,7 +73,9 @@ def test_crystal_plasticity_restart_round_trip(gpu, tmp_path):
     assert np.abs(blk[:, 9:18] - F_linear_tets(X, conn, a).reshape(-1, 9)).max() <= 1e-14
     assert np.array_equal(blk[:, 18:27], st[:, :9]) and np.array_equal(blk[:, 60], st[:, 9])
     assert np.array_equal(blk[:, 27:36], prev_state[:, :9]) and np.array_equal(blk[:, 61], prev_state[:, 9])
-    assert not blk[:, 36:60].any() and not blk[:, 62:64].any()
+    tau, gdot = pg.cp_resolved_shear(mat, blk[:, 0:9], st[:, :9], st[:, 9], R_cp)
+    assert np.array_equal(blk[:, 36:48], tau) and np.array_equal(blk[:, 48:60], gdot)
+    assert np.abs(tau).max() > 1.0 and not blk[:, 62:64].any()
     # a fresh context resumes from the file
     ctx2 = context()
     r1, r2 = pg.read_restart(ctx2, path)
