@@ -55,7 +55,7 @@ class ClockSampler:
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,clocks.mem,clocks.max.mem")
 
     def __init__(self, index):
         self.index = index
@@ -92,8 +92,11 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
         pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        mem = [float(r[9]) for r in rows if len(r) > 10 and r[9].replace(".", "").isdigit()]
+        mem_mx = [float(r[10]) for r in rows if len(r) > 10 and r[10].replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None,
+                "mem_mhz": statistics.median(mem) if mem else None, "mem_max_mhz": max(mem_mx) if mem_mx else None}
 
 
 def dist_setup(ngpus, backend=None):

@@ -7,14 +7,17 @@
 //
 //  k_qp_update<..., YREC = true>  one thread per quadrature point: F, the
 //      constitutive update (run_integration_algorithm,
-//      src/constitutive_model.cc:1100-1129; state n -> n+1) and a 40-double
-//      point record (structure of arrays) holding the matrices the element
-//      contraction needs:
+//      src/constitutive_model.cc:1100-1129; state n -> n+1) and a 26-double
+//      point record (structure of arrays) from which the assembly forms the
+//      matrices of the element contraction:
 //        G = (dX/dxi)^-1 F^-1      (p_a = G^T dN_a/dxi = F^-T grad_X N_a)
-//        T' = a1 w/2 1 + w tau,  U' = w a2 1 - 2/3 w s,  W' = w (a4 n + a5 dev(n^2)),
-//        s'' = -2/3 w s,  n,  h = a1 w / 2
+//        T' = a1 w/2 1 + w tau,  s'' = -2/3 w s,  U' = w a2 1 + s'',
+//        W' = w (a4 n + a5 dev(n^2)),  h = a1 w / 2
 //      for the spatial tangent c = a1 I + a2 1(x)1 - 2/3 (s(x)1 + 1(x)s)
 //      + a4 n(x)n + a5 n(x)dev(n^2) (cm_models.cuh) and w = det(dX/dxi) x weight.
+//      At a plastic point s = |s| n (radial return), so the record holds
+//      V = n and s'' = c V with c = -2/3 w (s : n); elsewhere V = s,
+//      c = -2/3 w and a4 = a5 = 0.
 //
 //  k_assemble_p2m  persistent grid over tiles of 4 consecutive elements, four
 //      warps per CTA, one element per warp in the contraction.  With the
@@ -33,9 +36,9 @@
 //      values and its p into shared memory (Y in the A-fragment order of the
 //      mma, so that each fragment load is 32 consecutive doubles), and the
 //      column offsets of node b's block in the rows of the element's nodes;
-//   C  warp per element: 36 mma.m8n8k4 for row nodes a = 0..7; rows 8 and 9
-//      from the same A fragments with FP64 FMAs (partial sums over the lane's
-//      contraction indices, combined by two shuffles);
+//   C  warp per element: 36 mma.m8n8k4 for row nodes a = 0..7 and 36 more on
+//      the same A fragments for row nodes 8 and 9 (B columns p_8, p_9
+//      repeated, so that every lane holds its row tiles' results);
 //   S  FP64 reductions of the 900 K entries and 30 R entries into the CSR
 //      through the node-block map (fd_res_assemble, src/fd_residuals.cc:58-73;
 //      PLoc_Sparse, src/PLoc_Sparse.cc:15-175).  Per reduction instruction a
@@ -49,7 +52,8 @@
 namespace pgb {
 
 constexpr int kQRec = kRec;  // point record of the linear-tet path: G 9, w, tau 6, s 6, n 6, dev(n^2) 6, a1 a2 a4 a5
-constexpr int kYRec = 40;  // point record of the tensor-core path: G 9, T' 6, U' 6, W' 6, s'' 6, n 6, h
+// point record of the tensor-core path: G 9, T' 6, V 6, w a2, c, w a4, w a5, h
+constexpr int kYRec = 26;
 constexpr int kMPtsT = 16;  // points per record tile (the assembly tile: 4 elements x 4 points)
 
 // index of field c of record slot qs in the tiled layout of the tensor-core path
@@ -151,16 +155,19 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   const double w = detJ * A.shp.w[q];
   if (YREC) {
     const double h = 0.5 * t.a1 * w, c23 = (2.0 / 3.0) * w;
+    // plastic point: n != 0 (the unit flow direction, s = (s : n) n)
+    const bool pl = PLASTIC && (t.n[0] != 0.0 || t.n[1] != 0.0 || t.n[2] != 0.0 || t.n[3] != 0.0 ||
+                                t.n[4] != 0.0 || t.n[5] != 0.0);
 #pragma unroll
     for (int c = 0; c < 6; c++) {
-      const double d = c < 3 ? 1.0 : 0.0;
-      rec[yrec_idx(qs, 9 + c)] = h * d + w * t.tau[c];
-      rec[yrec_idx(qs, 15 + c)] = w * t.a2 * d - c23 * t.s[c];
-      rec[yrec_idx(qs, 21 + c)] = w * (t.a4 * t.n[c] + t.a5 * t.D[c]);
-      rec[yrec_idx(qs, 27 + c)] = -c23 * t.s[c];
-      rec[yrec_idx(qs, 33 + c)] = t.n[c];
+      rec[yrec_idx(qs, 9 + c)] = h * (c < 3 ? 1.0 : 0.0) + w * t.tau[c];
+      rec[yrec_idx(qs, 15 + c)] = pl ? t.n[c] : t.s[c];
     }
-    rec[yrec_idx(qs, 39)] = h;
+    rec[yrec_idx(qs, 21)] = w * t.a2;
+    rec[yrec_idx(qs, 22)] = pl ? -c23 * sdot(t.s, t.n) : -c23;
+    rec[yrec_idx(qs, 23)] = w * t.a4;
+    rec[yrec_idx(qs, 24)] = w * t.a5;
+    rec[yrec_idx(qs, 25)] = h;
   } else {
     rec[9 * S + qs] = w;
 #pragma unroll
@@ -189,7 +196,9 @@ constexpr int kMPts = kMTE * 4;         // points per tile
 constexpr int kMY = 3 * 12 * 32 + 12;
 constexpr int kMP = 10 * 12 + 4;
 constexpr int kMCS = 36;                // column-table row stride (words): lane loads hit 32 banks
-constexpr int kMCol = 10 * kMCS;        // column table per element: [a 10][rr = 3 b + k, 30 -> R, 31 -> pad]
+// column table per element: [a 10][rr = 3 b + k, 30 -> R, 31 -> pad], element stride padded by three
+// words so that the item stores (element, column-node pair, point) spread over the banks
+constexpr int kMCol = 10 * kMCS + 3;
 constexpr int kMMeta = kMTE * 10;       // (element, node) pairs per tile
 constexpr int kMColR = -2;              // column-table marker of the residual row
 // Per-element scatter block (int32 words, 464 bytes so that it copies in 16-byte chunks):
@@ -263,15 +272,6 @@ __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double
                : "d"(a), "d"(b));
 }
 
-__device__ __forceinline__ void cpa4m(void *dst, const void *src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cpa16m(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
-               "l"(src)
-               : "memory");
-}
 
 // Item (point q, column nodes b0 and b0 + 5) of one element: p_b into P, the
 // 27 values Y_q[j][(b, i, k)] of each column node and, for b0 = 0, the
@@ -284,15 +284,32 @@ __device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3
   double G[9], Tm[6], Um[6], Wm[6], s2[6], nn[6];
 #pragma unroll
   for (int c = 0; c < 9; c++) G[c] = rec[c * RS];
+  const double wa2 = rec[21 * RS], cs = rec[22 * RS], h = rec[25 * RS];
 #pragma unroll
   for (int c = 0; c < 6; c++) {
     Tm[c] = rec[(9 + c) * RS];
-    Um[c] = rec[(15 + c) * RS];
-    Wm[c] = PLASTIC ? rec[(21 + c) * RS] : 0.0;
-    s2[c] = rec[(27 + c) * RS];
-    nn[c] = PLASTIC ? rec[(33 + c) * RS] : 0.0;
+    nn[c] = rec[(15 + c) * RS];
+    s2[c] = cs * nn[c];
+    Um[c] = s2[c] + (c < 3 ? wa2 : 0.0);
   }
-  const double h = rec[39 * RS];
+  if (PLASTIC) {
+    // W' = w a4 n + w a5 dev(n^2) (zero at elastic points: w a4 = w a5 = 0)
+    const double w4 = rec[23 * RS], w5 = rec[24 * RS];
+    const double *n = nn;
+    double n2[6];
+    n2[0] = n[0] * n[0] + n[5] * n[5] + n[4] * n[4];
+    n2[1] = n[5] * n[5] + n[1] * n[1] + n[3] * n[3];
+    n2[2] = n[4] * n[4] + n[3] * n[3] + n[2] * n[2];
+    n2[3] = n[5] * n[4] + n[1] * n[3] + n[3] * n[2];
+    n2[4] = n[0] * n[4] + n[5] * n[3] + n[4] * n[2];
+    n2[5] = n[0] * n[5] + n[5] * n[1] + n[4] * n[3];
+    const double t3 = (n2[0] + n2[1] + n2[2]) * (1.0 / 3.0);
+#pragma unroll
+    for (int c = 0; c < 6; c++) Wm[c] = w4 * n[c] + w5 * (n2[c] - (c < 3 ? t3 : 0.0));
+  } else {
+#pragma unroll
+    for (int c = 0; c < 6; c++) Wm[c] = nn[c] = 0.0;
+  }
   int tb[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
@@ -366,8 +383,9 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     for (int i = 0; i < 3; i++) sY[el * kMY + y_idx(t, 32 * i + 31)] = 0.0;
   }
   for (int x = tid; x < TE * 10; x += NT) {
-    sCol[x * kMCS + 30] = kMColR;
-    sCol[x * kMCS + 31] = -1;
+    int *row = sCol + (x / 10) * kMCol + (x % 10) * kMCS;
+    row[30] = kMColR;
+    row[31] = -1;
   }
 
   // one tile's point records (5120 contiguous bytes of the tiled layout) and
@@ -436,34 +454,28 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     if (e0 + stride < ne && tid == 0) issue(e0 + stride, mb ^ 1);
     // ---- C: the element's GEMM on the FP64 tensor cores ----
     // m8n8k4 for row nodes a = 0..7 (12 row tiles of 8 Y rows, 3 steps over
-    // the contraction); rows 8 and 9 from the same A fragments with FP64 FMAs
+    // the contraction) and, on the same A fragments, for row nodes 8 and 9
+    // with B columns (p_8, p_9) repeated four times: lane (rho, u) then holds
+    // C[8 m + rho][8 + c] of every row tile m in a89[m][c], and no lane
+    // exchange is needed to spread rows 8, 9 over the warp for the scatter
     const int el = warp;
     if (e0 + el >= ne) continue;
     const double *Y = sY + el * kMY;
     const double *P = sP + el * kMP;
     const int rho = lane >> 2, u = lane & 3;
-    double acc[12][2], r8[12], r9[12];
+    double acc[12][2], a89[12][2];
 #pragma unroll
-    for (int m = 0; m < 12; m++) acc[m][0] = acc[m][1] = r8[m] = r9[m] = 0.0;
+    for (int m = 0; m < 12; m++) acc[m][0] = acc[m][1] = a89[m][0] = a89[m][1] = 0.0;
 #pragma unroll
     for (int s = 0; s < 3; s++) {
       const double bf = P[rho * 12 + 4 * s + u];
-      const double p8 = P[8 * 12 + 4 * s + u], p9 = P[9 * 12 + 4 * s + u];
+      const double b89 = P[(8 + (rho & 1)) * 12 + 4 * s + u];
 #pragma unroll
       for (int m = 0; m < 12; m++) {
         const double af = Y[(s * 12 + m) * 32 + lane];
         dmma884(acc[m][0], acc[m][1], af, bf);
-        r8[m] = fma(p8, af, r8[m]);
-        r9[m] = fma(p9, af, r9[m]);
+        dmma884(a89[m][0], a89[m][1], af, b89);
       }
-    }
-    // rows 8, 9: sum the four lanes of a row group
-#pragma unroll
-    for (int m = 0; m < 12; m++) {
-      r8[m] += __shfl_xor_sync(0xffffffffu, r8[m], 1);
-      r9[m] += __shfl_xor_sync(0xffffffffu, r9[m], 1);
-      r8[m] += __shfl_xor_sync(0xffffffffu, r8[m], 2);
-      r9[m] += __shfl_xor_sync(0xffffffffu, r9[m], 2);
     }
     // ---- S: reductions into the CSR ----
     // C[r][a], r = 8 m + rho = 32 i + rr: K entry (row i of node a, column rr
@@ -471,10 +483,12 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     // reduction instruction per value, its target selected.
     const int *eb = sEB + (mb * TE + el) * kEBW;
     const int *ct = sCol + el * kMCol;
-    auto dst = [&](int rb, int rd, int cv) -> double * {
-      if (rb < 0) return nullptr;  // component i of node a is not free
-      if (cv >= 0) return args.K + (rb + cv);
-      return cv == kMColR ? args.R + rd : nullptr;
+    // the target of value v: K entry (row base rb, column offset cv >= 0) or,
+    // for the residual row (cv = kMColR), the residual entry rd; nothing when
+    // component i of node a is not free (rb < 0) or the column is (cv = -1)
+    auto red = [&](int rb, int rd, int cv, double v) {
+      const bool kk = cv >= 0;
+      if (rb >= 0 && (kk || cv == kMColR)) atomicAdd(kk ? args.K + (rb + cv) : args.R + rd, v);
     };
 #pragma unroll
     for (int c = 0; c < 2; c++) {
@@ -488,10 +502,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
 #pragma unroll
       for (int mq = 0; mq < 4; mq++) cv[mq] = ct[a * kMCS + 8 * mq + rho];
 #pragma unroll
-      for (int m = 0; m < 12; m++) {
-        double *d = dst(rb[m >> 2], rd[m >> 2], cv[m & 3]);
-        if (d) atomicAdd(d, acc[m][c]);
-      }
+      for (int m = 0; m < 12; m++) red(rb[m >> 2], rd[m >> 2], cv[m & 3], acc[m][c]);
     }
     {
       // lane u of a row group takes the row tile m = 4 mm + u (row i = mm)
@@ -499,16 +510,14 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       const int cv8 = ct[8 * kMCS + rr], cv9 = ct[9 * kMCS + rr];
 #pragma unroll
       for (int mm = 0; mm < 3; mm++) {
-        double v8 = r8[4 * mm], v9 = r9[4 * mm];
+        double v8 = a89[4 * mm][0], v9 = a89[4 * mm][1];
 #pragma unroll
         for (int x = 1; x < 4; x++) {
-          v8 = u == x ? r8[4 * mm + x] : v8;
-          v9 = u == x ? r9[4 * mm + x] : v9;
+          v8 = u == x ? a89[4 * mm + x][0] : v8;
+          v9 = u == x ? a89[4 * mm + x][1] : v9;
         }
-        double *d8 = dst(eb[24 + mm], eb[54 + mm], cv8);
-        double *d9 = dst(eb[27 + mm], eb[57 + mm], cv9);
-        if (d8) atomicAdd(d8, v8);
-        if (d9) atomicAdd(d9, v9);
+        red(eb[24 + mm], eb[54 + mm], cv8, v8);
+        red(eb[27 + mm], eb[57 + mm], cv9, v9);
       }
     }
   }
