@@ -94,9 +94,16 @@ class ClockSampler:
         pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
         mem = [float(r[9]) for r in rows if len(r) > 10 and r[9].replace(".", "").isdigit()]
         mem_mx = [float(r[10]) for r in rows if len(r) > 10 and r[10].replace(".", "").isdigit()]
+        ecc = None
+        try:
+            ecc = subprocess.run(["nvidia-smi", "--query-gpu=ecc.mode.current", "--format=csv,noheader",
+                                  "-i", str(self.index)], capture_output=True, text=True, timeout=10).stdout.strip()
+        except Exception:
+            pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None,
-                "mem_mhz": statistics.median(mem) if mem else None, "mem_max_mhz": max(mem_mx) if mem_mx else None}
+                "mem_mhz": statistics.median(mem) if mem else None, "mem_max_mhz": max(mem_mx) if mem_mx else None,
+                "ecc": ecc or None}
 
 
 def dist_setup(ngpus, backend=None):

@@ -211,7 +211,8 @@ constexpr int kEBPos = 60, kEBMask = 110;
 
 inline size_t p2m_smem_bytes() {
   return sizeof(double) * ((size_t)kMTE * kMY + (size_t)kMTE * kMP + (size_t)kYRec * kMPts) +
-         sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW + 2 * sizeof(uint64_t);
+         sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW + 2 * sizeof(uint64_t) +
+         2 * sizeof(long);
 }
 
 // bytes of one tile's copies: its point records and its elements' scatter blocks
@@ -372,9 +373,10 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
   int *sCol = reinterpret_cast<int *>(sRec + kYRec * kMPts);  // [TE][10][kMCS]
   int *sEB = sCol + TE * kMCol;                              // [2][TE][kEBW]
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sEB + 2 * TE * kEBW);  // [2]: tile copies landed
+  long *sTile = reinterpret_cast<long *>(mbar + 2);                    // [2]: the tile of each buffer
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long ne = args.ne;
-  const long stride = (long)gridDim.x * TE;
+  const long ntiles = (ne + TE - 1) / TE;
   // pad rows r = 32 i + 31 of Y stay zero; the column table marks the
   // residual row (rr = 30) and the pad row (rr = 31)
   for (int x = tid; x < TE * 12; x += NT) {
@@ -398,17 +400,27 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
-  auto issue = [&](long e0, int buf) {  // thread 0
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the generic reads of the buffers
-    mb_expect_tx(&mbar[buf], kMTileBytes);
-    bulk_g2s(sRec, args.qrec + (e0 / TE) * (long)(kYRec * kMPtsT), sizeof(double) * kYRec * kMPtsT, &mbar[buf]);
-    bulk_g2s(sEB + buf * TE * kEBW, args.eblk + e0 * kEBW, sizeof(int) * TE * kEBW, &mbar[buf]);
+  // Tiles are claimed in order from a global counter (zeroed before the
+  // launch), one tile ahead: all CTAs then work on neighbouring tiles of the
+  // processing order, and the CSR rows they reduce into stay in L2 between
+  // the contributions of neighbouring elements.  Thread 0 claims, records the
+  // tile in sTile[buf] and issues its copies; with no tile left it completes
+  // the buffer's phase by a plain arrive.
+  auto claim = [&](int buf) {  // thread 0
+    const long t = (long)atomicAdd(args.ticket, 1u);
+    sTile[buf] = t;
+    if (t < ntiles) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the generic reads of the buffers
+      mb_expect_tx(&mbar[buf], kMTileBytes);
+      bulk_g2s(sRec, args.qrec + t * (long)(kYRec * kMPtsT), sizeof(double) * kYRec * kMPtsT, &mbar[buf]);
+      bulk_g2s(sEB + buf * TE * kEBW, args.eblk + t * TE * kEBW, sizeof(int) * TE * kEBW, &mbar[buf]);
+    } else {
+      w_mb_arrive(&mbar[buf]);
+    }
   };
+  if (tid == 0) claim(0);
 
-  long e0 = (long)blockIdx.x * TE;
-  if (e0 < ne && tid == 0) issue(e0, 0);
-
-  for (int it = 0; e0 < ne; it++, e0 += stride) {
+  for (int it = 0;; it++) {
     const int mb = it & 1;
     // this tile's copies landed (bounded wait: a wait that runs out is
     // counted in status[3] and every thread leaves, after waiting -- again
@@ -421,6 +433,8 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       }
       break;
     }
+    const long e0 = sTile[mb] * TE;  // written before the barrier above
+    if (e0 >= ne) break;
     // ---- Y: items (element, column-node pair, point), point fastest ----
     if (tid < TE * 20) {
       const int el = tid / 20, rem = tid - el * 20;
@@ -450,8 +464,8 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       }
     }
     __syncthreads();  // Y, P and column offsets complete; the record buffer is free
-    // ---- prefetch the next tile's records and scatter blocks ----
-    if (e0 + stride < ne && tid == 0) issue(e0 + stride, mb ^ 1);
+    // ---- claim the next tile, prefetch its records and scatter blocks ----
+    if (tid == 0) claim(mb ^ 1);
     // ---- C: the element's GEMM on the FP64 tensor cores ----
     // m8n8k4 for row nodes a = 0..7 (12 row tiles of 8 Y rows, 3 steps over
     // the contraction) and, on the same A fragments, for row nodes 8 and 9

@@ -83,6 +83,7 @@ struct pgfem_gpu_ctx {
   double *F0_tab = nullptr;
   int ngroups = 0;
   unsigned *sched_ticket = nullptr;
+  unsigned *p2m_ticket = nullptr;  // tile counter of the quadratic-tet assembly
   int sched_epb = 0, sched_grab = 0;  // elements per block (0: default), tiles per steal (0: static)
   // failure-path tests: bound of the hand-off waits, one-shot withheld hand-off
   unsigned long long wait_ns = 2000000000ull;
@@ -312,7 +313,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->qrec, c->eblk, c->perm,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
-                  c->sched_ticket, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
+                  c->sched_ticket, c->p2m_ticket, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
                   c->nbc_load, c->tr_buf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -423,12 +424,14 @@ int launch_p2m(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
   CK(cudaEventRecord(c->zfork, s));
   CK(cudaStreamWaitEvent(c->zstream, c->zfork, 0));
   CK(cudaMemsetAsync(a0.K, 0, sizeof(double) * c->nnz, c->zstream));
+  CK(cudaMemsetAsync(c->p2m_ticket, 0, sizeof(unsigned), c->zstream));
   CK(cudaEventRecord(c->zjoin, c->zstream));
   if (int r = launch_qp_update<10, 4, MODEL>(c, s)) return r;
   CK(cudaStreamWaitEvent(s, c->zjoin, 0));
   AsmArgs a = a0;
   a.qrec = c->qrec;
   a.eblk = c->eblk;
+  a.ticket = c->p2m_ticket;
   const size_t smem = p2m_smem_bytes();
   auto kern = k_assemble_p2m<MODEL>;
   static bool attr_set = false;
@@ -1008,7 +1011,8 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
   // order, the second stream that zeroes K
   if (m->nne == 10 && c->model != PGFEM_MODEL_CP && c->mat.dev_pot != 2) {
     std::vector<int> perm = locality_order(m);
-    if ((r = upload(c, &c->perm, perm.data(), perm.size())) || (r = dalloc(c, &c->eblk, (size_t)((ne + kMTE - 1) / kMTE) * kMTE * kEBW)))
+    if ((r = upload(c, &c->perm, perm.data(), perm.size())) ||
+        (r = dalloc(c, &c->eblk, (size_t)((ne + kMTE - 1) / kMTE) * kMTE * kEBW)) || (r = dalloc(c, &c->p2m_ticket, 1)))
       return fail(r);
     if (cudaStreamCreateWithFlags(&c->zstream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&c->zfork, cudaEventDisableTiming) != cudaSuccess ||
