@@ -946,6 +946,168 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 #include "orc_bform.inc"
 
 // ---------------------------------------------------------------------------
+// Three-field (CM3F) element of the hyperelastic model, quasi-static, total
+// Lagrangian, one rank: the element loop of src/constitutive_model.cc:
+// 695-881 with CM_ThreeField (src/constitutive_model_3f.cc:47-491) and the
+// condensation condense_K_3F_to_1F / condense_F_3F_to_1F
+// (src/condense.cc:300-385).  CM3F carries one pressure P and one volume
+// theta per element (get_3f_pressure_volume_number,
+// src/three_field_element.cc:1399-1409), so Np = Nt = 1.  For HE, M = pF^-1
+// = I, eF = F, eFn = I, dM/du = dM/dtheta = 0, theta_n = tJn = Jn = 1, and
+// set_scalars' default dt_alpha_1_minus_alpha = -1
+// (include/constitutive_model_3f.h:58-65).  eSd, Ld: the deviatoric PK2 and
+// tangent of the elasticity (update_elasticity_dev, include/
+// constitutive_model.h:413-435: the material's potential without its
+// volumetric part); dU = kappa U'(theta), ddU = kappa U''(theta)
+// (include/constitutive_model.h:319-383).  Per point, with G the shape tensor
+// of (a, b), Psi = sym(G^T F), w = detJxW:
+//   Ru  += (Psi:eSd + P J tr(G F^-1)) w            Rp += (J - theta) w
+//   Rt  += (dU - P) w
+//   Kuu -= -w (Psi_ab:Ld:Psi_wg + P J (tr(G_ab F^-1) tr(G_wg F^-1)
+//             - tr(G_ab F^-1 G_wg F^-1)) + sym(G_ab^T G_wg):eSd)
+//   Kup -= -w J tr(F^-1 G)   Ktp -= w   Ktt -= -w ddU   (Kut = Ktu = 0)
+// then, with Kpu = Kup^T and Kpt = Ktp^T:
+//   K = Kuu - Kup Ktp^-1 Ktu + Kup Ktp^-1 Ktt Kpt^-1 Kpu - Kut Kpt^-1 Kpu
+//   f = fu + Kup Ktp^-1 Ktt Kpt^-1 fp - Kup Ktp^-1 ft - Kut Kpt^-1 fp.
+// blk (may be NULL) receives fp, ft, Ktp, Ktt and Kup[nd].
+// ---------------------------------------------------------------------------
+extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
+                              double Pe, double theta, double *fe, double *lk, double *blk) {
+  if (mat->model != ORC_MODEL_HE) return 1;
+  const int nne = P->nne, nd = nne * 3;
+  Quad qr = quad_rule(nne);
+  double Xe[30];
+  for (int a = 0; a < nne; a++)
+    for (int i = 0; i < 3; i++) Xe[a * 3 + i] = P->X[(long)P->conn[e * nne + a] * 3 + i];
+  Elast el = make_elast(mat);
+  Elast dev = el;
+  dev.kappa = 0.0;  // the deviatoric part alone
+  double dUs, d2Us;
+  vol_derivs(el.vol_pot, theta, dUs, d2Us);
+  const double dU = el.kappa * dUs, ddU = el.kappa * d2Us;
+  std::vector<double> fu(nd, 0.0), Kup(nd, 0.0), Kuu(lk ? nd * nd : 0, 0.0);
+  double fp = 0.0, ft = 0.0, Ktp = 0.0, Ktt = 0.0;
+  int err = 0;
+  for (int ip = 0; ip < qr.nint; ip++) {
+    double dN[30];
+    int terr = 0;
+    const double detJ = PGFem3D_dNdX(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], Xe, dN, &terr);
+    if (terr) { err += terr; break; }
+    const double w = detJ * qr.w[ip];
+    double F[9], Fi[9], C[9], S[9], L[81];
+    deformation_gradient(nne, u_e, dN, F);
+    if (P->F0)
+      for (int i = 0; i < 9; i++) F[i] += P->F0[i];
+    const double J = det3x3(F);
+    if (J <= 0.0 || inv3x3(F, Fi)) { err += 1; break; }
+    matmulTN(F, F, C);
+    he_stress_stiffness(dev, C, J, S, lk ? L : nullptr);
+    // per (a, b): Psi = sym(G^T F) and tr(G F^-1), G_ij = delta_ib dN_a,j
+    std::vector<double> Psi(nd * 9), trGFi(nd), GFi(nd * 9);
+    for (int a = 0; a < nne; a++)
+      for (int b = 0; b < 3; b++) {
+        const int r = a * 3 + b;
+        double G[9] = {0}, A[9], X[9];
+        for (int j = 0; j < 3; j++) G[b * 3 + j] = dN[a * 3 + j];
+        matmulTN(G, F, A);
+        for (int i = 0; i < 3; i++)
+          for (int j = 0; j < 3; j++) Psi[r * 9 + i * 3 + j] = 0.5 * (A[i * 3 + j] + A[j * 3 + i]);
+        matmul(G, Fi, X);
+        for (int i = 0; i < 9; i++) GFi[r * 9 + i] = X[i];
+        trGFi[r] = X[0] + X[4] + X[8];
+        double PsiS = 0.0;
+        for (int i = 0; i < 9; i++) PsiS += Psi[r * 9 + i] * S[i];
+        fu[r] += (PsiS + Pe * J * trGFi[r]) * w;
+        Kup[r] -= -w * J * trGFi[r];
+      }
+    fp += (J - theta) * w;
+    ft += (dU - Pe) * w;
+    Ktp -= w;
+    Ktt -= -w * ddU;
+    if (!lk) continue;
+    for (int r = 0; r < nd; r++) {
+      const int a = r / 3, b = r % 3;
+      double PsiL[9];
+      for (int ij = 0; ij < 9; ij++) {
+        double v = 0.0;
+        for (int kl = 0; kl < 9; kl++) v += Psi[r * 9 + kl] * L[kl * 9 + ij];
+        PsiL[ij] = v;
+      }
+      for (int c = 0; c < nd; c++) {
+        const int wn = c / 3, g = c % 3;
+        double PLP = 0.0;
+        for (int ij = 0; ij < 9; ij++) PLP += PsiL[ij] * Psi[c * 9 + ij];
+        double tr2 = 0.0;  // tr(G_ab F^-1 G_wg F^-1)
+        for (int i = 0; i < 3; i++)
+          for (int k = 0; k < 3; k++) tr2 += GFi[r * 9 + i * 3 + k] * GFi[c * 9 + k * 3 + i];
+        // sym(G_ab^T G_wg):eSd, (G_ab^T G_wg)_ij = delta_bg dN_a,i dN_w,j
+        double DPsiS = 0.0;
+        if (b == g)
+          for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++)
+              DPsiS += 0.5 * (dN[a * 3 + i] * dN[wn * 3 + j] + dN[a * 3 + j] * dN[wn * 3 + i]) * S[i * 3 + j];
+        Kuu[r * nd + c] -= -w * (PLP + Pe * J * (trGFi[r] * trGFi[c] - tr2) + DPsiS);
+      }
+    }
+  }
+  if (err) return err;
+  const double Kpt = Ktp, KtpI = 1.0 / Ktp, KptI = 1.0 / Kpt;
+  for (int r = 0; r < nd; r++) fe[r] = fu[r] + Kup[r] * KtpI * Ktt * KptI * fp - Kup[r] * KtpI * ft;
+  if (lk)
+    for (int r = 0; r < nd; r++)
+      for (int c = 0; c < nd; c++) lk[r * nd + c] = Kuu[r * nd + c] + Kup[r] * KtpI * Ktt * KptI * Kup[c];
+  if (blk) {
+    blk[0] = fp;
+    blk[1] = ft;
+    blk[2] = Ktp;
+    blk[3] = Ktt;
+    for (int r = 0; r < nd; r++) blk[4 + r] = Kup[r];
+  }
+  if (P->nbc_off) neumann_faces(P, e, Xe, u_e, fe, lk);
+  return 0;
+}
+
+// Global assembly of the three-field element: P_e, theta_e per element.
+extern "C" int orc_assemble_3f(const orc_problem *P, const orc_material *mat, const double *u,
+                               const double *u_presc, const double *Pe, const double *theta, double *R,
+                               double *K) {
+  const int nd = P->nne * 3;
+  return run_elements(P, 0, P->ne, 1, [&](long e) -> int {
+    double ue[30], fe[30];
+    std::vector<double> lk(K ? nd * nd : 0);
+    gather_u(P, e, u, u_presc, ue);
+    int err = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], fe, K ? lk.data() : nullptr, nullptr);
+    if (!err) scatter(P, e, fe, K ? lk.data() : nullptr, R, K);
+    return err;
+  });
+}
+
+// Increments of the element pressure and volume after a displacement
+// increment du (free-DOF vector; prescribed values unchanged):
+// compute_d_theta_dP (src/constitutive_model_3f.cc:494-549) with the blocks
+// at u, Ktu = 0 for HE:
+//   d_theta = -Kpt^-1 (Kpu du + fp),  dP = -Ktp^-1 (ft + Ktu du + Ktt d_theta).
+extern "C" int orc_update_3f(const orc_problem *P, const orc_material *mat, const double *u,
+                             const double *u_presc, const double *du, const double *Pe, const double *theta,
+                             double *dP, double *dtheta) {
+  const int nd = P->nne * 3;
+  int err = 0;
+  for (long e = 0; e < P->ne; e++) {
+    double ue[30], due[30], fe[30], blk[4 + 30];
+    gather_u(P, e, u, u_presc, ue);
+    gather_u(P, e, du, nullptr, due);
+    const int r = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], fe, nullptr, blk);
+    if (r) { err += r; continue; }
+    const double fp = blk[0], ft = blk[1], Ktp = blk[2], Ktt = blk[3], Kpt = Ktp;
+    double Kpu_du = 0.0;
+    for (int i = 0; i < nd; i++) Kpu_du += blk[4 + i] * due[i];
+    dtheta[e] = -(1.0 / Kpt) * (Kpu_du + fp);
+    dP[e] = -(1.0 / Ktp) * ft - (1.0 / Ktp) * Ktt * dtheta[e];
+  }
+  return err;
+}
+
+// ---------------------------------------------------------------------------
 // Transient (inertia) 1-field element of the hyperelastic model, one rank:
 // residual_with_inertia / stiffness_with_inertia (src/dynamics.cc:183-432),
 // which PGFem3D runs instead of the quasi-static element whenever the
