@@ -151,6 +151,35 @@ int pgfem_gpu_set_neumann(pgfem_gpu_ctx *ctx, long nface, const long *elem, cons
                           const int *feature, int nfeature, const int *load_type, const double *load_np1);
 int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *ctx, int nfeature, const double *load_np1);
 
+/* ---- three-field (CM3F) element -----------------------------------------
+ * The constitutive-model element with one pressure P and one volume theta per
+ * element (analysis type CM3F: get_3f_pressure_volume_number,
+ * src/three_field_element.cc:1399-1409; the element loop of
+ * src/constitutive_model.cc:695-881 with CM_ThreeField,
+ * src/constitutive_model_3f.cc:185-491, and the static condensation
+ * condense_K_3F_to_1F / condense_F_3F_to_1F, src/condense.cc:300-385), for
+ * quadratic tets and the hyperelastic model on the default R+K path (atomic
+ * scatter), total Lagrangian, quasi-static.  set_three_field gives P and
+ * theta per element (host arrays of ne, element order; theta > 0) and switches
+ * every later R+K and residual call of the context to the condensed
+ * three-field element; NULL, NULL switches back.  PGFEM_GPU_EINVAL for other
+ * elements or models, and, while it is on, for the element-level and the
+ * transient calls.  get_three_field reads P and theta back.
+ * three_field_increments: the local update after a displacement increment du
+ * (free-DOF vector; compute_d_theta_dP, src/constitutive_model_3f.cc:494-549)
+ * -- dP, d_theta per element from the blocks at u; the caller adds them.
+ * three_field_update_device: the same on device buffers; with d_out NULL the
+ * increments are added to the context's P and theta (what the device Newton
+ * step, pgfem_gpu_newton_step, does after each solve while three-field is on),
+ * else written to d_out (2 ne: dP, then d_theta). */
+int pgfem_gpu_set_three_field(pgfem_gpu_ctx *ctx, const double *P, const double *theta);
+int pgfem_gpu_get_three_field(pgfem_gpu_ctx *ctx, double *P, double *theta);
+int pgfem_gpu_three_field_enabled(const pgfem_gpu_ctx *ctx);
+int pgfem_gpu_three_field_increments(pgfem_gpu_ctx *ctx, const double *u, const double *u_presc,
+                                     const double *du, double *dP, double *dtheta, pgfem_gpu_status *st);
+int pgfem_gpu_three_field_update_device(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc,
+                                        const double *d_du, double *d_out, void *stream);
+
 /* Device bytes held by the context (mesh, map, state, scratch). */
 long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *ctx);
 long pgfem_gpu_nnz(const pgfem_gpu_ctx *ctx);

@@ -54,11 +54,15 @@ namespace pgb {
 constexpr int kQRec = kRec;  // point record of the linear-tet path: G 9, w, tau 6, s 6, n 6, dev(n^2) 6, a1 a2 a4 a5
 // point record of the tensor-core path: G 9, T' 6, V 6, w a2, c, w a4, w a5, h
 constexpr int kYRec = 26;
+// the three-field (CM3F) element adds w J, w and the element's theta and P
+constexpr int kYRecTF = 30;
+__host__ __device__ constexpr int yrec_fields(bool tf) { return tf ? kYRecTF : kYRec; }
 constexpr int kMPtsT = 16;  // points per record tile (the assembly tile: 4 elements x 4 points)
 
 // index of field c of record slot qs in the tiled layout of the tensor-core path
+template <int NRF = kYRec>
 __host__ __device__ __forceinline__ long yrec_idx(long qs, int c) {
-  return ((qs >> 4) * kYRec + c) * kMPtsT + (qs & (kMPtsT - 1));
+  return ((qs >> 4) * NRF + c) * kMPtsT + (qs & (kMPtsT - 1));
 }
 
 struct QpArgs {
@@ -79,12 +83,16 @@ struct QpArgs {
   const int *perm;
   Mat mat;
   ShapeTable shp;
+  // three-field element (10-node records, hyperelastic model): the pressure
+  // and the volume of each element (element order)
+  const double *tf_P, *tf_theta;
 };
 
-template <int NNE, int NQP, int MODEL, bool YREC = false>
+template <int NNE, int NQP, int MODEL, bool YREC = false, bool TF = false>
 __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   constexpr bool PLASTIC = (MODEL == 1);
-  constexpr int NR = YREC ? kYRec : kQRec;
+  constexpr int NRF = yrec_fields(TF);
+  constexpr int NR = YREC ? NRF : kQRec;
   const long qs = blockIdx.x * (long)blockDim.x + threadIdx.x;  // record slot
   if (qs >= A.nqp) return;
   const long es = qs / NQP;
@@ -129,7 +137,7 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   if (!ok) {
     atomicAdd(&A.status[0], 1ull);
 #pragma unroll
-    for (int c = 0; c < NR; c++) rec[YREC ? yrec_idx(qs, c) : c * S + qs] = 0.0;
+    for (int c = 0; c < NR; c++) rec[YREC ? yrec_idx<NRF>(qs, c) : c * S + qs] = 0.0;
     return;
   }
   double Ast[6] = {1, 1, 1, 0, 0, 0}, alpha = 0.0;
@@ -141,6 +149,20 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   QpTangent t;
   double Anp1[6], alpha_np1;
   spatial_update<PLASTIC>(A.mat, F, J, Ast, alpha, t, Anp1, &alpha_np1);
+  double tfP = 0.0, tfTh = 0.0;
+  if (TF) {
+    // three-field element: the volumetric stress is the element pressure,
+    // P J 1, at fixed P (no kappa J^2 U'' term in the tangent)
+    tfP = A.tf_P[e];
+    tfTh = A.tf_theta[e];
+    double dU, d2U;
+    vol_derivs(A.mat.vol_pot, J, dU, d2U);
+    const double pJ = A.mat.kappa * J * dU, PJ = tfP * J;
+#pragma unroll
+    for (int c = 0; c < 3; c++) t.tau[c] += PJ - pJ;
+    t.a1 += 2.0 * (pJ - PJ);
+    t.a2 += PJ - A.mat.kappa * (J * dU + J * J * d2U);
+  }
   if (PLASTIC && A.state_np1) {
 #pragma unroll
     for (int c = 0; c < 6; c++) A.state_np1[c * S + qp] = Anp1[c];
@@ -150,7 +172,7 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
   for (int i = 0; i < 3; i++)
 #pragma unroll
     for (int j = 0; j < 3; j++)
-      rec[YREC ? yrec_idx(qs, i * 3 + j) : (i * 3 + j) * S + qs] =
+      rec[YREC ? yrec_idx<NRF>(qs, i * 3 + j) : (i * 3 + j) * S + qs] =
           dXi[i * 3 + 0] * Fi[0 * 3 + j] + dXi[i * 3 + 1] * Fi[1 * 3 + j] + dXi[i * 3 + 2] * Fi[2 * 3 + j];
   const double w = detJ * A.shp.w[q];
   if (YREC) {
@@ -160,14 +182,20 @@ __global__ void __launch_bounds__(128) k_qp_update(const QpArgs A) {
                                 t.n[4] != 0.0 || t.n[5] != 0.0);
 #pragma unroll
     for (int c = 0; c < 6; c++) {
-      rec[yrec_idx(qs, 9 + c)] = h * (c < 3 ? 1.0 : 0.0) + w * t.tau[c];
-      rec[yrec_idx(qs, 15 + c)] = pl ? t.n[c] : t.s[c];
+      rec[yrec_idx<NRF>(qs, 9 + c)] = h * (c < 3 ? 1.0 : 0.0) + w * t.tau[c];
+      rec[yrec_idx<NRF>(qs, 15 + c)] = pl ? t.n[c] : t.s[c];
     }
-    rec[yrec_idx(qs, 21)] = w * t.a2;
-    rec[yrec_idx(qs, 22)] = pl ? -c23 * sdot(t.s, t.n) : -c23;
-    rec[yrec_idx(qs, 23)] = w * t.a4;
-    rec[yrec_idx(qs, 24)] = w * t.a5;
-    rec[yrec_idx(qs, 25)] = h;
+    rec[yrec_idx<NRF>(qs, 21)] = w * t.a2;
+    rec[yrec_idx<NRF>(qs, 22)] = pl ? -c23 * sdot(t.s, t.n) : -c23;
+    rec[yrec_idx<NRF>(qs, 23)] = w * t.a4;
+    rec[yrec_idx<NRF>(qs, 24)] = w * t.a5;
+    rec[yrec_idx<NRF>(qs, 25)] = h;
+    if (TF) {
+      rec[yrec_idx<NRF>(qs, 26)] = w * J;
+      rec[yrec_idx<NRF>(qs, 27)] = w;
+      rec[yrec_idx<NRF>(qs, 28)] = tfTh;
+      rec[yrec_idx<NRF>(qs, 29)] = tfP;
+    }
   } else {
     rec[9 * S + qs] = w;
 #pragma unroll
@@ -209,14 +237,16 @@ constexpr int kMColR = -2;              // column-table marker of the residual r
 constexpr int kEBW = 116;
 constexpr int kEBPos = 60, kEBMask = 110;
 
-inline size_t p2m_smem_bytes() {
-  return sizeof(double) * ((size_t)kMTE * kMY + (size_t)kMTE * kMP + (size_t)kYRec * kMPts) +
+inline size_t p2m_smem_bytes(bool tf = false) {
+  return sizeof(double) * ((size_t)kMTE * kMY + (size_t)kMTE * kMP + (size_t)yrec_fields(tf) * kMPts) +
          sizeof(int) * (size_t)kMTE * kMCol + sizeof(int) * 2 * (size_t)kMTE * kEBW + 2 * sizeof(uint64_t) +
          2 * sizeof(long);
 }
 
 // bytes of one tile's copies: its point records and its elements' scatter blocks
-constexpr unsigned kMTileBytes = (unsigned)(sizeof(double) * kYRec * kMPtsT + sizeof(int) * kMTE * kEBW);
+__host__ __device__ constexpr unsigned tile_bytes(bool tf) {
+  return (unsigned)(sizeof(double) * yrec_fields(tf) * kMPtsT + sizeof(int) * kMTE * kEBW);
+}
 
 // one-dimensional bulk copy global -> shared through the tensor memory
 // accelerator, completing on an mbarrier (16-byte aligned, size a multiple of 16)
@@ -277,11 +307,20 @@ __device__ __forceinline__ void dmma884(double &c0, double &c1, double a, double
 // Item (point q, column nodes b0 and b0 + 5) of one element: p_b into P, the
 // 27 values Y_q[j][(b, i, k)] of each column node and, for b0 = 0, the
 // residual rows Y_q[j][32 i + 30] = w tau_ij.  rec: the point's record fields
-// with stride RS; dN: the shape-function derivatives of the point.
+// with stride RS (the element's other points at rec - q + q'); shp: the
+// shape-function derivatives.
+// TF (three-field element, one pressure P and one volume theta per element):
+// the static condensation of (P, theta) adds c Kup Kup^T to the element's K and
+// s Kup to its R, with Kup_b = sum_q w J p_qb (the derivative of the volume
+// constraint), W = sum_q w, fp = sum_q w J - theta W, c = kappa U''(theta) / W
+// and s = c fp + kappa U'(theta) - P -- in the contraction, w J c Kup_b[k] is
+// added to U_b[k] and w J s delta_ij to the residual rows (the pressure part
+// of the point's stress is P J 1 already, from the point kernel).
 // Y[t][r] sits at y_idx(t, r) = tb(t) + 128 i + gk(3 b + k) for r = 32 i + 3 b + k.
-template <bool PLASTIC, int RS>
-__device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3], int q, int b0, double *Y,
-                                         double *P) {
+template <bool PLASTIC, int RS, bool TF = false>
+__device__ __forceinline__ void p2m_item(const double *rec, const ShapeTable &shp, int q, int b0, double *Y,
+                                         double *P, const Mat &mat) {
+  const double(*dN)[3] = shp.dNxi[q];
   double G[9], Tm[6], Um[6], Wm[6], s2[6], nn[6];
 #pragma unroll
   for (int c = 0; c < 9; c++) G[c] = rec[c * RS];
@@ -311,6 +350,22 @@ __device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3
 #pragma unroll
     for (int c = 0; c < 6; c++) Wm[c] = nn[c] = 0.0;
   }
+  double wJq = 0.0, tfc = 0.0, tfs = 0.0;
+  if (TF) {
+    const double *r0 = rec - q;  // point 0 of the element
+    double W = 0.0, SJ = 0.0;
+#pragma unroll
+    for (int qq = 0; qq < 4; qq++) {
+      SJ += r0[26 * RS + qq];
+      W += r0[27 * RS + qq];
+    }
+    wJq = rec[26 * RS];
+    const double th = rec[28 * RS], Pe = rec[29 * RS];
+    double dU, d2U;
+    vol_derivs(mat.vol_pot, th, dU, d2U);
+    tfc = mat.kappa * d2U / W;
+    tfs = tfc * (SJ - th * W) + mat.kappa * dU - Pe;
+  }
   int tb[3];
 #pragma unroll
   for (int j = 0; j < 3; j++) {
@@ -329,6 +384,21 @@ __device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3
     smv(Tm, p, T);
     smv(Um, p, U);
     if (PLASTIC) smv(Wm, p, W);
+    if (TF) {
+      // Kup_b = sum over the element's points of w J G^T dN_b
+      const double *r0 = rec - q;
+      double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+      for (int qq = 0; qq < 4; qq++) {
+        const double *rq = r0 + qq;
+        const double d0 = shp.dNxi[qq][b][0], d1 = shp.dNxi[qq][b][1], d2 = shp.dNxi[qq][b][2];
+        const double wj = rq[26 * RS];
+#pragma unroll
+        for (int j = 0; j < 3; j++) v[j] = fma(wj, rq[j * RS] * d0 + rq[(3 + j) * RS] * d1 + rq[(6 + j) * RS] * d2, v[j]);
+      }
+#pragma unroll
+      for (int k = 0; k < 3; k++) U[k] = fma(wJq * tfc, v[k], U[k]);
+    }
     int gk[3];
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -358,19 +428,20 @@ __device__ __forceinline__ void p2m_item(const double *rec, const double (*dN)[3
 #pragma unroll
     for (int j = 0; j < 3; j++)
 #pragma unroll
-      for (int i = 0; i < 3; i++) Y[tb[j] + 128 * i + 120] = Tm[vo(i, j)] - (i == j ? h : 0.0);
+      for (int i = 0; i < 3; i++) Y[tb[j] + 128 * i + 120] = Tm[vo(i, j)] - (i == j ? h - wJq * tfs : 0.0);
   }
 }
 
-template <int MODEL>
+template <int MODEL, bool TF = false>
 __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs args) {
   constexpr int NNE = 10, NQP = 4, TE = kMTE, NT = kMThreads;
   constexpr bool PLASTIC = (MODEL == 1);
+  constexpr int NRF = yrec_fields(TF);
   extern __shared__ __align__(16) double msm[];
   double *sY = msm;                                          // [TE][kMY]
   double *sP = sY + TE * kMY;                                // [TE][kMP]
-  double *sRec = sP + TE * kMP;                              // [kYRec][kMPts]
-  int *sCol = reinterpret_cast<int *>(sRec + kYRec * kMPts);  // [TE][10][kMCS]
+  double *sRec = sP + TE * kMP;                              // [NRF][kMPts]
+  int *sCol = reinterpret_cast<int *>(sRec + NRF * kMPts);    // [TE][10][kMCS]
   int *sEB = sCol + TE * kMCol;                              // [2][TE][kEBW]
   uint64_t *mbar = reinterpret_cast<uint64_t *>(sEB + 2 * TE * kEBW);  // [2]: tile copies landed
   long *sTile = reinterpret_cast<long *>(mbar + 2);                    // [2]: the tile of each buffer
@@ -411,8 +482,8 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
     sTile[buf] = t;
     if (t < ntiles) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // after the generic reads of the buffers
-      mb_expect_tx(&mbar[buf], kMTileBytes);
-      bulk_g2s(sRec, args.qrec + t * (long)(kYRec * kMPtsT), sizeof(double) * kYRec * kMPtsT, &mbar[buf]);
+      mb_expect_tx(&mbar[buf], tile_bytes(TF));
+      bulk_g2s(sRec, args.qrec + t * (long)(NRF * kMPtsT), sizeof(double) * NRF * kMPtsT, &mbar[buf]);
       bulk_g2s(sEB + buf * TE * kEBW, args.eblk + t * TE * kEBW, sizeof(int) * TE * kEBW, &mbar[buf]);
     } else {
       w_mb_arrive(&mbar[buf]);
@@ -440,7 +511,8 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       const int el = tid / 20, rem = tid - el * 20;
       const int bp = rem >> 2, q = rem & 3;
       if (e0 + el < ne) {
-        p2m_item<PLASTIC, kMPts>(sRec + el * NQP + q, args.shp.dNxi[q], q, bp, sY + el * kMY, sP + el * kMP);
+        p2m_item<PLASTIC, kMPts, TF>(sRec + el * NQP + q, args.shp, q, bp, sY + el * kMY, sP + el * kMP,
+                                     args.mat);
         // column offsets of node b's block inside the rows of nodes a = q, q+4, q+8
         const int *eb = sEB + (mb * TE + el) * kEBW;
         const uint16_t *pos16 = reinterpret_cast<const uint16_t *>(eb + kEBPos);
@@ -535,6 +607,73 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
       }
     }
   }
+}
+
+// Three-field element (one pressure P and one volume theta per element,
+// quadratic tets, hyperelastic model): the local update after a displacement
+// increment du (compute_d_theta_dP, src/constitutive_model_3f.cc:494-549, with
+// the blocks at u; thread per element): with W = sum_q w, fp = sum_q w J -
+// theta W and Kpu du = sum_q w J tr(Grad(du) F^-1),
+//   d_theta = (Kpu du + fp) / W,  dP = kappa U'(theta) - P + kappa U''(theta) d_theta.
+// An element with an inverted point gets zero increments and is counted.
+__global__ void k_tf_update(const QpArgs A, const double *dunode, double *dP, double *dtheta) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= A.ne) return;
+  double W = 0.0, SJ = 0.0, Kdu = 0.0;
+  bool ok = true;
+  for (int q = 0; q < 4 && ok; q++) {
+    double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dU[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0},
+           dD[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < 10; b++) {
+      const int n = A.conn[(long)b * A.ne + e];
+      const double g0 = A.shp.dNxi[q][b][0], g1 = A.shp.dNxi[q][b][1], g2 = A.shp.dNxi[q][b][2];
+      for (int i = 0; i < 3; i++) {
+        const double x = A.X[i * A.nn + n], u = A.unode[i * A.nn + n], d = dunode[i * A.nn + n];
+        dX[i * 3 + 0] += g0 * x;
+        dX[i * 3 + 1] += g1 * x;
+        dX[i * 3 + 2] += g2 * x;
+        dU[i * 3 + 0] += g0 * u;
+        dU[i * 3 + 1] += g1 * u;
+        dU[i * 3 + 2] += g2 * u;
+        dD[i * 3 + 0] += g0 * d;
+        dD[i * 3 + 1] += g1 * d;
+        dD[i * 3 + 2] += g2 * d;
+      }
+    }
+    const double detJ = det3(dX);
+    double dXi[9], F[9], Fi[9], L[9];
+    ok = detJ > 0.0 && inv3(dX, dXi);
+    if (!ok) break;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        F[i * 3 + j] = (i == j ? 1.0 : 0.0) + dU[i * 3 + 0] * dXi[0 * 3 + j] + dU[i * 3 + 1] * dXi[1 * 3 + j] +
+                       dU[i * 3 + 2] * dXi[2 * 3 + j];
+        L[i * 3 + j] = dD[i * 3 + 0] * dXi[0 * 3 + j] + dD[i * 3 + 1] * dXi[1 * 3 + j] + dD[i * 3 + 2] * dXi[2 * 3 + j];
+      }
+    if (A.F0)
+      for (int i = 0; i < 9; i++) F[i] += A.F0[i];
+    const double J = det3(F);
+    ok = J > 0.0 && inv3(F, Fi);
+    if (!ok) break;
+    const double w = detJ * A.shp.w[q];
+    double tr = 0.0;
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) tr += L[i * 3 + j] * Fi[j * 3 + i];
+    W += w;
+    SJ += w * J;
+    Kdu += w * J * tr;
+  }
+  if (!ok) {
+    atomicAdd(&A.status[0], 1ull);
+    dP[e] = dtheta[e] = 0.0;
+    return;
+  }
+  const double th = A.tf_theta[e], P = A.tf_P[e];
+  double dUv, d2U;
+  vol_derivs(A.mat.vol_pot, th, dUv, d2U);
+  const double dth = (Kdu + SJ - th * W) / W;
+  dtheta[e] = dth;
+  dP[e] = A.mat.kappa * dUv - P + A.mat.kappa * d2U * dth;
 }
 
 }  // namespace pgb

@@ -84,6 +84,12 @@ struct pgfem_gpu_ctx {
   int ngroups = 0;
   unsigned *sched_ticket = nullptr;
   unsigned *p2m_ticket = nullptr;  // tile counter of the quadratic-tet assembly
+  // three-field (CM3F) element: pressure and volume per element (element
+  // order), the expanded displacement increment of the local update, and the
+  // record width the point records were allocated with
+  int three_field = 0;
+  double *tf_P = nullptr, *tf_theta = nullptr, *tf_dunode = nullptr, *tf_inc = nullptr;
+  int qrec_fields = 0;
   int sched_epb = 0, sched_grab = 0;  // elements per block (0: default), tiles per steal (0: static)
   // failure-path tests: bound of the hand-off waits, one-shot withheld hand-off
   unsigned long long wait_ns = 2000000000ull;
@@ -313,7 +319,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->qrec, c->eblk, c->perm,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
-                  c->sched_ticket, c->p2m_ticket, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
+                  c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
                   c->nbc_load, c->tr_buf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -384,15 +390,21 @@ int launch_asm(const AsmArgs &a, long nitems, cudaStream_t s) {
 }
 
 // Point updates of all quadrature points into c->qrec (allocated on first use;
-// 40-double records for the tensor-core quadratic-tet kernel, 38 for the
-// linear-tet kernels).
-template <int NNE, int NQP, int MODEL>
+// 26-double records for the tensor-core quadratic-tet kernel, 30 for its
+// three-field form, 38 for the linear-tet kernels).
+template <int NNE, int NQP, int MODEL, bool TF = false>
 int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   constexpr bool YREC = NNE == 10;
+  const int nf = YREC ? yrec_fields(TF) : kQRec;
+  if (c->qrec && c->qrec_fields < nf) {  // a wider record than allocated
+    cudaFree(c->qrec);
+    c->qrec = nullptr;
+  }
   if (!c->qrec) {  // the tiled layout of the 10-node records is padded to whole tiles
     const size_t npts = YREC ? (size_t)((c->nqp + kMPtsT - 1) / kMPtsT) * kMPtsT : (size_t)c->nqp;
-    int r = dalloc(c, &c->qrec, (size_t)(YREC ? kYRec : kQRec) * npts);
+    int r = dalloc(c, &c->qrec, (size_t)nf * npts);
     if (r) return r;
+    c->qrec_fields = nf;
   }
   QpArgs q{};
   q.X = c->X;
@@ -411,7 +423,9 @@ int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   if (YREC) q.perm = c->perm;
   q.mat = c->mat;
   q.shp = c->shp;
-  k_qp_update<NNE, NQP, MODEL, YREC><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
+  q.tf_P = c->tf_P;
+  q.tf_theta = c->tf_theta;
+  k_qp_update<NNE, NQP, MODEL, YREC, TF><<<(unsigned)((c->nqp + 127) / 128), 128, 0, s>>>(q);
   CK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }
@@ -419,21 +433,22 @@ int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
 // quadratic tets in two kernels: point updates into c->qrec (40-double
 // records; K zeroed meanwhile on the context's second stream), then the
 // tensor-core element assembly from the records
-template <int MODEL>
+template <int MODEL, bool TF = false>
 int launch_p2m(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
+  if (!TF && MODEL == 0 && c->three_field) return launch_p2m<0, true>(c, a0, s);
   CK(cudaEventRecord(c->zfork, s));
   CK(cudaStreamWaitEvent(c->zstream, c->zfork, 0));
   CK(cudaMemsetAsync(a0.K, 0, sizeof(double) * c->nnz, c->zstream));
   CK(cudaMemsetAsync(c->p2m_ticket, 0, sizeof(unsigned), c->zstream));
   CK(cudaEventRecord(c->zjoin, c->zstream));
-  if (int r = launch_qp_update<10, 4, MODEL>(c, s)) return r;
+  if (int r = launch_qp_update<10, 4, MODEL, TF>(c, s)) return r;
   CK(cudaStreamWaitEvent(s, c->zjoin, 0));
   AsmArgs a = a0;
   a.qrec = c->qrec;
   a.eblk = c->eblk;
   a.ticket = c->p2m_ticket;
-  const size_t smem = p2m_smem_bytes();
-  auto kern = k_assemble_p2m<MODEL>;
+  const size_t smem = p2m_smem_bytes(TF);
+  auto kern = k_assemble_p2m<MODEL, TF>;
   static bool attr_set = false;
   if (!attr_set) {
     CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -723,6 +738,13 @@ bool uses_p2m(const pgfem_gpu_ctx *c) {
 // One assembly on device buffers (zeroing R and K first).
 int assemble_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc, double *d_R,
                     double *d_K, cudaStream_t s, double dt = 0.0) {
+  if (c->three_field) {  // the three-field element runs the tensor-core path only
+    if (!d_R || !uses_p2m(c)) return PGFEM_GPU_EINVAL;
+    if (!d_K) {  // residual only: the stiffness goes to a scratch K
+      if (int r = ensure_K_scratch(c)) return r;
+      d_K = c->d_K;
+    }
+  }
   if (d_R) CK(cudaMemsetAsync(d_R, 0, sizeof(double) * c->ndof, s));
   // the tensor-core quadratic-tet path zeroes K itself, beside its point kernel
   if (d_K && !(uses_p2m(c) && d_R)) CK(cudaMemsetAsync(d_K, 0, sizeof(double) * c->nnz, s));
@@ -1073,6 +1095,99 @@ int pgfem_gpu_destroy(pgfem_gpu_ctx *c) {
 int pgfem_gpu_set_scatter_mode(pgfem_gpu_ctx *c, int mode) {
   if (!c || (mode != PGFEM_SCATTER_ATOMIC && mode != PGFEM_SCATTER_COLOUR)) return PGFEM_GPU_EINVAL;
   c->scatter_mode = mode;
+  return PGFEM_GPU_OK;
+}
+
+// ---- three-field (CM3F) element -------------------------------------------
+
+static int ensure_scratch(pgfem_gpu_ctx *c, bool wantK);
+
+int pgfem_gpu_set_three_field(pgfem_gpu_ctx *c, const double *P, const double *theta) {
+  if (!c) return PGFEM_GPU_EINVAL;
+  if (!P && !theta) {
+    c->three_field = 0;
+    return PGFEM_GPU_OK;
+  }
+  if (!P || !theta) return PGFEM_GPU_EINVAL;
+  if (c->nne != 10 || c->model != PGFEM_MODEL_HE || !uses_p2m(c) || c->elem_group) return PGFEM_GPU_EINVAL;
+  for (long e = 0; e < c->ne; e++)
+    if (!(theta[e] > 0.0) || !std::isfinite(theta[e]) || !std::isfinite(P[e])) return PGFEM_GPU_EINVAL;
+  int r;
+  if (!c->tf_P && ((r = dalloc(c, &c->tf_P, c->ne)) || (r = dalloc(c, &c->tf_theta, c->ne)))) return r;
+  CK(cudaMemcpyAsync(c->tf_P, P, sizeof(double) * c->ne, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->tf_theta, theta, sizeof(double) * c->ne, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->three_field = 1;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_three_field_enabled(const pgfem_gpu_ctx *c) { return c && c->three_field ? 1 : 0; }
+
+// The local update on device buffers: increments into d_out (2 ne: dP then
+// d_theta), or, with d_out NULL, added to the context's P and theta.
+__global__ void k_tf_apply(long ne, const double *inc, double *P, double *theta) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  P[e] += inc[e];
+  theta[e] += inc[ne + e];
+}
+
+int pgfem_gpu_three_field_update_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc,
+                                        const double *d_du, double *d_out, void *stream) {
+  if (!c || !c->three_field || (c->ndof && (!d_u || !d_du)) || (c->npres && !d_presc)) return PGFEM_GPU_EINVAL;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int r;
+  if (!c->tf_dunode && ((r = dalloc(c, &c->tf_dunode, 3 * c->nn)) || (r = dalloc(c, &c->tf_inc, 2 * c->ne))))
+    return r;
+  const long n3 = 3 * c->nn;
+  k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_u, d_presc, c->unode);
+  k_expand_u<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(c->dof, c->nn, d_du, nullptr, c->tf_dunode);
+  QpArgs q{};
+  q.X = c->X;
+  q.unode = c->unode;
+  q.conn = c->conn;
+  q.nn = c->nn;
+  q.ne = c->ne;
+  q.F0 = c->F0;
+  q.status = c->status;
+  q.mat = c->mat;
+  q.shp = c->shp;
+  q.tf_P = c->tf_P;
+  q.tf_theta = c->tf_theta;
+  double *inc = d_out ? d_out : c->tf_inc;
+  const unsigned g = (unsigned)((c->ne + 127) / 128);
+  k_tf_update<<<g, 128, 0, s>>>(q, c->tf_dunode, inc, inc + c->ne);
+  if (!d_out) k_tf_apply<<<g, 128, 0, s>>>(c->ne, inc, c->tf_P, c->tf_theta);
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_three_field_increments(pgfem_gpu_ctx *c, const double *u, const double *presc, const double *du,
+                                     double *dP, double *dtheta, pgfem_gpu_status *st) {
+  if (!c || !c->three_field || !u || !du || !dP || !dtheta || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
+  int r = ensure_scratch(c, false);
+  if (r) return r;
+  if (!c->tf_dunode && ((r = dalloc(c, &c->tf_dunode, 3 * c->nn)) || (r = dalloc(c, &c->tf_inc, 2 * c->ne))))
+    return r;
+  // du staged in the residual scratch
+  CK(cudaMemcpyAsync(c->d_u, u, sizeof(double) * c->ndof, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->d_R, du, sizeof(double) * c->ndof, cudaMemcpyHostToDevice, c->stream));
+  if (c->npres)
+    CK(cudaMemcpyAsync(c->d_presc, presc, sizeof(double) * c->npres, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream));
+  if ((r = pgfem_gpu_three_field_update_device(c, c->d_u, c->npres ? c->d_presc : nullptr, c->d_R, c->tf_inc,
+                                               c->stream)))
+    return r;
+  CK(cudaMemcpyAsync(dP, c->tf_inc, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(dtheta, c->tf_inc + c->ne, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, c->stream));
+  return read_status(c, st, false);
+}
+
+int pgfem_gpu_get_three_field(pgfem_gpu_ctx *c, double *P, double *theta) {
+  if (!c || !c->three_field || !P || !theta) return PGFEM_GPU_EINVAL;
+  CK(cudaMemcpyAsync(P, c->tf_P, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(theta, c->tf_theta, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return PGFEM_GPU_OK;
 }
 
@@ -1616,7 +1731,7 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
                                     double *R, double *K, pgfem_gpu_status *st) {
   if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
     return PGFEM_GPU_EINVAL;
-  if (c->model != PGFEM_MODEL_HE || c->nbc_nface || c->F0 || c->elem_group) return PGFEM_GPU_EINVAL;
+  if (c->model != PGFEM_MODEL_HE || c->nbc_nface || c->F0 || c->elem_group || c->three_field) return PGFEM_GPU_EINVAL;
   if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
     return PGFEM_GPU_EINVAL;
   // below the reference's density threshold the element is the quasi-static one
@@ -1700,6 +1815,7 @@ int pgfem_gpu_read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, int clear) {
 static int element_level(pgfem_gpu_ctx *c, long nel, const long *elems, const double *u,
                          const double *presc, double dt, double *lk, double *fe, pgfem_gpu_status *st) {
   if (!c || nel < 0 || (nel && (!elems || !fe)) || !u || (c->npres && !presc)) return PGFEM_GPU_EINVAL;
+  if (c->three_field) return PGFEM_GPU_EINVAL;  // the element-level kernels are one-field
   if (nel == 0) return PGFEM_GPU_OK;
   for (long i = 0; i < nel; i++)
     if (elems[i] < 0 || elems[i] >= c->ne) return PGFEM_GPU_EINVAL;

@@ -899,6 +899,11 @@ int pgfem_gpu_newton_step(pgfem_gpu_ctx *ctx, pgfem_gpu_solver *s, double *d_u, 
       info->converged = 0;
       return PGFEM_GPU_OK;
     }
+    // three-field element: the element pressure and volume follow du
+    // (compute_d_theta_dP at the current u), then u += du
+    if (pgfem_gpu_three_field_enabled(ctx) &&
+        (r = pgfem_gpu_three_field_update_device(ctx, d_u, d_u_presc, s->du, nullptr, stream)))
+      return r;
     k_axpy<<<g, kBlk, 0, st>>>(s->n, 1.0, s->du, d_u, 0);
     SK(cudaGetLastError());
   }

@@ -77,6 +77,11 @@ def lib():
             "pgfem_gpu_assemble_RK_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                           C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_gpu_set_neumann_loads": (C.c_int, [_P, C.c_int, _P]),
+            "pgfem_gpu_set_three_field": (C.c_int, [_P, _P, _P]),
+            "pgfem_gpu_get_three_field": (C.c_int, [_P, _P, _P]),
+            "pgfem_gpu_three_field_enabled": (C.c_int, [_P]),
+            "pgfem_gpu_three_field_increments": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_three_field_update_device": (C.c_int, [_P, _P, _P, _P, _P, _P]),
             "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_device_bytes": (C.c_long, [_P]),
             "pgfem_gpu_nnz": (C.c_long, [_P]),
@@ -301,6 +306,37 @@ class Context:
     def set_neumann_loads(self, load_np1):
         ld = np.ascontiguousarray(np.reshape(load_np1, (-1, 3)), dtype=np.float64)
         _check("pgfem_gpu_set_neumann_loads", lib().pgfem_gpu_set_neumann_loads(self.h, len(ld), _ptr(ld)))
+
+    def set_three_field(self, P, theta):
+        """Three-field (CM3F) element: pressure P and volume theta per element
+        (element order); None, None switches back to the one-field element."""
+        if P is None and theta is None:
+            _check("pgfem_gpu_set_three_field", lib().pgfem_gpu_set_three_field(self.h, None, None))
+            return
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        theta = np.ascontiguousarray(theta, dtype=np.float64)
+        if P.shape != (self.ne,) or theta.shape != (self.ne,):
+            raise ValueError("P and theta need one value per element")
+        _check("pgfem_gpu_set_three_field", lib().pgfem_gpu_set_three_field(self.h, _ptr(P), _ptr(theta)))
+
+    def get_three_field(self):
+        P, theta = np.zeros(self.ne), np.zeros(self.ne)
+        _check("pgfem_gpu_get_three_field", lib().pgfem_gpu_get_three_field(self.h, _ptr(P), _ptr(theta)))
+        return P, theta
+
+    def three_field_enabled(self):
+        return bool(lib().pgfem_gpu_three_field_enabled(self.h))
+
+    def three_field_increments(self, u, du, u_presc=None):
+        """Element pressure / volume increments (dP, dtheta) after the
+        displacement increment du, from the blocks at u."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        dP, dth = np.zeros(self.ne), np.zeros(self.ne)
+        st = Status()
+        _check("pgfem_gpu_three_field_increments", lib().pgfem_gpu_three_field_increments(
+            self.h, _ptr(u), _ptr(self._presc(u_presc)), _ptr(du), _ptr(dP), _ptr(dth), C.byref(st)))
+        return dP, dth, st
 
     def set_scatter_mode(self, mode):
         _check("pgfem_gpu_set_scatter_mode", lib().pgfem_gpu_set_scatter_mode(self.h, mode))

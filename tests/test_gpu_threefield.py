@@ -1,0 +1,167 @@
+"""The three-field (CM3F) element on the GPU against the oracle, through the C
+ABI (pgfem_gpu_set_three_field and the R+K, residual, local-update and Newton
+entry points; the reference's element with one pressure and one volume per
+element, src/constitutive_model.cc:695-881, src/constitutive_model_3f.cc,
+src/condense.cc:300-385).
+
+Quadratic-tet tension boxes of the hyperelastic model, perturbed nodes, element
+pressures and volumes away from their local solution: R and K of the condensed
+element equal the oracle's at 1e-10 (with surface loads too), the residual
+call equals the R of the R+K call, the local update (compute_d_theta_dP)
+equals the oracle's, and the device Newton step -- local update after each
+solve -- follows the oracle's Newton loop to the same displacements,
+pressures and volumes.  The calls the three-field element does not cover are
+rejected."""
+import numpy as np
+import pytest
+from scipy.sparse import csr_matrix
+from scipy.sparse.linalg import spsolve
+
+import oracle
+import pgfem_gpu as pg
+import workloads as wl
+from test_gpu_parity import check_K, check_R
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(n=3, seed=5, vol_pot=99, curve=True):
+    p = wl.tension(n=n, nne=10, model="he", stretch=0.01, predictor=True)
+    p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.45, vol_pot=vol_pot)
+    rng = np.random.default_rng(seed)
+    if curve:
+        p.X = p.X + 0.02 / n * rng.uniform(-1, 1, p.X.shape)
+    ne = p.conn.shape[0]
+    P = 50.0 * rng.uniform(-1, 1, ne)
+    th = 1.0 + 0.01 * rng.uniform(-1, 1, ne)
+    return p, P, th
+
+
+@pytest.mark.parametrize("vol_pot", [99, 2, 3])
+def test_R_K_match_oracle(gpu, vol_pot):
+    p, P, th = _case(vol_pot=vol_pot)
+    ctx = p.context()
+    ctx.set_three_field(P, th)
+    assert ctx.three_field_enabled()
+    R, K, st = ctx.assemble_RK(p.u, p.u_presc)
+    assert st.ok(), st.as_dict()
+    Po, mat = oracle.from_workload(p)
+    err, Ro, Ko = Po.assemble_3f(mat, p.u, P, th, u_presc=p.u_presc)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    # the condensation carries weight: the one-field element differs
+    _, R1, K1, _ = Po.assemble(mat, p.u, p.u_presc)
+    assert np.linalg.norm(R1 - Ro) > 1e-3 * np.linalg.norm(Ro)
+    # the residual call
+    Rr, st = ctx.assemble_R(p.u, p.u_presc)
+    assert st.ok()
+    check_R(Rr, Ro)
+    # P and theta read back; switching back gives the one-field element
+    Pg, thg = ctx.get_three_field()
+    assert np.array_equal(Pg, P) and np.array_equal(thg, th)
+    ctx.set_three_field(None, None)
+    R1g, _ = ctx.assemble_R(p.u, p.u_presc)
+    check_R(R1g, R1)
+    ctx.close()
+
+
+def test_with_surface_loads(gpu):
+    p, P, th = _case(seed=9)
+    el, fc = wl.box_faces(p.X, p.conn, 2, 1.0)
+    p.X = p.X  # faces picked before any further change
+    ft = np.zeros(len(el), dtype=np.int32)
+    ctx = p.context()
+    ctx.set_neumann(el, fc, ft, np.array([1]), np.array([[30.0, 0.0, 0.0]]))
+    ctx.set_three_field(P, th)
+    R, K, st = ctx.assemble_RK(p.u, p.u_presc)
+    assert st.ok()
+    Po, mat = oracle.from_workload(p)
+    Po.set_neumann(el, fc, np.ones(len(el), dtype=np.int64), np.tile([30.0, 0.0, 0.0], (len(el), 1)))
+    err, Ro, Ko = Po.assemble_3f(mat, p.u, P, th, u_presc=p.u_presc)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    ctx.close()
+
+
+def test_local_update_matches_oracle(gpu):
+    p, P, th = _case(seed=2)
+    ctx = p.context()
+    ctx.set_three_field(P, th)
+    du = 1e-3 * np.random.default_rng(4).uniform(-1, 1, p.ndof)
+    dP, dth, st = ctx.three_field_increments(p.u, du, p.u_presc)
+    assert st.ok()
+    Po, mat = oracle.from_workload(p)
+    err, dPo, dtho = Po.update_3f(mat, p.u, du, P, th, u_presc=p.u_presc)
+    assert err == 0
+    assert np.abs(dP - dPo).max() <= 1e-10 * np.abs(dPo).max()
+    assert np.abs(dth - dtho).max() <= 1e-10 * np.abs(dtho).max()
+    ctx.close()
+
+
+def _oracle_newton(Po, mat, u, u_presc, P, th, iter_max=15, nor_min=1e-10):
+    u, P, th = u.copy(), P.copy(), th.copy()
+    hist, NORM = [], 1.0
+    for it in range(iter_max + 1):
+        err, R, K = Po.assemble_3f(mat, u, P, th, u_presc=u_presc)
+        assert err == 0
+        nor2 = float(np.linalg.norm(R))
+        NORM = nor2 if it == 0 else NORM
+        hist.append(nor2 / NORM)
+        if hist[-1] <= nor_min:
+            return u, P, th, hist, True
+        du = spsolve(csr_matrix((K, Po.Ai, Po.Ap), shape=(Po.ndof, Po.ndof)).tocsc(), -R)
+        err, dP, dth = Po.update_3f(mat, u, du, P, th, u_presc=u_presc)
+        assert err == 0
+        P, th, u = P + dP, th + dth, u + du
+    return u, P, th, hist, False
+
+
+def test_device_newton_matches_oracle(gpu):
+    import torch
+    p, _, _ = _case(n=3, seed=3, curve=False)
+    ne = p.conn.shape[0]
+    P0, th0 = np.zeros(ne), np.ones(ne)
+    Po, mat = oracle.from_workload(p)
+    uo, Pio, tho, ho, ok = _oracle_newton(Po, mat, p.u, p.u_presc, P0, th0)
+    assert ok and len(ho) >= 3
+    ctx = p.context()
+    ctx.set_three_field(P0, th0)
+    s = pg.Solver(p.Ap, p.Ai, p.ndof, maxit=20000, kdim=100, tol=1e-12)
+    du = torch.from_numpy(p.u.copy()).cuda()
+    dp = torch.from_numpy(p.u_presc.copy()).cuda()
+    info = s.newton_step(ctx, du.data_ptr(), dp.data_ptr(), iter_max=15, nor_min=1e-10)
+    assert info.converged and not info.lin_failed and info.elem_failures == 0
+    h = info.history()
+    assert len(h) == len(ho), (h, ho)
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - uo) <= 1e-8 * np.linalg.norm(uo)
+    Pg, thg = ctx.get_three_field()
+    assert np.abs(Pg - Pio).max() <= 1e-7 * np.abs(Pio).max()
+    assert np.abs(thg - tho).max() <= 1e-10
+    # at the solution the local constraints hold: theta = mean J, P = kappa U'(theta)
+    kap = 200e3 / (3 * (1 - 2 * 0.45))
+    assert np.abs(Pg - kap * (thg - 1.0)).max() <= 1e-6 * np.abs(Pg).max()
+    ctx.close()
+
+
+def test_rejections(gpu):
+    p1 = wl.he_p1(n=2, seed=1)
+    c1 = p1.context()
+    with pytest.raises(pg.PgfemError):
+        c1.set_three_field(np.zeros(p1.ne), np.ones(p1.ne))
+    c1.close()
+    pj = wl.j2_p2(n=2, seed=1, stretch=1e-3)
+    cj = pj.context()
+    with pytest.raises(pg.PgfemError):
+        cj.set_three_field(np.zeros(pj.ne), np.ones(pj.ne))
+    cj.close()
+    p, P, th = _case(n=2)
+    ctx = p.context()
+    with pytest.raises(pg.PgfemError):
+        ctx.set_three_field(P, -th)  # a volume must be positive
+    ctx.set_three_field(P, th)
+    with pytest.raises(pg.PgfemError):
+        ctx.stiffmatel_fd([0], p.u, p.u_presc)
+    ctx.close()
