@@ -214,13 +214,19 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(dev)
     t0 = time.perf_counter()
     he = args.workload == "he_p1"
+    tf = args.workload == "he3f_p2"  # the three-field element on the config-2 mesh
     p = wl.he_p1(n=10, seed=0) if he else wl.j2_p2(n=args.n, seed=1)
+    if tf:
+        p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.45)
+        p.state = None
     log("[rank %d] setup (mesh, DOFs, CSR pattern %d nnz) %.1f s" % (rank, p.nnz, time.perf_counter() - t0))
     t0 = time.perf_counter()
     ctx = p.context()
     log("[rank %d] context (device copy + element->CSR map) %.1f s, %.2f GB on device"
         % (rank, time.perf_counter() - t0, ctx.device_bytes() / 1e9))
     ctx.set_scatter_mode({"atomic": pg.SCATTER_ATOMIC, "colour": pg.SCATTER_COLOUR}[args.scatter])
+    if tf:  # element pressure 0 and volume 1 (the reference's initial values)
+        ctx.set_three_field(np.zeros(p.ne), np.ones(p.ne))
     fp64_peak = pg.fp64_peak_tflops()
     hbm_peak, hbm_src = measured_hbm_gbs()
 
@@ -265,7 +271,7 @@ def run_ours(args, ws, rank, local):
     ms_total = allreduce_max(ms_total, ws)
     ms_step = ms_total / args.steps
     value = ws * p.nqp * args.steps / (ms_total * 1e-3)
-    yielded = None if he else float((ctx.get_state(1)[:, 9] > 0).mean())
+    yielded = None if (he or tf) else float((ctx.get_state(1)[:, 9] > 0).mean())
 
     # end to end through the host-buffer entry point (pinned host memory)
     u_h = torch.from_numpy(p.u).pin_memory().numpy()
@@ -284,7 +290,8 @@ def run_ours(args, ws, rank, local):
     # roofline of the assembly kernels (quadratic tets: the point-update kernel
     # and the R+K assembly kernel together; linear tets: the fused kernel)
     k_ms = kms / max(kcalls, 1)
-    flops = (2.5e3 if he else FLOP_PER_QP) * p.nqp
+    # (the three-field element: the B-form count without the return map)
+    flops = (2.5e3 if he else FLOP_PER_QP - (600.0 if tf else 0.0)) * p.nqp
     nbytes = alg_bytes(p.X.shape[0], p.ndof, p.ne, p.nqp, p.nnz)
     t_fp64 = flops / (fp64_peak * 1e12)
     t_hbm = nbytes / (hbm_peak * 1e9)
@@ -296,8 +303,10 @@ def run_ours(args, ws, rank, local):
                 "peak_source": hbm_src}
     roof["frac"] = roof["achieved"] / roof["peak"]
     roof["kernel"] = ("k_assemble<4,1,0> (fused R+K)" if he else
+                      "k_qp_update<10,4,0,1,1> + k_assemble_p2m<0,1> (three-field point updates, then the condensed "
+                      "R+K on the FP64 tensor cores)" if tf else
                       "k_qp_update<10,4,1,1> + k_assemble_p2m<1> (point updates, then R+K on the FP64 tensor cores)")
-    roof["traffic"] = None if he else traffic_per_launch()
+    roof["traffic"] = None if (he or tf) else traffic_per_launch()
     roof["kernel_ms"] = k_ms
     roof["roofline_ms"] = 1e3 * max(t_fp64, t_hbm)
     roof["frac_of_roofline_step"] = max(t_fp64, t_hbm) / (ms_step * 1e-3)
@@ -311,6 +320,10 @@ def run_ours(args, ws, rank, local):
            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded splitmix64)",
            "config": {"workload": ("compressible neo-Hookean, linear tets, 10^3 cells x 6 (%d elements, %d DOFs, "
                                    "%d CSR non-zeros), one R+K iterate" % (p.ne, p.ndof, p.nnz)) if he else
+                                  ("three-field (CM3F) compressible neo-Hookean, one pressure and one volume per "
+                                   "element, quadratic tets, %d^3 cells x 6 (%d elements, %d quadrature points, %d "
+                                   "DOFs, %d CSR non-zeros), one condensed R+K iterate" %
+                                   (args.n, p.ne, p.nqp, p.ndof, p.nnz)) if tf else
                                   ("J2 finite-strain plasticity, quadratic tets, %d^3 cells x 6 (%d elements, "
                                    "%d quadrature points, %d DOFs, %d CSR non-zeros), one R+K iterate" %
                                    (args.n, p.ne, p.nqp, p.ndof, p.nnz)),
@@ -322,7 +335,7 @@ def run_ours(args, ws, rank, local):
            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * p.ndof,
                    "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "steps": n_e2e},
            "gpu_launches": args.steps * ctx.launches_per_assembly()}
-    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline and not tf:
         v, S, t = cpu_baseline_sample(p, args.cpu_seconds, nthreads=1)
         out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                                "sample": "first %d elements (%d qp) of the same workload, %.1f s, reference "
@@ -947,7 +960,7 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour"])
-    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch",
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he3f_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch",
                                                          "nr_step"])
     ap.add_argument("--nr-n", type=int, default=16)
     ap.add_argument("--nr-stretch", type=float, default=0.003)
