@@ -158,8 +158,9 @@ int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *ctx, int nfeature, const double *
  * src/constitutive_model.cc:695-881 with CM_ThreeField,
  * src/constitutive_model_3f.cc:185-491, and the static condensation
  * condense_K_3F_to_1F / condense_F_3F_to_1F, src/condense.cc:300-385), for
- * quadratic tets and the hyperelastic model on the default R+K path (atomic
- * scatter), total Lagrangian, quasi-static.  set_three_field gives P and
+ * quadratic tets and the hyperelastic model -- and this library's J2 model,
+ * whose isochoric return map is unchanged by the element's volume -- on the
+ * default R+K path (atomic scatter), total Lagrangian, quasi-static.  set_three_field gives P and
  * theta per element (host arrays of ne, element order; theta > 0) and switches
  * every later R+K and residual call of the context to the condensed
  * three-field element; NULL, NULL switches back.  PGFEM_GPU_EINVAL for other

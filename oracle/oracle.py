@@ -61,9 +61,9 @@ def lib():
                                                _P, C.c_int, _P]),
             "orc_assemble_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                  C.c_double, C.c_double, _P, _P]),
-            "orc_element_3f": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, C.c_double, _P, _P, _P]),
-            "orc_assemble_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P]),
-            "orc_update_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P]),
+            "orc_element_3f": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, C.c_double, _P, _P, _P, _P, _P]),
+            "orc_assemble_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+            "orc_update_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -200,31 +200,38 @@ class Problem:
         err = lib().orc_element(C.byref(self.s), C.byref(mat), e, _p(u_e), dt, _p(sn), _p(snp1), _p(fe), _p(lk))
         return err, fe, lk, snp1
 
-    def element_3f(self, mat, e, u_e, P, theta, want_K=True):
-        """Three-field (CM3F) element of the hyperelastic model: (err, fe, lk,
-        blocks) with blocks = (fp, ft, Ktp, Ktt, Kup[3 nne])."""
+    def element_3f(self, mat, e, u_e, P, theta, want_K=True, state_n=None):
+        """Three-field (CM3F) element of the hyperelastic or J2 model: (err, fe,
+        lk, blocks) with blocks = (fp, ft, Ktp, Ktt, Kup[3 nne])."""
         nd = self.conn.shape[1] * 3
         fe = np.zeros(nd)
         lk = np.zeros((nd, nd)) if want_K else None
         blk = np.zeros(4 + nd)
         u_e = np.ascontiguousarray(u_e, dtype=np.float64)
-        err = lib().orc_element_3f(C.byref(self.s), C.byref(mat), e, _p(u_e), float(P), float(theta), _p(fe), _p(lk),
-                                   _p(blk))
+        sn = None if state_n is None else np.ascontiguousarray(state_n, dtype=np.float64)
+        err = lib().orc_element_3f(C.byref(self.s), C.byref(mat), e, _p(u_e), float(P), float(theta), _p(sn), None,
+                                   _p(fe), _p(lk), _p(blk))
         return err, fe, lk, (blk[0], blk[1], blk[2], blk[3], blk[4:].copy())
 
-    def assemble_3f(self, mat, u, P, theta, u_presc=None, want_K=True):
-        """Global R, K of the three-field element (P, theta per element)."""
+    def assemble_3f(self, mat, u, P, theta, u_presc=None, want_K=True, state_n=None):
+        """Global R, K of the three-field element (P, theta per element); with a
+        J2 state at t_n also the state at t_{n+1}: (err, R, K[, state_np1])."""
         R = np.zeros(self.ndof)
         K = np.zeros(self.nnz) if want_K else None
-        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None for x in (u, u_presc, P, theta)]
-        err = lib().orc_assemble_3f(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(R), _p(K))
-        return err, R, K
+        ns = state_size(mat.model)
+        nint = lib().orc_nint(self.conn.shape[1])
+        snp1 = np.zeros((self.conn.shape[0] * nint, ns)) if ns else None
+        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None
+             for x in (u, u_presc, P, theta, state_n)]
+        err = lib().orc_assemble_3f(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(snp1), _p(R), _p(K))
+        return (err, R, K) if state_n is None else (err, R, K, snp1)
 
-    def update_3f(self, mat, u, du, P, theta, u_presc=None):
+    def update_3f(self, mat, u, du, P, theta, u_presc=None, state_n=None):
         """Element pressure / volume increments after the displacement increment du."""
         ne = self.conn.shape[0]
         dP, dth = np.zeros(ne), np.zeros(ne)
-        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None for x in (u, u_presc, du, P, theta)]
+        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None
+             for x in (u, u_presc, du, P, theta, state_n)]
         err = lib().orc_update_3f(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(dP), _p(dth))
         return err, dP, dth
 

@@ -946,8 +946,11 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 #include "orc_bform.inc"
 
 // ---------------------------------------------------------------------------
-// Three-field (CM3F) element of the hyperelastic model, quasi-static, total
-// Lagrangian, one rank: the element loop of src/constitutive_model.cc:
+// Three-field (CM3F) element of the hyperelastic model (and of this library's
+// J2 model, whose isochoric return map gives the deviatoric S, L from the
+// state at t_n, the state at t_{n+1} written to state_np1; the integration's
+// volume factor (theta / J)^(1/3), src/constitutive_model.cc:813-816, leaves an
+// isochoric update unchanged), quasi-static, total Lagrangian, one rank: the element loop of src/constitutive_model.cc:
 // 695-881 with CM_ThreeField (src/constitutive_model_3f.cc:47-491) and the
 // condensation condense_K_3F_to_1F / condense_F_3F_to_1F
 // (src/condense.cc:300-385).  CM3F carries one pressure P and one volume
@@ -972,8 +975,11 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 // blk (may be NULL) receives fp, ft, Ktp, Ktt and Kup[nd].
 // ---------------------------------------------------------------------------
 extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
-                              double Pe, double theta, double *fe, double *lk, double *blk) {
-  if (mat->model != ORC_MODEL_HE) return 1;
+                              double Pe, double theta, const double *state_n, double *state_np1, double *fe,
+                              double *lk, double *blk) {
+  if (mat->model != ORC_MODEL_HE && mat->model != ORC_MODEL_J2) return 1;
+  if (mat->model == ORC_MODEL_J2 && !state_n) return 1;
+  const int ns = orc_state_size(mat->model);
   const int nne = P->nne, nd = nne * 3;
   Quad qr = quad_rule(nne);
   double Xe[30];
@@ -1000,8 +1006,14 @@ extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, lon
       for (int i = 0; i < 9; i++) F[i] += P->F0[i];
     const double J = det3x3(F);
     if (J <= 0.0 || inv3x3(F, Fi)) { err += 1; break; }
-    matmulTN(F, F, C);
-    he_stress_stiffness(dev, C, J, S, lk ? L : nullptr);
+    if (mat->model == ORC_MODEL_J2) {
+      double stmp[10];
+      j2_update(dev, mat->sigma_y, mat->H, F, state_n + (long)ip * ns,
+                state_np1 ? state_np1 + (long)ip * ns : stmp, S, lk ? L : nullptr);
+    } else {
+      matmulTN(F, F, C);
+      he_stress_stiffness(dev, C, J, S, lk ? L : nullptr);
+    }
     // per (a, b): Psi = sym(G^T F) and tr(G F^-1), G_ij = delta_ib dN_a,j
     std::vector<double> Psi(nd * 9), trGFi(nd), GFi(nd * 9);
     for (int a = 0; a < nne; a++)
@@ -1069,14 +1081,17 @@ extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, lon
 
 // Global assembly of the three-field element: P_e, theta_e per element.
 extern "C" int orc_assemble_3f(const orc_problem *P, const orc_material *mat, const double *u,
-                               const double *u_presc, const double *Pe, const double *theta, double *R,
-                               double *K) {
+                               const double *u_presc, const double *Pe, const double *theta,
+                               const double *state_n, double *state_np1, double *R, double *K) {
   const int nd = P->nne * 3;
+  const int nint = orc_nint(P->nne), ns = orc_state_size(mat->model);
   return run_elements(P, 0, P->ne, 1, [&](long e) -> int {
     double ue[30], fe[30];
     std::vector<double> lk(K ? nd * nd : 0);
     gather_u(P, e, u, u_presc, ue);
-    int err = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], fe, K ? lk.data() : nullptr, nullptr);
+    const double *sn = state_n ? state_n + e * nint * ns : nullptr;
+    double *snp1 = state_np1 ? state_np1 + e * nint * ns : nullptr;
+    int err = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], sn, snp1, fe, K ? lk.data() : nullptr, nullptr);
     if (!err) scatter(P, e, fe, K ? lk.data() : nullptr, R, K);
     return err;
   });
@@ -1089,14 +1104,16 @@ extern "C" int orc_assemble_3f(const orc_problem *P, const orc_material *mat, co
 //   d_theta = -Kpt^-1 (Kpu du + fp),  dP = -Ktp^-1 (ft + Ktu du + Ktt d_theta).
 extern "C" int orc_update_3f(const orc_problem *P, const orc_material *mat, const double *u,
                              const double *u_presc, const double *du, const double *Pe, const double *theta,
-                             double *dP, double *dtheta) {
+                             const double *state_n, double *dP, double *dtheta) {
   const int nd = P->nne * 3;
+  const int nint = orc_nint(P->nne), ns = orc_state_size(mat->model);
   int err = 0;
   for (long e = 0; e < P->ne; e++) {
     double ue[30], due[30], fe[30], blk[4 + 30];
     gather_u(P, e, u, u_presc, ue);
     gather_u(P, e, du, nullptr, due);
-    const int r = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], fe, nullptr, blk);
+    const double *sn = state_n ? state_n + e * nint * ns : nullptr;
+    const int r = orc_element_3f(P, mat, e, ue, Pe[e], theta[e], sn, nullptr, fe, nullptr, blk);
     if (r) { err += r; continue; }
     const double fp = blk[0], ft = blk[1], Ktp = blk[2], Ktt = blk[3], Kpt = Ktp;
     double Kpu_du = 0.0;

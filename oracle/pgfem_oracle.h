@@ -115,17 +115,21 @@ int orc_assemble(const orc_problem *P, const orc_material *mat,
                  const double *state_n, double *state_np1, double *R,
                  double *K, long e0, long e1, int nthreads, int *iters);
 
-/* Three-field (CM3F) element of the hyperelastic model (one pressure and one
- * volume per element, condensed): element residual/stiffness at (u_e, P,
+/* Three-field (CM3F) element of the hyperelastic and J2 models (one pressure
+ * and one volume per element, condensed; J2 state per point at t_n in, t_{n+1}
+ * out, as in orc_element): element residual/stiffness at (u_e, P,
  * theta); blk (may be NULL) receives fp, ft, Ktp, Ktt, Kup[3 nne]. */
 int orc_element_3f(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
-                   double Pe, double theta, double *fe, double *lk, double *blk);
+                   double Pe, double theta, const double *state_n, double *state_np1, double *fe,
+                   double *lk, double *blk);
 /* Its global assembly (R, K accumulated; K may be NULL), and the element
  * pressure / volume increments after a displacement increment du. */
 int orc_assemble_3f(const orc_problem *P, const orc_material *mat, const double *u,
-                    const double *u_presc, const double *Pe, const double *theta, double *R, double *K);
+                    const double *u_presc, const double *Pe, const double *theta, const double *state_n,
+                    double *state_np1, double *R, double *K);
 int orc_update_3f(const orc_problem *P, const orc_material *mat, const double *u, const double *u_presc,
-                  const double *du, const double *Pe, const double *theta, double *dP, double *dtheta);
+                  const double *du, const double *Pe, const double *theta, const double *state_n,
+                  double *dP, double *dtheta);
 
 /* Same element integrals in the algebraically identical B-matrix form (the
  * "best CPU algorithm" baseline).  Same arguments as orc_assemble. */

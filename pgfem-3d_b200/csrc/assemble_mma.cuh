@@ -83,8 +83,8 @@ struct QpArgs {
   const int *perm;
   Mat mat;
   ShapeTable shp;
-  // three-field element (10-node records, hyperelastic model): the pressure
-  // and the volume of each element (element order)
+  // three-field element (10-node records, hyperelastic and J2 models): the
+  // pressure and the volume of each element (element order)
   const double *tf_P, *tf_theta;
 };
 
@@ -610,7 +610,7 @@ __global__ void __launch_bounds__(kMThreads, 4) k_assemble_p2m(const AsmArgs arg
 }
 
 // Three-field element (one pressure P and one volume theta per element,
-// quadratic tets, hyperelastic model): the local update after a displacement
+// quadratic tets, hyperelastic and J2 models): the local update after a displacement
 // increment du (compute_d_theta_dP, src/constitutive_model_3f.cc:494-549, with
 // the blocks at u; thread per element): with W = sum_q w, fp = sum_q w J -
 // theta W and Kpu du = sum_q w J tr(Grad(du) F^-1),

@@ -435,7 +435,7 @@ int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
 // tensor-core element assembly from the records
 template <int MODEL, bool TF = false>
 int launch_p2m(pgfem_gpu_ctx *c, const AsmArgs &a0, cudaStream_t s) {
-  if (!TF && MODEL == 0 && c->three_field) return launch_p2m<0, true>(c, a0, s);
+  if (!TF && c->three_field) return launch_p2m<MODEL, true>(c, a0, s);
   CK(cudaEventRecord(c->zfork, s));
   CK(cudaStreamWaitEvent(c->zstream, c->zfork, 0));
   CK(cudaMemsetAsync(a0.K, 0, sizeof(double) * c->nnz, c->zstream));
@@ -1109,7 +1109,9 @@ int pgfem_gpu_set_three_field(pgfem_gpu_ctx *c, const double *P, const double *t
     return PGFEM_GPU_OK;
   }
   if (!P || !theta) return PGFEM_GPU_EINVAL;
-  if (c->nne != 10 || c->model != PGFEM_MODEL_HE || !uses_p2m(c) || c->elem_group) return PGFEM_GPU_EINVAL;
+  if (c->nne != 10 || (c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_J2) || !uses_p2m(c) ||
+      c->elem_group)
+    return PGFEM_GPU_EINVAL;
   for (long e = 0; e < c->ne; e++)
     if (!(theta[e] > 0.0) || !std::isfinite(theta[e]) || !std::isfinite(P[e])) return PGFEM_GPU_EINVAL;
   int r;

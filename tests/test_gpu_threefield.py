@@ -4,7 +4,8 @@ entry points; the reference's element with one pressure and one volume per
 element, src/constitutive_model.cc:695-881, src/constitutive_model_3f.cc,
 src/condense.cc:300-385).
 
-Quadratic-tet tension boxes of the hyperelastic model, perturbed nodes, element
+Quadratic-tet tension boxes of the hyperelastic model (and of this library's
+J2 model, state at t_n given, yielding), perturbed nodes, element
 pressures and volumes away from their local solution: R and K of the condensed
 element equal the oracle's at 1e-10 (with surface loads too), the residual
 call equals the R of the R+K call, the local update (compute_d_theta_dP)
@@ -100,11 +101,12 @@ def test_local_update_matches_oracle(gpu):
     ctx.close()
 
 
-def _oracle_newton(Po, mat, u, u_presc, P, th, iter_max=15, nor_min=1e-10):
+def _oracle_newton(Po, mat, u, u_presc, P, th, iter_max=15, nor_min=1e-10, state_n=None):
     u, P, th = u.copy(), P.copy(), th.copy()
     hist, NORM = [], 1.0
     for it in range(iter_max + 1):
-        err, R, K = Po.assemble_3f(mat, u, P, th, u_presc=u_presc)
+        res = Po.assemble_3f(mat, u, P, th, u_presc=u_presc, state_n=state_n)
+        err, R, K = res[:3]
         assert err == 0
         nor2 = float(np.linalg.norm(R))
         NORM = nor2 if it == 0 else NORM
@@ -112,7 +114,7 @@ def _oracle_newton(Po, mat, u, u_presc, P, th, iter_max=15, nor_min=1e-10):
         if hist[-1] <= nor_min:
             return u, P, th, hist, True
         du = spsolve(csr_matrix((K, Po.Ai, Po.Ap), shape=(Po.ndof, Po.ndof)).tocsc(), -R)
-        err, dP, dth = Po.update_3f(mat, u, du, P, th, u_presc=u_presc)
+        err, dP, dth = Po.update_3f(mat, u, du, P, th, u_presc=u_presc, state_n=state_n)
         assert err == 0
         P, th, u = P + dP, th + dth, u + du
     return u, P, th, hist, False
@@ -152,11 +154,6 @@ def test_rejections(gpu):
     with pytest.raises(pg.PgfemError):
         c1.set_three_field(np.zeros(p1.ne), np.ones(p1.ne))
     c1.close()
-    pj = wl.j2_p2(n=2, seed=1, stretch=1e-3)
-    cj = pj.context()
-    with pytest.raises(pg.PgfemError):
-        cj.set_three_field(np.zeros(pj.ne), np.ones(pj.ne))
-    cj.close()
     p, P, th = _case(n=2)
     ctx = p.context()
     with pytest.raises(pg.PgfemError):
@@ -164,4 +161,48 @@ def test_rejections(gpu):
     ctx.set_three_field(P, th)
     with pytest.raises(pg.PgfemError):
         ctx.stiffmatel_fd([0], p.u, p.u_presc)
+    ctx.close()
+
+
+def test_j2_R_K_state_match_oracle(gpu):
+    p = wl.j2_p2(n=3, seed=11, stretch=4e-3, perturb=5e-3)
+    rng = np.random.default_rng(21)
+    P = 300.0 * rng.uniform(-1, 1, p.ne)
+    th = 1.0 + 0.002 * rng.uniform(-1, 1, p.ne)
+    ctx = p.context()
+    ctx.set_three_field(P, th)
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok(), st.as_dict()
+    Po, mat = oracle.from_workload(p)
+    err, Ro, Ko, so = Po.assemble_3f(mat, p.u, P, th, state_n=p.state)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    sg = ctx.get_state(1)
+    assert np.abs(sg - so).max() <= 1e-10 * np.abs(so).max()
+    assert (so[:, 9] > 0).mean() > 0.3  # points yield
+    ctx.close()
+
+
+def test_j2_device_newton_matches_oracle(gpu):
+    import torch
+    p = wl.tension(n=2, nne=10, model="j2", stretch=0.003, predictor=True)
+    ne = p.conn.shape[0]
+    P0, th0 = np.zeros(ne), np.ones(ne)
+    Po, mat = oracle.from_workload(p)
+    uo, Pio, tho, ho, ok = _oracle_newton(Po, mat, p.u, p.u_presc, P0, th0, state_n=p.state)
+    assert ok
+    ctx = p.context()
+    ctx.set_three_field(P0, th0)
+    s = pg.Solver(p.Ap, p.Ai, p.ndof, maxit=20000, kdim=100, tol=1e-12)
+    du = torch.from_numpy(p.u.copy()).cuda()
+    dp = torch.from_numpy(p.u_presc.copy()).cuda()
+    info = s.newton_step(ctx, du.data_ptr(), dp.data_ptr(), iter_max=15, nor_min=1e-10)
+    assert info.converged and not info.lin_failed and info.elem_failures == 0
+    assert len(info.history()) == len(ho)
+    u = du.cpu().numpy()
+    assert np.linalg.norm(u - uo) <= 1e-8 * np.linalg.norm(uo)
+    Pg, thg = ctx.get_three_field()
+    assert np.abs(Pg - Pio).max() <= 1e-7 * np.abs(Pio).max()
+    assert np.abs(thg - tho).max() <= 1e-10
     ctx.close()

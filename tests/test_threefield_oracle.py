@@ -1,4 +1,5 @@
-"""The three-field (CM3F) element of the oracle on the CPU
+"""The three-field (CM3F) element of the oracle on the CPU (hyperelastic model;
+the J2 model of this library with its isochoric return map)
 (oracle/pgfem_oracle.cpp, orc_element_3f / orc_assemble_3f / orc_update_3f:
 the reference's constitutive-model element with one pressure and one volume
 per element, src/constitutive_model.cc:695-881, src/constitutive_model_3f.cc,
@@ -37,9 +38,9 @@ def _mat(vol_pot=99):
     return oracle.material(oracle.HE, E=200.0, nu=0.45, vol_pot=vol_pot)
 
 
-def _local(P, mat, e, ue):
+def _local(P, mat, e, ue, sn=None):
     """theta* and P* of element e at ue (from the blocks at theta = 0)."""
-    _, _, _, (fp0, ft, Ktp, Ktt, Kup) = P.element_3f(mat, e, ue, 0.0, 0.0, want_K=False)
+    _, _, _, (fp0, ft, Ktp, Ktt, Kup) = P.element_3f(mat, e, ue, 0.0, 0.0, want_K=False, state_n=sn)
     W = -Ktp
     th = fp0 / W  # fp(theta = 0) = sum w J
     kap = mat.E / (3.0 * (1.0 - 2.0 * mat.nu))
@@ -141,3 +142,36 @@ def test_local_update_is_second_order():
     # from arbitrary (P, theta) the correction jumps to the local solution up
     # to the second-order remainder: halving du quarters the error
     assert errs[1] < 0.3 * errs[0]
+
+
+def test_j2_condensed_stiffness_is_derivative_of_condensed_residual():
+    """The J2 model (state at t_n fixed, points yielding): the same identity."""
+    X, conn, ids, ndof, Ap, Ai = _problem(1, 10)
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai)
+    mat = oracle.material(oracle.J2, E=200.0, nu=0.45, sigma_y=0.2, H=5.0)
+    rng = np.random.default_rng(17)
+    e = 3
+    ue = 0.03 * rng.uniform(-1, 1, 30)
+    sn = np.zeros((4, 10))
+    sn[:, [0, 4, 8]] = 1.0
+
+    def g(u):
+        th, pr = _local(P, mat, e, u, sn)
+        err, fe, _, _ = P.element_3f(mat, e, u, pr, th, want_K=False, state_n=sn)
+        assert err == 0
+        return fe
+
+    th, pr = _local(P, mat, e, ue, sn)
+    err, fe, lk, _ = P.element_3f(mat, e, ue, pr, th, state_n=sn)
+    assert err == 0
+    h = 1e-7
+    Kfd = np.zeros((30, 30))
+    for c in range(30):
+        d = np.zeros(30)
+        d[c] = h
+        Kfd[:, c] = (g(ue + d) - g(ue - d)) / (2 * h)
+    assert np.abs(lk - Kfd).max() <= 1e-5 * np.abs(lk).max()
+    # the points yield, and the plastic element differs from the hyperelastic one
+    mat_he = oracle.material(oracle.HE, E=200.0, nu=0.45)
+    _, fe_he, _, _ = P.element_3f(mat_he, e, ue, pr, th, want_K=False)
+    assert np.linalg.norm(fe - fe_he) > 1e-2 * np.linalg.norm(fe)
