@@ -140,10 +140,12 @@ def test_device_newton_matches_oracle(gpu):
     u = du.cpu().numpy()
     assert np.linalg.norm(u - uo) <= 1e-8 * np.linalg.norm(uo)
     Pg, thg = ctx.get_three_field()
-    assert np.abs(Pg - Pio).max() <= 1e-7 * np.abs(Pio).max()
-    assert np.abs(thg - tho).max() <= 1e-10
-    # at the solution the local constraints hold: theta = mean J, P = kappa U'(theta)
+    # theta follows u (1e-8 relative); P = kappa U'(theta) amplifies theta's
+    # difference by kappa
     kap = 200e3 / (3 * (1 - 2 * 0.45))
+    assert np.abs(thg - tho).max() <= 1e-8
+    assert np.abs(Pg - Pio).max() <= 1e-8 * kap
+    # at the solution the local constraints hold: theta = mean J, P = kappa U'(theta)
     assert np.abs(Pg - kap * (thg - 1.0)).max() <= 1e-6 * np.abs(Pg).max()
     ctx.close()
 
@@ -203,6 +205,7 @@ def test_j2_device_newton_matches_oracle(gpu):
     u = du.cpu().numpy()
     assert np.linalg.norm(u - uo) <= 1e-8 * np.linalg.norm(uo)
     Pg, thg = ctx.get_three_field()
-    assert np.abs(Pg - Pio).max() <= 1e-7 * np.abs(Pio).max()
-    assert np.abs(thg - tho).max() <= 1e-10
+    kap = 200e3 / (3 * (1 - 2 * 0.3))
+    assert np.abs(thg - tho).max() <= 1e-8
+    assert np.abs(Pg - Pio).max() <= 1e-8 * kap
     ctx.close()
