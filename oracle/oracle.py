@@ -29,7 +29,7 @@ class OrcProblem(C.Structure):
                 ("X", C.c_void_p), ("conn", C.c_void_p), ("id", C.c_void_p), ("ndof", C.c_long),
                 ("Ap", C.c_void_p), ("Ai", C.c_void_p), ("F0", C.c_void_p), ("R_cp", C.c_void_p),
                 ("nbc_off", C.c_void_p), ("nbc_face", C.c_void_p), ("nbc_type", C.c_void_p),
-                ("nbc_load", C.c_void_p)]
+                ("nbc_load", C.c_void_p), ("nbc_load_n", C.c_void_p), ("nbc_load_nm1", C.c_void_p)]
 
 
 _lib = None
@@ -162,15 +162,17 @@ class Problem:
                             _p(self.conn), _p(self.ids), ndof, _p(self.Ap), _p(self.Ai), _p(self.F0),
                             _p(self.R_cp))
 
-    def set_neumann(self, elem, face, load_type, load):
+    def set_neumann(self, elem, face, load_type, load, load_n=None, load_nm1=None):
         """Surface loads on element faces (the reference's NeumannBoundaryElement
         list, src/PGFem3D_data_structure.cc:825-895, flattened to one entry per
         face): elem (0-based), local face 0..3, number of load values (1 pressure,
-        2..3 traction) and the values at t_{n+1} (nface x 3).  Empty lists clear."""
+        2..3 traction) and the values at t_{n+1} (nface x 3); for the transient
+        element also at t_n and t_{n-1}.  Empty lists clear."""
         elem = np.asarray(elem, dtype=np.int64).ravel()
         if elem.size == 0:
             self.nbc = None
             self.s.nbc_off = self.s.nbc_face = self.s.nbc_type = self.s.nbc_load = None
+            self.s.nbc_load_n = self.s.nbc_load_nm1 = None
             return
         order = np.argsort(elem, kind="stable")
         ne = self.conn.shape[0]
@@ -180,9 +182,12 @@ class Problem:
         face = np.ascontiguousarray(np.asarray(face, dtype=np.int32).ravel()[order])
         ltype = np.ascontiguousarray(np.asarray(load_type, dtype=np.int32).ravel()[order])
         load = np.ascontiguousarray(np.asarray(load, dtype=np.float64).reshape(-1, 3)[order])
-        self.nbc = (off, face, ltype, load)
+        hist = [None if x is None else np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(-1, 3)[order])
+                for x in (load_n, load_nm1)]
+        self.nbc = (off, face, ltype, load, hist)
         self.s.nbc_off, self.s.nbc_face, self.s.nbc_type, self.s.nbc_load = (_p(off), _p(face), _p(ltype),
                                                                              _p(load))
+        self.s.nbc_load_n, self.s.nbc_load_nm1 = _p(hist[0]), _p(hist[1])
 
     @property
     def nnz(self):

@@ -608,6 +608,111 @@ void neumann_faces(const orc_problem *P, long e, const double *Xe, const double 
   }
 }
 
+// Surface loads of the transient element (compute_Neumann_boundary_conditions
+// and compute_Neumann_boundary_conditions_stiffnes_mat with include_inertia,
+// src/fd_residuals.cc:123-273, src/stiffmat_fd.cc:359-500): with the load
+// values P at t_{n+1}, t_n, t_{n-1} (pressure: (p, 0, p), as above) and the
+// displacements at the mid points U_{n+a} = mid(U_n, U_{n+1}),
+// U_{n-1+a} = mid(U_{n-1}, U_n), mid(a, b) = (1 - alpha) a + alpha b,
+//   f[a,i] += N_a w (dt_np1 (1 - alpha) J_{n+a} (F_{n+a}^-T PN_{n+a})_i
+//                    + dt_n alpha J_{n-1+a} (F_{n-1+a}^-T PN_{n-1+a})_i)
+//   k[a,d; c,d] += N_a w dt_np1 alpha (1 - alpha) J_{n+a} FIT_d(PN'_{n+a})
+// where, as in the reference, the mid-point load mixes the older value
+// projected on the normal with the newer raw value:
+//   residual   PN_{n+a} = (1 - alpha) PN_n + alpha P_{n+1},  PN_n = p_n n (pressure)
+//              PN_{n-1+a} = (1 - alpha) PN_{n-1} + alpha P_n
+//   stiffness  PN'_{n+a} = (1 - alpha) PN'_n + alpha P_{n+1},  PN'_n = (p_n n_0, 0, p_n n_2)
+// (tractions: the plain mid points).  The stiffness's time step is the
+// element's, dt_np1.
+void neumann_faces_transient(const orc_problem *P, long e, const double *Xe, const double *u2, const double *u1,
+                             const double *u0, double alpha, double dt_np1, double dt_n, double *fe, double *lk) {
+  const int nne = P->nne, nd = nne * 3, nb = nne == 10 ? 6 : 3;
+  const int npt = nne == 10 ? 3 : 1;
+  const double gk1[1] = {1.0 / 3.0}, ge1[1] = {1.0 / 3.0}, w1[1] = {0.5};
+  const double gk3[3] = {2.0 / 3.0, 1.0 / 6.0, 1.0 / 6.0}, ge3[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+  const double w3[3] = {1.0 / 6.0, 1.0 / 6.0, 1.0 / 6.0};
+  const double *gk = npt == 3 ? gk3 : gk1, *ge = npt == 3 ? ge3 : ge1, *wt = npt == 3 ? w3 : w1;
+  double Unpa[30], Unma[30];
+  for (int i = 0; i < nd; i++) {
+    Unpa[i] = (1.0 - alpha) * u1[i] + alpha * u2[i];
+    Unma[i] = (1.0 - alpha) * u0[i] + alpha * u1[i];
+  }
+  for (long k = P->nbc_off[e]; k < P->nbc_off[e + 1]; k++) {
+    const int f = P->nbc_face[k], type = P->nbc_type[k];
+    const int *v2b = nne == 10 ? kQTet2QTri[f] : kTet2Tri[f];
+    const int *km = kKezMapTet[f];
+    double P2[3] = {0, 0, 0}, P1[3] = {0, 0, 0}, P0[3] = {0, 0, 0};
+    for (int i = 0; i < type && i < 3; i++) {
+      P2[i] = P->nbc_load[k * 3 + i];
+      P1[i] = P->nbc_load_n[k * 3 + i];
+      P0[i] = P->nbc_load_nm1[k * 3 + i];
+    }
+    if (type == 1) {
+      P2[2] = P2[0];
+      P1[2] = P1[0];
+      P0[2] = P0[0];
+    }
+    for (int ip = 0; ip < npt; ip++) {
+      double kez[3] = {0.0, 0.0, 0.0};
+      kez[km[0]] = gk[ip];
+      kez[km[1]] = ge[ip];
+      if (f == 2) kez[km[2]] = 1.0 - gk[ip] - ge[ip];
+      double N[10], dN[30];
+      shape_N(nne, kez[0], kez[1], kez[2], N);
+      int terr = 0;
+      PGFem3D_dNdX(nne, kez[0], kez[1], kez[2], Xe, dN, &terr);
+      double db[12];
+      face_dN(nb, kez[km[0]], kez[km[1]], db);
+      double dX[6] = {0, 0, 0, 0, 0, 0};
+      for (int ib = 0; ib < 3; ib++)
+        for (int ic = 0; ic < 2; ic++)
+          for (int ia = 0; ia < nb; ia++) dX[ib * 2 + ic] += db[ia * 2 + ic] * Xe[v2b[ia] * 3 + ib];
+      const double v0 = dX[2] * dX[5] - dX[3] * dX[4];
+      const double v1 = dX[1] * dX[4] - dX[0] * dX[5];
+      const double v2 = dX[0] * dX[3] - dX[1] * dX[2];
+      const double Jf = std::sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+      const double n[3] = {v0 / Jf, v1 / Jf, v2 / Jf};
+      const double detJxW = Jf * wt[ip];
+      double PNn[3], PNnm1[3], PNk[3], PNnpa[3], PNnma[3], PNknpa[3];
+      for (int i = 0; i < 3; i++) {
+        PNn[i] = type == 1 ? P1[0] * n[i] : P1[i];
+        PNnm1[i] = type == 1 ? P0[0] * n[i] : P0[i];
+        PNk[i] = type == 1 ? P1[i] * n[i] : P1[i];
+        PNnpa[i] = (1.0 - alpha) * PNn[i] + alpha * P2[i];
+        PNnma[i] = (1.0 - alpha) * PNnm1[i] + alpha * P1[i];
+        PNknpa[i] = (1.0 - alpha) * PNk[i] + alpha * P2[i];
+      }
+      double Fa[9], Fb[9], FIa[9], FIb[9];
+      deformation_gradient(nne, Unpa, dN, Fa);
+      deformation_gradient(nne, Unma, dN, Fb);
+      const double Ja = det3x3(Fa), Jb = det3x3(Fb);
+      inv3x3(Fa, FIa);
+      inv3x3(Fb, FIb);
+      double Ta[3], Tb[3], Tk[3];
+      for (int i = 0; i < 3; i++) {
+        Ta[i] = FIa[0 * 3 + i] * PNnpa[0] + FIa[1 * 3 + i] * PNnpa[1] + FIa[2 * 3 + i] * PNnpa[2];
+        Tb[i] = FIb[0 * 3 + i] * PNnma[0] + FIb[1 * 3 + i] * PNnma[1] + FIb[2 * 3 + i] * PNnma[2];
+        Tk[i] = FIa[0 * 3 + i] * PNknpa[0] + FIa[1 * 3 + i] * PNknpa[1] + FIa[2 * 3 + i] * PNknpa[2];
+      }
+      for (int ia = 0; ia < nb; ia++) {
+        const int a = v2b[ia];
+        for (int i = 0; i < 3; i++)
+          fe[a * 3 + i] += N[a] * detJxW * (dt_np1 * (1.0 - alpha) * Ja * Ta[i] + dt_n * alpha * Jb * Tb[i]);
+        if (!lk) continue;
+        const double s = N[a] * detJxW * dt_np1 * alpha * (1.0 - alpha) * Ja;
+        for (int ic = 0; ic < nb; ic++) {
+          const int c = v2b[ic];
+          for (int d = 0; d < 3; d++) {
+            double g = 0.0;
+            for (int l = 0; l < 3; l++) g += FIa[l * 3 + d] * dN[ic * 3 + l];
+            lk[(a * 3 + d) * nd + c * 3 + d] += s * 2.0 * g * Tk[d];
+          }
+        }
+      }
+    }
+  }
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -1209,6 +1314,10 @@ extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *
     for (int i = 0; i < nd; i++) fe[i] -= fi[i];
     if (K)
       for (int i = 0; i < nd * nd; i++) lk[i] = -kI[i] - alpha * (1.0 - alpha) * dt_np1 * lk1[i];
+    if (P->nbc_off) {  // surface loads at the mid points (needs the values at t_n, t_{n-1})
+      if (!P->nbc_load_n || !P->nbc_load_nm1) { err++; continue; }
+      neumann_faces_transient(P, e, Xe, u2, u1, u0, alpha, dt_np1, dt_n, fe.data(), K ? lk.data() : nullptr);
+    }
     scatter(P, e, fe.data(), K ? lk.data() : nullptr, R, K);
   }
   return err;

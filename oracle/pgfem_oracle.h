@@ -67,6 +67,10 @@ typedef struct {
   const int *nbc_face;
   const int *nbc_type;
   const double *nbc_load;
+  /* the same faces' values at t_n and t_{n-1} (3k .. 3k+2), read by the
+   * transient element only (may be NULL otherwise) */
+  const double *nbc_load_n;
+  const double *nbc_load_nm1;
 } orc_problem;
 
 /* Reference: src/generate_dof_ids.cc:69-171 (generate_local_dof_ids) and

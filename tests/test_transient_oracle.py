@@ -77,3 +77,40 @@ def test_linear_in_the_static_parts():
     _, Rb, _, _ = P.assemble(mat, (1 - al) * u0 + al * u1, want_K=False)
     assert np.allclose(R, -dt1 * (1 - al) * Ra - dt0 * al * Rb, rtol=1e-12, atol=1e-12 * np.abs(Ra).max())
     assert np.allclose(K, -al * (1 - al) * dt1 * Ka, rtol=1e-12, atol=1e-12 * np.abs(Ka).max())
+
+
+def _surface_part(P, mat, us, al, dt1, dt0, faces, loads3):
+    """Transient R, K with the faces loaded minus without (the surface part)."""
+    el, fc, lt = faces
+    P.set_neumann(el, fc, lt, loads3[0], load_n=loads3[1], load_nm1=loads3[2])
+    err, R1, K1 = oracle.assemble_transient(P, mat, us[2], us[1], us[0], al, dt1, dt0, 2.0)
+    assert err == 0
+    P.set_neumann([], [], [], np.zeros((0, 3)))
+    err, R0, K0 = oracle.assemble_transient(P, mat, us[2], us[1], us[0], al, dt1, dt0, 2.0)
+    assert err == 0
+    return R1 - R0, K1 - K0
+
+
+@pytest.mark.parametrize("nne", [4, 10])
+def test_surface_loads_constant_in_time(nne):
+    """With u and the loads the same at the three times the transient surface
+    terms are the quasi-static ones scaled: traction -(dt_np1 (1 - a) + dt_n a)
+    on R and -dt_np1 a (1 - a) on K; a pressure at a = 0 (only the older value,
+    projected on the normal, enters) -dt_np1 on R and nothing on K."""
+    X, conn, ids, ndof, Ap, Ai = free_box(2, nne)
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai)
+    mat = oracle.material(oracle.HE)
+    u = 1e-3 * np.random.default_rng(5).uniform(-1, 1, ndof)
+    el, fc = wl.box_faces(X, conn, 0, 1.0)
+    dt1, dt0 = 0.2, 0.1
+    for lt, val, al in ((3, [3.0, -1.0, 2.0], 0.35), (1, [5.0, 0.0, 0.0], 0.0)):
+        loads = np.tile(val, (len(el), 1))
+        Rs, Ks = _surface_part(P, mat, (u, u, u), al, dt1, dt0, (el, fc, np.full(len(el), lt)), (loads,) * 3)
+        P.set_neumann(el, fc, np.full(len(el), lt), loads)
+        _, Rq1, Kq1, _ = P.assemble(mat, u)
+        P.set_neumann([], [], [], np.zeros((0, 3)))
+        _, Rq0, Kq0, _ = P.assemble(mat, u)
+        cR = -(dt1 * (1 - al) + dt0 * al) if lt != 1 else -dt1
+        cK = -dt1 * al * (1 - al)
+        np.testing.assert_allclose(Rs, cR * (Rq1 - Rq0), rtol=0, atol=1e-12 * np.abs(Rs).max())
+        np.testing.assert_allclose(Ks, cK * (Kq1 - Kq0), rtol=0, atol=1e-10 * np.abs(Kq1 - Kq0).max())
