@@ -150,6 +150,14 @@ int pgfem_gpu_set_wait_test(pgfem_gpu_ctx *ctx, double limit_s, int stall_next_a
 int pgfem_gpu_set_neumann(pgfem_gpu_ctx *ctx, long nface, const long *elem, const int *face,
                           const int *feature, int nfeature, const int *load_type, const double *load_np1);
 int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *ctx, int nfeature, const double *load_np1);
+/* The same features' values at t_n and t_{n-1} (3 per feature), which the
+ * transient call (pgfem_gpu_assemble_RK_transient) needs when faces are set:
+ * it applies the surface loads at the two mid points, as the reference's
+ * compute_Neumann_boundary_conditions(_stiffnes_mat) do with inertia
+ * (src/fd_residuals.cc:123-273, src/stiffmat_fd.cc:359-500; the loads at the
+ * three times from NBE compute_load_values, src/fd_residuals.cc:505-507). */
+int pgfem_gpu_set_neumann_load_history(pgfem_gpu_ctx *ctx, int nfeature, const double *load_n,
+                                       const double *load_nm1);
 
 /* ---- three-field (CM3F) element -----------------------------------------
  * The constitutive-model element with one pressure P and one volume theta per

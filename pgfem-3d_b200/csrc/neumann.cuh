@@ -31,6 +31,51 @@
 
 namespace pgb {
 
+// Per-feature load descriptor: PN = c n + t (residual), PN'_i = c'_i n_i + t'_i
+// (stiffness), stored as (c, t[3], c'[3], t'[3]).
+constexpr int kNbcDesc = 10;
+
+// The load values as the reference reads them: the first `type` values, and
+// for a pressure (type 1) value 0 copied to component 2 (component 1 stays 0),
+// src/fd_residuals.cc:199-203.
+inline void nbc_raw(int type, const double *L, double *P) {
+  P[0] = P[1] = P[2] = 0.0;
+  for (int i = 0; i < type && i < 3; i++) P[i] = L[i];
+  if (type == 1) P[2] = P[0];
+}
+
+// Quasi-static: pressure PN = p n, PN' = (p n_0, 0, p n_2); traction PN = PN' = t.
+inline void nbc_desc_static(int type, const double *L, double *d) {
+  double P[3];
+  nbc_raw(type, L, P);
+  for (int i = 0; i < kNbcDesc; i++) d[i] = 0.0;
+  if (type == 1) {
+    d[0] = P[0];
+    for (int i = 0; i < 3; i++) d[4 + i] = P[i];
+  } else {
+    for (int i = 0; i < 3; i++) d[1 + i] = d[7 + i] = P[i];
+  }
+}
+
+// A mid point of the transient element (older values Lo, newer Ln):
+// PN = (1 - a) PN_o + a P_n, PN' = (1 - a) PN'_o + a P_n, the newer value taken
+// raw as the reference does (src/fd_residuals.cc:238-239, src/stiffmat_fd.cc:465).
+inline void nbc_desc_mid(int type, const double *Lo, const double *Ln, double a, double *d) {
+  double Po[3], Pn[3];
+  nbc_raw(type, Lo, Po);
+  nbc_raw(type, Ln, Pn);
+  for (int i = 0; i < kNbcDesc; i++) d[i] = 0.0;
+  if (type == 1) {
+    d[0] = (1.0 - a) * Po[0];
+    for (int i = 0; i < 3; i++) {
+      d[1 + i] = d[7 + i] = a * Pn[i];
+      d[4 + i] = (1.0 - a) * Po[i];
+    }
+  } else {
+    for (int i = 0; i < 3; i++) d[1 + i] = d[7 + i] = (1.0 - a) * Po[i] + a * Pn[i];
+  }
+}
+
 struct NbcArgs {
   const double *X;         // 3*nn SoA
   const int *conn;         // NNE*ne  (conn[a*ne + e])
@@ -45,8 +90,9 @@ struct NbcArgs {
   const int *face_elem;    // nface, sorted by element
   const uint8_t *face_id;  // nface: local face 0..3
   const int *face_feat;    // nface: feature (load) index
-  const int *feat_type;    // nfeat: number of load values, 1 = pressure
-  const double *feat_load; // 3*nfeat: values at t_{n+1}
+  // kNbcDesc doubles per feature: the load of the residual PN = c n + t and
+  // of the stiffness PN'_i = c'_i n_i + t'_i, as (c, t[3], c'[3], t'[3])
+  const double *feat_desc;
   const int *elem_face_off;  // ne+1: faces of element e (element-level calls)
   double *R;               // ndof or nullptr
   double *K;               // nnz or nullptr
@@ -119,15 +165,12 @@ __device__ __forceinline__ void nbc_face_dN(double k, double e, double (*d)[2]) 
 // addR(a, i, v) and addK(a, c, d, v) receive R[a,i] and K[a,d; c,d] (volume
 // node numbers).
 template <int NNE, bool WANT_K, class AddR, class AddK>
-__device__ void nbc_face_terms(const double (*xe)[3], const double (*ue)[3], int f, int type,
-                               const double *load, AddR addR, AddK addK) {
+__device__ void nbc_face_terms(const double (*xe)[3], const double (*ue)[3], int f, const double *desc,
+                               AddR addR, AddK addK) {
   constexpr int NB = NNE == 10 ? 6 : 3;
   constexpr int NPT = NNE == 10 ? 3 : 1;
   const int *v2b = NNE == 10 ? c_qtet2qtri[f] : c_tet2tri[f];
   const int *km = c_kezmap[f];
-  double P[3] = {0.0, 0.0, 0.0};
-  for (int i = 0; i < type && i < 3; i++) P[i] = load[i];
-  if (type == 1) P[2] = P[0];  // P[1] stays 0 (only value 0 is read)
 #pragma unroll 1
   for (int ip = 0; ip < NPT; ip++) {
     const double gk = NPT == 1 ? 1.0 / 3.0 : (ip == 0 ? 2.0 / 3.0 : 1.0 / 6.0);
@@ -196,13 +239,13 @@ __device__ void nbc_face_terms(const double (*xe)[3], const double (*ue)[3], int
     double ftp[3], ftk[3];  // F^-T PN, F^-T PN'
 #pragma unroll
     for (int i = 0; i < 3; i++) {
-      const double pn0 = type == 1 ? P[0] * nrm[0] : P[0];
-      const double pn1 = type == 1 ? P[0] * nrm[1] : P[1];
-      const double pn2 = type == 1 ? P[0] * nrm[2] : P[2];
+      const double pn0 = desc[0] * nrm[0] + desc[1];
+      const double pn1 = desc[0] * nrm[1] + desc[2];
+      const double pn2 = desc[0] * nrm[2] + desc[3];
       ftp[i] = FI[0 * 3 + i] * pn0 + FI[1 * 3 + i] * pn1 + FI[2 * 3 + i] * pn2;
-      const double pk0 = type == 1 ? P[0] * nrm[0] : P[0];
-      const double pk1 = type == 1 ? P[1] * nrm[1] : P[1];
-      const double pk2 = type == 1 ? P[2] * nrm[2] : P[2];
+      const double pk0 = desc[4] * nrm[0] + desc[7];
+      const double pk1 = desc[5] * nrm[1] + desc[8];
+      const double pk2 = desc[6] * nrm[2] + desc[9];
       ftk[i] = FI[0 * 3 + i] * pk0 + FI[1 * 3 + i] * pk1 + FI[2 * 3 + i] * pk2;
     }
 #pragma unroll 1
@@ -249,7 +292,6 @@ __global__ void __launch_bounds__(128) k_neumann(const NbcArgs A) {
   int nd[NNE];
   double xe[NNE][3], ue[NNE][3];
   nbc_gather<NNE>(A, e, nd, xe, ue);
-  const double load[3] = {A.feat_load[3 * feat], A.feat_load[3 * feat + 1], A.feat_load[3 * feat + 2]};
   auto addR = [&](int a, int i, double v) {
     const int id = A.dof[i * A.nn + nd[a]];
     if (A.R && id > 0) atomicAdd(&A.R[id - 1], v);
@@ -262,7 +304,7 @@ __global__ void __launch_bounds__(128) k_neumann(const NbcArgs A) {
                      A.pos[(e * NNE + a) * NNE + c] + __popc(mc & ((1u << d) - 1u));
     atomicAdd(&A.K[off], v);
   };
-  nbc_face_terms<NNE, WANT_K>(xe, ue, A.face_id[k], A.feat_type[feat], load, addR, addK);
+  nbc_face_terms<NNE, WANT_K>(xe, ue, A.face_id[k], A.feat_desc + kNbcDesc * feat, addR, addK);
 }
 
 // Element-level calls: one thread per listed element, its faces added into
@@ -285,8 +327,7 @@ __global__ void __launch_bounds__(128) k_neumann_dense(const NbcArgs A) {
   auto addK = [&](int a, int c, int d, double v) { lk[(a * 3 + d) * ND + c * 3 + d] += v; };
   for (int k = k0; k < k1; k++) {
     const int feat = A.face_feat[k];
-    const double load[3] = {A.feat_load[3 * feat], A.feat_load[3 * feat + 1], A.feat_load[3 * feat + 2]};
-    nbc_face_terms<NNE, WANT_K>(xe, ue, A.face_id[k], A.feat_type[feat], load, addR, addK);
+    nbc_face_terms<NNE, WANT_K>(xe, ue, A.face_id[k], A.feat_desc + kNbcDesc * feat, addR, addK);
   }
 }
 

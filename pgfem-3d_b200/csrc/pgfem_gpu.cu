@@ -100,7 +100,14 @@ struct pgfem_gpu_ctx {
   int nbc_nfeat = 0;
   int *nbc_elem = nullptr, *nbc_feat = nullptr, *nbc_type = nullptr, *nbc_off = nullptr;
   uint8_t *nbc_face = nullptr;
-  double *nbc_load = nullptr;
+  double *nbc_load = nullptr;  // load descriptors (kNbcDesc per feature) at t_{n+1}
+  // host copies of the types and values (t_{n+1}; t_n, t_{n-1} for the
+  // transient element), the transient call's two mid-point descriptor sets,
+  // and the set the next assembly reads (nullptr: nbc_load)
+  std::vector<int> nbc_type_h;
+  std::vector<double> nbc_load_h, nbc_hist_n, nbc_hist_nm1;
+  double *nbc_desc_tr = nullptr;
+  const double *nbc_desc_cur = nullptr;
   // transient calls: u and prescribed values at t_{n+1}, t_n, t_{n-1}, a
   // mid-point / combination vector of each, the second residual
   double *tr_buf = nullptr;
@@ -319,7 +326,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->colour_elems, c->qrec, c->eblk, c->perm,
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
-                  c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
+                  c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_desc_tr, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
                   c->nbc_load, c->tr_buf};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -692,8 +699,7 @@ NbcArgs nbc_args(const pgfem_gpu_ctx *c) {
   A.face_elem = c->nbc_elem;
   A.face_id = c->nbc_face;
   A.face_feat = c->nbc_feat;
-  A.feat_type = c->nbc_type;
-  A.feat_load = c->nbc_load;
+  A.feat_desc = c->nbc_desc_cur ? c->nbc_desc_cur : c->nbc_load;
   A.elem_face_off = c->nbc_off;
   return A;
 }
@@ -1209,9 +1215,18 @@ int pgfem_gpu_set_neumann(pgfem_gpu_ctx *c, long nface, const long *elem, const 
     if (p) cudaFree(p);
   if (c->nbc_face) cudaFree(c->nbc_face);
   if (c->nbc_load) cudaFree(c->nbc_load);
+  if (c->nbc_desc_tr) {
+    cudaFree(c->nbc_desc_tr);
+    c->bytes -= (long)(sizeof(double) * 2 * kNbcDesc * c->nbc_nfeat);
+  }
   c->nbc_elem = c->nbc_feat = c->nbc_type = c->nbc_off = nullptr;
   c->nbc_face = nullptr;
-  c->nbc_load = nullptr;
+  c->nbc_load = c->nbc_desc_tr = nullptr;
+  c->nbc_desc_cur = nullptr;
+  c->nbc_type_h.clear();
+  c->nbc_load_h.clear();
+  c->nbc_hist_n.clear();
+  c->nbc_hist_nm1.clear();
   c->nbc_nface = 0;
   c->nbc_nfeat = 0;
   c->bytes -= c->nbc_bytes;
@@ -1231,9 +1246,8 @@ int pgfem_gpu_set_neumann(pgfem_gpu_ctx *c, long nface, const long *elem, const 
     off[fe_[k] + 1]++;
   }
   for (long e = 0; e < c->ne; e++) off[e + 1] += off[e];
-  std::vector<double> ld((size_t)3 * nfeature);
-  for (int f = 0; f < nfeature; f++)
-    for (int i = 0; i < 3; i++) ld[(size_t)3 * f + i] = i < load_type[f] ? load_np1[(size_t)3 * f + i] : 0.0;
+  std::vector<double> ld((size_t)kNbcDesc * nfeature);
+  for (int f = 0; f < nfeature; f++) nbc_desc_static(load_type[f], load_np1 + (size_t)3 * f, &ld[(size_t)kNbcDesc * f]);
   int r;
   if ((r = upload(c, &c->nbc_elem, fe_.data(), fe_.size())) || (r = upload(c, &c->nbc_face, fi.data(), fi.size())) ||
       (r = upload(c, &c->nbc_feat, ff.data(), ff.size())) || (r = upload(c, &c->nbc_type, load_type, nfeature)) ||
@@ -1245,20 +1259,28 @@ int pgfem_gpu_set_neumann(pgfem_gpu_ctx *c, long nface, const long *elem, const 
   CK(cudaStreamSynchronize(c->stream));
   c->nbc_nface = nface;
   c->nbc_nfeat = nfeature;
+  c->nbc_type_h.assign(load_type, load_type + nfeature);
+  c->nbc_load_h.assign(load_np1, load_np1 + (size_t)3 * nfeature);
   return PGFEM_GPU_OK;
 }
 
 int pgfem_gpu_set_neumann_loads(pgfem_gpu_ctx *c, int nfeature, const double *load_np1) {
   if (!c || nfeature != c->nbc_nfeat || (nfeature && !load_np1)) return PGFEM_GPU_EINVAL;
   if (!nfeature) return PGFEM_GPU_OK;
-  std::vector<int> t(nfeature);
-  CK(cudaMemcpyAsync(t.data(), c->nbc_type, sizeof(int) * nfeature, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  std::vector<double> ld((size_t)3 * nfeature);
+  std::vector<double> ld((size_t)kNbcDesc * nfeature);
   for (int f = 0; f < nfeature; f++)
-    for (int i = 0; i < 3; i++) ld[(size_t)3 * f + i] = i < t[f] ? load_np1[(size_t)3 * f + i] : 0.0;
+    nbc_desc_static(c->nbc_type_h[f], load_np1 + (size_t)3 * f, &ld[(size_t)kNbcDesc * f]);
   CK(cudaMemcpyAsync(c->nbc_load, ld.data(), sizeof(double) * ld.size(), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  c->nbc_load_h.assign(load_np1, load_np1 + (size_t)3 * nfeature);
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_neumann_load_history(pgfem_gpu_ctx *c, int nfeature, const double *load_n,
+                                       const double *load_nm1) {
+  if (!c || nfeature != c->nbc_nfeat || (nfeature && (!load_n || !load_nm1))) return PGFEM_GPU_EINVAL;
+  c->nbc_hist_n.assign(load_n, load_n + (size_t)3 * nfeature);
+  c->nbc_hist_nm1.assign(load_nm1, load_nm1 + (size_t)3 * nfeature);
   return PGFEM_GPU_OK;
 }
 
@@ -1733,7 +1755,9 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
                                     double *R, double *K, pgfem_gpu_status *st) {
   if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
     return PGFEM_GPU_EINVAL;
-  if (c->model != PGFEM_MODEL_HE || c->nbc_nface || c->F0 || c->elem_group || c->three_field) return PGFEM_GPU_EINVAL;
+  if (c->model != PGFEM_MODEL_HE || c->F0 || c->elem_group || c->three_field) return PGFEM_GPU_EINVAL;
+  // surface loads need their values at t_n and t_{n-1}
+  if (c->nbc_nface && c->nbc_hist_n.size() != (size_t)3 * c->nbc_nfeat) return PGFEM_GPU_EINVAL;
   if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
     return PGFEM_GPU_EINVAL;
   // below the reference's density threshold the element is the quasi-static one
@@ -1757,16 +1781,38 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
   CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), s));
   const unsigned gu = (unsigned)((nd + 255) / 256), gp = (unsigned)((np + 255) / 256);
   double *pres = c->npres ? tpa : nullptr;
+  if (c->nbc_nface) {
+    // the surface loads' mid points: the first set for u_{n+a}, the second
+    // for u_{n-1+a}
+    const int nf = c->nbc_nfeat;
+    std::vector<double> d((size_t)2 * kNbcDesc * nf);
+    for (int f = 0; f < nf; f++) {
+      const size_t o = (size_t)3 * f;
+      nbc_desc_mid(c->nbc_type_h[f], &c->nbc_hist_n[o], &c->nbc_load_h[o], alpha, &d[(size_t)kNbcDesc * f]);
+      nbc_desc_mid(c->nbc_type_h[f], &c->nbc_hist_nm1[o], &c->nbc_hist_n[o], alpha,
+                   &d[(size_t)kNbcDesc * (nf + f)]);
+    }
+    if (!c->nbc_desc_tr && (r = dalloc(c, &c->nbc_desc_tr, d.size()))) return r;
+    CK(cudaMemcpyAsync(c->nbc_desc_tr, d.data(), sizeof(double) * d.size(), cudaMemcpyHostToDevice, s));
+    c->nbc_desc_cur = c->nbc_desc_tr;
+  }
   // quasi-static R and K at u_{n+a}
   k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
   if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
   CK(cudaGetLastError());
-  if ((r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1))) return r;
+  r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1);
+  if (r) {
+    c->nbc_desc_cur = nullptr;
+    return r;
+  }
+  if (c->nbc_nface) c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
   // quasi-static R at u_{n-1+a}
   k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, c->ndof);
   if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, c->npres);
   CK(cudaGetLastError());
-  if ((r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n))) return r;
+  r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n);
+  c->nbc_desc_cur = nullptr;
+  if (r) return r;
   // the mid-point combination
   k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
   if (K) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,

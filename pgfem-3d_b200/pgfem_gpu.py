@@ -77,6 +77,7 @@ def lib():
             "pgfem_gpu_assemble_RK_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                           C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_gpu_set_neumann_loads": (C.c_int, [_P, C.c_int, _P]),
+            "pgfem_gpu_set_neumann_load_history": (C.c_int, [_P, C.c_int, _P, _P]),
             "pgfem_gpu_set_three_field": (C.c_int, [_P, _P, _P]),
             "pgfem_gpu_get_three_field": (C.c_int, [_P, _P, _P]),
             "pgfem_gpu_three_field_enabled": (C.c_int, [_P]),
@@ -306,6 +307,13 @@ class Context:
     def set_neumann_loads(self, load_np1):
         ld = np.ascontiguousarray(np.reshape(load_np1, (-1, 3)), dtype=np.float64)
         _check("pgfem_gpu_set_neumann_loads", lib().pgfem_gpu_set_neumann_loads(self.h, len(ld), _ptr(ld)))
+
+    def set_neumann_load_history(self, load_n, load_nm1):
+        """The features' load values at t_n and t_{n-1} (the transient call)."""
+        a = np.ascontiguousarray(np.reshape(load_n, (-1, 3)), dtype=np.float64)
+        b = np.ascontiguousarray(np.reshape(load_nm1, (-1, 3)), dtype=np.float64)
+        _check("pgfem_gpu_set_neumann_load_history",
+               lib().pgfem_gpu_set_neumann_load_history(self.h, len(a), _ptr(a), _ptr(b)))
 
     def set_three_field(self, P, theta):
         """Three-field (CM3F) element: pressure P and volume theta per element

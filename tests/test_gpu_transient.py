@@ -4,8 +4,10 @@ residual_with_inertia / stiffness_with_inertia, src/dynamics.cc:183-432, for
 the hyperelastic model): linear tets with a fixed face, quadratic tets with
 prescribed displacements (values at three times), two alphas and unequal
 steps, R and K at the parity tolerance (1e-10); below the density threshold
-the call is the quasi-static assembly at t_{n+1}; J2 contexts, contexts with
-surface loads and bad time parameters are rejected."""
+the call is the quasi-static assembly at t_{n+1}; with surface loads (tractions
+and pressures, values at the three times) the mid-point surface terms equal the
+oracle's; J2 contexts, surface loads without their earlier values and bad time
+parameters are rejected."""
 import numpy as np
 import pytest
 
@@ -87,3 +89,49 @@ def test_transient_rejections(gpu):
     with pytest.raises(pg.PgfemError):
         cq.assemble_RK_transient(q.u, q.u, q.u, 0.5, 0.1, 0.1, 1.0)
     cq.close()
+
+
+
+@pytest.mark.parametrize("maker,alpha", [("p1", 0.6), ("p2", 0.4)])
+def test_transient_with_surface_loads(gpu, maker, alpha):
+    if maker == "p1":
+        p = wl.he_p1(n=4, seed=3)
+    else:
+        p = wl.tension(n=3, nne=10, model="he", stretch=0.004, predictor=True)
+    us, ps = _three_states(p, seed=9)
+    planes = [(0, 1.0), (2, 1.0), (1, 0.0)]
+    types = np.array([3, 1, 2])
+    el, fc, ft = [], [], []
+    for k, (axis, v) in enumerate(planes):
+        e, f = wl.box_faces(p.X, p.conn, axis, v)
+        el.append(e)
+        fc.append(f)
+        ft.append(np.full(len(e), k, dtype=np.int32))
+    el, fc, ft = np.concatenate(el), np.concatenate(fc), np.concatenate(ft)
+    L2 = np.array([[12.0, -7.0, 3.0], [25.0, 0.0, 0.0], [-4.0, 6.0, 0.0]])
+    L1, L0 = 0.7 * L2 + 1.0, 0.4 * L2 - 2.0
+    dt1, dt0, rho = 0.02, 0.015, 2.0e4
+    ctx = p.context()
+    ctx.set_neumann(el, fc, ft, types, L2)
+    ctx.set_neumann_load_history(L1, L0)
+    pr = (ps[2], ps[1], ps[0]) if ps else (None, None, None)
+    R, K, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho, presc=pr)
+    assert st.ok(), st.as_dict()
+    P, mat = oracle.from_workload(p)
+    P.set_neumann(el, fc, types[ft], L2[ft], load_n=L1[ft], load_nm1=L0[ft])
+    args = dict(p_np1=ps[2], p_n=ps[1], p_nm1=ps[0]) if ps else {}
+    err, Ro, Ko = oracle.assemble_transient(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, **args)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    # the surface terms carry weight
+    P0, _ = oracle.from_workload(p)
+    _, R0, _ = oracle.assemble_transient(P0, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, **args)
+    assert np.linalg.norm(Ro - R0) > 1e-3 * np.linalg.norm(Ro)
+    # the quasi-static calls still use the values at t_{n+1}
+    Rq, Kq, st = ctx.assemble_RK(us[2], ps[2] if ps else None)
+    P.set_neumann(el, fc, types[ft], L2[ft])
+    _, Rqo, Kqo, _ = P.assemble(mat, us[2], ps[2] if ps else None)
+    check_R(Rq, Rqo)
+    check_K(Kq, Kqo, p.Ap)
+    ctx.close()
