@@ -403,12 +403,14 @@ template <int NNE, int NQP, int MODEL, bool TF = false>
 int launch_qp_update(pgfem_gpu_ctx *c, cudaStream_t s) {
   constexpr bool YREC = NNE == 10;
   const int nf = YREC ? yrec_fields(TF) : kQRec;
+  // the tiled layout of the 10-node records is padded to whole tiles
+  const size_t npts = YREC ? (size_t)((c->nqp + kMPtsT - 1) / kMPtsT) * kMPtsT : (size_t)c->nqp;
   if (c->qrec && c->qrec_fields < nf) {  // a wider record than allocated
     cudaFree(c->qrec);
+    c->bytes -= (long)(sizeof(double) * c->qrec_fields * npts);
     c->qrec = nullptr;
   }
-  if (!c->qrec) {  // the tiled layout of the 10-node records is padded to whole tiles
-    const size_t npts = YREC ? (size_t)((c->nqp + kMPtsT - 1) / kMPtsT) * kMPtsT : (size_t)c->nqp;
+  if (!c->qrec) {
     int r = dalloc(c, &c->qrec, (size_t)nf * npts);
     if (r) return r;
     c->qrec_fields = nf;

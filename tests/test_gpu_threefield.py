@@ -209,3 +209,25 @@ def test_j2_device_newton_matches_oracle(gpu):
     assert np.abs(thg - tho).max() <= 1e-8
     assert np.abs(Pg - Pio).max() <= 1e-8 * kap
     ctx.close()
+
+
+def test_larger_mesh_free_body_and_translations(gpu):
+    """24^3 cells (the config-2 mesh at a smaller n, every DOF free, K values
+    above L2): the condensed internal forces of a free body sum to zero per
+    component, and K maps a rigid translation to zero."""
+    p = wl.j2_p2(n=24, seed=1)
+    p.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.45)
+    p.state = None
+    rng = np.random.default_rng(8)
+    ctx = p.context()
+    ctx.set_three_field(300.0 * rng.uniform(-1, 1, p.ne), 1.0 + 0.002 * rng.uniform(-1, 1, p.ne))
+    R, K, st = ctx.assemble_RK(p.u)
+    assert st.ok()
+    Km = csr_matrix((K, p.Ai, p.Ap), shape=(p.ndof, p.ndof))
+    for c in range(3):
+        rows = p.ids[:, c] - 1
+        assert abs(R[rows].sum()) <= 1e-10 * np.abs(R[rows]).sum()
+        t = np.zeros(p.ndof)
+        t[rows] = 1.0
+        assert np.abs(Km @ t).max() <= 1e-10 * np.abs(Km).sum(axis=1).max()
+    ctx.close()
