@@ -61,6 +61,7 @@ def lib():
                                                _P, C.c_int, _P]),
             "orc_assemble_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                  C.c_double, C.c_double, _P, _P]),
+            "orc_cp_tangent_pair": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, _P, _P]),
             "orc_element_3f": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, C.c_double, _P, _P, _P, _P, _P]),
             "orc_assemble_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
             "orc_update_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -386,3 +387,11 @@ def j2_p2_problem(n, seed=1, perturb=1e-4, max_cells_z=None, E=200e3, nu=0.3, si
 def from_workload(p):
     """Oracle Problem + material for a pgfem-3d_b200 workloads.Problem."""
     return Problem(p.X, p.conn, p.ids, p.ndof, p.Ap, p.Ai, F0=p.F0, R_cp=p.R_cp), from_pg_material(p.mat)
+
+
+def cp_tangent_pair(mat, Fn, Fnp1, dt, Rcp, state_n):
+    """(err, dM/dF from the oracle's Newton, dM/dF from the reference's formula), 9 x 9 each."""
+    a = [np.ascontiguousarray(x, dtype=np.float64) for x in (Fn, Fnp1, Rcp, state_n)]
+    d1, d2 = np.zeros(81), np.zeros(81)
+    err = lib().orc_cp_tangent_pair(C.byref(mat), _p(a[0]), _p(a[1]), dt, _p(a[2]), _p(a[3]), _p(d1), _p(d2))
+    return err, d1.reshape(9, 9), d2.reshape(9, 9)

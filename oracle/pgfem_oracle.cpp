@@ -720,6 +720,7 @@ void neumann_faces_transient(const orc_problem *P, long e, const double *Xe, con
 // ===========================================================================
 namespace {
 #include "orc_cp.inc"
+#include "orc_cp_ref_tangent.inc"
 }
 
 extern "C" {
@@ -1025,6 +1026,37 @@ int run_elements(const orc_problem *P, long e0, long e1, int nthreads, Body body
 }
 
 }  // namespace
+
+// The crystal-plasticity tangent dM/dF (M = pF_n pF_{n+1}^-1) at F_{n+1} from
+// the state at t_n (pF_n 9, g_n) two ways: the oracle's implicit derivative of
+// its Newton system (CpResult::dMdF) and the reference's own formula
+// (cp_ref_dMdF) fed with the converged state, eF_n = F_n pF_n^-1 and
+// eF_{n+1} = F_{n+1} pF_{n+1}^-1.  Test hook.
+extern "C" int orc_cp_tangent_pair(const orc_material *mat, const double *Fn, const double *Fnp1, double dt,
+                                   const double *Rcp, const double *state_n, double *dMdF_newton,
+                                   double *dMdF_ref) {
+  Elast el = make_elast(mat);
+  CpResult res;
+  if (cp_update(mat, el, Fnp1, dt, Rcp, state_n, res)) return 1;
+  double P[kNSlip][9];
+  cp_schmid(Rcp, P);
+  double pFnI[9], pFnp1I[9], eFn[9], eFnp1[9], C[9], S[9], CS[9];
+  if (inv3x3(state_n, pFnI) || inv3x3(res.pFnp1, pFnp1I)) return 1;
+  matmul(Fn, pFnI, eFn);
+  matmul(Fnp1, pFnp1I, eFnp1);
+  matmulTN(eFnp1, eFnp1, C);
+  he_stress_stiffness(el, C, det3x3(eFnp1), S, nullptr);
+  matmul(C, S, CS);
+  double tau[kNSlip], gd[kNSlip];
+  for (int a = 0; a < kNSlip; a++) {
+    double t = 0.0;
+    for (int i = 0; i < 9; i++) t += CS[i] * P[a][i];
+    tau[a] = t;
+    gd[a] = res.dgam[a] / dt;
+  }
+  for (int i = 0; i < 81; i++) dMdF_newton[i] = res.dMdF[i];
+  return cp_ref_dMdF(mat, el, eFn, eFnp1, res.M, state_n[9], res.g, tau, gd, P, dt, dMdF_ref);
+}
 
 extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const double *u,
                             const double *u_presc, double dt, const double *state_n,
