@@ -196,8 +196,15 @@ long pgfem_gpu_nnz(const pgfem_gpu_ctx *ctx);
 /* ---- state (Model_parameters::set_init_vals / update_state_vars /
  *      reset_state_vars, src/constitutive_model.cc:1337-1497) ------------- */
 int pgfem_gpu_set_state(pgfem_gpu_ctx *ctx, const double *state_n); /* AoS ne*nint*ns, host */
-int pgfem_gpu_get_state(pgfem_gpu_ctx *ctx, int level, double *state); /* level 0: t_n, 1: t_{n+1} */
-int pgfem_gpu_commit_state(pgfem_gpu_ctx *ctx); /* n <- n+1 */
+int pgfem_gpu_get_state(pgfem_gpu_ctx *ctx, int level, double *state); /* level 0: t_n, 1: t_{n+1},
+                                                                          2: t_{n-1} (crystal plasticity) */
+/* Crystal plasticity keeps the state at t_{n-1} too (get_pF(m, pF, 0), the
+ * transient element's older mid point): set_state sets all three levels,
+ * set_state_nm1 only t_{n-1} (AoS nqp*10; PGFEM_GPU_EINVAL for other models),
+ * commit moves n to n-1 before n+1 to n, and a crystal-plasticity restart
+ * file sets it from its pF_{n-1}, g_{n-1} fields. */
+int pgfem_gpu_set_state_nm1(pgfem_gpu_ctx *ctx, const double *state_nm1);
+int pgfem_gpu_commit_state(pgfem_gpu_ctx *ctx); /* (n-1 <- n,) n <- n+1 */
 int pgfem_gpu_reset_state(pgfem_gpu_ctx *ctx);  /* n+1 <- n */
 
 /* ---- assembly (host buffers; synchronous) --------------------------------
@@ -231,8 +238,16 @@ int pgfem_gpu_read_status(pgfem_gpu_ctx *ctx, pgfem_gpu_status *st, int clear);
  * rho (dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1}) / (dt_np1 dt_n) and M
  * the consistent mass (rho N_A N_C) on the element's own quadrature rule.  With
  * |rho| < 1e-16 this is the quasi-static R, K at u_{n+1}, as in the reference.
- * Hyperelastic contexts without surface loads or macro deformation only
- * (PGFEM_GPU_EINVAL otherwise).  The status counts both mid-point assemblies. */
+ * Crystal plasticity (linear tets): the point update runs at u_{n+1} from the
+ * state at t_n (the state at t_{n+1} is written, as by assemble_RK), and each
+ * mid point takes the mid-point plastic part, pF = mid(pF_n, pF_{n+1}) and
+ * mid(pF_{n-1}, pF_n) with the context's state at t_{n-1}, M = pF^-1 and the
+ * factor det pF (residuals_el_constitutive_model_n_plus_alpha); K is the
+ * derivative of that R in u_{n+1} through F and pF_{n+1}.  Surface loads at
+ * the two mid points as pgfem_gpu_set_neumann_load_history sets them.
+ * Hyperelastic and crystal-plasticity contexts without macro deformation,
+ * mesh groups or the three-field element (PGFEM_GPU_EINVAL otherwise).  The
+ * status counts inverted elements at both mid points. */
 int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *ctx, const double *u_np1, const double *u_n,
                                     const double *u_nm1, const double *presc_np1, const double *presc_n,
                                     const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,

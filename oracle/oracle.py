@@ -61,6 +61,8 @@ def lib():
                                                _P, C.c_int, _P]),
             "orc_assemble_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
                                                  C.c_double, C.c_double, _P, _P]),
+            "orc_assemble_transient_state": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                                                       C.c_double, C.c_double, _P, _P, _P, _P, _P]),
             "orc_cp_tangent_pair": (C.c_int, [_P, _P, _P, C.c_double, _P, _P, _P, _P]),
             "orc_element_3f": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, C.c_double, _P, _P, _P, _P, _P]),
             "orc_assemble_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
@@ -273,6 +275,23 @@ def assemble_transient(P, mat, u_np1, u_n, u_nm1, alpha, dt_np1, dt_n, rho, p_np
     err = lib().orc_assemble_transient(C.byref(P.s), C.byref(mat), *[_p(a) for a in arr], alpha, dt_np1, dt_n, rho,
                                        _p(R), _p(K))
     return err, R, K
+
+
+def assemble_transient_cp(P, mat, u_np1, u_n, u_nm1, alpha, dt_np1, dt_n, rho, state_nm1, state_n,
+                          p_np1=None, p_n=None, p_nm1=None, want_K=True):
+    """Transient (mid-point rule) R, K of the crystal-plasticity element with the
+    state at t_{n-1} and t_n (AoS ne*nint*10): orc_assemble_transient_state.
+    Returns (err, R, K, state_np1)."""
+    R = np.zeros(P.ndof)
+    K = np.zeros(P.nnz) if want_K else None
+    arr = [np.ascontiguousarray(a, dtype=np.float64) if a is not None else None
+           for a in (u_np1, u_n, u_nm1, p_np1, p_n, p_nm1)]
+    s0 = np.ascontiguousarray(state_nm1, dtype=np.float64)
+    s1 = np.ascontiguousarray(state_n, dtype=np.float64)
+    s2 = np.zeros_like(s1)
+    err = lib().orc_assemble_transient_state(C.byref(P.s), C.byref(mat), *[_p(a) for a in arr], alpha, dt_np1,
+                                             dt_n, rho, _p(s0), _p(s1), _p(s2), _p(R), _p(K))
+    return err, R, K, s2
 
 
 def newton_step(P, mat, u0, u_presc=None, state_n=None, dt=0.0, iter_max=10, nor_min=1e-10,

@@ -1280,15 +1280,32 @@ extern "C" int orc_update_3f(const orc_problem *P, const orc_material *mat, cons
 //   k  = -rho / dt_np1 sum_q N_a N_c w delta_bd - alpha (1 - alpha) dt_np1 k(F(n+alpha))
 // with r, k the quasi-static element integrals at the given F (M = I); the
 // body force of the manufactured-solution tests is zero here.
+//
+// Crystal plasticity (orc_assemble_transient_state): the point update runs at
+// F_{n+1} from the state at t_n (run_integration_algorithm, :2886-2888), then
+// each mid point takes the mid-point plastic part, pF(n+alpha) =
+// mid(pF_n, pF_{n+1}) and pF(n-1+alpha) = mid(pF_{n-1}, pF_n) (get_pF at
+// levels 2, 1, 0, :2893-2895), M = pF^-1, eF = F M, the elastic stress at eF
+// and the factor det pF (residuals_el_constitutive_model_n_plus_alpha,
+// :1926-1975).  The stiffness is compute_stiffness_matrix at n+alpha with
+// M(n+alpha) (:2120-2156) and dM/du the derivative of M(n+alpha) through
+// pF_{n+1}, divided by alpha (the blend's alpha (1 - alpha) carries it):
+//   dM(n+alpha)/du / alpha = M(n+alpha) pF_{n+1} d(pF_{n+1}^-1)/du pF_{n+1} M(n+alpha),
+// with d(pF_{n+1}^-1)/du the consistent derivative of the local update (the
+// reference evaluates its own compute_dMdu formula at the mid-point values
+// instead, plasticity_compute_dMdu_npa, src/plasticity_model.cc:779-866).
 // ---------------------------------------------------------------------------
-extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
-                                      const double *u_n, const double *u_nm1, const double *p_np1,
-                                      const double *p_n, const double *p_nm1, double alpha, double dt_np1,
-                                      double dt_n, double rho, double *R, double *K) {
-  if (mat->model != ORC_MODEL_HE) return 1;
+extern "C" int orc_assemble_transient_state(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                            const double *u_n, const double *u_nm1, const double *p_np1,
+                                            const double *p_n, const double *p_nm1, double alpha, double dt_np1,
+                                            double dt_n, double rho, const double *state_nm1,
+                                            const double *state_n, double *state_np1, double *R, double *K) {
+  const bool cp = mat->model == ORC_MODEL_CP;
+  if (mat->model != ORC_MODEL_HE && !(cp && state_nm1 && state_n)) return 1;
   const int nne = P->nne, nd = nne * 3;
   int err = 0;
   Quad qr = quad_rule(nne);
+  Elast el = make_elast(mat);
   for (long e = 0; e < P->ne; e++) {
     double u2[30], u1[30], u0[30], Xe[30];
     gather_u(P, e, u_np1, p_np1, u2);
@@ -1317,18 +1334,64 @@ extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *
         Fnma[i] = (1.0 - alpha) * F0[i] + alpha * F1[i];
       }
       if (det3x3(Fnpa) <= 0.0 || det3x3(Fnma) <= 0.0) { eerr += 1; break; }  // getJacobian
-      double S[9], L[81], st[10];
-      if (orc_cm_update(mat, Fnpa, 0.0, nullptr, nullptr, st, S, K ? L : nullptr, nullptr)) { eerr++; break; }
-      compute_residual_vector(fe.data(), nne, dN, w, Fnpa, I3, I3, S, -dt_np1 * (1.0 - alpha));
-      if (K) {
-        double FrTFr[9];
-        matmulTN(Fnpa, Fnpa, FrTFr);
-        std::vector<double> dMdu(nd * 9, 0.0);
-        compute_stiffness_matrix(lk1.data(), nne, dN, w, Fnpa, I3, I3, I3, FrTFr, I3, S, L, dMdu.data(), 1.0);
+      if (!cp) {
+        double S[9], L[81], st[10];
+        if (orc_cm_update(mat, Fnpa, 0.0, nullptr, nullptr, st, S, K ? L : nullptr, nullptr)) { eerr++; break; }
+        compute_residual_vector(fe.data(), nne, dN, w, Fnpa, I3, I3, S, -dt_np1 * (1.0 - alpha));
+        if (K) {
+          double FrTFr[9];
+          matmulTN(Fnpa, Fnpa, FrTFr);
+          std::vector<double> dMdu(nd * 9, 0.0);
+          compute_stiffness_matrix(lk1.data(), nne, dN, w, Fnpa, I3, I3, I3, FrTFr, I3, S, L, dMdu.data(), 1.0);
+        }
+        double S0[9];
+        if (orc_cm_update(mat, Fnma, 0.0, nullptr, nullptr, st, S0, nullptr, nullptr)) { eerr++; break; }
+        compute_residual_vector(fe.data(), nne, dN, w, Fnma, I3, I3, S0, -dt_n * alpha);
+      } else {
+        const long q = e * qr.nint + ip;
+        const double *s0 = state_nm1 + q * 10, *s1 = state_n + q * 10;
+        CpResult res;
+        if (cp_update(mat, el, F2, dt_np1, P->R_cp ? P->R_cp + e * 9 : nullptr, s1, res)) { eerr++; break; }
+        if (state_np1) {
+          for (int i = 0; i < 9; i++) state_np1[q * 10 + i] = res.pFnp1[i];
+          state_np1[q * 10 + 9] = res.g;
+        }
+        double pFa[9], pFb[9], Ma[9], Mb[9];
+        for (int i = 0; i < 9; i++) {
+          pFa[i] = (1.0 - alpha) * s1[i] + alpha * res.pFnp1[i];
+          pFb[i] = (1.0 - alpha) * s0[i] + alpha * s1[i];
+        }
+        if (inv3x3(pFa, Ma) || inv3x3(pFb, Mb)) { eerr++; break; }
+        // one mid point: S at eF = F M, residual with the factor det pF
+        auto mid_point = [&](const double *Fm, const double *Mm, const double *pFm, double coef, double *Sm,
+                             double *Lm) {
+          double eF[9], Ce[9], MT[9];
+          matmul(Fm, Mm, eF);
+          matmulTN(eF, eF, Ce);
+          he_stress_stiffness(el, Ce, det3x3(eF), Sm, Lm);
+          transpose(Mm, MT);
+          compute_residual_vector(fe.data(), nne, dN, w, Fm, MT, Mm, Sm, coef * det3x3(pFm));
+        };
+        double Sa[9], La[81], Sb[9];
+        mid_point(Fnpa, Ma, pFa, -dt_np1 * (1.0 - alpha), Sa, K ? La : nullptr);
+        mid_point(Fnma, Mb, pFb, -dt_n * alpha, Sb, nullptr);
+        if (K) {
+          std::vector<double> dMtl(nd * 9, 0.0), dMa(nd * 9, 0.0);
+          cp_dMdu(res, nne, dN, dMtl.data());
+          for (int k = 0; k < nd; k++) {  // M(n+a) pF_{n+1} d(pF_{n+1}^-1) pF_{n+1} M(n+a)
+            double t1[9], t2[9], t3[9];
+            matmul(Ma, res.pFnp1, t1);
+            matmul(t1, dMtl.data() + k * 9, t2);
+            matmul(t2, res.pFnp1, t3);
+            matmul(t3, Ma, dMa.data() + k * 9);
+          }
+          double MaT[9], FrTFr[9];
+          transpose(Ma, MaT);
+          matmulTN(Fnpa, Fnpa, FrTFr);
+          compute_stiffness_matrix(lk1.data(), nne, dN, w, Fnpa, MaT, I3, Ma, FrTFr, Ma, Sa, La, dMa.data(),
+                                   det3x3(pFa));
+        }
       }
-      double S0[9];
-      if (orc_cm_update(mat, Fnma, 0.0, nullptr, nullptr, st, S0, nullptr, nullptr)) { eerr++; break; }
-      compute_residual_vector(fe.data(), nne, dN, w, Fnma, I3, I3, S0, -dt_n * alpha);
       // inertia (DISP_resid_w_inertia_el, src/dynamics.cc:78-181; mass of
       // stiffness_with_inertia, :383-396)
       double du[3] = {0.0, 0.0, 0.0};
@@ -1353,6 +1416,14 @@ extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *
     scatter(P, e, fe.data(), K ? lk.data() : nullptr, R, K);
   }
   return err;
+}
+
+extern "C" int orc_assemble_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                      const double *u_n, const double *u_nm1, const double *p_np1,
+                                      const double *p_n, const double *p_nm1, double alpha, double dt_np1,
+                                      double dt_n, double rho, double *R, double *K) {
+  return orc_assemble_transient_state(P, mat, u_np1, u_n, u_nm1, p_np1, p_n, p_nm1, alpha, dt_np1, dt_n, rho,
+                                      nullptr, nullptr, nullptr, R, K);
 }
 
 extern "C" long orc_cp_update_batch(const orc_material *mat, long nqp, const double *F, double dt,

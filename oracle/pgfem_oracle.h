@@ -169,6 +169,16 @@ int orc_assemble_transient(const orc_problem *P, const orc_material *mat, const 
                            const double *p_n, const double *p_nm1, double alpha, double dt_np1,
                            double dt_n, double rho, double *R, double *K);
 
+/* The same with the per-point state: crystal plasticity (state AoS 10 per
+ * point: pF, g) takes the state at t_{n-1} and t_n, runs the point update at
+ * F_{n+1} (state_np1 out, may be NULL) and evaluates each mid point with the
+ * mid-point plastic part; HE ignores the state.  Returns 1 for other models. */
+int orc_assemble_transient_state(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                 const double *u_n, const double *u_nm1, const double *p_np1,
+                                 const double *p_n, const double *p_nm1, double alpha, double dt_np1,
+                                 double dt_n, double rho, const double *state_nm1, const double *state_n,
+                                 double *state_np1, double *R, double *K);
+
 /* Number of quadrature points per element for nne (1 for 4, 4 for 10). */
 int orc_nint(int nne);
 

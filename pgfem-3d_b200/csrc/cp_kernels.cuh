@@ -796,7 +796,8 @@ inline size_t cp_tangent_smem() { return sizeof(double) * kCtPts * kCtQS; }
 
 namespace pgb {
 
-// Deformation gradient per point of linear tets (constant gradients).
+// Deformation gradient per point of linear tets (constant gradients); status
+// (inverted elements) and detJw may be null.
 __global__ void k_cp_F(const double *X, const double *unode, const int *conn, long nn, long ne,
                        const double *F0, double *F, double *detJw, unsigned long long *status) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -830,13 +831,63 @@ __global__ void k_cp_F(const double *X, const double *unode, const int *conn, lo
     ok = det3(Fe) > 0.0;
   }
   if (!ok) {
-    atomicAdd(&status[0], 1ull);
+    if (status) atomicAdd(&status[0], 1ull);
 #pragma unroll
     for (int i = 0; i < 9; i++) Fe[i] = (i % 4 == 0 ? 1.0 : 0.0);
   }
 #pragma unroll
   for (int i = 0; i < 9; i++) F[i * ne + e] = Fe[i];
-  detJw[e] = ok ? dJ / 6.0 : 0.0;
+  if (detJw) detJw[e] = ok ? dJ / 6.0 : 0.0;
+}
+
+// Directional derivative of P / pJ = F M S M^T, with pJ = det pF = 1 / det M
+// carried as -tr(M^-1 dM) F M S M^T, for the increments dF and dM
+// (Ce = M^T F^T F M; h the stress at Ce; C = F^T F, FM = F M, FMS = F M S,
+// Pk = F M S M^T, Mi = M^-1).
+__device__ __forceinline__ void cp_piola_dir(const Mat &mat, const NeoHooke &h, const double *F, const double *M,
+                                             const double *Mi, const double *C, const double *FM,
+                                             const double *FMS, const double *Pk, const double *dF,
+                                             const double *dM, double *dP) {
+  // dCe = dM^T C M + M^T (dF^T F + F^T dF) M + M^T C dM
+  double dC[9], a1[9], a2[9], dCe[9], CdM[9];
+  mm3tn(dF, F, a1);
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) dC[i * 3 + j] = a1[i * 3 + j] + a1[j * 3 + i];
+  mm3(C, dM, CdM);
+  mm3(dC, M, a1);
+  mm3tn(M, a1, a2);  // M^T dC M
+  double b1[9];
+  mm3tn(M, CdM, b1);  // M^T C dM
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int j = 0; j < 3; j++) dCe[i * 3 + j] = a2[i * 3 + j] + b1[i * 3 + j] + b1[j * 3 + i];
+  double dS[9];
+  nh_dS(mat, h, dCe, dS);
+  // dF M S M^T + F dM S M^T + F M dS M^T + F M S dM^T - tr(M^-1 dM) F M S M^T
+  double q1[9], q2[9], q3[9], tmp[9];
+  mm3(dF, M, tmp);
+  mm3(tmp, h.S, q1);
+  mm3nt(q1, M, dP);
+  mm3(F, dM, tmp);
+  mm3(tmp, h.S, q2);
+  mm3nt(q2, M, q3);
+#pragma unroll
+  for (int i = 0; i < 9; i++) dP[i] += q3[i];
+  mm3(FM, dS, q1);
+  mm3nt(q1, M, q3);
+#pragma unroll
+  for (int i = 0; i < 9; i++) dP[i] += q3[i];
+  mm3nt(FMS, dM, q3);
+  double trMdM = 0;
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int k = 0; k < 3; k++) trMdM += Mi[i * 3 + k] * dM[k * 3 + i];
+#pragma unroll
+  for (int i = 0; i < 9; i++) dP[i] += q3[i] - trMdM * Pk[i];
 }
 
 struct CpElemArgs {
@@ -857,6 +908,12 @@ struct CpElemArgs {
   long nlist;
   double *lk_out, *fe_out;
   Mat mat;
+  // transient (mid-point rule) element, k_cp_element_tr: F at t_n and
+  // t_{n-1} (SoA 9*ne), the state at t_{n+1} and t_{n-1}, alpha and the two
+  // mid points' residual factors; inverted mid points counted in status[0]
+  const double *F_n, *F_nm1, *state_np1, *state_nm1;
+  double alpha, cA, cB;
+  unsigned long long *status;
 };
 
 // Element residual and tangent of the CM 1-field element with plasticity
@@ -966,47 +1023,10 @@ __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
       dF[gc * 3 + 0] = gN[wn][0];
       dF[gc * 3 + 1] = gN[wn][1];
       dF[gc * 3 + 2] = gN[wn][2];
-      // dCe = dM^T C M + M^T (dF^T F + F^T dF) M + M^T C dM
-      double dC[9], a1[9], a2[9], dCe[9], CM[9], CdM[9];
-      mm3tn(dF, F, a1);
+      double dP[9];
+      cp_piola_dir(A.mat, h, F, M, Mi, C, FM, FMS, Pk, dF, dM, dP);
 #pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) dC[i * 3 + j] = a1[i * 3 + j] + a1[j * 3 + i];
-      mm3(C, M, CM);
-      mm3(C, dM, CdM);
-      mm3(dC, M, a1);
-      mm3tn(M, a1, a2);  // M^T dC M
-      double b1[9];
-      mm3tn(M, CdM, b1);  // M^T C dM
-#pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) dCe[i * 3 + j] = a2[i * 3 + j] + b1[i * 3 + j] + b1[j * 3 + i];
-      double dS[9];
-      nh_dS(A.mat, h, dCe, dS);
-      // dP/pJ = dF M S M^T + F dM S M^T + F M dS M^T + F M S dM^T - tr(M^-1 dM) F M S M^T
-      double q1[9], q2[9], q3[9], dP[9], tmp[9];
-      mm3(dF, M, tmp);
-      mm3(tmp, h.S, q1);
-      mm3nt(q1, M, dP);
-      mm3(F, dM, tmp);
-      mm3(tmp, h.S, q2);
-      mm3nt(q2, M, q3);
-#pragma unroll
-      for (int i = 0; i < 9; i++) dP[i] += q3[i];
-      mm3(FM, dS, q1);
-      mm3nt(q1, M, q3);
-#pragma unroll
-      for (int i = 0; i < 9; i++) dP[i] += q3[i];
-      mm3nt(FMS, dM, q3);
-      double trMdM = 0;
-#pragma unroll
-      for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int k = 0; k < 3; k++) trMdM += Mi[i * 3 + k] * dM[k * 3 + i];
-#pragma unroll
-      for (int i = 0; i < 9; i++) dP[i] = w * pJ * (dP[i] + q3[i] - trMdM * Pk[i]);
+      for (int i = 0; i < 9; i++) dP[i] *= w * pJ;
       if (dense) {  // column (wn, gc) of the element matrix, idx_K order
         for (int a = 0; a < 4; a++)
 #pragma unroll
@@ -1031,6 +1051,151 @@ __global__ void __launch_bounds__(128) k_cp_element(const CpElemArgs A) {
   }
 }
 
+// Transient (mid-point rule) element of crystal plasticity on linear tets
+// (residuals_el_constitutive_model_n_plus_alpha and
+// stiffness_el_constitutive_model_w_inertia_1f, src/constitutive_model.cc:
+// 1905-2170, 2803-2958).  At a mid point F = mid(F_a, F_b), pF = mid(pF_a,
+// pF_b), M = pF^-1 and P = det(pF) F M S(M^T F^T F M) M^T:
+//   R += cA w P(n+alpha) grad N_a + cB w P(n-1+alpha) grad N_a
+//   K += cA w dP(n+alpha) grad N_a
+// where only the newer mid point depends on u_{n+1}: dF(n+alpha) = alpha dF,
+// dM(n+alpha) = -M (alpha dpF_{n+1}) M and dpF_{n+1} = -pF_{n+1}
+// d(pF_{n+1}^-1) pF_{n+1}, from the consistent derivative of the local
+// update (pF_{n+1}^-1 = pF_n^-1 M_u, dM_u = dM/dF : dF).
+__global__ void __launch_bounds__(128) k_cp_element_tr(const CpElemArgs A) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= A.ne) return;
+  const long S = A.ne;
+  const double w = A.detJw[e];
+  if (!(w > 0.0)) return;
+  int nd[4];
+  double x[4][3];
+#pragma unroll
+  for (int a = 0; a < 4; a++) {
+    nd[a] = A.conn[(long)a * A.ne + e];
+#pragma unroll
+    for (int i = 0; i < 3; i++) x[a][i] = A.X[i * A.nn + nd[a]];
+  }
+  double dX[9], dXi[9];
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int c = 0; c < 3; c++) dX[i * 3 + c] = x[c + 1][i] - x[0][i];
+  inv3(dX, dXi);
+  double gN[4][3];
+#pragma unroll
+  for (int j = 0; j < 3; j++) {
+    gN[1][j] = dXi[0 * 3 + j];
+    gN[2][j] = dXi[1 * 3 + j];
+    gN[3][j] = dXi[2 * 3 + j];
+    gN[0][j] = -(gN[1][j] + gN[2][j] + gN[3][j]);
+  }
+  const double al = A.alpha;
+  double Fa[9], Fb[9], pFa[9], pFb[9], pF2[9], pF1[9];
+#pragma unroll
+  for (int i = 0; i < 9; i++) {
+    const double f2 = A.F[i * S + e], f1 = A.F_n[i * S + e], f0 = A.F_nm1[i * S + e];
+    pF2[i] = A.state_np1[i * S + e];
+    pF1[i] = A.state_n[i * S + e];
+    const double p0 = A.state_nm1[i * S + e];
+    Fa[i] = (1.0 - al) * f1 + al * f2;
+    Fb[i] = (1.0 - al) * f0 + al * f1;
+    pFa[i] = (1.0 - al) * pF1[i] + al * pF2[i];
+    pFb[i] = (1.0 - al) * p0 + al * pF1[i];
+  }
+  if (!(det3(Fa) > 0.0) || !(det3(Fb) > 0.0)) {  // getJacobian of each mid point
+    atomicAdd(&A.status[0], 1ull);
+    return;
+  }
+  double Ma[9], Mb[9];
+  if (!inv3(pFa, Ma) || !inv3(pFb, Mb)) return;
+  double Re[12];
+  {  // the older mid point: residual only
+    double C[9], t[9], Ce[9];
+    mm3tn(Fb, Fb, C);
+    mm3(C, Mb, t);
+    mm3tn(Mb, t, Ce);
+    NeoHooke hb;
+    if (!nh_stress(A.mat, Ce, hb)) return;
+    double FM[9], FMS[9], Pb[9];
+    mm3(Fb, Mb, FM);
+    mm3(FM, hb.S, FMS);
+    mm3nt(FMS, Mb, Pb);
+    const double cb = A.cB * w * det3(pFb);
+#pragma unroll
+    for (int a = 0; a < 4; a++)
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        Re[a * 3 + i] = cb * (Pb[i * 3] * gN[a][0] + Pb[i * 3 + 1] * gN[a][1] + Pb[i * 3 + 2] * gN[a][2]);
+  }
+  double C[9], FM[9], FMS[9], Pa[9];
+  NeoHooke h;
+  {
+    double t[9], Ce[9];
+    mm3tn(Fa, Fa, C);
+    mm3(C, Ma, t);
+    mm3tn(Ma, t, Ce);
+    if (!nh_stress(A.mat, Ce, h)) return;
+  }
+  mm3(Fa, Ma, FM);
+  mm3(FM, h.S, FMS);
+  mm3nt(FMS, Ma, Pa);
+  const double ca = A.cA * w * det3(pFa);
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+      Re[a * 3 + i] += ca * (Pa[i * 3] * gN[a][0] + Pa[i * 3 + 1] * gN[a][1] + Pa[i * 3 + 2] * gN[a][2]);
+  const unsigned mk[4] = {A.mask[nd[0]], A.mask[nd[1]], A.mask[nd[2]], A.mask[nd[3]]};
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      const int id = A.dof[i * A.nn + nd[a]];
+      if (id > 0) atomicAdd(A.R + (id - 1), Re[a * 3 + i]);
+    }
+  if (!A.K) return;
+  double pF1i[9];
+  inv3(pF1, pF1i);
+  for (int wn = 0; wn < 4; wn++) {
+    if (!mk[wn]) continue;
+    for (int gc = 0; gc < 3; gc++) {
+      if (!((mk[wn] >> gc) & 1u)) continue;
+      double dMu[9], dMtl[9], t1[9], t2[9], dMa[9];
+#pragma unroll
+      for (int ij = 0; ij < 9; ij++)
+        dMu[ij] = A.out[(9 + ij * 9 + gc * 3 + 0) * S + e] * gN[wn][0] +
+                  A.out[(9 + ij * 9 + gc * 3 + 1) * S + e] * gN[wn][1] +
+                  A.out[(9 + ij * 9 + gc * 3 + 2) * S + e] * gN[wn][2];
+      mm3(pF1i, dMu, dMtl);  // d(pF_{n+1}^-1)
+      mm3(pF2, dMtl, t1);
+      mm3(t1, pF2, t2);      // -dpF_{n+1}
+      mm3(Ma, t2, t1);
+      mm3(t1, Ma, dMa);
+#pragma unroll
+      for (int i = 0; i < 9; i++) dMa[i] *= al;
+      double dF[9];
+#pragma unroll
+      for (int i = 0; i < 9; i++) dF[i] = 0.0;
+      dF[gc * 3 + 0] = al * gN[wn][0];
+      dF[gc * 3 + 1] = al * gN[wn][1];
+      dF[gc * 3 + 2] = al * gN[wn][2];
+      double dP[9];
+      cp_piola_dir(A.mat, h, Fa, Ma, pFa, C, FM, FMS, Pa, dF, dMa, dP);
+      const long pcol = (e * 4 + 0) * 4 + wn;
+      for (int a = 0; a < 4; a++) {
+        if (!mk[a]) continue;
+        const long base = (long)A.rowptr0[nd[a]] + A.pos[pcol + a * 4] + rank_of(mk[wn], gc);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          if (!((mk[a] >> i) & 1u)) continue;
+          const double v = ca * (dP[i * 3] * gN[a][0] + dP[i * 3 + 1] * gN[a][1] + dP[i * 3 + 2] * gN[a][2]);
+          atomicAdd(A.K + base + (long)rank_of(mk[a], i) * A.rowlen[nd[a]], v);
+        }
+      }
+    }
+  }
+}
 
 // ---- learned warm start: features, guess, training pairs -------------------
 

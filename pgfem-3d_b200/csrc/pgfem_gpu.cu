@@ -50,6 +50,7 @@ struct pgfem_gpu_ctx {
   double *unode = nullptr;
   double *F0 = nullptr;
   double *state_n = nullptr, *state_np1 = nullptr;
+  double *state_nm1 = nullptr;  // crystal plasticity: the state at t_{n-1} (transient element)
   unsigned long long *status = nullptr;
   // scratch for host-buffer calls
   double *d_u = nullptr, *d_presc = nullptr, *d_R = nullptr, *d_K = nullptr;
@@ -111,6 +112,7 @@ struct pgfem_gpu_ctx {
   // transient calls: u and prescribed values at t_{n+1}, t_n, t_{n-1}, a
   // mid-point / combination vector of each, the second residual
   double *tr_buf = nullptr;
+  double *tr_F = nullptr;  // crystal plasticity: F at t_n and t_{n-1} per element (SoA 2 x 9*ne)
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -327,7 +329,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_desc_tr, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
-                  c->nbc_load, c->tr_buf};
+                  c->nbc_load, c->tr_buf, c->state_nm1, c->tr_F};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->zfork) cudaEventDestroy(c->zfork);
@@ -576,11 +578,17 @@ struct CpElemList {
   double *lk, *fe;
 };
 
+// the transient element stage of assemble_cp (k_cp_element_tr)
+struct CpTransient {
+  const double *F_n, *F_nm1;
+  double alpha, cA, cB;
+};
+
 // The CP path: F per element, the local Newton (optionally from the network's
 // guess), the consistent tangent, then the element stage -- scattered into the
 // CSR (d_R, d_K) or, with el, the listed elements' dense blocks.
 int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStream_t s,
-                const CpElemList *el = nullptr) {
+                const CpElemList *el = nullptr, const CpTransient *tr = nullptr) {
   k_cp_F<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(c->X, c->unode, c->conn, c->nn, c->ne, c->F0, c->cp_F,
                                                           c->cp_detJw, c->status);
   CK(cudaGetLastError());
@@ -669,6 +677,19 @@ int assemble_cp(pgfem_gpu_ctx *c, double *d_R, double *d_K, double dt, cudaStrea
     b.R = d_R;
     b.K = d_K;
     b.mat = c->mat;
+    if (tr) {  // mid-point rule: R into d_R, K (if any) into d_K
+      b.F_n = tr->F_n;
+      b.F_nm1 = tr->F_nm1;
+      b.state_np1 = c->state_np1;
+      b.state_nm1 = c->state_nm1;
+      b.alpha = tr->alpha;
+      b.cA = tr->cA;
+      b.cB = tr->cB;
+      b.status = c->status;
+      k_cp_element_tr<<<(unsigned)((c->ne + 127) / 128), 128, 0, s>>>(b);
+      CK(cudaGetLastError());
+      return PGFEM_GPU_OK;
+    }
     if (el) {  // element level: dense blocks of the listed elements
       b.elist = el->list;
       b.nlist = el->n;
@@ -1011,6 +1032,7 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     if ((r = dalloc(c, &c->state_n, (size_t)c->nstate * c->nqp)) ||
         (r = dalloc(c, &c->state_np1, (size_t)c->nstate * c->nqp)))
       return fail(r);
+    if (c->model == PGFEM_MODEL_CP && (r = dalloc(c, &c->state_nm1, (size_t)c->nstate * c->nqp))) return fail(r);
   }
   if (cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), c->stream) != cudaSuccess)
     return fail(PGFEM_GPU_ECUDA);
@@ -1079,6 +1101,8 @@ int pgfem_gpu_create(const pgfem_mesh_desc *m, const pgfem_material_desc *mat, c
     }
     cudaMemcpyAsync(c->state_n, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     cudaMemcpyAsync(c->state_np1, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (c->state_nm1)
+      cudaMemcpyAsync(c->state_nm1, s0.data(), s0.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return fail(PGFEM_GPU_ECUDA);
   }
   // colours for the deterministic scatter mode
@@ -1435,17 +1459,32 @@ int pgfem_gpu_set_state(pgfem_gpu_ctx *c, const double *st) {
   }
   CK(cudaMemcpyAsync(c->state_n, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->state_np1, c->state_n, soa.size() * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+  if (c->state_nm1)
+    CK(cudaMemcpyAsync(c->state_nm1, c->state_n, soa.size() * sizeof(double), cudaMemcpyDeviceToDevice,
+                       c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_state_nm1(pgfem_gpu_ctx *c, const double *st) {
+  if (!c || !st) return PGFEM_GPU_EINVAL;
+  if (!c->state_nm1) return PGFEM_GPU_EINVAL;  // crystal plasticity only
+  const long nq = c->nqp;
+  std::vector<double> soa((size_t)10 * nq);
+  for (long q = 0; q < nq; q++)
+    for (int k = 0; k < 10; k++) soa[k * nq + q] = st[q * 10 + k];
+  CK(cudaMemcpyAsync(c->state_nm1, soa.data(), soa.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return PGFEM_GPU_OK;
 }
 
 int pgfem_gpu_get_state(pgfem_gpu_ctx *c, int level, double *st) {
-  if (!c || !st || (level != 0 && level != 1)) return PGFEM_GPU_EINVAL;
+  if (!c || !st || level < 0 || level > 2 || (level == 2 && !c->state_nm1)) return PGFEM_GPU_EINVAL;
   if (!c->nstate) return PGFEM_GPU_OK;
   const long nq = c->nqp;
   std::vector<double> soa((size_t)c->nstate * nq);
-  CK(cudaMemcpyAsync(soa.data(), level ? c->state_np1 : c->state_n, soa.size() * sizeof(double),
-                     cudaMemcpyDeviceToHost, c->stream));
+  const double *src = level == 2 ? c->state_nm1 : level ? c->state_np1 : c->state_n;
+  CK(cudaMemcpyAsync(soa.data(), src, soa.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   for (long q = 0; q < nq; q++) {
     double *s = st + q * 10;
@@ -1463,6 +1502,9 @@ int pgfem_gpu_get_state(pgfem_gpu_ctx *c, int level, double *st) {
 
 int pgfem_gpu_commit_state(pgfem_gpu_ctx *c) {
   if (!c) return PGFEM_GPU_EINVAL;
+  if (c->state_nm1)  // n-1 <- n first
+    CK(cudaMemcpyAsync(c->state_nm1, c->state_n, sizeof(double) * c->nstate * c->nqp, cudaMemcpyDeviceToDevice,
+                       c->stream));
   if (c->nstate)
     CK(cudaMemcpyAsync(c->state_n, c->state_np1, sizeof(double) * c->nstate * c->nqp,
                        cudaMemcpyDeviceToDevice, c->stream));
@@ -1699,6 +1741,12 @@ int pgfem_gpu_read_restart(pgfem_gpu_ctx *c, const char *path, double *u_nm1, do
       st[10 * q + 9] = b[60];
     }
     if ((r = pgfem_gpu_set_state(c, st.data()))) return r;
+    for (long q = 0; q < c->nqp; q++) {  // pF_{n-1}, g_{n-1}: the state at t_{n-1}
+      const double *b = blocks.data() + (size_t)bs * q;
+      for (int k = 0; k < 9; k++) st[10 * q + k] = b[27 + k];
+      st[10 * q + 9] = b[61];
+    }
+    if ((r = pgfem_gpu_set_state_nm1(c, st.data()))) return r;
     CK(cudaMemcpyAsync(c->cp_Fn, Fs.data(), sizeof(double) * Fs.size(), cudaMemcpyHostToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
   }
@@ -1751,13 +1799,71 @@ int pgfem_gpu_assemble_RK(pgfem_gpu_ctx *c, const double *u, const double *presc
   return assemble_host(c, u, presc, R, K, st, dt);
 }
 
+// The crystal-plasticity transient on device buffers (displacements and
+// prescribed values at t_{n+1}, t_n, t_{n-1}; tua / tpa / tR2 scratch): the
+// surface terms at the two mid points, scaled like the element's, F at t_n
+// and t_{n-1}, then the point update at u_{n+1} and the mid-point element
+// stage (k_cp_element_tr) into the context's R and K.
+static int transient_cp(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, const double *tu0,
+                        const double *tp2, const double *tp1, const double *tp0, double *tua, double *tpa,
+                        double *tR2, double alpha, double dt_np1, double dt_n, bool wantK, cudaStream_t s) {
+  int r;
+  const long nd = c->ndof, np = c->npres;
+  const unsigned gu = (unsigned)((std::max<long>(1, nd) + 255) / 256),
+                 gp = (unsigned)((std::max<long>(1, np) + 255) / 256),
+                 g3 = (unsigned)((3 * c->nn + 255) / 256), ge = (unsigned)((c->ne + 127) / 128);
+  double *dK = wantK ? c->d_K : nullptr;
+  const double cA = -dt_np1 * (1.0 - alpha), cB = -dt_n * alpha;
+  CK(cudaMemsetAsync(c->d_R, 0, sizeof(double) * nd, s));
+  if (dK) CK(cudaMemsetAsync(dK, 0, sizeof(double) * c->nnz, s));
+  auto expand = [&](const double *u, const double *p) {
+    k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, u, np ? p : nullptr, c->unode);
+  };
+  auto blend = [&](const double *x, const double *y, const double *px, const double *py) {
+    k_blend<<<gu, 256, 0, s>>>(tua, x, y, alpha, nd);
+    if (np) k_blend<<<gp, 256, 0, s>>>(tpa, px, py, alpha, np);
+    expand(tua, tpa);
+  };
+  if (c->nbc_nface) {
+    // the newer mid point into R and K, scaled as the element's terms are
+    blend(tu1, tu2, tp1, tp2);
+    c->nbc_desc_cur = c->nbc_desc_tr;
+    r = launch_neumann(c, c->d_R, dK, s);
+    c->nbc_desc_cur = nullptr;
+    if (r) return r;
+    k_scale_add<<<gu, 256, 0, s>>>(c->d_R, cA, nullptr, 0.0, nd);
+    if (dK)
+      k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(dK, -alpha * (1.0 - alpha) * dt_np1, nullptr,
+                                                                     0.0, c->nnz);
+    // the older mid point: residual only
+    blend(tu0, tu1, tp0, tp1);
+    CK(cudaMemsetAsync(tR2, 0, sizeof(double) * nd, s));
+    c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
+    r = launch_neumann(c, tR2, nullptr, s);
+    c->nbc_desc_cur = nullptr;
+    if (r) return r;
+    k_scale_add<<<gu, 256, 0, s>>>(c->d_R, 1.0, tR2, cB, nd);
+  }
+  if (!c->tr_F && (r = dalloc(c, &c->tr_F, (size_t)18 * c->ne))) return r;
+  expand(tu1, tp1);
+  k_cp_F<<<ge, 128, 0, s>>>(c->X, c->unode, c->conn, c->nn, c->ne, nullptr, c->tr_F, nullptr, nullptr);
+  expand(tu0, tp0);
+  k_cp_F<<<ge, 128, 0, s>>>(c->X, c->unode, c->conn, c->nn, c->ne, nullptr, c->tr_F + (size_t)9 * c->ne, nullptr,
+                            nullptr);
+  expand(tu2, tp2);
+  CK(cudaGetLastError());
+  const CpTransient tr{c->tr_F, c->tr_F + (size_t)9 * c->ne, alpha, cA, cB};
+  return assemble_cp(c, c->d_R, dK, dt_np1, s, nullptr, &tr);
+}
+
 int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
                                     const double *u_nm1, const double *presc_np1, const double *presc_n,
                                     const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
                                     double *R, double *K, pgfem_gpu_status *st) {
   if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
     return PGFEM_GPU_EINVAL;
-  if (c->model != PGFEM_MODEL_HE || c->F0 || c->elem_group || c->three_field) return PGFEM_GPU_EINVAL;
+  if ((c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) || c->F0 || c->elem_group || c->three_field)
+    return PGFEM_GPU_EINVAL;
   // surface loads need their values at t_n and t_{n-1}
   if (c->nbc_nface && c->nbc_hist_n.size() != (size_t)3 * c->nbc_nfeat) return PGFEM_GPU_EINVAL;
   if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
@@ -1798,27 +1904,33 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
     CK(cudaMemcpyAsync(c->nbc_desc_tr, d.data(), sizeof(double) * d.size(), cudaMemcpyHostToDevice, s));
     c->nbc_desc_cur = c->nbc_desc_tr;
   }
-  // quasi-static R and K at u_{n+a}
-  k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
-  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
-  CK(cudaGetLastError());
-  r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1);
-  if (r) {
+  if (c->model == PGFEM_MODEL_CP) {
+    r = transient_cp(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, K != nullptr, s);
     c->nbc_desc_cur = nullptr;
-    return r;
+    if (r) return r;
+  } else {
+    // quasi-static R and K at u_{n+a}
+    k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
+    if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
+    CK(cudaGetLastError());
+    r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1);
+    if (r) {
+      c->nbc_desc_cur = nullptr;
+      return r;
+    }
+    if (c->nbc_nface) c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
+    // quasi-static R at u_{n-1+a}
+    k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, c->ndof);
+    if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, c->npres);
+    CK(cudaGetLastError());
+    r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n);
+    c->nbc_desc_cur = nullptr;
+    if (r) return r;
+    // the mid-point combination
+    k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
+    if (K) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
+                                                                         nullptr, 0.0, c->nnz);
   }
-  if (c->nbc_nface) c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
-  // quasi-static R at u_{n-1+a}
-  k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, c->ndof);
-  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, c->npres);
-  CK(cudaGetLastError());
-  r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n);
-  c->nbc_desc_cur = nullptr;
-  if (r) return r;
-  // the mid-point combination
-  k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
-  if (K) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
-                                                                       nullptr, 0.0, c->nnz);
   // inertia: v = dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1} at the nodes
   k_comb3<<<gu, 256, 0, s>>>(tua, tu2, dt_n, tu1, -(dt_np1 + dt_n), tu0, dt_np1, c->ndof);
   if (c->npres) k_comb3<<<gp, 256, 0, s>>>(tpa, tp2, dt_n, tp1, -(dt_np1 + dt_n), tp0, dt_np1, c->npres);

@@ -88,6 +88,7 @@ def lib():
             "pgfem_gpu_nnz": (C.c_long, [_P]),
             "pgfem_gpu_set_state": (C.c_int, [_P, _P]),
             "pgfem_gpu_get_state": (C.c_int, [_P, C.c_int, _P]),
+            "pgfem_gpu_set_state_nm1": (C.c_int, [_P, _P]),
             "pgfem_gpu_commit_state": (C.c_int, [_P]),
             "pgfem_gpu_reset_state": (C.c_int, [_P]),
             "pgfem_gpu_assemble_R": (C.c_int, [_P, _P, _P, C.c_double, _P, _P]),
@@ -359,7 +360,14 @@ class Context:
         state = np.ascontiguousarray(state, dtype=np.float64)
         _check("pgfem_gpu_set_state", lib().pgfem_gpu_set_state(self.h, _ptr(state)))
 
+    def set_state_nm1(self, state):
+        """Crystal plasticity: the state at t_{n-1} (the transient element's older
+        mid point); set_state sets it to the given state as well."""
+        state = np.ascontiguousarray(state, dtype=np.float64)
+        _check("pgfem_gpu_set_state_nm1", lib().pgfem_gpu_set_state_nm1(self.h, _ptr(state)))
+
     def get_state(self, level=1):
+        """level 0: t_n, 1: t_{n+1}, 2: t_{n-1} (crystal plasticity)."""
         out = np.zeros((self.ne * self.nint, max(self.ns, 1)))
         _check("pgfem_gpu_get_state", lib().pgfem_gpu_get_state(self.h, level, _ptr(out)))
         return out
@@ -394,9 +402,11 @@ class Context:
 
     def assemble_RK_transient(self, u_np1, u_n, u_nm1, alpha, dt_np1, dt_n, rho, presc=(None, None, None),
                               want_K=True):
-        """Transient (mid-point rule) R and K of a hyperelastic context
-        (pgfem_gpu_assemble_RK_transient); presc = prescribed values at
-        t_{n+1}, t_n, t_{n-1}.  Returns (R, K or None, Status)."""
+        """Transient (mid-point rule) R and K of a hyperelastic or
+        crystal-plasticity context (pgfem_gpu_assemble_RK_transient); presc =
+        prescribed values at t_{n+1}, t_n, t_{n-1}.  Crystal plasticity reads
+        the context's states at t_{n-1} and t_n and writes the state at
+        t_{n+1}.  Returns (R, K or None, Status)."""
         us = [np.ascontiguousarray(v, dtype=np.float64) for v in (u_np1, u_n, u_nm1)]
         ps = [self._presc(v) for v in presc]
         R = np.zeros(self.ndof)

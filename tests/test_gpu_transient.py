@@ -7,7 +7,10 @@ steps, R and K at the parity tolerance (1e-10); below the density threshold
 the call is the quasi-static assembly at t_{n+1}; with surface loads (tractions
 and pressures, values at the three times) the mid-point surface terms equal the
 oracle's; J2 contexts, surface loads without their earlier values and bad time
-parameters are rejected."""
+parameters are rejected.  Crystal plasticity (linear tets): with the states at
+t_{n-1} and t_n from two committed load steps, R, K and the state at t_{n+1}
+equal the oracle's mid-point element (orc_assemble_transient_state), with and
+without surface loads; the commit moves the state at t_n to t_{n-1}."""
 import numpy as np
 import pytest
 
@@ -134,4 +137,86 @@ def test_transient_with_surface_loads(gpu, maker, alpha):
     _, Rqo, Kqo, _ = P.assemble(mat, us[2], ps[2] if ps else None)
     check_R(Rq, Rqo)
     check_K(Kq, Kqo, p.Ap)
+    ctx.close()
+
+
+def _cp_marched(n=3, ngrains=8):
+    """A CP context and the oracle after two committed quasi-static load steps:
+    the states at t_{n-1} and t_n, the displacements of steps 1, 2 and a
+    perturbed step 3 as u_{n-1}, u_n, u_{n+1}."""
+    p = wl.cp_p1(n=n, seed=2, ngrains=ngrains)
+    ctx = p.context()
+    P, mat = oracle.from_workload(p)
+    st = p.state.copy()
+    hist = []
+    for s in (1, 2):
+        u = p.displacement(s)
+        _, _, status = ctx.assemble_RK(u, dt=p.dt)
+        assert status.ok(), status.as_dict()
+        ctx.commit_state()
+        err, _, _, st = P.assemble(mat, u, state_n=st, dt=p.dt, want_K=False, nthreads=8)
+        assert err == 0
+        hist.append(st)
+    s_nm1, s_n = hist
+    assert np.abs(ctx.get_state(2) - s_nm1).max() <= 1e-10 * np.abs(s_nm1).max()
+    assert np.abs(ctx.get_state(0) - s_n).max() <= 1e-10 * np.abs(s_n).max()
+    rng = np.random.default_rng(5)
+    u2 = p.displacement(3) + 2e-4 * rng.uniform(-1, 1, p.ndof) / n
+    return p, ctx, P, mat, (p.displacement(1), p.displacement(2), u2), s_nm1, s_n
+
+
+@pytest.mark.parametrize("alpha", [0.5, 0.3])
+def test_cp_transient_matches_oracle(gpu, alpha):
+    p, ctx, P, mat, us, s_nm1, s_n = _cp_marched()
+    dt1, dt0, rho = p.dt, 0.8 * p.dt, 5.0e4
+    R, K, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho)
+    assert st.ok(), st.as_dict()
+    err, Ro, Ko, so = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, s_nm1, s_n)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    sg = ctx.get_state(1)
+    assert np.abs(sg - so).max() <= 1e-10 * np.abs(so).max()
+    assert np.abs(so[:, :9] - s_n[:, :9]).max() > 1e-6  # the plastic part moves in this step
+    # inertia and the plastic mid points both carry weight
+    _, R0, _, _ = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, 0.0, s_nm1, s_n)
+    assert np.linalg.norm(Ro - R0) > 1e-2 * np.linalg.norm(Ro)
+    _, Rf, _, _ = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, s_n, s_n)
+    assert np.linalg.norm(Ro - Rf) > 1e-3 * np.linalg.norm(Ro)  # the state at t_{n-1} matters
+    # residual only: the same R
+    R2, K2, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho, want_K=False)
+    assert K2 is None and st.ok()
+    check_R(R2, R, 1e-13)
+    # commit: t_n -> t_{n-1}, t_{n+1} -> t_n
+    ctx.commit_state()
+    assert np.abs(ctx.get_state(2) - s_n).max() <= 1e-10 * np.abs(s_n).max()
+    assert np.abs(ctx.get_state(0) - so).max() <= 1e-10 * np.abs(so).max()
+    ctx.close()
+
+
+def test_cp_transient_with_surface_loads(gpu):
+    p, ctx, P, mat, us, s_nm1, s_n = _cp_marched()
+    el, fc, ft = [], [], []
+    for k, (axis, v) in enumerate([(0, 1.0), (2, 1.0)]):
+        e, f = wl.box_faces(p.X, p.conn, axis, v)
+        el.append(e)
+        fc.append(f)
+        ft.append(np.full(len(e), k, dtype=np.int32))
+    el, fc, ft = np.concatenate(el), np.concatenate(fc), np.concatenate(ft)
+    types = np.array([3, 1])
+    L2 = np.array([[40.0, -15.0, 9.0], [60.0, 0.0, 0.0]])
+    L1, L0 = 0.7 * L2 + 3.0, 0.4 * L2 - 5.0
+    ctx.set_neumann(el, fc, ft, types, L2)
+    ctx.set_neumann_load_history(L1, L0)
+    alpha, dt1, dt0, rho = 0.4, p.dt, 0.6 * p.dt, 5.0e4
+    R, K, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho)
+    assert st.ok(), st.as_dict()
+    P.set_neumann(el, fc, types[ft], L2[ft], load_n=L1[ft], load_nm1=L0[ft])
+    err, Ro, Ko, so = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, s_nm1, s_n)
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    P0, _ = oracle.from_workload(p)
+    _, R0, _, _ = oracle.assemble_transient_cp(P0, mat, us[2], us[1], us[0], alpha, dt1, dt0, rho, s_nm1, s_n)
+    assert np.linalg.norm(Ro - R0) > 1e-3 * np.linalg.norm(Ro)
     ctx.close()

@@ -114,3 +114,86 @@ def test_surface_loads_constant_in_time(nne):
         cK = -dt1 * al * (1 - al)
         np.testing.assert_allclose(Rs, cR * (Rq1 - Rq0), rtol=0, atol=1e-12 * np.abs(Rs).max())
         np.testing.assert_allclose(Ks, cK * (Kq1 - Kq0), rtol=0, atol=1e-10 * np.abs(Kq1 - Kq0).max())
+
+
+# ---- crystal plasticity: the mid-point plastic state ---------------------------
+def _cp_history(n=2, ngrains=4):
+    """A CP problem marched through two quasi-static steps of its ramp (slip
+    active): the states at t_{n-1} (step 1) and t_n (step 2) and the
+    displacements of steps 1, 2, 3 as u_{n-1}, u_n, u_{n+1}."""
+    p = wl.cp_p1(n=n, seed=2, ngrains=ngrains)
+    P, mat = oracle.from_workload(p)
+    us = [p.displacement(s) for s in (1, 2, 3)]
+    err, _, _, s_nm1 = P.assemble(mat, us[0], state_n=p.state, dt=p.dt, want_K=False)
+    assert err == 0
+    err, _, _, s_n = P.assemble(mat, us[1], state_n=s_nm1, dt=p.dt, want_K=False)
+    assert err == 0
+    return p, P, mat, us, s_nm1, s_n
+
+
+def test_cp_transient_end_points_are_the_quasi_static_residual():
+    """alpha = 1 keeps only the older mid point at (F_n, pF_n): R = -dt_n r_n;
+    alpha = 0 only the newer one at the same point: R = -dt_np1 r_n; r_n is the
+    quasi-static residual of the step that produced the state at t_n, K = 0
+    (rho = 0).  This pins which state each mid point reads."""
+    p, P, mat, us, s_nm1, s_n = _cp_history()
+    err, r_n, _, s_chk = P.assemble(mat, us[1], state_n=s_nm1, dt=p.dt, want_K=False)
+    assert err == 0 and np.abs(s_chk - s_n).max() <= 1e-13
+    dt1, dt0 = p.dt, 0.7 * p.dt
+    for al, coef in ((1.0, -dt0), (0.0, -dt1)):
+        err, R, K, _ = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], al, dt1, dt0, 0.0, s_nm1, s_n)
+        assert err == 0
+        np.testing.assert_allclose(R, coef * r_n, rtol=0, atol=1e-12 * np.abs(r_n).max())
+        assert np.abs(K).max() == 0.0
+
+
+def test_cp_transient_without_slip_is_the_hyperelastic_one():
+    """A slip resistance far above the stress stops every slip system
+    (gamma_dot = 0, pF = I, dM/du = 0): the CP transient is the hyperelastic
+    one with the same elasticity, inertia included."""
+    p, P, mat, us, _, _ = _cp_history()
+    ne = p.conn.shape[0]
+    st = np.zeros((ne, 10))
+    st[:, [0, 4, 8]] = 1.0
+    st[:, 9] = 1e30
+    mhe = oracle.from_pg_material(p.mat)
+    mhe.model = oracle.HE
+    al, dt1, dt0, rho = 0.35, p.dt, 0.8 * p.dt, 7.5e-3
+    err, R, K, s2 = oracle.assemble_transient_cp(P, mat, us[2], us[1], us[0], al, dt1, dt0, rho, st, st)
+    assert err == 0
+    np.testing.assert_array_equal(s2, st)
+    err, Rh, Kh = oracle.assemble_transient(P, mhe, us[2], us[1], us[0], al, dt1, dt0, rho)
+    assert err == 0
+    np.testing.assert_allclose(R, Rh, rtol=0, atol=1e-13 * np.abs(Rh).max())
+    np.testing.assert_allclose(K, Kh, rtol=0, atol=1e-13 * np.abs(Kh).max())
+
+
+def test_cp_transient_stiffness_is_the_derivative():
+    """K of the CP transient (mid-point plastic part through pF_{n+1}, the
+    consistent derivative of the local update) against central differences
+    of R in u_{n+1}, with slip active and inertia on."""
+    p, P, mat, us, s_nm1, s_n = _cp_history()
+    rng = np.random.default_rng(11)
+    u2 = us[2] + 2e-4 * rng.uniform(-1, 1, p.ndof) / p.meta["n"]
+    al, dt1, dt0, rho = 0.4, p.dt, 0.6 * p.dt, 3e-3
+    err, R, K, s2 = oracle.assemble_transient_cp(P, mat, u2, us[1], us[0], al, dt1, dt0, rho, s_nm1, s_n)
+    assert err == 0
+    assert np.abs(s2[:, :9] - s_n[:, :9]).max() > 1e-6  # the plastic part moved in this step
+    cols = rng.choice(p.ndof, 8, replace=False)
+    h = 1e-7
+    for j in cols:
+        up, um = u2.copy(), u2.copy()
+        up[j] += h
+        um[j] -= h
+        _, Rp, _, _ = oracle.assemble_transient_cp(P, mat, up, us[1], us[0], al, dt1, dt0, rho, s_nm1, s_n,
+                                                   want_K=False)
+        _, Rm, _, _ = oracle.assemble_transient_cp(P, mat, um, us[1], us[0], al, dt1, dt0, rho, s_nm1, s_n,
+                                                   want_K=False)
+        fd = (Rp - Rm) / (2 * h)
+        col = np.zeros(p.ndof)
+        for i in range(p.ndof):  # column j of the CSR K
+            row = slice(p.Ap[i], p.Ap[i + 1])
+            hit = np.nonzero(p.Ai[row] == j)[0]
+            if hit.size:
+                col[i] = K[p.Ap[i] + hit[0]]
+        assert np.abs(col - fd).max() <= 1e-6 * np.abs(col).max(), (j, np.abs(col - fd).max(), np.abs(col).max())
