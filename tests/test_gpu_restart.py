@@ -63,6 +63,7 @@ def test_crystal_plasticity_restart_round_trip(gpu, tmp_path):
         ctx.commit_state()
         hist.append((du.cpu().numpy(), presc))
     (u1, p1), (u2, p2) = hist[-2], hist[-1]
+    assert np.array_equal(ctx.get_state(2), prev_state)  # the context's state at t_{n-1}
     path = str(tmp_path / "box_0_3.res")
     pg.write_restart(ctx, path, u1, u2, p1, p2, state_nm1=prev_state)
     a, b, blocks = pg.restart_parse(path, pg.MODEL_CP, X.shape[0], conn.shape[0], 1)
@@ -81,6 +82,7 @@ def test_crystal_plasticity_restart_round_trip(gpu, tmp_path):
     r1, r2 = pg.read_restart(ctx2, path)
     assert np.array_equal(r1, u1) and np.array_equal(r2, u2)
     assert np.array_equal(ctx2.get_state(0), st)
+    assert np.array_equal(ctx2.get_state(2), prev_state)  # pF_{n-1}, g_{n-1} from the file
     dt, presc = steps[3]
     dp = torch.from_numpy(presc).cuda()
     du2 = torch.from_numpy(r2.copy()).cuda()
