@@ -172,8 +172,8 @@ int pgfem_gpu_set_neumann_load_history(pgfem_gpu_ctx *ctx, int nfeature, const d
  * theta per element (host arrays of ne, element order; theta > 0) and switches
  * every later R+K and residual call of the context to the condensed
  * three-field element; NULL, NULL switches back.  PGFEM_GPU_EINVAL for other
- * elements or models, and, while it is on, for the element-level and the
- * transient calls.  get_three_field reads P and theta back.
+ * elements or models, and, while it is on, for the element-level calls.
+ * get_three_field reads P and theta back.
  * three_field_increments: the local update after a displacement increment du
  * (free-DOF vector; compute_d_theta_dP, src/constitutive_model_3f.cc:494-549)
  * -- dP, d_theta per element from the blocks at u; the caller adds them.
@@ -188,6 +188,27 @@ int pgfem_gpu_three_field_increments(pgfem_gpu_ctx *ctx, const double *u, const 
                                      const double *du, double *dP, double *dtheta, pgfem_gpu_status *st);
 int pgfem_gpu_three_field_update_device(pgfem_gpu_ctx *ctx, const double *d_u, const double *d_u_presc,
                                         const double *d_du, double *d_out, void *stream);
+/* Three-field transient (hyperelastic; residuals_el_constitutive_model_w_inertia_3f
+ * / stiffness_el_constitutive_model_w_inertia_3f, src/constitutive_model.cc:
+ * 2190-2395, 2960-3229).  The context keeps P and theta at t_n and t_{n-1}
+ * per element: set_three_field starts them at its values the first time,
+ * set_three_field_history sets them, and commit_state moves t_n to t_{n-1}
+ * and the current P, theta to t_n.  pgfem_gpu_assemble_RK_transient on a
+ * three-field context (0 < alpha < 1) evaluates the newer mid point at
+ * u_{n+alpha}, P = mid(P_n, P), theta = mid(theta_n, theta) and the older one
+ * at u_{n-1+alpha}, mid(P_{n-1}, P_n), mid(theta_{n-1}, theta_n), combines the
+ * residuals (R_u, R_p, R_t) with -dt_np1 (1 - alpha) and -dt_n alpha, the blocks
+ * of the newer point with -dt_np1 alpha (1 - alpha), condenses, and adds the
+ * inertia terms.  three_field_increments_transient: the local update after a
+ * displacement increment du with those combined blocks (dP, d_theta per
+ * element; the caller adds them). */
+int pgfem_gpu_set_three_field_history(pgfem_gpu_ctx *ctx, const double *P_n, const double *theta_n,
+                                      const double *P_nm1, const double *theta_nm1);
+int pgfem_gpu_three_field_increments_transient(pgfem_gpu_ctx *ctx, const double *u_np1, const double *u_n,
+                                               const double *u_nm1, const double *presc_np1,
+                                               const double *presc_n, const double *presc_nm1, const double *du,
+                                               double alpha, double dt_np1, double dt_n, double *dP,
+                                               double *dtheta, pgfem_gpu_status *st);
 
 /* Device bytes held by the context (mesh, map, state, scratch). */
 long pgfem_gpu_device_bytes(const pgfem_gpu_ctx *ctx);
@@ -245,8 +266,9 @@ int pgfem_gpu_read_status(pgfem_gpu_ctx *ctx, pgfem_gpu_status *st, int clear);
  * factor det pF (residuals_el_constitutive_model_n_plus_alpha); K is the
  * derivative of that R in u_{n+1} through F and pF_{n+1}.  Surface loads at
  * the two mid points as pgfem_gpu_set_neumann_load_history sets them.
- * Hyperelastic and crystal-plasticity contexts without macro deformation,
- * mesh groups or the three-field element (PGFEM_GPU_EINVAL otherwise).  The
+ * Hyperelastic (one- and three-field) and crystal-plasticity contexts
+ * without macro deformation or mesh groups (PGFEM_GPU_EINVAL otherwise; the
+ * three-field form below needs 0 < alpha < 1).  The
  * status counts inverted elements at both mid points. */
 int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *ctx, const double *u_np1, const double *u_n,
                                     const double *u_nm1, const double *presc_np1, const double *presc_n,

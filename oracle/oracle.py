@@ -67,6 +67,10 @@ def lib():
             "orc_element_3f": (C.c_int, [_P, _P, C.c_long, _P, C.c_double, C.c_double, _P, _P, _P, _P, _P]),
             "orc_assemble_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
             "orc_update_3f": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
+            "orc_assemble_3f_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
+                                                    C.c_double, C.c_double, C.c_double, _P, _P]),
+            "orc_update_3f_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
+                                                  C.c_double, C.c_double, _P, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(L, k)
@@ -233,6 +237,31 @@ class Problem:
              for x in (u, u_presc, P, theta, state_n)]
         err = lib().orc_assemble_3f(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(snp1), _p(R), _p(K))
         return (err, R, K) if state_n is None else (err, R, K, snp1)
+
+    def assemble_3f_transient(self, mat, us, Ps, thetas, alpha, dt_np1, dt_n, rho, presc=(None, None, None),
+                              want_K=True):
+        """Transient three-field R, K (hyperelastic): us, presc, Ps, thetas are
+        the values at t_{n+1}, t_n, t_{n-1}.  Returns (err, R, K)."""
+        R = np.zeros(self.ndof)
+        K = np.zeros(self.nnz) if want_K else None
+        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None for x in (*us, *presc)]
+        P3 = np.ascontiguousarray(np.stack(Ps, axis=1), dtype=np.float64)
+        T3 = np.ascontiguousarray(np.stack(thetas, axis=1), dtype=np.float64)
+        err = lib().orc_assemble_3f_transient(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(P3), _p(T3),
+                                              alpha, dt_np1, dt_n, rho, _p(R), _p(K))
+        return err, R, K
+
+    def update_3f_transient(self, mat, us, du, Ps, thetas, alpha, dt_np1, dt_n, presc=(None, None, None)):
+        """Element pressure / volume increments of the transient three-field
+        element after the displacement increment du.  Returns (err, dP, dtheta)."""
+        ne = self.conn.shape[0]
+        dP, dth = np.zeros(ne), np.zeros(ne)
+        a = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None for x in (*us, *presc, du)]
+        P3 = np.ascontiguousarray(np.stack(Ps, axis=1), dtype=np.float64)
+        T3 = np.ascontiguousarray(np.stack(thetas, axis=1), dtype=np.float64)
+        err = lib().orc_update_3f_transient(C.byref(self.s), C.byref(mat), *[_p(x) for x in a], _p(P3), _p(T3),
+                                            alpha, dt_np1, dt_n, _p(dP), _p(dth))
+        return err, dP, dth
 
     def update_3f(self, mat, u, du, P, theta, u_presc=None, state_n=None):
         """Element pressure / volume increments after the displacement increment du."""

@@ -1111,9 +1111,11 @@ extern "C" int orc_assemble(const orc_problem *P, const orc_material *mat, const
 //   f = fu + Kup Ktp^-1 Ktt Kpt^-1 fp - Kup Ktp^-1 ft - Kut Kpt^-1 fp.
 // blk (may be NULL) receives fp, ft, Ktp, Ktt and Kup[nd].
 // ---------------------------------------------------------------------------
-extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
-                              double Pe, double theta, const double *state_n, double *state_np1, double *fe,
-                              double *lk, double *blk) {
+// The uncondensed blocks of one three-field element: fu (nd), Kuu (nd*nd, may
+// be null), and in blk fp, ft, Ktp, Ktt, Kup (nd).
+int element_3f_blocks(const orc_problem *P, const orc_material *mat, long e, const double *u_e, double Pe,
+                      double theta, const double *state_n, double *state_np1, double *fu_out, double *lk,
+                      double *blk) {
   if (mat->model != ORC_MODEL_HE && mat->model != ORC_MODEL_J2) return 1;
   if (mat->model == ORC_MODEL_J2 && !state_n) return 1;
   const int ns = orc_state_size(mat->model);
@@ -1200,19 +1202,48 @@ extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, lon
     }
   }
   if (err) return err;
-  const double Kpt = Ktp, KtpI = 1.0 / Ktp, KptI = 1.0 / Kpt;
+  for (int r = 0; r < nd; r++) fu_out[r] = fu[r];
+  if (lk)
+    for (int i = 0; i < nd * nd; i++) lk[i] = Kuu[i];
+  blk[0] = fp;
+  blk[1] = ft;
+  blk[2] = Ktp;
+  blk[3] = Ktt;
+  for (int r = 0; r < nd; r++) blk[4 + r] = Kup[r];
+  return 0;
+}
+
+// Static condensation of the element's (P, theta) for npres = nVol = 1
+// (condense_F_3F_to_1F / condense_K_3F_to_1F, src/constitutive_model_3f.cc,
+// with Ktu = Kut = 0): f = fu - Kup Ktp^-1 (ft - Ktt Kpt^-1 fp),
+// k = Kuu + Kup Ktp^-1 Ktt Kpt^-1 Kpu.
+void condense_3f(int nd, const double *fu, const double *Kuu, const double *blk, double *fe, double *lk) {
+  const double fp = blk[0], ft = blk[1], Ktp = blk[2], Ktt = blk[3], Kpt = Ktp;
+  const double KtpI = 1.0 / Ktp, KptI = 1.0 / Kpt;
+  const double *Kup = blk + 4;
   for (int r = 0; r < nd; r++) fe[r] = fu[r] + Kup[r] * KtpI * Ktt * KptI * fp - Kup[r] * KtpI * ft;
   if (lk)
     for (int r = 0; r < nd; r++)
       for (int c = 0; c < nd; c++) lk[r * nd + c] = Kuu[r * nd + c] + Kup[r] * KtpI * Ktt * KptI * Kup[c];
-  if (blk) {
-    blk[0] = fp;
-    blk[1] = ft;
-    blk[2] = Ktp;
-    blk[3] = Ktt;
-    for (int r = 0; r < nd; r++) blk[4 + r] = Kup[r];
+}
+
+extern "C" int orc_element_3f(const orc_problem *P, const orc_material *mat, long e, const double *u_e,
+                              double Pe, double theta, const double *state_n, double *state_np1, double *fe,
+                              double *lk, double *blk) {
+  const int nd = P->nne * 3;
+  std::vector<double> fu(nd), Kuu(lk ? nd * nd : 0), b(4 + nd);
+  const int err = element_3f_blocks(P, mat, e, u_e, Pe, theta, state_n, state_np1, fu.data(),
+                                    lk ? Kuu.data() : nullptr, b.data());
+  if (err) return err;
+  condense_3f(nd, fu.data(), lk ? Kuu.data() : nullptr, b.data(), fe, lk);
+  if (blk)
+    for (int i = 0; i < 4 + nd; i++) blk[i] = b[i];
+  if (P->nbc_off) {
+    double Xe[30];
+    for (int a = 0; a < P->nne; a++)
+      for (int i = 0; i < 3; i++) Xe[a * 3 + i] = P->X[(long)P->conn[e * P->nne + a] * 3 + i];
+    neumann_faces(P, e, Xe, u_e, fe, lk);
   }
-  if (P->nbc_off) neumann_faces(P, e, Xe, u_e, fe, lk);
   return 0;
 }
 
@@ -1414,6 +1445,141 @@ extern "C" int orc_assemble_transient_state(const orc_problem *P, const orc_mate
       neumann_faces_transient(P, e, Xe, u2, u1, u0, alpha, dt_np1, dt_n, fe.data(), K ? lk.data() : nullptr);
     }
     scatter(P, e, fe.data(), K ? lk.data() : nullptr, R, K);
+  }
+  return err;
+}
+
+// ---------------------------------------------------------------------------
+// Transient three-field element of the hyperelastic model, one rank:
+// residuals_el_constitutive_model_w_inertia_3f (src/constitutive_model.cc:
+// 2960-3229) and stiffness_el_constitutive_model_w_inertia_3f (:2190-2395),
+// combined with the inertia terms by residual_with_inertia /
+// stiffness_with_inertia (src/dynamics.cc:183-447, case CM3F).  With
+// mid(a, b) = (1 - alpha) a + alpha b, the newer mid point takes u_{n+alpha},
+// theta = mid(theta_n, theta_{n+1}), P = mid(P_n, P_{n+1}) and the older one
+// the same from t_{n-1}, t_n:
+//   R_x = -dt_np1 (1 - alpha) R_x(n+alpha) - dt_n alpha R_x(n-1+alpha)   (x = u, p, t)
+//   K_xy = -dt_np1 alpha (1 - alpha) K_xy(n+alpha)   (dt_alpha_1_minus_alpha of
+//        the blocks, src/constitutive_model_3f.cc:297-470)
+//   f = condense(R, K) - f_i,   k = condense(K) - M / dt_np1.
+// Pe3 / th3: per element the values at t_{n+1}, t_n, t_{n-1} (ne x 3).
+// ---------------------------------------------------------------------------
+namespace {
+struct Blocks3fTr {
+  std::vector<double> fu, Kuu, blk;  // combined (scaled) blocks of one element
+};
+
+int element_3f_transient(const orc_problem *P, const orc_material *mat, long e, const double *u2, const double *u1,
+                         const double *u0, const double *Pe3, const double *th3, double alpha, double dt_np1,
+                         double dt_n, bool wantK, Blocks3fTr &B) {
+  const int nd = P->nne * 3;
+  double ua[30], ub[30];
+  for (int i = 0; i < nd; i++) {
+    ua[i] = (1.0 - alpha) * u1[i] + alpha * u2[i];
+    ub[i] = (1.0 - alpha) * u0[i] + alpha * u1[i];
+  }
+  const double *pe = Pe3 + e * 3, *te = th3 + e * 3;
+  const double Pa = (1.0 - alpha) * pe[1] + alpha * pe[0], ta = (1.0 - alpha) * te[1] + alpha * te[0];
+  const double Pb = (1.0 - alpha) * pe[2] + alpha * pe[1], tb = (1.0 - alpha) * te[2] + alpha * te[1];
+  std::vector<double> fua(nd), fub(nd), Kuu(wantK ? nd * nd : 0), ba(4 + nd), bb(4 + nd);
+  int err = element_3f_blocks(P, mat, e, ua, Pa, ta, nullptr, nullptr, fua.data(), wantK ? Kuu.data() : nullptr,
+                              ba.data());
+  if (!err) err = element_3f_blocks(P, mat, e, ub, Pb, tb, nullptr, nullptr, fub.data(), nullptr, bb.data());
+  if (err) return err;
+  const double cA = -dt_np1 * (1.0 - alpha), cB = -dt_n * alpha, kK = -dt_np1 * alpha * (1.0 - alpha);
+  B.fu.assign(nd, 0.0);
+  B.blk.assign(4 + nd, 0.0);
+  for (int r = 0; r < nd; r++) B.fu[r] = cA * fua[r] + cB * fub[r];
+  B.blk[0] = cA * ba[0] + cB * bb[0];  // Rp
+  B.blk[1] = cA * ba[1] + cB * bb[1];  // Rt
+  B.blk[2] = kK * ba[2];               // Ktp
+  B.blk[3] = kK * ba[3];               // Ktt
+  for (int r = 0; r < nd; r++) B.blk[4 + r] = kK * ba[4 + r];  // Kup
+  if (wantK) {
+    B.Kuu.resize(nd * nd);
+    for (int i = 0; i < nd * nd; i++) B.Kuu[i] = kK * Kuu[i];
+  }
+  return 0;
+}
+}  // namespace
+
+extern "C" int orc_assemble_3f_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                         const double *u_n, const double *u_nm1, const double *p_np1,
+                                         const double *p_n, const double *p_nm1, const double *Pe3,
+                                         const double *th3, double alpha, double dt_np1, double dt_n, double rho,
+                                         double *R, double *K) {
+  if (mat->model != ORC_MODEL_HE) return 1;
+  const int nne = P->nne, nd = nne * 3;
+  Quad qr = quad_rule(nne);
+  int err = 0;
+  for (long e = 0; e < P->ne; e++) {
+    double u2[30], u1[30], u0[30], Xe[30];
+    gather_u(P, e, u_np1, p_np1, u2);
+    gather_u(P, e, u_n, p_n, u1);
+    gather_u(P, e, u_nm1, p_nm1, u0);
+    for (int a = 0; a < nne; a++)
+      for (int i = 0; i < 3; i++) Xe[a * 3 + i] = P->X[(long)P->conn[e * nne + a] * 3 + i];
+    Blocks3fTr B;
+    int r = element_3f_transient(P, mat, e, u2, u1, u0, Pe3, th3, alpha, dt_np1, dt_n, K != nullptr, B);
+    if (r) { err += r; continue; }
+    std::vector<double> fe(nd), lk(K ? nd * nd : 0);
+    condense_3f(nd, B.fu.data(), K ? B.Kuu.data() : nullptr, B.blk.data(), fe.data(), K ? lk.data() : nullptr);
+    // inertia (DISP_resid_w_inertia_el, src/dynamics.cc:78-181; mass of
+    // stiffness_with_inertia, :378-392)
+    for (int ip = 0; ip < qr.nint; ip++) {
+      double dN[30], N[10];
+      int terr = 0;
+      const double detJ = PGFem3D_dNdX(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], Xe, dN, &terr);
+      if (terr) { err += terr; break; }
+      const double w = detJ * qr.w[ip];
+      shape_N(nne, qr.ksi[ip], qr.eta[ip], qr.zet[ip], N);
+      double du[3] = {0.0, 0.0, 0.0};
+      for (int a = 0; a < nne; a++)
+        for (int b = 0; b < 3; b++)
+          du[b] += N[a] * (dt_n * u2[a * 3 + b] - (dt_np1 + dt_n) * u1[a * 3 + b] + dt_np1 * u0[a * 3 + b]);
+      for (int a = 0; a < nne; a++)
+        for (int b = 0; b < 3; b++) fe[a * 3 + b] -= rho / dt_np1 / dt_n * N[a] * du[b] * w;
+      if (K)
+        for (int a = 0; a < nne; a++)
+          for (int c = 0; c < nne; c++)
+            for (int b = 0; b < 3; b++) lk[(a * 3 + b) * nd + c * 3 + b] -= rho / dt_np1 * N[a] * N[c] * w;
+    }
+    if (P->nbc_off) {
+      if (!P->nbc_load_n || !P->nbc_load_nm1) { err++; continue; }
+      neumann_faces_transient(P, e, Xe, u2, u1, u0, alpha, dt_np1, dt_n, fe.data(), K ? lk.data() : nullptr);
+    }
+    scatter(P, e, fe.data(), K ? lk.data() : nullptr, R, K);
+  }
+  return err;
+}
+
+// Increments of the element pressure and volume in the transient
+// (update_3f_state_variables_w_inertia, src/constitutive_model.cc:3880-3898,
+// with compute_d_theta_dP, src/constitutive_model_3f.cc:494-549, Ktu = 0):
+// the combined blocks above, d_theta = -Kpt^-1 (Kpu du + Rp),
+// dP = -Ktp^-1 (Rt + Ktt d_theta).
+extern "C" int orc_update_3f_transient(const orc_problem *P, const orc_material *mat, const double *u_np1,
+                                       const double *u_n, const double *u_nm1, const double *p_np1,
+                                       const double *p_n, const double *p_nm1, const double *du,
+                                       const double *Pe3, const double *th3, double alpha, double dt_np1,
+                                       double dt_n, double *dP, double *dtheta) {
+  if (mat->model != ORC_MODEL_HE) return 1;
+  const int nd = P->nne * 3;
+  int err = 0;
+  for (long e = 0; e < P->ne; e++) {
+    double u2[30], u1[30], u0[30], due[30];
+    gather_u(P, e, u_np1, p_np1, u2);
+    gather_u(P, e, u_n, p_n, u1);
+    gather_u(P, e, u_nm1, p_nm1, u0);
+    gather_u(P, e, du, nullptr, due);
+    Blocks3fTr B;
+    int r = element_3f_transient(P, mat, e, u2, u1, u0, Pe3, th3, alpha, dt_np1, dt_n, false, B);
+    if (r) { err += r; continue; }
+    const double Rp = B.blk[0], Rt = B.blk[1], Ktp = B.blk[2], Ktt = B.blk[3], Kpt = Ktp;
+    double Kpu_du = 0.0;
+    for (int i = 0; i < nd; i++) Kpu_du += B.blk[4 + i] * due[i];
+    dtheta[e] = -(Kpu_du + Rp) / Kpt;
+    dP[e] = -(Rt + Ktt * dtheta[e]) / Ktp;
   }
   return err;
 }

@@ -676,4 +676,136 @@ __global__ void k_tf_update(const QpArgs A, const double *dunode, double *dP, do
   dP[e] = A.mat.kappa * dUv - P + A.mat.kappa * d2U * dth;
 }
 
+// The three-field element in the transient (quadratic tets, hyperelastic):
+// the corrections that turn the two condensed quasi-static assemblies at the
+// mid points into the reference's transient condensation
+// (residuals_el_constitutive_model_w_inertia_3f, src/constitutive_model.cc:
+// 2960-3229).  With the blocks of the newer mid point a scaled by
+// kK = -dt_np1 alpha (1 - alpha) and the residuals combined as
+// R_x = cA R_x(a) + cB R_x(b), the condensed residual is
+//   f = cA (fu_a + s_a Kup_a) + cB (fu_b + s_b Kup_b) - cB s_b Kup_b + d Kup_a,
+//   d = cB (c_a fp_b + kappa U'(theta_b) - P_b),
+// c = kappa U''(theta) / W, fp = sum w J - theta W, s = c fp + kappa U'(theta) - P
+// (the first two terms are the condensed assemblies at a and at b): this
+// kernel adds d Kup_a - cB s_b Kup_b into R.  With dunode set it instead
+// forms the local update (compute_d_theta_dP with the combined blocks,
+// :3880-3898): d_theta = (kK Kup_a du + Rp) / (kK W),
+// dP = (Rt + kK W kappa U''(theta_a) d_theta) / (kK W).
+struct TfTrArgs {
+  QpArgs A;               // X, conn, shp, mat, status; unode = u_{n+alpha}
+  const double *unode_b;  // u_{n-1+alpha} at the nodes (SoA 3*nn)
+  const double *mid;      // 4*ne: P_a, theta_a, P_b, theta_b
+  const int *dof;         // 3*nn SoA, 1-based free DOF ids
+  double *R;
+  const double *dunode;   // update mode: du at the nodes
+  double *dP, *dtheta;
+  double cA, cB, kK;
+};
+
+__global__ void k_tf_transient(const TfTrArgs T) {
+  const QpArgs &A = T.A;
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= A.ne) return;
+  const bool upd = T.dunode != nullptr;
+  int nd[10];
+  for (int b = 0; b < 10; b++) nd[b] = A.conn[(long)b * A.ne + e];
+  // point q: reference gradient inverse, w, and F, F^-1, J at both mid points
+  auto point = [&](int q, double *dXi, double &w, double *Fa, double *Fia, double &Ja, double *Fb, double *Fib,
+                   double &Jb, double *Ld) -> bool {
+    double dX[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, da[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0},
+           db[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, dd[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int b = 0; b < 10; b++) {
+      const int n = nd[b];
+      const double g[3] = {A.shp.dNxi[q][b][0], A.shp.dNxi[q][b][1], A.shp.dNxi[q][b][2]};
+      for (int i = 0; i < 3; i++) {
+        const double x = A.X[i * A.nn + n], ua = A.unode[i * A.nn + n], ub = T.unode_b[i * A.nn + n];
+        const double d = upd ? T.dunode[i * A.nn + n] : 0.0;
+        for (int c = 0; c < 3; c++) {
+          dX[i * 3 + c] += g[c] * x;
+          da[i * 3 + c] += g[c] * ua;
+          db[i * 3 + c] += g[c] * ub;
+          dd[i * 3 + c] += g[c] * d;
+        }
+      }
+    }
+    const double detJ = det3(dX);
+    if (!(detJ > 0.0) || !inv3(dX, dXi)) return false;
+    w = detJ * A.shp.w[q];
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) {
+        double fa = (i == j ? 1.0 : 0.0), fb = fa, l = 0.0;
+        for (int c = 0; c < 3; c++) {
+          fa += da[i * 3 + c] * dXi[c * 3 + j];
+          fb += db[i * 3 + c] * dXi[c * 3 + j];
+          l += dd[i * 3 + c] * dXi[c * 3 + j];
+        }
+        Fa[i * 3 + j] = fa;
+        Fb[i * 3 + j] = fb;
+        Ld[i * 3 + j] = l;
+      }
+    Ja = det3(Fa);
+    Jb = det3(Fb);
+    return Ja > 0.0 && Jb > 0.0 && inv3(Fa, Fia) && inv3(Fb, Fib);
+  };
+  double W = 0.0, SJa = 0.0, SJb = 0.0, Kdu = 0.0;
+  bool ok = true;
+  for (int q = 0; q < 4 && ok; q++) {
+    double dXi[9], w, Fa[9], Fia[9], Ja, Fb[9], Fib[9], Jb, Ld[9];
+    ok = point(q, dXi, w, Fa, Fia, Ja, Fb, Fib, Jb, Ld);
+    if (!ok) break;
+    W += w;
+    SJa += w * Ja;
+    SJb += w * Jb;
+    if (upd) {
+      double tr = 0.0;
+      for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) tr += Ld[i * 3 + j] * Fia[j * 3 + i];
+      Kdu += w * Ja * tr;
+    }
+  }
+  if (!ok) {
+    atomicAdd(&A.status[0], 1ull);
+    if (upd) T.dP[e] = T.dtheta[e] = 0.0;
+    return;
+  }
+  const double Pa = T.mid[e], tha = T.mid[A.ne + e], Pb = T.mid[2 * A.ne + e], thb = T.mid[3 * A.ne + e];
+  const double kap = A.mat.kappa;
+  double dUa, d2Ua, dUb, d2Ub;
+  vol_derivs(A.mat.vol_pot, tha, dUa, d2Ua);
+  vol_derivs(A.mat.vol_pot, thb, dUb, d2Ub);
+  if (upd) {
+    const double Rp = T.cA * (SJa - tha * W) + T.cB * (SJb - thb * W);
+    const double Rt = W * (T.cA * (kap * dUa - Pa) + T.cB * (kap * dUb - Pb));
+    const double dth = (T.kK * Kdu + Rp) / (T.kK * W);
+    T.dtheta[e] = dth;
+    T.dP[e] = (Rt + T.kK * W * kap * d2Ua * dth) / (T.kK * W);
+    return;
+  }
+  const double ca = kap * d2Ua / W, cb = kap * d2Ub / W, fpb = SJb - thb * W;
+  const double sb = cb * fpb + kap * dUb - Pb;
+  const double da_ = T.cB * (ca * fpb + kap * dUb - Pb), db_ = -T.cB * sb;
+  double out[10][3];
+  for (int b = 0; b < 10; b++) out[b][0] = out[b][1] = out[b][2] = 0.0;
+  for (int q = 0; q < 4; q++) {
+    double dXi[9], w, Fa[9], Fia[9], Ja, Fb[9], Fib[9], Jb, Ld[9];
+    point(q, dXi, w, Fa, Fia, Ja, Fb, Fib, Jb, Ld);
+    for (int b = 0; b < 10; b++) {
+      double gX[3];  // dN_b / dX
+      for (int j = 0; j < 3; j++)
+        gX[j] = A.shp.dNxi[q][b][0] * dXi[0 * 3 + j] + A.shp.dNxi[q][b][1] * dXi[1 * 3 + j] +
+                A.shp.dNxi[q][b][2] * dXi[2 * 3 + j];
+      for (int k = 0; k < 3; k++) {
+        const double ta = gX[0] * Fia[0 * 3 + k] + gX[1] * Fia[1 * 3 + k] + gX[2] * Fia[2 * 3 + k];
+        const double tb = gX[0] * Fib[0 * 3 + k] + gX[1] * Fib[1 * 3 + k] + gX[2] * Fib[2 * 3 + k];
+        out[b][k] += w * (da_ * Ja * ta + db_ * Jb * tb);
+      }
+    }
+  }
+  for (int b = 0; b < 10; b++)
+    for (int k = 0; k < 3; k++) {
+      const int id = T.dof[k * A.nn + nd[b]];
+      if (id > 0) atomicAdd(T.R + (id - 1), out[b][k]);
+    }
+}
+
 }  // namespace pgb

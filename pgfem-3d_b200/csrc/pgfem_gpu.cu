@@ -113,6 +113,10 @@ struct pgfem_gpu_ctx {
   // mid-point / combination vector of each, the second residual
   double *tr_buf = nullptr;
   double *tr_F = nullptr;  // crystal plasticity: F at t_n and t_{n-1} per element (SoA 2 x 9*ne)
+  // three-field transient: P_n, theta_n, P_{n-1}, theta_{n-1} per element
+  // (4*ne), and scratch for the mid-point P, theta (4*ne) and u_{n-1+a} at
+  // the nodes (3*nn)
+  double *tf_hist = nullptr, *tf_mid = nullptr;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -329,7 +333,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_desc_tr, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
-                  c->nbc_load, c->tr_buf, c->state_nm1, c->tr_F};
+                  c->nbc_load, c->tr_buf, c->state_nm1, c->tr_F, c->tf_hist, c->tf_mid};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->zfork) cudaEventDestroy(c->zfork);
@@ -1150,8 +1154,32 @@ int pgfem_gpu_set_three_field(pgfem_gpu_ctx *c, const double *P, const double *t
   if (!c->tf_P && ((r = dalloc(c, &c->tf_P, c->ne)) || (r = dalloc(c, &c->tf_theta, c->ne)))) return r;
   CK(cudaMemcpyAsync(c->tf_P, P, sizeof(double) * c->ne, cudaMemcpyHostToDevice, c->stream));
   CK(cudaMemcpyAsync(c->tf_theta, theta, sizeof(double) * c->ne, cudaMemcpyHostToDevice, c->stream));
+  if (!c->tf_hist) {  // the history starts at the given values
+    if ((r = dalloc(c, &c->tf_hist, (size_t)4 * c->ne))) return r;
+    for (int k = 0; k < 2; k++) {
+      CK(cudaMemcpyAsync(c->tf_hist + (size_t)2 * k * c->ne, P, sizeof(double) * c->ne, cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaMemcpyAsync(c->tf_hist + (size_t)(2 * k + 1) * c->ne, theta, sizeof(double) * c->ne,
+                         cudaMemcpyHostToDevice, c->stream));
+    }
+  }
   CK(cudaStreamSynchronize(c->stream));
   c->three_field = 1;
+  return PGFEM_GPU_OK;
+}
+
+int pgfem_gpu_set_three_field_history(pgfem_gpu_ctx *c, const double *P_n, const double *theta_n,
+                                      const double *P_nm1, const double *theta_nm1) {
+  if (!c || !c->three_field || !c->tf_hist || !P_n || !theta_n || !P_nm1 || !theta_nm1) return PGFEM_GPU_EINVAL;
+  for (long e = 0; e < c->ne; e++)
+    if (!(theta_n[e] > 0.0) || !(theta_nm1[e] > 0.0) || !std::isfinite(theta_n[e]) ||
+        !std::isfinite(theta_nm1[e]) || !std::isfinite(P_n[e]) || !std::isfinite(P_nm1[e]))
+      return PGFEM_GPU_EINVAL;
+  const double *src[4] = {P_n, theta_n, P_nm1, theta_nm1};
+  for (int k = 0; k < 4; k++)
+    CK(cudaMemcpyAsync(c->tf_hist + (size_t)k * c->ne, src[k], sizeof(double) * c->ne, cudaMemcpyHostToDevice,
+                       c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return PGFEM_GPU_OK;
 }
 
@@ -1505,6 +1533,13 @@ int pgfem_gpu_commit_state(pgfem_gpu_ctx *c) {
   if (c->state_nm1)  // n-1 <- n first
     CK(cudaMemcpyAsync(c->state_nm1, c->state_n, sizeof(double) * c->nstate * c->nqp, cudaMemcpyDeviceToDevice,
                        c->stream));
+  if (c->three_field && c->tf_hist) {  // three-field P, theta: n-1 <- n <- the current values
+    CK(cudaMemcpyAsync(c->tf_hist + (size_t)2 * c->ne, c->tf_hist, sizeof(double) * 2 * c->ne,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->tf_hist, c->tf_P, sizeof(double) * c->ne, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->tf_hist + c->ne, c->tf_theta, sizeof(double) * c->ne, cudaMemcpyDeviceToDevice,
+                       c->stream));
+  }
   if (c->nstate)
     CK(cudaMemcpyAsync(c->state_n, c->state_np1, sizeof(double) * c->nstate * c->nqp,
                        cudaMemcpyDeviceToDevice, c->stream));
@@ -1856,14 +1891,102 @@ static int transient_cp(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, 
   return assemble_cp(c, c->d_R, dK, dt_np1, s, nullptr, &tr);
 }
 
+// Mid-point P and theta of the three-field element: (P_a, theta_a) =
+// mid(values at t_n, current), (P_b, theta_b) = mid(t_{n-1}, t_n).
+__global__ void k_tf_mid(long ne, const double *P, const double *th, const double *hist, double a, double *mid) {
+  const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const double Pn = hist[e], tn = hist[ne + e], Pm = hist[2 * ne + e], tm = hist[3 * ne + e];
+  mid[e] = (1.0 - a) * Pn + a * P[e];
+  mid[ne + e] = (1.0 - a) * tn + a * th[e];
+  mid[2 * ne + e] = (1.0 - a) * Pm + a * Pn;
+  mid[3 * ne + e] = (1.0 - a) * tm + a * tn;
+}
+
+// The three-field transient's mid points (device buffers as transient_cp):
+// mid-point P and theta, u_{n-1+a} at the nodes in the scratch, and the
+// correction kernel's arguments.
+static int tf_transient_prep(pgfem_gpu_ctx *c, double alpha, double dt_np1, double dt_n, TfTrArgs &T) {
+  int r;
+  if (!c->tf_mid && (r = dalloc(c, &c->tf_mid, (size_t)4 * c->ne + 3 * c->nn))) return r;
+  T = TfTrArgs{};
+  T.A.X = c->X;
+  T.A.unode = c->unode;
+  T.A.conn = c->conn;
+  T.A.nn = c->nn;
+  T.A.ne = c->ne;
+  T.A.status = c->status;
+  T.A.mat = c->mat;
+  T.A.shp = c->shp;
+  T.unode_b = c->tf_mid + (size_t)4 * c->ne;
+  T.mid = c->tf_mid;
+  T.dof = c->dof;
+  T.cA = -dt_np1 * (1.0 - alpha);
+  T.cB = -dt_n * alpha;
+  T.kK = -dt_np1 * alpha * (1.0 - alpha);
+  return PGFEM_GPU_OK;
+}
+
+// The three-field transient (hyperelastic, quadratic tets): the condensed
+// assemblies at the two mid points (the older, residual only, first: its
+// call uses the K scratch), combined as the one-field transient combines
+// them, then k_tf_transient's correction of the condensation.
+static int transient_3f(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, const double *tu0,
+                        const double *tp2, const double *tp1, const double *tp0, double *tua, double *tpa,
+                        double *tR2, double alpha, double dt_np1, double dt_n, bool wantK, cudaStream_t s) {
+  TfTrArgs T;
+  int r = tf_transient_prep(c, alpha, dt_np1, dt_n, T);
+  if (r) return r;
+  const long nd = c->ndof, np = c->npres;
+  const unsigned gu = (unsigned)((std::max<long>(1, nd) + 255) / 256),
+                 gp = (unsigned)((std::max<long>(1, np) + 255) / 256),
+                 g3 = (unsigned)((3 * c->nn + 255) / 256), ge = (unsigned)((c->ne + 127) / 128);
+  double *pres = np ? tpa : nullptr;
+  k_tf_mid<<<ge, 128, 0, s>>>(c->ne, c->tf_P, c->tf_theta, c->tf_hist, alpha, c->tf_mid);
+  double *P_cur = c->tf_P, *th_cur = c->tf_theta;
+  auto restore = [&]() {
+    c->tf_P = P_cur;
+    c->tf_theta = th_cur;
+    c->nbc_desc_cur = nullptr;
+  };
+  // older mid point: u_{n-1+a}, P_b, theta_b
+  k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, nd);
+  if (np) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, np);
+  c->tf_P = c->tf_mid + (size_t)2 * c->ne;
+  c->tf_theta = c->tf_mid + (size_t)3 * c->ne;
+  if (c->nbc_nface) c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
+  r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n);
+  if (r) {
+    restore();
+    return r;
+  }
+  k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, tua, pres, c->tf_mid + (size_t)4 * c->ne);
+  // newer mid point: u_{n+a}, P_a, theta_a
+  k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, nd);
+  if (np) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, np);
+  c->tf_P = c->tf_mid;
+  c->tf_theta = c->tf_mid + c->ne;
+  c->nbc_desc_cur = c->nbc_nface ? c->nbc_desc_tr : nullptr;
+  r = assemble_device(c, tua, pres, c->d_R, wantK ? c->d_K : nullptr, s, dt_np1);
+  restore();
+  if (r) return r;
+  k_scale_add<<<gu, 256, 0, s>>>(c->d_R, T.cA, tR2, T.cB, nd);
+  if (wantK) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, T.kK, nullptr, 0.0, c->nnz);
+  T.R = c->d_R;
+  k_tf_transient<<<ge, 128, 0, s>>>(T);  // c->unode holds u_{n+a}
+  CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
 int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
                                     const double *u_nm1, const double *presc_np1, const double *presc_n,
                                     const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
                                     double *R, double *K, pgfem_gpu_status *st) {
   if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
     return PGFEM_GPU_EINVAL;
-  if ((c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) || c->F0 || c->elem_group || c->three_field)
-    return PGFEM_GPU_EINVAL;
+  if ((c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) || c->F0 || c->elem_group) return PGFEM_GPU_EINVAL;
+  // the three-field transient divides by alpha (1 - alpha) in its local update
+  if (c->three_field && (!c->tf_hist || !(alpha > 0.0 && alpha < 1.0))) return PGFEM_GPU_EINVAL;
   // surface loads need their values at t_n and t_{n-1}
   if (c->nbc_nface && c->nbc_hist_n.size() != (size_t)3 * c->nbc_nfeat) return PGFEM_GPU_EINVAL;
   if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
@@ -1904,7 +2027,11 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
     CK(cudaMemcpyAsync(c->nbc_desc_tr, d.data(), sizeof(double) * d.size(), cudaMemcpyHostToDevice, s));
     c->nbc_desc_cur = c->nbc_desc_tr;
   }
-  if (c->model == PGFEM_MODEL_CP) {
+  if (c->three_field) {
+    r = transient_3f(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, K != nullptr, s);
+    c->nbc_desc_cur = nullptr;
+    if (r) return r;
+  } else if (c->model == PGFEM_MODEL_CP) {
     r = transient_cp(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, K != nullptr, s);
     c->nbc_desc_cur = nullptr;
     if (r) return r;
@@ -1967,6 +2094,58 @@ int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *c, const double *d_u, const doub
                                  double dt, double *d_R, double *d_K, void *stream) {
   if (!c || !d_u || !d_R || !d_K) return PGFEM_GPU_EINVAL;
   return assemble_device(c, d_u, d_presc, d_R, d_K, (cudaStream_t)stream, dt);
+}
+
+int pgfem_gpu_three_field_increments_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
+                                               const double *u_nm1, const double *presc_np1,
+                                               const double *presc_n, const double *presc_nm1, const double *du,
+                                               double alpha, double dt_np1, double dt_n, double *dP,
+                                               double *dtheta, pgfem_gpu_status *st) {
+  if (!c || !c->three_field || !c->tf_hist || c->model != PGFEM_MODEL_HE || !u_np1 || !u_n || !u_nm1 || !du ||
+      !dP || !dtheta || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
+    return PGFEM_GPU_EINVAL;
+  if (!(alpha > 0.0 && alpha < 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0)) return PGFEM_GPU_EINVAL;
+  int r = ensure_scratch(c, false);
+  if (r) return r;
+  const long nd = std::max<long>(1, c->ndof), np = std::max<long>(1, c->npres);
+  if (!c->tr_buf && (r = dalloc(c, &c->tr_buf, (size_t)5 * nd + 4 * np))) return r;
+  if (!c->tf_dunode && ((r = dalloc(c, &c->tf_dunode, 3 * c->nn)) || (r = dalloc(c, &c->tf_inc, 2 * c->ne))))
+    return r;
+  double *tu2 = c->tr_buf, *tu1 = tu2 + nd, *tu0 = tu1 + nd, *tua = tu0 + nd, *tdu = tua + nd;
+  double *tp2 = tdu + nd, *tp1 = tp2 + np, *tp0 = tp1 + np, *tpa = tp0 + np;
+  cudaStream_t s = c->stream;
+  const size_t bu = sizeof(double) * c->ndof, bp = sizeof(double) * c->npres;
+  CK(cudaMemcpyAsync(tu2, u_np1, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu1, u_n, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu0, u_nm1, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tdu, du, bu, cudaMemcpyHostToDevice, s));
+  if (c->npres) {
+    CK(cudaMemcpyAsync(tp2, presc_np1, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp1, presc_n, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp0, presc_nm1, bp, cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), s));
+  TfTrArgs T;
+  if ((r = tf_transient_prep(c, alpha, dt_np1, dt_n, T))) return r;
+  const unsigned gu = (unsigned)((nd + 255) / 256), gp = (unsigned)((np + 255) / 256),
+                 g3 = (unsigned)((3 * c->nn + 255) / 256), ge = (unsigned)((c->ne + 127) / 128);
+  double *pres = c->npres ? tpa : nullptr;
+  k_tf_mid<<<ge, 128, 0, s>>>(c->ne, c->tf_P, c->tf_theta, c->tf_hist, alpha, c->tf_mid);
+  k_blend<<<gu, 256, 0, s>>>(tua, tu0, tu1, alpha, c->ndof);
+  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp0, tp1, alpha, c->npres);
+  k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, tua, pres, c->tf_mid + (size_t)4 * c->ne);
+  k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
+  if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
+  k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, tua, pres, c->unode);
+  k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, tdu, nullptr, c->tf_dunode);
+  T.dunode = c->tf_dunode;
+  T.dP = c->tf_inc;
+  T.dtheta = c->tf_inc + c->ne;
+  k_tf_transient<<<ge, 128, 0, s>>>(T);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(dP, c->tf_inc, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(dtheta, c->tf_inc + c->ne, sizeof(double) * c->ne, cudaMemcpyDeviceToHost, s));
+  return read_status(c, st, false);
 }
 
 int pgfem_gpu_read_status(pgfem_gpu_ctx *c, pgfem_gpu_status *st, int clear) {

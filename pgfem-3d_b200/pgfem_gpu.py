@@ -83,6 +83,9 @@ def lib():
             "pgfem_gpu_three_field_enabled": (C.c_int, [_P]),
             "pgfem_gpu_three_field_increments": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
             "pgfem_gpu_three_field_update_device": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+            "pgfem_gpu_set_three_field_history": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_gpu_three_field_increments_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
+                                                                     C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
             "pgfem_gpu_device_bytes": (C.c_long, [_P]),
             "pgfem_gpu_nnz": (C.c_long, [_P]),
@@ -345,6 +348,26 @@ class Context:
         st = Status()
         _check("pgfem_gpu_three_field_increments", lib().pgfem_gpu_three_field_increments(
             self.h, _ptr(u), _ptr(self._presc(u_presc)), _ptr(du), _ptr(dP), _ptr(dth), C.byref(st)))
+        return dP, dth, st
+
+    def set_three_field_history(self, P_n, theta_n, P_nm1, theta_nm1):
+        """Three-field P and theta per element at t_n and t_{n-1} (the
+        transient element's mid points)."""
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (P_n, theta_n, P_nm1, theta_nm1)]
+        _check("pgfem_gpu_set_three_field_history", lib().pgfem_gpu_set_three_field_history(
+            self.h, *[_ptr(x) for x in a]))
+
+    def three_field_increments_transient(self, u_np1, u_n, u_nm1, du, alpha, dt_np1, dt_n,
+                                         presc=(None, None, None)):
+        """Transient three-field local update: (dP, dtheta, Status) after the
+        displacement increment du."""
+        us = [np.ascontiguousarray(v, dtype=np.float64) for v in (u_np1, u_n, u_nm1, du)]
+        ps = [self._presc(v) for v in presc]
+        dP, dth = np.zeros(self.ne), np.zeros(self.ne)
+        st = Status()
+        _check("pgfem_gpu_three_field_increments_transient", lib().pgfem_gpu_three_field_increments_transient(
+            self.h, *[_ptr(v) for v in us[:3]], *[_ptr(v) for v in ps], _ptr(us[3]), alpha, dt_np1, dt_n,
+            _ptr(dP), _ptr(dth), C.byref(st)))
         return dP, dth, st
 
     def set_scatter_mode(self, mode):

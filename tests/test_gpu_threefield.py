@@ -12,7 +12,10 @@ call equals the R of the R+K call, the local update (compute_d_theta_dP)
 equals the oracle's, and the device Newton step -- local update after each
 solve -- follows the oracle's Newton loop to the same displacements,
 pressures and volumes.  The calls the three-field element does not cover are
-rejected."""
+rejected.  The transient form (inertia, mid-point rule; P and theta at t_n and
+t_{n-1} kept by the context): R, K and the local update equal the oracle's
+(orc_assemble_3f_transient / orc_update_3f_transient) at 1e-10, with surface
+loads too, and a commit moves the current P, theta to t_n and t_n to t_{n-1}."""
 import numpy as np
 import pytest
 from scipy.sparse import csr_matrix
@@ -231,3 +234,113 @@ def test_larger_mesh_free_body_and_translations(gpu):
         t[rows] = 1.0
         assert np.abs(Km @ t).max() <= 1e-10 * np.abs(Km).sum(axis=1).max()
     ctx.close()
+
+
+def _tr_case(seed=9):
+    """Displacements, prescribed values, element pressures and volumes at
+    t_{n+1}, t_n, t_{n-1} of a curved quadratic-tet tension box."""
+    p, P, th = _case(seed=seed, vol_pot=3)  # a potential whose U'' varies: theta's history weighs in R
+    rng = np.random.default_rng(seed + 1)
+    h = 1.0 / p.meta["n"]
+    us = [p.u * f + 1e-3 * h * rng.uniform(-1, 1, p.ndof) for f in (1.0, 0.7, 0.4)]
+    ps = [p.u_presc * f for f in (1.0, 0.7, 0.4)]
+    Ps = [P, 0.8 * P + 3.0, 0.5 * P - 4.0]
+    ths = [th, 1.0 + 0.7 * (th - 1.0) + 1e-3, 1.0 + 0.4 * (th - 1.0) - 1e-3]
+    return p, us, ps, Ps, ths
+
+
+def _tr_context(p, Ps, ths):
+    ctx = p.context()
+    ctx.set_three_field(Ps[0], ths[0])
+    ctx.set_three_field_history(Ps[1], ths[1], Ps[2], ths[2])
+    return ctx
+
+
+@pytest.mark.parametrize("alpha", [0.5, 0.3])
+def test_transient_R_K_update_match_oracle(gpu, alpha):
+    p, us, ps, Ps, ths = _tr_case()
+    ctx = _tr_context(p, Ps, ths)
+    dt1, dt0, rho = 0.02, 0.015, 2.0e4
+    R, K, st = ctx.assemble_RK_transient(us[0], us[1], us[2], alpha, dt1, dt0, rho, presc=tuple(ps))
+    assert st.ok(), st.as_dict()
+    Po, mat = oracle.from_workload(p)
+    err, Ro, Ko = Po.assemble_3f_transient(mat, us, Ps, ths, alpha, dt1, dt0, rho, presc=tuple(ps))
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    # the three-field history and the inertia both carry weight
+    _, Rh, _ = Po.assemble_3f_transient(mat, us, [Ps[0]] * 3, [ths[0]] * 3, alpha, dt1, dt0, rho,
+                                        presc=tuple(ps))
+    assert np.linalg.norm(Ro - Rh) > 1e-3 * np.linalg.norm(Ro)
+    _, R0, _ = Po.assemble_3f_transient(mat, us, Ps, ths, alpha, dt1, dt0, 0.0, presc=tuple(ps))
+    assert np.linalg.norm(Ro - R0) > 1e-2 * np.linalg.norm(Ro)
+    # residual only
+    R2, K2, st = ctx.assemble_RK_transient(us[0], us[1], us[2], alpha, dt1, dt0, rho, presc=tuple(ps),
+                                           want_K=False)
+    assert K2 is None and st.ok()
+    check_R(R2, Ro)
+    # the local update
+    du = 1e-3 / p.meta["n"] * np.random.default_rng(3).uniform(-1, 1, p.ndof)
+    dP, dth, st = ctx.three_field_increments_transient(us[0], us[1], us[2], du, alpha, dt1, dt0,
+                                                       presc=tuple(ps))
+    assert st.ok()
+    err, dPo, dtho = Po.update_3f_transient(mat, us, du, Ps, ths, alpha, dt1, dt0, presc=tuple(ps))
+    assert err == 0
+    assert np.abs(dth - dtho).max() <= 1e-10 * np.abs(dtho).max()
+    assert np.abs(dP - dPo).max() <= 1e-10 * np.abs(dPo).max()
+    # commit: the current P, theta become t_n, t_n becomes t_{n-1}
+    ctx.commit_state()
+    Pn = [Ps[0] + 1.0, Ps[0], Ps[1]]
+    tn = [ths[0] * 1.001, ths[0], ths[1]]
+    ctx.set_three_field(Pn[0], tn[0])
+    un = [us[0] * 1.2, us[0], us[1]]
+    pn = [ps[0] * 1.2, ps[0], ps[1]]
+    R, K, st = ctx.assemble_RK_transient(un[0], un[1], un[2], alpha, dt1, dt0, rho, presc=tuple(pn))
+    assert st.ok()
+    err, Ro, Ko = Po.assemble_3f_transient(mat, un, Pn, tn, alpha, dt1, dt0, rho, presc=tuple(pn))
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    ctx.close()
+
+
+def test_transient_with_surface_loads(gpu):
+    p, us, ps, Ps, ths = _tr_case(seed=4)
+    ctx = _tr_context(p, Ps, ths)
+    el, fc = wl.box_faces(p.X, p.conn, 2, 1.0)
+    ft = np.zeros(len(el), dtype=np.int32)
+    types = np.array([3])
+    L2 = np.array([[30.0, -10.0, 5.0]])
+    L1, L0 = 0.7 * L2 + 2.0, 0.4 * L2 - 3.0
+    ctx.set_neumann(el, fc, ft, types, L2)
+    ctx.set_neumann_load_history(L1, L0)
+    alpha, dt1, dt0, rho = 0.4, 0.02, 0.015, 2.0e4
+    R, K, st = ctx.assemble_RK_transient(us[0], us[1], us[2], alpha, dt1, dt0, rho, presc=tuple(ps))
+    assert st.ok(), st.as_dict()
+    Po, mat = oracle.from_workload(p)
+    Po.set_neumann(el, fc, types[ft], L2[ft], load_n=L1[ft], load_nm1=L0[ft])
+    err, Ro, Ko = Po.assemble_3f_transient(mat, us, Ps, ths, alpha, dt1, dt0, rho, presc=tuple(ps))
+    assert err == 0
+    check_R(R, Ro)
+    check_K(K, Ko, p.Ap)
+    P0, _ = oracle.from_workload(p)
+    _, R0, _ = P0.assemble_3f_transient(mat, us, Ps, ths, alpha, dt1, dt0, rho, presc=tuple(ps))
+    assert np.linalg.norm(Ro - R0) > 1e-3 * np.linalg.norm(Ro)
+    ctx.close()
+
+
+def test_transient_rejections(gpu):
+    p, us, ps, Ps, ths = _tr_case()
+    ctx = _tr_context(p, Ps, ths)
+    for a in (0.0, 1.0):  # the local update divides by alpha (1 - alpha)
+        with pytest.raises(pg.PgfemError):
+            ctx.assemble_RK_transient(us[0], us[1], us[2], a, 0.02, 0.015, 1.0, presc=tuple(ps))
+        with pytest.raises(pg.PgfemError):
+            ctx.three_field_increments_transient(us[0], us[1], us[2], us[0], a, 0.02, 0.015, presc=tuple(ps))
+    ctx.close()
+    c2 = p.context()
+    with pytest.raises(pg.PgfemError):  # not three-field
+        c2.three_field_increments_transient(us[0], us[1], us[2], us[0], 0.5, 0.02, 0.015, presc=tuple(ps))
+    with pytest.raises(pg.PgfemError):
+        c2.set_three_field_history(Ps[1], ths[1], Ps[2], ths[2])
+    c2.close()

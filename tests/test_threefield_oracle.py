@@ -175,3 +175,72 @@ def test_j2_condensed_stiffness_is_derivative_of_condensed_residual():
     mat_he = oracle.material(oracle.HE, E=200.0, nu=0.45)
     _, fe_he, _, _ = P.element_3f(mat_he, e, ue, pr, th, want_K=False)
     assert np.linalg.norm(fe - fe_he) > 1e-2 * np.linalg.norm(fe)
+
+
+# ---- transient (inertia) three-field element --------------------------------
+def _tr_setup(n=2, nne=10, fix=True, seed=3):
+    X, conn, ids, ndof, Ap, Ai = _problem(n, nne, fix=fix)
+    P = oracle.Problem(X, conn, ids, ndof, Ap, Ai)
+    rng = np.random.default_rng(seed)
+    ne = conn.shape[0]
+    us = [0.01 * k * rng.uniform(-1, 1, ndof) for k in (3, 2, 1)]  # t_{n+1}, t_n, t_{n-1}
+    Ps = [2.0 * k * rng.uniform(-1, 1, ne) for k in (3, 2, 1)]
+    ths = [1.0 + 0.004 * k * rng.uniform(-1, 1, ne) for k in (3, 2, 1)]
+    return P, us, Ps, ths
+
+
+def test_transient_3f_constant_in_time_is_the_scaled_quasi_static_element():
+    """u, P, theta the same at the three times, rho = 0: both mid points are
+    the quasi-static point, so R = -(dt_np1 (1 - a) + dt_n a) R_qs and
+    K = -dt_np1 a (1 - a) K_qs (the blocks' common factor drops out of the
+    condensation ratios)."""
+    P, us, Ps, ths = _tr_setup()
+    mat = _mat()
+    al, dt1, dt0 = 0.35, 0.2, 0.15
+    err, R, K = P.assemble_3f_transient(mat, [us[0]] * 3, [Ps[0]] * 3, [ths[0]] * 3, al, dt1, dt0, 0.0)
+    assert err == 0
+    err, Rq, Kq = P.assemble_3f(mat, us[0], Ps[0], ths[0])
+    assert err == 0
+    np.testing.assert_allclose(R, -(dt1 * (1 - al) + dt0 * al) * Rq, rtol=0, atol=1e-12 * np.abs(Rq).max())
+    np.testing.assert_allclose(K, -dt1 * al * (1 - al) * Kq, rtol=0, atol=1e-12 * np.abs(Kq).max())
+
+
+def test_transient_3f_inertia_part_is_the_one_field_one():
+    P, us, Ps, ths = _tr_setup()
+    mat = _mat()
+    al, dt1, dt0, rho = 0.6, 0.2, 0.15, 40.0
+    _, R1, K1 = P.assemble_3f_transient(mat, us, Ps, ths, al, dt1, dt0, rho)
+    _, R0, K0 = P.assemble_3f_transient(mat, us, Ps, ths, al, dt1, dt0, 0.0)
+    _, r1, k1 = oracle.assemble_transient(P, mat, *us, al, dt1, dt0, rho)
+    _, r0, k0 = oracle.assemble_transient(P, mat, *us, al, dt1, dt0, 0.0)
+    np.testing.assert_allclose(R1 - R0, r1 - r0, rtol=0, atol=1e-12 * np.abs(r1 - r0).max())
+    np.testing.assert_allclose(K1 - K0, k1 - k0, rtol=0, atol=1e-12 * np.abs(k1 - k0).max())
+
+
+def test_transient_3f_newton_converges_quadratically():
+    """Newton on (u_{n+1}, P_{n+1}, theta_{n+1}) with the condensed transient K
+    and the transient local update (compute_d_theta_dP with the combined
+    blocks): the condensed residual falls quadratically, so K and the update
+    are the exact linearisation of the mid-point three-field system."""
+    P, us, Ps, ths = _tr_setup(seed=5)
+    mat = _mat()
+    al, dt1, dt0, rho = 0.5, 0.05, 0.04, 20.0
+    from scipy.sparse import csr_matrix
+    from scipy.sparse.linalg import spsolve
+    u2, P2, t2 = us[0].copy(), Ps[0].copy(), ths[0].copy()
+    hist = []
+    for it in range(8):
+        err, R, K = P.assemble_3f_transient(mat, [u2, us[1], us[2]], [P2, Ps[1], Ps[2]], [t2, ths[1], ths[2]],
+                                            al, dt1, dt0, rho)
+        assert err == 0
+        hist.append(np.linalg.norm(R))
+        if hist[-1] <= 1e-11 * hist[0]:
+            break
+        du = spsolve(csr_matrix((K, P.Ai, P.Ap), shape=(P.ndof, P.ndof)).tocsc(), -R)
+        err, dP, dth = P.update_3f_transient(mat, [u2, us[1], us[2]], du, [P2, Ps[1], Ps[2]],
+                                             [t2, ths[1], ths[2]], al, dt1, dt0)
+        assert err == 0
+        u2, P2, t2 = u2 + du, P2 + dP, t2 + dth
+    assert hist[-1] <= 1e-11 * hist[0] and len(hist) <= 6, hist
+    rates = [hist[k + 1] / hist[k] ** 2 for k in range(1, len(hist) - 1) if hist[k] > 1e-8 * hist[0]]
+    assert rates and max(rates) * hist[0] < 10.0, (hist, rates)
