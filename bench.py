@@ -924,6 +924,137 @@ def run_nr(args, ws, rank, local):
     return out
 
 
+def run_transient(args, ws, rank, local):
+    """The transient (inertia, mid-point rule) element on the device
+    (pgfem_gpu_assemble_RK_transient_device): `cp_tr` -- crystal plasticity on
+    the config-3 mesh (`--cp-n`), states at t_{n-1}, t_n from two committed load
+    steps of the tension ramp, u_{n+1} the third step; `he3f_tr` -- the
+    three-field neo-Hookean element on the config-2 mesh (`--n`), P and theta
+    histories set.  A step = one transient R+K call (alpha 0.5, rho 7.85e-9,
+    dt 0.1); the quasi-static R+K at u_{n+1} is timed beside it."""
+    import torch
+
+    import pgfem_gpu as pg
+    import workloads as wl
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cp = args.workload == "cp_tr"
+    t0 = time.perf_counter()
+    alpha, dt1, dt0, rho = 0.5, 0.1, 0.1, 7.85e-9
+
+    def problem(n):
+        if cp:
+            q = wl.cp_p1(n=n, seed=2)
+            us = [q.displacement(3), q.displacement(2), q.displacement(1)]
+            return q, us, None, None
+        q = wl.j2_p2(n=n, seed=1)
+        q.mat = pg.material(pg.MODEL_HE, E=200e3, nu=0.45)
+        q.state = None
+        r = np.random.default_rng(4)
+        us = [q.u, 0.7 * q.u, 0.4 * q.u]
+        Ps = [np.zeros(q.ne), 5.0 * r.uniform(-1, 1, q.ne), 2.0 * r.uniform(-1, 1, q.ne)]
+        ths = [np.ones(q.ne), 1.0 + 1e-3 * r.uniform(-1, 1, q.ne), 1.0 + 1e-3 * r.uniform(-1, 1, q.ne)]
+        return q, us, Ps, ths
+
+    p, us, Ps, ths = problem(args.cp_n if cp else args.n)
+    ctx = p.context()
+    if cp:
+        for k in (1, 2):
+            _, _, st = ctx.assemble_RK(p.displacement(k), dt=p.dt)
+            assert st.ok(), st.as_dict()
+            ctx.commit_state()
+        dt1 = dt0 = p.dt
+    else:
+        ctx.set_three_field(Ps[0], ths[0])
+        ctx.set_three_field_history(Ps[1], ths[1], Ps[2], ths[2])
+    log("[rank %d] %s setup %.1f s, %d elements, %d nnz" % (rank, args.workload, time.perf_counter() - t0, p.ne,
+                                                          p.nnz))
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+    d_us = [torch.from_numpy(np.ascontiguousarray(u)).to(dev) for u in us]
+    d_R = torch.empty(p.ndof, dtype=torch.float64, device=dev)
+    d_K = torch.empty(p.nnz, dtype=torch.float64, device=dev)
+    ptrs = [d.data_ptr() for d in d_us]
+
+    def step():
+        ctx.assemble_RK_transient_device(ptrs, [0, 0, 0], alpha, dt1, dt0, rho, d_R.data_ptr(), d_K.data_ptr(), sh)
+
+    def quasi():
+        ctx.assemble_RK_device(ptrs[0], None, d_R.data_ptr(), d_K.data_ptr(), sh, dt=dt1)
+
+    def timed(fn, n):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    st = ctx.read_status(clear=True)
+    assert st.ok(), st.as_dict()
+    clk = ClockSampler(local)
+    clk.start()
+    time.sleep(0.3)
+    barrier(ws)
+    torch.cuda.synchronize()
+    ms = allreduce_max(timed(step, args.steps), ws)
+    clocks = clk.stop()
+    ms_qs = timed(quasi, 3)
+    # end to end: the host-buffer call (three displacement vectors in, R and K out)
+    t0 = time.perf_counter()
+    ne2 = 2
+    for _ in range(ne2):
+        ctx.assemble_RK_transient(us[0], us[1], us[2], alpha, dt1, dt0, rho)
+    e2e_s = (time.perf_counter() - t0) / ne2
+    nqp = p.ne * (1 if cp else 4)
+    out = {"metric": "quad-points/sec for the FP64 transient (mid-point rule) R+K", "value": nqp / (ms * 1e-3),
+           "unit": "qp/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded splitmix64 mesh perturbation / load ramp)",
+           "config": {"workload": ("crystal plasticity, linear tets, %d^3 cells x 6 (%d elements), transient R+K "
+                                   "with the mid-point plastic state" % (args.cp_n, p.ne)) if cp else
+                                  ("three-field neo-Hookean, quadratic tets, %d^3 cells x 6 (%d elements, %d qp, "
+                                   "%d nnz), transient R+K: two condensed assemblies + correction + inertia"
+                                   % (args.n, p.ne, nqp, p.nnz)),
+                      "alpha": alpha, "dt": [dt1, dt0], "rho": rho, "quasi_static_ms": ms_qs,
+                      "transient_over_quasi_static": ms / ms_qs,
+                      "l2": "inputs larger than L2 (K values %.2f GB)" % (8e-9 * p.nnz),
+                      "parallelism": "replicas%d" % ws if ws > 1 else "1 GPU"},
+           "roofline": None,
+           "roofline_note": "the transient call runs the quasi-static kernels (CP: one point update and the "
+                            "mid-point element; three-field: two condensed assemblies), whose rooflines are the "
+                            "cp_p1 and he3f_p2 lines; this line reports its cost against the quasi-static iterate",
+           "clocks": clocks,
+           "e2e": {"value": nqp / e2e_s, "unit": "qp/s", "h2d_bytes_per_step": 3 * 8 * p.ndof,
+                   "d2h_bytes_per_step": 8 * (p.ndof + p.nnz), "timer": "host wall clock around the synchronous call"}}
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        n_s = 16 if cp else 12
+        q, qus, qPs, qths = problem(n_s)
+        P, mat = oracle.from_workload(q)
+        t0 = time.perf_counter()
+        if cp:
+            _, _, _, s1 = P.assemble(mat, q.displacement(1), state_n=q.state, dt=q.dt, want_K=False)
+            _, _, _, s2 = P.assemble(mat, q.displacement(2), state_n=s1, dt=q.dt, want_K=False)
+            t0 = time.perf_counter()
+            oracle.assemble_transient_cp(P, mat, qus[0], qus[1], qus[2], alpha, q.dt, q.dt, rho, s1, s2)
+        else:
+            P.assemble_3f_transient(mat, qus, qPs, qths, alpha, dt1, dt0, rho)
+        t_cpu = time.perf_counter() - t0
+        nq = q.ne * (1 if cp else 4)
+        out["cpu_baseline"] = {"value": nq / t_cpu, "unit": "qp/s", "cores": 1, "kind": "port",
+                               "sample": "the same transient call on the %d^3-cell mesh (%d qp), oracle, 1 thread, "
+                                         "%.2f s" % (n_s, nq, t_cpu)}
+    ctx.close()
+    return out
+
+
 def run_reference(args, ws, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
@@ -977,7 +1108,7 @@ def main():
     ap.add_argument("--ref-layers", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scatter", default="atomic", choices=["atomic", "colour"])
-    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he3f_p2", "he_p1", "cp_p1", "cp_warm", "rve_batch",
+    ap.add_argument("--workload", default="j2_p2", choices=["j2_p2", "he3f_p2", "he_p1", "cp_p1", "cp_warm", "cp_tr", "he3f_tr", "rve_batch",
                                                          "nr_step"])
     ap.add_argument("--nr-n", type=int, default=16)
     ap.add_argument("--nr-stretch", type=float, default=0.003)
@@ -1011,6 +1142,8 @@ def main():
         out = run_rve(args, ws, rank, local)
     elif args.workload == "nr_step":
         out = run_nr(args, ws, rank, local)
+    elif args.workload in ("cp_tr", "he3f_tr"):
+        out = run_transient(args, ws, rank, local)
     else:
         out = run_ours(args, ws, rank, local)
     if rank == 0:

@@ -274,6 +274,15 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *ctx, const double *u_np1, con
                                     const double *u_nm1, const double *presc_np1, const double *presc_n,
                                     const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
                                     double *R, double *K, pgfem_gpu_status *st);
+/* The same on device buffers (free-DOF displacements d_u_* [ndof], prescribed
+ * values d_presc_* [npres], outputs d_R [ndof], d_K [nnz] or NULL), enqueued
+ * on stream (NULL: the context's stream); no copies, no synchronisation; the
+ * status accumulates until pgfem_gpu_read_status clears it. */
+int pgfem_gpu_assemble_RK_transient_device(pgfem_gpu_ctx *ctx, const double *d_u_np1, const double *d_u_n,
+                                           const double *d_u_nm1, const double *d_presc_np1,
+                                           const double *d_presc_n, const double *d_presc_nm1, double alpha,
+                                           double dt_np1, double dt_n, double rho, double *d_R, double *d_K,
+                                           void *stream);
 /* Launch count of the kernels of one assemble_RK call (for accounting). */
 int pgfem_gpu_launches_per_assembly(const pgfem_gpu_ctx *ctx);
 

@@ -1978,38 +1978,17 @@ static int transient_3f(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, 
   return PGFEM_GPU_OK;
 }
 
-int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
-                                    const double *u_nm1, const double *presc_np1, const double *presc_n,
-                                    const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
-                                    double *R, double *K, pgfem_gpu_status *st) {
-  if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
-    return PGFEM_GPU_EINVAL;
-  if ((c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) || c->F0 || c->elem_group) return PGFEM_GPU_EINVAL;
-  // the three-field transient divides by alpha (1 - alpha) in its local update
-  if (c->three_field && (!c->tf_hist || !(alpha > 0.0 && alpha < 1.0))) return PGFEM_GPU_EINVAL;
-  // surface loads need their values at t_n and t_{n-1}
-  if (c->nbc_nface && c->nbc_hist_n.size() != (size_t)3 * c->nbc_nfeat) return PGFEM_GPU_EINVAL;
-  if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
-    return PGFEM_GPU_EINVAL;
-  // below the reference's density threshold the element is the quasi-static one
-  if (std::fabs(rho) < 1.0e-16) return assemble_host(c, u_np1, presc_np1, R, K, st, dt_np1);
-  int r = ensure_scratch(c, K != nullptr);
-  if (r) return r;
+// The transient element on device buffers (displacements and prescribed
+// values at the three times), into the context's R and K buffers (K when
+// wantK): the surface-load descriptors, the mid-point assemblies and their
+// combination, and the inertia kernel.
+static int transient_core(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, const double *tu0,
+                          const double *tp2, const double *tp1, const double *tp0, double alpha, double dt_np1,
+                          double dt_n, double rho, bool wantK, cudaStream_t s) {
+  int r;
   const long nd = std::max<long>(1, c->ndof), np = std::max<long>(1, c->npres);
   if (!c->tr_buf && (r = dalloc(c, &c->tr_buf, (size_t)5 * nd + 4 * np))) return r;
-  double *tu2 = c->tr_buf, *tu1 = tu2 + nd, *tu0 = tu1 + nd, *tua = tu0 + nd, *tR2 = tua + nd;
-  double *tp2 = tR2 + nd, *tp1 = tp2 + np, *tp0 = tp1 + np, *tpa = tp0 + np;
-  cudaStream_t s = c->stream;
-  const size_t bu = sizeof(double) * c->ndof, bp = sizeof(double) * c->npres;
-  CK(cudaMemcpyAsync(tu2, u_np1, bu, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(tu1, u_n, bu, cudaMemcpyHostToDevice, s));
-  CK(cudaMemcpyAsync(tu0, u_nm1, bu, cudaMemcpyHostToDevice, s));
-  if (c->npres) {
-    CK(cudaMemcpyAsync(tp2, presc_np1, bp, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(tp1, presc_n, bp, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(tp0, presc_nm1, bp, cudaMemcpyHostToDevice, s));
-  }
-  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), s));
+  double *tua = c->tr_buf + 3 * nd, *tR2 = tua + nd, *tpa = c->tr_buf + 5 * nd + 3 * np;
   const unsigned gu = (unsigned)((nd + 255) / 256), gp = (unsigned)((np + 255) / 256);
   double *pres = c->npres ? tpa : nullptr;
   if (c->nbc_nface) {
@@ -2028,11 +2007,11 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
     c->nbc_desc_cur = c->nbc_desc_tr;
   }
   if (c->three_field) {
-    r = transient_3f(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, K != nullptr, s);
+    r = transient_3f(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, wantK, s);
     c->nbc_desc_cur = nullptr;
     if (r) return r;
   } else if (c->model == PGFEM_MODEL_CP) {
-    r = transient_cp(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, K != nullptr, s);
+    r = transient_cp(c, tu2, tu1, tu0, tp2, tp1, tp0, tua, tpa, tR2, alpha, dt_np1, dt_n, wantK, s);
     c->nbc_desc_cur = nullptr;
     if (r) return r;
   } else {
@@ -2040,7 +2019,7 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
     k_blend<<<gu, 256, 0, s>>>(tua, tu1, tu2, alpha, c->ndof);
     if (c->npres) k_blend<<<gp, 256, 0, s>>>(tpa, tp1, tp2, alpha, c->npres);
     CK(cudaGetLastError());
-    r = assemble_device(c, tua, pres, c->d_R, K ? c->d_K : nullptr, s, dt_np1);
+    r = assemble_device(c, tua, pres, c->d_R, wantK ? c->d_K : nullptr, s, dt_np1);
     if (r) {
       c->nbc_desc_cur = nullptr;
       return r;
@@ -2055,7 +2034,7 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
     if (r) return r;
     // the mid-point combination
     k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
-    if (K) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
+    if (wantK) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
                                                                          nullptr, 0.0, c->nnz);
   }
   // inertia: v = dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1} at the nodes
@@ -2079,15 +2058,81 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const
   ia.cR = rho / (dt_np1 * dt_n);
   ia.cK = rho / dt_np1;
   ia.R = c->d_R;
-  ia.K = K ? c->d_K : nullptr;
+  ia.K = wantK ? c->d_K : nullptr;
   ia.shp = c->shp;
   const unsigned ge = (unsigned)((c->ne + 127) / 128);
   if (c->nne == 10) k_inertia<10, 4><<<ge, 128, 0, s>>>(ia);
   else k_inertia<4, 1><<<ge, 128, 0, s>>>(ia);
   CK(cudaGetLastError());
+  return PGFEM_GPU_OK;
+}
+
+// Context and time parameters a transient call accepts.
+static bool transient_ok(const pgfem_gpu_ctx *c, double alpha, double dt_np1, double dt_n, double rho) {
+  if ((c->model != PGFEM_MODEL_HE && c->model != PGFEM_MODEL_CP) || c->F0 || c->elem_group) return false;
+  // the three-field transient divides by alpha (1 - alpha) in its local update
+  if (c->three_field && (!c->tf_hist || !(alpha > 0.0 && alpha < 1.0))) return false;
+  // surface loads need their values at t_n and t_{n-1}
+  if (c->nbc_nface && c->nbc_hist_n.size() != (size_t)3 * c->nbc_nfeat) return false;
+  if (!(alpha >= 0.0 && alpha <= 1.0) || !(dt_np1 > 0.0) || !(dt_n > 0.0) || !std::isfinite(rho))
+    return false;
+  return true;
+}
+
+int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *c, const double *u_np1, const double *u_n,
+                                    const double *u_nm1, const double *presc_np1, const double *presc_n,
+                                    const double *presc_nm1, double alpha, double dt_np1, double dt_n, double rho,
+                                    double *R, double *K, pgfem_gpu_status *st) {
+  if (!c || !u_np1 || !u_n || !u_nm1 || !R || (c->npres && (!presc_np1 || !presc_n || !presc_nm1)))
+    return PGFEM_GPU_EINVAL;
+  if (!transient_ok(c, alpha, dt_np1, dt_n, rho)) return PGFEM_GPU_EINVAL;
+  // below the reference's density threshold the element is the quasi-static one
+  if (std::fabs(rho) < 1.0e-16) return assemble_host(c, u_np1, presc_np1, R, K, st, dt_np1);
+  int r = ensure_scratch(c, K != nullptr);
+  if (r) return r;
+  const long nd = std::max<long>(1, c->ndof), np = std::max<long>(1, c->npres);
+  if (!c->tr_buf && (r = dalloc(c, &c->tr_buf, (size_t)5 * nd + 4 * np))) return r;
+  double *tu2 = c->tr_buf, *tu1 = tu2 + nd, *tu0 = tu1 + nd;
+  double *tp2 = c->tr_buf + 5 * nd, *tp1 = tp2 + np, *tp0 = tp1 + np;
+  cudaStream_t s = c->stream;
+  const size_t bu = sizeof(double) * c->ndof, bp = sizeof(double) * c->npres;
+  CK(cudaMemcpyAsync(tu2, u_np1, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu1, u_n, bu, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(tu0, u_nm1, bu, cudaMemcpyHostToDevice, s));
+  if (c->npres) {
+    CK(cudaMemcpyAsync(tp2, presc_np1, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp1, presc_n, bp, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(tp0, presc_nm1, bp, cudaMemcpyHostToDevice, s));
+  }
+  CK(cudaMemsetAsync(c->status, 0, 4 * sizeof(unsigned long long), s));
+  r = transient_core(c, tu2, tu1, tu0, tp2, tp1, tp0, alpha, dt_np1, dt_n, rho, K != nullptr, s);
+  if (r) return r;
   CK(cudaMemcpyAsync(R, c->d_R, bu, cudaMemcpyDeviceToHost, s));
   if (K) CK(cudaMemcpyAsync(K, c->d_K, sizeof(double) * c->nnz, cudaMemcpyDeviceToHost, s));
   return read_status(c, st, false);
+}
+
+int pgfem_gpu_assemble_RK_transient_device(pgfem_gpu_ctx *c, const double *d_u_np1, const double *d_u_n,
+                                           const double *d_u_nm1, const double *d_presc_np1,
+                                           const double *d_presc_n, const double *d_presc_nm1, double alpha,
+                                           double dt_np1, double dt_n, double rho, double *d_R, double *d_K,
+                                           void *stream) {
+  if (!c || !d_u_np1 || !d_u_n || !d_u_nm1 || !d_R || (c->npres && (!d_presc_np1 || !d_presc_n || !d_presc_nm1)))
+    return PGFEM_GPU_EINVAL;
+  if (!transient_ok(c, alpha, dt_np1, dt_n, rho)) return PGFEM_GPU_EINVAL;
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  if (std::fabs(rho) < 1.0e-16) return assemble_device(c, d_u_np1, d_presc_np1, d_R, d_K, s, dt_np1);
+  int r = ensure_scratch(c, false);
+  if (r) return r;
+  // the core writes the context's R and K buffers: point them at the caller's
+  double *R0 = c->d_R, *K0 = c->d_K;
+  c->d_R = d_R;
+  if (d_K) c->d_K = d_K;
+  r = transient_core(c, d_u_np1, d_u_n, d_u_nm1, d_presc_np1, d_presc_n, d_presc_nm1, alpha, dt_np1, dt_n, rho,
+                     d_K != nullptr, s);
+  c->d_R = R0;
+  if (d_K) c->d_K = K0;
+  return r;
 }
 
 int pgfem_gpu_assemble_RK_device(pgfem_gpu_ctx *c, const double *d_u, const double *d_presc,

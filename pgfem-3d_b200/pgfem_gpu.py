@@ -84,6 +84,8 @@ def lib():
             "pgfem_gpu_three_field_increments": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
             "pgfem_gpu_three_field_update_device": (C.c_int, [_P, _P, _P, _P, _P, _P]),
             "pgfem_gpu_set_three_field_history": (C.c_int, [_P, _P, _P, _P, _P]),
+            "pgfem_gpu_assemble_RK_transient_device": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.c_double, C.c_double,
+                                                                 C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_gpu_three_field_increments_transient": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
                                                                      C.c_double, C.c_double, _P, _P, _P]),
             "pgfem_mlp_set_wait_test": (C.c_int, [_P, C.c_double, C.c_int]),
@@ -439,6 +441,13 @@ class Context:
             self.h, *[_ptr(v) for v in us], *[_ptr(v) for v in ps], alpha, dt_np1, dt_n, rho, _ptr(R), _ptr(K),
             C.byref(st)))
         return R, K, st
+
+    def assemble_RK_transient_device(self, d_us, d_ps, alpha, dt_np1, dt_n, rho, d_R, d_K, stream):
+        """Device pointers (ints): d_us, d_ps at t_{n+1}, t_n, t_{n-1} (d_ps
+        entries 0 without prescribed values), d_R, d_K (0: residual only) and a
+        cudaStream_t handle (int)."""
+        _check("pgfem_gpu_assemble_RK_transient_device", lib().pgfem_gpu_assemble_RK_transient_device(
+            self.h, *d_us, *d_ps, alpha, dt_np1, dt_n, rho, d_R, d_K or None, stream))
 
     def assemble_RK_device(self, d_u, d_presc, d_R, d_K, stream, dt=0.0):
         """Device pointers (ints) and a cudaStream_t handle (int)."""

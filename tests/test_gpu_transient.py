@@ -187,6 +187,16 @@ def test_cp_transient_matches_oracle(gpu, alpha):
     R2, K2, st = ctx.assemble_RK_transient(us[2], us[1], us[0], alpha, dt1, dt0, rho, want_K=False)
     assert K2 is None and st.ok()
     check_R(R2, R, 1e-13)
+    # the device-buffer entry point: the same R and K
+    import torch
+    d_us = [torch.from_numpy(np.ascontiguousarray(u)).cuda() for u in (us[2], us[1], us[0])]
+    d_R = torch.empty(p.ndof, dtype=torch.float64, device="cuda")
+    d_K = torch.empty(p.nnz, dtype=torch.float64, device="cuda")
+    ctx.assemble_RK_transient_device([d.data_ptr() for d in d_us], [0, 0, 0], alpha, dt1, dt0, rho, d_R.data_ptr(),
+                                     d_K.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    check_R(d_R.cpu().numpy(), R, 1e-13)
+    check_K(d_K.cpu().numpy(), K, p.Ap, 1e-13)
     # commit: t_n -> t_{n-1}, t_{n+1} -> t_n
     ctx.commit_state()
     assert np.abs(ctx.get_state(2) - s_n).max() <= 1e-10 * np.abs(s_n).max()
