@@ -276,7 +276,8 @@ int pgfem_gpu_assemble_RK_transient(pgfem_gpu_ctx *ctx, const double *u_np1, con
                                     double *R, double *K, pgfem_gpu_status *st);
 /* The same on device buffers (free-DOF displacements d_u_* [ndof], prescribed
  * values d_presc_* [npres], outputs d_R [ndof], d_K [nnz] or NULL), enqueued
- * on stream (NULL: the context's stream); no copies, no synchronisation; the
+ * on stream (a cudaStream_t; NULL is the default stream, as for
+ * pgfem_gpu_assemble_RK_device); no copies, no synchronisation; the
  * status accumulates until pgfem_gpu_read_status clears it. */
 int pgfem_gpu_assemble_RK_transient_device(pgfem_gpu_ctx *ctx, const double *d_u_np1, const double *d_u_n,
                                            const double *d_u_nm1, const double *d_presc_np1,

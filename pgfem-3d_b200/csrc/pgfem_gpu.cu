@@ -2120,7 +2120,7 @@ int pgfem_gpu_assemble_RK_transient_device(pgfem_gpu_ctx *c, const double *d_u_n
   if (!c || !d_u_np1 || !d_u_n || !d_u_nm1 || !d_R || (c->npres && (!d_presc_np1 || !d_presc_n || !d_presc_nm1)))
     return PGFEM_GPU_EINVAL;
   if (!transient_ok(c, alpha, dt_np1, dt_n, rho)) return PGFEM_GPU_EINVAL;
-  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  cudaStream_t s = (cudaStream_t)stream;  // as assemble_RK_device: 0 is the default stream
   if (std::fabs(rho) < 1.0e-16) return assemble_device(c, d_u_np1, d_presc_np1, d_R, d_K, s, dt_np1);
   int r = ensure_scratch(c, false);
   if (r) return r;
