@@ -117,6 +117,9 @@ struct pgfem_gpu_ctx {
   // (4*ne), and scratch for the mid-point P, theta (4*ne) and u_{n-1+a} at
   // the nodes (3*nn)
   double *tf_hist = nullptr, *tf_mid = nullptr;
+  // transient calls: minus the consistent mass of unit density, CSR-aligned
+  // (nnz; geometry only, formed on the first transient R+K call)
+  double *mass_csr = nullptr;
   // kernel timing
   bool timing = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> events;
@@ -333,7 +336,7 @@ void release(pgfem_gpu_ctx *c) {
                   c->cp_R, c->cp_F, c->cp_detJw, c->cp_out, c->cp_guess, c->cp_iters, c->cp_counter,
                   c->cp_Fn, c->cp_feat, c->cp_pred, c->cp_fallbacks, c->elem_group, c->F0_tab, c->cp_conv,
                   c->sched_ticket, c->p2m_ticket, c->tf_P, c->tf_theta, c->tf_dunode, c->tf_inc, c->nbc_desc_tr, c->nbc_elem, c->nbc_feat, c->nbc_type, c->nbc_off, c->nbc_face,
-                  c->nbc_load, c->tr_buf, c->state_nm1, c->tr_F, c->tf_hist, c->tf_mid};
+                  c->nbc_load, c->tr_buf, c->state_nm1, c->tr_F, c->tf_hist, c->tf_mid, c->mass_csr};
   for (void *p : ptrs)
     if (p) cudaFree(p);
   if (c->zfork) cudaEventDestroy(c->zfork);
@@ -1971,7 +1974,6 @@ static int transient_3f(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, 
   restore();
   if (r) return r;
   k_scale_add<<<gu, 256, 0, s>>>(c->d_R, T.cA, tR2, T.cB, nd);
-  if (wantK) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, T.kK, nullptr, 0.0, c->nnz);
   T.R = c->d_R;
   k_tf_transient<<<ge, 128, 0, s>>>(T);  // c->unode holds u_{n+a}
   CK(cudaGetLastError());
@@ -2034,8 +2036,6 @@ static int transient_core(pgfem_gpu_ctx *c, const double *tu2, const double *tu1
     if (r) return r;
     // the mid-point combination
     k_scale_add<<<gu, 256, 0, s>>>(c->d_R, -dt_np1 * (1.0 - alpha), tR2, -dt_n * alpha, c->ndof);
-    if (wantK) k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, -alpha * (1.0 - alpha) * dt_np1,
-                                                                         nullptr, 0.0, c->nnz);
   }
   // inertia: v = dt_n u_{n+1} - (dt_np1 + dt_n) u_n + dt_np1 u_{n-1} at the nodes
   k_comb3<<<gu, 256, 0, s>>>(tua, tu2, dt_n, tu1, -(dt_np1 + dt_n), tu0, dt_np1, c->ndof);
@@ -2058,11 +2058,28 @@ static int transient_core(pgfem_gpu_ctx *c, const double *tu2, const double *tu1
   ia.cR = rho / (dt_np1 * dt_n);
   ia.cK = rho / dt_np1;
   ia.R = c->d_R;
-  ia.K = wantK ? c->d_K : nullptr;
+  ia.K = nullptr;  // the mass enters K below, from the cached CSR-aligned array
   ia.shp = c->shp;
   const unsigned ge = (unsigned)((c->ne + 127) / 128);
   if (c->nne == 10) k_inertia<10, 4><<<ge, 128, 0, s>>>(ia);
   else k_inertia<4, 1><<<ge, 128, 0, s>>>(ia);
+  if (wantK) {
+    // K = kscale K - rho / dt_np1 M: the mid-point stiffness factor (the CP
+    // element applies its own) and the consistent mass, in one pass
+    if (!c->mass_csr) {
+      if ((r = dalloc(c, &c->mass_csr, std::max<long>(1, c->nnz)))) return r;
+      CK(cudaMemsetAsync(c->mass_csr, 0, sizeof(double) * c->nnz, s));
+      InertiaArgs im = ia;
+      im.R = nullptr;
+      im.K = c->mass_csr;
+      im.cK = 1.0;
+      if (c->nne == 10) k_inertia<10, 4><<<ge, 128, 0, s>>>(im);
+      else k_inertia<4, 1><<<ge, 128, 0, s>>>(im);
+    }
+    const double kscale = c->model == PGFEM_MODEL_CP && !c->three_field ? 1.0 : -alpha * (1.0 - alpha) * dt_np1;
+    k_scale_add<<<(unsigned)((c->nnz + 255) / 256), 256, 0, s>>>(c->d_K, kscale, c->mass_csr, rho / dt_np1,
+                                                                   c->nnz);
+  }
   CK(cudaGetLastError());
   return PGFEM_GPU_OK;
 }

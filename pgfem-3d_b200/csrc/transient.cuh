@@ -50,13 +50,14 @@ struct InertiaArgs {
   const double *vnode;   // 3*nn SoA: v of the element nodes
   double cR;             // rho / (dt_np1 dt_n): f_i scale
   double cK;             // rho / dt_np1: mass scale
-  double *R, *K;         // K may be null
+  double *R, *K;         // either may be null
   ShapeTable shp;
 };
 
-// One thread per element: f_i into R (subtracted) and the mass into the
+// One thread per element: f_i into R (subtracted) and/or the mass into the
 // component-diagonal K entries (subtracted), FP64 atomics through the
-// element's node-block map.
+// element's node-block map.  The transient call forms the mass once (K alone,
+// cK = 1, into a cached CSR-aligned array) and then runs this kernel for R.
 template <int NNE, int NQP>
 __global__ void __launch_bounds__(128) k_inertia(const InertiaArgs A) {
   const long e = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -115,7 +116,7 @@ __global__ void __launch_bounds__(128) k_inertia(const InertiaArgs A) {
 #pragma unroll
     for (int b = 0; b < 3; b++) {
       if (!((ma >> b) & 1u)) continue;
-      atomicAdd(&A.R[A.dof[b * A.nn + nd[a]] - 1], -fi[a][b]);
+      if (A.R) atomicAdd(&A.R[A.dof[b * A.nn + nd[a]] - 1], -fi[a][b]);
       if (!A.K) continue;
       const long row = (long)A.rowptr0[nd[a]] + (long)__popc(ma & ((1u << b) - 1u)) * A.rowlen[nd[a]];
 #pragma unroll
