@@ -808,4 +808,58 @@ __global__ void k_tf_transient(const TfTrArgs T) {
     }
 }
 
+// Residual of the condensed three-field element from its point records alone
+// (quadratic tets; the residual rows of k_assemble_p2m without its stiffness):
+// R_bi = sum_q sum_j (w tau_ij + w J s delta_ij) p_qb,j with p_qb = G_q^T dN_b/dxi,
+// s = c (sum w J - theta W) + kappa U'(theta) - P, c = kappa U''(theta) / W;
+// w tau = record fields 9..14 minus the geometric term h on the diagonal.
+// One thread per record slot (element perm[es]); inverted elements have zeroed
+// records (W = 0) and are skipped, as the assembly skips them.
+__global__ void k_tf_residual(const QpArgs A, const int *dof, double *R) {
+  constexpr int NRF = kYRecTF;
+  const long es = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (es >= A.ne) return;
+  const long e = A.perm ? (long)A.perm[es] : es;
+  const double *rec = A.qrec;
+  double W = 0.0, SJ = 0.0;
+  for (int q = 0; q < 4; q++) {
+    SJ += rec[yrec_idx<NRF>(es * 4 + q, 26)];
+    W += rec[yrec_idx<NRF>(es * 4 + q, 27)];
+  }
+  if (!(W > 0.0)) return;
+  const double th = rec[yrec_idx<NRF>(es * 4, 28)], Pe = rec[yrec_idx<NRF>(es * 4, 29)];
+  double dU, d2U;
+  vol_derivs(A.mat.vol_pot, th, dU, d2U);
+  const double c = A.mat.kappa * d2U / W;
+  const double sc = c * (SJ - th * W) + A.mat.kappa * dU - Pe;
+  double out[10][3];
+  for (int b = 0; b < 10; b++) out[b][0] = out[b][1] = out[b][2] = 0.0;
+  for (int q = 0; q < 4; q++) {
+    const long qs = es * 4 + q;
+    double G[9], T[3][3];
+    for (int k = 0; k < 9; k++) G[k] = rec[yrec_idx<NRF>(qs, k)];
+    const double h = rec[yrec_idx<NRF>(qs, 25)], wJs = rec[yrec_idx<NRF>(qs, 26)] * sc;
+    double wt[6];
+    for (int k = 0; k < 6; k++) wt[k] = rec[yrec_idx<NRF>(qs, 9 + k)] - (k < 3 ? h : 0.0);
+    // Voigt order xx yy zz yz xz xy
+    T[0][0] = wt[0] + wJs; T[1][1] = wt[1] + wJs; T[2][2] = wt[2] + wJs;
+    T[1][2] = T[2][1] = wt[3];
+    T[0][2] = T[2][0] = wt[4];
+    T[0][1] = T[1][0] = wt[5];
+    for (int b = 0; b < 10; b++) {
+      const double g0 = A.shp.dNxi[q][b][0], g1 = A.shp.dNxi[q][b][1], g2 = A.shp.dNxi[q][b][2];
+      double p[3];
+      for (int j = 0; j < 3; j++) p[j] = G[j] * g0 + G[3 + j] * g1 + G[6 + j] * g2;
+      for (int i = 0; i < 3; i++) out[b][i] += T[i][0] * p[0] + T[i][1] * p[1] + T[i][2] * p[2];
+    }
+  }
+  for (int b = 0; b < 10; b++) {
+    const int n = A.conn[(long)b * A.ne + e];
+    for (int i = 0; i < 3; i++) {
+      const int id = dof[i * A.nn + n];
+      if (id > 0) atomicAdd(R + (id - 1), out[b][i]);
+    }
+  }
+}
+
 }  // namespace pgb

@@ -1931,9 +1931,10 @@ static int tf_transient_prep(pgfem_gpu_ctx *c, double alpha, double dt_np1, doub
 }
 
 // The three-field transient (hyperelastic, quadratic tets): the condensed
-// assemblies at the two mid points (the older, residual only, first: its
-// call uses the K scratch), combined as the one-field transient combines
-// them, then k_tf_transient's correction of the condensation.
+// residual at the older mid point (point records + k_tf_residual), the
+// condensed R+K assembly at the newer one, combined as the one-field
+// transient combines them, then k_tf_transient's correction of the
+// condensation.
 static int transient_3f(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, const double *tu0,
                         const double *tp2, const double *tp1, const double *tp0, double *tua, double *tpa,
                         double *tR2, double alpha, double dt_np1, double dt_n, bool wantK, cudaStream_t s) {
@@ -1958,7 +1959,23 @@ static int transient_3f(pgfem_gpu_ctx *c, const double *tu2, const double *tu1, 
   c->tf_P = c->tf_mid + (size_t)2 * c->ne;
   c->tf_theta = c->tf_mid + (size_t)3 * c->ne;
   if (c->nbc_nface) c->nbc_desc_cur = c->nbc_desc_tr + (size_t)kNbcDesc * c->nbc_nfeat;
-  r = assemble_device(c, tua, pres, tR2, nullptr, s, dt_n);
+  // residual only: the point records, then their residual rows (no stiffness)
+  CK(cudaMemsetAsync(tR2, 0, sizeof(double) * nd, s));
+  k_expand_u<<<g3, 256, 0, s>>>(c->dof, c->nn, tua, pres, c->unode);
+  r = launch_qp_update<10, 4, PGFEM_MODEL_HE, true>(c, s);
+  if (!r) {
+    QpArgs q{};
+    q.conn = c->conn;
+    q.nn = c->nn;
+    q.ne = c->ne;
+    q.qrec = c->qrec;
+    q.perm = c->perm;
+    q.mat = c->mat;
+    q.shp = c->shp;
+    k_tf_residual<<<ge, 128, 0, s>>>(q, c->dof, tR2);
+    CK(cudaGetLastError());
+    r = launch_neumann(c, tR2, nullptr, s);
+  }
   if (r) {
     restore();
     return r;
